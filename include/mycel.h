@@ -1,0 +1,208 @@
+/*
+ * mycel_b200 — C ABI of the B200 (sm_100a) implementation of Mycel.Core's FEM + SIMP inner loop.
+ *
+ * The reference (zmalrobot/mycel, C#/.NET 10) has no FFI today; its seams are the public static entry points
+ * TopologyOptimizer.Run and StaticAnalysis.Run plus the kernels they call. Each entry point below names the
+ * reference member it replaces (file:line, paths inside the reference project). A C# host binds these with
+ * [DllImport("mycel_b200")]; buffers are caller-owned, read or written only during the call (pin them with
+ * `fixed`), and all device memory is owned by the library and stays resident between calls.
+ *
+ * Conventions: every function returns int32_t status (MYCEL_OK = 0). Vectors are box-sized like the
+ * reference's: DOF vectors have 3*(nx+1)*(ny+1)*(nz+1) doubles (dof = 3*node + c), element arrays have
+ * nx*ny*nz entries (e = ix + nx*(iy + ny*iz)); "active" arrays list active elements in ascending e.
+ * Calls on one problem are not re-entrant (the reference serialises solves through FemWorkTeam's lock).
+ */
+#ifndef MYCEL_B200_H
+#define MYCEL_B200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (reference exception each one maps to) ---- */
+#define MYCEL_OK 0
+#define MYCEL_E_ARG 1               /* ArgumentException / ArgumentOutOfRangeException */
+#define MYCEL_E_UNDERCONSTRAINED 2  /* InvalidOperationException: < 6 fixed DOFs on active nodes (PcgSolver.cs:95-100) */
+#define MYCEL_E_NOT_CONVERGED 3     /* InvalidOperationException: "FEM solver did not converge ..." (StaticAnalysis.cs:88-92) */
+#define MYCEL_E_BREAKDOWN 4         /* PCG breakdown reported as a non-converged PcgResult (PcgSolver.cs:245-346) */
+#define MYCEL_E_CANCELLED 5         /* OperationCanceledException / loop break on cancellation (TopologyOptimizer.cs:169-172) */
+#define MYCEL_E_TIMEOUT 6           /* new: a bounded device wait gave up */
+#define MYCEL_E_DEVICE 7            /* new: CUDA error */
+#define MYCEL_E_OOM 8               /* new: device memory or admission budget exhausted */
+#define MYCEL_E_INVALID_OPERATION 9 /* InvalidOperationException (FeModel.AssembleForces: empty patch with force) */
+
+#define MYCEL_PRECISION_FP64 0  /* plain method: FP64 throughout, reproduces the reference's arithmetic */
+#define MYCEL_PRECISION_MIXED 1 /* FP32 inner PCG (K·u, Jacobi) inside FP64 iterative refinement */
+
+typedef struct mycel_ctx mycel_ctx;
+typedef struct mycel_problem mycel_problem;
+typedef struct mycel_filter mycel_filter;
+typedef struct mycel_simp_session mycel_simp_session;
+
+/* GridSpec (Voxelization/GridSpec.cs:11-44); origin does not enter the path. h is float like GridSpec.H. */
+typedef struct {
+  int32_t nx, ny, nz;
+  float h;
+} mycel_grid;
+
+/* FeMaterial(E0, Nu, EminRatio) (Fem/FeMaterial.cs:11-16); Emin = E0 * EminRatio. */
+typedef struct {
+  double e0, nu, emin_ratio;
+} mycel_material;
+
+/* LoadCase(SurfacePatch, Vector3 TotalForce) (Fem/LoadCase.cs:10-19; SurfacePatch.cs:25-49). */
+typedef struct {
+  int32_t n_nodes;
+  const int32_t* nodes;
+  const double* node_area;
+  float force[3];
+} mycel_load_case;
+
+typedef struct {
+  int64_t total_elements, total_nodes, total_dofs;
+  int64_t active_elements, active_nodes, active_fixed_dofs;
+  int64_t device_bytes; /* device memory held by the problem */
+} mycel_problem_info;
+
+/* PcgResult (Fem/PcgResult.cs:7-14) plus refinement bookkeeping of the mixed form. */
+typedef struct {
+  int32_t iterations;
+  double final_residual;
+  int32_t converged;
+  double elapsed_ms;
+  int32_t refinement_steps; /* mixed form: outer FP64 refinement steps; 0 for FP64 */
+  int32_t inner_iterations; /* mixed form: FP32 PCG iterations summed over refinement steps */
+  char message[256];
+} mycel_pcg_result;
+
+/* StaticAnalysisOptions (Fem/StaticAnalysis.cs:8-17); the preconditioner is Jacobi. */
+typedef struct {
+  double tolerance;        /* default 1e-6 */
+  int32_t max_iterations;  /* default 5000 */
+  int32_t throw_on_non_convergence; /* default 1 */
+  int32_t precision;       /* MYCEL_PRECISION_* */
+} mycel_static_options;
+
+/* OptimizerOptions (Optimization/OptimizerOptions.cs:5-26). */
+typedef struct {
+  double volume_fraction;   /* 0.4 */
+  double filter_radius_mm;  /* 2.0 */
+  double penal;             /* 3.0 */
+  double move_limit;        /* 0.2 */
+  int32_t max_iterations;   /* 200 */
+  double solver_tolerance_initial; /* 1e-4 */
+  double solver_tolerance_final;   /* 1e-6 */
+  int32_t solver_max_iterations;   /* 5000 */
+  int32_t continuation;     /* 0 */
+  int32_t enable_heaviside; /* 0 */
+  double rho_min;           /* 1e-3 */
+  const uint8_t* passive_mask; /* box-sized or NULL */
+  int64_t passive_mask_len;
+  int32_t protect_boundary_hinges; /* 1 */
+  const float* initial_density;    /* box-sized or active-sized, or NULL */
+  int64_t initial_density_len;
+  int32_t start_iteration;         /* 1 */
+  const double* warm_start_displacements; /* total_dofs or NULL (other lengths are ignored, as in the reference) */
+  int64_t warm_start_len;
+  int32_t enforce_minimum_filter_radius; /* 1 */
+  int32_t precision;                     /* MYCEL_PRECISION_* */
+} mycel_simp_options;
+
+/* IterationSnapshot scalars + IterationTimings (Optimization/IterationSnapshot.cs:5-31). */
+typedef struct {
+  int32_t iteration;
+  double compliance, volume_fraction, max_change, grey_level;
+  int32_t solver_iterations;
+  double solver_residual;
+  double max_displacement;
+  double solve_ms, sensitivity_ms, filter_ms, update_ms, total_ms;
+  int32_t refinement_steps;
+} mycel_iter_record;
+
+/* IProgress<IterationSnapshot>.Report: called on the calling thread after every SIMP iteration with the
+   record and box-sized float physical/design densities (valid during the call only). */
+typedef void (*mycel_progress_fn)(void* user, const mycel_iter_record* rec, const float* physical_density,
+                                  const float* design_density);
+
+/* ---- context ---- */
+int32_t mycel_version(void);
+int32_t mycel_ctx_create(int32_t device, mycel_ctx** out);
+int32_t mycel_ctx_destroy(mycel_ctx* ctx);
+/* The CUDA stream (cudaStream_t) all work of this context is issued on. */
+void* mycel_ctx_stream(mycel_ctx* ctx);
+/* Message of the last failed call on this context (thread-local copy valid until the next call). */
+const char* mycel_last_error(mycel_ctx* ctx);
+/* Kernel launches issued by this context since creation (all of them are this library's own kernels). */
+int64_t mycel_ctx_launch_count(mycel_ctx* ctx);
+
+/* ---- problem: FeModel + FemOperator (Fem/FeModel.cs:43-184, Fem/FemOperator.cs:33-108) ----
+   element_density: box-sized (default 1.0 when NULL); penal: FeModel.Penal. */
+int32_t mycel_problem_create(mycel_ctx* ctx, const mycel_grid* grid, const uint8_t* domain,
+                             const mycel_material* material, const int32_t* fixed_dofs, int32_t n_fixed,
+                             const mycel_load_case* loads, int32_t n_loads, const double* element_density,
+                             double penal, mycel_problem** out);
+int32_t mycel_problem_destroy(mycel_problem* p);
+int32_t mycel_problem_info_get(mycel_problem* p, mycel_problem_info* out);
+/* FeModel.AssembleForces (Fem/FeModel.cs:263-321): box-sized nodal forces. */
+int32_t mycel_problem_forces(mycel_problem* p, double* f_out);
+
+/* ---- kernel-level entry points ---- */
+/* FemOperator.UpdateDensities (Fem/FemOperator.cs:114-138): E_e = Emin + rho^p (E0-Emin) and DiagA. */
+int32_t mycel_update_densities(mycel_problem* p, const double* density_box, double penal);
+/* FemOperator.DiagA after AssembleDiagonal (Fem/FemOperator.cs:143-172). */
+int32_t mycel_diagonal(mycel_problem* p, double* diag_out);
+/* FemOperator.ApplyK (projected=0, Fem/FemOperator.cs:196-243) / ApplyA with xIsAlreadyProjected (projected=1,
+   :250-273): y = K(rho) x by node-centric gather in the reference's colour order. precision selects the
+   FP64 kernel or the FP32 kernel (x, y converted at the boundary). */
+int32_t mycel_apply_k(mycel_problem* p, const double* x, double* y, int32_t projected, int32_t precision);
+/* PcgSolver.Solve with JacobiPreconditioner (Fem/PcgSolver.cs:80-370): x is the warm start in, solution out. */
+int32_t mycel_pcg_solve(mycel_problem* p, const double* b, double* x, double tol, int32_t max_iterations,
+                        int32_t precision, mycel_pcg_result* res);
+/* StaticAnalysis.Run (Fem/StaticAnalysis.cs:35-142). warm_start may be NULL; a non-NULL warm_start whose
+   length differs from total_dofs is MYCEL_E_ARG (:62-67). reactions_out / von_mises_out may be NULL. */
+int32_t mycel_static_solve(mycel_problem* p, const mycel_static_options* opt, const double* warm_start,
+                           int64_t warm_start_len, double* u_out, double* reactions_out, double* von_mises_out,
+                           double* compliance_out, double* max_displacement_out, mycel_pcg_result* res);
+
+/* DensityFilter (Optimization/DensityFilter.cs:34-199) over the problem's active elements, radius in elements. */
+int32_t mycel_filter_create(mycel_problem* p, double rmin, mycel_filter** out);
+int32_t mycel_filter_destroy(mycel_filter* f);
+/* ApplyFilter (DensityFilter.cs:205-251), ApplySensitivityFilter (:257-303); active-indexed in/out. */
+int32_t mycel_filter_apply(mycel_filter* f, const double* in_active, double* out_active);
+int32_t mycel_filter_adjoint(mycel_filter* f, const double* in_active, double* out_active);
+/* DensityFilter.S (:187-198). */
+int32_t mycel_filter_s(mycel_filter* f, double* s_active);
+
+/* SensitivityAnalysis.ComputeComplianceSensitivities (Optimization/SensitivityAnalysis.cs:13-146). */
+int32_t mycel_sensitivities(mycel_problem* p, const double* u, const double* rho_phys_active, double penal,
+                            double* dc_active);
+/* OcOptimizer.Update (Optimization/OcOptimizer.cs:12-132); passive may be NULL; rho_new may alias rho. */
+int32_t mycel_oc_update(mycel_ctx* ctx, int32_t n, const double* rho, const double* dc, const double* s,
+                        const uint8_t* passive, double* rho_new, double target_volume_fraction, double move_limit,
+                        double rho_min, double lambda_guess, int32_t max_bisection_steps, double volume_tolerance,
+                        double* lambda_out);
+
+/* ---- SIMP loop: TopologyOptimizer.Run (Optimization/TopologyOptimizer.cs:16-407) ----
+   cancel / pause: polled between iterations (CancellationToken, IterationController.CheckAndBlock);
+   history: room for history_cap records; u_out (total_dofs), physical/design_density_out (box, float) may
+   be NULL. Non-convergence of a solve returns MYCEL_E_NOT_CONVERGED with the reference's message. */
+int32_t mycel_simp_run(mycel_problem* p, const mycel_simp_options* opt, mycel_progress_fn progress, void* user,
+                       const volatile int32_t* cancel, const volatile int32_t* pause, mycel_iter_record* history,
+                       int32_t history_cap, int32_t* n_iterations, int32_t* converged, double* u_out,
+                       float* physical_density_out, float* design_density_out);
+
+/* Session form of the same loop for callers that keep the state (rho, u, PCG vectors, lambda) resident and
+   step it themselves (the serving loop, the benchmark). step runs one SIMP iteration; *done is set when the
+   stop rule fires or max_iterations is reached. */
+int32_t mycel_simp_begin(mycel_problem* p, const mycel_simp_options* opt, mycel_simp_session** out);
+int32_t mycel_simp_step(mycel_simp_session* s, mycel_iter_record* rec, int32_t* done);
+int32_t mycel_simp_read(mycel_simp_session* s, double* u_out, float* physical_density_out, float* design_density_out,
+                        double* rho_phys_active_out, double* rho_design_active_out, double* lambda_out);
+int32_t mycel_simp_end(mycel_simp_session* s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,415 @@
+"""Mycel.Core-shaped host interface over the C ABI (the Python side of the drop-in boundary).
+
+``StaticAnalysis.run`` and ``TopologyOptimizer.run`` take the same inputs and return the same results as the
+reference's ``StaticAnalysis.Run`` (src/Mycel.Core/Fem/StaticAnalysis.cs:35) and ``TopologyOptimizer.Run``
+(src/Mycel.Core/Optimization/TopologyOptimizer.cs:16), raising the same error classes. The kernel-level methods
+of ``Problem`` mirror FemOperator / PcgSolver / DensityFilter / SensitivityAnalysis / OcOptimizer.
+All arithmetic runs in libmycel_b200.so on the GPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+from typing import Callable, Optional
+
+import numpy as np
+
+from . import _lib as L
+from .model import (ArgumentError, CancelledError, DeviceError, FeModel, InvalidOperationError, IterationSnapshot,
+                    MycelError, OptimizerOptions, OutOfMemoryError, PcgResult, StaticAnalysisOptions,
+                    StaticAnalysisResult, TimeoutError_, TopologyOptimizationResult)
+
+FP64 = 0
+MIXED = 1
+_PREC = {"fp64": FP64, "mixed": MIXED, FP64: FP64, MIXED: MIXED}
+
+_ERRORS = {1: ArgumentError, 2: InvalidOperationError, 3: InvalidOperationError, 4: InvalidOperationError,
+           5: CancelledError, 6: TimeoutError_, 7: DeviceError, 8: OutOfMemoryError, 9: InvalidOperationError}
+
+
+def _check(status: int, ctx=None):
+    if status == 0:
+        return
+    lib = L.load()
+    msg = lib.mycel_last_error(ctx.handle if ctx is not None else None)
+    text = msg.decode("utf-8", "replace") if msg else f"status {status}"
+    raise _ERRORS.get(status, MycelError)(text)
+
+
+class Context:
+    """One CUDA device and stream (mycel_ctx)."""
+
+    def __init__(self, device: int = 0):
+        lib = L.load()
+        h = C.c_void_p()
+        _check(lib.mycel_ctx_create(device, C.byref(h)))
+        self.handle = h.value
+        self.device = device
+
+    def close(self):
+        if getattr(self, "handle", None):
+            L.load().mycel_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self) -> int:
+        return L.load().mycel_ctx_stream(self.handle) or 0
+
+    @property
+    def launch_count(self) -> int:
+        return int(L.load().mycel_ctx_launch_count(self.handle))
+
+
+_default_ctx = None
+_default_lock = threading.Lock()
+
+
+def default_context() -> Context:
+    global _default_ctx
+    with _default_lock:
+        if _default_ctx is None:
+            _default_ctx = Context(0)
+        return _default_ctx
+
+
+def _pcg_result(r: L.PcgResultC) -> PcgResult:
+    msg = r.message.decode("utf-8", "replace")
+    return PcgResult(int(r.iterations), float(r.final_residual), bool(r.converged), float(r.elapsed_ms), msg or None,
+                     int(r.refinement_steps))
+
+
+class Problem:
+    """A FeModel resident on the device (mycel_problem): FeModel + FemOperator state."""
+
+    def __init__(self, model: FeModel, ctx: Optional[Context] = None):
+        self.ctx = ctx or default_context()
+        self.model = model
+        lib = L.load()
+        g = model.grid
+        grid = L.Grid(g.nx, g.ny, g.nz, float(np.float32(g.h)))
+        mat = L.Material(model.material.e0, model.material.nu, model.material.emin_ratio)
+        self._keep = []
+        loads = (L.LoadCaseC * max(1, len(model.loads)))()
+        for i, lc in enumerate(model.loads):
+            nodes = np.ascontiguousarray(lc.patch.nodes, dtype=np.int32)
+            areas = np.ascontiguousarray(lc.patch.node_area, dtype=np.float64)
+            self._keep += [nodes, areas]
+            loads[i].n_nodes = nodes.size
+            loads[i].nodes = nodes.ctypes.data
+            loads[i].node_area = areas.ctypes.data
+            loads[i].force[:] = [np.float32(v) for v in lc.total_force]
+        fixed = np.ascontiguousarray(model.fixed_dofs, dtype=np.int32)
+        dens = L.f64(model.element_density)
+        h = C.c_void_p()
+        _check(lib.mycel_problem_create(self.ctx.handle, C.byref(grid), model.domain.ctypes.data, C.byref(mat),
+                                        fixed.ctypes.data if fixed.size else None, fixed.size, loads, len(model.loads),
+                                        dens.ctypes.data, model.penal, C.byref(h)), self.ctx)
+        self.handle = h.value
+        self._keep = []
+
+    def close(self):
+        if getattr(self, "handle", None):
+            L.load().mycel_problem_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- info ----
+    def info(self) -> dict:
+        pi = L.ProblemInfo()
+        _check(L.load().mycel_problem_info_get(self.handle, C.byref(pi)), self.ctx)
+        return {k: int(getattr(pi, k)) for k, _ in L.ProblemInfo._fields_}
+
+    @property
+    def n_dofs(self) -> int:
+        return self.model.total_dofs
+
+    def forces(self) -> np.ndarray:
+        f = np.zeros(self.n_dofs)
+        _check(L.load().mycel_problem_forces(self.handle, f.ctypes.data), self.ctx)
+        return f
+
+    # ---- FemOperator ----
+    def update_densities(self, density_box, penal: float):
+        d = L.f64(density_box)
+        _check(L.load().mycel_update_densities(self.handle, d.ctypes.data, float(penal)), self.ctx)
+
+    def diagonal(self) -> np.ndarray:
+        out = np.zeros(self.n_dofs)
+        _check(L.load().mycel_diagonal(self.handle, out.ctypes.data), self.ctx)
+        return out
+
+    def apply_k(self, x, projected: bool = False, precision="fp64") -> np.ndarray:
+        x = L.f64(x)
+        y = np.zeros(self.n_dofs)
+        _check(L.load().mycel_apply_k(self.handle, x.ctypes.data, y.ctypes.data, int(projected), _PREC[precision]),
+               self.ctx)
+        return y
+
+    def apply_a(self, x, precision="fp64") -> np.ndarray:
+        return self.apply_k(x, True, precision)
+
+    # ---- PcgSolver ----
+    def pcg_solve(self, b, x0=None, tol: float = 1e-6, max_iterations: int = 5000, precision="fp64"):
+        b = L.f64(b)
+        x = np.zeros(self.n_dofs) if x0 is None else np.array(x0, dtype=np.float64)
+        r = L.PcgResultC()
+        _check(L.load().mycel_pcg_solve(self.handle, b.ctypes.data, x.ctypes.data, tol, max_iterations,
+                                        _PREC[precision], C.byref(r)), self.ctx)
+        return x, _pcg_result(r)
+
+    # ---- SensitivityAnalysis ----
+    def sensitivities(self, u, rho_phys_active, penal: float) -> np.ndarray:
+        u = L.f64(u)
+        rho = L.f64(rho_phys_active)
+        dc = np.zeros(self.model.active_element_count)
+        _check(L.load().mycel_sensitivities(self.handle, u.ctypes.data, rho.ctypes.data, float(penal), dc.ctypes.data),
+               self.ctx)
+        return dc
+
+
+class DensityFilter:
+    """DensityFilter over a problem's active elements (radius in elements)."""
+
+    def __init__(self, problem: Problem, rmin: float):
+        self.problem = problem
+        h = C.c_void_p()
+        _check(L.load().mycel_filter_create(problem.handle, float(rmin), C.byref(h)), problem.ctx)
+        self.handle = h.value
+        self.n = problem.model.active_element_count
+
+    def close(self):
+        if getattr(self, "handle", None):
+            L.load().mycel_filter_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def apply(self, rho_active) -> np.ndarray:
+        x = L.f64(rho_active)
+        if x.size < self.n:
+            raise ArgumentError("Buffer lengths must be at least ActiveCount.")
+        out = np.zeros(self.n)
+        _check(L.load().mycel_filter_apply(self.handle, x.ctypes.data, out.ctypes.data), self.problem.ctx)
+        return out
+
+    def adjoint(self, dc_active) -> np.ndarray:
+        x = L.f64(dc_active)
+        if x.size < self.n:
+            raise ArgumentError("Buffer lengths must be at least ActiveCount.")
+        out = np.zeros(self.n)
+        _check(L.load().mycel_filter_adjoint(self.handle, x.ctypes.data, out.ctypes.data), self.problem.ctx)
+        return out
+
+    @property
+    def s(self) -> np.ndarray:
+        out = np.zeros(self.n)
+        _check(L.load().mycel_filter_s(self.handle, out.ctypes.data), self.problem.ctx)
+        return out
+
+
+def oc_update(rho, dc, s, passive, target_volume_fraction, move_limit=0.2, rho_min=1e-3, lambda_guess=1.0,
+              max_bisection_steps=60, volume_tolerance=1e-8, ctx: Optional[Context] = None):
+    """OcOptimizer.Update; returns (rho_new, lambda)."""
+    ctx = ctx or default_context()
+    rho = L.f64(rho)
+    n = rho.size
+    dc = L.f64(dc)
+    s = L.f64(s)
+    if dc.size < n or s.size < n:
+        raise ArgumentError("All spans must have length >= rho.Length.")
+    pas = None if passive is None else np.ascontiguousarray(passive, dtype=np.uint8)
+    out = np.zeros(n)
+    lam = C.c_double(0)
+    _check(L.load().mycel_oc_update(ctx.handle, n, rho.ctypes.data, dc.ctypes.data, s.ctypes.data, L.ptr(pas),
+                                    out.ctypes.data, target_volume_fraction, move_limit, rho_min, lambda_guess,
+                                    max_bisection_steps, volume_tolerance, C.byref(lam)), ctx)
+    return out, lam.value
+
+
+class StaticAnalysis:
+    @staticmethod
+    def run(model: FeModel, options: Optional[StaticAnalysisOptions] = None, ctx: Optional[Context] = None,
+            reactions: bool = True, von_mises: bool = True) -> StaticAnalysisResult:
+        options = options or StaticAnalysisOptions()
+        prob = Problem(model, ctx)
+        try:
+            n = model.total_dofs
+            u = np.zeros(n)
+            rx = np.zeros(n) if reactions else None
+            vm = np.zeros(model.total_elements) if von_mises else None
+            ws = None if options.warm_start_displacements is None else L.f64(options.warm_start_displacements)
+            o = L.StaticOptions(options.tolerance, options.max_iterations, int(options.throw_on_non_convergence),
+                                _PREC[options.precision])
+            c = C.c_double(0)
+            md = C.c_double(0)
+            r = L.PcgResultC()
+            _check(L.load().mycel_static_solve(prob.handle, C.byref(o), L.ptr(ws), 0 if ws is None else ws.size,
+                                               u.ctypes.data, L.ptr(rx), L.ptr(vm), C.byref(c), C.byref(md),
+                                               C.byref(r)), prob.ctx)
+            return StaticAnalysisResult(u, c.value, rx, md.value, _pcg_result(r), vm)
+        finally:
+            prob.close()
+
+
+class IterationController:
+    """Cooperative pause / resume / stop between SIMP iterations (IterationController.cs:9-65)."""
+
+    def __init__(self):
+        self._cancel = C.c_int32(0)
+        self._pause = C.c_int32(0)
+
+    def pause(self):
+        self._pause.value = 1
+
+    def resume(self):
+        self._pause.value = 0
+
+    def stop(self):
+        self._cancel.value = 1
+        self._pause.value = 0
+
+    def reset(self):
+        self._cancel.value = 0
+        self._pause.value = 0
+
+    @property
+    def is_paused(self):
+        return bool(self._pause.value)
+
+    @property
+    def is_stopped(self):
+        return bool(self._cancel.value)
+
+
+def _simp_options(o: OptimizerOptions, keep: list) -> L.SimpOptions:
+    def arr(a, dt):
+        if a is None:
+            return None, 0
+        a = np.ascontiguousarray(a, dtype=dt)
+        keep.append(a)
+        return a.ctypes.data, a.size
+
+    pm, pl = arr(o.passive_mask, np.uint8)
+    idp, idl = arr(o.initial_density, np.float32)
+    wp, wl = arr(o.warm_start_displacements, np.float64)
+    return L.SimpOptions(o.volume_fraction, o.filter_radius_mm, o.penal, o.move_limit, o.max_iterations,
+                         o.solver_tolerance_initial, o.solver_tolerance_final, o.solver_max_iterations,
+                         int(o.continuation), int(o.enable_heaviside), o.rho_min, pm, pl,
+                         int(o.protect_boundary_hinges), idp, idl, o.start_iteration, wp, wl,
+                         int(o.enforce_minimum_filter_radius), _PREC[o.precision])
+
+
+def _snapshot(r: L.IterRecord, phys=None, design=None) -> IterationSnapshot:
+    return IterationSnapshot(int(r.iteration), r.compliance, r.volume_fraction, r.max_change, r.grey_level,
+                             int(r.solver_iterations), r.solver_residual, r.max_displacement, r.solve_ms,
+                             r.sensitivity_ms, r.filter_ms, r.update_ms, r.total_ms, phys, design)
+
+
+class TopologyOptimizer:
+    @staticmethod
+    def run(model: FeModel, options: Optional[OptimizerOptions] = None,
+            progress: Optional[Callable[[IterationSnapshot], None]] = None,
+            controller: Optional[IterationController] = None, ctx: Optional[Context] = None,
+            keep_snapshots: bool = False) -> TopologyOptimizationResult:
+        options = options or OptimizerOptions()
+        prob = Problem(model, ctx)
+        keep = []
+        try:
+            so = _simp_options(options, keep)
+            cap = max(1, options.max_iterations - options.start_iteration + 1)
+            hist = (L.IterRecord * cap)()
+            ni = C.c_int32(0)
+            cv = C.c_int32(0)
+            u = np.zeros(model.total_dofs)
+            phys = np.zeros(model.total_elements, dtype=np.float32)
+            des = np.zeros(model.total_elements, dtype=np.float32)
+            snaps_arrays = {}
+            ne = model.total_elements
+
+            def cb(user, rec, pp, dp):
+                r = rec.contents
+                pa = np.ctypeslib.as_array(pp, shape=(ne,)).copy() if (keep_snapshots or progress) else None
+                da = np.ctypeslib.as_array(dp, shape=(ne,)).copy() if (keep_snapshots or progress) else None
+                if keep_snapshots:
+                    snaps_arrays[int(r.iteration)] = (pa, da)
+                if progress is not None:
+                    progress(_snapshot(r, pa, da))
+
+            cfn = L.PROGRESS_FN(cb) if (progress is not None or keep_snapshots) else L.PROGRESS_FN()
+            cancel = controller._cancel if controller else None
+            pause = controller._pause if controller else None
+            st = L.load().mycel_simp_run(prob.handle, C.byref(so), cfn, None,
+                                         C.addressof(cancel) if cancel is not None else None,
+                                         C.addressof(pause) if pause is not None else None, hist, cap, C.byref(ni),
+                                         C.byref(cv), u.ctypes.data, phys.ctypes.data, des.ctypes.data)
+            _check(st, prob.ctx)
+            snaps = []
+            for r in hist[:ni.value]:
+                pa, da = snaps_arrays.get(int(r.iteration), (None, None))
+                snaps.append(_snapshot(r, pa, da))
+            if snaps:
+                snaps[-1].physical_density = phys
+                snaps[-1].design_density = des
+            final_c = snaps[-1].compliance if snaps else 0.0
+            final_v = snaps[-1].volume_fraction if snaps else 0.0
+            return TopologyOptimizationResult(bool(cv.value), ni.value, snaps, final_c, final_v, phys, des, u)
+        finally:
+            prob.close()
+
+
+class SimpSession:
+    """Device-resident SIMP state stepped by the caller (mycel_simp_begin / step / read / end)."""
+
+    def __init__(self, problem: Problem, options: OptimizerOptions):
+        self.problem = problem
+        self._keep = []
+        so = _simp_options(options, self._keep)
+        h = C.c_void_p()
+        _check(L.load().mycel_simp_begin(problem.handle, C.byref(so), C.byref(h)), problem.ctx)
+        self.handle = h.value
+        self.done = False
+
+    def step(self) -> IterationSnapshot:
+        r = L.IterRecord()
+        d = C.c_int32(0)
+        _check(L.load().mycel_simp_step(self.handle, C.byref(r), C.byref(d)), self.problem.ctx)
+        self.done = bool(d.value)
+        return _snapshot(r)
+
+    def read(self, u=True, densities=True, active=False):
+        m = self.problem.model
+        uu = np.zeros(m.total_dofs) if u else None
+        ph = np.zeros(m.total_elements, dtype=np.float32) if densities else None
+        de = np.zeros(m.total_elements, dtype=np.float32) if densities else None
+        rpa = np.zeros(m.active_element_count) if active else None
+        rda = np.zeros(m.active_element_count) if active else None
+        lam = C.c_double(0)
+        _check(L.load().mycel_simp_read(self.handle, L.ptr(uu), L.ptr(ph), L.ptr(de), L.ptr(rpa), L.ptr(rda),
+                                        C.byref(lam)), self.problem.ctx)
+        return dict(u=uu, physical=ph, design=de, rho_phys_active=rpa, rho_design_active=rda, lam=lam.value)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            L.load().mycel_simp_end(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

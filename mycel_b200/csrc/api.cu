@@ -1,0 +1,776 @@
+// C ABI of libmycel_b200: context, problem residency, the PCG driver, StaticAnalysis.Run and the SIMP loop
+// (TopologyOptimizer.Run). Host code here only marshals descriptors, sequences kernels and reads back scalars;
+// every vector operation of the path runs in this library's kernels.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <deque>
+#include <string>
+#include <thread>
+#include <unordered_set>
+#include <vector>
+
+#include "internal.h"
+
+using namespace mycel;
+
+namespace mycel {
+
+static thread_local std::string tls_error;
+
+int32_t set_error(mycel_ctx* ctx, int32_t code, const std::string& msg) {
+  if (ctx) ctx->last_error = msg;
+  tls_error = msg;
+  return code;
+}
+
+}  // namespace mycel
+
+namespace {
+
+template <class T>
+cudaError_t dalloc(mycel_problem* p, T** ptr, size_t count) {
+  size_t bytes = std::max<size_t>(sizeof(T) * count, 16);
+  bytes = (bytes + 15) & ~size_t(15);
+  cudaError_t e = cudaMalloc((void**)ptr, bytes);
+  if (e == cudaSuccess) p->device_bytes += (int64_t)bytes;
+  return e;
+}
+
+void dfree(void* ptr) {
+  if (ptr) cudaFree(ptr);
+}
+
+std::string fmt_e3(double v) {
+  // .NET "E3": one digit, '.', three digits, 'E', sign, at least three exponent digits
+  if (std::isnan(v)) return "NaN";
+  if (std::isinf(v)) return v > 0 ? "\xe2\x88\x9e" : "-\xe2\x88\x9e";
+  char buf[64];
+  std::snprintf(buf, sizeof buf, "%.3E", v);
+  char* e = std::strchr(buf, 'E');
+  if (e) {
+    char sign = e[1];
+    int ex = std::atoi(e + 2);
+    std::snprintf(e, sizeof buf - (size_t)(e - buf), "E%c%03d", sign, ex);
+  }
+  return buf;
+}
+
+std::string underconstrained_msg(int64_t n) {
+  return "Model has fewer than 6 unique fixed DOFs on active nodes (found " + std::to_string(n) +
+         "). At least 6 fixed DOFs are required to prevent rigid body modes in 3D.";
+}
+
+// PcgResult.Message for a finished device state (PcgSolver.cs:149-367)
+void fill_result(const PcgState& st, mycel_pcg_result* res) {
+  res->iterations = st.iter;
+  res->final_residual = st.rel;
+  res->converged = 0;
+  std::string m;
+  switch (st.status) {
+    case PCG_CONVERGED: res->converged = 1; break;
+    case PCG_INIT_CONVERGED:
+      res->converged = 1;
+      m = "Initial guess already converged.";
+      break;
+    case PCG_RHS_ZERO:
+      res->converged = 1;
+      res->final_residual = 0.0;
+      m = "RHS is zero. Solution is zero.";
+      break;
+    case PCG_BREAK_CURVATURE:
+      m = "PCG curvature breakdown (p\xe1\xb5\x80" "Ap = " + fmt_e3(st.last_bad) +
+          " <= 0). Is the model not sufficiently constrained?";
+      break;
+    case PCG_BREAK_ALPHA:
+      m = "PCG step breakdown (alpha = " + fmt_e3(st.last_bad) + "). Is the model not sufficiently constrained?";
+      break;
+    case PCG_STAGNATED: m = "PCG stagnated: residual stopped decreasing. Is the model not sufficiently constrained?"; break;
+    case PCG_BREAK_BETA:
+      m = "PCG search direction breakdown (beta = " + fmt_e3(st.last_bad) +
+          "). Is the model not sufficiently constrained?";
+      break;
+    default: m = "PCG reached maximum iterations without converging. Is the model not sufficiently constrained?"; break;
+  }
+  std::snprintf(res->message, sizeof res->message, "%s", m.c_str());
+}
+
+}  // namespace
+namespace mycel {
+int32_t ensure_pcg_workspace(mycel_problem* p) {
+  if (p->d_x) return MYCEL_OK;
+  int64_t nd = p->g.nd;
+  int64_t nb = num_blocks8192(nd);
+  if (dalloc(p, &p->d_x, nd) || dalloc(p, &p->d_r, nd) || dalloc(p, &p->d_z, nd) || dalloc(p, &p->d_p, nd) ||
+      dalloc(p, &p->d_ap, nd) || dalloc(p, &p->d_part, 2 * nb + 64) || dalloc(p, &p->d_state, 1))
+    return set_error(p->ctx, MYCEL_E_OOM, "out of device memory for the PCG workspace");
+  cudaMemsetAsync(p->d_state, 0, sizeof(PcgState), p->ctx->stream);
+  return MYCEL_OK;
+}
+}  // namespace mycel
+namespace {
+
+PcgState* pinned_state(mycel_ctx* c) { return (PcgState*)c->pinned; }
+
+int32_t read_state(mycel_problem* p, PcgState* out) {
+  PcgState* hs = pinned_state(p->ctx);
+  MYCEL_CUDA(p->ctx, cudaMemcpyAsync(hs, p->d_state, sizeof(PcgState), cudaMemcpyDeviceToHost, p->ctx->stream));
+  MYCEL_CUDA(p->ctx, cudaStreamSynchronize(p->ctx->stream));
+  *out = *hs;
+  return MYCEL_OK;
+}
+
+__global__ void k_state_init(PcgState* st, double tol, int max_iter) {
+  PcgState s = {};
+  s.status = PCG_RUNNING;
+  s.max_iter = max_iter;
+  s.tol = tol;
+  *st = s;
+}
+
+__global__ void k_state_rel_from_b(PcgState* st) {
+  // zero warm start: rNormSq = bNormSq (PcgSolver.cs:185-192)
+  st->rn2 = st->bn2;
+  double rel = sqrt(st->bn2) / st->bnorm;
+  st->rel = rel;
+  st->prev = rel;
+  if (rel <= st->tol) st->status = PCG_INIT_CONVERGED;
+}
+
+// ordered list of indices i with b[i] != 0 and DOF i unconstrained (P b non-zeros, ascending)
+__global__ void k_nz_count(int64_t n, const double* __restrict__ b, const uint8_t* __restrict__ nf, int32_t* cnt) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  int v = 0;
+  if (i < n) v = (b[i] != 0.0) && !(nf[i / 3] & (1 << (i % 3)));
+  v = __syncthreads_count(v);
+  if (threadIdx.x == 0) cnt[blockIdx.x] = v;
+}
+__global__ void k_nz_write(int64_t n, const double* __restrict__ b, const uint8_t* __restrict__ nf,
+                           const int32_t* __restrict__ cnt, int32_t* out, int32_t* total) {
+  __shared__ int32_t base;
+  __shared__ int32_t wsum[32];
+  if (threadIdx.x == 0) {
+    int32_t s = 0;
+    for (unsigned k = 0; k < blockIdx.x; ++k) s += cnt[k];
+    base = s;
+    if (blockIdx.x == gridDim.x - 1) *total = s + cnt[blockIdx.x];
+  }
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  int v = 0;
+  if (i < n) v = (b[i] != 0.0) && !(nf[i / 3] & (1 << (i % 3)));
+  unsigned m = __ballot_sync(0xffffffffu, v);
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) wsum[w] = __popc(m);
+  __syncthreads();
+  if (v) {
+    int32_t off = base;
+    for (int k = 0; k < w; ++k) off += wsum[k];
+    off += __popc(m & ((1u << lane) - 1u));
+    out[off] = (int32_t)i;
+  }
+}
+
+// Build the ordered P b non-zero list for an arbitrary device vector b into dst (capacity nd); returns count.
+int32_t build_nz_list(mycel_problem* p, const double* d_bvec, int32_t* dst, int32_t* count) {
+  int64_t n = p->g.nd;
+  unsigned nb = (unsigned)((n + 255) / 256);
+  int32_t* cnt = (int32_t*)p->d_part2;  // borrow: needs nb + 1 ints
+  cudaStream_t s = p->ctx->stream;
+  k_nz_count<<<nb, 256, 0, s>>>(n, d_bvec, p->d_nflags, cnt);
+  k_nz_write<<<nb, 256, 0, s>>>(n, d_bvec, p->d_nflags, cnt, dst, cnt + nb);
+  p->ctx->launches += 2;
+  int32_t* h = (int32_t*)p->ctx->pinned;
+  MYCEL_CUDA(p->ctx, cudaMemcpyAsync(h, cnt + nb, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  MYCEL_CUDA(p->ctx, cudaStreamSynchronize(s));
+  *count = *h;
+  return MYCEL_OK;
+}
+
+const int kChunkIters = 16;
+
+int32_t capture_pcg_graph(mycel_problem* p) {
+  if (p->pcg_graph) return MYCEL_OK;
+  cudaStream_t s = p->ctx->stream;
+  cudaGraph_t graph;
+  int64_t before = p->ctx->launches;
+  MYCEL_CUDA(p->ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  for (int i = 0; i < kChunkIters; ++i) launch_pcg_iteration(p);
+  MYCEL_CUDA(p->ctx, cudaStreamEndCapture(s, &graph));
+  p->ctx->launches = before;  // captured launches are counted when the graph is replayed
+  MYCEL_CUDA(p->ctx, cudaGraphInstantiate(&p->pcg_graph, graph, 0));
+  cudaGraphDestroy(graph);
+  p->pcg_graph_chunk = kChunkIters;
+  return MYCEL_OK;
+}
+
+}  // namespace
+
+namespace mycel {
+
+// FP64 PCG (PcgSolver.Solve with Jacobi) on device vectors. d_b: right-hand side; nz list: ascending indices of
+// the non-zero entries of P b; d_xv: warm start in, solution out. cancel may be NULL.
+int32_t pcg_solve_fp64(mycel_problem* p, const double* d_bv, const int32_t* d_nz, int32_t n_nz, double* d_xv,
+                       double tol, int max_iter, const volatile int32_t* cancel, mycel_pcg_result* res) {
+  mycel_ctx* c = p->ctx;
+  cudaStream_t s = c->stream;
+  auto t0 = std::chrono::steady_clock::now();
+  std::memset(res, 0, sizeof *res);
+  if (p->n_active_fixed < 6) return set_error(c, MYCEL_E_UNDERCONSTRAINED, underconstrained_msg(p->n_active_fixed));
+  int32_t st = ensure_pcg_workspace(p);
+  if (st) return st;
+  // The kernels work on p->d_x / p->d_b; bind the caller's vectors.
+  if (d_xv != p->d_x) MYCEL_CUDA(c, cudaMemcpyAsync(p->d_x, d_xv, sizeof(double) * p->g.nd, cudaMemcpyDeviceToDevice, s));
+  double* saved_b = p->d_b;
+  int32_t* saved_nz = p->d_bnz;
+  int32_t saved_n = p->n_bnz;
+  p->d_b = const_cast<double*>(d_bv);
+  p->d_bnz = const_cast<int32_t*>(d_nz);
+  p->n_bnz = n_nz;
+  struct Restore {
+    mycel_problem* p; double* b; int32_t* nz; int32_t n;
+    ~Restore() { p->d_b = b; p->d_bnz = nz; p->n_bnz = n; }
+  } restore{p, saved_b, saved_nz, saved_n};
+
+  k_state_init<<<1, 1, 0, s>>>(p->d_state, tol, max_iter);
+  c->launches++;
+  launch_project_x(p, p->d_x, &p->d_state->nonzero_x);
+  launch_pcg_bnorm(p);
+  PcgState hs;
+  if ((st = read_state(p, &hs))) return st;
+  if (hs.bnorm <= 1e-30) {
+    MYCEL_CUDA(c, cudaMemsetAsync(p->d_x, 0, sizeof(double) * p->g.nd, s));
+    if (d_xv != p->d_x) MYCEL_CUDA(c, cudaMemcpyAsync(d_xv, p->d_x, sizeof(double) * p->g.nd, cudaMemcpyDeviceToDevice, s));
+    MYCEL_CUDA(c, cudaStreamSynchronize(s));
+    hs.status = PCG_RHS_ZERO;
+    hs.iter = 0;
+    fill_result(hs, res);
+    res->elapsed_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return MYCEL_OK;
+  }
+  if (hs.nonzero_x) {
+    launch_matvec64(p, p->d_x, p->d_ap, 1, nullptr);
+    launch_pcg_init_r(p, 1);
+    launch_pcg_dot_rr(p);
+  } else {
+    launch_pcg_init_r(p, 0);
+    k_state_rel_from_b<<<1, 1, 0, s>>>(p->d_state);
+    c->launches++;
+  }
+  launch_pcg_init_z(p);
+  if ((st = capture_pcg_graph(p))) return st;
+  int64_t launched = 0;
+  for (;;) {
+    if ((st = read_state(p, &hs))) return st;
+    if (hs.status != PCG_RUNNING) break;
+    if (cancel && *cancel) return set_error(c, MYCEL_E_CANCELLED, "The operation was canceled.");
+    // the device state machine stops by itself at max_iter; this bound only guards against a broken state
+    if (launched > (int64_t)max_iter + 4 * p->pcg_graph_chunk)
+      return set_error(c, MYCEL_E_TIMEOUT, "PCG device state did not reach a final status");
+    MYCEL_CUDA(c, cudaGraphLaunch(p->pcg_graph, s));
+    launched += p->pcg_graph_chunk;
+    c->launches += 4 * p->pcg_graph_chunk;
+  }
+  if (d_xv != p->d_x) MYCEL_CUDA(c, cudaMemcpyAsync(d_xv, p->d_x, sizeof(double) * p->g.nd, cudaMemcpyDeviceToDevice, s));
+  MYCEL_CUDA(c, cudaStreamSynchronize(s));
+  fill_result(hs, res);
+  res->elapsed_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  return MYCEL_OK;
+}
+
+}  // namespace mycel
+
+// ======================================================================================================
+// context
+// ======================================================================================================
+extern "C" int32_t mycel_version(void) { return 100; }
+
+extern "C" int32_t mycel_ctx_create(int32_t device, mycel_ctx** out) {
+  if (!out) return set_error(nullptr, MYCEL_E_ARG, "out is NULL");
+  *out = nullptr;
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0)
+    return set_error(nullptr, MYCEL_E_DEVICE, std::string("no CUDA device: ") + cudaGetErrorString(e));
+  if (device < 0 || device >= n) return set_error(nullptr, MYCEL_E_ARG, "device index out of range");
+  mycel_ctx* c = new mycel_ctx();
+  c->device = device;
+  if ((e = cudaSetDevice(device)) != cudaSuccess ||
+      (e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+      (e = cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess ||
+      (e = cudaMallocHost(&c->pinned, 1 << 16)) != cudaSuccess) {
+    std::string m = cudaGetErrorString(e);
+    delete c;
+    return set_error(nullptr, MYCEL_E_DEVICE, m);
+  }
+  c->pinned_bytes = 1 << 16;
+  *out = c;
+  return MYCEL_OK;
+}
+
+extern "C" int32_t mycel_ctx_destroy(mycel_ctx* c) {
+  if (!c) return MYCEL_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) {
+    cudaStreamSynchronize(c->stream);
+    cudaStreamDestroy(c->stream);
+  }
+  if (c->pinned) cudaFreeHost(c->pinned);
+  delete c;
+  return MYCEL_OK;
+}
+
+extern "C" void* mycel_ctx_stream(mycel_ctx* c) { return c ? (void*)c->stream : nullptr; }
+extern "C" const char* mycel_last_error(mycel_ctx* c) { return c ? c->last_error.c_str() : tls_error.c_str(); }
+extern "C" int64_t mycel_ctx_launch_count(mycel_ctx* c) { return c ? c->launches : 0; }
+
+// ======================================================================================================
+// problem
+// ======================================================================================================
+extern "C" int32_t mycel_problem_create(mycel_ctx* c, const mycel_grid* grid, const uint8_t* domain,
+                                        const mycel_material* mat, const int32_t* fixed, int32_t n_fixed,
+                                        const mycel_load_case* loads, int32_t n_loads, const double* density,
+                                        double penal, mycel_problem** out) {
+  if (!c || !grid || !domain || !mat || !out) return set_error(c, MYCEL_E_ARG, "NULL argument");
+  *out = nullptr;
+  if (grid->nx <= 0 || grid->ny <= 0 || grid->nz <= 0)
+    return set_error(c, MYCEL_E_ARG, "Grid dimensions must be strictly positive.");
+  if (!(grid->h > 0.0f)) return set_error(c, MYCEL_E_ARG, "Voxel pitch must be positive.");
+  if (n_fixed < 0 || n_loads < 0 || (n_fixed > 0 && !fixed) || (n_loads > 0 && !loads))
+    return set_error(c, MYCEL_E_ARG, "invalid fixed DOF or load arrays");
+  GridDims g = make_dims(grid->nx, grid->ny, grid->nz);
+  if (g.nd >= (int64_t)INT32_MAX) return set_error(c, MYCEL_E_ARG, "grid too large for 32-bit DOF indices");
+  for (int32_t i = 0; i < n_fixed; ++i)
+    if (fixed[i] < 0 || (int64_t)fixed[i] >= g.nd)
+      return set_error(c, MYCEL_E_ARG, "Fixed DOF " + std::to_string(fixed[i]) + " is out of bounds [0, " +
+                                           std::to_string(g.nd - 1) + "].");
+  cudaSetDevice(c->device);
+  mycel_problem* p = new mycel_problem();
+  p->ctx = c;
+  p->g = g;
+  p->h = grid->h;
+  p->e0 = mat->e0;
+  p->nu = mat->nu;
+  p->emin_ratio = mat->emin_ratio;
+  p->emin = mat->e0 * mat->emin_ratio;  // FeMaterial.Emin
+  p->penal = penal;
+  build_ke((double)grid->h, mat->nu, p->ke.v);
+  for (int i = 0; i < 576; ++i) p->kef.v[i] = (float)p->ke.v[i];
+  for (int i = 0; i < 24; ++i) p->diag_ke[i] = p->ke.v[i * 24 + i];
+  p->fixed_host.assign(fixed, fixed + n_fixed);
+
+  // FeModel.AssembleForces (FeModel.cs:263-321): descriptor marshalling of the load patches, O(patch nodes).
+  p->forces_host.assign(g.nd, 0.0);
+  std::unordered_set<int32_t> seen;
+  for (int32_t li = 0; li < n_loads && !p->assemble_status; ++li) {
+    const mycel_load_case& L = loads[li];
+    for (int32_t q = 0; q < L.n_nodes; ++q)
+      if (seen.insert(L.nodes[q]).second) p->load_nodes_host.push_back(L.nodes[q]);
+    if (L.n_nodes == 0) {
+      if (L.force[0] != 0.0f || L.force[1] != 0.0f || L.force[2] != 0.0f) {
+        p->assemble_status = MYCEL_E_INVALID_OPERATION;
+        p->assemble_msg = "Cannot assemble load case: surface patch contains 0 nodes.";
+      }
+      continue;
+    }
+    double total = 0.0;
+    for (int32_t q = 0; q < L.n_nodes; ++q) total += L.node_area[q];
+    for (int32_t q = 0; q < L.n_nodes; ++q)
+      if (L.nodes[q] < 0 || (int64_t)L.nodes[q] >= g.nn) {
+        p->assemble_status = MYCEL_E_INVALID_OPERATION;
+        p->assemble_msg = "Patch node index " + std::to_string(L.nodes[q]) + " is out of bounds [0, " +
+                          std::to_string(g.nn - 1) + "].";
+      }
+    if (p->assemble_status) break;
+    if (total <= 0.0) {
+      double inv = 1.0 / L.n_nodes;
+      double fx = (double)L.force[0] * inv, fy = (double)L.force[1] * inv, fz = (double)L.force[2] * inv;
+      for (int32_t q = 0; q < L.n_nodes; ++q) {
+        int64_t n = L.nodes[q];
+        p->forces_host[3 * n] += fx;
+        p->forces_host[3 * n + 1] += fy;
+        p->forces_host[3 * n + 2] += fz;
+      }
+    } else {
+      double inv = 1.0 / total;
+      for (int32_t q = 0; q < L.n_nodes; ++q) {
+        int64_t n = L.nodes[q];
+        double w = L.node_area[q] * inv;
+        p->forces_host[3 * n] += (double)L.force[0] * w;
+        p->forces_host[3 * n + 1] += (double)L.force[1] * w;
+        p->forces_host[3 * n + 2] += (double)L.force[2] * w;
+      }
+    }
+  }
+  std::vector<int32_t> active;
+  active.reserve((size_t)g.ne);
+  for (int64_t e = 0; e < g.ne; ++e)
+    if (domain[e]) active.push_back((int32_t)e);
+  p->n_active = (int64_t)active.size();
+  std::vector<int32_t> fnz;
+  for (int64_t i = 0; i < g.nd; ++i)
+    if (p->forces_host[i] != 0.0) fnz.push_back((int32_t)i);
+  p->n_fnz = (int32_t)fnz.size();
+
+  cudaStream_t s = c->stream;
+  int32_t* d_cnt = nullptr;
+  bool ok = !dalloc(p, &p->d_domain, g.ne) && !dalloc(p, &p->d_nflags, (g.nn + 3) & ~int64_t(3)) &&
+            !dalloc(p, &p->d_active, std::max<int64_t>(p->n_active, 1)) && !dalloc(p, &p->d_F, g.nd) &&
+            !dalloc(p, &p->d_b, g.nd) && !dalloc(p, &p->d_fnz, std::max<int32_t>(p->n_fnz, 1)) &&
+            !dalloc(p, &p->d_bnz, std::max<int32_t>(p->n_fnz, 1)) && !dalloc(p, &p->d_rho_box, g.ne) &&
+            !dalloc(p, &p->d_E, g.ne) && !dalloc(p, &p->d_Ef, g.ne) && !dalloc(p, &p->d_diag, g.nd) &&
+            !dalloc(p, &p->d_invd, g.nd) && !dalloc(p, &p->d_invdf, g.nd) && !dalloc(p, &p->d_tmp0, g.nd) &&
+            !dalloc(p, &p->d_tmp1, g.nd) && !dalloc(p, &p->d_fixed, std::max<int32_t>(n_fixed, 1)) &&
+            !dalloc(p, &d_cnt, 4);
+  if (ok) ok = !dalloc(p, &p->d_part2, std::max<int64_t>(g.nd / 256 + 1024, 65536));
+  p->n_part2 = std::max<int64_t>(g.nd / 256 + 1024, 65536);
+  if (!ok) {
+    dfree(d_cnt);
+    mycel_problem_destroy(p);
+    return set_error(c, MYCEL_E_OOM, "out of device memory for the problem");
+  }
+  cudaMemcpyAsync(p->d_domain, domain, g.ne, cudaMemcpyHostToDevice, s);
+  if (p->n_active) cudaMemcpyAsync(p->d_active, active.data(), sizeof(int32_t) * p->n_active, cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(p->d_F, p->forces_host.data(), sizeof(double) * g.nd, cudaMemcpyHostToDevice, s);
+  if (p->n_fnz) cudaMemcpyAsync(p->d_fnz, fnz.data(), sizeof(int32_t) * p->n_fnz, cudaMemcpyHostToDevice, s);
+  if (n_fixed) cudaMemcpyAsync(p->d_fixed, fixed, sizeof(int32_t) * n_fixed, cudaMemcpyHostToDevice, s);
+  if (density) {
+    cudaMemcpyAsync(p->d_rho_box, density, sizeof(double) * g.ne, cudaMemcpyHostToDevice, s);
+  } else {
+    std::vector<double> ones((size_t)g.ne, 1.0);
+    cudaMemcpyAsync(p->d_rho_box, ones.data(), sizeof(double) * g.ne, cudaMemcpyHostToDevice, s);
+    cudaStreamSynchronize(s);
+  }
+  cudaMemsetAsync(d_cnt, 0, 16, s);
+  cudaMemsetAsync(p->d_E, 0, sizeof(double) * g.ne, s);
+  cudaMemsetAsync(p->d_Ef, 0, sizeof(float) * g.ne, s);
+  launch_setup_nodes(p, p->d_fixed, n_fixed, d_cnt);
+  // b = P F and its ordered non-zero list
+  int32_t nb_cnt = 0;
+  {
+    // d_b = F masked by the constrained flags: reuse the non-zero list builder on F itself
+    cudaMemcpyAsync(p->d_b, p->d_F, sizeof(double) * g.nd, cudaMemcpyDeviceToDevice, s);
+  }
+  int32_t st = build_nz_list(p, p->d_F, p->d_bnz, &nb_cnt);
+  if (st) {
+    dfree(d_cnt);
+    mycel_problem_destroy(p);
+    return st;
+  }
+  p->n_bnz = nb_cnt;
+  // zero b on constrained DOFs: download flags once (set-up) to count active nodes and fixed DOFs
+  std::vector<uint8_t> nf((size_t)g.nn);
+  int32_t hcnt = 0;
+  cudaMemcpyAsync(nf.data(), p->d_nflags, g.nn, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(&hcnt, d_cnt, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+  cudaError_t e = cudaStreamSynchronize(s);
+  dfree(d_cnt);
+  if (e != cudaSuccess) {
+    mycel_problem_destroy(p);
+    return set_error(c, MYCEL_E_DEVICE, std::string("problem set-up: ") + cudaGetErrorString(e));
+  }
+  int64_t an = 0;
+  for (int64_t n = 0; n < g.nn; ++n) an += (nf[n] & NF_ACTIVE) ? 1 : 0;
+  p->n_active_nodes = an;
+  p->n_active_fixed = hcnt;
+  // b = P F on device
+  {
+    std::vector<double> b(p->forces_host);
+    for (int64_t i = 0; i < g.nd; ++i)
+      if (nf[i / 3] & (1 << (i % 3))) b[i] = 0.0;
+    cudaMemcpyAsync(p->d_b, b.data(), sizeof(double) * g.nd, cudaMemcpyHostToDevice, s);
+    cudaStreamSynchronize(s);
+  }
+  launch_update_E(p, p->d_rho_box, penal);
+  launch_diag(p);
+  if ((e = cudaStreamSynchronize(s)) != cudaSuccess) {
+    mycel_problem_destroy(p);
+    return set_error(c, MYCEL_E_DEVICE, std::string("problem set-up: ") + cudaGetErrorString(e));
+  }
+  *out = p;
+  return MYCEL_OK;
+}
+
+extern "C" int32_t mycel_problem_destroy(mycel_problem* p) {
+  if (!p) return MYCEL_OK;
+  cudaSetDevice(p->ctx->device);
+  cudaStreamSynchronize(p->ctx->stream);
+  if (p->pcg_graph) cudaGraphExecDestroy(p->pcg_graph);
+  if (p->pcg32_graph) cudaGraphExecDestroy(p->pcg32_graph);
+  void* ptrs[] = {p->d_domain, p->d_nflags, p->d_fixed, p->d_active, p->d_e2a, p->d_F, p->d_b, p->d_fnz, p->d_bnz, p->d_rho_box,
+                  p->d_E, p->d_Ef, p->d_diag, p->d_invd, p->d_invdf, p->d_r, p->d_z, p->d_p, p->d_ap, p->d_x,
+                  p->d_part, p->d_state, p->f_x, p->f_r, p->f_z, p->f_p0, p->f_p1, p->f_ap, p->d_r64, p->d_part2,
+                  p->d_tmp0, p->d_tmp1};
+  for (void* q : ptrs) dfree(q);
+  delete p;
+  return MYCEL_OK;
+}
+
+extern "C" int32_t mycel_problem_info_get(mycel_problem* p, mycel_problem_info* o) {
+  if (!p || !o) return set_error(p ? p->ctx : nullptr, MYCEL_E_ARG, "NULL argument");
+  o->total_elements = p->g.ne;
+  o->total_nodes = p->g.nn;
+  o->total_dofs = p->g.nd;
+  o->active_elements = p->n_active;
+  o->active_nodes = p->n_active_nodes;
+  o->active_fixed_dofs = p->n_active_fixed;
+  o->device_bytes = p->device_bytes;
+  return MYCEL_OK;
+}
+
+extern "C" int32_t mycel_problem_forces(mycel_problem* p, double* f) {
+  if (!p || !f) return set_error(p ? p->ctx : nullptr, MYCEL_E_ARG, "NULL argument");
+  if (p->assemble_status) return set_error(p->ctx, p->assemble_status, p->assemble_msg);
+  std::memcpy(f, p->forces_host.data(), sizeof(double) * p->g.nd);
+  return MYCEL_OK;
+}
+
+// ======================================================================================================
+// kernel-level entry points
+// ======================================================================================================
+extern "C" int32_t mycel_update_densities(mycel_problem* p, const double* dens, double penal) {
+  if (!p || !dens) return set_error(p ? p->ctx : nullptr, MYCEL_E_ARG, "NULL argument");
+  cudaSetDevice(p->ctx->device);
+  cudaStream_t s = p->ctx->stream;
+  MYCEL_CUDA(p->ctx, cudaMemcpyAsync(p->d_rho_box, dens, sizeof(double) * p->g.ne, cudaMemcpyHostToDevice, s));
+  p->penal = penal;
+  launch_update_E(p, p->d_rho_box, penal);
+  launch_diag(p);
+  MYCEL_CUDA(p->ctx, cudaStreamSynchronize(s));
+  return MYCEL_OK;
+}
+
+extern "C" int32_t mycel_diagonal(mycel_problem* p, double* out) {
+  if (!p || !out) return set_error(p ? p->ctx : nullptr, MYCEL_E_ARG, "NULL argument");
+  cudaSetDevice(p->ctx->device);
+  MYCEL_CUDA(p->ctx, cudaMemcpyAsync(out, p->d_diag, sizeof(double) * p->g.nd, cudaMemcpyDeviceToHost, p->ctx->stream));
+  MYCEL_CUDA(p->ctx, cudaStreamSynchronize(p->ctx->stream));
+  return MYCEL_OK;
+}
+
+extern "C" int32_t mycel_apply_k(mycel_problem* p, const double* x, double* y, int32_t projected, int32_t precision) {
+  if (!p || !x || !y) return set_error(p ? p->ctx : nullptr, MYCEL_E_ARG, "NULL argument");
+  cudaSetDevice(p->ctx->device);
+  cudaStream_t s = p->ctx->stream;
+  MYCEL_CUDA(p->ctx, cudaMemcpyAsync(p->d_tmp0, x, sizeof(double) * p->g.nd, cudaMemcpyHostToDevice, s));
+  if (precision == MYCEL_PRECISION_MIXED) {
+    int32_t st = ensure_pcg_workspace(p);
+    if (st) return st;
+    launch_E_to_f32(p);
+    // FP32 operator on the FP32-rounded input
+    mixed_apply_k_f64io(p, p->d_tmp0, p->d_tmp1, projected);
+  } else {
+    launch_matvec64(p, p->d_tmp0, p->d_tmp1, projected, nullptr);
+  }
+  MYCEL_CUDA(p->ctx, cudaMemcpyAsync(y, p->d_tmp1, sizeof(double) * p->g.nd, cudaMemcpyDeviceToHost, s));
+  MYCEL_CUDA(p->ctx, cudaStreamSynchronize(s));
+  return MYCEL_OK;
+}
+
+extern "C" int32_t mycel_pcg_solve(mycel_problem* p, const double* b, double* x, double tol, int32_t max_iter,
+                                   int32_t precision, mycel_pcg_result* res) {
+  if (!p || !b || !x || !res) return set_error(p ? p->ctx : nullptr, MYCEL_E_ARG, "NULL argument");
+  cudaSetDevice(p->ctx->device);
+  cudaStream_t s = p->ctx->stream;
+  int32_t st = ensure_pcg_workspace(p);
+  if (st) return st;
+  MYCEL_CUDA(p->ctx, cudaMemcpyAsync(p->d_tmp1, b, sizeof(double) * p->g.nd, cudaMemcpyHostToDevice, s));
+  MYCEL_CUDA(p->ctx, cudaMemcpyAsync(p->d_x, x, sizeof(double) * p->g.nd, cudaMemcpyHostToDevice, s));
+  int32_t* nz = (int32_t*)p->d_tmp0;
+  int32_t cnt = 0;
+  if ((st = build_nz_list(p, p->d_tmp1, nz, &cnt))) return st;
+  if (precision == MYCEL_PRECISION_MIXED) {
+    st = mixed_solve_entry(p, p->d_tmp1, nz, cnt, p->d_x, tol, max_iter, nullptr, res);
+  } else {
+    st = pcg_solve_fp64(p, p->d_tmp1, nz, cnt, p->d_x, tol, max_iter, nullptr, res);
+  }
+  if (st) return st;
+  MYCEL_CUDA(p->ctx, cudaMemcpyAsync(x, p->d_x, sizeof(double) * p->g.nd, cudaMemcpyDeviceToHost, s));
+  MYCEL_CUDA(p->ctx, cudaStreamSynchronize(s));
+  return MYCEL_OK;
+}
+
+namespace mycel {
+int32_t solve_dispatch(mycel_problem* p, double* d_u, double tol, int max_iter, int precision,
+                       const volatile int32_t* cancel, mycel_pcg_result* res) {
+  if (precision == MYCEL_PRECISION_MIXED) {
+    return mixed_solve_entry(p, p->d_b, p->d_bnz, p->n_bnz, d_u, tol, max_iter, cancel, res);
+  }
+  return pcg_solve_fp64(p, p->d_b, p->d_bnz, p->n_bnz, d_u, tol, max_iter, cancel, res);
+}
+}  // namespace mycel
+
+extern "C" int32_t mycel_static_solve(mycel_problem* p, const mycel_static_options* opt, const double* warm,
+                                      int64_t warm_len, double* u_out, double* reactions_out, double* vm_out,
+                                      double* compliance_out, double* maxdisp_out, mycel_pcg_result* res) {
+  if (!p || !u_out) return set_error(p ? p->ctx : nullptr, MYCEL_E_ARG, "NULL argument");
+  mycel_ctx* c = p->ctx;
+  cudaSetDevice(c->device);
+  cudaStream_t s = c->stream;
+  mycel_static_options o = opt ? *opt : mycel_static_options{1e-6, 5000, 1, MYCEL_PRECISION_FP64};
+  if (p->n_active_fixed < 6) return set_error(c, MYCEL_E_UNDERCONSTRAINED, underconstrained_msg(p->n_active_fixed));
+  if (p->assemble_status) return set_error(c, p->assemble_status, p->assemble_msg);
+  if (warm && warm_len != p->g.nd)
+    return set_error(c, MYCEL_E_ARG, "WarmStartDisplacements length (" + std::to_string(warm_len) +
+                                         ") must match TotalDofs (" + std::to_string(p->g.nd) + "). (Parameter 'options')");
+  int32_t st = ensure_pcg_workspace(p);
+  if (st) return st;
+  // new FemOperator(model): E from ElementDensity and Penal
+  launch_update_E(p, p->d_rho_box, p->penal);
+  launch_diag(p);
+  if (warm) MYCEL_CUDA(c, cudaMemcpyAsync(p->d_x, warm, sizeof(double) * p->g.nd, cudaMemcpyHostToDevice, s));
+  else MYCEL_CUDA(c, cudaMemsetAsync(p->d_x, 0, sizeof(double) * p->g.nd, s));
+  mycel_pcg_result local;
+  mycel_pcg_result* r = res ? res : &local;
+  st = solve_dispatch(p, p->d_x, o.tolerance, o.max_iterations, o.precision, nullptr, r);
+  if (st) return st;
+  if (o.throw_on_non_convergence && !r->converged)
+    return set_error(c, MYCEL_E_NOT_CONVERGED,
+                     "FEM solver did not converge in " + std::to_string(r->iterations) + " iterations (" + r->message +
+                         "). Is the model not sufficiently constrained?");
+  double* d_sc = p->d_part2;  // [0] compliance, [1] max disp
+  launch_compliance(p, p->d_x, d_sc);
+  launch_max_disp(p, p->d_x, d_sc + 1);
+  if (reactions_out) {
+    launch_matvec64(p, p->d_x, p->d_ap, 0, nullptr);  // ApplyK(u) (StaticAnalysis.cs:103-110)
+    launch_reactions(p, p->d_ap, p->d_tmp1, p->d_fixed, (int32_t)p->fixed_host.size());
+    MYCEL_CUDA(c, cudaMemcpyAsync(reactions_out, p->d_tmp1, sizeof(double) * p->g.nd, cudaMemcpyDeviceToHost, s));
+  }
+  if (vm_out) {
+    launch_von_mises(p, p->d_x, p->d_tmp0);
+    MYCEL_CUDA(c, cudaMemcpyAsync(vm_out, p->d_tmp0, sizeof(double) * p->g.ne, cudaMemcpyDeviceToHost, s));
+  }
+  double* hsc = (double*)c->pinned;
+  MYCEL_CUDA(c, cudaMemcpyAsync(hsc, d_sc, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  MYCEL_CUDA(c, cudaMemcpyAsync(u_out, p->d_x, sizeof(double) * p->g.nd, cudaMemcpyDeviceToHost, s));
+  MYCEL_CUDA(c, cudaStreamSynchronize(s));
+  if (compliance_out) *compliance_out = hsc[0];
+  if (maxdisp_out) *maxdisp_out = hsc[1];
+  return MYCEL_OK;
+}
+
+// ---- filter ----
+extern "C" int32_t mycel_filter_create(mycel_problem* p, double rmin, mycel_filter** out) {
+  if (!p || !out) return set_error(p ? p->ctx : nullptr, MYCEL_E_ARG, "NULL argument");
+  cudaSetDevice(p->ctx->device);
+  mycel_filter* f = new mycel_filter();
+  f->p = p;
+  f->rmin = rmin;
+  int st = filter_setup(f);
+  if (st) {
+    mycel_filter_destroy(f);
+    return set_error(p->ctx, st, "filter set-up failed");
+  }
+  *out = f;
+  return MYCEL_OK;
+}
+
+extern "C" int32_t mycel_filter_destroy(mycel_filter* f) {
+  if (!f) return MYCEL_OK;
+  cudaStreamSynchronize(f->p->ctx->stream);
+  dfree(f->d_off);
+  dfree(f->d_w);
+  dfree(f->d_invhs);
+  dfree(f->d_s);
+  delete f;
+  return MYCEL_OK;
+}
+
+static int32_t filter_io(mycel_filter* f, const double* in, double* out, int adj) {
+  if (!f || !in || !out) return set_error(f ? f->p->ctx : nullptr, MYCEL_E_ARG, "NULL argument");
+  mycel_problem* p = f->p;
+  cudaSetDevice(p->ctx->device);
+  cudaStream_t s = p->ctx->stream;
+  double* d_in = p->d_tmp0;   // active-sized staging
+  double* d_box = p->d_tmp1;  // box
+  int32_t st = ensure_pcg_workspace(p);
+  if (st) return st;
+  double* d_outbox = p->d_z;
+  MYCEL_CUDA(p->ctx, cudaMemcpyAsync(d_in, in, sizeof(double) * p->n_active, cudaMemcpyHostToDevice, s));
+  launch_scatter_active(p, d_in, d_box, 0.0);
+  if (adj) launch_filter_adj(f, d_box, d_outbox);
+  else launch_filter_fwd(f, d_box, d_outbox);
+  launch_gather_active(p, d_outbox, d_in);
+  MYCEL_CUDA(p->ctx, cudaMemcpyAsync(out, d_in, sizeof(double) * p->n_active, cudaMemcpyDeviceToHost, s));
+  MYCEL_CUDA(p->ctx, cudaStreamSynchronize(s));
+  return MYCEL_OK;
+}
+
+extern "C" int32_t mycel_filter_apply(mycel_filter* f, const double* in, double* out) { return filter_io(f, in, out, 0); }
+extern "C" int32_t mycel_filter_adjoint(mycel_filter* f, const double* in, double* out) { return filter_io(f, in, out, 1); }
+
+extern "C" int32_t mycel_filter_s(mycel_filter* f, double* out) {
+  if (!f || !out) return set_error(f ? f->p->ctx : nullptr, MYCEL_E_ARG, "NULL argument");
+  mycel_problem* p = f->p;
+  cudaSetDevice(p->ctx->device);
+  launch_gather_active(p, f->d_s, p->d_tmp0);
+  MYCEL_CUDA(p->ctx, cudaMemcpyAsync(out, p->d_tmp0, sizeof(double) * p->n_active, cudaMemcpyDeviceToHost, p->ctx->stream));
+  MYCEL_CUDA(p->ctx, cudaStreamSynchronize(p->ctx->stream));
+  return MYCEL_OK;
+}
+
+extern "C" int32_t mycel_sensitivities(mycel_problem* p, const double* u, const double* rho_active, double penal,
+                                       double* dc_active) {
+  if (!p || !u || !rho_active || !dc_active) return set_error(p ? p->ctx : nullptr, MYCEL_E_ARG, "NULL argument");
+  cudaSetDevice(p->ctx->device);
+  cudaStream_t s = p->ctx->stream;
+  int32_t st = ensure_pcg_workspace(p);
+  if (st) return st;
+  MYCEL_CUDA(p->ctx, cudaMemcpyAsync(p->d_r, u, sizeof(double) * p->g.nd, cudaMemcpyHostToDevice, s));
+  MYCEL_CUDA(p->ctx, cudaMemcpyAsync(p->d_tmp0, rho_active, sizeof(double) * p->n_active, cudaMemcpyHostToDevice, s));
+  launch_scatter_active(p, p->d_tmp0, p->d_tmp1, 0.0);
+  launch_sens(p, p->d_r, p->d_tmp1, penal, p->d_z);
+  launch_gather_active(p, p->d_z, p->d_tmp0);
+  MYCEL_CUDA(p->ctx, cudaMemcpyAsync(dc_active, p->d_tmp0, sizeof(double) * p->n_active, cudaMemcpyDeviceToHost, s));
+  MYCEL_CUDA(p->ctx, cudaStreamSynchronize(s));
+  return MYCEL_OK;
+}
+
+extern "C" int32_t mycel_oc_update(mycel_ctx* c, int32_t n, const double* rho, const double* dc, const double* sv,
+                                   const uint8_t* passive, double* rho_new, double f, double move, double rho_min,
+                                   double lambda_guess, int32_t max_bisect, double vol_tol, double* lambda_out) {
+  if (!c || n < 0 || (n > 0 && (!rho || !dc || !sv || !rho_new)))
+    return set_error(c, MYCEL_E_ARG, "All spans must have length >= rho.Length.");
+  cudaSetDevice(c->device);
+  cudaStream_t s = c->stream;
+  size_t nn = (size_t)std::max(n, 1);
+  double *d_rho, *d_dc, *d_s, *d_new, *d_scr;
+  uint8_t* d_pas = nullptr;
+  OcOut* d_out;
+  size_t scr = (size_t)c->num_sms * 2 * 8 + 64;
+  MYCEL_CUDA(c, cudaMallocAsync((void**)&d_rho, nn * 8, s));
+  MYCEL_CUDA(c, cudaMallocAsync((void**)&d_dc, nn * 8, s));
+  MYCEL_CUDA(c, cudaMallocAsync((void**)&d_s, nn * 8, s));
+  MYCEL_CUDA(c, cudaMallocAsync((void**)&d_new, nn * 8, s));
+  MYCEL_CUDA(c, cudaMallocAsync((void**)&d_scr, scr * 8, s));
+  MYCEL_CUDA(c, cudaMallocAsync((void**)&d_out, sizeof(OcOut), s));
+  if (passive) MYCEL_CUDA(c, cudaMallocAsync((void**)&d_pas, nn, s));
+  MYCEL_CUDA(c, cudaMemsetAsync(d_out, 0, sizeof(OcOut), s));
+  if (n) {
+    cudaMemcpyAsync(d_rho, rho, n * 8, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_dc, dc, n * 8, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_s, sv, n * 8, cudaMemcpyHostToDevice, s);
+    if (passive) cudaMemcpyAsync(d_pas, passive, n, cudaMemcpyHostToDevice, s);
+  }
+  OcParams prm{f, move, rho_min, lambda_guess, vol_tol, max_bisect, 0};
+  int st = launch_oc(c, n, nullptr, d_rho, d_dc, d_s, d_pas, d_new, nullptr, nullptr, prm, d_scr, d_out);
+  OcOut* ho = (OcOut*)c->pinned;
+  std::memset(ho, 0, sizeof(OcOut));
+  if (!st) {
+    cudaMemcpyAsync(ho, d_out, sizeof(OcOut), cudaMemcpyDeviceToHost, s);
+    if (n) cudaMemcpyAsync(rho_new, d_new, n * 8, cudaMemcpyDeviceToHost, s);
+  }
+  cudaError_t e = cudaStreamSynchronize(s);
+  OcOut h = *ho;
+  cudaFreeAsync(d_rho, s); cudaFreeAsync(d_dc, s); cudaFreeAsync(d_s, s); cudaFreeAsync(d_new, s);
+  cudaFreeAsync(d_scr, s); cudaFreeAsync(d_out, s);
+  if (d_pas) cudaFreeAsync(d_pas, s);
+  cudaStreamSynchronize(s);
+  if (st || e != cudaSuccess) return set_error(c, MYCEL_E_DEVICE, std::string("OC kernel: ") + cudaGetErrorString(e));
+  if (h.trials == 0) return set_error(c, MYCEL_E_TIMEOUT, "OC grid barrier timed out");
+  if (lambda_out) *lambda_out = h.lambda;
+  return MYCEL_OK;
+}

@@ -1,0 +1,1151 @@
+// Plain FP64 path: reproduces Mycel.Core's arithmetic on sm_100a.
+// This translation unit is compiled with -fmad=false: no a*b+c is contracted, as in the reference (RyuJIT).
+//
+// Kernels and the reference code whose rounding sequence they reproduce:
+//   k_matvec64      FemOperator.ApplyK/ApplyA (Fem/FemOperator.cs:196-294, MultiplyElementUnsafe :379-422).
+//                   Node-centric gather: one thread per node sums its <= 8 element contributions in the
+//                   8-colour order the reference scatters them, each contribution computed with the
+//                   reference's scale-then-dot order (ue = x*E; four lane chains; Vector256.Sum).
+//                   Threads are grouped by node parity class so every warp follows the same colour order and
+//                   reads the same KE rows (broadcast from the kernel parameter bank).
+//   k_diag          FemOperator.AssembleDiagonal (:143-172), same colour order; Jacobi inverse (JacobiPreconditioner.cs:25).
+//   k_dot_exact     PcgSolver DotParallel/ProcessDotChunk (Fem/PcgSolver.cs:385-450): one CTA per 8192-block,
+//                   producer warps stage products in shared memory, lanes 0-3 of warp 0 run the four
+//                   sequential lane chains, the last CTA adds the block partials in block order.
+//   k_xr_exact      ProcessUpdateXrNormChunk + ProcessApplyPrecDotChunk (:452-527) fused: two chain sets.
+//   k_update_p      ProcessUpdatePChunk (:529-553).
+//   k_filter_*      DensityFilter (Optimization/DensityFilter.cs:34-303) as a stencil in the reference's
+//                   neighbour order (jz, jy, jx ascending), weights (rmin - dist) * invHs_row.
+//   k_sens          SensitivityAnalysis (Optimization/SensitivityAnalysis.cs:98-144).
+//   k_oc            OcOptimizer.Update (Optimization/OcOptimizer.cs:12-175): one persistent cooperative kernel.
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "internal.h"
+
+namespace mycel {
+
+constexpr int kBlock = 8192;  // PcgSolver.BlockSize
+constexpr int kChunk = 1024;  // products staged per shared-memory buffer
+constexpr int kDotThreads = 256;
+
+// ---------------------------------------------------------------------------------------------------------
+// helpers
+// ---------------------------------------------------------------------------------------------------------
+__device__ __forceinline__ double lane_sum(int mode, double a0, double a1, double a2, double a3) {
+  // Vector256<double>.Sum: Sum(lower) + Sum(upper) on .NET 8+ (mode 0); alternatives for the noise-floor study.
+  if (mode == 1) return (a0 + a2) + (a1 + a3);
+  if (mode == 2) return ((a0 + a1) + a2) + a3;
+  return (a0 + a1) + (a2 + a3);
+}
+
+// Correctly rounded x^n (n small, >= 0): exact power carried as a double-double, rounded once.
+__device__ __forceinline__ double pow_int_cr(double x, int n) {
+  if (n == 0) return 1.0;
+  if (n == 1) return x;
+  double hi = x, lo = 0.0;
+  for (int k = 1; k < n; ++k) {
+    double ph = __dmul_rn(hi, x);
+    double pl = __fma_rn(hi, x, -ph);
+    pl = __dadd_rn(pl, __dmul_rn(lo, x));
+    double s = __dadd_rn(ph, pl);
+    lo = __dsub_rn(pl, __dsub_rn(s, ph));
+    hi = s;
+  }
+  return hi;
+}
+
+// Math.Pow on the path: integer exponents (the SIMP penalty p = 1, 2, 3 and p - 1) are correctly rounded;
+// other exponents use CUDA's pow.
+__device__ __forceinline__ double path_pow(double x, double y) {
+  double r = rint(y);
+  if (r == y && r >= 0.0 && r <= 16.0 && x >= 0.0 && isfinite(x)) return pow_int_cr(x, (int)r);
+  return pow(x, y);
+}
+
+__device__ __forceinline__ int local_index(int ox, int oy, int oz) {
+  // Hex8 local node order (Hex8Element.cs:8-16): (0,0,0),(1,0,0),(1,1,0),(0,1,0), then the same at z=1
+  int base = oy ? (ox ? 2 : 3) : (ox ? 1 : 0);
+  return base + 4 * oz;
+}
+
+__device__ __forceinline__ double ld_volatile(const double* p) { return *(const volatile double*)p; }
+
+// Parity-class node mapping: blockIdx.y = class (px | py<<1 | pz<<2); nodes of one class have the same
+// parity in i, j, k, so the colour order of their incident elements is the same for the whole warp.
+struct ClassNode {
+  int i, j, k, px, py, pz;
+  bool valid;
+};
+__device__ __forceinline__ ClassNode class_node(const GridDims& g, int cls, int64_t t) {
+  ClassNode c;
+  c.px = cls & 1; c.py = (cls >> 1) & 1; c.pz = (cls >> 2) & 1;
+  int cx = (g.nx1 - c.px + 1) >> 1, cy = (g.ny1 - c.py + 1) >> 1, cz = (g.nz1 - c.pz + 1) >> 1;
+  int64_t tot = (int64_t)cx * cy * cz;
+  c.valid = t < tot;
+  if (!c.valid) { c.i = c.j = c.k = 0; return c; }
+  int a = (int)(t % cx);
+  int64_t rest = t / cx;
+  int b = (int)(rest % cy);
+  int cc = (int)(rest / cy);
+  c.i = c.px + 2 * a; c.j = c.py + 2 * b; c.k = c.pz + 2 * cc;
+  return c;
+}
+
+inline dim3 class_grid(const GridDims& g, int threads) {
+  int cx = (g.nx1 + 1) >> 1, cy = (g.ny1 + 1) >> 1, cz = (g.nz1 + 1) >> 1;
+  int64_t tot = (int64_t)cx * cy * cz;
+  return dim3((unsigned)((tot + threads - 1) / threads), 8, 1);
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// problem set-up: active nodes, constrained mask (FeModel.cs:80-183)
+// ---------------------------------------------------------------------------------------------------------
+__global__ void k_node_flags(GridDims g, const uint8_t* __restrict__ dom, uint8_t* __restrict__ nf) {
+  int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= g.nn) return;
+  int i = (int)(n % g.nx1);
+  int64_t r = n / g.nx1;
+  int j = (int)(r % g.ny1), k = (int)(r / g.ny1);
+  bool act = false;
+  for (int dz = -1; dz <= 0; ++dz)
+    for (int dy = -1; dy <= 0; ++dy)
+      for (int dx = -1; dx <= 0; ++dx) {
+        int ie = i + dx, je = j + dy, ke = k + dz;
+        if (ie >= 0 && ie < g.nx && je >= 0 && je < g.ny && ke >= 0 && ke < g.nz)
+          act |= dom[ie + (int64_t)g.nx * (je + (int64_t)g.ny * ke)] != 0;
+      }
+  nf[n] = act ? NF_ACTIVE : (uint8_t)(NF_CX | NF_CY | NF_CZ);
+}
+
+__global__ void k_fixed_flags(GridDims g, const int32_t* __restrict__ fixed, int32_t nfix, uint8_t* nf) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nfix) return;
+  int32_t d = fixed[t];
+  int64_t node = d / 3;
+  int c = d % 3;
+  // several threads may touch one node byte: use a 32-bit atomicOr on the containing word
+  unsigned int* w = (unsigned int*)((uintptr_t)(nf + node) & ~(uintptr_t)3);
+  int sh = (int)(((uintptr_t)(nf + node) & 3) * 8);
+  atomicOr(w, (unsigned int)(1u << c) << sh);
+}
+
+// count unique fixed DOFs on active nodes (FeModel.ActiveFixedDofCount, :165-183)
+__global__ void k_count_active_fixed(GridDims g, const uint8_t* __restrict__ nf, const uint8_t* __restrict__ fixmask,
+                                     int32_t* count) {
+  int64_t d = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  int v = 0;
+  if (d < g.nd) v = (fixmask[d] != 0) && (nf[d / 3] & NF_ACTIVE);
+  v = __syncthreads_count(v);
+  if (threadIdx.x == 0 && v) atomicAdd(count, v);
+}
+
+__global__ void k_mark_fixed(const int32_t* __restrict__ fixed, int32_t nfix, uint8_t* fixmask) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < nfix) fixmask[fixed[t]] = 1;
+}
+
+void launch_setup_nodes(mycel_problem* p, const int32_t* d_fixed, int32_t n_fixed, int32_t* d_count) {
+  const GridDims& g = p->g;
+  cudaStream_t s = p->ctx->stream;
+  k_node_flags<<<(unsigned)((g.nn + 255) / 256), 256, 0, s>>>(g, p->d_domain, p->d_nflags);
+  p->ctx->launches++;
+  if (n_fixed > 0) {
+    k_fixed_flags<<<(n_fixed + 255) / 256, 256, 0, s>>>(g, d_fixed, n_fixed, p->d_nflags);
+    p->ctx->launches++;
+    // reuse tmp0 as a byte mask of fixed DOFs
+    uint8_t* fixmask = (uint8_t*)p->d_tmp0;
+    cudaMemsetAsync(fixmask, 0, (size_t)g.nd, s);
+    k_mark_fixed<<<(n_fixed + 255) / 256, 256, 0, s>>>(d_fixed, n_fixed, fixmask);
+    k_count_active_fixed<<<(unsigned)((g.nd + 255) / 256), 256, 0, s>>>(g, p->d_nflags, fixmask, d_count);
+    p->ctx->launches += 2;
+  }
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// E_e = Emin + rho^p (E0 - Emin)   (FemOperator.cs:100, :133)
+// ---------------------------------------------------------------------------------------------------------
+__global__ void k_update_E(int64_t na, const int32_t* __restrict__ active, const double* __restrict__ rho,
+                           double emin, double e0, double penal, double* __restrict__ E, float* __restrict__ Ef) {
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= na) return;
+  int32_t e = active[t];
+  double v = emin + path_pow(rho[e], penal) * (e0 - emin);
+  E[e] = v;
+  if (Ef) Ef[e] = (float)v;
+}
+
+void launch_update_E(mycel_problem* p, const double* d_rho_box, double penal) {
+  if (p->n_active == 0) return;
+  k_update_E<<<(unsigned)((p->n_active + 255) / 256), 256, 0, p->ctx->stream>>>(
+      p->n_active, p->d_active, d_rho_box, p->emin, p->e0, penal, p->d_E, p->d_Ef);
+  p->ctx->launches++;
+}
+
+// DiagA[dof] = sum over colours of E_e * DiagKe[k]; constrained -> 1; invD = |d| > 1e-30 ? 1/d : 1
+struct Diag24 { double v[24]; };
+__global__ void __launch_bounds__(256) k_diag(GridDims g, const __grid_constant__ Diag24 dk, const double* __restrict__ E,
+                                              const uint8_t* __restrict__ dom, const uint8_t* __restrict__ nf,
+                                              double* __restrict__ diag, double* __restrict__ invd,
+                                              float* __restrict__ invdf) {
+  ClassNode cn = class_node(g, blockIdx.y, blockIdx.x * (int64_t)blockDim.x + threadIdx.x);
+  if (!cn.valid) return;
+  double d0 = 0.0, d1 = 0.0, d2 = 0.0;
+#pragma unroll 1
+  for (int col = 0; col < 8; ++col) {
+    int ox = (col & 1) ^ cn.px, oy = ((col >> 1) & 1) ^ cn.py, oz = ((col >> 2) & 1) ^ cn.pz;
+    int ie = cn.i - ox, je = cn.j - oy, ke = cn.k - oz;
+    if (ie < 0 || ie >= g.nx || je < 0 || je >= g.ny || ke < 0 || ke >= g.nz) continue;
+    int64_t e = ie + (int64_t)g.nx * (je + (int64_t)g.ny * ke);
+    if (!dom[e]) continue;
+    double ee = E[e];
+    int a = local_index(ox, oy, oz);
+    d0 = d0 + ee * dk.v[3 * a];
+    d1 = d1 + ee * dk.v[3 * a + 1];
+    d2 = d2 + ee * dk.v[3 * a + 2];
+  }
+  int64_t n = cn.i + (int64_t)g.nx1 * (cn.j + (int64_t)g.ny1 * cn.k);
+  uint8_t f = nf[n];
+  double dd[3] = {d0, d1, d2};
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    double d = (f & (1 << c)) ? 1.0 : dd[c];
+    double iv = fabs(d) > 1e-30 ? 1.0 / d : 1.0;
+    diag[3 * n + c] = d;
+    invd[3 * n + c] = iv;
+    if (invdf) invdf[3 * n + c] = (float)iv;
+  }
+}
+
+void launch_diag(mycel_problem* p) {
+  Diag24 dk;
+  for (int i = 0; i < 24; ++i) dk.v[i] = p->diag_ke[i];
+  k_diag<<<class_grid(p->g, 256), 256, 0, p->ctx->stream>>>(p->g, dk, p->d_E, p->d_domain, p->d_nflags, p->d_diag,
+                                                            p->d_invd, p->d_invdf);
+  p->ctx->launches++;
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// y = K x (projected: y = x on constrained DOFs, ApplyA with xIsAlreadyProjected)
+// ---------------------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_matvec64(GridDims g, const __grid_constant__ KeD ke, const double* __restrict__ x,
+                                                  double* __restrict__ y, const double* __restrict__ E,
+                                                  const uint8_t* __restrict__ dom, const uint8_t* __restrict__ nf,
+                                                  int projected, int mode, const int* __restrict__ status) {
+  if (status && *status != PCG_RUNNING) return;
+  ClassNode cn = class_node(g, blockIdx.y, blockIdx.x * (int64_t)blockDim.x + threadIdx.x);
+  if (!cn.valid) return;
+  const int64_t sx = 1, sy = g.nx1, sz = (int64_t)g.nx1 * g.ny1;
+  double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
+#pragma unroll 1
+  for (int col = 0; col < 8; ++col) {
+    int ox = (col & 1) ^ cn.px, oy = ((col >> 1) & 1) ^ cn.py, oz = ((col >> 2) & 1) ^ cn.pz;
+    int ie = cn.i - ox, je = cn.j - oy, kk = cn.k - oz;
+    if (ie < 0 || ie >= g.nx || je < 0 || je >= g.ny || kk < 0 || kk >= g.nz) continue;
+    int64_t e = ie + (int64_t)g.nx * (je + (int64_t)g.ny * kk);
+    if (!__ldg(dom + e)) continue;
+    double ee = __ldg(E + e);
+    int64_t n0 = ie + sy * je + sz * kk;
+    const int64_t off[8] = {0, sx, sx + sy, sy, sz, sz + sx, sz + sx + sy, sz + sy};
+    double ue[24];
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      const double* xp = x + 3 * (n0 + off[b]);
+      ue[3 * b] = __ldg(xp) * ee;
+      ue[3 * b + 1] = __ldg(xp + 1) * ee;
+      ue[3 * b + 2] = __ldg(xp + 2) * ee;
+    }
+    const int a = local_index(ox, oy, oz);
+    double res[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const double* row = ke.v + (3 * a + c) * 24;
+      double l[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        double s = row[q] * ue[q] + row[4 + q] * ue[4 + q];
+        s = s + row[8 + q] * ue[8 + q];
+        s = s + row[12 + q] * ue[12 + q];
+        s = s + row[16 + q] * ue[16 + q];
+        s = s + row[20 + q] * ue[20 + q];
+        l[q] = s;
+      }
+      res[c] = lane_sum(mode, l[0], l[1], l[2], l[3]);
+    }
+    acc0 = acc0 + res[0];
+    acc1 = acc1 + res[1];
+    acc2 = acc2 + res[2];
+  }
+  int64_t n = cn.i + sy * cn.j + sz * cn.k;
+  double out[3] = {acc0, acc1, acc2};
+  uint8_t f = projected ? nf[n] : 0;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) y[3 * n + c] = (f & (1 << c)) ? x[3 * n + c] : out[c];
+}
+
+void launch_matvec64(mycel_problem* p, const double* x, double* y, int projected, const int* d_status) {
+  k_matvec64<<<class_grid(p->g, 256), 256, 0, p->ctx->stream>>>(p->g, p->ke, x, y, p->d_E, p->d_domain,
+                                                                p->d_nflags, projected, p->lane_mode, d_status);
+  p->ctx->launches++;
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// exact block/lane reductions
+// ---------------------------------------------------------------------------------------------------------
+// Sequential 4-lane chain consumer: lanes 0..3 of the calling warp add buf[lane], buf[lane+4], ... in order.
+__device__ __forceinline__ double chain4(double acc, const double* buf, int m, int lane4) {
+  int q = lane4;
+  for (; q + 28 < m; q += 32) {
+    double v0 = buf[q], v1 = buf[q + 4], v2 = buf[q + 8], v3 = buf[q + 12];
+    double v4 = buf[q + 16], v5 = buf[q + 20], v6 = buf[q + 24], v7 = buf[q + 28];
+    acc = acc + v0; acc = acc + v1; acc = acc + v2; acc = acc + v3;
+    acc = acc + v4; acc = acc + v5; acc = acc + v6; acc = acc + v7;
+  }
+  for (; q < m; q += 4) acc = acc + buf[q];
+  return acc;
+}
+
+// Last-CTA election for the final, block-ordered sum (returns true in exactly one CTA, for all its threads).
+__device__ __forceinline__ bool elect_last(unsigned int* counter) {
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned int prev = atomicAdd(counter, 1u);
+    last = (prev == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (last) __threadfence();
+  return last;
+}
+
+// Phases of the single-chain dot kernel.
+enum DotPhase : int { PH_PAP = 0, PH_INIT_RR = 1 };
+
+__global__ void __launch_bounds__(kDotThreads) k_dot_exact(const double* __restrict__ a, const double* __restrict__ b,
+                                                           int64_t n, double* part, PcgState* st, int mode,
+                                                           int phase) {
+  if (st->status != PCG_RUNNING) return;
+  __shared__ double buf[2][kChunk];
+  const int64_t start = (int64_t)blockIdx.x * kBlock;
+  const int cnt = (int)min((int64_t)kBlock, n - start);
+  const int vc4 = cnt & ~3;
+  const int nch = (vc4 + kChunk - 1) / kChunk;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  double acc = 0.0;
+  for (int t = 0; t <= nch; ++t) {
+    if (warp > 0 && t < nch) {
+      const int base = t * kChunk;
+      double* dst = buf[t & 1];
+      for (int q = tid - 32; q < kChunk; q += kDotThreads - 32) {
+        int idx = base + q;
+        if (idx < vc4) dst[q] = a[start + idx] * b[start + idx];
+      }
+    }
+    if (warp == 0 && t > 0 && lane < 4) {
+      const int base = (t - 1) * kChunk;
+      acc = chain4(acc, buf[(t - 1) & 1], min(kChunk, vc4 - base), lane);
+    }
+    __syncthreads();
+  }
+  if (warp == 0) {
+    double l0 = __shfl_sync(0xffffffffu, acc, 0), l1 = __shfl_sync(0xffffffffu, acc, 1);
+    double l2 = __shfl_sync(0xffffffffu, acc, 2), l3 = __shfl_sync(0xffffffffu, acc, 3);
+    if (lane == 0) {
+      double s = lane_sum(mode, l0, l1, l2, l3);
+      for (int idx = vc4; idx < cnt; ++idx) s = s + a[start + idx] * b[start + idx];
+      part[blockIdx.x] = s;
+    }
+  }
+  if (!elect_last(&st->counter)) return;
+  if (tid != 0) return;
+  double sum = 0.0;
+  for (unsigned k = 0; k < gridDim.x; ++k) sum = sum + ld_volatile(part + k);
+  st->counter = 0;
+  if (phase == PH_PAP) {
+    st->iter += 1;
+    double pap = sum;
+    st->pap = pap;
+    if (!(pap > 1e-30) || !isfinite(pap)) {
+      st->last_bad = pap;
+      st->status = PCG_BREAK_CURVATURE;
+      return;
+    }
+    double alpha = st->rho0 / pap;
+    if (!isfinite(alpha) || alpha <= 0.0) {
+      st->last_bad = alpha;
+      st->status = PCG_BREAK_ALPHA;
+      return;
+    }
+    st->alpha = alpha;
+  } else {  // PH_INIT_RR: rNormSq for a non-zero warm start (PcgSolver.cs:176-197)
+    st->rn2 = sum;
+    double rel = sqrt(sum) / st->bnorm;
+    st->rel = rel;
+    st->prev = rel;
+    if (rel <= st->tol) st->status = PCG_INIT_CONVERGED;
+  }
+}
+
+// Fused x/r update with ||r||^2 and z = r*invD with r.z. init=1: only the z part (rho0, p = z).
+__global__ void __launch_bounds__(kDotThreads) k_xr_exact(double* __restrict__ x, double* __restrict__ r,
+                                                          double* __restrict__ z, double* __restrict__ p,
+                                                          const double* __restrict__ ap,
+                                                          const double* __restrict__ invd, int64_t n, double* part,
+                                                          PcgState* st, int mode, int init) {
+  if (st->status != PCG_RUNNING) return;
+  __shared__ double bufA[2][kChunk];
+  __shared__ double bufB[2][kChunk];
+  const double alpha = st->alpha;
+  const int64_t start = (int64_t)blockIdx.x * kBlock;
+  const int cnt = (int)min((int64_t)kBlock, n - start);
+  const int vc4 = cnt & ~3;
+  const int nch = (vc4 + kChunk - 1) / kChunk;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  double acc = 0.0;
+  for (int t = 0; t <= nch; ++t) {
+    if (warp > 0 && t < nch) {
+      const int base = t * kChunk;
+      double* da = bufA[t & 1];
+      double* db = bufB[t & 1];
+      for (int q = tid - 32; q < kChunk; q += kDotThreads - 32) {
+        int idx = base + q;
+        if (idx < vc4) {
+          int64_t j = start + idx;
+          double rv;
+          if (!init) {
+            double xv = x[j] + alpha * p[j];
+            rv = r[j] - alpha * ap[j];
+            x[j] = xv;
+            r[j] = rv;
+            da[q] = rv * rv;
+          } else {
+            rv = r[j];
+          }
+          double zv = rv * invd[j];
+          z[j] = zv;
+          if (init) p[j] = zv;
+          db[q] = rv * zv;
+        }
+      }
+    }
+    if (warp == 0 && t > 0 && lane < 8) {
+      const int base = (t - 1) * kChunk;
+      const int m = min(kChunk, vc4 - base);
+      if (lane < 4) {
+        if (!init) acc = chain4(acc, bufA[(t - 1) & 1], m, lane);
+      } else {
+        acc = chain4(acc, bufB[(t - 1) & 1], m, lane - 4);
+      }
+    }
+    __syncthreads();
+  }
+  if (warp == 0) {
+    double a0 = __shfl_sync(0xffffffffu, acc, 0), a1 = __shfl_sync(0xffffffffu, acc, 1);
+    double a2 = __shfl_sync(0xffffffffu, acc, 2), a3 = __shfl_sync(0xffffffffu, acc, 3);
+    double b0 = __shfl_sync(0xffffffffu, acc, 4), b1 = __shfl_sync(0xffffffffu, acc, 5);
+    double b2 = __shfl_sync(0xffffffffu, acc, 6), b3 = __shfl_sync(0xffffffffu, acc, 7);
+    if (lane == 0) {
+      double sa = lane_sum(mode, a0, a1, a2, a3);
+      double sb = lane_sum(mode, b0, b1, b2, b3);
+      if (!init) {
+        for (int idx = vc4; idx < cnt; ++idx) {
+          int64_t j = start + idx;
+          double xi = x[j] + alpha * p[j];
+          double ri = r[j] - alpha * ap[j];
+          x[j] = xi;
+          r[j] = ri;
+          sa = sa + ri * ri;
+        }
+      }
+      for (int idx = vc4; idx < cnt; ++idx) {
+        int64_t j = start + idx;
+        double zi = r[j] * invd[j];
+        z[j] = zi;
+        if (init) p[j] = zi;
+        sb = sb + r[j] * zi;
+      }
+      part[blockIdx.x] = sa;
+      part[gridDim.x + blockIdx.x] = sb;
+    }
+  }
+  if (!elect_last(&st->counter)) return;
+  if (tid != 0) return;
+  st->counter = 0;
+  const unsigned nb = gridDim.x;
+  if (init) {
+    double rho = 0.0;
+    for (unsigned k = 0; k < nb; ++k) rho = rho + ld_volatile(part + nb + k);
+    st->rho0 = rho;
+    if (st->max_iter <= 0) st->status = PCG_MAXITER;
+    return;
+  }
+  double rn2 = 0.0;
+  for (unsigned k = 0; k < nb; ++k) rn2 = rn2 + ld_volatile(part + k);
+  st->rn2 = rn2;
+  double rel = sqrt(rn2) / st->bnorm;
+  st->rel = rel;
+  if (rel <= st->tol) {
+    st->status = PCG_CONVERGED;
+    return;
+  }
+  if (fabs(rel - st->prev) < 1e-15 * rel) {
+    st->stag += 1;
+    if (st->stag > 50) {
+      st->status = PCG_STAGNATED;
+      return;
+    }
+  } else {
+    st->stag = 0;
+  }
+  st->prev = rel;
+  double rho1 = 0.0;
+  for (unsigned k = 0; k < nb; ++k) rho1 = rho1 + ld_volatile(part + nb + k);
+  double beta = rho1 / st->rho0;
+  if (!isfinite(beta) || beta < 0.0) {
+    st->last_bad = beta;
+    st->status = PCG_BREAK_BETA;
+    return;
+  }
+  st->beta = beta;
+  st->rho0 = rho1;
+  if (st->iter >= st->max_iter) st->status = PCG_MAXITER;
+}
+
+__global__ void k_update_p(double* __restrict__ p, const double* __restrict__ z, int64_t n, const PcgState* st) {
+  if (st->status != PCG_RUNNING) return;
+  const double beta = st->beta;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    p[i] = z[i] + beta * p[i];
+}
+
+// x projection (PcgSolver.cs:113-125) and "has non-zero x" flag
+__global__ void k_project_x(int64_t nd, const uint8_t* __restrict__ nf, double* x, int* flag) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  int nz = 0;
+  if (i < nd) {
+    if (nf[i / 3] & (1 << (i % 3))) x[i] = 0.0;
+    else nz = x[i] != 0.0;
+  }
+  if (__syncthreads_or(nz) && threadIdx.x == 0) atomicOr(flag, 1);
+}
+
+// ||P b||^2: the reference adds b_i^2 over unconstrained i in index order; zero terms leave the running sum
+// unchanged, so the sum over the ascending list of non-zero P b entries is the same number.
+__global__ void k_bnorm_list(const double* __restrict__ b, const int32_t* __restrict__ idx, int32_t cnt,
+                             PcgState* st) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double s = 0.0;
+  for (int32_t q = 0; q < cnt; ++q) {
+    double v = b[idx[q]];
+    s = s + v * v;
+  }
+  st->bn2 = s;
+  st->bnorm = sqrt(s);
+}
+
+void launch_project_x(mycel_problem* p, double* x, int* d_flag) {
+  k_project_x<<<(unsigned)((p->g.nd + 255) / 256), 256, 0, p->ctx->stream>>>(p->g.nd, p->d_nflags, x, d_flag);
+  p->ctx->launches++;
+}
+
+void launch_pcg_bnorm(mycel_problem* p) {
+  k_bnorm_list<<<1, 32, 0, p->ctx->stream>>>(p->d_b, p->d_bnz, p->n_bnz, p->d_state);
+  p->ctx->launches++;
+}
+
+// r = P(b - A x) or P b (PcgSolver.cs:176-192)
+__global__ void k_init_r(int64_t nd, const uint8_t* __restrict__ nf, const double* __restrict__ b,
+                         const double* __restrict__ ap, double* __restrict__ r, int nonzero) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= nd) return;
+  bool con = nf[i / 3] & (1 << (i % 3));
+  r[i] = con ? 0.0 : (nonzero ? (b[i] - ap[i]) : b[i]);
+}
+
+void launch_pcg_init_r(mycel_problem* p, int nonzero) {
+  k_init_r<<<(unsigned)((p->g.nd + 255) / 256), 256, 0, p->ctx->stream>>>(p->g.nd, p->d_nflags, p->d_b, p->d_ap,
+                                                                         p->d_r, nonzero);
+  p->ctx->launches++;
+}
+
+void launch_pcg_dot_rr(mycel_problem* p) {
+  int64_t nb = num_blocks8192(p->g.nd);
+  k_dot_exact<<<(unsigned)nb, kDotThreads, 0, p->ctx->stream>>>(p->d_r, p->d_r, p->g.nd, p->d_part, p->d_state,
+                                                                p->lane_mode, PH_INIT_RR);
+  p->ctx->launches++;
+}
+
+void launch_pcg_init_z(mycel_problem* p) {
+  int64_t nb = num_blocks8192(p->g.nd);
+  k_xr_exact<<<(unsigned)nb, kDotThreads, 0, p->ctx->stream>>>(p->d_x, p->d_r, p->d_z, p->d_p, p->d_ap, p->d_invd,
+                                                               p->g.nd, p->d_part, p->d_state, p->lane_mode, 1);
+  p->ctx->launches++;
+}
+
+// One PCG iteration (PcgSolver.cs:235-357): Ap = A p; pAp, alpha; x, r, ||r||; z, rho1, beta; p = z + beta p.
+void launch_pcg_iteration(mycel_problem* p) {
+  cudaStream_t s = p->ctx->stream;
+  int64_t nb = num_blocks8192(p->g.nd);
+  launch_matvec64(p, p->d_p, p->d_ap, 1, &p->d_state->status);
+  k_dot_exact<<<(unsigned)nb, kDotThreads, 0, s>>>(p->d_p, p->d_ap, p->g.nd, p->d_part, p->d_state, p->lane_mode,
+                                                   PH_PAP);
+  k_xr_exact<<<(unsigned)nb, kDotThreads, 0, s>>>(p->d_x, p->d_r, p->d_z, p->d_p, p->d_ap, p->d_invd, p->g.nd,
+                                                  p->d_part, p->d_state, p->lane_mode, 0);
+  k_update_p<<<(unsigned)std::min<int64_t>((p->g.nd + 255) / 256, 4096), 256, 0, s>>>(p->d_p, p->d_z, p->g.nd,
+                                                                                        p->d_state);
+  p->ctx->launches += 3;
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// compliance C = F.u (sequential over non-zero F in index order), max |u| over active nodes, reactions
+// ---------------------------------------------------------------------------------------------------------
+__global__ void k_compliance(const double* __restrict__ F, const double* __restrict__ u,
+                             const int32_t* __restrict__ idx, int32_t cnt, double* out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double c = 0.0;
+  for (int32_t q = 0; q < cnt; ++q) c = c + F[idx[q]] * u[idx[q]];
+  *out = c;
+}
+
+void launch_compliance(mycel_problem* p, const double* u, double* d_out) {
+  k_compliance<<<1, 32, 0, p->ctx->stream>>>(p->d_F, u, p->d_fnz, p->n_fnz, d_out);
+  p->ctx->launches++;
+}
+
+__device__ __forceinline__ unsigned long long dbl_key(double v) {
+  // non-negative doubles order like their bit patterns
+  return (unsigned long long)__double_as_longlong(v);
+}
+
+__global__ void k_max_disp(GridDims g, const uint8_t* __restrict__ nf, const double* __restrict__ u,
+                           unsigned long long* out) {
+  double m = 0.0;
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < g.nn; n += (int64_t)gridDim.x * blockDim.x) {
+    if (!(nf[n] & NF_ACTIVE)) continue;
+    double ux = u[3 * n], uy = u[3 * n + 1], uz = u[3 * n + 2];
+    double s = ux * ux + uy * uy + uz * uz;
+    if (s > m) m = s;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    double v = __shfl_down_sync(0xffffffffu, m, o);
+    if (v > m) m = v;
+  }
+  if ((threadIdx.x & 31) == 0 && m > 0.0) atomicMax(out, dbl_key(m));
+}
+
+__global__ void k_sqrt_inplace(unsigned long long* v) {
+  double d = __longlong_as_double((long long)*v);
+  *(double*)v = sqrt(d);
+}
+
+void launch_max_disp(mycel_problem* p, const double* u, double* d_out) {
+  cudaMemsetAsync(d_out, 0, sizeof(double), p->ctx->stream);
+  int blocks = std::max(1, std::min<int>((int)((p->g.nn + 255) / 256), p->ctx->num_sms * 8));
+  k_max_disp<<<blocks, 256, 0, p->ctx->stream>>>(p->g, p->d_nflags, u, (unsigned long long*)d_out);
+  k_sqrt_inplace<<<1, 1, 0, p->ctx->stream>>>((unsigned long long*)d_out);
+  p->ctx->launches += 2;
+}
+
+__global__ void k_reactions(const double* __restrict__ ku, double* out, const int32_t* __restrict__ fixed, int32_t nf) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < nf) out[fixed[t]] = ku[fixed[t]];
+}
+
+void launch_reactions(mycel_problem* p, const double* ku, double* out, const int32_t* d_fixed, int32_t n_fixed) {
+  cudaMemsetAsync(out, 0, sizeof(double) * p->g.nd, p->ctx->stream);
+  if (n_fixed > 0) {
+    k_reactions<<<(n_fixed + 255) / 256, 256, 0, p->ctx->stream>>>(ku, out, d_fixed, n_fixed);
+    p->ctx->launches++;
+  }
+}
+
+// Element von Mises at the centroid (StaticAnalysis.cs:144-216)
+struct VmConst {
+  double bc[144];
+  double d[36];
+  double invh;
+};
+__global__ void k_von_mises(GridDims g, const __grid_constant__ VmConst vc, const double* __restrict__ u, const double* __restrict__ E,
+                            const uint8_t* __restrict__ dom, double* __restrict__ vm) {
+  int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= g.ne) return;
+  if (!dom[e]) {
+    vm[e] = 0.0;
+    return;
+  }
+  int ix = (int)(e % g.nx);
+  int64_t r = e / g.nx;
+  int iy = (int)(r % g.ny), iz = (int)(r / g.ny);
+  const int64_t sy = g.nx1, sz = (int64_t)g.nx1 * g.ny1;
+  int64_t n0 = ix + sy * iy + sz * iz;
+  const int64_t off[8] = {0, 1, 1 + sy, sy, sz, sz + 1, sz + 1 + sy, sz + sy};
+  double ue[24];
+  for (int b = 0; b < 8; ++b)
+    for (int c = 0; c < 3; ++c) ue[3 * b + c] = u[3 * (n0 + off[b]) + c];
+  double eps[6], sig[6];
+  for (int q = 0; q < 6; ++q) {
+    double s = 0.0;
+    for (int k = 0; k < 24; ++k) s = s + vc.bc[q * 24 + k] * ue[k];
+    eps[q] = s * vc.invh;
+  }
+  double ee = E[e];
+  for (int q = 0; q < 6; ++q) {
+    double s = 0.0;
+    for (int k = 0; k < 6; ++k) s = s + vc.d[q * 6 + k] * eps[k];
+    sig[q] = s * ee;
+  }
+  double d1 = sig[0] - sig[1], d2 = sig[1] - sig[2], d3 = sig[2] - sig[0];
+  vm[e] = sqrt(0.5 * (d1 * d1 + d2 * d2 + d3 * d3) + 3.0 * (sig[3] * sig[3] + sig[4] * sig[4] + sig[5] * sig[5]));
+}
+
+void launch_von_mises(mycel_problem* p, const double* u, double* vm) {
+  VmConst vc;
+  // Hex8Element.BaseBc = EvaluateB(0,0,0,h=1) (Hex8Element.cs:71, :183-215)
+  static const double xi[8] = {-1, 1, 1, -1, -1, 1, 1, -1}, eta[8] = {-1, -1, 1, 1, -1, -1, 1, 1},
+                      zeta[8] = {-1, -1, -1, -1, 1, 1, 1, 1};
+  for (int i = 0; i < 144; ++i) vc.bc[i] = 0.0;
+  for (int a = 0; a < 8; ++a) {
+    double dx = (0.25 * 1.0) * xi[a] * (1.0 + eta[a] * 0.0) * (1.0 + zeta[a] * 0.0);
+    double dy = (0.25 * 1.0) * eta[a] * (1.0 + xi[a] * 0.0) * (1.0 + zeta[a] * 0.0);
+    double dz = (0.25 * 1.0) * zeta[a] * (1.0 + xi[a] * 0.0) * (1.0 + eta[a] * 0.0);
+    vc.bc[0 * 24 + 3 * a] = dx; vc.bc[1 * 24 + 3 * a + 1] = dy; vc.bc[2 * 24 + 3 * a + 2] = dz;
+    vc.bc[3 * 24 + 3 * a + 1] = dz; vc.bc[3 * 24 + 3 * a + 2] = dy;
+    vc.bc[4 * 24 + 3 * a] = dz; vc.bc[4 * 24 + 3 * a + 2] = dx;
+    vc.bc[5 * 24 + 3 * a] = dy; vc.bc[5 * 24 + 3 * a + 1] = dx;
+  }
+  double nu = p->nu;
+  double factor = 1.0 / ((1.0 + nu) * (1.0 - 2.0 * nu));
+  double c1 = factor * (1.0 - nu), c2 = factor * nu, c3 = 1.0 / (2.0 * (1.0 + nu));
+  for (int i = 0; i < 36; ++i) vc.d[i] = 0.0;
+  vc.d[0] = c1; vc.d[1] = c2; vc.d[2] = c2; vc.d[6] = c2; vc.d[7] = c1; vc.d[8] = c2;
+  vc.d[12] = c2; vc.d[13] = c2; vc.d[14] = c1; vc.d[21] = c3; vc.d[28] = c3; vc.d[35] = c3;
+  vc.invh = 1.0 / (double)p->h;
+  k_von_mises<<<(unsigned)((p->g.ne + 255) / 256), 256, 0, p->ctx->stream>>>(p->g, vc, u, p->d_E, p->d_domain, vm);
+  p->ctx->launches++;
+}
+
+// active <-> box index maps
+__global__ void k_scatter_active(int64_t na, const int32_t* __restrict__ act, const double* __restrict__ src,
+                                 double* __restrict__ dst) {
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t < na) dst[act[t]] = src[t];
+}
+__global__ void k_gather_active(int64_t na, const int32_t* __restrict__ act, const double* __restrict__ src,
+                                double* __restrict__ dst) {
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t < na) dst[t] = src[act[t]];
+}
+__global__ void k_fill(int64_t n, double* p, double v) {
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t < n) p[t] = v;
+}
+
+void launch_scatter_active(mycel_problem* p, const double* src_active, double* dst_box, double fill) {
+  k_fill<<<(unsigned)((p->g.ne + 255) / 256), 256, 0, p->ctx->stream>>>(p->g.ne, dst_box, fill);
+  p->ctx->launches++;
+  if (p->n_active == 0) return;
+  k_scatter_active<<<(unsigned)((p->n_active + 255) / 256), 256, 0, p->ctx->stream>>>(p->n_active, p->d_active,
+                                                                                      src_active, dst_box);
+  p->ctx->launches++;
+}
+
+void launch_gather_active(mycel_problem* p, const double* src_box, double* dst_active) {
+  if (p->n_active == 0) return;
+  k_gather_active<<<(unsigned)((p->n_active + 255) / 256), 256, 0, p->ctx->stream>>>(p->n_active, p->d_active,
+                                                                                     src_box, dst_active);
+  p->ctx->launches++;
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// Density filter as a stencil (DensityFilter.cs:61-198)
+// ---------------------------------------------------------------------------------------------------------
+// invHs per active element: hs accumulated over included neighbours in loop order.
+__global__ void k_filter_invhs(GridDims g, const uint8_t* __restrict__ dom, const int4* __restrict__ off,
+                               const double* __restrict__ w, int noff, double* __restrict__ invhs) {
+  int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= g.ne || !dom[e]) return;
+  int ex = (int)(e % g.nx);
+  int64_t r = e / g.nx;
+  int ey = (int)(r % g.ny), ez = (int)(r / g.ny);
+  double hs = 0.0;
+  for (int q = 0; q < noff; ++q) {
+    int4 o = off[q];
+    int jx = ex + o.x, jy = ey + o.y, jz = ez + o.z;
+    if (jx < 0 || jx >= g.nx || jy < 0 || jy >= g.ny || jz < 0 || jz >= g.nz) continue;
+    if (!dom[jx + (int64_t)g.nx * (jy + (int64_t)g.ny * jz)]) continue;
+    hs = hs + w[q];
+  }
+  invhs[e] = hs > 0.0 ? 1.0 / hs : 1.0;
+}
+
+// forward: out_r = sum_j (w_rj * invHs_r) * in_j, j in loop order.
+// adjoint: out_i = sum_r (w_ri * invHs_r) * in_r, r ascending (the adjoint CSR rows are filled in forward-row
+//          order, DensityFilter.cs:172-185); with in = 1 this is S_i (:188-198).
+template <int ADJ>
+__global__ void k_filter_apply(GridDims g, const uint8_t* __restrict__ dom, const int4* __restrict__ off,
+                               const double* __restrict__ w, int noff, const double* __restrict__ invhs,
+                               const double* __restrict__ in, double* __restrict__ out, int ones) {
+  int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= g.ne || !dom[e]) return;
+  int ex = (int)(e % g.nx);
+  int64_t r = e / g.nx;
+  int ey = (int)(r % g.ny), ez = (int)(r / g.ny);
+  double s = 0.0;
+  const double ih = invhs[e];
+  for (int q = 0; q < noff; ++q) {
+    int4 o = off[q];
+    int jx = ex + o.x, jy = ey + o.y, jz = ez + o.z;
+    if (jx < 0 || jx >= g.nx || jy < 0 || jy >= g.ny || jz < 0 || jz >= g.nz) continue;
+    int64_t j = jx + (int64_t)g.nx * (jy + (int64_t)g.ny * jz);
+    if (!dom[j]) continue;
+    if (ADJ) {
+      double wt = w[q] * invhs[j];
+      s = s + (ones ? wt : wt * in[j]);
+    } else {
+      s = s + (w[q] * ih) * in[j];
+    }
+  }
+  out[e] = s;
+}
+
+int filter_setup(mycel_filter* f) {
+  mycel_problem* p = f->p;
+  double rmin = f->rmin;
+  int rc = (int)ceil(rmin);
+  double rsq = rmin * rmin;
+  std::vector<int4> offs;
+  std::vector<double> ws;
+  for (int dz = -rc; dz <= rc; ++dz)
+    for (int dy = -rc; dy <= rc; ++dy)
+      for (int dx = -rc; dx <= rc; ++dx) {
+        int ds = dz * dz + dy * dy + dx * dx;
+        if (!((double)ds < rsq)) continue;
+        double dist = sqrt((double)ds);
+        if (!(dist < rmin)) continue;
+        offs.push_back(make_int4(dx, dy, dz, 0));
+        ws.push_back(rmin - dist);
+      }
+  f->n_off = (int)offs.size();
+  cudaStream_t s = p->ctx->stream;
+  if (cudaMalloc(&f->d_off, sizeof(int4) * offs.size()) != cudaSuccess) return MYCEL_E_OOM;
+  if (cudaMalloc(&f->d_w, sizeof(double) * ws.size()) != cudaSuccess) return MYCEL_E_OOM;
+  if (cudaMalloc(&f->d_invhs, sizeof(double) * p->g.ne) != cudaSuccess) return MYCEL_E_OOM;
+  if (cudaMalloc(&f->d_s, sizeof(double) * p->g.ne) != cudaSuccess) return MYCEL_E_OOM;
+  cudaMemcpyAsync(f->d_off, offs.data(), sizeof(int4) * offs.size(), cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(f->d_w, ws.data(), sizeof(double) * ws.size(), cudaMemcpyHostToDevice, s);
+  cudaMemsetAsync(f->d_invhs, 0, sizeof(double) * p->g.ne, s);
+  cudaMemsetAsync(f->d_s, 0, sizeof(double) * p->g.ne, s);
+  unsigned nb = (unsigned)((p->g.ne + 127) / 128);
+  k_filter_invhs<<<nb, 128, 0, s>>>(p->g, p->d_domain, f->d_off, f->d_w, f->n_off, f->d_invhs);
+  k_filter_apply<1><<<nb, 128, 0, s>>>(p->g, p->d_domain, f->d_off, f->d_w, f->n_off, f->d_invhs, nullptr, f->d_s, 1);
+  p->ctx->launches += 2;
+  cudaStreamSynchronize(s);  // host vectors above must outlive the copies
+  return cudaGetLastError() == cudaSuccess ? MYCEL_OK : MYCEL_E_DEVICE;
+}
+
+void launch_filter_fwd(mycel_filter* f, const double* in_box, double* out_box) {
+  mycel_problem* p = f->p;
+  k_filter_apply<0><<<(unsigned)((p->g.ne + 127) / 128), 128, 0, p->ctx->stream>>>(
+      p->g, p->d_domain, f->d_off, f->d_w, f->n_off, f->d_invhs, in_box, out_box, 0);
+  p->ctx->launches++;
+}
+
+void launch_filter_adj(mycel_filter* f, const double* in_box, double* out_box) {
+  mycel_problem* p = f->p;
+  k_filter_apply<1><<<(unsigned)((p->g.ne + 127) / 128), 128, 0, p->ctx->stream>>>(
+      p->g, p->d_domain, f->d_off, f->d_w, f->n_off, f->d_invhs, in_box, out_box, 0);
+  p->ctx->launches++;
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// compliance sensitivities dc/drhoBar_e = -(p rho^(p-1) dE) * ue^T KE ue   (SensitivityAnalysis.cs:98-144)
+// ---------------------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_sens(GridDims g, const __grid_constant__ KeD ke, const double* __restrict__ u,
+                                              const double* __restrict__ rho, const uint8_t* __restrict__ dom,
+                                              double penal, double dE, double* __restrict__ dc) {
+  int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= g.ne || !dom[e]) return;
+  int ix = (int)(e % g.nx);
+  int64_t r = e / g.nx;
+  int iy = (int)(r % g.ny), iz = (int)(r / g.ny);
+  const int64_t sy = g.nx1, sz = (int64_t)g.nx1 * g.ny1;
+  int64_t n0 = ix + sy * iy + sz * iz;
+  const int64_t off[8] = {0, 1, 1 + sy, sy, sz, sz + 1, sz + 1 + sy, sz + sy};
+  double ue[24];
+#pragma unroll
+  for (int b = 0; b < 8; ++b)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) ue[3 * b + c] = __ldg(u + 3 * (n0 + off[b]) + c);
+  double se = 0.0;
+#pragma unroll
+  for (int rr = 0; rr < 24; ++rr) {
+    double s = 0.0;
+#pragma unroll
+    for (int c = 0; c < 24; ++c) s = s + ke.v[rr * 24 + c] * ue[c];
+    se = se + ue[rr] * s;
+  }
+  double dEdr = penal * path_pow(rho[e], penal - 1.0) * dE;
+  dc[e] = -dEdr * se;
+}
+
+void launch_sens(mycel_problem* p, const double* u, const double* rho_box, double penal, double* dc_box) {
+  k_sens<<<(unsigned)((p->g.ne + 127) / 128), 128, 0, p->ctx->stream>>>(p->g, p->ke, u, rho_box, p->d_domain, penal,
+                                                                        p->e0 - p->emin, dc_box);
+  p->ctx->launches++;
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// OC update: persistent cooperative kernel with a bounded grid barrier
+// ---------------------------------------------------------------------------------------------------------
+constexpr long long kBarrierSpinLimit = 1ll << 24;  // ~1 s of __nanosleep(64) polling before giving up
+
+__device__ bool grid_sync_bounded(unsigned int* bar, int* err) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned int* vgen = bar + 1;
+    unsigned int gen = *vgen;
+    __threadfence();
+    unsigned int arrived = atomicAdd(bar, 1u);
+    if (arrived == gridDim.x - 1) {
+      bar[0] = 0;
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      long long spins = 0;
+      while (*vgen == gen) {
+        if (++spins > kBarrierSpinLimit || *(volatile int*)err) {
+          atomicExch(err, 1);
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return *(volatile int*)err == 0;
+}
+
+__device__ __forceinline__ double clampd(double v, double lo, double hi) {
+  if (v < lo) return lo;
+  if (v > hi) return hi;
+  return v;
+}
+__device__ __forceinline__ double maxd(double a, double b) {
+  if (isnan(a) || isnan(b)) return __longlong_as_double(0x7ff8000000000000ll);
+  return a > b ? a : b;
+}
+__device__ __forceinline__ double mind(double a, double b) {
+  if (isnan(a) || isnan(b)) return __longlong_as_double(0x7ff8000000000000ll);
+  return a < b ? a : b;
+}
+
+// volume term of element i for multiplier lam (OcOptimizer.EvaluateVolume :134-175) and the new density
+__device__ __forceinline__ double oc_new_rho(double r, double dc, double si, bool pas, double lam, double move,
+                                             double rmin) {
+  if (pas) return 1.0;
+  double lo = maxd(rmin, r - move), hi = mind(1.0, r + move);
+  double nd = -dc;
+  if (nd <= 0.0 || si <= 0.0) return lo;
+  double b = nd / (lam * si);
+  return clampd(r * sqrt(b), lo, hi);
+}
+
+__device__ double block_sum(double v, double* sh) {
+  for (int o = 16; o > 0; o >>= 1) v = v + __shfl_down_sync(0xffffffffu, v, o);
+  int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t = t + sh[k];
+  }
+  return t;  // valid in thread 0
+}
+
+struct OcArgs {
+  int64_t n;
+  const int32_t* idx;
+  const double* rho;
+  const double* dc;
+  const double* s;
+  const uint8_t* pas;
+  double* rho_new;
+  const double* rho_phys;
+  const double* rho_grey;
+  double* scratch;  // 2 * gridDim.x * 3 doubles
+  unsigned int* bar;
+  int* err;
+  OcOut* out;
+};
+
+// Grid-wide deterministic sum of per-thread values; every block returns the same total (thread 0 valid).
+__device__ double grid_total(double mine, const OcArgs& a, int slot, double* sh, bool* ok) {
+  double bs = block_sum(mine, sh);
+  double* part = a.scratch + (size_t)slot * gridDim.x;
+  if (threadIdx.x == 0) part[blockIdx.x] = bs;
+  if (!grid_sync_bounded(a.bar, a.err)) {
+    *ok = false;
+    return 0.0;
+  }
+  double t = 0.0;
+  if (threadIdx.x == 0)
+    for (unsigned k = 0; k < gridDim.x; ++k) t = t + ld_volatile(part + k);
+  return t;
+}
+
+__global__ void __launch_bounds__(256) k_oc(OcArgs a, OcParams prm) {
+  __shared__ double sh[32];
+  __shared__ double bc[4];
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t t0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  bool ok = true;
+  int slot = 0;
+  auto element = [&](int64_t i) -> int64_t { return a.idx ? (int64_t)a.idx[i] : i; };
+  auto volume = [&](double lam) -> double {
+    double v = 0.0;
+    for (int64_t i = t0; i < a.n; i += stride) {
+      int64_t e = element(i);
+      bool pas = a.pas && a.pas[e];
+      double si = a.s[e];
+      v = v + si * (pas ? 1.0 : oc_new_rho(a.rho[e], a.dc[e], si, false, lam, prm.move, prm.rho_min));
+    }
+    double tot = grid_total(v, a, slot, sh, &ok);
+    slot ^= 1;
+    if (threadIdx.x == 0) bc[0] = tot;
+    __syncthreads();
+    return bc[0];
+  };
+  // total S (OcOptimizer.cs:177-182)
+  double sv = 0.0;
+  for (int64_t i = t0; i < a.n; i += stride) sv = sv + a.s[element(i)];
+  double ts = grid_total(sv, a, slot, sh, &ok);
+  slot ^= 1;
+  if (threadIdx.x == 0) bc[0] = ts;
+  __syncthreads();
+  ts = bc[0];
+  if (!ok) return;
+  const double tv = prm.f * ts;
+  const double lg = prm.lambda_guess;
+  bool gok = lg > 0.0 && !isinf(lg) && !isnan(lg);
+  double l1 = gok ? lg * 0.5 : 1e-12;
+  double l2 = gok ? lg * 2.0 : 1e12;
+  if (l1 <= 1e-50) l1 = 1e-12;
+  if (l2 <= l1) l2 = l1 * 10.0;
+  int trials = 0;
+  double v1 = volume(l1);
+  double v2 = volume(l2);
+  trials += 2;
+  if (!ok) return;
+  int ex = 0;
+  while (v1 < tv && l1 > 1e-50 && ex++ < 50) {
+    l2 = l1;
+    v2 = v1;
+    l1 *= 0.1;
+    v1 = volume(l1);
+    ++trials;
+    if (!ok) return;
+  }
+  ex = 0;
+  while (v2 > tv && l2 < 1e50 && ex++ < 50) {
+    l1 = l2;
+    v1 = v2;
+    l2 *= 10.0;
+    v2 = volume(l2);
+    ++trials;
+    if (!ok) return;
+  }
+  double lm = sqrt(l1 * l2);
+  for (int st = 0; st < prm.max_bisect; ++st) {
+    lm = sqrt(l1 * l2);
+    double vm = volume(lm);
+    ++trials;
+    if (!ok) return;
+    double re = fabs(vm - tv) / maxd(tv, 1e-12);
+    if (re <= prm.vol_tol) break;
+    if (vm > tv) l1 = lm;
+    else l2 = lm;
+    if (fabs(l2 - l1) <= 1e-15 * lm) break;
+  }
+  // final densities and the iteration metrics (TopologyOptimizer.cs:323-338)
+  double mc = 0.0, vs = 0.0, gs = 0.0;
+  for (int64_t i = t0; i < a.n; i += stride) {
+    int64_t e = element(i);
+    bool pas = a.pas && a.pas[e];
+    double r = a.rho[e];
+    double nr = oc_new_rho(r, a.dc[e], a.s[e], pas, lm, prm.move, prm.rho_min);
+    a.rho_new[e] = nr;
+    double d = fabs(nr - r);
+    if (d > mc) mc = d;
+    if (a.rho_phys) {
+      vs = vs + a.rho_phys[e];
+      double rb = a.rho_grey[e];
+      gs = gs + rb * (1.0 - rb);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    double v = __shfl_down_sync(0xffffffffu, mc, o);
+    if (v > mc) mc = v;
+  }
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = mc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k)
+      if (sh[k] > mc) mc = sh[k];
+  }
+  double* part = a.scratch + (size_t)2 * 2 * gridDim.x;  // slots 4..6
+  double bvs = block_sum(vs, sh);
+  double bgs = block_sum(gs, sh);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = mc;
+    part[gridDim.x + blockIdx.x] = bvs;
+    part[2 * gridDim.x + blockIdx.x] = bgs;
+  }
+  if (!grid_sync_bounded(a.bar, a.err)) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    double m = 0.0, v = 0.0, gg = 0.0;
+    for (unsigned k = 0; k < gridDim.x; ++k) {
+      double q = ld_volatile(part + k);
+      if (q > m) m = q;
+      v = v + ld_volatile(part + gridDim.x + k);
+      gg = gg + ld_volatile(part + 2 * gridDim.x + k);
+    }
+    a.out->lambda = lm;
+    a.out->max_change = m;
+    a.out->vol_sum = v;
+    a.out->grey_sum = gg;
+    a.out->err = 0;
+    a.out->trials = trials;
+  }
+}
+
+int launch_oc(mycel_ctx* ctx, int64_t n, const int32_t* d_index, const double* rho, const double* dc, const double* s,
+              const uint8_t* passive, double* rho_new, const double* rho_phys_for_metrics,
+              const double* rho_tilde_for_grey, const OcParams& prm, double* d_scratch, OcOut* d_out) {
+  static int blocks_per_sm = -1;
+  if (blocks_per_sm < 0) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_oc, 256, 0);
+    if (blocks_per_sm < 1) blocks_per_sm = 1;
+    if (blocks_per_sm > 2) blocks_per_sm = 2;
+  }
+  int grid = ctx->num_sms * blocks_per_sm;
+  // scratch layout: [7 * grid] doubles of partials, then barrier words + error flag
+  unsigned int* bar = (unsigned int*)(d_scratch + 8 * grid);
+  int* err = (int*)(bar + 4);
+  cudaMemsetAsync(bar, 0, 8 * sizeof(unsigned int), ctx->stream);
+  OcArgs a{n, d_index, rho, dc, s, passive, rho_new, rho_phys_for_metrics,
+           rho_tilde_for_grey ? rho_tilde_for_grey : rho_phys_for_metrics, d_scratch, bar, err, d_out};
+  OcParams pp = prm;
+  void* args[] = {&a, &pp};
+  cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_oc, dim3(grid), dim3(256), args, 0, ctx->stream);
+  ctx->launches++;
+  if (e != cudaSuccess) return MYCEL_E_DEVICE;
+  return MYCEL_OK;
+}
+
+}  // namespace mycel

@@ -1,0 +1,90 @@
+// Hex8 element stiffness for the library (set-up only; the matrix is passed to the kernels by value).
+// Follows Hex8Element.CreateKe (src/Mycel.Core/Fem/Hex8Element.cs:98-178): 2x2x2 Gauss points at +-1/sqrt(3),
+// weight det(J) = 1/8 for h = 1, Ke(h) = h Ke(1); nu = 0.3 takes the fast path BaseKe * h (:104-112), where
+// BaseKe itself is the Gauss-integrated Ke(1, 0.3). Compiled with -ffp-contract=off.
+#include <cmath>
+
+#include "internal.h"
+
+namespace mycel {
+namespace {
+
+void constitutive_unit(double nu, double d[36]) {
+  double factor = 1.0 / ((1.0 + nu) * (1.0 - 2.0 * nu));
+  double c1 = factor * (1.0 - nu), c2 = factor * nu, c3 = 1.0 / (2.0 * (1.0 + nu));
+  for (int i = 0; i < 36; ++i) d[i] = 0.0;
+  d[0] = c1; d[1] = c2; d[2] = c2;
+  d[6] = c2; d[7] = c1; d[8] = c2;
+  d[12] = c2; d[13] = c2; d[14] = c1;
+  d[21] = c3; d[28] = c3; d[35] = c3;
+}
+
+// strain-displacement matrix (6 x 24) at (xi, eta, zeta) for unit edge, Voigt order xx yy zz yz zx xy
+void strain_matrix(double xi, double eta, double zeta, double b[144]) {
+  static const double sx[8] = {-1, 1, 1, -1, -1, 1, 1, -1};
+  static const double sy[8] = {-1, -1, 1, 1, -1, -1, 1, 1};
+  static const double sz[8] = {-1, -1, -1, -1, 1, 1, 1, 1};
+  for (int i = 0; i < 144; ++i) b[i] = 0.0;
+  const double q = 0.25 * (1.0 / 1.0);
+  for (int a = 0; a < 8; ++a) {
+    double gx = q * sx[a] * (1.0 + sy[a] * eta) * (1.0 + sz[a] * zeta);
+    double gy = q * sy[a] * (1.0 + sx[a] * xi) * (1.0 + sz[a] * zeta);
+    double gz = q * sz[a] * (1.0 + sx[a] * xi) * (1.0 + sy[a] * eta);
+    b[0 * 24 + 3 * a] = gx;
+    b[1 * 24 + 3 * a + 1] = gy;
+    b[2 * 24 + 3 * a + 2] = gz;
+    b[3 * 24 + 3 * a + 1] = gz;
+    b[3 * 24 + 3 * a + 2] = gy;
+    b[4 * 24 + 3 * a] = gz;
+    b[4 * 24 + 3 * a + 2] = gx;
+    b[5 * 24 + 3 * a] = gy;
+    b[5 * 24 + 3 * a + 1] = gx;
+  }
+}
+
+void gauss_ke_unit(double nu, double ke[576]) {
+  const double gp = 1.0 / std::sqrt(3.0);
+  const double pts[2] = {-gp, gp};
+  double d[36], b[144], db[144];
+  constitutive_unit(nu, d);
+  for (int i = 0; i < 576; ++i) ke[i] = 0.0;
+  for (int ix = 0; ix < 2; ++ix)
+    for (int iy = 0; iy < 2; ++iy)
+      for (int iz = 0; iz < 2; ++iz) {
+        strain_matrix(pts[ix], pts[iy], pts[iz], b);
+        for (int r = 0; r < 6; ++r)
+          for (int c = 0; c < 24; ++c) {
+            double s = 0.0;
+            for (int k = 0; k < 6; ++k) s += d[r * 6 + k] * b[k * 24 + c];
+            db[r * 24 + c] = s;
+          }
+        for (int i = 0; i < 24; ++i)
+          for (int j = 0; j < 24; ++j) {
+            double s = 0.0;
+            for (int k = 0; k < 6; ++k) s += b[k * 24 + i] * db[k * 24 + j];
+            ke[i * 24 + j] += s * (1.0 / 8.0);
+          }
+      }
+}
+
+}  // namespace
+
+void build_ke(double h, double nu, double* ke) {
+  if (std::fabs(nu - 0.3) < 1e-15) {
+    static double base[576];
+    static bool have = false;
+    if (!have) {
+      gauss_ke_unit(0.3, base);
+      have = true;
+    }
+    for (int i = 0; i < 576; ++i) ke[i] = base[i] * h;
+    return;
+  }
+  gauss_ke_unit(nu, ke);
+  if (std::fabs(h - 1.0) > 1e-15)
+    for (int i = 0; i < 576; ++i) ke[i] *= h;
+}
+
+int64_t num_blocks8192(int64_t n) { return (n + 8191) / 8192; }
+
+}  // namespace mycel

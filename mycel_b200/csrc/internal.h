@@ -1,0 +1,217 @@
+// Internal declarations of libmycel_b200: device state of a problem, kernel launchers, helpers.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/mycel.h"
+
+namespace mycel {
+
+// ---- small POD passed by value to kernels (kernel parameter space is broadcast like constant memory) ----
+struct GridDims {
+  int nx, ny, nz;    // elements per axis
+  int nx1, ny1, nz1; // nodes per axis
+  int64_t ne, nn, nd;
+};
+
+inline GridDims make_dims(int nx, int ny, int nz) {
+  GridDims g;
+  g.nx = nx; g.ny = ny; g.nz = nz;
+  g.nx1 = nx + 1; g.ny1 = ny + 1; g.nz1 = nz + 1;
+  g.ne = (int64_t)nx * ny * nz;
+  g.nn = (int64_t)g.nx1 * g.ny1 * g.nz1;
+  g.nd = 3 * g.nn;
+  return g;
+}
+
+struct KeD { double v[576]; };  // element stiffness (row-major), FP64
+struct KeF { float v[576]; };   // FP32 copy for the mixed form
+
+// Node flag bits (one byte per node): bits 0-2 = DOF c constrained, bit 3 = node active.
+enum : uint8_t { NF_CX = 1, NF_CY = 2, NF_CZ = 4, NF_ACTIVE = 8 };
+
+// PCG status word (device). 0 = running.
+enum PcgStatus : int {
+  PCG_RUNNING = 0,
+  PCG_CONVERGED = 1,
+  PCG_BREAK_CURVATURE = 2,
+  PCG_BREAK_ALPHA = 3,
+  PCG_STAGNATED = 4,
+  PCG_BREAK_BETA = 5,
+  PCG_MAXITER = 6,
+  PCG_INIT_CONVERGED = 7,
+  PCG_RHS_ZERO = 8,
+};
+
+// Device-resident scalar state of one PCG solve (PcgSolver.cs:231-357 locals).
+struct PcgState {
+  int status;
+  int iter;
+  int max_iter;
+  int stag;
+  int nonzero_x;
+  int pad_;
+  double tol, bnorm, bn2, rho0, rel, prev, alpha, beta, pap, rn2, last_bad;
+  unsigned int counter;  // completion counter for the last-block pattern
+  unsigned int counter2;
+  double dot_acc;        // scratch (mixed form)
+};
+
+// ---- device memory helpers ----
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace mycel
+
+// ---- opaque handles of the C ABI ----
+struct mycel_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int num_sms = 148;
+  int64_t launches = 0;
+  std::string last_error;
+  void* pinned = nullptr;  // small pinned scratch for scalar readbacks
+  size_t pinned_bytes = 0;
+};
+
+struct mycel_problem {
+  mycel_ctx* ctx = nullptr;
+  mycel::GridDims g{};
+  float h = 1.0f;
+  double e0 = 1, nu = 0.3, emin_ratio = 1e-6, emin = 1e-6, penal = 3.0;
+  mycel::KeD ke{};
+  mycel::KeF kef{};
+  double diag_ke[24];
+  int64_t n_active = 0, n_active_nodes = 0, n_active_fixed = 0;
+  std::vector<int32_t> fixed_host;        // FixedDofs as given (may repeat)
+  std::vector<int32_t> load_nodes_host;   // union of load patch nodes (hinge shell)
+  std::vector<double> forces_host;        // AssembleForces result (box DOF vector)
+  int assemble_status = 0;
+  std::string assemble_msg;
+  // device arrays
+  uint8_t* d_domain = nullptr;    // [ne]
+  uint8_t* d_nflags = nullptr;    // [nn]
+  int32_t* d_fixed = nullptr;     // FixedDofs as given
+  int32_t* d_active = nullptr;    // [n_active] ascending box element index
+  int32_t* d_e2a = nullptr;       // [ne] active index or -1
+  double* d_F = nullptr;          // [nd] nodal forces
+  double* d_b = nullptr;          // [nd] P F
+  int32_t* d_fnz = nullptr;       // indices i with F[i] != 0, ascending
+  int32_t n_fnz = 0;
+  int32_t* d_bnz = nullptr;       // indices with b[i] != 0, ascending
+  int32_t n_bnz = 0;
+  double* d_rho_box = nullptr;    // [ne] FeModel.ElementDensity
+  double* d_E = nullptr;          // [ne] E_e (active elements)
+  float* d_Ef = nullptr;          // [ne] FP32 copy
+  double* d_diag = nullptr;       // [nd] DiagA
+  double* d_invd = nullptr;       // [nd] Jacobi inverse diagonal
+  float* d_invdf = nullptr;       // [nd] FP32 copy
+  // PCG workspace (FP64)
+  double *d_r = nullptr, *d_z = nullptr, *d_p = nullptr, *d_ap = nullptr, *d_x = nullptr;
+  double* d_part = nullptr;       // [2*nblocks] partial sums
+  mycel::PcgState* d_state = nullptr;
+  // mixed-form workspace
+  float *f_x = nullptr, *f_r = nullptr, *f_z = nullptr, *f_p0 = nullptr, *f_p1 = nullptr, *f_ap = nullptr;
+  double* d_r64 = nullptr;        // refinement residual
+  double* d_part2 = nullptr;      // [many] FP64 partials for mixed dots
+  int64_t n_part2 = 0;
+  int64_t device_bytes = 0;
+  // scratch for API calls
+  double* d_tmp0 = nullptr;       // [nd]
+  double* d_tmp1 = nullptr;       // [nd]
+  int lane_mode = 0;
+  cudaGraphExec_t pcg_graph = nullptr;
+  int pcg_graph_chunk = 0;
+  cudaGraphExec_t pcg32_graph = nullptr;
+  int pcg32_graph_chunk = 0;
+  int pcg32_graph_parity = -1;
+};
+
+struct mycel_filter {
+  mycel_problem* p = nullptr;
+  double rmin = 1.5;
+  int n_off = 0;
+  int4* d_off = nullptr;        // (dx, dy, dz, unused) in the reference's loop order
+  double* d_w = nullptr;        // rmin - dist per offset
+  double* d_invhs = nullptr;    // [ne]
+  double* d_s = nullptr;        // [ne]
+};
+
+namespace mycel {
+
+// ---- error plumbing ----
+int32_t set_error(mycel_ctx* ctx, int32_t code, const std::string& msg);
+#define MYCEL_CUDA(ctx, call)                                                                      \
+  do {                                                                                             \
+    cudaError_t e_ = (call);                                                                       \
+    if (e_ != cudaSuccess)                                                                         \
+      return ::mycel::set_error((ctx), MYCEL_E_DEVICE, std::string(#call ": ") + cudaGetErrorString(e_)); \
+  } while (0)
+
+// ---- host setup ----
+void build_ke(double h, double nu, double* ke);  // Hex8Element.CreateKe semantics
+int64_t num_blocks8192(int64_t n);
+
+// ---- FP64 plain-path launchers (fp64_kernels.cu, compiled with -fmad=false) ----
+void launch_setup_nodes(mycel_problem* p, const int32_t* d_fixed, int32_t n_fixed, int32_t* d_count);
+void launch_update_E(mycel_problem* p, const double* d_rho_box, double penal);
+void launch_diag(mycel_problem* p);
+void launch_matvec64(mycel_problem* p, const double* x, double* y, int projected, const int* d_status);
+void launch_project_x(mycel_problem* p, double* x, int* d_flag);
+void launch_pcg_bnorm(mycel_problem* p);
+void launch_pcg_init_r(mycel_problem* p, int nonzero);
+void launch_pcg_dot_rr(mycel_problem* p);
+void launch_pcg_init_z(mycel_problem* p);
+void launch_pcg_iteration(mycel_problem* p);
+void launch_compliance(mycel_problem* p, const double* u, double* d_out);
+void launch_max_disp(mycel_problem* p, const double* u, double* d_out);
+void launch_reactions(mycel_problem* p, const double* ku, double* out, const int32_t* d_fixed, int32_t n_fixed);
+void launch_von_mises(mycel_problem* p, const double* u, double* vm);
+void launch_scatter_active(mycel_problem* p, const double* src_active, double* dst_box, double fill);
+void launch_gather_active(mycel_problem* p, const double* src_box, double* dst_active);
+
+// filter
+int filter_setup(mycel_filter* f);
+void launch_filter_fwd(mycel_filter* f, const double* in_box, double* out_box);
+void launch_filter_adj(mycel_filter* f, const double* in_box, double* out_box);
+void launch_sens(mycel_problem* p, const double* u, const double* rho_box, double penal, double* dc_box);
+
+// OC (persistent cooperative kernel); returns 0 or MYCEL_E_TIMEOUT / MYCEL_E_DEVICE
+struct OcParams {
+  double f, move, rho_min, lambda_guess, vol_tol;
+  int max_bisect;
+  int heaviside;
+};
+struct OcOut {
+  double lambda;
+  double max_change;
+  double vol_sum;
+  double grey_sum;
+  int err;
+  int trials;
+};
+int launch_oc(mycel_ctx* ctx, int64_t n, const int32_t* d_index /*box index of element i or null*/,
+              const double* rho, const double* dc, const double* s, const uint8_t* passive, double* rho_new,
+              const double* rho_phys_for_metrics, const double* rho_tilde_for_grey, const OcParams& prm,
+              double* d_scratch, OcOut* d_out);
+
+// ---- mixed form (fp32_kernels.cu) ----
+void launch_E_to_f32(mycel_problem* p);
+void launch_matvec32(mycel_problem* p, const float* x, float* y, int projected);
+void mixed_apply_k_f64io(mycel_problem* p, const double* x, double* y, int projected);
+int32_t mixed_solve_entry(mycel_problem* p, const double* d_b, const int32_t* d_nz, int32_t n_nz, double* d_u,
+                          double tol, int max_iter, const volatile int32_t* cancel, mycel_pcg_result* res);
+
+// ---- drivers (api.cu) ----
+int32_t pcg_solve_fp64(mycel_problem* p, const double* d_b, const int32_t* d_nz, int32_t n_nz, double* d_x,
+                       double tol, int max_iter, const volatile int32_t* cancel, mycel_pcg_result* res);
+int32_t solve_dispatch(mycel_problem* p, double* d_u, double tol, int max_iter, int precision,
+                       const volatile int32_t* cancel, mycel_pcg_result* res);
+int32_t ensure_pcg_workspace(mycel_problem* p);
+
+}  // namespace mycel

@@ -1,0 +1,444 @@
+// SIMP loop: TopologyOptimizer.Run (src/Mycel.Core/Optimization/TopologyOptimizer.cs:16-407) with the design
+// state resident on the device. Per iteration: filter -> (Heaviside) -> E/DiagA -> tolerance schedule -> warm
+// PCG -> compliance, max |u| -> sensitivities -> adjoint filter -> OC bisection -> metrics. Only scalars (and
+// requested snapshots) cross PCIe.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <deque>
+#include <string>
+#include <thread>
+#include <unordered_set>
+#include <vector>
+
+#include "internal.h"
+
+using namespace mycel;
+
+struct mycel_simp_session {
+  mycel_problem* p = nullptr;
+  mycel_simp_options o{};
+  mycel_filter* filt = nullptr;
+  double rmin = 1.5;
+  std::vector<std::string> warnings;
+  double *d_rho = nullptr, *d_rho_new = nullptr, *d_rt = nullptr, *d_rb = nullptr, *d_dcb = nullptr,
+         *d_dct = nullptr, *d_dc = nullptr, *d_u = nullptr, *d_scal = nullptr, *d_oc_scr = nullptr;
+  OcOut* d_oc = nullptr;
+  uint8_t* d_pas = nullptr;
+  float *d_phys_f = nullptr, *d_des_f = nullptr;
+  int iter = 1, start = 1, maxit = 200;
+  double lambda = 1.0, max_change = 1.0, beta = 1.0;
+  std::deque<double> chist;
+  bool converged = false, done = false;
+  int count = 0;
+  cudaEvent_t ev[5] = {};
+  std::vector<float> h_phys, h_des;
+};
+
+namespace {
+
+__global__ void k_heaviside_project(int64_t na, const int32_t* __restrict__ act, const double* __restrict__ rt,
+                                    double* __restrict__ rb, double beta, double eta) {
+  // HeavisideProjection.Project (HeavisideProjection.cs:12-24)
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= na) return;
+  int32_t e = act[t];
+  double den = tanh(beta * eta) + tanh(beta * (1.0 - eta));
+  double inv = 1.0 / den;
+  double tbe = tanh(beta * eta);
+  double v = (tbe + tanh(beta * (rt[e] - eta))) * inv;
+  rb[e] = v < 0.0 ? 0.0 : (v > 1.0 ? 1.0 : v);
+}
+
+__global__ void k_heaviside_chain(int64_t na, const int32_t* __restrict__ act, const double* __restrict__ rt,
+                                  const double* __restrict__ dcb, double* __restrict__ dct, double beta, double eta) {
+  // HeavisideProjection.Derivative (:26-37) times dc/drhoBar (TopologyOptimizer.cs:283-287)
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= na) return;
+  int32_t e = act[t];
+  double den = tanh(beta * eta) + tanh(beta * (1.0 - eta));
+  double inv = 1.0 / den;
+  double th = tanh(beta * (rt[e] - eta));
+  double d = beta * (1.0 - th * th) * inv;
+  d = d > 1e-12 ? d : 1e-12;
+  dct[e] = dcb[e] * d;
+}
+
+__global__ void k_snapshot(int64_t ne, const uint8_t* __restrict__ dom, const double* __restrict__ rb,
+                           const double* __restrict__ rho, float* __restrict__ pf, float* __restrict__ df) {
+  int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= ne) return;
+  bool a = dom[e] != 0;
+  pf[e] = a ? (float)rb[e] : 0.0f;
+  df[e] = a ? (float)rho[e] : 0.0f;
+}
+
+template <class T>
+cudaError_t salloc(mycel_simp_session* s, T** ptr, size_t count) {
+  size_t bytes = std::max<size_t>(sizeof(T) * count, 16);
+  cudaError_t e = cudaMalloc((void**)ptr, bytes);
+  if (e == cudaSuccess) s->p->device_bytes += (int64_t)bytes;
+  return e;
+}
+
+double clampd(double v, double lo, double hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+}  // namespace
+
+extern "C" int32_t mycel_simp_end(mycel_simp_session* s);
+
+extern "C" int32_t mycel_simp_begin(mycel_problem* p, const mycel_simp_options* opt, mycel_simp_session** out) {
+  if (!p || !opt || !out) return set_error(p ? p->ctx : nullptr, MYCEL_E_ARG, "NULL argument");
+  *out = nullptr;
+  mycel_ctx* c = p->ctx;
+  cudaSetDevice(c->device);
+  cudaStream_t st = c->stream;
+  const GridDims& g = p->g;
+  mycel_simp_session* s = new mycel_simp_session();
+  s->p = p;
+  s->o = *opt;
+  const mycel_simp_options& o = s->o;
+  // filter radius in voxels (TopologyOptimizer.cs:28-39)
+  double h = (double)p->h;
+  s->rmin = o.filter_radius_mm / h;
+  if (s->rmin < 1.5) {
+    char buf[160];
+    std::snprintf(buf, sizeof buf, "Filter radius %.2f mm (%.2f voxels) is below 1.5h (%.2f mm).", o.filter_radius_mm,
+                  s->rmin, 1.5 * h);
+    s->warnings.push_back(buf);
+    if (o.enforce_minimum_filter_radius) s->rmin = 1.5;
+  }
+  if (p->assemble_status) {
+    int32_t code = p->assemble_status;
+    std::string m = p->assemble_msg;
+    delete s;
+    return set_error(c, code, m);
+  }
+  // passive mask (TopologyOptimizer.cs:45-84): option mask and hinge shell PassiveRegion.Build(r = 1)
+  std::vector<uint8_t> pas((size_t)g.ne, 0);
+  std::vector<uint8_t> dom((size_t)g.ne);
+  cudaMemcpyAsync(dom.data(), p->d_domain, g.ne, cudaMemcpyDeviceToHost, st);
+  cudaStreamSynchronize(st);
+  if (o.passive_mask)
+    for (int64_t e = 0; e < g.ne; ++e)
+      if (dom[e] && e < o.passive_mask_len && o.passive_mask[e] != 0) pas[e] = 1;
+  if (o.protect_boundary_hinges) {
+    std::vector<int32_t> nodes(p->load_nodes_host);
+    std::unordered_set<int32_t> seen(nodes.begin(), nodes.end());
+    for (int32_t d : p->fixed_host)
+      if (seen.insert(d / 3).second) nodes.push_back(d / 3);
+    for (int32_t n : nodes) {
+      int64_t nx1 = g.nx1, ny1 = g.ny1;
+      int nk = (int)(n / (nx1 * ny1));
+      int64_t rem = n % (nx1 * ny1);
+      int nj = (int)(rem / nx1), ni = (int)(rem % nx1);
+      auto cl = [](int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); };
+      int x0 = cl(ni - 1, 0, g.nx - 1), x1 = cl(ni, 0, g.nx - 1);
+      int y0 = cl(nj - 1, 0, g.ny - 1), y1 = cl(nj, 0, g.ny - 1);
+      int z0 = cl(nk - 1, 0, g.nz - 1), z1 = cl(nk, 0, g.nz - 1);
+      for (int iz = z0; iz <= z1; ++iz)
+        for (int iy = y0; iy <= y1; ++iy)
+          for (int ix = x0; ix <= x1; ++ix) {
+            int64_t e = ix + (int64_t)g.nx * (iy + (int64_t)g.ny * iz);
+            if (dom[e]) pas[e] = 1;
+          }
+    }
+  }
+  // initial design (TopologyOptimizer.cs:90-122)
+  std::vector<double> rho((size_t)g.ne, 0.0);
+  if (o.initial_density) {
+    if (o.initial_density_len == g.ne) {
+      for (int64_t e = 0; e < g.ne; ++e)
+        if (dom[e]) rho[e] = (double)o.initial_density[e];
+    } else if (o.initial_density_len == p->n_active) {
+      int64_t i = 0;
+      for (int64_t e = 0; e < g.ne; ++e)
+        if (dom[e]) rho[e] = (double)o.initial_density[i++];
+    } else {
+      delete s;
+      return set_error(c, MYCEL_E_ARG, "InitialDensity length (" + std::to_string(o.initial_density_len) +
+                                           ") must match either TotalElements (" + std::to_string(g.ne) +
+                                           ") or ActiveElementCount (" + std::to_string(p->n_active) + ").");
+    }
+  } else {
+    for (int64_t e = 0; e < g.ne; ++e)
+      if (dom[e]) rho[e] = pas[e] ? 1.0 : o.volume_fraction;
+  }
+  for (int64_t e = 0; e < g.ne; ++e)
+    if (pas[e]) rho[e] = 1.0;
+  int32_t rc = ensure_pcg_workspace(p);
+  if (rc) {
+    delete s;
+    return rc;
+  }
+  bool ok = !salloc(s, &s->d_rho, g.ne) && !salloc(s, &s->d_rho_new, g.ne) && !salloc(s, &s->d_rt, g.ne) &&
+            !salloc(s, &s->d_dcb, g.ne) && !salloc(s, &s->d_dc, g.ne) && !salloc(s, &s->d_u, g.nd) &&
+            !salloc(s, &s->d_scal, 16) && !salloc(s, &s->d_oc_scr, (size_t)c->num_sms * 2 * 8 + 64) &&
+            !salloc(s, &s->d_oc, 1) && !salloc(s, &s->d_pas, g.ne) && !salloc(s, &s->d_phys_f, g.ne) &&
+            !salloc(s, &s->d_des_f, g.ne);
+  if (ok && o.enable_heaviside) ok = !salloc(s, &s->d_rb, g.ne) && !salloc(s, &s->d_dct, g.ne);
+  if (!ok) {
+    mycel_simp_end(s);
+    return set_error(c, MYCEL_E_OOM, "out of device memory for the SIMP state");
+  }
+  if (!o.enable_heaviside) s->d_rb = s->d_rt;
+  cudaMemcpyAsync(s->d_rho, rho.data(), sizeof(double) * g.ne, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(s->d_rho_new, rho.data(), sizeof(double) * g.ne, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(s->d_pas, pas.data(), g.ne, cudaMemcpyHostToDevice, st);
+  cudaMemsetAsync(s->d_rt, 0, sizeof(double) * g.ne, st);
+  cudaMemsetAsync(s->d_dcb, 0, sizeof(double) * g.ne, st);
+  cudaMemsetAsync(s->d_dc, 0, sizeof(double) * g.ne, st);
+  if (o.warm_start_displacements && o.warm_start_len == g.nd)
+    cudaMemcpyAsync(s->d_u, o.warm_start_displacements, sizeof(double) * g.nd, cudaMemcpyHostToDevice, st);
+  else
+    cudaMemsetAsync(s->d_u, 0, sizeof(double) * g.nd, st);
+  for (auto& e : s->ev) cudaEventCreate(&e);
+  rc = mycel_filter_create(p, s->rmin, &s->filt);
+  if (rc) {
+    mycel_simp_end(s);
+    return rc;
+  }
+  s->start = s->iter = o.start_iteration;
+  s->maxit = o.max_iterations;
+  s->done = s->iter > s->maxit;
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    mycel_simp_end(s);
+    return set_error(c, MYCEL_E_DEVICE, std::string("SIMP set-up: ") + cudaGetErrorString(e));
+  }
+  // initial options' pointers are not kept beyond begin
+  s->o.passive_mask = nullptr;
+  s->o.initial_density = nullptr;
+  s->o.warm_start_displacements = nullptr;
+  *out = s;
+  return MYCEL_OK;
+}
+
+static int32_t simp_step_impl(mycel_simp_session* s, mycel_iter_record* rec, int32_t* done,
+                              const volatile int32_t* cancel) {
+  mycel_problem* p = s->p;
+  mycel_ctx* c = p->ctx;
+  cudaSetDevice(c->device);
+  cudaStream_t st = c->stream;
+  const mycel_simp_options& o = s->o;
+  if (done) *done = s->done ? 1 : 0;
+  if (s->done) return MYCEL_OK;
+  const int iter = s->iter;
+  auto t0 = std::chrono::steady_clock::now();
+  // 1. penalisation continuation (:176-183)
+  double penal = o.penal;
+  if (o.continuation) penal = iter < 20 ? 1.0 : (iter < 40 ? 2.0 : o.penal);
+  cudaEventRecord(s->ev[0], st);
+  // 2. filter (:191-202); passive elements are kept at 1 by the OC kernel and the initial design
+  launch_filter_fwd(s->filt, s->d_rho, s->d_rt);
+  if (o.enable_heaviside) {
+    k_heaviside_project<<<(unsigned)((p->n_active + 255) / 256), 256, 0, st>>>(p->n_active, p->d_active, s->d_rt,
+                                                                              s->d_rb, s->beta, 0.5);
+    c->launches++;
+  }
+  cudaEventRecord(s->ev[1], st);
+  // E_e and DiagA from the physical densities (:204-209)
+  launch_update_E(p, s->d_rb, penal);
+  launch_diag(p);
+  // 3. solver tolerance schedule (:211-224): host scalar control, glibc log10/pow as Math.Log10/Math.Pow
+  double tol;
+  if (iter == s->start) {
+    tol = o.solver_tolerance_initial;
+  } else {
+    double ta = clampd((s->max_change - 0.01) / 0.09, 0.0, 1.0);
+    double li = std::log10(std::max(o.solver_tolerance_initial, 1e-15));
+    double lf = std::log10(std::max(o.solver_tolerance_final, 1e-15));
+    double lt = lf + ta * (li - lf);
+    tol = std::pow(10.0, lt);
+  }
+  // 4. warm-started PCG (:226-253)
+  mycel_pcg_result pr;
+  int32_t rc = solve_dispatch(p, s->d_u, tol, o.solver_max_iterations, o.precision, cancel, &pr);
+  if (rc) return rc;
+  cudaEventRecord(s->ev[2], st);
+  if (!pr.converged)
+    return set_error(c, MYCEL_E_NOT_CONVERGED,
+                     "FEM solver did not converge in " + std::to_string(pr.iterations) + " iterations (" + pr.message +
+                         "). Is the model not sufficiently constrained?");
+  // compliance and max |u| (:255-276)
+  launch_compliance(p, s->d_u, s->d_scal);
+  launch_max_disp(p, s->d_u, s->d_scal + 1);
+  // 5. sensitivities and adjoint filter (:278-294)
+  launch_sens(p, s->d_u, s->d_rb, penal, s->d_dcb);
+  if (o.enable_heaviside) {
+    k_heaviside_chain<<<(unsigned)((p->n_active + 255) / 256), 256, 0, st>>>(p->n_active, p->d_active, s->d_rt,
+                                                                            s->d_dcb, s->d_dct, s->beta, 0.5);
+    c->launches++;
+    launch_filter_adj(s->filt, s->d_dct, s->d_dc);
+  } else {
+    launch_filter_adj(s->filt, s->d_dcb, s->d_dc);
+  }
+  cudaEventRecord(s->ev[3], st);
+  // 6. OC update with lambda carried over (:296-311) + metrics (:322-338)
+  OcParams prm{o.volume_fraction, o.move_limit, o.rho_min, s->lambda, 1e-8, 60, o.enable_heaviside};
+  rc = launch_oc(c, p->n_active, p->d_active, s->d_rho, s->d_dc, s->filt->d_s, s->d_pas, s->d_rho_new, s->d_rb,
+                 o.enable_heaviside ? s->d_rt : s->d_rb, prm, s->d_oc_scr, s->d_oc);
+  if (rc) return set_error(c, rc, "OC kernel launch failed");
+  cudaEventRecord(s->ev[4], st);
+  double* hsc = (double*)c->pinned;
+  OcOut* ho = (OcOut*)((char*)c->pinned + 64);
+  MYCEL_CUDA(c, cudaMemcpyAsync(hsc, s->d_scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  MYCEL_CUDA(c, cudaMemcpyAsync(ho, s->d_oc, sizeof(OcOut), cudaMemcpyDeviceToHost, st));
+  MYCEL_CUDA(c, cudaStreamSynchronize(st));
+  if (ho->trials == 0) return set_error(c, MYCEL_E_TIMEOUT, "OC grid barrier timed out");
+  std::swap(s->d_rho, s->d_rho_new);
+  s->lambda = ho->lambda;
+  if (o.enable_heaviside && iter % 25 == 0 && s->beta < 8.0) s->beta = std::min(8.0, s->beta * 2.0);
+  s->max_change = ho->max_change;
+  double na = (double)p->n_active;
+  mycel_iter_record r{};
+  r.iteration = iter;
+  r.compliance = hsc[0];
+  r.volume_fraction = ho->vol_sum / na;
+  r.max_change = ho->max_change;
+  r.grey_level = (4.0 * ho->grey_sum / na) * 100.0;
+  r.solver_iterations = pr.iterations;
+  r.solver_residual = pr.final_residual;
+  r.max_displacement = hsc[1];
+  r.refinement_steps = pr.refinement_steps;
+  float ms = 0;
+  cudaEventElapsedTime(&ms, s->ev[0], s->ev[1]);
+  r.filter_ms = ms;
+  r.solve_ms = pr.elapsed_ms;
+  cudaEventElapsedTime(&ms, s->ev[2], s->ev[3]);
+  r.sensitivity_ms = ms;
+  cudaEventElapsedTime(&ms, s->ev[3], s->ev[4]);
+  r.update_ms = ms;
+  r.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  if (rec) *rec = r;
+  s->count++;
+  // stop rule (:374-390)
+  s->chist.push_back(r.compliance);
+  if (s->chist.size() > 6) s->chist.pop_front();
+  if (s->chist.size() == 6) {
+    double rel = std::fabs(r.compliance - s->chist.front()) / r.compliance;
+    if (s->max_change < 0.01 && rel < 1e-3) {
+      s->converged = true;
+      s->done = true;
+    }
+  }
+  s->iter++;
+  if (s->iter > s->maxit) s->done = true;
+  if (done) *done = s->done ? 1 : 0;
+  return MYCEL_OK;
+}
+
+extern "C" int32_t mycel_simp_step(mycel_simp_session* s, mycel_iter_record* rec, int32_t* done) {
+  if (!s) return set_error(nullptr, MYCEL_E_ARG, "NULL session");
+  return simp_step_impl(s, rec, done, nullptr);
+}
+
+static int32_t snapshot(mycel_simp_session* s) {
+  mycel_problem* p = s->p;
+  cudaStream_t st = p->ctx->stream;
+  k_snapshot<<<(unsigned)((p->g.ne + 255) / 256), 256, 0, st>>>(p->g.ne, p->d_domain, s->d_rb, s->d_rho, s->d_phys_f,
+                                                                 s->d_des_f);
+  p->ctx->launches++;
+  return MYCEL_OK;
+}
+
+extern "C" int32_t mycel_simp_read(mycel_simp_session* s, double* u, float* phys, float* des, double* rpa,
+                                   double* rda, double* lambda) {
+  if (!s) return set_error(nullptr, MYCEL_E_ARG, "NULL session");
+  mycel_problem* p = s->p;
+  mycel_ctx* c = p->ctx;
+  cudaSetDevice(c->device);
+  cudaStream_t st = c->stream;
+  if (phys || des) {
+    snapshot(s);
+    if (phys) MYCEL_CUDA(c, cudaMemcpyAsync(phys, s->d_phys_f, sizeof(float) * p->g.ne, cudaMemcpyDeviceToHost, st));
+    if (des) MYCEL_CUDA(c, cudaMemcpyAsync(des, s->d_des_f, sizeof(float) * p->g.ne, cudaMemcpyDeviceToHost, st));
+  }
+  if (u) MYCEL_CUDA(c, cudaMemcpyAsync(u, s->d_u, sizeof(double) * p->g.nd, cudaMemcpyDeviceToHost, st));
+  if (rpa) {
+    launch_gather_active(p, s->d_rb, p->d_tmp0);
+    MYCEL_CUDA(c, cudaMemcpyAsync(rpa, p->d_tmp0, sizeof(double) * p->n_active, cudaMemcpyDeviceToHost, st));
+    MYCEL_CUDA(c, cudaStreamSynchronize(st));
+  }
+  if (rda) {
+    launch_gather_active(p, s->d_rho, p->d_tmp1);
+    MYCEL_CUDA(c, cudaMemcpyAsync(rda, p->d_tmp1, sizeof(double) * p->n_active, cudaMemcpyDeviceToHost, st));
+  }
+  MYCEL_CUDA(c, cudaStreamSynchronize(st));
+  if (lambda) *lambda = s->lambda;
+  return MYCEL_OK;
+}
+
+extern "C" int32_t mycel_simp_end(mycel_simp_session* s) {
+  if (!s) return MYCEL_OK;
+  cudaSetDevice(s->p->ctx->device);
+  cudaStreamSynchronize(s->p->ctx->stream);
+  if (s->filt) mycel_filter_destroy(s->filt);
+  double* dptr[] = {s->d_rho, s->d_rho_new, s->d_rt, s->d_dcb, s->d_dc, s->d_u, s->d_scal, s->d_oc_scr};
+  for (double* q : dptr)
+    if (q) cudaFree(q);
+  if (s->o.enable_heaviside) {
+    if (s->d_rb) cudaFree(s->d_rb);
+    if (s->d_dct) cudaFree(s->d_dct);
+  }
+  if (s->d_oc) cudaFree(s->d_oc);
+  if (s->d_pas) cudaFree(s->d_pas);
+  if (s->d_phys_f) cudaFree(s->d_phys_f);
+  if (s->d_des_f) cudaFree(s->d_des_f);
+  for (auto& e : s->ev)
+    if (e) cudaEventDestroy(e);
+  delete s;
+  return MYCEL_OK;
+}
+
+extern "C" int32_t mycel_simp_run(mycel_problem* p, const mycel_simp_options* opt, mycel_progress_fn progress,
+                                  void* user, const volatile int32_t* cancel, const volatile int32_t* pause,
+                                  mycel_iter_record* history, int32_t cap, int32_t* n_iters, int32_t* converged,
+                                  double* u_out, float* phys_out, float* des_out) {
+  if (n_iters) *n_iters = 0;
+  if (converged) *converged = 0;
+  mycel_simp_session* s = nullptr;
+  int32_t rc = mycel_simp_begin(p, opt, &s);
+  if (rc) return rc;
+  mycel_ctx* c = p->ctx;
+  if (progress) {
+    s->h_phys.resize((size_t)p->g.ne);
+    s->h_des.resize((size_t)p->g.ne);
+  }
+  int32_t err = MYCEL_OK;
+  while (!s->done) {
+    // IterationController.CheckAndBlock / CancellationToken (:168-172)
+    if (cancel && *cancel) break;
+    while (pause && *pause && !(cancel && *cancel)) std::this_thread::sleep_for(std::chrono::milliseconds(1));
+    if (cancel && *cancel) break;
+    mycel_iter_record r;
+    int32_t d = 0;
+    err = simp_step_impl(s, &r, &d, cancel);
+    if (err == MYCEL_E_CANCELLED) {
+      err = MYCEL_OK;
+      break;
+    }
+    if (err) break;
+    if (history && s->count - 1 < cap) history[s->count - 1] = r;
+    if (progress) {
+      snapshot(s);
+      cudaMemcpyAsync(s->h_phys.data(), s->d_phys_f, sizeof(float) * p->g.ne, cudaMemcpyDeviceToHost, c->stream);
+      cudaMemcpyAsync(s->h_des.data(), s->d_des_f, sizeof(float) * p->g.ne, cudaMemcpyDeviceToHost, c->stream);
+      cudaStreamSynchronize(c->stream);
+      progress(user, &r, s->h_phys.data(), s->h_des.data());
+    }
+  }
+  if (n_iters) *n_iters = s->count;
+  if (converged) *converged = s->converged ? 1 : 0;
+  std::string msg = c->last_error;
+  if (s->count > 0 || !err) {
+    int32_t rr = mycel_simp_read(s, u_out, phys_out, des_out, nullptr, nullptr, nullptr);
+    if (!err) err = rr;
+  }
+  mycel_simp_end(s);
+  if (err) c->last_error = msg;
+  return err;
+}
