@@ -1,0 +1,361 @@
+#!/usr/bin/env python
+"""SIMP iterations/s of the mixed-precision path on the 192x96x96 bridge (1,769,472 Hex8 elements, 5.4M DOFs).
+
+One step = one SIMP iteration (filter, E/DiagA, warm-started PCG to the tolerance, compliance, sensitivities,
+adjoint filter, OC bisection) on the device-resident state. Prints one JSON line.
+
+  value      SIMP iter/s with the state resident in HBM (CUDA events on the library's stream, max over ranks)
+  e2e        the same metric for a whole job through the C ABI from host buffers: problem upload, W+K
+             iterations each followed by the density snapshot read-back (what the App consumes), final u
+  roofline   the FP32 stiffness matvec (the dominant kernel), timed live by events captured in the PCG graph
+  fp64       the plain FP64 path (bit-exact drop-in) on the same workload, and the mixed-vs-FP64 compliance error
+  cpu_baseline  the CPU oracle (C++ restatement, all host threads) on a bounded sample of the same iteration
+
+--impl reference runs only the CPU restatement of the reference path (rank 0) on the same workload.
+Multi-GPU (torchrun): each rank runs its own replica of the workload (no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# PCG iterations per SIMP iteration of the plain FP64 path on this workload (iterations 4-13, measured on B200;
+# the FP64 path reproduces the reference's iteration counts bit for bit). Used only to scale the CPU sample.
+FP64_PCG_PER_SIMP_ITER = None
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="mycel", choices=["mycel", "reference"])
+    ap.add_argument("--workload", default="bridge_192x96x96", choices=["bridge_192x96x96", "cantilever_40x20x10"])
+    ap.add_argument("--fp64-steps", type=int, default=2)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-sample-iters", type=int, default=6)
+    return ap.parse_args()
+
+
+def workload(name):
+    from mycel_b200 import workloads as W
+    if name == "bridge_192x96x96":
+        m, o = W.bridge_192x96x96()
+    else:
+        m, o = W.simp_cantilever_40x20x10()
+    return m, o
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(ws, v):
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class Clocks:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            if len(r) < 9:
+                continue
+            for k, nm in enumerate(names):
+                if "Active" in r[5 + k] and "Not" not in r[5 + k]:
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return None
+
+
+def matvec_bytes_fp32(model):
+    """Algorithmic bytes of one fused FP32 matvec launch of the inner PCG: read z and p_{t-1}, write p_t and
+    K p_t (4 x 12 B per node), E and the domain byte per element (5 B), the node flag byte (1 B)."""
+    nn = model.total_nodes
+    ne = model.total_elements
+    return 48 * nn + 5 * ne + nn
+
+
+def run_mycel(args):
+    import torch
+    from mycel_b200 import api
+    ws, rank, local = dist_init()
+    ctx = api.Context(local)
+    model, opts = workload(args.workload)
+    mixed = opts.replace(precision="mixed")
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
+
+    # ---------------- value: device-resident SIMP iterations ----------------
+    prob = api.Problem(model, ctx)
+    sess = api.SimpSession(prob, mixed)
+    for _ in range(args.warmup):
+        sess.step()
+    launches0 = ctx.launch_count
+    ctx.set_profiling(True)
+    clocks = Clocks(local)
+    barrier(ws)
+    torch.cuda.synchronize(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    recs = [sess.step() for _ in range(args.steps)]
+    e1.record(stream)
+    torch.cuda.synchronize(local)
+    clk = clocks.stop()
+    barrier(ws)
+    t_ms = e0.elapsed_time(e1)
+    timing = ctx.kernel_timing(0)
+    ctx.set_profiling(False)
+    gpu_launches = ctx.launch_count - launches0
+    t_max = max_over_ranks(ws, t_ms)
+    value = ws * args.steps / (t_max / 1000.0)
+    pcg_inner = [r.solver_iterations for r in recs]
+    comp_mixed = [r.compliance for r in recs]
+    sess.close()
+    prob.close()
+
+    # ---------------- roofline of the FP32 matvec ----------------
+    pk = peaks()
+    per_launch_ms = timing["total_ms"] / max(1, timing["launches"])
+    mv_bytes = matvec_bytes_fp32(model)
+    achieved = mv_bytes / (per_launch_ms / 1000.0) / 1e9 if timing["launches"] else None
+    hbm = (pk or {}).get("hbm_gbs") or 6650.0
+    roof = {"kernel": "k_mv32 (FP32 Hex8 K.p, fused p update + p.Ap partials)", "bound": "hbm",
+            "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "frac": (achieved / hbm) if achieved else None, "traffic": None,
+            "peak_source": "measured" if pk else "fallback", "avg_launch_us": per_launch_ms * 1000.0,
+            "timed_launches": timing["launches"], "algorithmic_bytes_per_launch": mv_bytes,
+            "flops_per_launch": 1152 * model.active_element_count,
+            "tflops": 1152 * model.active_element_count / (per_launch_ms / 1000.0) / 1e12 if timing["launches"] else None}
+
+    out = {"metric": "SIMP iter/s (mixed FP32-inner/FP64-refined, 192x96x96 bridge)", "value": value,
+           "unit": "SIMP iter/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f32 inner PCG + f64 refinement/reductions", "data": "synthetic",
+           "config": {"workload": args.workload, "elements": model.total_elements, "dofs": model.total_dofs,
+                      "precision": "mixed", "volfrac": opts.volume_fraction, "rmin": opts.filter_radius_mm,
+                      "penal": opts.penal, "emin_ratio": model.material.emin_ratio,
+                      "pcg_tol": opts.solver_tolerance_final, "inputs_vs_l2": "inputs > L2 (126 MB); no flush",
+                      "parallelism": f"replicas x{ws}"},
+           "roofline": roof, "gpu_launches": gpu_launches, "clocks": clk,
+           "pcg_inner_iters_per_step": pcg_inner, "compliance_mixed": comp_mixed}
+
+    # ---------------- plain FP64 path on the same iterations ----------------
+    if args.fp64_steps > 0 and rank == 0:
+        prob = api.Problem(model, ctx)
+        sess = api.SimpSession(prob, opts.replace(precision="fp64"))
+        ctx.set_profiling(True)
+        f_recs = []
+        t64 = []
+        for i in range(args.warmup + args.fp64_steps):
+            f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            f0.record(stream)
+            r = sess.step()
+            f1.record(stream)
+            torch.cuda.synchronize(local)
+            f_recs.append(r)
+            if i >= args.warmup:
+                t64.append(f0.elapsed_time(f1))
+        tm64 = ctx.kernel_timing(1)
+        ctx.set_profiling(False)
+        sess.close()
+        prob.close()
+        # compliance of the same iterations (1..W+fp64_steps) in the mixed run: rerun them from the start
+        prob = api.Problem(model, ctx)
+        sess = api.SimpSession(prob, mixed)
+        m_recs = [sess.step() for _ in range(args.warmup + args.fp64_steps)]
+        sess.close()
+        prob.close()
+        errs = [abs(a.compliance - b.compliance) / abs(b.compliance) for a, b in zip(m_recs, f_recs)]
+        per64 = tm64["total_ms"] / max(1, tm64["launches"])
+        out["fp64"] = {"simp_iter_s": 1000.0 * len(t64) / sum(t64) if t64 else None,
+                       "ms_per_step": statistics.mean(t64) if t64 else None,
+                       "pcg_iters_per_step": [r.solver_iterations for r in f_recs[args.warmup:]],
+                       "matvec_us": per64 * 1000.0,
+                       "matvec_gbs": (48 * model.total_nodes + 9 * model.total_elements) / (per64 / 1000.0) / 1e9 if tm64["launches"] else None,
+                       "mixed_vs_fp64_rel_compliance_err": errs, "max_rel_compliance_err": max(errs) if errs else None}
+        out["speedup_mixed_vs_fp64"] = (value / ws) / out["fp64"]["simp_iter_s"] if out["fp64"]["simp_iter_s"] else None
+
+    # ---------------- e2e: whole job through the C ABI from host buffers ----------------
+    if not args.no_e2e:
+        barrier(ws)
+        torch.cuda.synchronize(local)
+        n_it = args.warmup + args.steps
+        h2d = model.domain.nbytes + model.element_density.nbytes + model.fixed_dofs.nbytes + \
+            sum(lc.patch.nodes.nbytes + lc.patch.node_area.nbytes for lc in model.loads)
+        d2h_step = 2 * 4 * model.total_elements + 112
+        t0 = time.perf_counter()
+        prob = api.Problem(model, ctx)
+        sess = api.SimpSession(prob, mixed.replace(max_iterations=n_it))
+        for _ in range(n_it):
+            sess.step()
+            sess.read(u=False, densities=True)
+        final = sess.read(u=True, densities=False)
+        torch.cuda.synchronize(local)
+        t_e2e = time.perf_counter() - t0
+        sess.close()
+        prob.close()
+        t_e2e = max_over_ranks(ws, t_e2e)
+        out["e2e"] = {"value": ws * n_it / t_e2e, "unit": "SIMP iter/s",
+                      "h2d_bytes_per_step": int(h2d / n_it), "d2h_bytes_per_step": int(d2h_step + final["u"].nbytes / n_it),
+                      "iterations": n_it, "includes": "problem upload, set-up, W+K SIMP iterations from iteration 1, "
+                                                      "per-iteration float density snapshots, final u"}
+
+    # ---------------- CPU baseline (rank 0, bounded sample) ----------------
+    if rank == 0 and not args.no_cpu:
+        pcg_per_it = (statistics.mean(out["fp64"]["pcg_iters_per_step"]) if "fp64" in out else
+                      FP64_PCG_PER_SIMP_ITER or statistics.mean(pcg_inner))
+        out["cpu_baseline"] = cpu_sample(model, opts, pcg_per_it, args.cpu_sample_iters)
+
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def cpu_sample(model, opts, pcg_per_simp_iter, sample_iters):
+    """Oracle (C++ restatement, OpenMP over all host threads) on a bounded sample of one SIMP iteration:
+    the density filter, E/DiagA, `sample_iters` PCG iterations, sensitivities + adjoint filter, OC update.
+    One SIMP iteration is estimated as the non-PCG part + pcg_per_simp_iter * (time per PCG iteration)."""
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    O.set_modes(0, 0, threads=threads)
+    m = O.Model(model)
+    act = model.active_elements
+    t = time.perf_counter()
+    f = O.Filter(model.grid, model.domain, act, max(1.5, opts.filter_radius_mm / model.grid.h))
+    t_setup = time.perf_counter() - t
+    rho = np.full(act.size, opts.volume_fraction)
+    t = time.perf_counter()
+    rb = f.apply(rho)
+    dens = np.ones(model.total_elements)
+    dens[act] = rb
+    m.update_densities(dens, opts.penal)
+    t_filter = time.perf_counter() - t
+    b = m.forces() * (m.constrained() == 0)
+    t = time.perf_counter()
+    m.pcg_solve(b, tol=1e-30, max_iter=1)
+    t1 = time.perf_counter() - t
+    t = time.perf_counter()
+    u, res = m.pcg_solve(b, tol=1e-30, max_iter=1 + sample_iters)
+    t_pcg = (time.perf_counter() - t - t1) / sample_iters
+    t = time.perf_counter()
+    dcb = m.sensitivities(u, rb, opts.penal)
+    dc = f.adjoint(dcb)
+    t_sens = time.perf_counter() - t
+    t = time.perf_counter()
+    O.oc_update(rho, dc, f.s, None, opts.volume_fraction, opts.move_limit, opts.rho_min, 1.0)
+    t_oc = time.perf_counter() - t
+    t_iter = t_filter + t_sens + t_oc + pcg_per_simp_iter * t_pcg
+    return {"value": 1.0 / t_iter, "unit": "SIMP iter/s", "cores": threads, "kind": "port",
+            "sample": (f"oracle on the same workload: filter, E/DiagA, {sample_iters} PCG iterations "
+                       f"({t_pcg * 1e3:.1f} ms each), sensitivities + adjoint, OC; SIMP iteration = non-PCG part + "
+                       f"{pcg_per_simp_iter:.0f} PCG iterations (the FP64 path's count per iteration)"),
+            "pcg_iter_ms": t_pcg * 1e3, "filter_setup_s": t_setup}
+
+
+def run_reference(args):
+    ws, rank, local = dist_init()
+    if rank != 0:
+        return
+    model, opts = workload(args.workload)
+    pcg_per_it = FP64_PCG_PER_SIMP_ITER or 1000
+    vals = []
+    for i in range(args.warmup + args.steps):
+        t = time.perf_counter()
+        r = cpu_sample(model, opts, pcg_per_it, 2)
+        if i >= args.warmup:
+            vals.append(r["value"])
+    v = statistics.mean(vals)
+    out = {"impl": "reference", "metric": "SIMP iter/s (mixed FP32-inner/FP64-refined, 192x96x96 bridge)",
+           "value": v, "unit": "SIMP iter/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": args.workload},
+           "cpu_baseline": {"value": v, "unit": "SIMP iter/s", "cores": r["cores"], "kind": "port",
+                            "sample": r["sample"]},
+           "e2e": {"value": v, "unit": "SIMP iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_mycel(a)

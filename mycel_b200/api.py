@@ -65,6 +65,15 @@ class Context:
     def launch_count(self) -> int:
         return int(L.load().mycel_ctx_launch_count(self.handle))
 
+    def set_profiling(self, on: bool = True):
+        _check(L.load().mycel_ctx_set_profiling(self.handle, int(on)), self)
+
+    def kernel_timing(self, which: int = 0) -> dict:
+        ms, n, nodes, els = C.c_double(0), C.c_int64(0), C.c_int64(0), C.c_int64(0)
+        _check(L.load().mycel_ctx_kernel_timing(self.handle, which, C.byref(ms), C.byref(n), C.byref(nodes),
+                                                C.byref(els)), self)
+        return dict(total_ms=ms.value, launches=n.value, nodes=nodes.value, active_elements=els.value)
+
 
 _default_ctx = None
 _default_lock = threading.Lock()

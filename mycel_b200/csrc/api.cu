@@ -193,18 +193,37 @@ int32_t build_nz_list(mycel_problem* p, const double* d_bvec, int32_t* dst, int3
 const int kChunkIters = 16;
 
 int32_t capture_pcg_graph(mycel_problem* p) {
-  if (p->pcg_graph) return MYCEL_OK;
-  cudaStream_t s = p->ctx->stream;
-  cudaGraph_t graph;
-  int64_t before = p->ctx->launches;
-  MYCEL_CUDA(p->ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-  for (int i = 0; i < kChunkIters; ++i) launch_pcg_iteration(p);
-  MYCEL_CUDA(p->ctx, cudaStreamEndCapture(s, &graph));
-  p->ctx->launches = before;  // captured launches are counted when the graph is replayed
-  MYCEL_CUDA(p->ctx, cudaGraphInstantiate(&p->pcg_graph, graph, 0));
-  cudaGraphDestroy(graph);
+  mycel_ctx* c = p->ctx;
+  if (p->pcg_graph[0] && p->pcg_graph_profiled == c->profile) return MYCEL_OK;
+  cudaStream_t s = c->stream;
+  int64_t before = c->launches;
+  for (int k = 0; k < 2; ++k) {
+    if (p->pcg_graph[k]) cudaGraphExecDestroy(p->pcg_graph[k]);
+    p->pcg_graph[k] = nullptr;
+    for (int j = 0; j < 2; ++j)
+      if (!p->prof64_ev[k][j]) cudaEventCreate(&p->prof64_ev[k][j]);
+    cudaGraph_t graph;
+    MYCEL_CUDA(c, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    for (int i = 0; i < kChunkIters; ++i) launch_pcg_iteration(p, c->profile && i == 0);
+    MYCEL_CUDA(c, cudaStreamEndCapture(s, &graph));
+    MYCEL_CUDA(c, cudaGraphInstantiate(&p->pcg_graph[k], graph, 0));
+    cudaGraphDestroy(graph);
+  }
+  c->launches = before;  // captured launches are counted when the graph is replayed
   p->pcg_graph_chunk = kChunkIters;
+  p->pcg_graph_profiled = c->profile;
   return MYCEL_OK;
+}
+
+// Chunk launch; when profiling, the first matvec runs directly between two stream events (outside the graph).
+void launch_pcg_chunk(mycel_problem* p, int gi) {
+  cudaStream_t s = p->ctx->stream;
+  if (p->pcg_graph_profiled) {
+    cudaEventRecord(p->prof64_ev[gi][0], s);
+    launch_matvec64(p, p->d_p, p->d_ap, 1, &p->d_state->status);
+    cudaEventRecord(p->prof64_ev[gi][1], s);
+  }
+  cudaGraphLaunch(p->pcg_graph[gi], s);
 }
 
 }  // namespace
@@ -262,17 +281,48 @@ int32_t pcg_solve_fp64(mycel_problem* p, const double* d_bv, const int32_t* d_nz
   }
   launch_pcg_init_z(p);
   if ((st = capture_pcg_graph(p))) return st;
-  int64_t launched = 0;
-  for (;;) {
+  if ((st = read_state(p, &hs))) return st;
+  if (hs.status == PCG_RUNNING) {
+    // pipeline: chunk k is queued while the status after chunk k-1 is read
+    PcgState* slot[2] = {(PcgState*)((char*)c->pinned + 4096), (PcgState*)((char*)c->pinned + 4096 + 512)};
+    cudaEvent_t evs[2];
+    cudaEventCreateWithFlags(&evs[0], cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&evs[1], cudaEventDisableTiming);
+    struct EvGuard { cudaEvent_t* e; ~EvGuard() { cudaEventDestroy(e[0]); cudaEventDestroy(e[1]); } } evg{evs};
+    int64_t launched = 0;
+    for (int64_t k = 0;; ++k) {
+      if (cancel && *cancel) {
+        cudaStreamSynchronize(s);
+        return set_error(c, MYCEL_E_CANCELLED, "The operation was canceled.");
+      }
+      // the device state machine stops by itself at max_iter; this bound only guards against a broken state
+      if (launched > (int64_t)max_iter + 4 * p->pcg_graph_chunk) {
+        cudaStreamSynchronize(s);
+        return set_error(c, MYCEL_E_TIMEOUT, "PCG device state did not reach a final status");
+      }
+      int gi = (int)(k & 1);
+      launch_pcg_chunk(p, gi);
+      MYCEL_CUDA(c, cudaGetLastError());
+      launched += p->pcg_graph_chunk;
+      c->launches += 4 * p->pcg_graph_chunk - (p->pcg_graph_profiled ? 1 : 0);  // direct matvec counted itself
+      MYCEL_CUDA(c, cudaMemcpyAsync(slot[gi], p->d_state, sizeof(PcgState), cudaMemcpyDeviceToHost, s));
+      MYCEL_CUDA(c, cudaEventRecord(evs[gi], s));
+      if (k == 0) continue;
+      int pi = (int)((k - 1) & 1);
+      MYCEL_CUDA(c, cudaEventSynchronize(evs[pi]));
+      if (slot[pi]->status != PCG_RUNNING) break;
+      if (c->profile) {
+        float ms_ = 0.f;
+        if (cudaEventElapsedTime(&ms_, p->prof64_ev[pi][0], p->prof64_ev[pi][1]) == cudaSuccess) {
+          c->prof_ms[1] += ms_;
+          c->prof_n[1] += 1;
+          c->prof_nodes[1] += p->g.nn;
+          c->prof_elems[1] += p->n_active;
+        }
+      }
+    }
+    MYCEL_CUDA(c, cudaStreamSynchronize(s));
     if ((st = read_state(p, &hs))) return st;
-    if (hs.status != PCG_RUNNING) break;
-    if (cancel && *cancel) return set_error(c, MYCEL_E_CANCELLED, "The operation was canceled.");
-    // the device state machine stops by itself at max_iter; this bound only guards against a broken state
-    if (launched > (int64_t)max_iter + 4 * p->pcg_graph_chunk)
-      return set_error(c, MYCEL_E_TIMEOUT, "PCG device state did not reach a final status");
-    MYCEL_CUDA(c, cudaGraphLaunch(p->pcg_graph, s));
-    launched += p->pcg_graph_chunk;
-    c->launches += 4 * p->pcg_graph_chunk;
   }
   if (d_xv != p->d_x) MYCEL_CUDA(c, cudaMemcpyAsync(d_xv, p->d_x, sizeof(double) * p->g.nd, cudaMemcpyDeviceToDevice, s));
   MYCEL_CUDA(c, cudaStreamSynchronize(s));
@@ -327,6 +377,23 @@ extern "C" void* mycel_ctx_stream(mycel_ctx* c) { return c ? (void*)c->stream : 
 extern "C" const char* mycel_last_error(mycel_ctx* c) { return c ? c->last_error.c_str() : tls_error.c_str(); }
 extern "C" int64_t mycel_ctx_launch_count(mycel_ctx* c) { return c ? c->launches : 0; }
 
+extern "C" int32_t mycel_ctx_set_profiling(mycel_ctx* c, int32_t enable) {
+  if (!c) return set_error(nullptr, MYCEL_E_ARG, "NULL context");
+  c->profile = enable ? 1 : 0;
+  for (int k = 0; k < 4; ++k) c->prof_ms[k] = 0, c->prof_n[k] = 0, c->prof_nodes[k] = 0, c->prof_elems[k] = 0;
+  return MYCEL_OK;
+}
+
+extern "C" int32_t mycel_ctx_kernel_timing(mycel_ctx* c, int32_t which, double* total_ms, int64_t* launches,
+                                           int64_t* nodes, int64_t* elems) {
+  if (!c || which < 0 || which > 3) return set_error(c, MYCEL_E_ARG, "invalid argument");
+  if (total_ms) *total_ms = c->prof_ms[which];
+  if (launches) *launches = c->prof_n[which];
+  if (nodes) *nodes = c->prof_nodes[which];
+  if (elems) *elems = c->prof_elems[which];
+  return MYCEL_OK;
+}
+
 // ======================================================================================================
 // problem
 // ======================================================================================================
@@ -348,6 +415,7 @@ extern "C" int32_t mycel_problem_create(mycel_ctx* c, const mycel_grid* grid, co
       return set_error(c, MYCEL_E_ARG, "Fixed DOF " + std::to_string(fixed[i]) + " is out of bounds [0, " +
                                            std::to_string(g.nd - 1) + "].");
   cudaSetDevice(c->device);
+  (void)cudaGetLastError();  // do not report a stale error of an earlier, unrelated call
   mycel_problem* p = new mycel_problem();
   p->ctx = c;
   p->g = g;
@@ -466,7 +534,8 @@ extern "C" int32_t mycel_problem_create(mycel_ctx* c, const mycel_grid* grid, co
   int32_t hcnt = 0;
   cudaMemcpyAsync(nf.data(), p->d_nflags, g.nn, cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(&hcnt, d_cnt, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
-  cudaError_t e = cudaStreamSynchronize(s);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   dfree(d_cnt);
   if (e != cudaSuccess) {
     mycel_problem_destroy(p);
@@ -486,7 +555,7 @@ extern "C" int32_t mycel_problem_create(mycel_ctx* c, const mycel_grid* grid, co
   }
   launch_update_E(p, p->d_rho_box, penal);
   launch_diag(p);
-  if ((e = cudaStreamSynchronize(s)) != cudaSuccess) {
+  if ((e = cudaGetLastError()) != cudaSuccess || (e = cudaStreamSynchronize(s)) != cudaSuccess) {
     mycel_problem_destroy(p);
     return set_error(c, MYCEL_E_DEVICE, std::string("problem set-up: ") + cudaGetErrorString(e));
   }
@@ -498,8 +567,16 @@ extern "C" int32_t mycel_problem_destroy(mycel_problem* p) {
   if (!p) return MYCEL_OK;
   cudaSetDevice(p->ctx->device);
   cudaStreamSynchronize(p->ctx->stream);
-  if (p->pcg_graph) cudaGraphExecDestroy(p->pcg_graph);
-  if (p->pcg32_graph) cudaGraphExecDestroy(p->pcg32_graph);
+  for (int k = 0; k < 2; ++k) {
+    if (p->pcg_graph[k]) cudaGraphExecDestroy(p->pcg_graph[k]);
+    for (int j = 0; j < 2; ++j)
+      if (p->prof64_ev[k][j]) cudaEventDestroy(p->prof64_ev[k][j]);
+  }
+  for (int k = 0; k < 2; ++k) {
+    if (p->pcg32_graph[k]) cudaGraphExecDestroy(p->pcg32_graph[k]);
+    for (int j = 0; j < 2; ++j)
+      if (p->prof_ev[k][j]) cudaEventDestroy(p->prof_ev[k][j]);
+  }
   void* ptrs[] = {p->d_domain, p->d_nflags, p->d_fixed, p->d_active, p->d_e2a, p->d_F, p->d_b, p->d_fnz, p->d_bnz, p->d_rho_box,
                   p->d_E, p->d_Ef, p->d_diag, p->d_invd, p->d_invdf, p->d_r, p->d_z, p->d_p, p->d_ap, p->d_x,
                   p->d_part, p->d_state, p->f_x, p->f_r, p->f_z, p->f_p0, p->f_p1, p->f_ap, p->d_r64, p->d_part2,
@@ -656,13 +733,15 @@ extern "C" int32_t mycel_static_solve(mycel_problem* p, const mycel_static_optio
 extern "C" int32_t mycel_filter_create(mycel_problem* p, double rmin, mycel_filter** out) {
   if (!p || !out) return set_error(p ? p->ctx : nullptr, MYCEL_E_ARG, "NULL argument");
   cudaSetDevice(p->ctx->device);
+  (void)cudaGetLastError();
   mycel_filter* f = new mycel_filter();
   f->p = p;
   f->rmin = rmin;
   int st = filter_setup(f);
   if (st) {
+    std::string m = p->ctx->last_error;
     mycel_filter_destroy(f);
-    return set_error(p->ctx, st, "filter set-up failed");
+    return set_error(p->ctx, st, m.empty() ? std::string("filter set-up failed") : m);
   }
   *out = f;
   return MYCEL_OK;

@@ -1,18 +1,25 @@
 // Mixed-precision form: FP32 inner Jacobi-PCG (K·u and the preconditioner in FP32 with FP32 accumulation)
 // inside FP64 iterative refinement. FP64 is kept only for the refinement residual f - K u, the CG alpha/beta
-// dot products (FP32 operands, products and sums in FP64), and the outer update u += s d.
+// dot products (FP32 operands, products and sums in FP64), and the accumulated solution u.
+//
+// Refinement is done by reliable updating: the FP32 CG recurrence runs continuously; whenever its recursive
+// residual has dropped by kFlushFactor since the last replacement (or reaches the target), the FP32 correction
+// is added to u in FP64, the true residual P(b - A u) is recomputed in FP64 and replaces the FP32 residual, and
+// the search direction is kept (beta = rho_new / rho_old), so the Krylov progress is not thrown away.
 //
 // Per inner iteration two kernels:
 //   k_mv32   p_t = z + beta p_{t-1} (on the fly for every gathered node), Ap_t = K p_t, and the FP64 partials of
 //            p_t . Ap_t; the last CTA forms alpha.
-//   k_xr32   x += alpha p, r -= alpha Ap, z = r invD, FP64 partials of r.r and r.z; the last CTA forms the inner
-//            residual, the stop test and beta.
-// Reductions use a fixed CTA decomposition and a block-ordered final sum, so results do not depend on timing.
+//   k_xr32   x += alpha p, r -= alpha Ap, z = r invD, FP64 partials of r.r and r.z; the last CTA forms the
+//            recursive residual, the replacement/stop triggers and beta.
+// Reductions use a fixed CTA decomposition and a fixed-order final sum, so results do not depend on timing.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <cstring>
 #include <string>
 
@@ -20,28 +27,22 @@
 
 namespace mycel {
 
-enum MixStatus : int { MIX_RUNNING = 0, MIX_DONE = 1, MIX_BREAKDOWN = 2, MIX_MAXITER = 3 };
+enum MixStatus : int { MIX_RUNNING = 0, MIX_FLUSH = 1, MIX_BREAKDOWN = 2, MIX_MAXITER = 3 };
 
 struct MixState {
   int status;
-  int iter;      // inner iterations of this refinement step
+  int iter;      // inner iterations in total
   int max_iter;
-  int pad;
-  double eta;    // inner relative tolerance
-  double r0n2;   // ||r32_0||^2
-  double rho0, alpha, beta, rel_in, rn2, pap;
+  int first;     // next k_mv32 starts a new direction (p = z)
+  double target;     // absolute residual at which to verify convergence (tol * ||P b|| * safety)
+  double flush_at;   // absolute recursive residual that triggers a true-residual replacement
+  double rho0, alpha, beta, rn, pap;
   unsigned int counter;
   unsigned int pad2;
 };
 
 constexpr int kT = 256;
-
-__device__ __forceinline__ int local_index32(int ox, int oy, int oz) {
-  int base = oy ? (ox ? 2 : 3) : (ox ? 1 : 0);
-  return base + 4 * oz;
-}
-
-__device__ __forceinline__ double ld_vol(const double* p) { return *(const volatile double*)p; }
+constexpr double kFlushFactor = 1e-2;
 
 __device__ __forceinline__ bool elect_last32(unsigned int* counter) {
   __shared__ bool last;
@@ -56,108 +57,177 @@ __device__ __forceinline__ bool elect_last32(unsigned int* counter) {
   return last;
 }
 
-// deterministic block sum of a double (result valid in thread 0)
+// deterministic block sum of a double (result valid in linear thread 0); works for 1-D and 2-D blocks
 __device__ __forceinline__ double bsum(double v, double* sh) {
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  const int nw = (blockDim.x * blockDim.y) >> 5;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
   __syncthreads();
-  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  if ((tid & 31) == 0) sh[tid >> 5] = v;
   __syncthreads();
   double t = 0.0;
-  if (threadIdx.x == 0)
-    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += sh[k];
+  if (tid == 0)
+    for (int k = 0; k < nw; ++k) t += sh[k];
   return t;
 }
 
+// deterministic sum of part[0..n) by one warp (lane l takes l, l+32, ...; fixed shuffle tree); all lanes get it
+__device__ __forceinline__ double warp_sum_parts(const double* part, unsigned n) {
+  int lane = threadIdx.x & 31;
+  double s = 0.0;
+  for (unsigned q = lane; q < n; q += 32) s += *(const volatile double*)(part + q);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  return s;
+}
+
 // ---------------------------------------------------------------------------------------------------------
-// FP32 K p with on-the-fly p update (parity-class node mapping as in the FP64 kernel)
+// FP32 K p, z-marching shared-memory tiles.
+// A CTA owns a TX x TY column of nodes and marches over ZSEG node planes. Three node planes of the input
+// (with a one-node halo) and two element planes of E live in shared memory; rows are loaded contiguously.
+// Each thread keeps its 27-node neighbourhood in registers and applies the 8 incident elements' KE rows
+// (compile-time indices, so KE is read as constant-bank FFMA operands).
+// MODE 1 (inner PCG step): the input is p_t = z + beta p_{t-1} formed while loading; owned nodes write p_t;
+// the CTA adds p_t . K p_t into an FP64 partial and the last CTA forms alpha.
+// Inactive elements carry E = 0, elements outside the grid and halo nodes outside the grid read as 0.
 // ---------------------------------------------------------------------------------------------------------
-template <int MODE>  // 0: y = K x (plain), 1: inner-PCG step (p update + pAp partials)
-__global__ void __launch_bounds__(kT) k_mv32(GridDims g, const __grid_constant__ KeF ke, const float* __restrict__ xin,
-                                             const float* __restrict__ z, const float* __restrict__ pold,
-                                             float* __restrict__ pnew, float* __restrict__ y,
-                                             const float* __restrict__ E, const uint8_t* __restrict__ dom,
-                                             const uint8_t* __restrict__ nf, int projected, MixState* st,
-                                             double* part) {
+constexpr int TX = 32, TY = 8;
+constexpr int PX = TX + 2, PY = TY + 2;  // node plane with halo
+constexpr int EX = TX + 1, EY = TY + 1;  // element plane
+
+template <int MODE>
+__global__ void __launch_bounds__(TX * TY, 2) k_mv32(GridDims g, const __grid_constant__ KeF ke,
+                                                     const float* __restrict__ xin, const float* __restrict__ z,
+                                                     const float* __restrict__ pold, float* __restrict__ pnew,
+                                                     float* __restrict__ y, const float* __restrict__ E,
+                                                     const uint8_t* __restrict__ nf, int projected, MixState* st,
+                                                     double* part, int zseg) {
+  __shared__ float xs[3][PY][PX][3];
+  __shared__ float es[2][EY][EX];
   __shared__ double sh[32];
   if (MODE == 1 && st->status != MIX_RUNNING) return;
   const float beta = MODE == 1 ? (float)st->beta : 0.0f;
-  const bool first = MODE == 1 ? (st->iter == 0) : true;
-  const int cls = blockIdx.y;
-  const int px = cls & 1, py = (cls >> 1) & 1, pz = (cls >> 2) & 1;
-  const int cx = (g.nx1 - px + 1) >> 1, cy = (g.ny1 - py + 1) >> 1, cz = (g.nz1 - pz + 1) >> 1;
-  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  const bool valid = t < (int64_t)cx * cy * cz;
-  double pap = 0.0;
-  if (valid) {
-    int a_ = (int)(t % cx);
-    int64_t rest = t / cx;
-    int i = px + 2 * a_, j = py + 2 * (int)(rest % cy), k = pz + 2 * (int)(rest / cy);
-    const int64_t sy = g.nx1, sz = (int64_t)g.nx1 * g.ny1;
-    float acc0 = 0.f, acc1 = 0.f, acc2 = 0.f;
-#pragma unroll 1
-    for (int col = 0; col < 8; ++col) {
-      int ox = (col & 1) ^ px, oy = ((col >> 1) & 1) ^ py, oz = ((col >> 2) & 1) ^ pz;
-      int ie = i - ox, je = j - oy, kk = k - oz;
-      if (ie < 0 || ie >= g.nx || je < 0 || je >= g.ny || kk < 0 || kk >= g.nz) continue;
-      int64_t e = ie + (int64_t)g.nx * (je + (int64_t)g.ny * kk);
-      if (!__ldg(dom + e)) continue;
-      float ee = __ldg(E + e);
-      int64_t n0 = ie + sy * je + sz * kk;
-      const int64_t off[8] = {0, 1, 1 + sy, sy, sz, sz + 1, sz + 1 + sy, sz + sy};
-      float ue[24];
-#pragma unroll
-      for (int b = 0; b < 8; ++b) {
-        int64_t q = 3 * (n0 + off[b]);
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          float v;
-          if (MODE == 1) v = first ? __ldg(z + q + c) : fmaf(beta, __ldg(pold + q + c), __ldg(z + q + c));
-          else v = __ldg(xin + q + c);
-          ue[3 * b + c] = v * ee;
+  const bool first = MODE == 1 ? (st->first != 0) : true;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY, k0 = blockIdx.z * zseg;
+  const int k1 = min(k0 + zseg, g.nz1);
+  const int64_t sy = g.nx1, sz = (int64_t)g.nx1 * g.ny1;
+
+  // load node plane kk into slot; owned interior nodes of owned planes write p_t
+  auto load_plane = [&](int kk, int slot) {
+    const bool owned_plane = kk >= k0 && kk < k1;
+    for (int q = tid; q < PY * PX * 3; q += TX * TY) {
+      int c = q % 3, rest = q / 3, lx = rest % PX, ly = rest / PX;
+      int i = i0 - 1 + lx, j = j0 - 1 + ly;
+      float v = 0.f;
+      if (kk >= 0 && kk < g.nz1 && i >= 0 && i < g.nx1 && j >= 0 && j < g.ny1) {
+        int64_t idx = 3 * (i + sy * j + sz * kk) + c;
+        if (MODE == 1) {
+          v = first ? __ldg(z + idx) : fmaf(beta, __ldg(pold + idx), __ldg(z + idx));
+          if (owned_plane && lx >= 1 && lx <= TX && ly >= 1 && ly <= TY) pnew[idx] = v;
+        } else {
+          v = __ldg(xin + idx);
         }
       }
-      const int a = local_index32(ox, oy, oz);
-      const float* r0 = ke.v + (3 * a) * 24;
-      float s0 = 0.f, s1 = 0.f, s2 = 0.f;
-#pragma unroll
-      for (int c = 0; c < 24; ++c) {
-        s0 = fmaf(r0[c], ue[c], s0);
-        s1 = fmaf(r0[24 + c], ue[c], s1);
-        s2 = fmaf(r0[48 + c], ue[c], s2);
-      }
-      acc0 += s0;
-      acc1 += s1;
-      acc2 += s2;
+      xs[slot][ly][lx][c] = v;
     }
-    int64_t n = i + sy * j + sz * k;
-    uint8_t f = projected ? nf[n] : 0;
-    float out[3] = {acc0, acc1, acc2};
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      int64_t q = 3 * n + c;
-      float pv;
-      if (MODE == 1) {
-        pv = first ? z[q] : fmaf(beta, pold[q], z[q]);
-        pnew[q] = pv;
-      } else {
-        pv = xin[q];
-      }
-      float yv = (f & (1 << c)) ? pv : out[c];
-      y[q] = yv;
-      if (MODE == 1) pap += (double)pv * (double)yv;
+  };
+  auto load_eplane = [&](int ke_, int slot) {
+    for (int q = tid; q < EY * EX; q += TX * TY) {
+      int lx = q % EX, ly = q / EX;
+      int ie = i0 - 1 + lx, je = j0 - 1 + ly;
+      float v = 0.f;
+      if (ke_ >= 0 && ke_ < g.nz && ie >= 0 && ie < g.nx && je >= 0 && je < g.ny)
+        v = __ldg(E + ie + (int64_t)g.nx * (je + (int64_t)g.ny * ke_));
+      es[slot][ly][lx] = v;
     }
+  };
+
+  load_plane(k0 - 1, (k0 + 2) % 3);
+  load_plane(k0, k0 % 3);
+  load_eplane(k0 - 1, (k0 + 1) & 1);
+  const int i = i0 + tx, j = j0 + ty;
+  const bool mine = i < g.nx1 && j < g.ny1;
+  double pap = 0.0;
+  for (int k = k0; k < k1; ++k) {
+    load_plane(k + 1, (k + 1) % 3);
+    load_eplane(k, k & 1);
+    __syncthreads();
+    if (mine) {
+      float xn[3][3][3][3];  // [dz][dy][dx][c], offsets -1..+1
+#pragma unroll
+      for (int dz = 0; dz < 3; ++dz) {
+        const int slot = (k - 1 + dz + 3) % 3;
+#pragma unroll
+        for (int dy = 0; dy < 3; ++dy)
+#pragma unroll
+          for (int dx = 0; dx < 3; ++dx)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) xn[dz][dy][dx][c] = xs[slot][ty + dy][tx + dx][c];
+      }
+      float acc0 = 0.f, acc1 = 0.f, acc2 = 0.f;
+#pragma unroll
+      for (int sz_ = 0; sz_ < 2; ++sz_) {
+        const int eslot = (k - 1 + sz_) & 1;
+#pragma unroll
+        for (int sy_ = 0; sy_ < 2; ++sy_)
+#pragma unroll
+          for (int sx_ = 0; sx_ < 2; ++sx_) {
+            const float ee = es[eslot][ty + sy_][tx + sx_];
+            // this node sits at local (1-sx, 1-sy, 1-sz) of the element
+            const int ox = 1 - sx_, oy = 1 - sy_, oz = 1 - sz_;
+            const int a = (oy ? (ox ? 2 : 3) : (ox ? 1 : 0)) + 4 * oz;
+            float s0 = 0.f, s1 = 0.f, s2 = 0.f;
+#pragma unroll
+            for (int b = 0; b < 8; ++b) {
+              const int bx = (b == 1 || b == 2 || b == 5 || b == 6) ? 1 : 0;
+              const int by = (b == 2 || b == 3 || b == 6 || b == 7) ? 1 : 0;
+              const int bz = b >= 4 ? 1 : 0;
+#pragma unroll
+              for (int c = 0; c < 3; ++c) {
+                const float xv = xn[sz_ + bz][sy_ + by][sx_ + bx][c];
+                s0 = fmaf(ke.v[(3 * a + 0) * 24 + 3 * b + c], xv, s0);
+                s1 = fmaf(ke.v[(3 * a + 1) * 24 + 3 * b + c], xv, s1);
+                s2 = fmaf(ke.v[(3 * a + 2) * 24 + 3 * b + c], xv, s2);
+              }
+            }
+            acc0 = fmaf(ee, s0, acc0);
+            acc1 = fmaf(ee, s1, acc1);
+            acc2 = fmaf(ee, s2, acc2);
+          }
+      }
+      const int64_t n = i + sy * j + sz * k;
+      const uint8_t f = projected ? nf[n] : 0;
+      const float out[3] = {acc0, acc1, acc2};
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const float pv = xn[1][1][1][c];
+        const float yv = (f & (1 << c)) ? pv : out[c];
+        y[3 * n + c] = yv;
+        if (MODE == 1) pap += (double)pv * (double)yv;
+      }
+    }
+    __syncthreads();
   }
   if (MODE != 1) return;
   double b = bsum(pap, sh);
-  const unsigned nblk = gridDim.x * gridDim.y;
-  const unsigned bid = blockIdx.y * gridDim.x + blockIdx.x;
-  if (threadIdx.x == 0) part[bid] = b;
-  if (!elect_last32(&st->counter)) return;
-  if (threadIdx.x != 0) return;
+  const unsigned nblk = gridDim.x * gridDim.y * gridDim.z;
+  const unsigned bid = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+  if (tid == 0) part[bid] = b;
+  // last-CTA election over the 3-D grid
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) last = (atomicAdd(&st->counter, 1u) == nblk - 1);
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (tid >= 32) return;
+  double s = warp_sum_parts(part, nblk);
+  if (tid != 0) return;
   st->counter = 0;
-  double s = 0.0;
-  for (unsigned q = 0; q < nblk; ++q) s += ld_vol(part + q);
+  st->first = 0;
   st->pap = s;
   if (!(s > 0.0) || !isfinite(s)) {
     st->status = MIX_BREAKDOWN;
@@ -166,26 +236,62 @@ __global__ void __launch_bounds__(kT) k_mv32(GridDims g, const __grid_constant__
   st->alpha = st->rho0 / s;
 }
 
-// x += alpha p, r -= alpha Ap, z = r invD; partials of r.r and r.z (FP64)
+// z-segment length: enough segments that the grid holds about 8 CTAs per SM (the kernel is latency-bound
+// with one CTA per SM), at least 2 planes per segment.
+static int tile_zseg(const GridDims& g, int num_sms) {
+  int64_t txy = (int64_t)((g.nx1 + TX - 1) / TX) * ((g.ny1 + TY - 1) / TY);
+  int64_t segs = std::max<int64_t>(1, (8 * (int64_t)num_sms + txy - 1) / txy);
+  return (int)std::max<int64_t>(2, (g.nz1 + segs - 1) / segs);
+}
+
+static dim3 tile_grid(const GridDims& g, int zseg) {
+  return dim3((unsigned)((g.nx1 + TX - 1) / TX), (unsigned)((g.ny1 + TY - 1) / TY), (unsigned)((g.nz1 + zseg - 1) / zseg));
+}
+
+// x += alpha p, r -= alpha Ap, z = r invD; partials of r.r and r.z (FP64). mode 0: CG step; 1: residual
+// replacement (z, rho from the new r; beta = rho_new / rho_old); 2: start (z, rho; next step starts p = z).
 __global__ void __launch_bounds__(kT) k_xr32(int64_t n, float* __restrict__ x, float* __restrict__ r,
                                              float* __restrict__ z, const float* __restrict__ p,
                                              const float* __restrict__ ap, const float* __restrict__ invd,
-                                             MixState* st, double* part, int init) {
+                                             MixState* st, double* part, int mode) {
   __shared__ double sh[32];
-  if (st->status != MIX_RUNNING) return;
-  const float alpha = init ? 0.f : (float)st->alpha;
+  if (mode == 0 && st->status != MIX_RUNNING) return;
+  const float alpha = mode ? 0.f : (float)st->alpha;
   double rr = 0.0, rz = 0.0;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    float rv = r[i];
-    if (!init) {
-      x[i] = fmaf(alpha, p[i], x[i]);
-      rv = fmaf(-alpha, ap[i], rv);
-      r[i] = rv;
+  const int64_t n4 = n >> 2;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n4; i += stride) {
+    float4 rv = reinterpret_cast<const float4*>(r)[i];
+    float4 iv = reinterpret_cast<const float4*>(invd)[i];
+    if (mode == 0) {
+      float4 xv = reinterpret_cast<const float4*>(x)[i];
+      float4 pv = reinterpret_cast<const float4*>(p)[i];
+      float4 av = reinterpret_cast<const float4*>(ap)[i];
+      xv.x = fmaf(alpha, pv.x, xv.x); xv.y = fmaf(alpha, pv.y, xv.y);
+      xv.z = fmaf(alpha, pv.z, xv.z); xv.w = fmaf(alpha, pv.w, xv.w);
+      rv.x = fmaf(-alpha, av.x, rv.x); rv.y = fmaf(-alpha, av.y, rv.y);
+      rv.z = fmaf(-alpha, av.z, rv.z); rv.w = fmaf(-alpha, av.w, rv.w);
+      reinterpret_cast<float4*>(x)[i] = xv;
+      reinterpret_cast<float4*>(r)[i] = rv;
     }
-    float zv = rv * invd[i];
-    z[i] = zv;
-    rr += (double)rv * (double)rv;
-    rz += (double)rv * (double)zv;
+    float4 zv = make_float4(rv.x * iv.x, rv.y * iv.y, rv.z * iv.z, rv.w * iv.w);
+    reinterpret_cast<float4*>(z)[i] = zv;
+    rr += (double)rv.x * rv.x + (double)rv.y * rv.y + (double)rv.z * rv.z + (double)rv.w * rv.w;
+    rz += (double)rv.x * zv.x + (double)rv.y * zv.y + (double)rv.z * zv.z + (double)rv.w * zv.w;
+  }
+  if (blockIdx.x == 0) {  // tail (n not a multiple of 4)
+    for (int64_t i = 4 * n4 + threadIdx.x; i < n; i += blockDim.x) {
+      float rv = r[i];
+      if (mode == 0) {
+        x[i] = fmaf(alpha, p[i], x[i]);
+        rv = fmaf(-alpha, ap[i], rv);
+        r[i] = rv;
+      }
+      float zv = rv * invd[i];
+      z[i] = zv;
+      rr += (double)rv * rv;
+      rz += (double)rv * zv;
+    }
   }
   double brr = bsum(rr, sh);
   double brz = bsum(rz, sh);
@@ -194,27 +300,36 @@ __global__ void __launch_bounds__(kT) k_xr32(int64_t n, float* __restrict__ x, f
     part[gridDim.x + blockIdx.x] = brz;
   }
   if (!elect_last32(&st->counter)) return;
+  if (threadIdx.x >= 32) return;
+  double srr = warp_sum_parts(part, gridDim.x);
+  double srz = warp_sum_parts(part + gridDim.x, gridDim.x);
   if (threadIdx.x != 0) return;
   st->counter = 0;
-  double srr = 0.0, srz = 0.0;
-  for (unsigned q = 0; q < gridDim.x; ++q) {
-    srr += ld_vol(part + q);
-    srz += ld_vol(part + gridDim.x + q);
-  }
-  if (init) {
-    st->r0n2 = srr;
+  const double rn = sqrt(srr);
+  st->rn = rn;
+  if (mode == 2) {  // start of a solve
     st->rho0 = srz;
-    st->iter = 0;
-    st->rel_in = 1.0;
-    if (!(srr > 0.0)) st->status = MIX_DONE;
+    st->first = 1;
+    st->status = (rn <= st->target) ? MIX_FLUSH : MIX_RUNNING;
+    st->flush_at = rn * kFlushFactor;
+    return;
+  }
+  if (mode == 1) {  // true residual replaced the recursive one: keep the direction
+    if (st->first || !(st->rho0 > 0.0)) {
+      st->first = 1;
+    } else {
+      double beta = srz / st->rho0;
+      if (!isfinite(beta) || beta < 0.0) st->first = 1;
+      else st->beta = beta;
+    }
+    st->rho0 = srz;
+    st->flush_at = rn * kFlushFactor;
+    st->status = MIX_RUNNING;
     return;
   }
   st->iter += 1;
-  st->rn2 = srr;
-  double rel = sqrt(srr / st->r0n2);
-  st->rel_in = rel;
-  if (rel <= st->eta) {
-    st->status = MIX_DONE;
+  if (rn <= st->target || rn <= st->flush_at) {
+    st->status = MIX_FLUSH;  // rho0 stays rho_k for the beta after the replacement
     return;
   }
   double beta = srz / st->rho0;
@@ -227,15 +342,22 @@ __global__ void __launch_bounds__(kT) k_xr32(int64_t n, float* __restrict__ x, f
   if (st->iter >= st->max_iter) st->status = MIX_MAXITER;
 }
 
-// FP64 refinement residual r64 = P(b - A u) with partials of r64.r64; scaled FP32 copy r32 = r64 / ||r64||
+// FP64 refinement: u += x32, x32 = 0; then (after A u) r64 = P(b - A u), r32 = (float) r64, partials of r64^2
+__global__ void k_flush_u(int64_t n, double* __restrict__ u, float* __restrict__ x32) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    u[i] += (double)x32[i];
+    x32[i] = 0.f;
+  }
+}
+
 __global__ void k_resid64(int64_t n, const uint8_t* __restrict__ nf, const double* __restrict__ b,
-                          const double* __restrict__ au, double* __restrict__ r64, double* part) {
+                          const double* __restrict__ au, float* __restrict__ r32, double* part) {
   __shared__ double sh[32];
   double s = 0.0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     bool con = nf[i / 3] & (1 << (i % 3));
     double v = con ? 0.0 : (b[i] - au[i]);
-    r64[i] = v;
+    r32[i] = (float)v;
     s += v * v;
   }
   double bs = bsum(s, sh);
@@ -243,25 +365,9 @@ __global__ void k_resid64(int64_t n, const uint8_t* __restrict__ nf, const doubl
 }
 
 __global__ void k_sum_part(const double* part, int nb, double* out) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  double s = 0.0;
-  for (int q = 0; q < nb; ++q) s += part[q];
-  *out = s;
-}
-
-__global__ void k_scale_to_f32(int64_t n, const double* __restrict__ r64, const double* __restrict__ n2,
-                               float* __restrict__ r32, float* __restrict__ x32) {
-  double inv = 1.0 / sqrt(*n2);
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    r32[i] = (float)(r64[i] * inv);
-    x32[i] = 0.f;
-  }
-}
-
-__global__ void k_axpy_u(int64_t n, double* __restrict__ u, const float* __restrict__ d, const double* __restrict__ n2) {
-  double s = sqrt(*n2);
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    u[i] += s * (double)d[i];
+  if (blockIdx.x != 0 || threadIdx.x >= 32) return;
+  double s = warp_sum_parts(part, (unsigned)nb);
+  if (threadIdx.x == 0) *out = s;
 }
 
 __global__ void k_to_f32(int64_t n, const double* __restrict__ a, float* __restrict__ b) {
@@ -273,13 +379,11 @@ __global__ void k_to_f64(int64_t n, const float* __restrict__ a, double* __restr
     b[i] = (double)a[i];
 }
 
-static dim3 cls_grid(const GridDims& g) {
-  int cx = (g.nx1 + 1) >> 1, cy = (g.ny1 + 1) >> 1, cz = (g.nz1 + 1) >> 1;
-  int64_t tot = (int64_t)cx * cy * cz;
-  return dim3((unsigned)((tot + kT - 1) / kT), 8, 1);
+// grid for the streaming kernels: fixed by n (deterministic reductions), at most 8 CTAs per SM
+static int stream_blocks(mycel_problem* p) {
+  int64_t want = (p->g.nd / 4 + (int64_t)kT * 4 - 1) / ((int64_t)kT * 4);
+  return (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)p->ctx->num_sms * 8));
 }
-
-static int stream_blocks(mycel_problem* p) { return p->ctx->num_sms * 8; }
 
 void launch_E_to_f32(mycel_problem* p) {
   (void)p;  // k_update_E writes the FP32 copy of E alongside the FP64 one
@@ -291,8 +395,9 @@ void mixed_apply_k_f64io(mycel_problem* p, const double* x, double* y, int proje
   float* fx = (float*)p->d_r;  // borrow FP64 workspace as FP32 staging
   float* fy = fx + n;
   k_to_f32<<<stream_blocks(p), kT, 0, s>>>(n, x, fx);
-  k_mv32<0><<<cls_grid(p->g), kT, 0, s>>>(p->g, p->kef, fx, nullptr, nullptr, nullptr, fy, p->d_Ef, p->d_domain,
-                                         p->d_nflags, projected, nullptr, nullptr);
+  int zs = tile_zseg(p->g, p->ctx->num_sms);
+  k_mv32<0><<<tile_grid(p->g, zs), dim3(TX, TY), 0, s>>>(p->g, p->kef, fx, nullptr, nullptr, nullptr, fy, p->d_Ef,
+                                                         p->d_nflags, projected, nullptr, nullptr, zs);
   k_to_f64<<<stream_blocks(p), kT, 0, s>>>(n, fy, y);
   p->ctx->launches += 3;
 }
@@ -307,49 +412,92 @@ static int32_t ensure_mixed(mycel_problem* p) {
     if ((e = cudaMalloc((void**)b, fb)) != cudaSuccess) break;
     p->device_bytes += (int64_t)fb;
   }
-  if (e == cudaSuccess) {
-    e = cudaMalloc((void**)&p->d_r64, sizeof(double) * (size_t)n + 64);
-    p->device_bytes += (int64_t)(sizeof(double) * n);
-  }
   if (e != cudaSuccess) return set_error(p->ctx, MYCEL_E_OOM, "out of device memory for the mixed-precision workspace");
   return MYCEL_OK;
 }
 
-static MixState* mix_state(mycel_problem* p) {
-  // lives after the FP64 PcgState in the same allocation? use the tail of d_part2
-  return (MixState*)(p->d_part2 + p->n_part2 - 64);
-}
+static MixState* mix_state(mycel_problem* p) { return (MixState*)(p->d_part2 + p->n_part2 - 64); }
 
-__global__ void k_mix_init(MixState* st, double eta, int max_iter) {
+__global__ void k_mix_init(MixState* st, double target, int max_iter) {
   MixState s = {};
   s.status = MIX_RUNNING;
-  s.eta = eta;
+  s.target = target;
   s.max_iter = max_iter;
+  s.first = 1;
   *st = s;
 }
 
+__global__ void k_mix_set(MixState* st, int status) { st->status = status; }
+
+// Chunk of inner iterations as a graph; p alternates between two buffers (even chunk length, each chunk starts
+// from the direction held in f_p1). When the context profiles, the first matvec of a chunk is launched directly
+// between two stream events (outside the graph) and the graph holds the rest of the chunk.
 static int32_t capture_mixed_graph(mycel_problem* p, int chunk) {
-  if (p->pcg32_graph) return MYCEL_OK;
-  cudaStream_t s = p->ctx->stream;
+  mycel_ctx* c = p->ctx;
+  if (p->pcg32_graph[0] && p->pcg32_graph_profiled == c->profile) return MYCEL_OK;
+  for (int k = 0; k < 2; ++k) {
+    if (p->pcg32_graph[k]) cudaGraphExecDestroy(p->pcg32_graph[k]);
+    p->pcg32_graph[k] = nullptr;
+    for (int j = 0; j < 2; ++j)
+      if (!p->prof_ev[k][j]) cudaEventCreate(&p->prof_ev[k][j]);
+  }
+  cudaStream_t s = c->stream;
   int64_t n = p->g.nd;
   MixState* st = mix_state(p);
   double* part = p->d_part2;
   int sb = stream_blocks(p);
-  int64_t before = p->ctx->launches;
-  cudaGraph_t graph;
-  MYCEL_CUDA(p->ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-  for (int t = 0; t < chunk; ++t) {
-    float* pcur = (t & 1) ? p->f_p1 : p->f_p0;
-    float* pprev = (t & 1) ? p->f_p0 : p->f_p1;
-    k_mv32<1><<<cls_grid(p->g), kT, 0, s>>>(p->g, p->kef, nullptr, p->f_z, pprev, pcur, p->f_ap, p->d_Ef,
-                                           p->d_domain, p->d_nflags, 1, st, part);
-    k_xr32<<<sb, kT, 0, s>>>(n, p->f_x, p->f_r, p->f_z, pcur, p->f_ap, p->d_invdf, st, part, 0);
+  int64_t before = c->launches;
+  const int zs = tile_zseg(p->g, c->num_sms);
+  for (int k = 0; k < 2; ++k) {
+    cudaGraph_t graph;
+    MYCEL_CUDA(c, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    for (int t = 0; t < chunk; ++t) {
+      float* pcur = (t & 1) ? p->f_p1 : p->f_p0;
+      float* pprev = (t & 1) ? p->f_p0 : p->f_p1;
+      if (!(c->profile && t == 0))
+        k_mv32<1><<<tile_grid(p->g, zs), dim3(TX, TY), 0, s>>>(p->g, p->kef, nullptr, p->f_z, pprev, pcur,
+                                                               p->f_ap, p->d_Ef, p->d_nflags, 1, st, part, zs);
+      k_xr32<<<sb, kT, 0, s>>>(n, p->f_x, p->f_r, p->f_z, pcur, p->f_ap, p->d_invdf, st, part, 0);
+    }
+    MYCEL_CUDA(c, cudaStreamEndCapture(s, &graph));
+    MYCEL_CUDA(c, cudaGraphInstantiate(&p->pcg32_graph[k], graph, 0));
+    cudaGraphDestroy(graph);
   }
-  MYCEL_CUDA(p->ctx, cudaStreamEndCapture(s, &graph));
-  p->ctx->launches = before;
-  MYCEL_CUDA(p->ctx, cudaGraphInstantiate(&p->pcg32_graph, graph, 0));
-  cudaGraphDestroy(graph);
+  c->launches = before;
   p->pcg32_graph_chunk = chunk;
+  p->pcg32_graph_profiled = c->profile;
+  return MYCEL_OK;
+}
+
+static void launch_chunk(mycel_problem* p, int gi) {
+  mycel_ctx* c = p->ctx;
+  cudaStream_t s = c->stream;
+  if (p->pcg32_graph_profiled) {
+    cudaEventRecord(p->prof_ev[gi][0], s);
+    int zs = tile_zseg(p->g, c->num_sms);
+    k_mv32<1><<<tile_grid(p->g, zs), dim3(TX, TY), 0, s>>>(p->g, p->kef, nullptr, p->f_z, p->f_p1, p->f_p0,
+                                                           p->f_ap, p->d_Ef, p->d_nflags, 1, mix_state(p),
+                                                           p->d_part2, zs);
+    cudaEventRecord(p->prof_ev[gi][1], s);
+  }
+  cudaGraphLaunch(p->pcg32_graph[gi], s);
+}
+
+// r32 = P(b - A u) in FP64, returns ||r|| (synchronises)
+static int32_t true_residual(mycel_problem* p, const double* d_b, const double* d_u, double* rn) {
+  mycel_ctx* c = p->ctx;
+  cudaStream_t s = c->stream;
+  int sb = stream_blocks(p);
+  double* part = p->d_part2;
+  double* scal = p->d_part2 + p->n_part2 - 128;
+  launch_matvec64(p, d_u, p->d_ap, 1, nullptr);
+  k_resid64<<<sb, kT, 0, s>>>(p->g.nd, p->d_nflags, d_b, p->d_ap, p->f_r, part);
+  k_sum_part<<<1, 32, 0, s>>>(part, sb, scal);
+  c->launches += 2;
+  double* h = (double*)((char*)c->pinned + 1024);
+  MYCEL_CUDA(c, cudaMemcpyAsync(h, scal, sizeof(double), cudaMemcpyDeviceToHost, s));
+  MYCEL_CUDA(c, cudaStreamSynchronize(s));
+  *rn = std::sqrt(h[0]);
   return MYCEL_OK;
 }
 
@@ -371,9 +519,7 @@ int32_t mixed_solve_entry(mycel_problem* p, const double* d_b, const int32_t* d_
   const int64_t n = p->g.nd;
   const int sb = stream_blocks(p);
   double* part = p->d_part2;
-  double* scal = p->d_part2 + p->n_part2 - 128;  // [0] ||r64||^2
   MixState* ms = mix_state(p);
-  // project u and ||P b|| (same kernels as the FP64 path)
   double* saved_b = p->d_b;
   int32_t* saved_nz = p->d_bnz;
   int32_t saved_n = p->n_bnz;
@@ -384,6 +530,7 @@ int32_t mixed_solve_entry(mycel_problem* p, const double* d_b, const int32_t* d_
     mycel_problem* p; double* b; int32_t* nz; int32_t n;
     ~Restore() { p->d_b = b; p->d_bnz = nz; p->n_bnz = n; }
   } restore{p, saved_b, saved_nz, saved_n};
+  // project u and ||P b|| (same kernels as the FP64 path)
   cudaMemsetAsync(p->d_state, 0, sizeof(PcgState), s);
   launch_project_x(p, d_u, &p->d_state->nonzero_x);
   launch_pcg_bnorm(p);
@@ -398,56 +545,92 @@ int32_t mixed_solve_entry(mycel_problem* p, const double* d_b, const int32_t* d_
     std::snprintf(res->message, sizeof res->message, "RHS is zero. Solution is zero.");
     return MYCEL_OK;
   }
-  if ((st = capture_mixed_graph(p, 16))) return st;
-  int total_inner = 0, steps = 0;
-  double rel = 0.0;
-  bool ok = false, broke = false;
-  const int max_steps = 30;
-  double* hsc = (double*)((char*)c->pinned + 1024);
-  MixState* hms = (MixState*)((char*)c->pinned + 2048);
-  for (;;) {
-    // r64 = P(b - A u), ||r64||
-    launch_matvec64(p, d_u, p->d_ap, 1, nullptr);
-    k_resid64<<<sb, kT, 0, s>>>(n, p->d_nflags, d_b, p->d_ap, p->d_r64, part);
-    k_sum_part<<<1, 32, 0, s>>>(part, sb, scal);
+  const int chunk = 16;
+  if ((st = capture_mixed_graph(p, chunk))) return st;
+  double rn = 0.0;
+  if ((st = true_residual(p, d_b, d_u, &rn))) return st;
+  double rel = rn / bnorm;
+  int flushes = 0;
+  bool ok = rel <= tol;
+  if (ok) std::snprintf(res->message, sizeof res->message, "Initial guess already converged.");
+  MixState* slot[2] = {(MixState*)((char*)c->pinned + 2048), (MixState*)((char*)c->pinned + 3072)};
+  cudaEvent_t evs[2];
+  cudaEventCreateWithFlags(&evs[0], cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&evs[1], cudaEventDisableTiming);
+  struct EvGuard { cudaEvent_t* e; ~EvGuard() { cudaEventDestroy(e[0]); cudaEventDestroy(e[1]); } } evg{evs};
+  int total_iter = 0;
+  if (!ok) {
+    cudaMemsetAsync(p->f_x, 0, sizeof(float) * n, s);
+    k_mix_init<<<1, 1, 0, s>>>(ms, 0.5 * tol * bnorm, max_iter);
+    k_xr32<<<sb, kT, 0, s>>>(n, p->f_x, p->f_r, p->f_z, p->f_p0, p->f_ap, p->d_invdf, ms, part, 2);
     c->launches += 2;
-    MYCEL_CUDA(c, cudaMemcpyAsync(hsc, scal, sizeof(double), cudaMemcpyDeviceToHost, s));
-    MYCEL_CUDA(c, cudaStreamSynchronize(s));
-    rel = std::sqrt(hsc[0]) / bnorm;
-    if (rel <= tol) {
-      ok = true;
-      break;
-    }
-    if (steps >= max_steps || total_inner >= max_iter || broke) break;
-    if (cancel && *cancel) return set_error(c, MYCEL_E_CANCELLED, "The operation was canceled.");
-    // inner FP32 solve of A d = r64 / ||r64|| to relative accuracy eta
-    double eta = std::max(0.5 * tol / rel, 1e-5);
-    eta = std::min(eta, 0.1);
-    k_scale_to_f32<<<sb, kT, 0, s>>>(n, p->d_r64, scal, p->f_r, p->f_x);
-    k_mix_init<<<1, 1, 0, s>>>(ms, eta, max_iter - total_inner);
-    k_xr32<<<sb, kT, 0, s>>>(n, p->f_x, p->f_r, p->f_z, p->f_p0, p->f_ap, p->d_invdf, ms, part, 1);
-    c->launches += 3;
     int64_t launched = 0;
+    const int64_t cap = (int64_t)max_iter + 64 * chunk + 4096;
+    int iter_at_resume = 0;
     for (;;) {
-      MYCEL_CUDA(c, cudaMemcpyAsync(hms, ms, sizeof(MixState), cudaMemcpyDeviceToHost, s));
+      // pipeline: chunk k is queued while the status after chunk k-1 is read
+      int64_t k = 0;
+      int status = MIX_RUNNING;
+      for (;; ++k) {
+        if (cancel && *cancel) {
+          cudaStreamSynchronize(s);
+          return set_error(c, MYCEL_E_CANCELLED, "The operation was canceled.");
+        }
+        if (launched > cap) {
+          cudaStreamSynchronize(s);
+          return set_error(c, MYCEL_E_TIMEOUT, "inner PCG device state did not reach a final status");
+        }
+        int gi = (int)(k & 1);
+        launch_chunk(p, gi);
+        MYCEL_CUDA(c, cudaGetLastError());
+        launched += chunk;
+        c->launches += 2 * chunk;
+        MYCEL_CUDA(c, cudaMemcpyAsync(slot[gi], ms, sizeof(MixState), cudaMemcpyDeviceToHost, s));
+        MYCEL_CUDA(c, cudaEventRecord(evs[gi], s));
+        if (k == 0) continue;
+        int pi = (int)((k - 1) & 1);
+        MYCEL_CUDA(c, cudaEventSynchronize(evs[pi]));
+        status = slot[pi]->status;
+        if (status != MIX_RUNNING) break;
+        if (c->profile) {  // every iteration of chunk k-1 ran: its first matvec is a full launch
+          float ms_ = 0.f;
+          if (cudaEventElapsedTime(&ms_, p->prof_ev[pi][0], p->prof_ev[pi][1]) == cudaSuccess) {
+            c->prof_ms[0] += ms_;
+            c->prof_n[0] += 1;
+            c->prof_nodes[0] += p->g.nn;
+            c->prof_elems[0] += p->n_active;
+          }
+        }
+      }
       MYCEL_CUDA(c, cudaStreamSynchronize(s));
-      if (hms->status != MIX_RUNNING) break;
-      if (launched > (int64_t)(max_iter - total_inner) + 4 * p->pcg32_graph_chunk)
-        return set_error(c, MYCEL_E_TIMEOUT, "inner PCG device state did not reach a final status");
-      launched += p->pcg32_graph_chunk;
-      if (cancel && *cancel) return set_error(c, MYCEL_E_CANCELLED, "The operation was canceled.");
-      MYCEL_CUDA(c, cudaGraphLaunch(p->pcg32_graph, s));
-      c->launches += 2 * p->pcg32_graph_chunk;
+      MixState* h = slot[0];
+      MYCEL_CUDA(c, cudaMemcpyAsync(h, ms, sizeof(MixState), cudaMemcpyDeviceToHost, s));
+      MYCEL_CUDA(c, cudaStreamSynchronize(s));
+      total_iter = h->iter;
+      status = h->status;
+      // the latest direction is in f_p{(m-1)&1} after m iterations since the chunks restarted
+      int m = total_iter - iter_at_resume;
+      if (m > 0 && (m & 1))
+        MYCEL_CUDA(c, cudaMemcpyAsync(p->f_p1, p->f_p0, sizeof(float) * n, cudaMemcpyDeviceToDevice, s));
+      // reliable update: u += x32; r = P(b - A u) in FP64
+      k_flush_u<<<sb, kT, 0, s>>>(n, d_u, p->f_x);
+      c->launches++;
+      ++flushes;
+      if ((st = true_residual(p, d_b, d_u, &rn))) return st;
+      rel = rn / bnorm;
+      if (rel <= tol) {
+        ok = true;
+        break;
+      }
+      if (status != MIX_FLUSH || total_iter >= max_iter) break;
+      k_xr32<<<sb, kT, 0, s>>>(n, p->f_x, p->f_r, p->f_z, p->f_p0, p->f_ap, p->d_invdf, ms, part, 1);
+      c->launches++;
+      iter_at_resume = total_iter;
     }
-    total_inner += hms->iter;
-    if (hms->status == MIX_BREAKDOWN && hms->iter == 0) broke = true;
-    k_axpy_u<<<sb, kT, 0, s>>>(n, d_u, p->f_x, scal);
-    c->launches++;
-    ++steps;
   }
-  res->iterations = total_inner;
-  res->inner_iterations = total_inner;
-  res->refinement_steps = steps;
+  res->iterations = total_iter;
+  res->inner_iterations = total_iter;
+  res->refinement_steps = flushes;
   res->final_residual = rel;
   res->converged = ok ? 1 : 0;
   if (!ok)

@@ -18,6 +18,7 @@
 //                   neighbour order (jz, jy, jx ascending), weights (rmin - dist) * invHs_row.
 //   k_sens          SensitivityAnalysis (Optimization/SensitivityAnalysis.cs:98-144).
 //   k_oc            OcOptimizer.Update (Optimization/OcOptimizer.cs:12-175): one persistent cooperative kernel.
+#include <algorithm>
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <math.h>
@@ -229,65 +230,133 @@ void launch_diag(mycel_problem* p) {
 
 // ---------------------------------------------------------------------------------------------------------
 // y = K x (projected: y = x on constrained DOFs, ApplyA with xIsAlreadyProjected)
+// z-marching shared-memory tiles: a CTA owns 64 x 4 nodes and marches over ZSEG node planes; three planes of x
+// (one-node halo) and two element planes of E and the domain live in shared memory. Warp w handles the nodes
+// of one parity in x (i = i0 + 2 lane + (w & 1)) of row j0 + (w >> 1), so the colour order of the incident
+// elements, and the KE rows they read, are the same for the whole warp. The shared planes are stored
+// parity-split in x, so a warp's 8-byte loads hit consecutive words.
 // ---------------------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_matvec64(GridDims g, const __grid_constant__ KeD ke, const double* __restrict__ x,
-                                                  double* __restrict__ y, const double* __restrict__ E,
-                                                  const uint8_t* __restrict__ dom, const uint8_t* __restrict__ nf,
-                                                  int projected, int mode, const int* __restrict__ status) {
+constexpr int MX = 64, MY = 4;
+constexpr int MPX = MX + 2, MPY = MY + 2;   // node plane with halo
+constexpr int MEX = MX + 1, MEY = MY + 1;   // element plane
+constexpr int MPXH = (MPX + 1) / 2, MEXH = (MEX + 1) / 2;
+
+__device__ __forceinline__ int psplit(int lx, int half) { return (lx & 1) * half + (lx >> 1); }
+
+__global__ void __launch_bounds__(256) k_matvec64(GridDims g, const __grid_constant__ KeD ke,
+                                                  const double* __restrict__ x, double* __restrict__ y,
+                                                  const double* __restrict__ E, const uint8_t* __restrict__ dom,
+                                                  const uint8_t* __restrict__ nf, int projected, int mode,
+                                                  const int* __restrict__ status, int zseg) {
+  __shared__ double xs[3][3][MPY][2 * MPXH];  // [slot][c][ly][parity-split lx]
+  __shared__ double es[2][MEY][2 * MEXH];
+  __shared__ uint8_t ds[2][MEY][2 * MEXH];
   if (status && *status != PCG_RUNNING) return;
-  ClassNode cn = class_node(g, blockIdx.y, blockIdx.x * (int64_t)blockDim.x + threadIdx.x);
-  if (!cn.valid) return;
-  const int64_t sx = 1, sy = g.nx1, sz = (int64_t)g.nx1 * g.ny1;
-  double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
-#pragma unroll 1
-  for (int col = 0; col < 8; ++col) {
-    int ox = (col & 1) ^ cn.px, oy = ((col >> 1) & 1) ^ cn.py, oz = ((col >> 2) & 1) ^ cn.pz;
-    int ie = cn.i - ox, je = cn.j - oy, kk = cn.k - oz;
-    if (ie < 0 || ie >= g.nx || je < 0 || je >= g.ny || kk < 0 || kk >= g.nz) continue;
-    int64_t e = ie + (int64_t)g.nx * (je + (int64_t)g.ny * kk);
-    if (!__ldg(dom + e)) continue;
-    double ee = __ldg(E + e);
-    int64_t n0 = ie + sy * je + sz * kk;
-    const int64_t off[8] = {0, sx, sx + sy, sy, sz, sz + sx, sz + sx + sy, sz + sy};
-    double ue[24];
-#pragma unroll
-    for (int b = 0; b < 8; ++b) {
-      const double* xp = x + 3 * (n0 + off[b]);
-      ue[3 * b] = __ldg(xp) * ee;
-      ue[3 * b + 1] = __ldg(xp + 1) * ee;
-      ue[3 * b + 2] = __ldg(xp + 2) * ee;
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int px = w & 1, ty = w >> 1;
+  const int i0 = blockIdx.x * MX, j0 = blockIdx.y * MY, k0 = blockIdx.z * zseg;
+  const int k1 = min(k0 + zseg, g.nz1);
+  const int64_t sy = g.nx1, sz = (int64_t)g.nx1 * g.ny1;
+
+  auto load_plane = [&](int kk, int slot) {
+    for (int q = tid; q < MPY * MPX * 3; q += 256) {
+      int c = q % 3, rest = q / 3, lx = rest % MPX, ly = rest / MPX;
+      int i = i0 - 1 + lx, j = j0 - 1 + ly;
+      double v = 0.0;
+      if (kk >= 0 && kk < g.nz1 && i >= 0 && i < g.nx1 && j >= 0 && j < g.ny1) v = __ldg(x + 3 * (i + sy * j + sz * kk) + c);
+      xs[slot][c][ly][psplit(lx, MPXH)] = v;
     }
-    const int a = local_index(ox, oy, oz);
-    double res[3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const double* row = ke.v + (3 * a + c) * 24;
-      double l[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        double s = row[q] * ue[q] + row[4 + q] * ue[4 + q];
-        s = s + row[8 + q] * ue[8 + q];
-        s = s + row[12 + q] * ue[12 + q];
-        s = s + row[16 + q] * ue[16 + q];
-        s = s + row[20 + q] * ue[20 + q];
-        l[q] = s;
+  };
+  auto load_eplane = [&](int ke_, int slot) {
+    for (int q = tid; q < MEY * MEX; q += 256) {
+      int lx = q % MEX, ly = q / MEX;
+      int ie = i0 - 1 + lx, je = j0 - 1 + ly;
+      double v = 0.0;
+      uint8_t d = 0;
+      if (ke_ >= 0 && ke_ < g.nz && ie >= 0 && ie < g.nx && je >= 0 && je < g.ny) {
+        int64_t e = ie + (int64_t)g.nx * (je + (int64_t)g.ny * ke_);
+        d = __ldg(dom + e);
+        if (d) v = __ldg(E + e);
       }
-      res[c] = lane_sum(mode, l[0], l[1], l[2], l[3]);
+      es[slot][ly][psplit(lx, MEXH)] = v;
+      ds[slot][ly][psplit(lx, MEXH)] = d;
     }
-    acc0 = acc0 + res[0];
-    acc1 = acc1 + res[1];
-    acc2 = acc2 + res[2];
-  }
-  int64_t n = cn.i + sy * cn.j + sz * cn.k;
-  double out[3] = {acc0, acc1, acc2};
-  uint8_t f = projected ? nf[n] : 0;
+  };
+
+  load_plane(k0 - 1, (k0 + 2) % 3);
+  load_plane(k0, k0 % 3);
+  load_eplane(k0 - 1, (k0 + 1) & 1);
+  const int lxn = 1 + 2 * lane + px;  // plane-local x of this thread's node
+  const int i = i0 + lxn - 1, j = j0 + ty;
+  const bool mine = i < g.nx1 && j < g.ny1;
+  for (int k = k0; k < k1; ++k) {
+    load_plane(k + 1, (k + 1) % 3);
+    load_eplane(k, k & 1);
+    __syncthreads();
+    if (mine) {
+      double acc[3] = {0.0, 0.0, 0.0};
+#pragma unroll 1
+      for (int col = 0; col < 8; ++col) {
+        // node offset inside the element of colour col, and the element's local position
+        const int ox = (col & 1) ^ (i & 1), oy = ((col >> 1) & 1) ^ (j & 1), oz = ((col >> 2) & 1) ^ (k & 1);
+        const int sx = 1 - ox, sy_ = 1 - oy, sz_ = 1 - oz;  // element offset from (i-1, j-1, k-1)
+        const int lxe = lxn - 1 + sx, lye = ty + sy_;      // element plane coordinates
+        const int eslot = (k - 1 + sz_) & 1;
+        const uint8_t act = ds[eslot][lye][psplit(lxe, MEXH)];
+        if (!act) continue;  // outside the grid or inactive: no contribution
+        const double ee = es[eslot][lye][psplit(lxe, MEXH)];
+        double ue[24];
 #pragma unroll
-  for (int c = 0; c < 3; ++c) y[3 * n + c] = (f & (1 << c)) ? x[3 * n + c] : out[c];
+        for (int b = 0; b < 8; ++b) {
+          const int bx = (b == 1 || b == 2 || b == 5 || b == 6) ? 1 : 0;
+          const int by = (b == 2 || b == 3 || b == 6 || b == 7) ? 1 : 0;
+          const int bz = b >= 4 ? 1 : 0;
+          const int slot = (k - 1 + sz_ + bz + 3) % 3;
+          const int lx = lxn - 1 + sx + bx, ly = ty + sy_ + by;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) ue[3 * b + c] = xs[slot][c][ly][psplit(lx, MPXH)] * ee;
+        }
+        const int a = (oy ? (ox ? 2 : 3) : (ox ? 1 : 0)) + 4 * oz;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const double* row = ke.v + (3 * a + c) * 24;
+          double l[4];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            double s = row[q] * ue[q] + row[4 + q] * ue[4 + q];
+            s = s + row[8 + q] * ue[8 + q];
+            s = s + row[12 + q] * ue[12 + q];
+            s = s + row[16 + q] * ue[16 + q];
+            s = s + row[20 + q] * ue[20 + q];
+            l[q] = s;
+          }
+          acc[c] = acc[c] + lane_sum(mode, l[0], l[1], l[2], l[3]);
+        }
+      }
+      const int64_t n = i + sy * j + sz * k;
+      const uint8_t f = projected ? nf[n] : 0;
+      const int cslot = k % 3;
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        y[3 * n + c] = (f & (1 << c)) ? xs[cslot][c][ty + 1][psplit(lxn, MPXH)] : acc[c];
+    }
+    __syncthreads();
+  }
+}
+
+// z-segment length giving about 8 CTAs per SM (at least 2 planes per segment)
+inline int matvec64_zseg(const GridDims& g, int num_sms) {
+  int64_t txy = (int64_t)((g.nx1 + MX - 1) / MX) * ((g.ny1 + MY - 1) / MY);
+  int64_t segs = std::max<int64_t>(1, (8 * (int64_t)num_sms + txy - 1) / txy);
+  return (int)std::max<int64_t>(2, (g.nz1 + segs - 1) / segs);
 }
 
 void launch_matvec64(mycel_problem* p, const double* x, double* y, int projected, const int* d_status) {
-  k_matvec64<<<class_grid(p->g, 256), 256, 0, p->ctx->stream>>>(p->g, p->ke, x, y, p->d_E, p->d_domain,
-                                                                p->d_nflags, projected, p->lane_mode, d_status);
+  const GridDims& g = p->g;
+  int zs = matvec64_zseg(g, p->ctx->num_sms);
+  dim3 grid((unsigned)((g.nx1 + MX - 1) / MX), (unsigned)((g.ny1 + MY - 1) / MY), (unsigned)((g.nz1 + zs - 1) / zs));
+  k_matvec64<<<grid, 256, 0, p->ctx->stream>>>(g, p->ke, x, y, p->d_E, p->d_domain, p->d_nflags, projected,
+                                               p->lane_mode, d_status, zs);
   p->ctx->launches++;
 }
 
@@ -586,10 +655,10 @@ void launch_pcg_init_z(mycel_problem* p) {
 }
 
 // One PCG iteration (PcgSolver.cs:235-357): Ap = A p; pAp, alpha; x, r, ||r||; z, rho1, beta; p = z + beta p.
-void launch_pcg_iteration(mycel_problem* p) {
+void launch_pcg_iteration(mycel_problem* p, bool skip_matvec) {
   cudaStream_t s = p->ctx->stream;
   int64_t nb = num_blocks8192(p->g.nd);
-  launch_matvec64(p, p->d_p, p->d_ap, 1, &p->d_state->status);
+  if (!skip_matvec) launch_matvec64(p, p->d_p, p->d_ap, 1, &p->d_state->status);
   k_dot_exact<<<(unsigned)nb, kDotThreads, 0, s>>>(p->d_p, p->d_ap, p->g.nd, p->d_part, p->d_state, p->lane_mode,
                                                    PH_PAP);
   k_xr_exact<<<(unsigned)nb, kDotThreads, 0, s>>>(p->d_x, p->d_r, p->d_z, p->d_p, p->d_ap, p->d_invd, p->g.nd,
@@ -842,8 +911,14 @@ int filter_setup(mycel_filter* f) {
   k_filter_invhs<<<nb, 128, 0, s>>>(p->g, p->d_domain, f->d_off, f->d_w, f->n_off, f->d_invhs);
   k_filter_apply<1><<<nb, 128, 0, s>>>(p->g, p->d_domain, f->d_off, f->d_w, f->n_off, f->d_invhs, nullptr, f->d_s, 1);
   p->ctx->launches += 2;
-  cudaStreamSynchronize(s);  // host vectors above must outlive the copies
-  return cudaGetLastError() == cudaSuccess ? MYCEL_OK : MYCEL_E_DEVICE;
+  cudaError_t le = cudaGetLastError();
+  cudaError_t se = cudaStreamSynchronize(s);  // host vectors above must outlive the copies
+  if (le != cudaSuccess || se != cudaSuccess) {
+    set_error(p->ctx, MYCEL_E_DEVICE, std::string("filter set-up: ") +
+                                          cudaGetErrorString(le != cudaSuccess ? le : se));
+    return MYCEL_E_DEVICE;
+  }
+  return MYCEL_OK;
 }
 
 void launch_filter_fwd(mycel_filter* f, const double* in_box, double* out_box) {

@@ -77,6 +77,12 @@ struct mycel_ctx {
   std::string last_error;
   void* pinned = nullptr;  // small pinned scratch for scalar readbacks
   size_t pinned_bytes = 0;
+  // optional live timing of the dominant kernel (CUDA events captured around one matvec per PCG chunk)
+  int profile = 0;
+  double prof_ms[4] = {0, 0, 0, 0};  // [0] FP32 matvec, [1] FP64 matvec
+  int64_t prof_n[4] = {0, 0, 0, 0};
+  int64_t prof_nodes[4] = {0, 0, 0, 0};     // nodes processed by the timed launches
+  int64_t prof_elems[4] = {0, 0, 0, 0};     // active elements processed by the timed launches
 };
 
 struct mycel_problem {
@@ -125,11 +131,14 @@ struct mycel_problem {
   double* d_tmp0 = nullptr;       // [nd]
   double* d_tmp1 = nullptr;       // [nd]
   int lane_mode = 0;
-  cudaGraphExec_t pcg_graph = nullptr;
+  cudaGraphExec_t pcg_graph[2] = {nullptr, nullptr};
   int pcg_graph_chunk = 0;
-  cudaGraphExec_t pcg32_graph = nullptr;
+  cudaEvent_t prof64_ev[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+  cudaGraphExec_t pcg32_graph[2] = {nullptr, nullptr};
   int pcg32_graph_chunk = 0;
-  int pcg32_graph_parity = -1;
+  int pcg32_graph_profiled = 0;
+  cudaEvent_t prof_ev[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+  int pcg_graph_profiled = 0;
 };
 
 struct mycel_filter {
@@ -167,7 +176,7 @@ void launch_pcg_bnorm(mycel_problem* p);
 void launch_pcg_init_r(mycel_problem* p, int nonzero);
 void launch_pcg_dot_rr(mycel_problem* p);
 void launch_pcg_init_z(mycel_problem* p);
-void launch_pcg_iteration(mycel_problem* p);
+void launch_pcg_iteration(mycel_problem* p, bool skip_matvec = false);
 void launch_compliance(mycel_problem* p, const double* u, double* d_out);
 void launch_max_disp(mycel_problem* p, const double* u, double* d_out);
 void launch_reactions(mycel_problem* p, const double* ku, double* out, const int32_t* d_fixed, int32_t n_fixed);

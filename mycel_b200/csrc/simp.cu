@@ -95,6 +95,7 @@ extern "C" int32_t mycel_simp_begin(mycel_problem* p, const mycel_simp_options* 
   *out = nullptr;
   mycel_ctx* c = p->ctx;
   cudaSetDevice(c->device);
+  (void)cudaGetLastError();  // do not report a stale error of an earlier, unrelated call
   cudaStream_t st = c->stream;
   const GridDims& g = p->g;
   mycel_simp_session* s = new mycel_simp_session();
@@ -196,6 +197,11 @@ extern "C" int32_t mycel_simp_begin(mycel_problem* p, const mycel_simp_options* 
   else
     cudaMemsetAsync(s->d_u, 0, sizeof(double) * g.nd, st);
   for (auto& e : s->ev) cudaEventCreate(&e);
+  cudaError_t pe = cudaGetLastError();
+  if (pe != cudaSuccess) {
+    mycel_simp_end(s);
+    return set_error(c, MYCEL_E_DEVICE, std::string("SIMP set-up: ") + cudaGetErrorString(pe));
+  }
   rc = mycel_filter_create(p, s->rmin, &s->filt);
   if (rc) {
     mycel_simp_end(s);

@@ -1,0 +1,67 @@
+"""Mixed-precision form (FP32 inner PCG, FP64 refinement) against the FP64 oracle.
+
+Tolerances (stated): FP32 matvec within 2e-6 of max|K x| (FP32 accumulation of 24-term rows over 8 elements);
+solves to the same FP64 residual tolerance agree in compliance to 1e-8 relative and in u to 1e-6 of max|u|;
+the SIMP loop agrees in compliance to 1e-6 relative per iteration.
+"""
+import numpy as np
+import pytest
+
+from mycel_b200 import api
+from mycel_b200 import workloads as W
+from mycel_b200.model import StaticAnalysisOptions
+from models import carved_model, tiny_test_model
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(autouse=True)
+def exact_oracle(oracle):
+    oracle.set_modes(0, 1, threads=8)
+    yield
+    oracle.set_modes(0, 0)
+
+
+@pytest.mark.parametrize("shape", [(1, 1, 1), (5, 3, 2), (33, 17, 9), (70, 9, 20)])
+def test_fp32_matvec_close_to_fp64(oracle, ctx, shape):
+    m = carved_model(*shape, seed=3, frac=0.15) if shape[0] > 2 else tiny_test_model(*shape)
+    om, pr = oracle.Model(m), api.Problem(m, ctx)
+    x = np.random.default_rng(2).uniform(-1, 1, m.total_dofs)
+    y64 = om.apply_k(x)
+    y32 = pr.apply_k(x, precision="mixed")
+    assert np.abs(y32 - y64).max() <= 2e-6 * np.abs(y64).max()
+    xp = x * (om.constrained() == 0)
+    assert np.abs(pr.apply_k(xp, True, "mixed") - om.apply_a(xp)).max() <= 2e-6 * np.abs(y64).max()
+
+
+def test_mixed_static_solve_matches_fp64(oracle, ctx):
+    m = carved_model(24, 10, 8, seed=5, emin_ratio=1e-9)
+    ref = oracle.static_run(m, 1e-10, 20000)
+    r = api.StaticAnalysis.run(m, StaticAnalysisOptions(tolerance=1e-10, max_iterations=20000, precision="mixed"), ctx)
+    assert r.solver_info.converged and r.solver_info.final_residual <= 1e-10
+    assert abs(r.compliance - ref.compliance) <= 1e-8 * abs(ref.compliance)
+    assert np.abs(r.u - ref.u).max() <= 1e-6 * np.abs(ref.u).max()
+    assert np.array_equal(r.u[m.fixed_dofs], np.zeros(m.fixed_dofs.size))
+
+
+def test_mixed_warm_start_and_zero_rhs(ctx):
+    m = tiny_test_model()
+    pr = api.Problem(m, ctx)
+    b = pr.forces()
+    u1, r1 = pr.pcg_solve(b, tol=1e-9, precision="mixed")
+    u2, r2 = pr.pcg_solve(b, x0=u1, tol=1e-9, precision="mixed")
+    assert r1.converged and r2.converged and r2.iterations <= 2
+    u0, r0 = pr.pcg_solve(np.zeros(m.total_dofs), x0=np.ones(m.total_dofs), precision="mixed")
+    assert r0.converged and not u0.any()
+
+
+def test_mixed_simp_cantilever_within_1e6(oracle, ctx):
+    m, o = W.simp_cantilever_40x20x10()
+    o = o.replace(max_iterations=12)
+    ref = oracle.topopt_run(m, o)
+    res = api.TopologyOptimizer.run(m, o.replace(precision="mixed"), ctx=ctx)
+    assert res.total_iterations == ref.n_iters
+    for a, b in zip(res.snapshots, ref.records):
+        assert abs(a.compliance - b["compliance"]) <= 1e-6 * abs(b["compliance"])
+        assert a.solver_residual <= 1e-8
+    assert np.abs(res.final_physical_density - ref.phys).max() <= 1e-5
