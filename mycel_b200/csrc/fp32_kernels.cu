@@ -95,16 +95,30 @@ __device__ __forceinline__ double warp_sum_parts(const double* part, unsigned n)
 constexpr int TX = 32, TY = 8;
 constexpr int PX = TX + 2, PY = TY + 2;  // node plane with halo
 constexpr int EX = TX + 1, EY = TY + 1;  // element plane
+constexpr int ROWF = 3 * PX;             // floats per node row of a plane (contiguous in global memory)
+constexpr int NSLOT = 4;                 // rolling node planes: k-1, k, k+1 in use, k+2 arriving
+constexpr int NESLOT = 3;                // rolling element planes: k-1, k in use, k+1 arriving
+
+// Plane loader: warp w copies rows w and w + 8 of a plane (3 * PX contiguous floats each), lane l the offsets
+// l, l+32, l+64, l+96 of a row. Everything that does not depend on the plane index is computed once.
+struct RowLoad {
+  int nrows;         // 1 or 2
+  int ly[2];
+  int64_t gofs[2];   // global float offset of (row start + lane) at plane 0 (may be negative at i = -1)
+  unsigned rowok;    // bit q: row q exists and lies in the grid in y
+  unsigned xmask;    // bit r: offset lane + 32 r lies in the grid in x (and < ROWF)
+  unsigned own;      // bit 4 * row + r: interior node of an owned row (written back as p_t)
+};
 
 template <int MODE>
-__global__ void __launch_bounds__(TX * TY, 2) k_mv32(GridDims g, const __grid_constant__ KeF ke,
+__global__ void __launch_bounds__(TX * TY, 3) k_mv32(GridDims g, const __grid_constant__ KeF ke,
                                                      const float* __restrict__ xin, const float* __restrict__ z,
                                                      const float* __restrict__ pold, float* __restrict__ pnew,
                                                      float* __restrict__ y, const float* __restrict__ E,
                                                      const uint8_t* __restrict__ nf, int projected, MixState* st,
                                                      double* part, int zseg) {
-  __shared__ float xs[3][PY][PX][3];
-  __shared__ float es[2][EY][EX];
+  __shared__ float4 xs[NSLOT][PY][PX];  // node planes, one float4 per node (w unused)
+  __shared__ float es[NESLOT][EY][EX];
   __shared__ double sh[32];
   if (MODE == 1 && st->status != MIX_RUNNING) return;
   const float beta = MODE == 1 ? (float)st->beta : 0.0f;
@@ -113,63 +127,151 @@ __global__ void __launch_bounds__(TX * TY, 2) k_mv32(GridDims g, const __grid_co
   const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY, k0 = blockIdx.z * zseg;
   const int k1 = min(k0 + zseg, g.nz1);
   const int64_t sy = g.nx1, sz = (int64_t)g.nx1 * g.ny1;
+  const int64_t plane_f = 3 * sz;  // floats per node plane
 
-  // load node plane kk into slot; owned interior nodes of owned planes write p_t
-  auto load_plane = [&](int kk, int slot) {
-    const bool owned_plane = kk >= k0 && kk < k1;
-    for (int q = tid; q < PY * PX * 3; q += TX * TY) {
-      int c = q % 3, rest = q / 3, lx = rest % PX, ly = rest / PX;
-      int i = i0 - 1 + lx, j = j0 - 1 + ly;
-      float v = 0.f;
-      if (kk >= 0 && kk < g.nz1 && i >= 0 && i < g.nx1 && j >= 0 && j < g.ny1) {
-        int64_t idx = 3 * (i + sy * j + sz * kk) + c;
-        if (MODE == 1) {
-          v = first ? __ldg(z + idx) : fmaf(beta, __ldg(pold + idx), __ldg(z + idx));
-          if (owned_plane && lx >= 1 && lx <= TX && ly >= 1 && ly <= TY) pnew[idx] = v;
-        } else {
-          v = __ldg(xin + idx);
+  // ---- per-thread load plan (node rows) ----
+  RowLoad rl;
+  rl.nrows = (ty + 8 < PY) ? 2 : 1;
+  rl.xmask = 0;
+  rl.own = 0;
+  rl.rowok = 0;
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    int off = tx + 32 * r;
+    int lx = off / 3;
+    int i = i0 - 1 + lx;
+    if (off < ROWF && i >= 0 && i < g.nx1) rl.xmask |= 1u << r;
+  }
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    int ly = ty + 8 * q;
+    rl.ly[q] = ly;
+    int j = j0 - 1 + ly;
+    bool ok = q < rl.nrows && j >= 0 && j < g.ny1;
+    rl.gofs[q] = 3 * ((int64_t)(i0 - 1) + sy * j) + tx;
+    if (ok) rl.rowok |= 1u << q;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      int off = tx + 32 * r, lx = off / 3;
+      if (ok && (rl.xmask >> r & 1) && ly >= 1 && ly <= TY && lx >= 1 && lx <= TX) rl.own |= 1u << (4 * q + r);
+    }
+  }
+  // element plane: warp w copies element row w (row 8 by warp 0); lane l the elements l and 32 (lane 0)
+  const int erows = (ty == 0) ? 2 : 1;
+  int64_t eofs[2];
+  unsigned emask = 0;
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    int ly = ty + 8 * q;
+    int je = j0 - 1 + ly;
+    bool ok = q < erows && je >= 0 && je < g.ny;
+    eofs[q] = (int64_t)(i0 - 1) + tx + (int64_t)g.nx * je;  // element (i0-1+tx, je) at element plane 0
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      int lx = tx + 32 * r, ie = i0 - 1 + lx;
+      if (ok && lx < EX && ie >= 0 && ie < g.nx) emask |= 1u << (2 * q + r);
+    }
+  }
+  const int64_t eplane = (int64_t)g.nx * g.ny;
+
+  float pre[2][4];   // prefetched node-plane values (z, or x for MODE 0)
+  float prep[2][4];  // prefetched p_{t-1} (MODE 1); p_t = z + beta p_{t-1} is formed at commit time
+  float epre[2][2];
+  auto fetch = [&](int kk) {
+    const bool inz = kk >= 0 && kk < g.nz1;
+#pragma unroll
+    for (int q = 0; q < 2; ++q)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        float v = 0.f, w = 0.f;
+        if (inz && (rl.rowok >> q & 1) && (rl.xmask >> r & 1)) {
+          int64_t idx = rl.gofs[q] + plane_f * kk + 32 * r;
+          if (MODE == 1) {
+            v = __ldg(z + idx);
+            if (!first) w = __ldg(pold + idx);
+          } else {
+            v = __ldg(xin + idx);
+          }
         }
+        pre[q][r] = v;
+        prep[q][r] = w;
       }
-      xs[slot][ly][lx][c] = v;
+  };
+  auto commit = [&](int kk) {
+    const int slot = (kk + NSLOT) % NSLOT;
+    const bool owned_plane = kk >= k0 && kk < k1;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      if (q >= rl.nrows) break;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        int off = tx + 32 * r;
+        const float v = (MODE == 1 && !first) ? fmaf(beta, prep[q][r], pre[q][r]) : pre[q][r];
+        if (off < ROWF) reinterpret_cast<float*>(&xs[slot][rl.ly[q]][0])[4 * (off / 3) + off % 3] = v;
+        if (MODE == 1 && owned_plane && (rl.own >> (4 * q + r) & 1))
+          pnew[rl.gofs[q] + plane_f * kk + 32 * r] = v;
+      }
     }
   };
-  auto load_eplane = [&](int ke_, int slot) {
-    for (int q = tid; q < EY * EX; q += TX * TY) {
-      int lx = q % EX, ly = q / EX;
-      int ie = i0 - 1 + lx, je = j0 - 1 + ly;
-      float v = 0.f;
-      if (ke_ >= 0 && ke_ < g.nz && ie >= 0 && ie < g.nx && je >= 0 && je < g.ny)
-        v = __ldg(E + ie + (int64_t)g.nx * (je + (int64_t)g.ny * ke_));
-      es[slot][ly][lx] = v;
+  auto efetch = [&](int ke_) {
+    const bool inz = ke_ >= 0 && ke_ < g.nz;
+#pragma unroll
+    for (int q = 0; q < 2; ++q)
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        float v = 0.f;
+        if (inz && (emask >> (2 * q + r) & 1)) v = __ldg(E + eofs[q] + eplane * ke_ + 32 * r);
+        epre[q][r] = v;
+      }
+  };
+  auto ecommit = [&](int ke_) {
+    const int slot = (ke_ + NESLOT) % NESLOT;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      if (q >= erows) break;
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        int lx = tx + 32 * r;
+        if (lx < EX) es[slot][ty + 8 * q][lx] = epre[q][r];
+      }
     }
   };
 
-  load_plane(k0 - 1, (k0 + 2) % 3);
-  load_plane(k0, k0 % 3);
-  load_eplane(k0 - 1, (k0 + 1) & 1);
+  // prologue: planes k0-1, k0, k0+1 and element planes k0-1, k0 in shared memory; plane k0+2 in flight
+  fetch(k0 - 1); commit(k0 - 1);
+  fetch(k0); commit(k0);
+  fetch(k0 + 1); commit(k0 + 1);
+  efetch(k0 - 1); ecommit(k0 - 1);
+  efetch(k0); ecommit(k0);
+  __syncthreads();
   const int i = i0 + tx, j = j0 + ty;
   const bool mine = i < g.nx1 && j < g.ny1;
   double pap = 0.0;
   for (int k = k0; k < k1; ++k) {
-    load_plane(k + 1, (k + 1) % 3);
-    load_eplane(k, k & 1);
-    __syncthreads();
+    const bool more = k + 1 < k1;
+    if (more) {
+      fetch(k + 2);
+      efetch(k + 1);
+    }
     if (mine) {
       float xn[3][3][3][3];  // [dz][dy][dx][c], offsets -1..+1
 #pragma unroll
       for (int dz = 0; dz < 3; ++dz) {
-        const int slot = (k - 1 + dz + 3) % 3;
+        const int slot = (k - 1 + dz + NSLOT) % NSLOT;
 #pragma unroll
         for (int dy = 0; dy < 3; ++dy)
 #pragma unroll
-          for (int dx = 0; dx < 3; ++dx)
-#pragma unroll
-            for (int c = 0; c < 3; ++c) xn[dz][dy][dx][c] = xs[slot][ty + dy][tx + dx][c];
+          for (int dx = 0; dx < 3; ++dx) {
+            const float4 v4 = xs[slot][ty + dy][tx + dx];
+            xn[dz][dy][dx][0] = v4.x;
+            xn[dz][dy][dx][1] = v4.y;
+            xn[dz][dy][dx][2] = v4.z;
+          }
       }
       float acc0 = 0.f, acc1 = 0.f, acc2 = 0.f;
 #pragma unroll
       for (int sz_ = 0; sz_ < 2; ++sz_) {
-        const int eslot = (k - 1 + sz_) & 1;
+        const int eslot = (k - 1 + sz_ + NESLOT) % NESLOT;
 #pragma unroll
         for (int sy_ = 0; sy_ < 2; ++sy_)
 #pragma unroll
@@ -207,6 +309,10 @@ __global__ void __launch_bounds__(TX * TY, 2) k_mv32(GridDims g, const __grid_co
         y[3 * n + c] = yv;
         if (MODE == 1) pap += (double)pv * (double)yv;
       }
+    }
+    if (more) {
+      commit(k + 2);   // slot (k+2)%4 held plane k-2: no longer read
+      ecommit(k + 1);  // slot (k+1)%3 held element plane k-2
     }
     __syncthreads();
   }
