@@ -46,6 +46,10 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-sample-iters", type=int, default=6)
+    ap.add_argument("--probe", choices=["mixed", "fp64"], default=None,
+                    help="kernel probe for profilers: one PCG solve of --probe-iters iterations on a bridge grid")
+    ap.add_argument("--probe-grid", default="96x48x48")
+    ap.add_argument("--probe-iters", type=int, default=40)
     return ap.parse_args()
 
 
@@ -353,9 +357,22 @@ def run_reference(args):
     print(json.dumps(out), flush=True)
 
 
+def run_probe(args):
+    """A short PCG solve (fixed iteration count) on a bridge grid: the case the ncu captures in profiles/ use."""
+    from mycel_b200 import api, workloads as W
+    nx, ny, nz = (int(v) for v in args.probe_grid.split("x"))
+    ctx = api.Context(0)
+    pr = api.Problem(W.bridge(nx, ny, nz), ctx)
+    u, r = pr.pcg_solve(pr.forces(), tol=1e-30, max_iterations=args.probe_iters, precision=args.probe)
+    print(json.dumps({"probe": args.probe, "grid": args.probe_grid, "iterations": r.iterations,
+                      "elapsed_ms": r.elapsed_ms}))
+
+
 if __name__ == "__main__":
     a = parse()
-    if a.impl == "reference":
+    if a.probe:
+        run_probe(a)
+    elif a.impl == "reference":
         run_reference(a)
     else:
         run_mycel(a)
