@@ -190,6 +190,19 @@ int32_t mycel_oc_update(mycel_ctx* ctx, int32_t n, const double* rho, const doub
                         double rho_min, double lambda_guess, int32_t max_bisection_steps, double volume_tolerance,
                         double* lambda_out);
 
+/* OC update that allocates no device memory. No counterpart in the reference: it is for callers that cannot
+   allocate device memory when they run this step (a host whose device memory is all reserved by another
+   allocator in the process, or a loop that must not take the synchronisation of a cudaMalloc/cudaFree).
+   rho, dc, s, passive (may be NULL) and rho_new are device pointers owned by the caller; lambda_out is a host
+   pointer. The kernel's scratch is a fixed 65.7 KB array inside the library, held by every GPU that loads it
+   until the process exits, sized for 1024 persistent blocks (devices that need more return MYCEL_E_ARG).
+   The first call on a device looks up that array's device address, so make it before any stream capture.
+   All calls share the array: calls that overlap on the GPU (other streams, other threads) race. */
+int32_t mycel_oc_update_noalloc(mycel_ctx* ctx, int32_t n, const double* rho, const double* dc, const double* s,
+                                const uint8_t* passive, double* rho_new, double target_volume_fraction,
+                                double move_limit, double rho_min, double lambda_guess, int32_t max_bisection_steps,
+                                double volume_tolerance, double* lambda_out);
+
 /* ---- SIMP loop: TopologyOptimizer.Run (Optimization/TopologyOptimizer.cs:16-407) ----
    cancel / pause: polled between iterations (CancellationToken, IterationController.CheckAndBlock);
    history: room for history_cap records; u_out (total_dofs), physical/design_density_out (box, float) may

@@ -92,6 +92,7 @@ SIGNATURES = {
     "mycel_filter_s": (i32, [P, P]),
     "mycel_sensitivities": (i32, [P, P, P, dbl, P]),
     "mycel_oc_update": (i32, [P, i32, P, P, P, P, P, dbl, dbl, dbl, dbl, i32, dbl, C.POINTER(dbl)]),
+    "mycel_oc_update_noalloc": (i32, [P, i32, P, P, P, P, P, dbl, dbl, dbl, dbl, i32, dbl, C.POINTER(dbl)]),
     "mycel_simp_run": (i32, [P, C.POINTER(SimpOptions), PROGRESS_FN, P, P, P, C.POINTER(IterRecord), i32,
                              C.POINTER(i32), C.POINTER(i32), P, P, P]),
     "mycel_simp_begin": (i32, [P, C.POINTER(SimpOptions), C.POINTER(P)]),

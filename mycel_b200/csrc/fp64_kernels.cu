@@ -19,6 +19,8 @@
 //   k_sens          SensitivityAnalysis (Optimization/SensitivityAnalysis.cs:98-144).
 //   k_oc            OcOptimizer.Update (Optimization/OcOptimizer.cs:12-175): one persistent cooperative kernel.
 #include <algorithm>
+#include <mutex>
+#include <string>
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <math.h>
@@ -1223,4 +1225,74 @@ int launch_oc(mycel_ctx* ctx, int64_t n, const int32_t* d_index, const double* r
   return MYCEL_OK;
 }
 
+// ---------------------------------------------------------------------------------------------------------
+// OC update without device allocation.
+// Some callers cannot allocate device memory at the time they run the OC step: a host whose device memory is
+// reserved in full by another allocator in the same process (a caching allocator or a fixed pool), or a loop
+// that must not pay the device-wide synchronisation a cudaMalloc/cudaFree pair can cost. This entry point
+// takes the caller's device buffers and keeps the OC kernel's scratch (block partials, barrier words, result)
+// in the file-scope array below, which every GPU that loads the library holds until the process exits.
+// ---------------------------------------------------------------------------------------------------------
+constexpr int kOcNoAllocMaxBlocks = 1024;                                // persistent OC blocks it can serve
+constexpr int kOcNoAllocScratch = 8 * kOcNoAllocMaxBlocks + 8;           // partials + barrier words + error flag
+constexpr int kOcNoAllocOut = (int)((sizeof(OcOut) + sizeof(double) - 1) / sizeof(double));
+static __device__ __align__(256) double g_oc_noalloc[kOcNoAllocScratch + kOcNoAllocOut];  // 65.7 KB
+
+namespace {
+std::mutex g_oc_noalloc_mu;
+void* g_oc_noalloc_addr[128] = {};  // device address of g_oc_noalloc, per device, filled on first use
+}  // namespace
+
 }  // namespace mycel
+
+extern "C" int32_t mycel_oc_update_noalloc(mycel_ctx* ctx, int32_t n, const double* rho, const double* dc,
+                                           const double* s, const uint8_t* passive, double* rho_new,
+                                           double target_volume_fraction, double move_limit, double rho_min,
+                                           double lambda_guess, int32_t max_bisection_steps,
+                                           double volume_tolerance, double* lambda_out) {
+  using namespace mycel;
+  if (!ctx) return set_error(nullptr, MYCEL_E_ARG, "NULL context");
+  if (n < 0 || (n > 0 && (!rho || !dc || !s || !rho_new)) || !lambda_out)
+    return set_error(ctx, MYCEL_E_ARG, "All spans must have length >= rho.Length.");
+  if (ctx->device < 0 || ctx->device >= 128) return set_error(ctx, MYCEL_E_ARG, "device index out of range");
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return set_error(ctx, MYCEL_E_DEVICE, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+  // set-up, once per device, with that device current: the host-side name of the array is not a device
+  // address, so the kernel gets the address the runtime reports for this device
+  void* base = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_oc_noalloc_mu);
+    if (!g_oc_noalloc_addr[ctx->device]) {
+      e = cudaGetSymbolAddress(&g_oc_noalloc_addr[ctx->device], g_oc_noalloc);
+      if (e != cudaSuccess) {
+        g_oc_noalloc_addr[ctx->device] = nullptr;
+        return set_error(ctx, MYCEL_E_DEVICE, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+      }
+    }
+    base = g_oc_noalloc_addr[ctx->device];
+  }
+  int blocks_per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_oc, 256, 0);
+  if (e != cudaSuccess) return set_error(ctx, MYCEL_E_DEVICE, std::string("occupancy query: ") + cudaGetErrorString(e));
+  blocks_per_sm = std::max(1, std::min(blocks_per_sm, 2));
+  const int grid = ctx->num_sms * blocks_per_sm;  // the grid launch_oc uses
+  if (grid > kOcNoAllocMaxBlocks)
+    return set_error(ctx, MYCEL_E_ARG, "OC without allocation: this device needs " + std::to_string(grid) +
+                                           " persistent blocks, the static scratch holds " +
+                                           std::to_string(kOcNoAllocMaxBlocks));
+  double* scratch = static_cast<double*>(base);
+  OcOut* out = reinterpret_cast<OcOut*>(scratch + kOcNoAllocScratch);
+  // the array keeps the previous call's contents: clear the result (launch_oc clears the barrier words)
+  e = cudaMemsetAsync(out, 0, sizeof(OcOut), ctx->stream);
+  if (e != cudaSuccess) return set_error(ctx, MYCEL_E_DEVICE, std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));
+  OcParams prm{target_volume_fraction, move_limit, rho_min, lambda_guess, volume_tolerance, max_bisection_steps, 0};
+  if (launch_oc(ctx, n, nullptr, rho, dc, s, passive, rho_new, nullptr, nullptr, prm, scratch, out))
+    return set_error(ctx, MYCEL_E_DEVICE, std::string("OC kernel launch: ") + cudaGetErrorString(cudaGetLastError()));
+  OcOut* h = reinterpret_cast<OcOut*>(ctx->pinned);
+  e = cudaMemcpyAsync(h, out, sizeof(OcOut), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return set_error(ctx, MYCEL_E_DEVICE, std::string("OC kernel: ") + cudaGetErrorString(e));
+  if (h->trials == 0) return set_error(ctx, MYCEL_E_TIMEOUT, "OC grid barrier timed out");
+  *lambda_out = h->lambda;
+  return MYCEL_OK;
+}
