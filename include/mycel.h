@@ -151,6 +151,13 @@ int32_t mycel_problem_create(mycel_ctx* ctx, const mycel_grid* grid, const uint8
                              double penal, mycel_problem** out);
 int32_t mycel_problem_destroy(mycel_problem* p);
 int32_t mycel_problem_info_get(mycel_problem* p, mycel_problem_info* out);
+/* Tuning of the kernels of one problem (no counterpart in the reference, which has one CPU kernel per step).
+   MYCEL_TUNE_MATVEC32: FP32 stiffness matvec of the mixed form; 0 = chosen by timing both on first use
+   (default), 1 = SIMT FFMA kernel, 2 = tensor-core (tcgen05, 3xTF32) kernel. get returns the variant in use
+   (0 while not chosen yet). */
+#define MYCEL_TUNE_MATVEC32 1
+int32_t mycel_problem_set_tuning(mycel_problem* p, int32_t key, int32_t value);
+int32_t mycel_problem_get_tuning(mycel_problem* p, int32_t key, int32_t* value);
 /* FeModel.AssembleForces (Fem/FeModel.cs:263-321): box-sized nodal forces. */
 int32_t mycel_problem_forces(mycel_problem* p, double* f_out);
 

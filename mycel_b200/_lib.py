@@ -79,6 +79,8 @@ SIGNATURES = {
     "mycel_problem_destroy": (i32, [P]),
     "mycel_problem_info_get": (i32, [P, C.POINTER(ProblemInfo)]),
     "mycel_problem_forces": (i32, [P, P]),
+    "mycel_problem_set_tuning": (i32, [P, i32, i32]),
+    "mycel_problem_get_tuning": (i32, [P, i32, C.POINTER(i32)]),
     "mycel_update_densities": (i32, [P, P, dbl]),
     "mycel_diagonal": (i32, [P, P]),
     "mycel_apply_k": (i32, [P, P, P, i32, i32]),

@@ -143,6 +143,17 @@ class Problem:
     def n_dofs(self) -> int:
         return self.model.total_dofs
 
+    MATVEC32_AUTO, MATVEC32_SIMT, MATVEC32_TENSOR = 0, 1, 2
+
+    def set_matvec32(self, variant: int):
+        """FP32 matvec variant of the mixed form: 0 autotune (default), 1 SIMT, 2 tensor cores."""
+        _check(L.load().mycel_problem_set_tuning(self.handle, 1, int(variant)), self.ctx)
+
+    def matvec32(self) -> int:
+        v = C.c_int32(0)
+        _check(L.load().mycel_problem_get_tuning(self.handle, 1, C.byref(v)), self.ctx)
+        return v.value
+
     def forces(self) -> np.ndarray:
         f = np.zeros(self.n_dofs)
         _check(L.load().mycel_problem_forces(self.handle, f.ctypes.data), self.ctx)

@@ -427,6 +427,7 @@ extern "C" int32_t mycel_problem_create(mycel_ctx* c, const mycel_grid* grid, co
   p->penal = penal;
   build_ke((double)grid->h, mat->nu, p->ke.v);
   for (int i = 0; i < 576; ++i) p->kef.v[i] = (float)p->ke.v[i];
+  split_ke_tf32(p->ke.v, &p->ketf);
   for (int i = 0; i < 24; ++i) p->diag_ke[i] = p->ke.v[i * 24 + i];
   p->fixed_host.assign(fixed, fixed + n_fixed);
 
@@ -492,6 +493,7 @@ extern "C" int32_t mycel_problem_create(mycel_ctx* c, const mycel_grid* grid, co
             !dalloc(p, &p->d_E, g.ne) && !dalloc(p, &p->d_Ef, g.ne) && !dalloc(p, &p->d_diag, g.nd) &&
             !dalloc(p, &p->d_invd, g.nd) && !dalloc(p, &p->d_invdf, g.nd) && !dalloc(p, &p->d_tmp0, g.nd) &&
             !dalloc(p, &p->d_tmp1, g.nd) && !dalloc(p, &p->d_fixed, std::max<int32_t>(n_fixed, 1)) &&
+            !dalloc(p, &p->d_err, 4) &&
             !dalloc(p, &d_cnt, 4);
   if (ok) ok = !dalloc(p, &p->d_part2, std::max<int64_t>(g.nd / 256 + 1024, 65536));
   p->n_part2 = std::max<int64_t>(g.nd / 256 + 1024, 65536);
@@ -513,6 +515,7 @@ extern "C" int32_t mycel_problem_create(mycel_ctx* c, const mycel_grid* grid, co
     cudaStreamSynchronize(s);
   }
   cudaMemsetAsync(d_cnt, 0, 16, s);
+  cudaMemsetAsync(p->d_err, 0, 16, s);
   cudaMemsetAsync(p->d_E, 0, sizeof(double) * g.ne, s);
   cudaMemsetAsync(p->d_Ef, 0, sizeof(float) * g.ne, s);
   launch_setup_nodes(p, p->d_fixed, n_fixed, d_cnt);
@@ -577,7 +580,7 @@ extern "C" int32_t mycel_problem_destroy(mycel_problem* p) {
     for (int j = 0; j < 2; ++j)
       if (p->prof_ev[k][j]) cudaEventDestroy(p->prof_ev[k][j]);
   }
-  void* ptrs[] = {p->d_domain, p->d_nflags, p->d_fixed, p->d_active, p->d_e2a, p->d_F, p->d_b, p->d_fnz, p->d_bnz, p->d_rho_box,
+  void* ptrs[] = {p->d_domain, p->d_nflags, p->d_fixed, p->d_err, p->d_active, p->d_e2a, p->d_F, p->d_b, p->d_fnz, p->d_bnz, p->d_rho_box,
                   p->d_E, p->d_Ef, p->d_diag, p->d_invd, p->d_invdf, p->d_r, p->d_z, p->d_p, p->d_ap, p->d_x,
                   p->d_part, p->d_state, p->f_x, p->f_r, p->f_z, p->f_p0, p->f_p1, p->f_ap, p->d_r64, p->d_part2,
                   p->d_tmp0, p->d_tmp1};
@@ -596,6 +599,31 @@ extern "C" int32_t mycel_problem_info_get(mycel_problem* p, mycel_problem_info* 
   o->active_fixed_dofs = p->n_active_fixed;
   o->device_bytes = p->device_bytes;
   return MYCEL_OK;
+}
+
+extern "C" int32_t mycel_problem_set_tuning(mycel_problem* p, int32_t key, int32_t value) {
+  if (!p) return set_error(nullptr, MYCEL_E_ARG, "NULL problem");
+  if (key == MYCEL_TUNE_MATVEC32) {
+    if (value < 0 || value > 2) return set_error(p->ctx, MYCEL_E_ARG, "matvec variant must be 0, 1 or 2");
+    p->tune_mv32 = value;
+    p->use_tc = value == 0 ? -1 : (value == 2 ? 1 : 0);
+    for (int k = 0; k < 2; ++k)
+      if (p->pcg32_graph[k]) {
+        cudaGraphExecDestroy(p->pcg32_graph[k]);
+        p->pcg32_graph[k] = nullptr;
+      }
+    return MYCEL_OK;
+  }
+  return set_error(p->ctx, MYCEL_E_ARG, "unknown tuning key");
+}
+
+extern "C" int32_t mycel_problem_get_tuning(mycel_problem* p, int32_t key, int32_t* value) {
+  if (!p || !value) return set_error(p ? p->ctx : nullptr, MYCEL_E_ARG, "NULL argument");
+  if (key == MYCEL_TUNE_MATVEC32) {
+    *value = p->use_tc < 0 ? 0 : (p->use_tc ? 2 : 1);
+    return MYCEL_OK;
+  }
+  return set_error(p->ctx, MYCEL_E_ARG, "unknown tuning key");
 }
 
 extern "C" int32_t mycel_problem_forces(mycel_problem* p, double* f) {

@@ -354,6 +354,389 @@ static dim3 tile_grid(const GridDims& g, int zseg) {
   return dim3((unsigned)((g.nx1 + TX - 1) / TX), (unsigned)((g.ny1 + TY - 1) / TY), (unsigned)((g.nz1 + zseg - 1) / zseg));
 }
 
+// ---------------------------------------------------------------------------------------------------------
+// FP32 K p on the 5th-generation tensor cores (tcgen05, kind::tf32, 3xTF32 for FP32-level products).
+// A CTA takes a 16 x 8 tile of elements per element plane (one MMA row per element, M = 128) and owns the
+// 15 x 7 nodes strictly inside it; CTAs overlap by one element in x and y. It marches over z: for element
+// plane kk it
+//   1. gathers each element's 24 DOF values from the two node planes in shared memory, splits them into
+//      TF32 hi + lo and writes them into tensor memory (A operand, one TMEM lane per element),
+//   2. one thread issues D = A_hi B_hi + A_lo B_hi + A_hi B_lo over the three K-steps (9 MMAs, M128 N32 K8,
+//      B = KE^T hi/lo, K-major in shared memory, rows 24-31 zero) and commits them to an mbarrier,
+//   3. reads D (24 outputs per element) back with tcgen05.ld, scales it by E_e and stages it in shared memory,
+//   4. each owned node adds the bottom outputs of its 4 elements in this plane to the partial sum it carries
+//      from the plane below (node plane kk is then complete and written) and starts node plane kk+1 with the
+//      top outputs, always in the same order.
+// MODE 1 fuses the inner PCG's p update and p.Ap partials exactly as k_mv32 does.
+// ---------------------------------------------------------------------------------------------------------
+constexpr int CX = 16, CY = 8;          // element tile (M = 128)
+constexpr int OX = CX - 1, OY = CY - 1; // owned nodes per tile
+constexpr int NX = CX + 1, NY = CY + 1; // node plane of the tile
+constexpr int TC_THREADS = 128;
+constexpr int TC_TMEM_COLS = 128;       // D: cols 0-31, A_hi: 32-55, A_lo: 64-87
+constexpr long long kMbarSpinLimit = 1ll << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint32_t to_tf32(float v) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(v));
+  return r;
+}
+
+// K-major, no-swizzle shared-memory matrix descriptor: 8-row core matrices of 16 bytes per row, `lbo` bytes
+// between the two 16-byte K halves of a K-step, `sbo` bytes between 8-row groups.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFF);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version for sm_100
+  return d;               // base offset 0, legacy LBO mode, layout type 0 (no swizzle)
+}
+
+// instruction descriptor: D f32, A and B tf32, both K-major, N = 32, M = 128
+constexpr uint32_t kIdescTf32 = (1u << 4) | (2u << 7) | (2u << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
+
+__device__ __forceinline__ void mma_tf32_ts(uint32_t tmem_d, uint32_t tmem_a, uint64_t desc_b, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %3, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %4, {%5, %5, %5, %5}, p;\n\t}\n"
+      :
+      : "r"(tmem_d), "r"(tmem_a), "l"(desc_b), "r"(accumulate), "r"(kIdescTf32), "r"(0u));
+}
+
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t (&v)[8]) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};\n"
+               :
+               : "r"(taddr), "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7])
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr)
+      : "memory");
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// bounded wait for phase `parity` of an mbarrier; returns false if it gave up
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+  for (long long spin = 0; spin < kMbarSpinLimit; ++spin) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(TC_THREADS) k_mv32tc(GridDims g, const __grid_constant__ KeTf kt,
+                                                      const float* __restrict__ xin, const float* __restrict__ z,
+                                                      const float* __restrict__ pold, float* __restrict__ pnew,
+                                                      float* __restrict__ y, const float* __restrict__ E,
+                                                      const uint8_t* __restrict__ nf, int projected, MixState* st,
+                                                      double* part, int zseg, int* err) {
+  __shared__ __align__(128) float4 bsm[2][6][32];  // B hi/lo: [K chunk of 4][row n] (16 B per row), K-major
+  __shared__ float4 xs[3][NY][NX];                // node planes (w unused)
+  __shared__ float dsm[CX * CY][25];              // scaled MMA outputs per element
+  __shared__ __align__(8) unsigned long long mbar;
+  __shared__ uint32_t tmem_base_sh;
+  __shared__ double sh[32];
+  __shared__ int fail_sh;
+  if (MODE == 1 && st->status != MIX_RUNNING) return;
+  const float beta = MODE == 1 ? (float)st->beta : 0.0f;
+  const bool first = MODE == 1 ? (st->first != 0) : true;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int ie0 = blockIdx.x * OX - 1, je0 = blockIdx.y * OY - 1;  // element tile origin
+  const int k0 = blockIdx.z * zseg, k1 = min(k0 + zseg, g.nz1);
+  const int64_t sy = g.nx1, sz = (int64_t)g.nx1 * g.ny1;
+
+  // B operand: row n = output row, K = column of KE (canonical K-major layout, no swizzle)
+  for (int q = tid; q < 2 * 6 * 32; q += TC_THREADS) {
+    int h = q / (6 * 32), rem = q % (6 * 32), kc = rem / 32, n = rem % 32;
+    const float* src = (h ? kt.lo : kt.hi) + n * 24 + 4 * kc;
+    bsm[h][kc][n] = make_float4(src[0], src[1], src[2], src[3]);
+  }
+  if (tid == 0) {
+    fail_sh = 0;
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(&mbar)), "r"(1u) : "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n"
+                 ::"r"(smem_u32(&tmem_base_sh)), "r"((uint32_t)TC_TMEM_COLS) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // B writes visible to the tensor core
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tbase = tmem_base_sh;
+  const uint32_t lane_base = (uint32_t)(32 * warp) << 16;  // this warp's TMEM lanes
+
+  // node plane loader (z + beta p_{t-1} for MODE 1; owned interior nodes of owned planes write p_t)
+  auto load_plane = [&](int kk) {
+    const int slot = (kk + 3) % 3;
+    const bool owned_plane = kk >= k0 && kk < k1;
+    for (int q = tid; q < NY * NX * 3; q += TC_THREADS) {
+      int c = q % 3, rest = q / 3, lx = rest % NX, ly = rest / NX;
+      int i = ie0 + lx, j = je0 + ly;
+      float v = 0.f;
+      if (kk >= 0 && kk < g.nz1 && i >= 0 && i < g.nx1 && j >= 0 && j < g.ny1) {
+        int64_t idx = 3 * (i + sy * j + sz * kk) + c;
+        if (MODE == 1) {
+          v = first ? __ldg(z + idx) : fmaf(beta, __ldg(pold + idx), __ldg(z + idx));
+          if (owned_plane && lx >= 1 && lx <= OX && ly >= 1 && ly <= OY) pnew[idx] = v;
+        } else {
+          v = __ldg(xin + idx);
+        }
+      }
+      reinterpret_cast<float*>(&xs[slot][ly][lx])[c] = v;
+    }
+  };
+
+  // element handled by this thread (one TMEM lane)
+  const int ex = tid % CX, ey = tid / CX;
+  const int ie = ie0 + ex, je = je0 + ey;
+  const bool e_in = ie >= 0 && ie < g.nx && je >= 0 && je < g.ny;
+  // owned node handled by this thread (tid < OX * OY)
+  const bool owner = tid < OX * OY;
+  const int na = 1 + (owner ? tid % OX : 0), nb = 1 + (owner ? tid / OX : 0);
+  const int ni = ie0 + na, nj = je0 + nb;
+  const bool n_in = owner && ni < g.nx1 && nj < g.ny1;
+  float carry[3] = {0.f, 0.f, 0.f};  // top contributions of the plane below
+  double pap = 0.0;
+  uint32_t phase = 0;
+  bool ok = true;
+
+  load_plane(k0 - 1);
+  for (int kk = k0 - 1; kk < k1; ++kk) {  // element plane kk couples node planes kk and kk+1
+    load_plane(kk + 1);
+    __syncthreads();
+    // 1. A operand: element DOF values, TF32 hi/lo, into TMEM columns 32.. and 64..
+    {
+      float ee = 0.f;
+      if (e_in && kk >= 0 && kk < g.nz) ee = __ldg(E + ie + (int64_t)g.nx * (je + (int64_t)g.ny * kk));
+      uint32_t hi[24], lo[24];
+#pragma unroll
+      for (int b = 0; b < 8; ++b) {
+        const int bx = (b == 1 || b == 2 || b == 5 || b == 6) ? 1 : 0;
+        const int by = (b == 2 || b == 3 || b == 6 || b == 7) ? 1 : 0;
+        const int bz = b >= 4 ? 1 : 0;
+        const float4 v4 = xs[(kk + bz + 3) % 3][ey + by][ex + bx];
+        const float u[3] = {v4.x, v4.y, v4.z};
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const float uv = ee != 0.f ? u[c] : 0.f;
+          const uint32_t h = to_tf32(uv);
+          hi[3 * b + c] = h;
+          lo[3 * b + c] = to_tf32(uv - __uint_as_float(h));
+        }
+      }
+      dsm[tid][24] = ee;
+#pragma unroll
+      for (int s = 0; s < 3; ++s) {
+        uint32_t vh[8], vl[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          vh[q] = hi[8 * s + q];
+          vl[q] = lo[8 * s + q];
+        }
+        tmem_st8(tbase + lane_base + 32 + 8 * s, vh);
+        tmem_st8(tbase + lane_base + 64 + 8 * s, vl);
+      }
+      asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    // 2. nine MMAs, one issuing thread, completion on the mbarrier
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+      const uint32_t b0 = smem_u32(&bsm[0][0][0]), b1 = smem_u32(&bsm[1][0][0]);
+#pragma unroll
+      for (int s = 0; s < 3; ++s) {
+        const uint64_t dh = smem_desc(b0 + s * 1024, 512, 128);
+        const uint64_t dl = smem_desc(b1 + s * 1024, 512, 128);
+        mma_tf32_ts(tbase, tbase + 32 + 8 * s, dh, s > 0 ? 1u : 0u);
+        mma_tf32_ts(tbase, tbase + 64 + 8 * s, dh, 1u);
+        mma_tf32_ts(tbase, tbase + 32 + 8 * s, dl, 1u);
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
+                   ::"r"(smem_u32(&mbar)) : "memory");
+    }
+    // 3. D back to registers, scaled by E_e, staged for the node gather
+    if (!mbar_wait(smem_u32(&mbar), phase)) {
+      ok = false;
+      fail_sh = 1;
+    }
+    phase ^= 1u;
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    {
+      float d[32];
+      tmem_ld32(tbase + lane_base, d);
+      const float ee = dsm[tid][24];
+#pragma unroll
+      for (int r = 0; r < 24; ++r) dsm[tid][r] = d[r] * ee;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (fail_sh) break;
+    // 4. owned nodes: bottom outputs finish node plane kk, top outputs start node plane kk+1
+    if (owner) {
+      float bot[3] = {0.f, 0.f, 0.f}, top[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+      for (int sy_ = 0; sy_ < 2; ++sy_)
+#pragma unroll
+        for (int sx_ = 0; sx_ < 2; ++sx_) {
+          const int m = (nb - 1 + sy_) * CX + (na - 1 + sx_);  // element (na-1+sx, nb-1+sy)
+          const int ox = 1 - sx_, oy = 1 - sy_;                 // this node's position in that element
+          const int a2 = oy ? (ox ? 2 : 3) : (ox ? 1 : 0);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            bot[c] += dsm[m][3 * a2 + c];
+            top[c] += dsm[m][3 * (a2 + 4) + c];
+          }
+        }
+      if (kk >= k0 && n_in) {
+        const int64_t n = ni + sy * nj + sz * kk;
+        const uint8_t f = projected ? nf[n] : 0;
+        const float4 pv4 = xs[(kk + 3) % 3][nb][na];
+        const float pv[3] = {pv4.x, pv4.y, pv4.z};
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const float acc = carry[c] + bot[c];
+          const float yv = (f & (1 << c)) ? pv[c] : acc;
+          y[3 * n + c] = yv;
+          if (MODE == 1) pap += (double)pv[c] * (double)yv;
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) carry[c] = top[c];
+    }
+    __syncthreads();  // dsm and the node plane slot of kk-1 are reused by the next plane
+  }
+  // release tensor memory
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tbase), "r"((uint32_t)TC_TMEM_COLS)
+                 : "memory");
+  }
+  if (!ok && tid == 0 && err) atomicExch(err, 1);
+  if (MODE != 1) return;
+  double bsum_v = bsum(pap, sh);
+  const unsigned nblk = gridDim.x * gridDim.y * gridDim.z;
+  const unsigned bid = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+  if (tid == 0) part[bid] = bsum_v;
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) last = (atomicAdd(&st->counter, 1u) == nblk - 1);
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (tid >= 32) return;
+  double s = warp_sum_parts(part, nblk);
+  if (tid != 0) return;
+  st->counter = 0;
+  st->first = 0;
+  st->pap = s;
+  if (fail_sh || (err && *(volatile int*)err)) {
+    st->status = MIX_BREAKDOWN;
+    return;
+  }
+  if (!(s > 0.0) || !isfinite(s)) {
+    st->status = MIX_BREAKDOWN;
+    return;
+  }
+  st->alpha = st->rho0 / s;
+}
+
+static int tc_zseg(const GridDims& g, int num_sms) {
+  int64_t txy = (int64_t)((g.nx1 + OX - 1) / OX) * ((g.ny1 + OY - 1) / OY);
+  int64_t segs = std::max<int64_t>(1, (8 * (int64_t)num_sms + txy - 1) / txy);
+  return (int)std::max<int64_t>(2, (g.nz1 + segs - 1) / segs);
+}
+
+static dim3 tc_grid(const GridDims& g, int zseg) {
+  return dim3((unsigned)((g.nx1 + OX - 1) / OX), (unsigned)((g.ny1 + OY - 1) / OY), (unsigned)((g.nz1 + zseg - 1) / zseg));
+}
+
+// 20 KB of unused dynamic shared memory keeps the tensor-core kernel at <= 4 CTAs per SM, so the CTAs on an
+// SM never ask for more than its 512 TMEM columns (4 x 128).
+constexpr int kTcPadSmem = 20 * 1024;
+
+// FP32 matvec launch, variant chosen per problem (SIMT FFMA kernel or tensor-core kernel)
+template <int MODE>
+static void launch_mv32_variant(mycel_problem* p, cudaStream_t s, const float* xin, const float* z, const float* pold,
+                                float* pnew, float* y, int projected, MixState* st, double* part) {
+  const GridDims& g = p->g;
+  if (p->use_tc == 1) {
+    int zs = tc_zseg(g, p->ctx->num_sms);
+    k_mv32tc<MODE><<<tc_grid(g, zs), TC_THREADS, kTcPadSmem, s>>>(g, p->ketf, xin, z, pold, pnew, y, p->d_Ef,
+                                                                  p->d_nflags, projected, st, part, zs, p->d_err);
+  } else {
+    int zs = tile_zseg(g, p->ctx->num_sms);
+    k_mv32<MODE><<<tile_grid(g, zs), dim3(TX, TY), 0, s>>>(g, p->kef, xin, z, pold, pnew, y, p->d_Ef, p->d_nflags,
+                                                           projected, st, part, zs);
+  }
+}
+
+// Autotuner: on first use, time both variants (K x on the problem's FP32 buffers, after one warm-up launch)
+// and keep the faster; a tensor-core run that reports a failed wait is never chosen.
+static int32_t resolve_mv32(mycel_problem* p) {
+  if (p->use_tc >= 0) return MYCEL_OK;
+  mycel_ctx* c = p->ctx;
+  cudaStream_t s = c->stream;
+  const int64_t n = p->g.nd;
+  MYCEL_CUDA(c, cudaMemsetAsync(p->f_r, 0, sizeof(float) * n, s));
+  MYCEL_CUDA(c, cudaMemsetAsync(p->d_err, 0, sizeof(int), s));
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float t[2] = {0.f, 0.f};
+  for (int v = 0; v < 2; ++v) {
+    p->use_tc = v;
+    launch_mv32_variant<0>(p, s, p->f_r, nullptr, nullptr, nullptr, p->f_ap, 1, nullptr, nullptr);
+    cudaEventRecord(e0, s);
+    for (int r = 0; r < 3; ++r)
+      launch_mv32_variant<0>(p, s, p->f_r, nullptr, nullptr, nullptr, p->f_ap, 1, nullptr, nullptr);
+    cudaEventRecord(e1, s);
+    c->launches += 4;
+    cudaError_t e = cudaEventSynchronize(e1);
+    if (e != cudaSuccess) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      p->use_tc = -1;
+      return set_error(c, MYCEL_E_DEVICE, std::string("matvec autotune: ") + cudaGetErrorString(e));
+    }
+    cudaEventElapsedTime(&t[v], e0, e1);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  int herr = 0;
+  MYCEL_CUDA(c, cudaMemcpy(&herr, p->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  p->use_tc = (!herr && t[1] < t[0]) ? 1 : 0;
+  return MYCEL_OK;
+}
+
 // x += alpha p, r -= alpha Ap, z = r invD; partials of r.r and r.z (FP64). mode 0: CG step; 1: residual
 // replacement (z, rho from the new r; beta = rho_new / rho_old); 2: start (z, rho; next step starts p = z).
 __global__ void __launch_bounds__(kT) k_xr32(int64_t n, float* __restrict__ x, float* __restrict__ r,
@@ -501,9 +884,7 @@ void mixed_apply_k_f64io(mycel_problem* p, const double* x, double* y, int proje
   float* fx = (float*)p->d_r;  // borrow FP64 workspace as FP32 staging
   float* fy = fx + n;
   k_to_f32<<<stream_blocks(p), kT, 0, s>>>(n, x, fx);
-  int zs = tile_zseg(p->g, p->ctx->num_sms);
-  k_mv32<0><<<tile_grid(p->g, zs), dim3(TX, TY), 0, s>>>(p->g, p->kef, fx, nullptr, nullptr, nullptr, fy, p->d_Ef,
-                                                         p->d_nflags, projected, nullptr, nullptr, zs);
+  launch_mv32_variant<0>(p, s, fx, nullptr, nullptr, nullptr, fy, projected, nullptr, nullptr);
   k_to_f64<<<stream_blocks(p), kT, 0, s>>>(n, fy, y);
   p->ctx->launches += 3;
 }
@@ -553,7 +934,6 @@ static int32_t capture_mixed_graph(mycel_problem* p, int chunk) {
   double* part = p->d_part2;
   int sb = stream_blocks(p);
   int64_t before = c->launches;
-  const int zs = tile_zseg(p->g, c->num_sms);
   for (int k = 0; k < 2; ++k) {
     cudaGraph_t graph;
     MYCEL_CUDA(c, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
@@ -561,8 +941,7 @@ static int32_t capture_mixed_graph(mycel_problem* p, int chunk) {
       float* pcur = (t & 1) ? p->f_p1 : p->f_p0;
       float* pprev = (t & 1) ? p->f_p0 : p->f_p1;
       if (!(c->profile && t == 0))
-        k_mv32<1><<<tile_grid(p->g, zs), dim3(TX, TY), 0, s>>>(p->g, p->kef, nullptr, p->f_z, pprev, pcur,
-                                                               p->f_ap, p->d_Ef, p->d_nflags, 1, st, part, zs);
+        launch_mv32_variant<1>(p, s, nullptr, p->f_z, pprev, pcur, p->f_ap, 1, st, part);
       k_xr32<<<sb, kT, 0, s>>>(n, p->f_x, p->f_r, p->f_z, pcur, p->f_ap, p->d_invdf, st, part, 0);
     }
     MYCEL_CUDA(c, cudaStreamEndCapture(s, &graph));
@@ -580,10 +959,7 @@ static void launch_chunk(mycel_problem* p, int gi) {
   cudaStream_t s = c->stream;
   if (p->pcg32_graph_profiled) {
     cudaEventRecord(p->prof_ev[gi][0], s);
-    int zs = tile_zseg(p->g, c->num_sms);
-    k_mv32<1><<<tile_grid(p->g, zs), dim3(TX, TY), 0, s>>>(p->g, p->kef, nullptr, p->f_z, p->f_p1, p->f_p0,
-                                                           p->f_ap, p->d_Ef, p->d_nflags, 1, mix_state(p),
-                                                           p->d_part2, zs);
+    launch_mv32_variant<1>(p, s, nullptr, p->f_z, p->f_p1, p->f_p0, p->f_ap, 1, mix_state(p), p->d_part2);
     cudaEventRecord(p->prof_ev[gi][1], s);
   }
   cudaGraphLaunch(p->pcg32_graph[gi], s);
@@ -652,6 +1028,7 @@ int32_t mixed_solve_entry(mycel_problem* p, const double* d_b, const int32_t* d_
     return MYCEL_OK;
   }
   const int chunk = 16;
+  if ((st = resolve_mv32(p))) return st;
   if ((st = capture_mixed_graph(p, chunk))) return st;
   double rn = 0.0;
   if ((st = true_residual(p, d_b, d_u, &rn))) return st;

@@ -3,6 +3,7 @@
 // weight det(J) = 1/8 for h = 1, Ke(h) = h Ke(1); nu = 0.3 takes the fast path BaseKe * h (:104-112), where
 // BaseKe itself is the Gauss-integrated Ke(1, 0.3). Compiled with -ffp-contract=off.
 #include <cmath>
+#include <cstring>
 
 #include "internal.h"
 
@@ -86,5 +87,29 @@ void build_ke(double h, double nu, double* ke) {
 }
 
 int64_t num_blocks8192(int64_t n) { return (n + 8191) / 8192; }
+
+// Round an FP32 value to TF32 (10 explicit mantissa bits), to nearest with ties away from zero, as the
+// device's cvt.rna.tf32.f32 does; non-finite values pass through.
+static float tf32_rna(float v) {
+  uint32_t u;
+  std::memcpy(&u, &v, 4);
+  if ((u & 0x7f800000u) == 0x7f800000u) return v;
+  u += 0x1000u;      // half of the 13 dropped bits: ties round away from zero in magnitude
+  u &= 0xffffe000u;
+  float r;
+  std::memcpy(&r, &u, 4);
+  return r;
+}
+
+void split_ke_tf32(const double* ke, KeTf* out) {
+  for (int i = 0; i < 32 * 24; ++i) out->hi[i] = out->lo[i] = 0.0f;
+  for (int r = 0; r < 24; ++r)
+    for (int c = 0; c < 24; ++c) {
+      float f = (float)ke[r * 24 + c];
+      float hi = tf32_rna(f);
+      out->hi[r * 24 + c] = hi;
+      out->lo[r * 24 + c] = tf32_rna(f - hi);
+    }
+}
 
 }  // namespace mycel

@@ -29,6 +29,8 @@ inline GridDims make_dims(int nx, int ny, int nz) {
 
 struct KeD { double v[576]; };  // element stiffness (row-major), FP64
 struct KeF { float v[576]; };   // FP32 copy for the mixed form
+// KE split for 3xTF32 tensor-core products: rows padded to 32 (rows 24..31 zero), row-major [32][24]
+struct KeTf { float hi[32 * 24]; float lo[32 * 24]; };
 
 // Node flag bits (one byte per node): bits 0-2 = DOF c constrained, bit 3 = node active.
 enum : uint8_t { NF_CX = 1, NF_CY = 2, NF_CZ = 4, NF_ACTIVE = 8 };
@@ -92,6 +94,10 @@ struct mycel_problem {
   double e0 = 1, nu = 0.3, emin_ratio = 1e-6, emin = 1e-6, penal = 3.0;
   mycel::KeD ke{};
   mycel::KeF kef{};
+  mycel::KeTf ketf{};
+  int use_tc = -1;                // FP32 matvec variant: -1 not chosen yet, 0 SIMT, 1 tensor cores
+  int tune_mv32 = 0;              // requested variant: 0 autotune, 1 SIMT, 2 tensor cores
+  int* d_err = nullptr;           // device error word (bounded waits that gave up)
   double diag_ke[24];
   int64_t n_active = 0, n_active_nodes = 0, n_active_fixed = 0;
   std::vector<int32_t> fixed_host;        // FixedDofs as given (may repeat)
@@ -164,6 +170,7 @@ int32_t set_error(mycel_ctx* ctx, int32_t code, const std::string& msg);
 
 // ---- host setup ----
 void build_ke(double h, double nu, double* ke);  // Hex8Element.CreateKe semantics
+void split_ke_tf32(const double* ke, KeTf* out);   // hi = tf32(KE), lo = tf32(KE - hi), rows padded to 32
 int64_t num_blocks8192(int64_t n);
 
 // ---- FP64 plain-path launchers (fp64_kernels.cu, compiled with -fmad=false) ----

@@ -22,10 +22,13 @@ def exact_oracle(oracle):
     oracle.set_modes(0, 0)
 
 
-@pytest.mark.parametrize("shape", [(1, 1, 1), (5, 3, 2), (33, 17, 9), (70, 9, 20)])
-def test_fp32_matvec_close_to_fp64(oracle, ctx, shape):
+@pytest.mark.parametrize("variant", [1, 2], ids=["simt", "tensor"])
+@pytest.mark.parametrize("shape", [(1, 1, 1), (5, 3, 2), (33, 17, 9), (70, 9, 20), (16, 8, 3)])
+def test_fp32_matvec_close_to_fp64(oracle, ctx, shape, variant):
     m = carved_model(*shape, seed=3, frac=0.15) if shape[0] > 2 else tiny_test_model(*shape)
     om, pr = oracle.Model(m), api.Problem(m, ctx)
+    pr.set_matvec32(variant)
+    assert pr.matvec32() == variant
     x = np.random.default_rng(2).uniform(-1, 1, m.total_dofs)
     y64 = om.apply_k(x)
     y32 = pr.apply_k(x, precision="mixed")
@@ -42,6 +45,19 @@ def test_mixed_static_solve_matches_fp64(oracle, ctx):
     assert abs(r.compliance - ref.compliance) <= 1e-8 * abs(ref.compliance)
     assert np.abs(r.u - ref.u).max() <= 1e-6 * np.abs(ref.u).max()
     assert np.array_equal(r.u[m.fixed_dofs], np.zeros(m.fixed_dofs.size))
+
+
+@pytest.mark.parametrize("variant", [1, 2], ids=["simt", "tensor"])
+def test_mixed_pcg_each_matvec_variant(oracle, ctx, variant):
+    m = carved_model(31, 12, 9, seed=8, emin_ratio=1e-9)
+    om, pr = oracle.Model(m), api.Problem(m, ctx)
+    pr.set_matvec32(variant)
+    b = om.forces() * (om.constrained() == 0)
+    ref, _ = om.pcg_solve(b, tol=1e-10, max_iter=20000)
+    u, r = pr.pcg_solve(b, tol=1e-10, max_iterations=20000, precision="mixed")
+    assert r.converged and r.final_residual <= 1e-10
+    assert np.abs(u - ref).max() <= 1e-6 * np.abs(ref).max()
+    assert pr.matvec32() == variant
 
 
 def test_mixed_warm_start_and_zero_rhs(ctx):
