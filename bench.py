@@ -50,6 +50,8 @@ def parse():
                     help="kernel probe for profilers: one PCG solve of --probe-iters iterations on a bridge grid")
     ap.add_argument("--probe-grid", default="96x48x48")
     ap.add_argument("--probe-iters", type=int, default=40)
+    ap.add_argument("--probe-variant", type=int, default=0,
+                    help="FP32 matvec variant for --probe mixed (0 autotune, 1 dense, 2 tensor, 3 factored)")
     return ap.parse_args()
 
 
@@ -363,9 +365,12 @@ def run_probe(args):
     nx, ny, nz = (int(v) for v in args.probe_grid.split("x"))
     ctx = api.Context(0)
     pr = api.Problem(W.bridge(nx, ny, nz), ctx)
+    if args.probe == "mixed" and args.probe_variant:
+        pr.set_matvec32(args.probe_variant)
     u, r = pr.pcg_solve(pr.forces(), tol=1e-30, max_iterations=args.probe_iters, precision=args.probe)
     print(json.dumps({"probe": args.probe, "grid": args.probe_grid, "iterations": r.iterations,
-                      "elapsed_ms": r.elapsed_ms}))
+                      "elapsed_ms": r.elapsed_ms, "final_residual": r.final_residual,
+                      "matvec32": pr.matvec32() if args.probe == "mixed" else None}))
 
 
 if __name__ == "__main__":

@@ -152,10 +152,14 @@ int32_t mycel_problem_create(mycel_ctx* ctx, const mycel_grid* grid, const uint8
 int32_t mycel_problem_destroy(mycel_problem* p);
 int32_t mycel_problem_info_get(mycel_problem* p, mycel_problem_info* out);
 /* Tuning of the kernels of one problem (no counterpart in the reference, which has one CPU kernel per step).
-   MYCEL_TUNE_MATVEC32: FP32 stiffness matvec of the mixed form; 0 = chosen by timing both on first use
-   (default), 1 = SIMT FFMA kernel, 2 = tensor-core (tcgen05, 3xTF32) kernel. get returns the variant in use
-   (0 while not chosen yet). */
+   MYCEL_TUNE_MATVEC32: FP32 stiffness matvec of the mixed form; 0 = chosen by timing all variants on first
+   use (default), 1 = dense KE rows on the FMA pipe, 2 = dense KE on the tensor cores (tcgen05, 3xTF32),
+   3 = factorised cube-element operator (Walsh-Hadamard basis, about 190 flops per element instead of 1152).
+   get returns the variant in use (0 while not chosen yet). */
 #define MYCEL_TUNE_MATVEC32 1
+#define MYCEL_MV32_DENSE 1
+#define MYCEL_MV32_TENSOR 2
+#define MYCEL_MV32_FACTORED 3
 int32_t mycel_problem_set_tuning(mycel_problem* p, int32_t key, int32_t value);
 int32_t mycel_problem_get_tuning(mycel_problem* p, int32_t key, int32_t* value);
 /* FeModel.AssembleForces (Fem/FeModel.cs:263-321): box-sized nodal forces. */

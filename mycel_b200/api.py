@@ -146,7 +146,8 @@ class Problem:
     MATVEC32_AUTO, MATVEC32_SIMT, MATVEC32_TENSOR = 0, 1, 2
 
     def set_matvec32(self, variant: int):
-        """FP32 matvec variant of the mixed form: 0 autotune (default), 1 SIMT, 2 tensor cores."""
+        """FP32 matvec variant of the mixed form: 0 autotune (default), 1 dense KE on the FMA pipe, 2 dense KE on
+        the tensor cores, 3 factorised cube-element operator."""
         _check(L.load().mycel_problem_set_tuning(self.handle, 1, int(variant)), self.ctx)
 
     def matvec32(self) -> int:

@@ -428,6 +428,7 @@ extern "C" int32_t mycel_problem_create(mycel_ctx* c, const mycel_grid* grid, co
   build_ke((double)grid->h, mat->nu, p->ke.v);
   for (int i = 0; i < 576; ++i) p->kef.v[i] = (float)p->ke.v[i];
   split_ke_tf32(p->ke.v, &p->ketf);
+  build_hexop((double)grid->h, mat->nu, &p->hexop);
   for (int i = 0; i < 24; ++i) p->diag_ke[i] = p->ke.v[i * 24 + i];
   p->fixed_host.assign(fixed, fixed + n_fixed);
 
@@ -491,7 +492,7 @@ extern "C" int32_t mycel_problem_create(mycel_ctx* c, const mycel_grid* grid, co
             !dalloc(p, &p->d_b, g.nd) && !dalloc(p, &p->d_fnz, std::max<int32_t>(p->n_fnz, 1)) &&
             !dalloc(p, &p->d_bnz, std::max<int32_t>(p->n_fnz, 1)) && !dalloc(p, &p->d_rho_box, g.ne) &&
             !dalloc(p, &p->d_E, g.ne) && !dalloc(p, &p->d_Ef, g.ne) && !dalloc(p, &p->d_diag, g.nd) &&
-            !dalloc(p, &p->d_invd, g.nd) && !dalloc(p, &p->d_invdf, g.nd) && !dalloc(p, &p->d_tmp0, g.nd) &&
+            !dalloc(p, &p->d_invd, g.nd) && !dalloc(p, &p->d_invdf, g.n32) && !dalloc(p, &p->d_tmp0, g.nd) &&
             !dalloc(p, &p->d_tmp1, g.nd) && !dalloc(p, &p->d_fixed, std::max<int32_t>(n_fixed, 1)) &&
             !dalloc(p, &p->d_err, 4) &&
             !dalloc(p, &d_cnt, 4);
@@ -502,6 +503,7 @@ extern "C" int32_t mycel_problem_create(mycel_ctx* c, const mycel_grid* grid, co
     mycel_problem_destroy(p);
     return set_error(c, MYCEL_E_OOM, "out of device memory for the problem");
   }
+  cudaMemsetAsync(p->d_invdf, 0, sizeof(float) * g.n32, s);  // pads of the padded FP32 layout stay zero
   cudaMemcpyAsync(p->d_domain, domain, g.ne, cudaMemcpyHostToDevice, s);
   if (p->n_active) cudaMemcpyAsync(p->d_active, active.data(), sizeof(int32_t) * p->n_active, cudaMemcpyHostToDevice, s);
   cudaMemcpyAsync(p->d_F, p->forces_host.data(), sizeof(double) * g.nd, cudaMemcpyHostToDevice, s);
@@ -604,9 +606,10 @@ extern "C" int32_t mycel_problem_info_get(mycel_problem* p, mycel_problem_info* 
 extern "C" int32_t mycel_problem_set_tuning(mycel_problem* p, int32_t key, int32_t value) {
   if (!p) return set_error(nullptr, MYCEL_E_ARG, "NULL problem");
   if (key == MYCEL_TUNE_MATVEC32) {
-    if (value < 0 || value > 2) return set_error(p->ctx, MYCEL_E_ARG, "matvec variant must be 0, 1 or 2");
+    if (value < 0 || value > MYCEL_MV32_FACTORED)
+      return set_error(p->ctx, MYCEL_E_ARG, "matvec variant must be 0 (auto), 1, 2 or 3");
     p->tune_mv32 = value;
-    p->use_tc = value == 0 ? -1 : (value == 2 ? 1 : 0);
+    p->mv32 = value == 0 ? -1 : value;
     for (int k = 0; k < 2; ++k)
       if (p->pcg32_graph[k]) {
         cudaGraphExecDestroy(p->pcg32_graph[k]);
@@ -620,7 +623,7 @@ extern "C" int32_t mycel_problem_set_tuning(mycel_problem* p, int32_t key, int32
 extern "C" int32_t mycel_problem_get_tuning(mycel_problem* p, int32_t key, int32_t* value) {
   if (!p || !value) return set_error(p ? p->ctx : nullptr, MYCEL_E_ARG, "NULL argument");
   if (key == MYCEL_TUNE_MATVEC32) {
-    *value = p->use_tc < 0 ? 0 : (p->use_tc ? 2 : 1);
+    *value = p->mv32 < 0 ? 0 : p->mv32;
     return MYCEL_OK;
   }
   return set_error(p->ctx, MYCEL_E_ARG, "unknown tuning key");
@@ -666,7 +669,7 @@ extern "C" int32_t mycel_apply_k(mycel_problem* p, const double* x, double* y, i
     if (st) return st;
     launch_E_to_f32(p);
     // FP32 operator on the FP32-rounded input
-    mixed_apply_k_f64io(p, p->d_tmp0, p->d_tmp1, projected);
+    if ((st = mixed_apply_k_f64io(p, p->d_tmp0, p->d_tmp1, projected))) return st;
   } else {
     launch_matvec64(p, p->d_tmp0, p->d_tmp1, projected, nullptr);
   }

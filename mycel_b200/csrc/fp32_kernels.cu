@@ -13,6 +13,8 @@
 //   k_xr32   x += alpha p, r -= alpha Ap, z = r invD, FP64 partials of r.r and r.z; the last CTA forms the
 //            recursive residual, the replacement/stop triggers and beta.
 // Reductions use a fixed CTA decomposition and a fixed-order final sum, so results do not depend on timing.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -20,7 +22,10 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include "internal.h"
@@ -82,6 +87,25 @@ __device__ __forceinline__ double warp_sum_parts(const double* part, unsigned n)
   return s;
 }
 
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+constexpr long long kMbarSpinLimit = 1ll << 22;
+// bounded wait for phase `parity` of an mbarrier; returns false if it gave up
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+  for (long long spin = 0; spin < kMbarSpinLimit; ++spin) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+
 // ---------------------------------------------------------------------------------------------------------
 // FP32 K p, z-marching shared-memory tiles.
 // A CTA owns a TX x TY column of nodes and marches over ZSEG node planes. Three node planes of the input
@@ -127,7 +151,7 @@ __global__ void __launch_bounds__(TX * TY, 3) k_mv32(GridDims g, const __grid_co
   const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY, k0 = blockIdx.z * zseg;
   const int k1 = min(k0 + zseg, g.nz1);
   const int64_t sy = g.nx1, sz = (int64_t)g.nx1 * g.ny1;
-  const int64_t plane_f = 3 * sz;  // floats per node plane
+  const int64_t plane_f = (int64_t)g.rp * g.ny1;  // floats per node plane (padded FP32 layout)
 
   // ---- per-thread load plan (node rows) ----
   RowLoad rl;
@@ -148,7 +172,7 @@ __global__ void __launch_bounds__(TX * TY, 3) k_mv32(GridDims g, const __grid_co
     rl.ly[q] = ly;
     int j = j0 - 1 + ly;
     bool ok = q < rl.nrows && j >= 0 && j < g.ny1;
-    rl.gofs[q] = 3 * ((int64_t)(i0 - 1) + sy * j) + tx;
+    rl.gofs[q] = 3 * (int64_t)(i0 - 1) + (int64_t)g.rp * j + tx;
     if (ok) rl.rowok |= 1u << q;
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
@@ -306,7 +330,7 @@ __global__ void __launch_bounds__(TX * TY, 3) k_mv32(GridDims g, const __grid_co
       for (int c = 0; c < 3; ++c) {
         const float pv = xn[1][1][1][c];
         const float yv = (f & (1 << c)) ? pv : out[c];
-        y[3 * n + c] = yv;
+        y[plane_f * k + (int64_t)g.rp * j + 3 * i + c] = yv;
         if (MODE == 1) pap += (double)pv * (double)yv;
       }
     }
@@ -355,6 +379,311 @@ static dim3 tile_grid(const GridDims& g, int zseg) {
 }
 
 // ---------------------------------------------------------------------------------------------------------
+// FP32 K p with the factorised cube-element operator (HexOpF, built by build_hexop): per element an 8-point
+// Walsh-Hadamard transform of each displacement component, 21 eigenvalue products, 24 products coupling
+// pairs of components, and the inverse transform: about 190 flops per element instead of the 1152 of a dense
+// 24 x 24 KE product. Results differ from the dense product only by FP32 rounding.
+// Element-centric z-marching tiles: a CTA of FX x FY threads computes the FX x FY elements of each element
+// plane of its column (thread (l, w) the element (i0 - 1 + l, j0 - 1 + w)) and owns the FOX x FOY nodes
+// strictly inside that element tile. A node receives the contributions of its x-neighbour element through a
+// warp shuffle and those of its y-neighbour elements through a small shared-memory exchange; the part from
+// the element plane below is carried in registers. Node planes with a one-node halo are staged in shared
+// memory (two slots, the next-but-one prefetched into registers while the current plane is worked on); each
+// plane step has one __syncthreads.
+// MODE 1 fuses p_t = z + beta p_{t-1}, the write of p_t and the p.Ap partials, as k_mv32 does.
+// ---------------------------------------------------------------------------------------------------------
+constexpr int FX = 32, FY = 8;
+constexpr int FOX = FX - 1, FOY = FY - 1;  // owned nodes per tile
+constexpr int FPX = FX + 1, FPY = FY + 1;  // node plane with halo
+
+// 8-point Walsh-Hadamard butterflies over the index bits (x, y, z): afterwards v[p] = sum_a s_p(a) v_a,
+// s_p(a) the product over the axes odd in p of (2 a_axis - 1).
+__device__ __forceinline__ void wht8(float (&v)[8]) {
+#pragma unroll
+  for (int bit = 1; bit < 8; bit <<= 1)
+#pragma unroll
+    for (int a = 0; a < 8; ++a)
+      if (!(a & bit)) {
+        const float lo = v[a], hi = v[a | bit];
+        v[a] = hi + lo;
+        v[a | bit] = hi - lo;
+      }
+}
+
+// node values from basis coefficients: per axis (even e, odd o) -> (e - o, e + o)
+__device__ __forceinline__ void iwht8(float (&v)[8]) {
+#pragma unroll
+  for (int bit = 1; bit < 8; bit <<= 1)
+#pragma unroll
+    for (int a = 0; a < 8; ++a)
+      if (!(a & bit)) {
+        const float e = v[a], o = v[a | bit];
+        v[a] = e - o;
+        v[a | bit] = e + o;
+      }
+}
+
+// y = E KE(h) u for one element; u[c][a], y[c][a]: component c at local node a = x | y << 1 | z << 2
+// (node order (0,0,0),(1,0,0),(0,1,0),(1,1,0),(0,0,1),... by bits, not the reference's local numbering).
+__device__ __forceinline__ void hex_apply(const HexOpF& op, float E, float (&u)[3][8], float (&y)[3][8]) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) wht8(u[c]);
+  float d[2][3], lam[2], mu[2];
+#pragma unroll
+  for (int a = 0; a < 2; ++a) {
+#pragma unroll
+    for (int n = 0; n < 3; ++n) d[a][n] = E * op.dcl[a][n];
+    lam[a] = E * op.lam[a];
+    mu[a] = E * op.mu[a];
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    y[c][0] = 0.f;  // rigid translation: no force
+#pragma unroll
+    for (int p = 1; p < 8; ++p) {
+      const int pc = (p >> c) & 1;
+      const int n = (p & 1) + ((p >> 1) & 1) + ((p >> 2) & 1) - pc;
+      float acc = d[pc][n] * u[c][p];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        if (j == c) continue;
+        const int k = 3 - c - j;
+        const int pj = (p >> j) & 1, pk = (p >> k) & 1;
+        const int q = p ^ (1 << c) ^ (1 << j);
+        if (pc == 1 && pj == 0) acc = fmaf(lam[pk], u[j][q], acc);
+        if (pc == 0 && pj == 1) acc = fmaf(mu[pk], u[j][q], acc);
+      }
+      y[c][p] = acc;
+    }
+    iwht8(y[c]);
+  }
+}
+
+// p.Ap partials of a matvec launch: CTA sum, fixed-order sum of the CTA partials by the last CTA, alpha.
+// A launch whose bounded waits gave up has set *err; its last CTA then ends the inner solve as a breakdown.
+__device__ __forceinline__ void mv32_finish(double pap, double* sh, MixState* st, double* part, int tid,
+                                            const int* err) {
+  const double b = bsum(pap, sh);
+  const unsigned nblk = gridDim.x * gridDim.y * gridDim.z;
+  const unsigned bid = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+  if (tid == 0) part[bid] = b;
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) last = (atomicAdd(&st->counter, 1u) == nblk - 1);
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (tid >= 32) return;
+  const double s = warp_sum_parts(part, nblk);
+  if (tid != 0) return;
+  st->counter = 0;
+  st->first = 0;
+  st->pap = s;
+  if ((err && *(const volatile int*)err) || !(s > 0.0) || !isfinite(s)) {
+    st->status = MIX_BREAKDOWN;
+    return;
+  }
+  st->alpha = st->rho0 / s;
+}
+
+// TMA (cp.async.bulk.tensor) node-plane loads: the FP32 vectors are 3-D tensors [nz1][ny1][rp] floats; a copy
+// brings a [FPY][FBW] box whose x start is rounded down to 16 bytes, and zero-fills what lies outside the grid.
+constexpr int FNST = 4;                                     // node-plane stages in flight
+constexpr int FBW = 104;                                    // floats per staged node row (>= 99 + 3 of rounding)
+constexpr int kFacStageBytes = FPY * FBW * 4;               // bytes landed per array per stage
+constexpr int kFacStagePitch = (kFacStageBytes + 127) & ~127;
+constexpr size_t fac_smem_bytes(int mode) {
+  return (size_t)FNST * kFacStagePitch * (mode == 1 ? 2 : 1) + sizeof(float) * 2 * FY * 6 * FX;
+}
+
+__device__ __forceinline__ void tma_load_plane(void* dst, const CUtensorMap* map, int x, int y, int z, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n"
+      ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(bar)
+      : "memory");
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(FX * FY, 3) k_mv32f(GridDims g, const __grid_constant__ HexOpF op,
+                                                      const __grid_constant__ CUtensorMap tm_a,
+                                                      const __grid_constant__ CUtensorMap tm_b,
+                                                      float* __restrict__ pnew, float* __restrict__ y,
+                                                      const float* __restrict__ E, const uint8_t* __restrict__ nf,
+                                                      int projected, MixState* st, double* part, int zseg, int* err) {
+  extern __shared__ __align__(128) unsigned char fac_smem[];
+  // [FNST] stages of x (MODE 0) or z (MODE 1), then MODE 1: [FNST] stages of p_{t-1}; then y-exchange
+  float* yb = reinterpret_cast<float*>(fac_smem + (size_t)FNST * kFacStagePitch * (MODE == 1 ? 2 : 1));
+  __shared__ __align__(8) unsigned long long full[FNST];
+  __shared__ double sh[32];
+  if (MODE == 1 && st->status != MIX_RUNNING) return;
+  const float beta = MODE == 1 ? (float)st->beta : 0.0f;
+  const bool two = MODE == 1 && st->first == 0;  // p_t = z + beta p_{t-1} (else p_t = z)
+  const int l = threadIdx.x, w = threadIdx.y, tid = w * FX + l;
+  const int i0 = blockIdx.x * FOX, j0 = blockIdx.y * FOY, k0 = blockIdx.z * zseg;
+  const int k1 = min(k0 + zseg, g.nz1);
+  const int xs = (3 * (i0 - 1)) & ~3;   // staged row start (floats), 16-byte aligned, may be -4
+  const int rem = 3 * (i0 - 1) - xs;    // offset of node i0 - 1 in a staged row
+  const uint32_t tx_bytes = (uint32_t)kFacStageBytes * (two ? 2u : 1u);
+
+  // plane kk (k0 - 1 <= kk <= k1) lives in stage (kk - k0 + 1) % FNST, its use of the stage has parity
+  // ((kk - k0 + 1) / FNST) & 1
+  auto stage_of = [&](int kk) { return (kk - k0 + 1) % FNST; };
+  auto parity_of = [&](int kk) { return (uint32_t)(((kk - k0 + 1) / FNST) & 1); };
+  auto plane_a = [&](int sl) { return reinterpret_cast<float*>(fac_smem + (size_t)sl * kFacStagePitch); };
+  auto plane_b = [&](int sl) { return reinterpret_cast<float*>(fac_smem + (size_t)(FNST + sl) * kFacStagePitch); };
+  auto issue = [&](int kk) {  // one thread
+    const int sl = stage_of(kk);
+    const uint32_t bar = smem_u32(&full[sl]);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(tx_bytes) : "memory");
+    tma_load_plane(plane_a(sl), &tm_a, xs, j0 - 1, kk, bar);
+    if (two) tma_load_plane(plane_b(sl), &tm_b, xs, j0 - 1, kk, bar);
+  };
+  if (tid == 0) {
+    for (int q = 0; q < FNST; ++q)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&full[q])) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  }
+  __syncthreads();
+  if (tid == 0)
+    for (int kk = k0 - 1; kk <= min(k0 - 2 + FNST, k1); ++kk) issue(kk);
+  bool ok = true;
+  auto wait_plane = [&](int kk) {
+    if (!mbar_wait(smem_u32(&full[stage_of(kk)]), parity_of(kk))) ok = false;
+  };
+  // the 4 nodes of this thread's element in node plane kk: (x, y) = (0,0), (1,0), (0,1), (1,1)
+  auto gather4 = [&](int kk, float (&v)[4][3]) {
+    const int sl = stage_of(kk);
+    const float* a = plane_a(sl);
+    const float* b = plane_b(sl);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int o = (w + (q >> 1)) * FBW + rem + 3 * (l + (q & 1));
+#pragma unroll
+      for (int c = 0; c < 3; ++c) v[q][c] = two ? fmaf(beta, b[o + c], a[o + c]) : a[o + c];
+    }
+  };
+
+  const int ex = i0 - 1 + l, ey = j0 - 1 + w;
+  const bool exy = ex >= 0 && ex < g.nx && ey >= 0 && ey < g.ny;
+  const int64_t ebase = (int64_t)ex + (int64_t)g.nx * ey, eplane = (int64_t)g.nx * g.ny;
+  auto eload = [&](int kk) -> float { return (exy && kk >= 0 && kk < g.nz) ? __ldg(E + ebase + eplane * kk) : 0.f; };
+  const int nxo = i0 + l, nyo = j0 + w;  // owned node (local node (1, 1) of this thread's element)
+  const bool mine = l < FOX && w < FOY && nxo < g.nx1 && nyo < g.ny1;
+  const int64_t nbase = nxo + (int64_t)g.nx1 * nyo;                 // node index at plane 0
+  const int64_t fbase = (int64_t)g.rp * nyo + 3 * nxo;              // padded FP32 offset at plane 0
+  const int64_t fplane = (int64_t)g.rp * g.ny1;
+  const int64_t nplane = (int64_t)g.nx1 * g.ny1;
+
+  wait_plane(k0 - 1);
+  wait_plane(k0);
+  float ub[4][3];
+  gather4(k0 - 1, ub);
+  __syncthreads();  // the stage of plane k0 - 1 is refilled in the first step
+  float carry[3] = {0.f, 0.f, 0.f};
+  double pap = 0.0;
+  float e0 = eload(k0 - 1), e1 = eload(k0);
+  uint8_t f_next = (mine && projected && k0 < k1) ? nf[nbase + nplane * k0] : (uint8_t)0;
+  for (int kk = k0 - 1; kk < k1; ++kk) {
+    wait_plane(kk + 1);
+    float ut[4][3];
+    gather4(kk + 1, ut);
+    // stage of plane kk: read before the previous step's barrier (or the prologue's); refill it
+    if (tid == 0 && kk + FNST <= k1) {
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      issue(kk + FNST);
+    }
+    const float e_cur = e0;
+    e0 = e1;
+    e1 = eload(kk + 2);
+    const bool outp = mine && kk >= k0;
+    const uint8_t f = f_next;
+    if (outp && projected && kk + 1 < k1) f_next = nf[nbase + nplane * (kk + 1)];
+    if (MODE == 1 && mine && kk + 1 >= k0 && kk + 1 < k1) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) pnew[fbase + fplane * (kk + 1) + c] = ut[3][c];
+    }
+    float u[3][8], yv[3][8];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        u[c][b] = ub[b][c];
+        u[c][b + 4] = ut[b][c];
+      }
+    hex_apply(op, e_cur, u, yv);
+    // x: node column ex + 1 = own local x = 1 nodes + the x-neighbour element's local x = 0 nodes
+    float comb[2][2][3];  // [y][z][c]
+#pragma unroll
+    for (int by = 0; by < 2; ++by)
+#pragma unroll
+      for (int bz = 0; bz < 2; ++bz)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const float nb = __shfl_down_sync(0xffffffffu, yv[c][2 * by + 4 * bz], 1);
+          comb[by][bz][c] = yv[c][1 + 2 * by + 4 * bz] + nb;
+        }
+    // y: the row above adds its local y = 0 sums to this row's local y = 1 sums
+    float* ybw = yb + ((kk & 1) * FY + w) * 6 * FX + l;
+#pragma unroll
+    for (int bz = 0; bz < 2; ++bz)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) ybw[(3 * bz + c) * FX] = comb[0][bz][c];
+    __syncthreads();
+    if (mine) {
+      const float* ybr = yb + ((kk & 1) * FY + w + 1) * 6 * FX + l;
+      float top[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const float bot = comb[1][0][c] + ybr[c * FX];
+        top[c] = comb[1][1][c] + ybr[(3 + c) * FX];
+        if (outp) {
+          const float pv = ub[3][c];
+          const float out = carry[c] + bot;
+          const float yo = (f >> c & 1) ? pv : out;
+          y[fbase + fplane * kk + c] = yo;
+          if (MODE == 1) pap += (double)pv * (double)yo;
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) carry[c] = top[c];
+    }
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) ub[b][c] = ut[b][c];
+  }
+  if (!ok && err) atomicExch(err, 1);
+  if (MODE == 1) mv32_finish(pap, sh, st, part, tid, err);
+}
+
+// z-segment length of the factorised kernel: the CTAs of a launch run in ceil(CTAs / resident) waves of
+// (segment length + 1) plane steps each (the extra element plane below each segment); pick the segment
+// count with the least waves x steps, at least 4 planes per segment.
+static int fac_zseg(const GridDims& g, int resident) {
+  const int64_t txy = (int64_t)((g.nx1 + FOX - 1) / FOX) * ((g.ny1 + FOY - 1) / FOY);
+  const int max_segs = std::max(1, g.nz1 / 4);
+  int best_z = g.nz1;
+  int64_t best_cost = INT64_MAX;
+  for (int segs = 1; segs <= max_segs; ++segs) {
+    const int zs = (g.nz1 + segs - 1) / segs;
+    const int64_t n = txy * ((g.nz1 + zs - 1) / zs);
+    const int64_t cost = ((n + resident - 1) / resident) * (zs + 1);
+    if (cost < best_cost) {
+      best_cost = cost;
+      best_z = zs;
+    }
+  }
+  return best_z;
+}
+
+static dim3 fac_grid(const GridDims& g, int zseg) {
+  return dim3((unsigned)((g.nx1 + FOX - 1) / FOX), (unsigned)((g.ny1 + FOY - 1) / FOY),
+              (unsigned)((g.nz1 + zseg - 1) / zseg));
+}
+
+// ---------------------------------------------------------------------------------------------------------
 // FP32 K p on the 5th-generation tensor cores (tcgen05, kind::tf32, 3xTF32 for FP32-level products).
 // A CTA takes a 16 x 8 tile of elements per element plane (one MMA row per element, M = 128) and owns the
 // 15 x 7 nodes strictly inside it; CTAs overlap by one element in x and y. It marches over z: for element
@@ -374,9 +703,7 @@ constexpr int OX = CX - 1, OY = CY - 1; // owned nodes per tile
 constexpr int NX = CX + 1, NY = CY + 1; // node plane of the tile
 constexpr int TC_THREADS = 128;
 constexpr int TC_TMEM_COLS = 128;       // D: cols 0-31, A_hi: 32-55, A_lo: 64-87
-constexpr long long kMbarSpinLimit = 1ll << 22;
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 __device__ __forceinline__ uint32_t to_tf32(float v) {
   uint32_t r;
@@ -428,22 +755,6 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 #pragma unroll
   for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
-}
-
-// bounded wait for phase `parity` of an mbarrier; returns false if it gave up
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
-  for (long long spin = 0; spin < kMbarSpinLimit; ++spin) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(done)
-        : "r"(mbar), "r"(parity)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
 }
 
 template <int MODE>
@@ -499,7 +810,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_mv32tc(GridDims g, const __grid_
       int i = ie0 + lx, j = je0 + ly;
       float v = 0.f;
       if (kk >= 0 && kk < g.nz1 && i >= 0 && i < g.nx1 && j >= 0 && j < g.ny1) {
-        int64_t idx = 3 * (i + sy * j + sz * kk) + c;
+        int64_t idx = pidx(g, i, j + (int64_t)g.ny1 * kk, c);
         if (MODE == 1) {
           v = first ? __ldg(z + idx) : fmaf(beta, __ldg(pold + idx), __ldg(z + idx));
           if (owned_plane && lx >= 1 && lx <= OX && ly >= 1 && ly <= OY) pnew[idx] = v;
@@ -622,7 +933,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_mv32tc(GridDims g, const __grid_
         for (int c = 0; c < 3; ++c) {
           const float acc = carry[c] + bot[c];
           const float yv = (f & (1 << c)) ? pv[c] : acc;
-          y[3 * n + c] = yv;
+          y[pidx(g, ni, nj + (int64_t)g.ny1 * kk, c)] = yv;
           if (MODE == 1) pap += (double)pv[c] * (double)yv;
         }
       }
@@ -683,38 +994,92 @@ static dim3 tc_grid(const GridDims& g, int zseg) {
 // SM never ask for more than its 512 TMEM columns (4 x 128).
 constexpr int kTcPadSmem = 20 * 1024;
 
-// FP32 matvec launch, variant chosen per problem (SIMT FFMA kernel or tensor-core kernel)
+// TMA descriptor of an FP32 work vector: 3-D [nz1][ny1][rp] floats, box [1][FPY][FBW], zero fill outside.
+static int32_t encode_plane_map(mycel_problem* p, float* base, CUtensorMap* out) {
+  static PFN_cuTensorMapEncodeTiled encode = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled>(fn);
+  });
+  if (!encode) return set_error(p->ctx, MYCEL_E_DEVICE, "cuTensorMapEncodeTiled is not available from the driver");
+  const GridDims& g = p->g;
+  cuuint64_t dims[3] = {(cuuint64_t)g.rp, (cuuint64_t)g.ny1, (cuuint64_t)g.nz1};
+  cuuint64_t strides[2] = {(cuuint64_t)g.rp * 4, (cuuint64_t)g.rp * g.ny1 * 4};
+  cuuint32_t box[3] = {(cuuint32_t)FBW, (cuuint32_t)FPY, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = encode(out, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, estr,
+                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS)
+    return set_error(p->ctx, MYCEL_E_DEVICE, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+  return MYCEL_OK;
+}
+
+static const CUtensorMap* tmap_of(mycel_problem* p, const float* ptr) {
+  const float* bufs[4] = {p->f_r, p->f_z, p->f_p0, p->f_p1};
+  for (int q = 0; q < 4; ++q)
+    if (ptr == bufs[q]) return &p->f_tmap[q];
+  return nullptr;
+}
+
+// FP32 matvec launch, variant chosen per problem (MYCEL_MV32_*)
 template <int MODE>
 static void launch_mv32_variant(mycel_problem* p, cudaStream_t s, const float* xin, const float* z, const float* pold,
                                 float* pnew, float* y, int projected, MixState* st, double* part) {
   const GridDims& g = p->g;
-  if (p->use_tc == 1) {
+  if (p->mv32 == MYCEL_MV32_TENSOR) {
     int zs = tc_zseg(g, p->ctx->num_sms);
     k_mv32tc<MODE><<<tc_grid(g, zs), TC_THREADS, kTcPadSmem, s>>>(g, p->ketf, xin, z, pold, pnew, y, p->d_Ef,
                                                                   p->d_nflags, projected, st, part, zs, p->d_err);
-  } else {
+  } else if (p->mv32 == MYCEL_MV32_DENSE) {
     int zs = tile_zseg(g, p->ctx->num_sms);
     k_mv32<MODE><<<tile_grid(g, zs), dim3(TX, TY), 0, s>>>(g, p->kef, xin, z, pold, pnew, y, p->d_Ef, p->d_nflags,
                                                            projected, st, part, zs);
+  } else {
+    static int occ = 0;  // resident CTAs per SM (same for both modes: same block, registers within bounds)
+    if (!occ) {
+      int o = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_mv32f<1>, FX * FY, fac_smem_bytes(1));
+      occ = std::max(1, o);
+    }
+    int zs = fac_zseg(g, occ * p->ctx->num_sms);
+    const CUtensorMap* ta = tmap_of(p, MODE == 1 ? z : xin);
+    const CUtensorMap* tb = MODE == 1 ? tmap_of(p, pold) : ta;
+    if (!ta || !tb) {  // internal invariant: inputs are always one of the four mapped work vectors
+      std::fprintf(stderr, "mycel: FP32 matvec input is not a mapped work vector\n");
+      std::abort();
+    }
+    k_mv32f<MODE><<<fac_grid(g, zs), dim3(FX, FY), fac_smem_bytes(MODE), s>>>(
+        g, p->hexop, *ta, *tb, pnew, y, p->d_Ef, p->d_nflags, projected, st, part, zs, p->d_err);
   }
 }
 
-// Autotuner: on first use, time both variants (K x on the problem's FP32 buffers, after one warm-up launch)
-// and keep the faster; a tensor-core run that reports a failed wait is never chosen.
+// Autotuner: on first use, time every variant (K x on the problem's FP32 buffers, after one warm-up launch)
+// and keep the fastest; a tensor-core run that reports a failed wait is never chosen.
 static int32_t resolve_mv32(mycel_problem* p) {
-  if (p->use_tc >= 0) return MYCEL_OK;
+  if (p->mv32 > 0) return MYCEL_OK;
   mycel_ctx* c = p->ctx;
   cudaStream_t s = c->stream;
-  const int64_t n = p->g.nd;
-  MYCEL_CUDA(c, cudaMemsetAsync(p->f_r, 0, sizeof(float) * n, s));
+  MYCEL_CUDA(c, cudaMemsetAsync(p->f_r, 0, sizeof(float) * p->g.n32, s));
   MYCEL_CUDA(c, cudaMemsetAsync(p->d_err, 0, sizeof(int), s));
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  float t[2] = {0.f, 0.f};
-  for (int v = 0; v < 2; ++v) {
-    p->use_tc = v;
+  const int variants[3] = {MYCEL_MV32_FACTORED, MYCEL_MV32_DENSE, MYCEL_MV32_TENSOR};
+  float t[3] = {0.f, 0.f, 0.f};
+  int herr = 0;
+  for (int v = 0; v < 3; ++v) {
+    p->mv32 = variants[v];
+    (void)cudaGetLastError();
     launch_mv32_variant<0>(p, s, p->f_r, nullptr, nullptr, nullptr, p->f_ap, 1, nullptr, nullptr);
+    const cudaError_t le = cudaGetLastError();
+    const bool launched = le == cudaSuccess;  // a variant that cannot launch here is skipped, with a warning
+    if (!launched)
+      std::fprintf(stderr, "mycel: FP32 matvec variant %d not launchable: %s\n", variants[v], cudaGetErrorString(le));
     cudaEventRecord(e0, s);
     for (int r = 0; r < 3; ++r)
       launch_mv32_variant<0>(p, s, p->f_r, nullptr, nullptr, nullptr, p->f_ap, 1, nullptr, nullptr);
@@ -724,16 +1089,26 @@ static int32_t resolve_mv32(mycel_problem* p) {
     if (e != cudaSuccess) {
       cudaEventDestroy(e0);
       cudaEventDestroy(e1);
-      p->use_tc = -1;
+      p->mv32 = -1;
       return set_error(c, MYCEL_E_DEVICE, std::string("matvec autotune: ") + cudaGetErrorString(e));
     }
     cudaEventElapsedTime(&t[v], e0, e1);
+    if (!launched) t[v] = 1e30f;
+    MYCEL_CUDA(c, cudaMemcpy(&herr, p->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (herr) {  // a bounded wait gave up: never choose this variant
+      t[v] = 1e30f;
+      MYCEL_CUDA(c, cudaMemset(p->d_err, 0, sizeof(int)));
+    }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  int herr = 0;
-  MYCEL_CUDA(c, cudaMemcpy(&herr, p->d_err, sizeof(int), cudaMemcpyDeviceToHost));
-  p->use_tc = (!herr && t[1] < t[0]) ? 1 : 0;
+  int best = 0;
+  for (int v = 1; v < 3; ++v)
+    if (t[v] < t[best]) best = v;
+  p->mv32 = variants[best];
+  if (std::getenv("MYCEL_VERBOSE"))
+    std::fprintf(stderr, "mycel: FP32 matvec autotune (ms per 3 launches) factored %.4f dense %.4f tensor %.4f -> %d\n",
+                 t[0], t[1], t[2], p->mv32);
   return MYCEL_OK;
 }
 
@@ -831,24 +1206,34 @@ __global__ void __launch_bounds__(kT) k_xr32(int64_t n, float* __restrict__ x, f
   if (st->iter >= st->max_iter) st->status = MIX_MAXITER;
 }
 
-// FP64 refinement: u += x32, x32 = 0; then (after A u) r64 = P(b - A u), r32 = (float) r64, partials of r64^2
-__global__ void k_flush_u(int64_t n, double* __restrict__ u, float* __restrict__ x32) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    u[i] += (double)x32[i];
-    x32[i] = 0.f;
-  }
+// Conversions between box-ordered FP64 DOF vectors and the padded FP32 layout walk node rows: row q = j + ny1 k
+// holds DOFs [3 nx1 q, 3 nx1 (q + 1)) in FP64 and floats [rp q, rp q + 3 nx1) in FP32. CTA b takes rows b,
+// b + gridDim.x, ...; its threads the DOFs of a row.
+// FP64 refinement: u += x32, x32 = 0
+__global__ void k_flush_u(GridDims g, double* __restrict__ u, float* __restrict__ x32) {
+  const int rl = 3 * g.nx1;
+  for (int64_t q = blockIdx.x; q < (int64_t)g.ny1 * g.nz1; q += gridDim.x)
+    for (int t = threadIdx.x; t < rl; t += blockDim.x) {
+      const int64_t f = (int64_t)g.rp * q + t;
+      u[(int64_t)rl * q + t] += (double)x32[f];
+      x32[f] = 0.f;
+    }
 }
 
-__global__ void k_resid64(int64_t n, const uint8_t* __restrict__ nf, const double* __restrict__ b,
+// after A u: r64 = P(b - A u), r32 = (float) r64, CTA partials of r64^2
+__global__ void k_resid64(GridDims g, const uint8_t* __restrict__ nf, const double* __restrict__ b,
                           const double* __restrict__ au, float* __restrict__ r32, double* part) {
   __shared__ double sh[32];
   double s = 0.0;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    bool con = nf[i / 3] & (1 << (i % 3));
-    double v = con ? 0.0 : (b[i] - au[i]);
-    r32[i] = (float)v;
-    s += v * v;
-  }
+  const int rl = 3 * g.nx1;
+  for (int64_t q = blockIdx.x; q < (int64_t)g.ny1 * g.nz1; q += gridDim.x)
+    for (int t = threadIdx.x; t < rl; t += blockDim.x) {
+      const int64_t i = (int64_t)rl * q + t;
+      const bool con = nf[i / 3] & (1 << (t % 3));
+      const double v = con ? 0.0 : (b[i] - au[i]);
+      r32[(int64_t)g.rp * q + t] = (float)v;
+      s += v * v;
+    }
   double bs = bsum(s, sh);
   if (threadIdx.x == 0) part[blockIdx.x] = bs;
 }
@@ -859,13 +1244,15 @@ __global__ void k_sum_part(const double* part, int nb, double* out) {
   if (threadIdx.x == 0) *out = s;
 }
 
-__global__ void k_to_f32(int64_t n, const double* __restrict__ a, float* __restrict__ b) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    b[i] = (float)a[i];
+__global__ void k_to_f32(GridDims g, const double* __restrict__ a, float* __restrict__ b) {
+  const int rl = 3 * g.nx1;
+  for (int64_t q = blockIdx.x; q < (int64_t)g.ny1 * g.nz1; q += gridDim.x)
+    for (int t = threadIdx.x; t < rl; t += blockDim.x) b[(int64_t)g.rp * q + t] = (float)a[(int64_t)rl * q + t];
 }
-__global__ void k_to_f64(int64_t n, const float* __restrict__ a, double* __restrict__ b) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    b[i] = (double)a[i];
+__global__ void k_to_f64(GridDims g, const float* __restrict__ a, double* __restrict__ b) {
+  const int rl = 3 * g.nx1;
+  for (int64_t q = blockIdx.x; q < (int64_t)g.ny1 * g.nz1; q += gridDim.x)
+    for (int t = threadIdx.x; t < rl; t += blockDim.x) b[(int64_t)rl * q + t] = (double)a[(int64_t)g.rp * q + t];
 }
 
 // grid for the streaming kernels: fixed by n (deterministic reductions), at most 8 CTAs per SM
@@ -878,28 +1265,35 @@ void launch_E_to_f32(mycel_problem* p) {
   (void)p;  // k_update_E writes the FP32 copy of E alongside the FP64 one
 }
 
-void mixed_apply_k_f64io(mycel_problem* p, const double* x, double* y, int projected) {
-  cudaStream_t s = p->ctx->stream;
-  int64_t n = p->g.nd;
-  float* fx = (float*)p->d_r;  // borrow FP64 workspace as FP32 staging
-  float* fy = fx + n;
-  k_to_f32<<<stream_blocks(p), kT, 0, s>>>(n, x, fx);
-  launch_mv32_variant<0>(p, s, fx, nullptr, nullptr, nullptr, fy, projected, nullptr, nullptr);
-  k_to_f64<<<stream_blocks(p), kT, 0, s>>>(n, fy, y);
-  p->ctx->launches += 3;
-}
-
+// FP32 work vectors of the mixed form (padded layout, pads zero) and their TMA descriptors
 static int32_t ensure_mixed(mycel_problem* p) {
   if (p->f_x) return MYCEL_OK;
-  int64_t n = p->g.nd;
-  size_t fb = sizeof(float) * (size_t)n + 64;
+  const size_t fb = sizeof(float) * (size_t)p->g.n32 + 64;
   cudaError_t e = cudaSuccess;
   float** bufs[] = {&p->f_x, &p->f_r, &p->f_z, &p->f_p0, &p->f_p1, &p->f_ap};
   for (float** b : bufs) {
     if ((e = cudaMalloc((void**)b, fb)) != cudaSuccess) break;
     p->device_bytes += (int64_t)fb;
+    cudaMemsetAsync(*b, 0, fb, p->ctx->stream);
   }
   if (e != cudaSuccess) return set_error(p->ctx, MYCEL_E_OOM, "out of device memory for the mixed-precision workspace");
+  float* mapped[4] = {p->f_r, p->f_z, p->f_p0, p->f_p1};
+  for (int q = 0; q < 4; ++q) {
+    int32_t st = encode_plane_map(p, mapped[q], &p->f_tmap[q]);
+    if (st) return st;
+  }
+  return MYCEL_OK;
+}
+
+// y = K x (projected: ApplyA form) through the FP32 operator; x and y box-ordered FP64 device vectors
+int32_t mixed_apply_k_f64io(mycel_problem* p, const double* x, double* y, int projected) {
+  int32_t st = ensure_mixed(p);
+  if (st) return st;
+  cudaStream_t s = p->ctx->stream;
+  k_to_f32<<<stream_blocks(p), kT, 0, s>>>(p->g, x, p->f_r);
+  launch_mv32_variant<0>(p, s, p->f_r, nullptr, nullptr, nullptr, p->f_ap, projected, nullptr, nullptr);
+  k_to_f64<<<stream_blocks(p), kT, 0, s>>>(p->g, p->f_ap, y);
+  p->ctx->launches += 3;
   return MYCEL_OK;
 }
 
@@ -929,7 +1323,6 @@ static int32_t capture_mixed_graph(mycel_problem* p, int chunk) {
       if (!p->prof_ev[k][j]) cudaEventCreate(&p->prof_ev[k][j]);
   }
   cudaStream_t s = c->stream;
-  int64_t n = p->g.nd;
   MixState* st = mix_state(p);
   double* part = p->d_part2;
   int sb = stream_blocks(p);
@@ -942,7 +1335,7 @@ static int32_t capture_mixed_graph(mycel_problem* p, int chunk) {
       float* pprev = (t & 1) ? p->f_p0 : p->f_p1;
       if (!(c->profile && t == 0))
         launch_mv32_variant<1>(p, s, nullptr, p->f_z, pprev, pcur, p->f_ap, 1, st, part);
-      k_xr32<<<sb, kT, 0, s>>>(n, p->f_x, p->f_r, p->f_z, pcur, p->f_ap, p->d_invdf, st, part, 0);
+      k_xr32<<<sb, kT, 0, s>>>(p->g.n32, p->f_x, p->f_r, p->f_z, pcur, p->f_ap, p->d_invdf, st, part, 0);
     }
     MYCEL_CUDA(c, cudaStreamEndCapture(s, &graph));
     MYCEL_CUDA(c, cudaGraphInstantiate(&p->pcg32_graph[k], graph, 0));
@@ -973,7 +1366,7 @@ static int32_t true_residual(mycel_problem* p, const double* d_b, const double* 
   double* part = p->d_part2;
   double* scal = p->d_part2 + p->n_part2 - 128;
   launch_matvec64(p, d_u, p->d_ap, 1, nullptr);
-  k_resid64<<<sb, kT, 0, s>>>(p->g.nd, p->d_nflags, d_b, p->d_ap, p->f_r, part);
+  k_resid64<<<sb, kT, 0, s>>>(p->g, p->d_nflags, d_b, p->d_ap, p->f_r, part);
   k_sum_part<<<1, 32, 0, s>>>(part, sb, scal);
   c->launches += 2;
   double* h = (double*)((char*)c->pinned + 1024);
@@ -1028,6 +1421,7 @@ int32_t mixed_solve_entry(mycel_problem* p, const double* d_b, const int32_t* d_
     return MYCEL_OK;
   }
   const int chunk = 16;
+  MYCEL_CUDA(c, cudaMemsetAsync(p->d_err, 0, sizeof(int), s));  // bounded-wait failures of this solve only
   if ((st = resolve_mv32(p))) return st;
   if ((st = capture_mixed_graph(p, chunk))) return st;
   double rn = 0.0;
@@ -1043,9 +1437,9 @@ int32_t mixed_solve_entry(mycel_problem* p, const double* d_b, const int32_t* d_
   struct EvGuard { cudaEvent_t* e; ~EvGuard() { cudaEventDestroy(e[0]); cudaEventDestroy(e[1]); } } evg{evs};
   int total_iter = 0;
   if (!ok) {
-    cudaMemsetAsync(p->f_x, 0, sizeof(float) * n, s);
+    cudaMemsetAsync(p->f_x, 0, sizeof(float) * p->g.n32, s);
     k_mix_init<<<1, 1, 0, s>>>(ms, 0.5 * tol * bnorm, max_iter);
-    k_xr32<<<sb, kT, 0, s>>>(n, p->f_x, p->f_r, p->f_z, p->f_p0, p->f_ap, p->d_invdf, ms, part, 2);
+    k_xr32<<<sb, kT, 0, s>>>(p->g.n32, p->f_x, p->f_r, p->f_z, p->f_p0, p->f_ap, p->d_invdf, ms, part, 2);
     c->launches += 2;
     int64_t launched = 0;
     const int64_t cap = (int64_t)max_iter + 64 * chunk + 4096;
@@ -1094,9 +1488,9 @@ int32_t mixed_solve_entry(mycel_problem* p, const double* d_b, const int32_t* d_
       // the latest direction is in f_p{(m-1)&1} after m iterations since the chunks restarted
       int m = total_iter - iter_at_resume;
       if (m > 0 && (m & 1))
-        MYCEL_CUDA(c, cudaMemcpyAsync(p->f_p1, p->f_p0, sizeof(float) * n, cudaMemcpyDeviceToDevice, s));
+        MYCEL_CUDA(c, cudaMemcpyAsync(p->f_p1, p->f_p0, sizeof(float) * p->g.n32, cudaMemcpyDeviceToDevice, s));
       // reliable update: u += x32; r = P(b - A u) in FP64
-      k_flush_u<<<sb, kT, 0, s>>>(n, d_u, p->f_x);
+      k_flush_u<<<sb, kT, 0, s>>>(p->g, d_u, p->f_x);
       c->launches++;
       ++flushes;
       if ((st = true_residual(p, d_b, d_u, &rn))) return st;
@@ -1106,7 +1500,7 @@ int32_t mixed_solve_entry(mycel_problem* p, const double* d_b, const int32_t* d_
         break;
       }
       if (status != MIX_FLUSH || total_iter >= max_iter) break;
-      k_xr32<<<sb, kT, 0, s>>>(n, p->f_x, p->f_r, p->f_z, p->f_p0, p->f_ap, p->d_invdf, ms, part, 1);
+      k_xr32<<<sb, kT, 0, s>>>(p->g.n32, p->f_x, p->f_r, p->f_z, p->f_p0, p->f_ap, p->d_invdf, ms, part, 1);
       c->launches++;
       iter_at_resume = total_iter;
     }

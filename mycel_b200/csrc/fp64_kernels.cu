@@ -218,7 +218,7 @@ __global__ void __launch_bounds__(256) k_diag(GridDims g, const __grid_constant_
     double iv = fabs(d) > 1e-30 ? 1.0 / d : 1.0;
     diag[3 * n + c] = d;
     invd[3 * n + c] = iv;
-    if (invdf) invdf[3 * n + c] = (float)iv;
+    if (invdf) invdf[pidx(g, cn.i, cn.j + (int64_t)g.ny1 * cn.k, c)] = (float)iv;
   }
 }
 

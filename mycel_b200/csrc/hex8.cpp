@@ -112,4 +112,28 @@ void split_ke_tf32(const double* ke, KeTf* out) {
     }
 }
 
+// Factorised KE for the FP32 fast path. With trilinear shape functions N_a = phi(x) phi(y) phi(z) on a cube
+// and exact (2x2x2 Gauss) integration, every 3x3 block of KE(1, nu) is a sum of Kronecker products of the 1-D
+// 2x2 matrices S = int phi'_a phi'_b, M = int phi_a phi_b and C = int phi'_a phi_b:
+//   K[i][i] = (lambda + 2 mu) S_i M_j M_k + mu (M_i S_j M_k + M_i M_j S_k)
+//   K[i][j] = lambda C_i C^T_j M_k + mu C^T_i C_j M_k                      (i != j, k the third axis)
+// (lambda = nu / ((1 + nu)(1 - 2 nu)), mu = 1 / (2 (1 + nu)) for E = 1, as in the constitutive matrix of
+// Hex8Element.CreateConstitutiveMatrix, src/Mycel.Core/Fem/Hex8Element.cs:183-215). In the basis
+// e = (1, 1), o = (-1, 1) of each axis: S e = 0, S o = 2 o; M e = e / 2, M o = o / 6; C e = o, C o = 0;
+// C^T o = e, C^T e = 0. So K is diagonal per component (eigenvalues below) plus one coupling per pair of
+// components between basis functions whose parities on the two axes are swapped. Coefficients of an
+// element vector in that basis are its 8-point Walsh-Hadamard transform / 8; the h / 8 is folded in here.
+void build_hexop(double h, double nu, HexOpF* out) {
+  const double lam = nu / ((1.0 + nu) * (1.0 - 2.0 * nu)), mu = 1.0 / (2.0 * (1.0 + nu));
+  const double l2m = lam + 2.0 * mu, sc = h / 8.0;
+  const double dcl[2][3] = {{0.0, mu / 2.0, mu / 3.0},
+                            {l2m / 2.0, l2m / 6.0 + mu / 6.0, l2m / 18.0 + mu / 9.0}};
+  for (int a = 0; a < 2; ++a)
+    for (int n = 0; n < 3; ++n) out->dcl[a][n] = (float)(dcl[a][n] * sc);
+  out->lam[0] = (float)(lam / 2.0 * sc);
+  out->lam[1] = (float)(lam / 6.0 * sc);
+  out->mu[0] = (float)(mu / 2.0 * sc);
+  out->mu[1] = (float)(mu / 6.0 * sc);
+}
+
 }  // namespace mycel

@@ -1,5 +1,6 @@
 // Internal declarations of libmycel_b200: device state of a problem, kernel launchers, helpers.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -15,6 +16,10 @@ struct GridDims {
   int nx, ny, nz;    // elements per axis
   int nx1, ny1, nz1; // nodes per axis
   int64_t ne, nn, nd;
+  // FP32 vectors of the mixed form use a padded layout: each node row (fixed j, k) holds its 3 nx1 DOFs
+  // contiguously from a 16-byte aligned start, row pitch rp floats (multiple of 4); pads stay zero.
+  int rp;
+  int64_t n32;       // rp * ny1 * nz1
 };
 
 inline GridDims make_dims(int nx, int ny, int nz) {
@@ -24,13 +29,26 @@ inline GridDims make_dims(int nx, int ny, int nz) {
   g.ne = (int64_t)nx * ny * nz;
   g.nn = (int64_t)g.nx1 * g.ny1 * g.nz1;
   g.nd = 3 * g.nn;
+  g.rp = (3 * g.nx1 + 3) & ~3;
+  g.n32 = (int64_t)g.rp * g.ny1 * g.nz1;
   return g;
 }
+
+// index of DOF c of node (i, j, k) in the padded FP32 layout
+#ifdef __CUDACC__
+__host__ __device__
+#endif
+inline int64_t pidx(const GridDims& g, int i, int64_t jk, int c) { return (int64_t)g.rp * jk + 3 * i + c; }
 
 struct KeD { double v[576]; };  // element stiffness (row-major), FP64
 struct KeF { float v[576]; };   // FP32 copy for the mixed form
 // KE split for 3xTF32 tensor-core products: rows padded to 32 (rows 24..31 zero), row-major [32][24]
 struct KeTf { float hi[32 * 24]; float lo[32 * 24]; };
+// Hex8 operator of a cube element in the per-axis (sum, difference) basis, FP32, scaled by h / 8 (see
+// build_hexop). dcl[pc][n]: eigenvalue of component c at a basis function whose c-axis factor is even (0) or
+// odd (1) and with n odd factors on the other two axes; lam[pk], mu[pk]: coupling constants lambda m(pk),
+// mu m(pk) of two different components, pk the parity on the third axis.
+struct HexOpF { float dcl[2][3]; float lam[2]; float mu[2]; };
 
 // Node flag bits (one byte per node): bits 0-2 = DOF c constrained, bit 3 = node active.
 enum : uint8_t { NF_CX = 1, NF_CY = 2, NF_CZ = 4, NF_ACTIVE = 8 };
@@ -95,8 +113,9 @@ struct mycel_problem {
   mycel::KeD ke{};
   mycel::KeF kef{};
   mycel::KeTf ketf{};
-  int use_tc = -1;                // FP32 matvec variant: -1 not chosen yet, 0 SIMT, 1 tensor cores
-  int tune_mv32 = 0;              // requested variant: 0 autotune, 1 SIMT, 2 tensor cores
+  mycel::HexOpF hexop{};
+  int mv32 = -1;                  // FP32 matvec variant in use: -1 not chosen yet, else MYCEL_MV32_* (1..3)
+  int tune_mv32 = 0;              // requested variant: 0 autotune, else MYCEL_MV32_*
   int* d_err = nullptr;           // device error word (bounded waits that gave up)
   double diag_ke[24];
   int64_t n_active = 0, n_active_nodes = 0, n_active_fixed = 0;
@@ -122,13 +141,14 @@ struct mycel_problem {
   float* d_Ef = nullptr;          // [ne] FP32 copy
   double* d_diag = nullptr;       // [nd] DiagA
   double* d_invd = nullptr;       // [nd] Jacobi inverse diagonal
-  float* d_invdf = nullptr;       // [nd] FP32 copy
+  float* d_invdf = nullptr;       // [n32] FP32 copy, padded layout
   // PCG workspace (FP64)
   double *d_r = nullptr, *d_z = nullptr, *d_p = nullptr, *d_ap = nullptr, *d_x = nullptr;
   double* d_part = nullptr;       // [2*nblocks] partial sums
   mycel::PcgState* d_state = nullptr;
   // mixed-form workspace
   float *f_x = nullptr, *f_r = nullptr, *f_z = nullptr, *f_p0 = nullptr, *f_p1 = nullptr, *f_ap = nullptr;
+  CUtensorMap f_tmap[4];          // TMA descriptors of f_r, f_z, f_p0, f_p1 (node-plane boxes of the FP32 matvec)
   double* d_r64 = nullptr;        // refinement residual
   double* d_part2 = nullptr;      // [many] FP64 partials for mixed dots
   int64_t n_part2 = 0;
@@ -171,6 +191,7 @@ int32_t set_error(mycel_ctx* ctx, int32_t code, const std::string& msg);
 // ---- host setup ----
 void build_ke(double h, double nu, double* ke);  // Hex8Element.CreateKe semantics
 void split_ke_tf32(const double* ke, KeTf* out);   // hi = tf32(KE), lo = tf32(KE - hi), rows padded to 32
+void build_hexop(double h, double nu, HexOpF* out);  // factorised form of KE(h, nu), FP32
 int64_t num_blocks8192(int64_t n);
 
 // ---- FP64 plain-path launchers (fp64_kernels.cu, compiled with -fmad=false) ----
@@ -219,7 +240,7 @@ int launch_oc(mycel_ctx* ctx, int64_t n, const int32_t* d_index /*box index of e
 // ---- mixed form (fp32_kernels.cu) ----
 void launch_E_to_f32(mycel_problem* p);
 void launch_matvec32(mycel_problem* p, const float* x, float* y, int projected);
-void mixed_apply_k_f64io(mycel_problem* p, const double* x, double* y, int projected);
+int32_t mixed_apply_k_f64io(mycel_problem* p, const double* x, double* y, int projected);
 int32_t mixed_solve_entry(mycel_problem* p, const double* d_b, const int32_t* d_nz, int32_t n_nz, double* d_u,
                           double tol, int max_iter, const volatile int32_t* cancel, mycel_pcg_result* res);
 

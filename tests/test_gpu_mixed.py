@@ -22,7 +22,7 @@ def exact_oracle(oracle):
     oracle.set_modes(0, 0)
 
 
-@pytest.mark.parametrize("variant", [1, 2], ids=["simt", "tensor"])
+@pytest.mark.parametrize("variant", [1, 2, 3], ids=["dense", "tensor", "factored"])
 @pytest.mark.parametrize("shape", [(1, 1, 1), (5, 3, 2), (33, 17, 9), (70, 9, 20), (16, 8, 3)])
 def test_fp32_matvec_close_to_fp64(oracle, ctx, shape, variant):
     m = carved_model(*shape, seed=3, frac=0.15) if shape[0] > 2 else tiny_test_model(*shape)
@@ -47,7 +47,7 @@ def test_mixed_static_solve_matches_fp64(oracle, ctx):
     assert np.array_equal(r.u[m.fixed_dofs], np.zeros(m.fixed_dofs.size))
 
 
-@pytest.mark.parametrize("variant", [1, 2], ids=["simt", "tensor"])
+@pytest.mark.parametrize("variant", [1, 2, 3], ids=["dense", "tensor", "factored"])
 def test_mixed_pcg_each_matvec_variant(oracle, ctx, variant):
     m = carved_model(31, 12, 9, seed=8, emin_ratio=1e-9)
     om, pr = oracle.Model(m), api.Problem(m, ctx)
