@@ -394,68 +394,79 @@ static dim3 tile_grid(const GridDims& g, int zseg) {
 // ---------------------------------------------------------------------------------------------------------
 constexpr int FX = 32, FY = 8;
 constexpr int FOX = FX - 1, FOY = FY - 1;  // owned nodes per tile
-constexpr int FPX = FX + 1, FPY = FY + 1;  // node plane with halo
+constexpr int FPY = FY + 1;                // node rows of a staged plane (with halo)
+
+// Packed FP32x2 arithmetic (sm_100): lane .x and lane .y are two independent elements.
+__device__ __forceinline__ float2 f2(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 f2add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 f2sub(float2 a, float2 b) { return __ffma2_rn(b, f2(-1.f), a); }  // exact -b
+__device__ __forceinline__ float2 f2mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 f2fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 
 // 8-point Walsh-Hadamard butterflies over the index bits (x, y, z): afterwards v[p] = sum_a s_p(a) v_a,
 // s_p(a) the product over the axes odd in p of (2 a_axis - 1).
-__device__ __forceinline__ void wht8(float (&v)[8]) {
+__device__ __forceinline__ void wht8x2(float2 (&v)[8]) {
 #pragma unroll
   for (int bit = 1; bit < 8; bit <<= 1)
 #pragma unroll
     for (int a = 0; a < 8; ++a)
       if (!(a & bit)) {
-        const float lo = v[a], hi = v[a | bit];
-        v[a] = hi + lo;
-        v[a | bit] = hi - lo;
+        const float2 lo = v[a], hi = v[a | bit];
+        v[a] = f2add(hi, lo);
+        v[a | bit] = f2sub(hi, lo);
       }
 }
 
 // node values from basis coefficients: per axis (even e, odd o) -> (e - o, e + o)
-__device__ __forceinline__ void iwht8(float (&v)[8]) {
+__device__ __forceinline__ void iwht8x2(float2 (&v)[8]) {
 #pragma unroll
   for (int bit = 1; bit < 8; bit <<= 1)
 #pragma unroll
     for (int a = 0; a < 8; ++a)
       if (!(a & bit)) {
-        const float e = v[a], o = v[a | bit];
-        v[a] = e - o;
-        v[a | bit] = e + o;
+        const float2 e = v[a], o = v[a | bit];
+        v[a] = f2sub(e, o);
+        v[a | bit] = f2add(e, o);
       }
 }
 
-// y = E KE(h) u for one element; u[c][a], y[c][a]: component c at local node a = x | y << 1 | z << 2
-// (node order (0,0,0),(1,0,0),(0,1,0),(1,1,0),(0,0,1),... by bits, not the reference's local numbering).
-__device__ __forceinline__ void hex_apply(const HexOpF& op, float E, float (&u)[3][8], float (&y)[3][8]) {
+// y = E KE(h) u for two elements at once (lanes .x, .y); u[c][a]: component c at local node
+// a = x | y << 1 | z << 2 (bit order, not the reference's local numbering). The outputs of component c are
+// handed to sink(c, y_c[8]) as soon as they are formed, which keeps few of them live.
+template <class Sink>
+__device__ __forceinline__ void hex_apply2(const HexOpF& op, float2 E, float2 (&u)[3][8], Sink&& sink) {
 #pragma unroll
-  for (int c = 0; c < 3; ++c) wht8(u[c]);
-  float d[2][3], lam[2], mu[2];
+  for (int c = 0; c < 3; ++c) wht8x2(u[c]);
+  float2 d[2][3], lam[2], mu[2];
 #pragma unroll
   for (int a = 0; a < 2; ++a) {
 #pragma unroll
-    for (int n = 0; n < 3; ++n) d[a][n] = E * op.dcl[a][n];
-    lam[a] = E * op.lam[a];
-    mu[a] = E * op.mu[a];
+    for (int n = 0; n < 3; ++n) d[a][n] = f2mul(E, f2(op.dcl[a][n]));
+    lam[a] = f2mul(E, f2(op.lam[a]));
+    mu[a] = f2mul(E, f2(op.mu[a]));
   }
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    y[c][0] = 0.f;  // rigid translation: no force
+    float2 y[8];
+    y[0] = f2(0.f);  // rigid translation: no force
 #pragma unroll
     for (int p = 1; p < 8; ++p) {
       const int pc = (p >> c) & 1;
       const int n = (p & 1) + ((p >> 1) & 1) + ((p >> 2) & 1) - pc;
-      float acc = d[pc][n] * u[c][p];
+      float2 acc = f2mul(d[pc][n], u[c][p]);
 #pragma unroll
       for (int j = 0; j < 3; ++j) {
         if (j == c) continue;
         const int k = 3 - c - j;
         const int pj = (p >> j) & 1, pk = (p >> k) & 1;
         const int q = p ^ (1 << c) ^ (1 << j);
-        if (pc == 1 && pj == 0) acc = fmaf(lam[pk], u[j][q], acc);
-        if (pc == 0 && pj == 1) acc = fmaf(mu[pk], u[j][q], acc);
+        if (pc == 1 && pj == 0) acc = f2fma(lam[pk], u[j][q], acc);
+        if (pc == 0 && pj == 1) acc = f2fma(mu[pk], u[j][q], acc);
       }
-      y[c][p] = acc;
+      y[p] = acc;
     }
-    iwht8(y[c]);
+    iwht8x2(y);
+    sink(c, y);
   }
 }
 
@@ -494,7 +505,7 @@ constexpr int FBW = 104;                                    // floats per staged
 constexpr int kFacStageBytes = FPY * FBW * 4;               // bytes landed per array per stage
 constexpr int kFacStagePitch = (kFacStageBytes + 127) & ~127;
 constexpr size_t fac_smem_bytes(int mode) {
-  return (size_t)FNST * kFacStagePitch * (mode == 1 ? 2 : 1) + sizeof(float) * 2 * FY * 6 * FX;
+  return (size_t)FNST * kFacStagePitch * (mode == 1 ? 2 : 1) + sizeof(float) * 2 * FY * 9 * FX;
 }
 
 __device__ __forceinline__ void tma_load_plane(void* dst, const CUtensorMap* map, int x, int y, int z, uint32_t bar) {
@@ -505,7 +516,7 @@ __device__ __forceinline__ void tma_load_plane(void* dst, const CUtensorMap* map
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(FX * FY, 3) k_mv32f(GridDims g, const __grid_constant__ HexOpF op,
+__global__ void __launch_bounds__(FX * FY, 2) k_mv32f(GridDims g, const __grid_constant__ HexOpF op,
                                                       const __grid_constant__ CUtensorMap tm_a,
                                                       const __grid_constant__ CUtensorMap tm_b,
                                                       float* __restrict__ pnew, float* __restrict__ y,
@@ -525,19 +536,20 @@ __global__ void __launch_bounds__(FX * FY, 3) k_mv32f(GridDims g, const __grid_c
   const int xs = (3 * (i0 - 1)) & ~3;   // staged row start (floats), 16-byte aligned, may be -4
   const int rem = 3 * (i0 - 1) - xs;    // offset of node i0 - 1 in a staged row
   const uint32_t tx_bytes = (uint32_t)kFacStageBytes * (two ? 2u : 1u);
+  // Element planes k0-1 .. k1-1 are taken two per step (the last step may add plane k1, whose nodes are
+  // not owned). Node plane k0 - 1 + r ("rel r", r = 0 .. rmax) lives in stage r % FNST; its use of the
+  // stage has mbarrier parity (r / FNST) & 1. Step m needs rel 2m (carried), 2m + 1 and 2m + 2.
+  const int nsteps = (k1 - k0 + 2) >> 1;
+  const int rmax = 2 * nsteps;
 
-  // plane kk (k0 - 1 <= kk <= k1) lives in stage (kk - k0 + 1) % FNST, its use of the stage has parity
-  // ((kk - k0 + 1) / FNST) & 1
-  auto stage_of = [&](int kk) { return (kk - k0 + 1) % FNST; };
-  auto parity_of = [&](int kk) { return (uint32_t)(((kk - k0 + 1) / FNST) & 1); };
   auto plane_a = [&](int sl) { return reinterpret_cast<float*>(fac_smem + (size_t)sl * kFacStagePitch); };
   auto plane_b = [&](int sl) { return reinterpret_cast<float*>(fac_smem + (size_t)(FNST + sl) * kFacStagePitch); };
-  auto issue = [&](int kk) {  // one thread
-    const int sl = stage_of(kk);
+  auto issue = [&](int r) {  // one thread
+    const int sl = r % FNST;
     const uint32_t bar = smem_u32(&full[sl]);
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(tx_bytes) : "memory");
-    tma_load_plane(plane_a(sl), &tm_a, xs, j0 - 1, kk, bar);
-    if (two) tma_load_plane(plane_b(sl), &tm_b, xs, j0 - 1, kk, bar);
+    tma_load_plane(plane_a(sl), &tm_a, xs, j0 - 1, k0 - 1 + r, bar);
+    if (two) tma_load_plane(plane_b(sl), &tm_b, xs, j0 - 1, k0 - 1 + r, bar);
   };
   if (tid == 0) {
     for (int q = 0; q < FNST; ++q)
@@ -547,14 +559,15 @@ __global__ void __launch_bounds__(FX * FY, 3) k_mv32f(GridDims g, const __grid_c
   }
   __syncthreads();
   if (tid == 0)
-    for (int kk = k0 - 1; kk <= min(k0 - 2 + FNST, k1); ++kk) issue(kk);
+    for (int r = 0; r < FNST && r <= rmax; ++r) issue(r);
   bool ok = true;
-  auto wait_plane = [&](int kk) {
-    if (!mbar_wait(smem_u32(&full[stage_of(kk)]), parity_of(kk))) ok = false;
+  auto wait_rel = [&](int r) {
+    if (!mbar_wait(smem_u32(&full[r % FNST]), (uint32_t)((r / FNST) & 1))) ok = false;
   };
-  // the 4 nodes of this thread's element in node plane kk: (x, y) = (0,0), (1,0), (0,1), (1,1)
-  auto gather4 = [&](int kk, float (&v)[4][3]) {
-    const int sl = stage_of(kk);
+  // the 4 nodes of this thread's element column in node plane rel r: (x, y) = (0,0), (1,0), (0,1), (1,1);
+  // MODE 1 forms p_t = z + beta p_{t-1}
+  auto gather4 = [&](int r, float (&v)[4][3]) {
+    const int sl = r % FNST;
     const float* a = plane_a(sl);
     const float* b = plane_b(sl);
 #pragma unroll
@@ -569,85 +582,101 @@ __global__ void __launch_bounds__(FX * FY, 3) k_mv32f(GridDims g, const __grid_c
   const bool exy = ex >= 0 && ex < g.nx && ey >= 0 && ey < g.ny;
   const int64_t ebase = (int64_t)ex + (int64_t)g.nx * ey, eplane = (int64_t)g.nx * g.ny;
   auto eload = [&](int kk) -> float { return (exy && kk >= 0 && kk < g.nz) ? __ldg(E + ebase + eplane * kk) : 0.f; };
-  const int nxo = i0 + l, nyo = j0 + w;  // owned node (local node (1, 1) of this thread's element)
+  const int nxo = i0 + l, nyo = j0 + w;  // owned node (local node (1, 1) of this thread's elements)
   const bool mine = l < FOX && w < FOY && nxo < g.nx1 && nyo < g.ny1;
-  const int64_t nbase = nxo + (int64_t)g.nx1 * nyo;                 // node index at plane 0
-  const int64_t fbase = (int64_t)g.rp * nyo + 3 * nxo;              // padded FP32 offset at plane 0
+  const int64_t nbase = nxo + (int64_t)g.nx1 * nyo;     // node index at plane 0
+  const int64_t fbase = (int64_t)g.rp * nyo + 3 * nxo;  // padded FP32 offset at plane 0
   const int64_t fplane = (int64_t)g.rp * g.ny1;
   const int64_t nplane = (int64_t)g.nx1 * g.ny1;
+  auto fload = [&](int kk) -> uint8_t {
+    return (mine && projected && kk >= k0 && kk < k1) ? nf[nbase + nplane * kk] : (uint8_t)0;
+  };
 
-  wait_plane(k0 - 1);
-  wait_plane(k0);
+  wait_rel(0);
   float ub[4][3];
-  gather4(k0 - 1, ub);
-  __syncthreads();  // the stage of plane k0 - 1 is refilled in the first step
+  gather4(0, ub);
+  __syncthreads();  // stage of rel 0 is refilled in the first step
   float carry[3] = {0.f, 0.f, 0.f};
   double pap = 0.0;
-  float e0 = eload(k0 - 1), e1 = eload(k0);
-  uint8_t f_next = (mine && projected && k0 < k1) ? nf[nbase + nplane * k0] : (uint8_t)0;
-  for (int kk = k0 - 1; kk < k1; ++kk) {
-    wait_plane(kk + 1);
-    float ut[4][3];
-    gather4(kk + 1, ut);
-    // stage of plane kk: read before the previous step's barrier (or the prologue's); refill it
-    if (tid == 0 && kk + FNST <= k1) {
+  float2 e_next = make_float2(eload(k0 - 1), eload(k0));
+  uint8_t f_next0 = fload(k0 - 1), f_next1 = fload(k0);
+  for (int m = 0; m < nsteps; ++m) {
+    const int kk = k0 - 1 + 2 * m;  // element planes kk (lane .x) and kk + 1 (lane .y)
+    wait_rel(2 * m + 1);
+    wait_rel(2 * m + 2);
+    float um[4][3], ut[4][3];
+    gather4(2 * m + 1, um);
+    gather4(2 * m + 2, ut);
+    // stages of rel 2m - 1 and 2m were last read in the previous step (or the prologue); refill them
+    if (tid == 0) {
       asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-      issue(kk + FNST);
-    }
-    const float e_cur = e0;
-    e0 = e1;
-    e1 = eload(kk + 2);
-    const bool outp = mine && kk >= k0;
-    const uint8_t f = f_next;
-    if (outp && projected && kk + 1 < k1) f_next = nf[nbase + nplane * (kk + 1)];
-    if (MODE == 1 && mine && kk + 1 >= k0 && kk + 1 < k1) {
 #pragma unroll
-      for (int c = 0; c < 3; ++c) pnew[fbase + fplane * (kk + 1) + c] = ut[3][c];
+      for (int r = 2 * m + 3; r <= 2 * m + 4; ++r)
+        if (r >= FNST && r <= rmax) issue(r);
     }
-    float u[3][8], yv[3][8];
+    const float2 e2 = e_next;
+    e_next = make_float2(eload(kk + 2), eload(kk + 3));
+    const uint8_t f0 = f_next0, f1 = f_next1;
+    f_next0 = fload(kk + 2);
+    f_next1 = fload(kk + 3);
+    if (MODE == 1 && mine) {
+      if (kk + 1 >= k0 && kk + 1 < k1) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) pnew[fbase + fplane * (kk + 1) + c] = um[3][c];
+      }
+      if (kk + 2 < k1) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) pnew[fbase + fplane * (kk + 2) + c] = ut[3][c];
+      }
+    }
+    float2 u[3][8];
 #pragma unroll
     for (int c = 0; c < 3; ++c)
 #pragma unroll
       for (int b = 0; b < 4; ++b) {
-        u[c][b] = ub[b][c];
-        u[c][b + 4] = ut[b][c];
+        u[c][b] = make_float2(ub[b][c], um[b][c]);      // local z = 0: planes kk, kk + 1
+        u[c][b + 4] = make_float2(um[b][c], ut[b][c]);  // local z = 1: planes kk + 1, kk + 2
       }
-    hex_apply(op, e_cur, u, yv);
-    // x: node column ex + 1 = own local x = 1 nodes + the x-neighbour element's local x = 0 nodes
-    float comb[2][2][3];  // [y][z][c]
+    // comb[by][pl][c]: node column ex + 1, node row ey + by, node plane kk + pl, after the x-neighbour's part
+    float comb[2][3][3];
+    hex_apply2(op, e2, u, [&](int c, float2 (&yc)[8]) {
 #pragma unroll
-    for (int by = 0; by < 2; ++by)
+      for (int by = 0; by < 2; ++by) {
+        const int a = 2 * by;
+        const float s1[3] = {yc[a + 1].x, yc[a + 5].x + yc[a + 1].y, yc[a + 5].y};  // local x = 1
+        const float s0[3] = {yc[a].x, yc[a + 4].x + yc[a].y, yc[a + 4].y};          // local x = 0
 #pragma unroll
-      for (int bz = 0; bz < 2; ++bz)
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          const float nb = __shfl_down_sync(0xffffffffu, yv[c][2 * by + 4 * bz], 1);
-          comb[by][bz][c] = yv[c][1 + 2 * by + 4 * bz] + nb;
-        }
+        for (int pl = 0; pl < 3; ++pl) comb[by][pl][c] = s1[pl] + __shfl_down_sync(0xffffffffu, s0[pl], 1);
+      }
+    });
     // y: the row above adds its local y = 0 sums to this row's local y = 1 sums
-    float* ybw = yb + ((kk & 1) * FY + w) * 6 * FX + l;
+    float* ybw = yb + ((m & 1) * FY + w) * 9 * FX + l;
 #pragma unroll
-    for (int bz = 0; bz < 2; ++bz)
+    for (int pl = 0; pl < 3; ++pl)
 #pragma unroll
-      for (int c = 0; c < 3; ++c) ybw[(3 * bz + c) * FX] = comb[0][bz][c];
+      for (int c = 0; c < 3; ++c) ybw[(3 * pl + c) * FX] = comb[0][pl][c];
     __syncthreads();
     if (mine) {
-      const float* ybr = yb + ((kk & 1) * FY + w + 1) * 6 * FX + l;
-      float top[3];
+      const float* ybr = yb + ((m & 1) * FY + w + 1) * 9 * FX + l;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        const float bot = comb[1][0][c] + ybr[c * FX];
-        top[c] = comb[1][1][c] + ybr[(3 + c) * FX];
-        if (outp) {
+        const float s0 = comb[1][0][c] + ybr[c * FX];
+        const float s1 = comb[1][1][c] + ybr[(3 + c) * FX];
+        const float s2 = comb[1][2][c] + ybr[(6 + c) * FX];
+        if (kk >= k0) {  // node plane kk: the element plane below (carried) + plane kk's bottom faces
           const float pv = ub[3][c];
-          const float out = carry[c] + bot;
-          const float yo = (f >> c & 1) ? pv : out;
+          const float yo = (f0 >> c & 1) ? pv : carry[c] + s0;
           y[fbase + fplane * kk + c] = yo;
           if (MODE == 1) pap += (double)pv * (double)yo;
         }
+        if (kk + 1 < k1) {  // node plane kk + 1: complete within this step
+          const float pv = um[3][c];
+          const float yo = (f1 >> c & 1) ? pv : s1;
+          y[fbase + fplane * (kk + 1) + c] = yo;
+          if (MODE == 1) pap += (double)pv * (double)yo;
+        }
+        carry[c] = s2;
       }
-#pragma unroll
-      for (int c = 0; c < 3; ++c) carry[c] = top[c];
     }
 #pragma unroll
     for (int b = 0; b < 4; ++b)
@@ -659,7 +688,7 @@ __global__ void __launch_bounds__(FX * FY, 3) k_mv32f(GridDims g, const __grid_c
 }
 
 // z-segment length of the factorised kernel: the CTAs of a launch run in ceil(CTAs / resident) waves of
-// (segment length + 1) plane steps each (the extra element plane below each segment); pick the segment
+// (segment length + 2) / 2 steps of two element planes (one extra element plane below each segment); pick the segment
 // count with the least waves x steps, at least 4 planes per segment.
 static int fac_zseg(const GridDims& g, int resident) {
   const int64_t txy = (int64_t)((g.nx1 + FOX - 1) / FOX) * ((g.ny1 + FOY - 1) / FOY);
@@ -669,7 +698,7 @@ static int fac_zseg(const GridDims& g, int resident) {
   for (int segs = 1; segs <= max_segs; ++segs) {
     const int zs = (g.nz1 + segs - 1) / segs;
     const int64_t n = txy * ((g.nz1 + zs - 1) / zs);
-    const int64_t cost = ((n + resident - 1) / resident) * (zs + 1);
+    const int64_t cost = ((n + resident - 1) / resident) * ((zs + 2) / 2);  // two element planes per step
     if (cost < best_cost) {
       best_cost = cost;
       best_z = zs;
@@ -1265,8 +1294,18 @@ void launch_E_to_f32(mycel_problem* p) {
   (void)p;  // k_update_E writes the FP32 copy of E alongside the FP64 one
 }
 
-// FP32 work vectors of the mixed form (padded layout, pads zero) and their TMA descriptors
+// FP32 work vectors of the mixed form (padded layout, pads zero) and their TMA descriptors; also grants the
+// factorised matvec its shared memory above the 48 KB default (once per process, before any launch or capture)
 static int32_t ensure_mixed(mycel_problem* p) {
+  static std::once_flag smem_once;
+  static cudaError_t smem_err = cudaSuccess;
+  std::call_once(smem_once, [] {
+    cudaError_t a = cudaFuncSetAttribute(k_mv32f<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fac_smem_bytes(0));
+    cudaError_t b = cudaFuncSetAttribute(k_mv32f<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fac_smem_bytes(1));
+    smem_err = a != cudaSuccess ? a : b;
+  });
+  if (smem_err != cudaSuccess)
+    return set_error(p->ctx, MYCEL_E_DEVICE, std::string("matvec shared memory: ") + cudaGetErrorString(smem_err));
   if (p->f_x) return MYCEL_OK;
   const size_t fb = sizeof(float) * (size_t)p->g.n32 + 64;
   cudaError_t e = cudaSuccess;
