@@ -52,6 +52,21 @@ def parse():
     ap.add_argument("--probe-iters", type=int, default=40)
     ap.add_argument("--probe-variant", type=int, default=0,
                     help="FP32 matvec variant for --probe mixed (0 autotune, 1 dense, 2 tensor, 3 factored)")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving sample of the default run")
+    ap.add_argument("--serve-sample-jobs", type=int, default=12)
+    ap.add_argument("--serve-sample-max-elems", type=int, default=250_000)
+    ap.add_argument("--serve", action="store_true",
+                    help="served job stream only (Poisson arrivals, log-uniform sizes, HBM-budget admission)")
+    ap.add_argument("--serve-jobs", type=int, default=500)
+    ap.add_argument("--serve-rate", type=float, default=20.0)
+    ap.add_argument("--serve-max-elems", type=int, default=1_000_000)
+    ap.add_argument("--serve-slots", type=int, default=6)
+    ap.add_argument("--serve-budget-gb", type=float, default=150.0)
+    ap.add_argument("--serve-precisions", default="mixed,fp64")
+    ap.add_argument("--serve-fp64-jobs", type=int, default=None, help="prefix of the stream run in FP64 (default all)")
+    ap.add_argument("--batched", action="store_true", help="48 independent problems submitted at once")
+    ap.add_argument("--batched-count", type=int, default=48)
+    ap.add_argument("--batched-iters", type=int, default=4)
     return ap.parse_args()
 
 
@@ -157,6 +172,102 @@ def matvec_bytes_fp32(model):
     return 48 * nn + 5 * ne + nn
 
 
+def serve_stream(jobs, precision, slots, budget_bytes, rate_scale=1.0):
+    """Submit the jobs at their arrival times to a server and wait for all; returns the stats, per-job
+    compliance histories and the wall time. Arrival times are the stream's (seconds from the first)."""
+    from mycel_b200 import api
+    from mycel_b200 import workloads as W
+    specs = [W.served_job(nx, ny, nz, it, seed, precision=precision) for (_t, nx, ny, nz, it, seed) in jobs]
+    hist = []
+    with api.Server(slots=slots, hbm_budget_bytes=int(budget_bytes)) as srv:
+        t0 = time.perf_counter()
+        ids = []
+        for (arr, *_rest), (m, o) in zip(jobs, specs):
+            dt = arr * rate_scale - (time.perf_counter() - t0)
+            if dt > 0:
+                time.sleep(dt)
+            ids.append(srv.submit(m, o))
+        srv.wait()
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+        for jid in ids:
+            r = srv.result(jid) if srv.info(jid)["state"] == "done" else None
+            hist.append([h.compliance for h in r["history"]] if r else None)
+    elems = sum(nx * ny * nz for (_t, nx, ny, nz, _i, _s) in jobs)
+    span = st["last_finish_s"] - st["first_submit_s"]
+    return {"jobs": len(jobs), "completed": st["completed"], "failed": st["failed"],
+            "simp_iterations": st["simp_iterations"], "simp_iter_s": st["simp_iterations"] / span if span > 0 else None,
+            "p50_latency_s": st["p50_latency_s"], "p99_latency_s": st["p99_latency_s"],
+            "mean_latency_s": st["mean_latency_s"], "p50_queue_s": st["p50_queue_s"], "p99_queue_s": st["p99_queue_s"],
+            "peak_admitted_gb": st["peak_admitted_bytes"] / 1e9, "elements_total": elems, "wall_s": wall}, hist
+
+
+def compare_histories(h_mixed, h_fp64):
+    """Relative compliance differences, mixed vs FP64, of the same jobs iteration by iteration. Iteration 1
+    starts both from the same state (the solver's precision alone); later iterations also carry the
+    divergence of the two SIMP trajectories."""
+    errs, first = [], []
+    for a, b in zip(h_mixed, h_fp64):
+        if not a or not b:
+            continue
+        first.append(abs(a[0] - b[0]) / abs(b[0]))
+        for x, y in zip(a, b):
+            errs.append(abs(x - y) / abs(y))
+    if not errs:
+        return None
+    return {"max": max(errs), "median": float(np.median(errs)), "iteration1_max": max(first)}
+
+
+def serving_report(args, n_jobs, max_elems, rate, slots, budget_gb, precisions, fp64_jobs=None):
+    from mycel_b200 import workloads as W
+    jobs = W.job_stream(n_jobs=n_jobs, rate=rate, seed=11, max_elems=max_elems)
+    out = {"stream": {"jobs": n_jobs, "rate_jobs_s": rate, "elements": [8000, max_elems], "iterations": [20, 60],
+                      "slots": slots, "hbm_budget_gb": budget_gb, "seed": 11}}
+    hists = {}
+    for prec in precisions:
+        sel = jobs if (prec != "fp64" or fp64_jobs is None) else jobs[:fp64_jobs]
+        out[prec], hists[prec] = serve_stream(sel, prec, slots, budget_gb * 1e9)
+    if "mixed" in hists and "fp64" in hists:
+        out["rel_compliance_err_mixed_vs_fp64"] = compare_histories(hists["mixed"], hists["fp64"])
+        n = min(len(hists["mixed"]), len(hists["fp64"]))
+        if out["fp64"]["simp_iter_s"]:
+            out["speedup_mixed_vs_fp64"] = out["mixed"]["simp_iter_s"] / out["fp64"]["simp_iter_s"] \
+                if n == len(hists["mixed"]) else None
+    return out
+
+
+def run_serve(args):
+    precisions = [p for p in args.serve_precisions.split(",") if p]
+    out = {"metric": "served SIMP job stream: p50/p99 job latency and aggregate SIMP iter/s",
+           **serving_report(args, args.serve_jobs, args.serve_max_elems, args.serve_rate, args.serve_slots,
+                            args.serve_budget_gb, precisions, args.serve_fp64_jobs)}
+    print(json.dumps(out), flush=True)
+
+
+def run_batched(args):
+    """Batched instances: all problems submitted at once; aggregate SIMP iter/s, mixed vs FP64."""
+    from mycel_b200 import api
+    from mycel_b200 import workloads as W
+    probs = W.batched_instances(count=args.batched_count)
+    out = {"metric": "batched instances: aggregate SIMP iter/s", "problems": len(probs),
+           "iterations_each": args.batched_iters,
+           "elements_total": int(sum(bp.model.total_elements for bp in probs))}
+    hists = {}
+    for prec in ("mixed", "fp64"):
+        with api.Server(slots=args.serve_slots, hbm_budget_bytes=int(args.serve_budget_gb * 1e9)) as srv:
+            ids = [srv.submit(bp.model, bp.options.replace(max_iterations=args.batched_iters, precision=prec))
+                   for bp in probs]
+            srv.wait()
+            st = srv.stats()
+            hists[prec] = [[h.compliance for h in srv.result(j)["history"]] for j in ids]
+        span = st["last_finish_s"] - st["first_submit_s"]
+        out[prec] = {"simp_iter_s": st["simp_iterations"] / span, "wall_s": span, "completed": st["completed"],
+                     "p50_latency_s": st["p50_latency_s"], "p99_latency_s": st["p99_latency_s"]}
+    out["speedup_mixed_vs_fp64"] = out["mixed"]["simp_iter_s"] / out["fp64"]["simp_iter_s"]
+    out["rel_compliance_err_mixed_vs_fp64"] = compare_histories(hists["mixed"], hists["fp64"])
+    print(json.dumps(out), flush=True)
+
+
 def run_mycel(args):
     import torch
     from mycel_b200 import api
@@ -192,6 +303,7 @@ def run_mycel(args):
     value = ws * args.steps / (t_max / 1000.0)
     pcg_inner = [r.solver_iterations for r in recs]
     comp_mixed = [r.compliance for r in recs]
+    mv_variant = prob.matvec32()
     sess.close()
     prob.close()
 
@@ -201,12 +313,14 @@ def run_mycel(args):
     mv_bytes = matvec_bytes_fp32(model)
     achieved = mv_bytes / (per_launch_ms / 1000.0) / 1e9 if timing["launches"] else None
     hbm = (pk or {}).get("hbm_gbs") or 6650.0
-    roof = {"kernel": "k_mv32 (FP32 Hex8 K.p, fused p update + p.Ap partials)", "bound": "hbm",
+    kname = {1: "k_mv32 (dense KE rows, FMA pipe)", 2: "k_mv32tc (dense KE, tcgen05 3xTF32)",
+             3: "k_mv32f (factorised Hex8 operator, TMA-fed)"}.get(mv_variant, "FP32 matvec")
+    roof = {"kernel": kname + ": FP32 Hex8 K.p with fused p update + p.Ap partials", "bound": "hbm",
             "achieved": achieved, "peak": hbm, "unit": "GB/s",
             "frac": (achieved / hbm) if achieved else None, "traffic": None,
             "peak_source": "measured" if pk else "fallback", "avg_launch_us": per_launch_ms * 1000.0,
             "timed_launches": timing["launches"], "algorithmic_bytes_per_launch": mv_bytes,
-            "flops_per_launch": 1152 * model.active_element_count,
+            "flops_per_launch": 1152 * model.active_element_count, "flops_note": "dense-KE equivalent",
             "tflops": 1152 * model.active_element_count / (per_launch_ms / 1000.0) / 1e12 if timing["launches"] else None}
 
     out = {"metric": "SIMP iter/s (mixed FP32-inner/FP64-refined, 192x96x96 bridge)", "value": value,
@@ -287,6 +401,13 @@ def run_mycel(args):
         pcg_per_it = (statistics.mean(out["fp64"]["pcg_iters_per_step"]) if "fp64" in out else
                       FP64_PCG_PER_SIMP_ITER or statistics.mean(pcg_inner))
         out["cpu_baseline"] = cpu_sample(model, opts, pcg_per_it, args.cpu_sample_iters)
+
+    # ---------------- serving sample (rank 0): Poisson job stream through the serving loop ----------------
+    if rank == 0 and not args.no_serve:
+        out["serving"] = serving_report(args, args.serve_sample_jobs, args.serve_sample_max_elems, 20.0,
+                                        args.serve_slots, 150.0, ["mixed", "fp64"])
+        out["serving"]["note"] = ("bounded sample of the served stream: first jobs of the Poisson(20/s) stream, "
+                                  "sizes log-uniform up to serve_sample_max_elems; full stream: bench.py --serve")
 
     if rank == 0:
         print(json.dumps(out), flush=True)
@@ -377,6 +498,10 @@ if __name__ == "__main__":
     a = parse()
     if a.probe:
         run_probe(a)
+    elif a.serve and a.impl != "reference":
+        run_serve(a)
+    elif a.batched and a.impl != "reference":
+        run_batched(a)
     elif a.impl == "reference":
         run_reference(a)
     else:

@@ -232,6 +232,81 @@ int32_t mycel_simp_read(mycel_simp_session* s, double* u_out, float* physical_de
                         double* rho_phys_active_out, double* rho_design_active_out, double* lambda_out);
 int32_t mycel_simp_end(mycel_simp_session* s);
 
+/* ---- serving: continuous batching of SIMP jobs on one GPU ----
+   No counterpart in the reference, whose App runs one optimisation at a time (OptimizationCoordinator.cs:229
+   through the FemWorkTeam lock, FemWorkTeam.cs:109). A server runs `slots` jobs at once, each on its own CUDA
+   stream and host thread, so their PCG iterations interleave on the device; a queued job is admitted, in
+   arrival order with backfill of later jobs that fit, when a slot is free and the device memory of the
+   running jobs plus its own (mycel_job_device_bytes) stays within hbm_budget_bytes. A job's state (rho, u,
+   PCG vectors, lambda) stays resident on the device from its first to its last iteration. Each job's results
+   do not depend on what else runs: every reduction has a fixed order. */
+typedef struct mycel_server mycel_server;
+
+typedef struct {
+  int32_t device;
+  int32_t slots;             /* jobs running at once (>= 1) */
+  int64_t hbm_budget_bytes;  /* admission limit on the summed device memory of running jobs */
+} mycel_server_options;
+
+/* One optimisation job: the arguments of mycel_problem_create and mycel_simp_run. Every array (including
+   those inside loads and options) is copied by mycel_server_submit. */
+typedef struct {
+  mycel_grid grid;
+  const uint8_t* domain;
+  mycel_material material;
+  const int32_t* fixed_dofs;
+  int32_t n_fixed;
+  const mycel_load_case* loads;
+  int32_t n_loads;
+  const double* element_density; /* box-sized or NULL */
+  double penal;
+  mycel_simp_options options;
+  int32_t keep_u;                /* keep the final u for mycel_server_job_result */
+} mycel_job_spec;
+
+#define MYCEL_JOB_QUEUED 0
+#define MYCEL_JOB_RUNNING 1
+#define MYCEL_JOB_DONE 2
+#define MYCEL_JOB_FAILED 3
+
+typedef struct {
+  int32_t state;            /* MYCEL_JOB_* */
+  int32_t status;           /* MYCEL_* of a failed job, else MYCEL_OK */
+  int32_t iterations, converged;
+  int64_t device_bytes;     /* admission estimate */
+  double submit_s, start_s, finish_s; /* seconds since the server was created */
+  double final_compliance;
+  int64_t solver_iterations; /* PCG iterations summed over the job's SIMP iterations */
+  char message[256];
+} mycel_job_info;
+
+typedef struct {
+  int64_t submitted, completed, failed, running, queued;
+  int64_t simp_iterations;   /* summed over completed jobs */
+  double first_submit_s, last_finish_s;
+  double p50_latency_s, p99_latency_s, mean_latency_s, max_latency_s; /* submit -> finish, completed jobs */
+  double p50_queue_s, p99_queue_s;                                    /* submit -> start */
+  int64_t admitted_bytes, peak_admitted_bytes;
+} mycel_server_stats;
+
+int32_t mycel_server_create(const mycel_server_options* opt, mycel_server** out);
+int32_t mycel_server_submit(mycel_server* s, const mycel_job_spec* job, int64_t* job_id);
+int32_t mycel_server_job_info(mycel_server* s, int64_t job_id, mycel_job_info* out);
+/* Waits for one job (job_id >= 0) or for every submitted job (job_id < 0); MYCEL_E_TIMEOUT after timeout_s
+   (timeout_s < 0: no limit). */
+int32_t mycel_server_wait(mycel_server* s, int64_t job_id, double timeout_s);
+/* Results of a finished job; any output may be NULL. history: up to cap records; densities box-sized float;
+   u total_dofs (when the job kept it). */
+int32_t mycel_server_job_result(mycel_server* s, int64_t job_id, mycel_iter_record* history, int32_t cap,
+                                float* physical_density_out, float* design_density_out, double* u_out);
+int32_t mycel_server_stats_get(mycel_server* s, mycel_server_stats* out);
+/* Lets running jobs finish, fails queued ones, joins the workers and frees everything. */
+int32_t mycel_server_destroy(mycel_server* s);
+const char* mycel_server_last_error(mycel_server* s);
+/* Device memory a job holds while it runs (problem, PCG and mixed workspaces, SIMP session, filter): the
+   admission estimate, an upper bound of mycel_problem_info.device_bytes for the same job. */
+int64_t mycel_job_device_bytes(const mycel_job_spec* job);
+
 #ifdef __cplusplus
 }
 #endif

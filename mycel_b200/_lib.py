@@ -64,6 +64,29 @@ class IterRecord(C.Structure):
 
 PROGRESS_FN = C.CFUNCTYPE(None, P, C.POINTER(IterRecord), C.POINTER(C.c_float), C.POINTER(C.c_float))
 
+
+class ServerOptions(C.Structure):
+    _fields_ = [("device", i32), ("slots", i32), ("hbm_budget_bytes", i64)]
+
+
+class JobSpec(C.Structure):
+    _fields_ = [("grid", Grid), ("domain", P), ("material", Material), ("fixed_dofs", P), ("n_fixed", i32),
+                ("loads", P), ("n_loads", i32), ("element_density", P), ("penal", dbl), ("options", SimpOptions),
+                ("keep_u", i32)]
+
+
+class JobInfo(C.Structure):
+    _fields_ = [("state", i32), ("status", i32), ("iterations", i32), ("converged", i32), ("device_bytes", i64),
+                ("submit_s", dbl), ("start_s", dbl), ("finish_s", dbl), ("final_compliance", dbl),
+                ("solver_iterations", i64), ("message", C.c_char * 256)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", i64), ("completed", i64), ("failed", i64), ("running", i64), ("queued", i64),
+                ("simp_iterations", i64), ("first_submit_s", dbl), ("last_finish_s", dbl), ("p50_latency_s", dbl),
+                ("p99_latency_s", dbl), ("mean_latency_s", dbl), ("max_latency_s", dbl), ("p50_queue_s", dbl),
+                ("p99_queue_s", dbl), ("admitted_bytes", i64), ("peak_admitted_bytes", i64)]
+
 # name -> (restype, argtypes); exactly the entry points of include/mycel.h
 SIGNATURES = {
     "mycel_version": (i32, []),
@@ -101,6 +124,15 @@ SIGNATURES = {
     "mycel_simp_step": (i32, [P, C.POINTER(IterRecord), C.POINTER(i32)]),
     "mycel_simp_read": (i32, [P, P, P, P, P, P, C.POINTER(dbl)]),
     "mycel_simp_end": (i32, [P]),
+    "mycel_server_create": (i32, [C.POINTER(ServerOptions), C.POINTER(P)]),
+    "mycel_server_submit": (i32, [P, C.POINTER(JobSpec), C.POINTER(i64)]),
+    "mycel_server_job_info": (i32, [P, i64, C.POINTER(JobInfo)]),
+    "mycel_server_wait": (i32, [P, i64, dbl]),
+    "mycel_server_job_result": (i32, [P, i64, C.POINTER(IterRecord), i32, P, P, P]),
+    "mycel_server_stats_get": (i32, [P, C.POINTER(ServerStats)]),
+    "mycel_server_destroy": (i32, [P]),
+    "mycel_server_last_error": (C.c_char_p, [P]),
+    "mycel_job_device_bytes": (i64, [C.POINTER(JobSpec)]),
 }
 
 _lib = None

@@ -434,3 +434,112 @@ class SimpSession:
             self.close()
         except Exception:
             pass
+
+
+def _server_check(status: int, handle):
+    if status == 0:
+        return
+    msg = L.load().mycel_server_last_error(handle)
+    text = msg.decode("utf-8", "replace") if msg else f"status {status}"
+    raise _ERRORS.get(status, MycelError)(text)
+
+
+_JOB_STATES = {0: "queued", 1: "running", 2: "done", 3: "failed"}
+
+
+class Server:
+    """Continuous batching of SIMP jobs on one GPU (mycel_server): ``slots`` jobs run at once on their own
+    streams, admitted in arrival order (with backfill) against ``hbm_budget_bytes`` of device memory."""
+
+    def __init__(self, slots: int = 4, hbm_budget_bytes: int = 150 * 10**9, device: int = 0):
+        so = L.ServerOptions(device, slots, int(hbm_budget_bytes))
+        h = C.c_void_p()
+        st = L.load().mycel_server_create(C.byref(so), C.byref(h))
+        if st:
+            _check(st, None)
+        self.handle = h.value
+        self._models = {}
+
+    @staticmethod
+    def _spec(model: FeModel, options: OptimizerOptions, keep_u: bool, keep: list) -> L.JobSpec:
+        g = model.grid
+        loads = (L.LoadCaseC * max(1, len(model.loads)))()
+        for i, lc in enumerate(model.loads):
+            nodes = np.ascontiguousarray(lc.patch.nodes, dtype=np.int32)
+            areas = np.ascontiguousarray(lc.patch.node_area, dtype=np.float64)
+            keep += [nodes, areas]
+            loads[i].n_nodes = nodes.size
+            loads[i].nodes = nodes.ctypes.data
+            loads[i].node_area = areas.ctypes.data
+            loads[i].force[:] = [np.float32(v) for v in lc.total_force]
+        fixed = np.ascontiguousarray(model.fixed_dofs, dtype=np.int32)
+        dom = np.ascontiguousarray(model.domain, dtype=np.uint8)
+        dens = L.f64(model.element_density)
+        keep += [loads, fixed, dom, dens]
+        return L.JobSpec(L.Grid(g.nx, g.ny, g.nz, float(np.float32(g.h))), dom.ctypes.data,
+                         L.Material(model.material.e0, model.material.nu, model.material.emin_ratio),
+                         fixed.ctypes.data if fixed.size else None, fixed.size, C.cast(loads, C.c_void_p),
+                         len(model.loads), dens.ctypes.data, model.penal, _simp_options(options, keep),
+                         int(bool(keep_u)))
+
+    @staticmethod
+    def device_bytes(model: FeModel, options: OptimizerOptions) -> int:
+        """Admission estimate of one job (mycel_job_device_bytes)."""
+        keep = []
+        spec = Server._spec(model, options, False, keep)
+        return int(L.load().mycel_job_device_bytes(C.byref(spec)))
+
+    def submit(self, model: FeModel, options: OptimizerOptions, keep_u: bool = False) -> int:
+        keep = []
+        spec = self._spec(model, options, keep_u, keep)
+        jid = C.c_int64(-1)
+        _server_check(L.load().mycel_server_submit(self.handle, C.byref(spec), C.byref(jid)), self.handle)
+        self._models[jid.value] = model
+        return jid.value
+
+    def info(self, job: int) -> dict:
+        ji = L.JobInfo()
+        _server_check(L.load().mycel_server_job_info(self.handle, job, C.byref(ji)), self.handle)
+        d = {k: getattr(ji, k) for k, _ in L.JobInfo._fields_}
+        d["message"] = ji.message.decode("utf-8", "replace")
+        d["state"] = _JOB_STATES.get(ji.state, str(ji.state))
+        return d
+
+    def wait(self, job: int = -1, timeout: Optional[float] = None) -> None:
+        _server_check(L.load().mycel_server_wait(self.handle, job, -1.0 if timeout is None else float(timeout)),
+                      self.handle)
+
+    def result(self, job: int, u: bool = False) -> dict:
+        m = self._models[job]
+        info = self.info(job)
+        cap = max(1, int(info["iterations"]))
+        hist = (L.IterRecord * cap)()
+        ph = np.zeros(m.total_elements, dtype=np.float32)
+        de = np.zeros(m.total_elements, dtype=np.float32)
+        uu = np.zeros(m.total_dofs) if u else None
+        _server_check(L.load().mycel_server_job_result(self.handle, job, hist, cap, ph.ctypes.data, de.ctypes.data,
+                                                       L.ptr(uu)), self.handle)
+        return dict(info=info, history=[_snapshot(r) for r in hist[:info["iterations"]]], physical=ph, design=de,
+                    u=uu)
+
+    def stats(self) -> dict:
+        s = L.ServerStats()
+        _server_check(L.load().mycel_server_stats_get(self.handle, C.byref(s)), self.handle)
+        return {k: getattr(s, k) for k, _ in L.ServerStats._fields_}
+
+    def close(self):
+        if getattr(self, "handle", None):
+            L.load().mycel_server_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

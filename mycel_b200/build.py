@@ -24,6 +24,7 @@ UNITS = [
     ("api.cu", ["-fmad=true"]),
     ("simp.cu", ["-fmad=true"]),
     ("hex8.cpp", []),
+    ("server.cpp", []),
 ]
 
 

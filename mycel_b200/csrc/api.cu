@@ -36,13 +36,15 @@ template <class T>
 cudaError_t dalloc(mycel_problem* p, T** ptr, size_t count) {
   size_t bytes = std::max<size_t>(sizeof(T) * count, 16);
   bytes = (bytes + 15) & ~size_t(15);
-  cudaError_t e = cudaMalloc((void**)ptr, bytes);
+  // stream-ordered: no device-wide synchronisation, so set-up and tear-down of one problem do not stall the
+  // work of others running on other streams (the serving loop)
+  cudaError_t e = cudaMallocAsync((void**)ptr, bytes, p->ctx->stream);
   if (e == cudaSuccess) p->device_bytes += (int64_t)bytes;
   return e;
 }
 
-void dfree(void* ptr) {
-  if (ptr) cudaFree(ptr);
+void dfree(cudaStream_t s, void* ptr) {
+  if (ptr) cudaFreeAsync(ptr, s);
 }
 
 std::string fmt_e3(double v) {
@@ -499,7 +501,7 @@ extern "C" int32_t mycel_problem_create(mycel_ctx* c, const mycel_grid* grid, co
   if (ok) ok = !dalloc(p, &p->d_part2, std::max<int64_t>(g.nd / 256 + 1024, 65536));
   p->n_part2 = std::max<int64_t>(g.nd / 256 + 1024, 65536);
   if (!ok) {
-    dfree(d_cnt);
+    dfree(c->stream, d_cnt);
     mycel_problem_destroy(p);
     return set_error(c, MYCEL_E_OOM, "out of device memory for the problem");
   }
@@ -529,7 +531,7 @@ extern "C" int32_t mycel_problem_create(mycel_ctx* c, const mycel_grid* grid, co
   }
   int32_t st = build_nz_list(p, p->d_F, p->d_bnz, &nb_cnt);
   if (st) {
-    dfree(d_cnt);
+    dfree(c->stream, d_cnt);
     mycel_problem_destroy(p);
     return st;
   }
@@ -541,7 +543,7 @@ extern "C" int32_t mycel_problem_create(mycel_ctx* c, const mycel_grid* grid, co
   cudaMemcpyAsync(&hcnt, d_cnt, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  dfree(d_cnt);
+  dfree(c->stream, d_cnt);
   if (e != cudaSuccess) {
     mycel_problem_destroy(p);
     return set_error(c, MYCEL_E_DEVICE, std::string("problem set-up: ") + cudaGetErrorString(e));
@@ -586,7 +588,7 @@ extern "C" int32_t mycel_problem_destroy(mycel_problem* p) {
                   p->d_E, p->d_Ef, p->d_diag, p->d_invd, p->d_invdf, p->d_r, p->d_z, p->d_p, p->d_ap, p->d_x,
                   p->d_part, p->d_state, p->f_x, p->f_r, p->f_z, p->f_p0, p->f_p1, p->f_ap, p->d_r64, p->d_part2,
                   p->d_tmp0, p->d_tmp1};
-  for (void* q : ptrs) dfree(q);
+  for (void* q : ptrs) dfree(p->ctx->stream, q);
   delete p;
   return MYCEL_OK;
 }
@@ -781,10 +783,10 @@ extern "C" int32_t mycel_filter_create(mycel_problem* p, double rmin, mycel_filt
 extern "C" int32_t mycel_filter_destroy(mycel_filter* f) {
   if (!f) return MYCEL_OK;
   cudaStreamSynchronize(f->p->ctx->stream);
-  dfree(f->d_off);
-  dfree(f->d_w);
-  dfree(f->d_invhs);
-  dfree(f->d_s);
+  dfree(f->p->ctx->stream, f->d_off);
+  dfree(f->p->ctx->stream, f->d_w);
+  dfree(f->p->ctx->stream, f->d_invhs);
+  dfree(f->p->ctx->stream, f->d_s);
   delete f;
   return MYCEL_OK;
 }

@@ -25,8 +25,10 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
+#include <tuple>
 
 #include "internal.h"
 
@@ -1089,8 +1091,22 @@ static void launch_mv32_variant(mycel_problem* p, cudaStream_t s, const float* x
 
 // Autotuner: on first use, time every variant (K x on the problem's FP32 buffers, after one warm-up launch)
 // and keep the fastest; a tensor-core run that reports a failed wait is never chosen.
+// Variant choices are shared by every problem of the process with the same grid, so a problem's arithmetic
+// does not depend on what else was running when it was first timed (first measurement wins).
+static std::mutex g_mv32_mu;
+static std::map<std::tuple<int, int, int>, int> g_mv32_choice;
+
 static int32_t resolve_mv32(mycel_problem* p) {
   if (p->mv32 > 0) return MYCEL_OK;
+  const auto key = std::make_tuple(p->g.nx, p->g.ny, p->g.nz);
+  {
+    std::lock_guard<std::mutex> lk(g_mv32_mu);
+    auto it = g_mv32_choice.find(key);
+    if (it != g_mv32_choice.end()) {
+      p->mv32 = it->second;
+      return MYCEL_OK;
+    }
+  }
   mycel_ctx* c = p->ctx;
   cudaStream_t s = c->stream;
   MYCEL_CUDA(c, cudaMemsetAsync(p->f_r, 0, sizeof(float) * p->g.n32, s));
@@ -1123,10 +1139,13 @@ static int32_t resolve_mv32(mycel_problem* p) {
     }
     cudaEventElapsedTime(&t[v], e0, e1);
     if (!launched) t[v] = 1e30f;
-    MYCEL_CUDA(c, cudaMemcpy(&herr, p->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    int* herr_p = (int*)((char*)c->pinned + 8192);
+    MYCEL_CUDA(c, cudaMemcpyAsync(herr_p, p->d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    MYCEL_CUDA(c, cudaStreamSynchronize(s));
+    herr = *herr_p;
     if (herr) {  // a bounded wait gave up: never choose this variant
       t[v] = 1e30f;
-      MYCEL_CUDA(c, cudaMemset(p->d_err, 0, sizeof(int)));
+      MYCEL_CUDA(c, cudaMemsetAsync(p->d_err, 0, sizeof(int), s));
     }
   }
   cudaEventDestroy(e0);
@@ -1135,6 +1154,10 @@ static int32_t resolve_mv32(mycel_problem* p) {
   for (int v = 1; v < 3; ++v)
     if (t[v] < t[best]) best = v;
   p->mv32 = variants[best];
+  {
+    std::lock_guard<std::mutex> lk(g_mv32_mu);
+    p->mv32 = g_mv32_choice.emplace(key, p->mv32).first->second;  // another thread may have stored one first
+  }
   if (std::getenv("MYCEL_VERBOSE"))
     std::fprintf(stderr, "mycel: FP32 matvec autotune (ms per 3 launches) factored %.4f dense %.4f tensor %.4f -> %d\n",
                  t[0], t[1], t[2], p->mv32);
@@ -1311,7 +1334,7 @@ static int32_t ensure_mixed(mycel_problem* p) {
   cudaError_t e = cudaSuccess;
   float** bufs[] = {&p->f_x, &p->f_r, &p->f_z, &p->f_p0, &p->f_p1, &p->f_ap};
   for (float** b : bufs) {
-    if ((e = cudaMalloc((void**)b, fb)) != cudaSuccess) break;
+    if ((e = cudaMallocAsync((void**)b, fb, p->ctx->stream)) != cudaSuccess) break;
     p->device_bytes += (int64_t)fb;
     cudaMemsetAsync(*b, 0, fb, p->ctx->stream);
   }

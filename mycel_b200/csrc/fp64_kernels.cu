@@ -901,10 +901,11 @@ int filter_setup(mycel_filter* f) {
       }
   f->n_off = (int)offs.size();
   cudaStream_t s = p->ctx->stream;
-  if (cudaMalloc(&f->d_off, sizeof(int4) * offs.size()) != cudaSuccess) return MYCEL_E_OOM;
-  if (cudaMalloc(&f->d_w, sizeof(double) * ws.size()) != cudaSuccess) return MYCEL_E_OOM;
-  if (cudaMalloc(&f->d_invhs, sizeof(double) * p->g.ne) != cudaSuccess) return MYCEL_E_OOM;
-  if (cudaMalloc(&f->d_s, sizeof(double) * p->g.ne) != cudaSuccess) return MYCEL_E_OOM;
+  if (cudaMallocAsync(&f->d_off, sizeof(int4) * offs.size(), s) != cudaSuccess) return MYCEL_E_OOM;
+  if (cudaMallocAsync(&f->d_w, sizeof(double) * ws.size(), s) != cudaSuccess) return MYCEL_E_OOM;
+  if (cudaMallocAsync(&f->d_invhs, sizeof(double) * p->g.ne, s) != cudaSuccess) return MYCEL_E_OOM;
+  if (cudaMallocAsync(&f->d_s, sizeof(double) * p->g.ne, s) != cudaSuccess) return MYCEL_E_OOM;
+  p->device_bytes += (int64_t)(sizeof(int4) * offs.size() + sizeof(double) * ws.size() + 16 * p->g.ne);
   cudaMemcpyAsync(f->d_off, offs.data(), sizeof(int4) * offs.size(), cudaMemcpyHostToDevice, s);
   cudaMemcpyAsync(f->d_w, ws.data(), sizeof(double) * ws.size(), cudaMemcpyHostToDevice, s);
   cudaMemsetAsync(f->d_invhs, 0, sizeof(double) * p->g.ne, s);

@@ -241,6 +241,7 @@ int launch_oc(mycel_ctx* ctx, int64_t n, const int32_t* d_index /*box index of e
 void launch_E_to_f32(mycel_problem* p);
 void launch_matvec32(mycel_problem* p, const float* x, float* y, int projected);
 int32_t mixed_apply_k_f64io(mycel_problem* p, const double* x, double* y, int projected);
+bool simp_session_converged(const mycel_simp_session* s);  // the SIMP stop rule fired
 int32_t mixed_solve_entry(mycel_problem* p, const double* d_b, const int32_t* d_nz, int32_t n_nz, double* d_u,
                           double tol, int max_iter, const volatile int32_t* cancel, mycel_pcg_result* res);
 

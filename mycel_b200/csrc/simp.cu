@@ -79,7 +79,7 @@ __global__ void k_snapshot(int64_t ne, const uint8_t* __restrict__ dom, const do
 template <class T>
 cudaError_t salloc(mycel_simp_session* s, T** ptr, size_t count) {
   size_t bytes = std::max<size_t>(sizeof(T) * count, 16);
-  cudaError_t e = cudaMalloc((void**)ptr, bytes);
+  cudaError_t e = cudaMallocAsync((void**)ptr, bytes, s->p->ctx->stream);  // stream-ordered, no device sync
   if (e == cudaSuccess) s->p->device_bytes += (int64_t)bytes;
   return e;
 }
@@ -383,17 +383,18 @@ extern "C" int32_t mycel_simp_end(mycel_simp_session* s) {
   cudaSetDevice(s->p->ctx->device);
   cudaStreamSynchronize(s->p->ctx->stream);
   if (s->filt) mycel_filter_destroy(s->filt);
+  cudaStream_t st = s->p->ctx->stream;
   double* dptr[] = {s->d_rho, s->d_rho_new, s->d_rt, s->d_dcb, s->d_dc, s->d_u, s->d_scal, s->d_oc_scr};
   for (double* q : dptr)
-    if (q) cudaFree(q);
+    if (q) cudaFreeAsync(q, st);
   if (s->o.enable_heaviside) {
-    if (s->d_rb) cudaFree(s->d_rb);
-    if (s->d_dct) cudaFree(s->d_dct);
+    if (s->d_rb) cudaFreeAsync(s->d_rb, st);
+    if (s->d_dct) cudaFreeAsync(s->d_dct, st);
   }
-  if (s->d_oc) cudaFree(s->d_oc);
-  if (s->d_pas) cudaFree(s->d_pas);
-  if (s->d_phys_f) cudaFree(s->d_phys_f);
-  if (s->d_des_f) cudaFree(s->d_des_f);
+  if (s->d_oc) cudaFreeAsync(s->d_oc, st);
+  if (s->d_pas) cudaFreeAsync(s->d_pas, st);
+  if (s->d_phys_f) cudaFreeAsync(s->d_phys_f, st);
+  if (s->d_des_f) cudaFreeAsync(s->d_des_f, st);
   for (auto& e : s->ev)
     if (e) cudaEventDestroy(e);
   delete s;
@@ -448,3 +449,7 @@ extern "C" int32_t mycel_simp_run(mycel_problem* p, const mycel_simp_options* op
   if (err) c->last_error = msg;
   return err;
 }
+
+namespace mycel {
+bool simp_session_converged(const mycel_simp_session* s) { return s && s->converged; }
+}  // namespace mycel

@@ -47,6 +47,15 @@ def simp_cantilever_40x20x10():
 
 def _face_connected_from_x0(active: np.ndarray) -> np.ndarray:
     """Keep the elements face-connected (6-neighbour) to the x=0 layer; active is (nz, ny, nx) bool."""
+    try:
+        from scipy import ndimage
+    except ImportError:  # pragma: no cover - scipy is part of the environment; the loop below is the same rule
+        ndimage = None
+    if ndimage is not None:
+        lab, _n = ndimage.label(active)  # default structure: 6-connectivity in 3-D
+        roots = np.unique(lab[:, :, 0])
+        roots = roots[roots > 0]
+        return np.isin(lab, roots) & active
     keep = np.zeros_like(active)
     keep[:, :, 0] = active[:, :, 0]
     frontier = keep.copy()
@@ -196,3 +205,54 @@ def job_stream(n_jobs=500, rate=20.0, seed=11, min_elems=8_000, max_elems=1_000_
         nx = max(8, int(round(ne / (ny * nz))))
         jobs.append((t, nx, ny, nz, int(rng.integers(iters[0], iters[1] + 1)), int(rng.integers(0, 2**31 - 1))))
     return jobs
+
+
+def served_job(nx: int, ny: int, nz: int, n_iters: int, seed: int, precision: str = "mixed", tol: float = 1e-6):
+    """One job of the served stream: a box with seeded spheres (radius 2-5 voxels, about 15 % of the volume)
+    carved out and the part face-connected to x=0 kept; all DOFs of the active x=0 nodes fixed; 1-3 load cases
+    of random unit direction on seeded 4x4 node patches of the x=nx face (active nodes, equal areas);
+    volfrac in [0.1, 0.4], rmin in [1.2, 3.0], n_iters SIMP iterations, warm-started PCG to relative residual
+    ``tol`` in every iteration (as the 192x96x96 bridge). Returns (model, options)."""
+    rng = np.random.default_rng(seed)
+    g = GridSpec(nx, ny, nz, 1.0)
+    act = np.ones((nz, ny, nx), dtype=bool)
+    target = 0.85 * act.size
+    n_act = act.size
+    for _ in range(100_000):
+        if n_act <= target:
+            break
+        c = rng.uniform([0, 0, 0], [nx, ny, nz])
+        r = rng.uniform(2.0, 5.0)
+        lo = [max(0, int(np.floor(c[a] - r))) for a in range(3)]
+        hi = [min(n, int(np.ceil(c[a] + r)) + 1) for a, n in enumerate((nx, ny, nz))]
+        zz, yy, xx = np.meshgrid(np.arange(lo[2], hi[2]) + 0.5, np.arange(lo[1], hi[1]) + 0.5,
+                                 np.arange(lo[0], hi[0]) + 0.5, indexing="ij")
+        inside = (xx - c[0]) ** 2 + (yy - c[1]) ** 2 + (zz - c[2]) ** 2 <= r * r
+        inside &= (xx > 1.0) & (xx < nx - 1.0)  # keep the clamped layer x=0 and the loaded layer x=nx-1
+        box = act[lo[2]:hi[2], lo[1]:hi[1], lo[0]:hi[0]]
+        n_act -= int((box & inside).sum())
+        box &= ~inside
+    act = _face_connected_from_x0(act)
+    dom = act.reshape(-1).astype(np.uint8)
+    node_act = np.zeros((nz + 1, ny + 1, nx + 1), dtype=bool)
+    for dz in (0, 1):
+        for dy in (0, 1):
+            for dx in (0, 1):
+                node_act[dz:dz + nz, dy:dy + ny, dx:dx + nx] |= act
+    fixed_nodes = [g.node_index(0, j, k) for k in range(nz + 1) for j in range(ny + 1) if node_act[k, j, 0]]
+    cases = []
+    for _c in range(int(rng.integers(1, 4))):
+        v = rng.normal(size=3)
+        v /= np.linalg.norm(v)
+        j0 = int(rng.integers(0, max(1, ny - 2)))
+        k0 = int(rng.integers(0, max(1, nz - 2)))
+        nodes = [g.node_index(nx, j, k) for k in range(k0, min(k0 + 4, nz + 1)) for j in range(j0, min(j0 + 4, ny + 1))
+                 if node_act[k, j, nx]]
+        if not nodes:
+            nodes = [g.node_index(nx, j, k) for k in range(nz + 1) for j in range(ny + 1) if node_act[k, j, nx]]
+        cases.append(LoadCase(SurfacePatch(nodes, np.ones(len(nodes))), tuple(float(x) for x in v)))
+    model = FeModel(g, dom, FeMaterial(1.0, 0.3, 1e-9), FeModel.fix_dofs(fixed_nodes), cases)
+    opts = OptimizerOptions(volume_fraction=float(rng.uniform(0.1, 0.4)), filter_radius_mm=float(rng.uniform(1.2, 3.0)),
+                            penal=3.0, move_limit=0.2, max_iterations=int(n_iters), solver_tolerance_initial=tol,
+                            solver_tolerance_final=tol, solver_max_iterations=20000, precision=precision)
+    return model, opts

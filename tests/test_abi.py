@@ -46,3 +46,16 @@ def test_context_without_device_fails_loudly():
     from mycel_b200.model import DeviceError
     with pytest.raises(DeviceError):
         api.Context(0)
+
+
+def test_job_device_bytes_needs_no_device():
+    """The admission estimate is host arithmetic: it grows with the grid and with the mixed workspace."""
+    from mycel_b200 import api, workloads as W
+    small = W.served_job(16, 8, 8, 2, seed=1, precision="fp64")
+    big = W.served_job(32, 16, 16, 2, seed=1, precision="fp64")
+    mixed = W.served_job(16, 8, 8, 2, seed=1, precision="mixed")
+    b_small, b_big, b_mixed = (api.Server.device_bytes(m, o) for m, o in (small, big, mixed))
+    assert 0 < b_small < b_big
+    assert b_mixed > b_small
+    # at least the problem's own FP64 vectors (F, b, diag, invD, 2 temporaries, 5 PCG vectors, u): 12 x 8 B/DOF
+    assert b_small >= 12 * 8 * small[0].total_dofs
