@@ -67,6 +67,8 @@ def parse():
     ap.add_argument("--batched", action="store_true", help="48 independent problems submitted at once")
     ap.add_argument("--batched-count", type=int, default=48)
     ap.add_argument("--batched-iters", type=int, default=4)
+    ap.add_argument("--job-tol", type=float, default=1e-8,
+                    help="PCG relative residual of the served and batched jobs (every SIMP iteration)")
     return ap.parse_args()
 
 
@@ -172,12 +174,12 @@ def matvec_bytes_fp32(model):
     return 48 * nn + 5 * ne + nn
 
 
-def serve_stream(jobs, precision, slots, budget_bytes, rate_scale=1.0):
+def serve_stream(jobs, precision, slots, budget_bytes, tol, rate_scale=1.0):
     """Submit the jobs at their arrival times to a server and wait for all; returns the stats, per-job
     compliance histories and the wall time. Arrival times are the stream's (seconds from the first)."""
     from mycel_b200 import api
     from mycel_b200 import workloads as W
-    specs = [W.served_job(nx, ny, nz, it, seed, precision=precision) for (_t, nx, ny, nz, it, seed) in jobs]
+    specs = [W.served_job(nx, ny, nz, it, seed, precision=precision, tol=tol) for (_t, nx, ny, nz, it, seed) in jobs]
     hist = []
     with api.Server(slots=slots, hbm_budget_bytes=int(budget_bytes)) as srv:
         t0 = time.perf_counter()
@@ -222,11 +224,11 @@ def serving_report(args, n_jobs, max_elems, rate, slots, budget_gb, precisions, 
     from mycel_b200 import workloads as W
     jobs = W.job_stream(n_jobs=n_jobs, rate=rate, seed=11, max_elems=max_elems)
     out = {"stream": {"jobs": n_jobs, "rate_jobs_s": rate, "elements": [8000, max_elems], "iterations": [20, 60],
-                      "slots": slots, "hbm_budget_gb": budget_gb, "seed": 11}}
+                      "slots": slots, "hbm_budget_gb": budget_gb, "seed": 11, "pcg_tol": args.job_tol}}
     hists = {}
     for prec in precisions:
         sel = jobs if (prec != "fp64" or fp64_jobs is None) else jobs[:fp64_jobs]
-        out[prec], hists[prec] = serve_stream(sel, prec, slots, budget_gb * 1e9)
+        out[prec], hists[prec] = serve_stream(sel, prec, slots, budget_gb * 1e9, args.job_tol)
     if "mixed" in hists and "fp64" in hists:
         out["rel_compliance_err_mixed_vs_fp64"] = compare_histories(hists["mixed"], hists["fp64"])
         n = min(len(hists["mixed"]), len(hists["fp64"]))
@@ -250,12 +252,14 @@ def run_batched(args):
     from mycel_b200 import workloads as W
     probs = W.batched_instances(count=args.batched_count)
     out = {"metric": "batched instances: aggregate SIMP iter/s", "problems": len(probs),
-           "iterations_each": args.batched_iters,
+           "iterations_each": args.batched_iters, "pcg_tol": args.job_tol,
            "elements_total": int(sum(bp.model.total_elements for bp in probs))}
     hists = {}
     for prec in ("mixed", "fp64"):
         with api.Server(slots=args.serve_slots, hbm_budget_bytes=int(args.serve_budget_gb * 1e9)) as srv:
-            ids = [srv.submit(bp.model, bp.options.replace(max_iterations=args.batched_iters, precision=prec))
+            ids = [srv.submit(bp.model, bp.options.replace(max_iterations=args.batched_iters, precision=prec,
+                                                          solver_tolerance_initial=args.job_tol,
+                                                          solver_tolerance_final=args.job_tol))
                    for bp in probs]
             srv.wait()
             st = srv.stats()

@@ -75,6 +75,10 @@ typedef struct {
   int32_t refinement_steps; /* mixed form: outer FP64 refinement steps; 0 for FP64 */
   int32_t inner_iterations; /* mixed form: FP32 PCG iterations summed over refinement steps */
   char message[256];
+  /* mixed form: iterations of the FP64 PCG that finished a solve whose FP32 inner iteration stalled (a
+     refinement cycle 4x slower than the average so far), broke down or ran out of iterations; 0 otherwise.
+     iterations = inner_iterations + fallback_iterations. */
+  int32_t fallback_iterations;
 } mycel_pcg_result;
 
 /* StaticAnalysisOptions (Fem/StaticAnalysis.cs:8-17); the preconditioner is Jacobi. */
@@ -149,6 +153,8 @@ int32_t mycel_problem_create(mycel_ctx* ctx, const mycel_grid* grid, const uint8
                              const mycel_material* material, const int32_t* fixed_dofs, int32_t n_fixed,
                              const mycel_load_case* loads, int32_t n_loads, const double* element_density,
                              double penal, mycel_problem** out);
+/* Ends the problem's live SIMP sessions (as mycel_simp_end), then frees the problem; do not use those
+   sessions afterwards. */
 int32_t mycel_problem_destroy(mycel_problem* p);
 int32_t mycel_problem_info_get(mycel_problem* p, mycel_problem_info* out);
 /* Tuning of the kernels of one problem (no counterpart in the reference, which has one CPU kernel per step).

@@ -38,7 +38,8 @@ class ProblemInfo(C.Structure):
 
 class PcgResultC(C.Structure):
     _fields_ = [("iterations", i32), ("final_residual", dbl), ("converged", i32), ("elapsed_ms", dbl),
-                ("refinement_steps", i32), ("inner_iterations", i32), ("message", C.c_char * 256)]
+                ("refinement_steps", i32), ("inner_iterations", i32), ("message", C.c_char * 256),
+                ("fallback_iterations", i32)]
 
 
 class StaticOptions(C.Structure):

@@ -10,6 +10,7 @@ from __future__ import annotations
 
 import ctypes as C
 import threading
+import weakref
 from typing import Callable, Optional
 
 import numpy as np
@@ -90,7 +91,7 @@ def default_context() -> Context:
 def _pcg_result(r: L.PcgResultC) -> PcgResult:
     msg = r.message.decode("utf-8", "replace")
     return PcgResult(int(r.iterations), float(r.final_residual), bool(r.converged), float(r.elapsed_ms), msg or None,
-                     int(r.refinement_steps))
+                     int(r.refinement_steps), int(r.inner_iterations), int(r.fallback_iterations))
 
 
 class Problem:
@@ -124,6 +125,8 @@ class Problem:
 
     def close(self):
         if getattr(self, "handle", None):
+            for sess in list(getattr(self, "_sessions", ())):
+                sess.close()
             L.load().mycel_problem_destroy(self.handle)
             self.handle = None
 
@@ -404,6 +407,9 @@ class SimpSession:
         _check(L.load().mycel_simp_begin(problem.handle, C.byref(so), C.byref(h)), problem.ctx)
         self.handle = h.value
         self.done = False
+        if not hasattr(problem, "_sessions"):
+            problem._sessions = weakref.WeakSet()
+        problem._sessions.add(self)
 
     def step(self) -> IterationSnapshot:
         r = L.IterRecord()
@@ -426,7 +432,8 @@ class SimpSession:
 
     def close(self):
         if getattr(self, "handle", None):
-            L.load().mycel_simp_end(self.handle)
+            if getattr(self.problem, "handle", None):  # a destroyed problem has ended its sessions already
+                L.load().mycel_simp_end(self.handle)
             self.handle = None
 
     def __del__(self):

@@ -572,6 +572,7 @@ extern "C" int32_t mycel_problem_create(mycel_ctx* c, const mycel_grid* grid, co
 
 extern "C" int32_t mycel_problem_destroy(mycel_problem* p) {
   if (!p) return MYCEL_OK;
+  while (!p->sessions.empty()) mycel_simp_end(p->sessions.back());  // sessions cannot outlive their problem
   cudaSetDevice(p->ctx->device);
   cudaStreamSynchronize(p->ctx->stream);
   for (int k = 0; k < 2; ++k) {

@@ -21,6 +21,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -44,12 +45,13 @@ struct MixState {
   double target;     // absolute residual at which to verify convergence (tol * ||P b|| * safety)
   double flush_at;   // absolute recursive residual that triggers a true-residual replacement
   double rho0, alpha, beta, rn, pap;
+  double flush_factor;  // a replacement when the recursive residual has dropped by this factor
   unsigned int counter;
   unsigned int pad2;
 };
 
 constexpr int kT = 256;
-constexpr double kFlushFactor = 1e-2;
+constexpr double kFlushFactor = 1e-1;
 
 __device__ __forceinline__ bool elect_last32(unsigned int* counter) {
   __shared__ bool last;
@@ -1227,7 +1229,7 @@ __global__ void __launch_bounds__(kT) k_xr32(int64_t n, float* __restrict__ x, f
     st->rho0 = srz;
     st->first = 1;
     st->status = (rn <= st->target) ? MIX_FLUSH : MIX_RUNNING;
-    st->flush_at = rn * kFlushFactor;
+    st->flush_at = rn * st->flush_factor;
     return;
   }
   if (mode == 1) {  // true residual replaced the recursive one: keep the direction
@@ -1239,7 +1241,7 @@ __global__ void __launch_bounds__(kT) k_xr32(int64_t n, float* __restrict__ x, f
       else st->beta = beta;
     }
     st->rho0 = srz;
-    st->flush_at = rn * kFlushFactor;
+    st->flush_at = rn * st->flush_factor;
     st->status = MIX_RUNNING;
     return;
   }
@@ -1361,12 +1363,13 @@ int32_t mixed_apply_k_f64io(mycel_problem* p, const double* x, double* y, int pr
 
 static MixState* mix_state(mycel_problem* p) { return (MixState*)(p->d_part2 + p->n_part2 - 64); }
 
-__global__ void k_mix_init(MixState* st, double target, int max_iter) {
+__global__ void k_mix_init(MixState* st, double target, int max_iter, double flush_factor) {
   MixState s = {};
   s.status = MIX_RUNNING;
   s.target = target;
   s.max_iter = max_iter;
   s.first = 1;
+  s.flush_factor = flush_factor;
   *st = s;
 }
 
@@ -1483,6 +1486,7 @@ int32_t mixed_solve_entry(mycel_problem* p, const double* d_b, const int32_t* d_
     return MYCEL_OK;
   }
   const int chunk = 16;
+  const bool verbose = std::getenv("MYCEL_VERBOSE") != nullptr;
   MYCEL_CUDA(c, cudaMemsetAsync(p->d_err, 0, sizeof(int), s));  // bounded-wait failures of this solve only
   if ((st = resolve_mv32(p))) return st;
   if ((st = capture_mixed_graph(p, chunk))) return st;
@@ -1498,14 +1502,20 @@ int32_t mixed_solve_entry(mycel_problem* p, const double* d_b, const int32_t* d_
   cudaEventCreateWithFlags(&evs[1], cudaEventDisableTiming);
   struct EvGuard { cudaEvent_t* e; ~EvGuard() { cudaEventDestroy(e[0]); cudaEventDestroy(e[1]); } } evg{evs};
   int total_iter = 0;
+  bool stalled = false;
   if (!ok) {
     cudaMemsetAsync(p->f_x, 0, sizeof(float) * p->g.n32, s);
-    k_mix_init<<<1, 1, 0, s>>>(ms, 0.5 * tol * bnorm, max_iter);
+    k_mix_init<<<1, 1, 0, s>>>(ms, 0.5 * tol * bnorm, max_iter, kFlushFactor);
     k_xr32<<<sb, kT, 0, s>>>(p->g.n32, p->f_x, p->f_r, p->f_z, p->f_p0, p->f_ap, p->d_invdf, ms, part, 2);
     c->launches += 2;
     int64_t launched = 0;
     const int64_t cap = (int64_t)max_iter + 64 * chunk + 4096;
     int iter_at_resume = 0;
+    // stall watch: a refinement cycle gains log10(1/kFlushFactor) orders of the true residual; after two
+    // cycles, one that runs 4x longer than the average iterations per order so far (and at least 500
+    // iterations) has stalled (FP32 CG on a badly conditioned system)
+    const double rel_start = rel;
+    int64_t cycle_limit = INT64_MAX;
     for (;;) {
       // pipeline: chunk k is queued while the status after chunk k-1 is read
       int64_t k = 0;
@@ -1531,6 +1541,12 @@ int32_t mixed_solve_entry(mycel_problem* p, const double* d_b, const int32_t* d_
         MYCEL_CUDA(c, cudaEventSynchronize(evs[pi]));
         status = slot[pi]->status;
         if (status != MIX_RUNNING) break;
+        if (slot[pi]->iter - iter_at_resume > cycle_limit) {
+          stalled = true;
+          k_mix_set<<<1, 1, 0, s>>>(ms, MIX_FLUSH);  // the queued chunk and what follows skip their work
+          c->launches++;
+          break;
+        }
         if (c->profile) {  // every iteration of chunk k-1 ran: its first matvec is a full launch
           float ms_ = 0.f;
           if (cudaEventElapsedTime(&ms_, p->prof_ev[pi][0], p->prof_ev[pi][1]) == cudaSuccess) {
@@ -1557,19 +1573,39 @@ int32_t mixed_solve_entry(mycel_problem* p, const double* d_b, const int32_t* d_
       ++flushes;
       if ((st = true_residual(p, d_b, d_u, &rn))) return st;
       rel = rn / bnorm;
+      if (verbose)
+        std::fprintf(stderr, "mycel: mixed refinement %d: inner %d, status %d, recursive %.3e, true %.3e (tol %.1e)\n",
+                     flushes, total_iter, status, h->rn / bnorm, rel, tol);
       if (rel <= tol) {
         ok = true;
         break;
       }
-      if (status != MIX_FLUSH || total_iter >= max_iter) break;
+      const double orders = std::log10(rel_start / rel);
+      if (flushes >= 2 && orders > 0.0)
+        cycle_limit = std::max<int64_t>(500, (int64_t)(4.0 * std::log10(1.0 / kFlushFactor) * total_iter / orders));
+      if (stalled || status != MIX_FLUSH || total_iter >= max_iter) break;
       k_xr32<<<sb, kT, 0, s>>>(p->g.n32, p->f_x, p->f_r, p->f_z, p->f_p0, p->f_ap, p->d_invdf, ms, part, 1);
       c->launches++;
       iter_at_resume = total_iter;
     }
   }
-  res->iterations = total_iter;
+  // FP32 inner iteration stalled, broke down or ran out of iterations: finish with the plain FP64 PCG,
+  // warm-started from the refined solution (on the device, like everything else)
+  int fb_iter = 0;
+  if (!ok) {
+    mycel_pcg_result r64;
+    if ((st = pcg_solve_fp64(p, d_b, d_nz, n_nz, d_u, tol, max_iter, cancel, &r64))) return st;
+    fb_iter = r64.iterations;
+    ok = r64.converged != 0;
+    rel = r64.final_residual;
+    if (verbose)
+      std::fprintf(stderr, "mycel: mixed solve finished in FP64 (%s after %d inner iterations): %d iterations, %.3e\n",
+                   stalled ? "stalled" : "not converged", total_iter, fb_iter, rel);
+  }
+  res->iterations = total_iter + fb_iter;
   res->inner_iterations = total_iter;
   res->refinement_steps = flushes;
+  res->fallback_iterations = fb_iter;
   res->final_residual = rel;
   res->converged = ok ? 1 : 0;
   if (!ok)

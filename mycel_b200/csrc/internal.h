@@ -119,6 +119,7 @@ struct mycel_problem {
   int* d_err = nullptr;           // device error word (bounded waits that gave up)
   double diag_ke[24];
   int64_t n_active = 0, n_active_nodes = 0, n_active_fixed = 0;
+  std::vector<mycel_simp_session*> sessions;  // live SIMP sessions on this problem (ended by problem_destroy)
   std::vector<int32_t> fixed_host;        // FixedDofs as given (may repeat)
   std::vector<int32_t> load_nodes_host;   // union of load patch nodes (hinge shell)
   std::vector<double> forces_host;        // AssembleForces result (box DOF vector)

@@ -219,6 +219,7 @@ extern "C" int32_t mycel_simp_begin(mycel_problem* p, const mycel_simp_options* 
   s->o.passive_mask = nullptr;
   s->o.initial_density = nullptr;
   s->o.warm_start_displacements = nullptr;
+  p->sessions.push_back(s);
   *out = s;
   return MYCEL_OK;
 }
@@ -380,6 +381,8 @@ extern "C" int32_t mycel_simp_read(mycel_simp_session* s, double* u, float* phys
 
 extern "C" int32_t mycel_simp_end(mycel_simp_session* s) {
   if (!s) return MYCEL_OK;
+  auto& live = s->p->sessions;
+  live.erase(std::remove(live.begin(), live.end(), s), live.end());
   cudaSetDevice(s->p->ctx->device);
   cudaStreamSynchronize(s->p->ctx->stream);
   if (s->filt) mycel_filter_destroy(s->filt);

@@ -228,6 +228,8 @@ class PcgResult:
     elapsed_ms: float = 0.0
     message: Optional[str] = None
     refinement_steps: int = 0
+    inner_iterations: int = 0     # mixed form: FP32 inner iterations
+    fallback_iterations: int = 0  # mixed form: FP64 iterations that finished a stalled solve
 
 
 @dataclass

@@ -81,3 +81,20 @@ def test_mixed_simp_cantilever_within_1e6(oracle, ctx):
         assert abs(a.compliance - b["compliance"]) <= 1e-6 * abs(b["compliance"])
         assert a.solver_residual <= 1e-8
     assert np.abs(res.final_physical_density - ref.phys).max() <= 1e-5
+
+
+def test_mixed_solve_finishes_in_fp64_when_inner_iterations_run_out(oracle, ctx):
+    """An iteration budget the FP32 inner loop alone cannot meet: the solve is finished by the FP64 PCG from
+    the refined solution, reports both counts, and matches the FP64 oracle to the solve tolerance."""
+    m = carved_model(31, 12, 9, seed=8, emin_ratio=1e-9)
+    om, pr = oracle.Model(m), api.Problem(m, ctx)
+    b = om.forces() * (om.constrained() == 0)
+    ref, _ = om.pcg_solve(b, tol=1e-8, max_iter=20000)
+    _u0, r0 = pr.pcg_solve(b, tol=1e-8, max_iterations=20000, precision="mixed")
+    assert r0.converged and r0.fallback_iterations == 0
+    budget = int(r0.inner_iterations * 0.75)
+    u, r = pr.pcg_solve(b, tol=1e-8, max_iterations=budget, precision="mixed")
+    assert r.inner_iterations <= budget
+    assert r.fallback_iterations > 0 and r.iterations == r.inner_iterations + r.fallback_iterations
+    assert r.converged and r.final_residual <= 1e-8
+    assert np.abs(u - ref).max() <= 1e-5 * np.abs(ref).max()
