@@ -229,6 +229,10 @@ def serving_report(args, n_jobs, max_elems, rate, slots, budget_gb, precisions, 
     for prec in precisions:
         sel = jobs if (prec != "fp64" or fp64_jobs is None) else jobs[:fp64_jobs]
         out[prec], hists[prec] = serve_stream(sel, prec, slots, budget_gb * 1e9, args.job_tol)
+    if "fp64f" in hists and "fp64" in hists:
+        out["rel_compliance_err_fp64f_vs_fp64"] = compare_histories(hists["fp64f"], hists["fp64"])
+        if out["fp64"]["simp_iter_s"]:
+            out["speedup_fp64f_vs_fp64"] = out["fp64f"]["simp_iter_s"] / out["fp64"]["simp_iter_s"]
     if "mixed" in hists and "fp64" in hists:
         out["rel_compliance_err_mixed_vs_fp64"] = compare_histories(hists["mixed"], hists["fp64"])
         n = min(len(hists["mixed"]), len(hists["fp64"]))

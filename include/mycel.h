@@ -35,6 +35,9 @@ extern "C" {
 
 #define MYCEL_PRECISION_FP64 0  /* plain method: FP64 throughout, reproduces the reference's arithmetic */
 #define MYCEL_PRECISION_MIXED 1 /* FP32 inner PCG (K·u, Jacobi) inside FP64 iterative refinement */
+/* FP64 throughout with the factorised cube-element operator (same tolerance test on the exact FP64 residual,
+   not bit-exact with the reference's colour-ordered product); also what a stalled mixed solve goes on in */
+#define MYCEL_PRECISION_FP64_FACTORED 2
 
 typedef struct mycel_ctx mycel_ctx;
 typedef struct mycel_problem mycel_problem;
@@ -76,7 +79,10 @@ typedef struct {
   int32_t inner_iterations; /* mixed form: FP32 PCG iterations summed over refinement steps */
   char message[256];
   /* mixed form: iterations of the FP64 PCG that finished a solve whose FP32 inner iteration stalled (a
-     refinement cycle 4x slower than the average so far), broke down or ran out of iterations; 0 otherwise.
+     refinement cycle 4x slower than the average so far), broke down or ran out of iterations: the solve goes
+     on in the fast FP64 form (MYCEL_PRECISION_FP64_FACTORED) from the refined u, then, should that fail too,
+     in the plain FP64 PCG. After a stall, later mixed solves of the same problem start in the fast FP64 form
+     (inner_iterations 0). For MYCEL_PRECISION_FP64_FACTORED: the plain FP64 PCG's iterations.
      iterations = inner_iterations + fallback_iterations. */
   int32_t fallback_iterations;
 } mycel_pcg_result;

@@ -22,7 +22,8 @@ from .model import (ArgumentError, CancelledError, DeviceError, FeModel, Invalid
 
 FP64 = 0
 MIXED = 1
-_PREC = {"fp64": FP64, "mixed": MIXED, FP64: FP64, MIXED: MIXED}
+FP64_FACTORED = 2
+_PREC = {"fp64": FP64, "mixed": MIXED, "fp64f": FP64_FACTORED, FP64: FP64, MIXED: MIXED, FP64_FACTORED: FP64_FACTORED}
 
 _ERRORS = {1: ArgumentError, 2: InvalidOperationError, 3: InvalidOperationError, 4: InvalidOperationError,
            5: CancelledError, 6: TimeoutError_, 7: DeviceError, 8: OutOfMemoryError, 9: InvalidOperationError}

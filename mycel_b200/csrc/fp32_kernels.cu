@@ -717,6 +717,245 @@ static dim3 fac_grid(const GridDims& g, int zseg) {
 }
 
 // ---------------------------------------------------------------------------------------------------------
+// FP64 K p with the factorised cube-element operator (fast FP64 form; not bit-exact with the reference's
+// colour-ordered product, equal to it up to FP64 rounding). Same tiling as k_mv32f with one element plane
+// per step, FP64 node planes by TMA from the padded FP64 layout (row starts rounded down to 16 bytes, boxes
+// of FPY x FBW64 doubles), one thread per element, x-neighbour by shuffle, y-neighbour by shared exchange.
+// MODE 1 fuses p_t = z + beta p_{t-1}, the write of p_t and the p.Ap partials.
+// ---------------------------------------------------------------------------------------------------------
+template <class T>
+__device__ __forceinline__ void wht8s(T (&v)[8]) {
+#pragma unroll
+  for (int bit = 1; bit < 8; bit <<= 1)
+#pragma unroll
+    for (int a = 0; a < 8; ++a)
+      if (!(a & bit)) {
+        const T lo = v[a], hi = v[a | bit];
+        v[a] = hi + lo;
+        v[a | bit] = hi - lo;
+      }
+}
+
+template <class T>
+__device__ __forceinline__ void iwht8s(T (&v)[8]) {
+#pragma unroll
+  for (int bit = 1; bit < 8; bit <<= 1)
+#pragma unroll
+    for (int a = 0; a < 8; ++a)
+      if (!(a & bit)) {
+        const T e = v[a], o = v[a | bit];
+        v[a] = e - o;
+        v[a | bit] = e + o;
+      }
+}
+
+// y = E KE(h) u for one element in FP64 (same basis and constants as hex_apply2); sink(c, y_c[8])
+template <class Sink>
+__device__ __forceinline__ void hex_apply64(const HexOpD& op, double E, double (&u)[3][8], Sink&& sink) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) wht8s(u[c]);
+  double d[2][3], lam[2], mu[2];
+#pragma unroll
+  for (int a = 0; a < 2; ++a) {
+#pragma unroll
+    for (int n = 0; n < 3; ++n) d[a][n] = E * op.dcl[a][n];
+    lam[a] = E * op.lam[a];
+    mu[a] = E * op.mu[a];
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    double y[8];
+    y[0] = 0.0;
+#pragma unroll
+    for (int p = 1; p < 8; ++p) {
+      const int pc = (p >> c) & 1;
+      const int n = (p & 1) + ((p >> 1) & 1) + ((p >> 2) & 1) - pc;
+      double acc = d[pc][n] * u[c][p];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        if (j == c) continue;
+        const int k = 3 - c - j;
+        const int pj = (p >> j) & 1, pk = (p >> k) & 1;
+        const int q = p ^ (1 << c) ^ (1 << j);
+        if (pc == 1 && pj == 0) acc = fma(lam[pk], u[j][q], acc);
+        if (pc == 0 && pj == 1) acc = fma(mu[pk], u[j][q], acc);
+      }
+      y[p] = acc;
+    }
+    iwht8s(y);
+    sink(c, y);
+  }
+}
+
+constexpr int FBW64 = 100;                                       // doubles per staged node row (>= 99 + 1)
+constexpr int kFac64StageBytes = FPY * FBW64 * 8;
+constexpr int kFac64StagePitch = (kFac64StageBytes + 127) & ~127;
+constexpr size_t fac64_smem_bytes(int mode) {
+  return (size_t)FNST * kFac64StagePitch * (mode == 1 ? 2 : 1) + sizeof(double) * 2 * FY * 6 * FX;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(FX * FY, 1) k_mv64f(GridDims g, const __grid_constant__ HexOpD op,
+                                                      const __grid_constant__ CUtensorMap tm_a,
+                                                      const __grid_constant__ CUtensorMap tm_b,
+                                                      double* __restrict__ pnew, double* __restrict__ y,
+                                                      const double* __restrict__ E, const uint8_t* __restrict__ nf,
+                                                      int projected, MixState* st, double* part, int zseg, int* err) {
+  extern __shared__ __align__(128) unsigned char fac_smem[];
+  double* yb = reinterpret_cast<double*>(fac_smem + (size_t)FNST * kFac64StagePitch * (MODE == 1 ? 2 : 1));
+  __shared__ __align__(8) unsigned long long full[FNST];
+  __shared__ double sh[32];
+  if (MODE == 1 && st->status != MIX_RUNNING) return;
+  const double beta = MODE == 1 ? st->beta : 0.0;
+  const bool two = MODE == 1 && st->first == 0;
+  const int l = threadIdx.x, w = threadIdx.y, tid = w * FX + l;
+  const int i0 = blockIdx.x * FOX, j0 = blockIdx.y * FOY, k0 = blockIdx.z * zseg;
+  const int k1 = min(k0 + zseg, g.nz1);
+  const int xs = (3 * (i0 - 1)) & ~1;   // staged row start (doubles), 16-byte aligned, may be -4
+  const int rem = 3 * (i0 - 1) - xs;    // 0 or 1
+  const uint32_t tx_bytes = (uint32_t)kFac64StageBytes * (two ? 2u : 1u);
+  auto stage_of = [&](int kk) { return (kk - k0 + 1) % FNST; };
+  auto parity_of = [&](int kk) { return (uint32_t)(((kk - k0 + 1) / FNST) & 1); };
+  auto plane_a = [&](int sl) { return reinterpret_cast<double*>(fac_smem + (size_t)sl * kFac64StagePitch); };
+  auto plane_b = [&](int sl) { return reinterpret_cast<double*>(fac_smem + (size_t)(FNST + sl) * kFac64StagePitch); };
+  auto issue = [&](int kk) {  // one thread
+    const int sl = stage_of(kk);
+    const uint32_t bar = smem_u32(&full[sl]);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(tx_bytes) : "memory");
+    tma_load_plane(plane_a(sl), &tm_a, xs, j0 - 1, kk, bar);
+    if (two) tma_load_plane(plane_b(sl), &tm_b, xs, j0 - 1, kk, bar);
+  };
+  if (tid == 0) {
+    for (int q = 0; q < FNST; ++q)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&full[q])) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  }
+  __syncthreads();
+  if (tid == 0)
+    for (int kk = k0 - 1; kk <= min(k0 - 2 + FNST, k1); ++kk) issue(kk);
+  bool ok = true;
+  auto wait_plane = [&](int kk) {
+    if (!mbar_wait(smem_u32(&full[stage_of(kk)]), parity_of(kk))) ok = false;
+  };
+  auto gather4 = [&](int kk, double (&v)[4][3]) {
+    const int sl = stage_of(kk);
+    const double* a = plane_a(sl);
+    const double* b = plane_b(sl);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int o = (w + (q >> 1)) * FBW64 + rem + 3 * (l + (q & 1));
+#pragma unroll
+      for (int c = 0; c < 3; ++c) v[q][c] = two ? fma(beta, b[o + c], a[o + c]) : a[o + c];
+    }
+  };
+  const int ex = i0 - 1 + l, ey = j0 - 1 + w;
+  const bool exy = ex >= 0 && ex < g.nx && ey >= 0 && ey < g.ny;
+  const int64_t ebase = (int64_t)ex + (int64_t)g.nx * ey, eplane = (int64_t)g.nx * g.ny;
+  auto eload = [&](int kk) -> double { return (exy && kk >= 0 && kk < g.nz) ? __ldg(E + ebase + eplane * kk) : 0.0; };
+  const int nxo = i0 + l, nyo = j0 + w;
+  const bool mine = l < FOX && w < FOY && nxo < g.nx1 && nyo < g.ny1;
+  const int64_t nbase = nxo + (int64_t)g.nx1 * nyo;
+  const int64_t fbase = (int64_t)g.rp64 * nyo + 3 * nxo;
+  const int64_t fplane = (int64_t)g.rp64 * g.ny1;
+  const int64_t nplane = (int64_t)g.nx1 * g.ny1;
+
+  wait_plane(k0 - 1);
+  wait_plane(k0);
+  double ub[4][3];
+  gather4(k0 - 1, ub);
+  __syncthreads();  // the stage of plane k0 - 1 is refilled in the first step
+  double carry[3] = {0.0, 0.0, 0.0};
+  double pap = 0.0;
+  double e0 = eload(k0 - 1), e1 = eload(k0);
+  uint8_t f_next = (mine && projected && k0 < k1) ? nf[nbase + nplane * k0] : (uint8_t)0;
+  for (int kk = k0 - 1; kk < k1; ++kk) {
+    wait_plane(kk + 1);
+    double ut[4][3];
+    gather4(kk + 1, ut);
+    if (tid == 0 && kk + FNST <= k1) {
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      issue(kk + FNST);
+    }
+    const double e_cur = e0;
+    e0 = e1;
+    e1 = eload(kk + 2);
+    const bool outp = mine && kk >= k0;
+    const uint8_t f = f_next;
+    if (outp && projected && kk + 1 < k1) f_next = nf[nbase + nplane * (kk + 1)];
+    if (MODE == 1 && mine && kk + 1 >= k0 && kk + 1 < k1) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) pnew[fbase + fplane * (kk + 1) + c] = ut[3][c];
+    }
+    double u[3][8];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        u[c][b] = ub[b][c];
+        u[c][b + 4] = ut[b][c];
+      }
+    double comb[2][2][3];  // [y][z][c]
+    hex_apply64(op, e_cur, u, [&](int c, double (&yc)[8]) {
+#pragma unroll
+      for (int by = 0; by < 2; ++by)
+#pragma unroll
+        for (int bz = 0; bz < 2; ++bz) {
+          const double nb = __shfl_down_sync(0xffffffffu, yc[2 * by + 4 * bz], 1);
+          comb[by][bz][c] = yc[1 + 2 * by + 4 * bz] + nb;
+        }
+    });
+    double* ybw = yb + ((kk & 1) * FY + w) * 6 * FX + l;
+#pragma unroll
+    for (int bz = 0; bz < 2; ++bz)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) ybw[(3 * bz + c) * FX] = comb[0][bz][c];
+    __syncthreads();
+    if (mine) {
+      const double* ybr = yb + ((kk & 1) * FY + w + 1) * 6 * FX + l;
+      double top[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const double bot = comb[1][0][c] + ybr[c * FX];
+        top[c] = comb[1][1][c] + ybr[(3 + c) * FX];
+        if (outp) {
+          const double pv = ub[3][c];
+          const double yo = (f >> c & 1) ? pv : carry[c] + bot;
+          y[fbase + fplane * kk + c] = yo;
+          if (MODE == 1) pap += pv * yo;
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) carry[c] = top[c];
+    }
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) ub[b][c] = ut[b][c];
+  }
+  if (!ok && err) atomicExch(err, 1);
+  if (MODE == 1) mv32_finish(pap, sh, st, part, tid, err);
+}
+
+// z-segment length of the FP64 factorised kernel: one element plane per step
+static int fac64_zseg(const GridDims& g, int resident) {
+  const int64_t txy = (int64_t)((g.nx1 + FOX - 1) / FOX) * ((g.ny1 + FOY - 1) / FOY);
+  const int max_segs = std::max(1, g.nz1 / 4);
+  int best_z = g.nz1;
+  int64_t best_cost = INT64_MAX;
+  for (int segs = 1; segs <= max_segs; ++segs) {
+    const int zs = (g.nz1 + segs - 1) / segs;
+    const int64_t n = txy * ((g.nz1 + zs - 1) / zs);
+    const int64_t cost = ((n + resident - 1) / resident) * (zs + 1);
+    if (cost < best_cost) {
+      best_cost = cost;
+      best_z = zs;
+    }
+  }
+  return best_z;
+}
+
+// ---------------------------------------------------------------------------------------------------------
 // FP32 K p on the 5th-generation tensor cores (tcgen05, kind::tf32, 3xTF32 for FP32-level products).
 // A CTA takes a 16 x 8 tile of elements per element plane (one MMA row per element, M = 128) and owns the
 // 15 x 7 nodes strictly inside it; CTAs overlap by one element in x and y. It marches over z: for element
@@ -1027,8 +1266,9 @@ static dim3 tc_grid(const GridDims& g, int zseg) {
 // SM never ask for more than its 512 TMEM columns (4 x 128).
 constexpr int kTcPadSmem = 20 * 1024;
 
-// TMA descriptor of an FP32 work vector: 3-D [nz1][ny1][rp] floats, box [1][FPY][FBW], zero fill outside.
-static int32_t encode_plane_map(mycel_problem* p, float* base, CUtensorMap* out) {
+// TMA descriptor of a work vector: 3-D [nz1][ny1][pitch] elements (floats: pitch rp, box [1][FPY][FBW];
+// doubles: pitch rp64, box [1][FPY][FBW64]), zero fill outside.
+static int32_t encode_plane_map(mycel_problem* p, void* base, bool f64, CUtensorMap* out) {
   static PFN_cuTensorMapEncodeTiled encode = nullptr;
   static std::once_flag once;
   std::call_once(once, [] {
@@ -1040,13 +1280,14 @@ static int32_t encode_plane_map(mycel_problem* p, float* base, CUtensorMap* out)
   });
   if (!encode) return set_error(p->ctx, MYCEL_E_DEVICE, "cuTensorMapEncodeTiled is not available from the driver");
   const GridDims& g = p->g;
-  cuuint64_t dims[3] = {(cuuint64_t)g.rp, (cuuint64_t)g.ny1, (cuuint64_t)g.nz1};
-  cuuint64_t strides[2] = {(cuuint64_t)g.rp * 4, (cuuint64_t)g.rp * g.ny1 * 4};
-  cuuint32_t box[3] = {(cuuint32_t)FBW, (cuuint32_t)FPY, 1};
+  const cuuint64_t pitch = f64 ? (cuuint64_t)g.rp64 : (cuuint64_t)g.rp, es = f64 ? 8 : 4;
+  cuuint64_t dims[3] = {pitch, (cuuint64_t)g.ny1, (cuuint64_t)g.nz1};
+  cuuint64_t strides[2] = {pitch * es, pitch * g.ny1 * es};
+  cuuint32_t box[3] = {(cuuint32_t)(f64 ? FBW64 : FBW), (cuuint32_t)FPY, 1};
   cuuint32_t estr[3] = {1, 1, 1};
-  CUresult r = encode(out, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, estr,
-                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  CUresult r = encode(out, f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims,
+                      strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                      CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS)
     return set_error(p->ctx, MYCEL_E_DEVICE, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
   return MYCEL_OK;
@@ -1057,6 +1298,37 @@ static const CUtensorMap* tmap_of(mycel_problem* p, const float* ptr) {
   for (int q = 0; q < 4; ++q)
     if (ptr == bufs[q]) return &p->f_tmap[q];
   return nullptr;
+}
+
+static const CUtensorMap* tmap64_of(mycel_problem* p, const double* ptr) {
+  const double* bufs[4] = {p->g_r, p->g_z, p->g_p0, p->g_p1};
+  for (int q = 0; q < 4; ++q)
+    if (ptr == bufs[q]) return &p->g_tmap[q];
+  return nullptr;
+}
+
+// FP64 factorised matvec launch (fast FP64 form); inputs are mapped FP64 work vectors
+template <int MODE>
+static void launch_mv64f(mycel_problem* p, cudaStream_t s, const double* xin, const double* z, const double* pold,
+                         double* pnew, double* y, int projected, MixState* st, double* part) {
+  const GridDims& g = p->g;
+  static int occ = 0;
+  if (!occ) {
+    int o = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_mv64f<1>, FX * FY, fac64_smem_bytes(1));
+    occ = std::max(1, o);
+  }
+  const int zs = fac64_zseg(g, occ * p->ctx->num_sms);
+  const CUtensorMap* ta = tmap64_of(p, MODE == 1 ? z : xin);
+  const CUtensorMap* tb = MODE == 1 ? tmap64_of(p, pold) : ta;
+  if (!ta || !tb) {  // internal invariant: inputs are always one of the four mapped work vectors
+    std::fprintf(stderr, "mycel: FP64 matvec input is not a mapped work vector\n");
+    std::abort();
+  }
+  const dim3 grid((unsigned)((g.nx1 + FOX - 1) / FOX), (unsigned)((g.ny1 + FOY - 1) / FOY),
+                  (unsigned)((g.nz1 + zs - 1) / zs));
+  k_mv64f<MODE><<<grid, dim3(FX, FY), fac64_smem_bytes(MODE), s>>>(g, p->hexop64, *ta, *tb, pnew, y, p->d_E,
+                                                                     p->d_nflags, projected, st, part, zs, p->d_err);
 }
 
 // FP32 matvec launch, variant chosen per problem (MYCEL_MV32_*)
@@ -1166,51 +1438,9 @@ static int32_t resolve_mv32(mycel_problem* p) {
   return MYCEL_OK;
 }
 
-// x += alpha p, r -= alpha Ap, z = r invD; partials of r.r and r.z (FP64). mode 0: CG step; 1: residual
-// replacement (z, rho from the new r; beta = rho_new / rho_old); 2: start (z, rho; next step starts p = z).
-__global__ void __launch_bounds__(kT) k_xr32(int64_t n, float* __restrict__ x, float* __restrict__ r,
-                                             float* __restrict__ z, const float* __restrict__ p,
-                                             const float* __restrict__ ap, const float* __restrict__ invd,
-                                             MixState* st, double* part, int mode) {
-  __shared__ double sh[32];
-  if (mode == 0 && st->status != MIX_RUNNING) return;
-  const float alpha = mode ? 0.f : (float)st->alpha;
-  double rr = 0.0, rz = 0.0;
-  const int64_t n4 = n >> 2;
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n4; i += stride) {
-    float4 rv = reinterpret_cast<const float4*>(r)[i];
-    float4 iv = reinterpret_cast<const float4*>(invd)[i];
-    if (mode == 0) {
-      float4 xv = reinterpret_cast<const float4*>(x)[i];
-      float4 pv = reinterpret_cast<const float4*>(p)[i];
-      float4 av = reinterpret_cast<const float4*>(ap)[i];
-      xv.x = fmaf(alpha, pv.x, xv.x); xv.y = fmaf(alpha, pv.y, xv.y);
-      xv.z = fmaf(alpha, pv.z, xv.z); xv.w = fmaf(alpha, pv.w, xv.w);
-      rv.x = fmaf(-alpha, av.x, rv.x); rv.y = fmaf(-alpha, av.y, rv.y);
-      rv.z = fmaf(-alpha, av.z, rv.z); rv.w = fmaf(-alpha, av.w, rv.w);
-      reinterpret_cast<float4*>(x)[i] = xv;
-      reinterpret_cast<float4*>(r)[i] = rv;
-    }
-    float4 zv = make_float4(rv.x * iv.x, rv.y * iv.y, rv.z * iv.z, rv.w * iv.w);
-    reinterpret_cast<float4*>(z)[i] = zv;
-    rr += (double)rv.x * rv.x + (double)rv.y * rv.y + (double)rv.z * rv.z + (double)rv.w * rv.w;
-    rz += (double)rv.x * zv.x + (double)rv.y * zv.y + (double)rv.z * zv.z + (double)rv.w * zv.w;
-  }
-  if (blockIdx.x == 0) {  // tail (n not a multiple of 4)
-    for (int64_t i = 4 * n4 + threadIdx.x; i < n; i += blockDim.x) {
-      float rv = r[i];
-      if (mode == 0) {
-        x[i] = fmaf(alpha, p[i], x[i]);
-        rv = fmaf(-alpha, ap[i], rv);
-        r[i] = rv;
-      }
-      float zv = rv * invd[i];
-      z[i] = zv;
-      rr += (double)rv * rv;
-      rz += (double)rv * zv;
-    }
-  }
+// End of a vector step: CTA sums of r.r and r.z, fixed-order sums by the last CTA, and the inner PCG's scalar
+// logic (recursive residual, replacement and stop triggers, beta).
+__device__ __forceinline__ void xr_tail(double rr, double rz, MixState* st, double* part, int mode, double* sh) {
   double brr = bsum(rr, sh);
   double brz = bsum(rz, sh);
   if (threadIdx.x == 0) {
@@ -1260,23 +1490,112 @@ __global__ void __launch_bounds__(kT) k_xr32(int64_t n, float* __restrict__ x, f
   if (st->iter >= st->max_iter) st->status = MIX_MAXITER;
 }
 
-// Conversions between box-ordered FP64 DOF vectors and the padded FP32 layout walk node rows: row q = j + ny1 k
-// holds DOFs [3 nx1 q, 3 nx1 (q + 1)) in FP64 and floats [rp q, rp q + 3 nx1) in FP32. CTA b takes rows b,
-// b + gridDim.x, ...; its threads the DOFs of a row.
-// FP64 refinement: u += x32, x32 = 0
-__global__ void k_flush_u(GridDims g, double* __restrict__ u, float* __restrict__ x32) {
+// FP64 vectors of the fast FP64 form (padded layout, n even): the same step as k_xr32
+__global__ void __launch_bounds__(kT) k_xr64(int64_t n, double* __restrict__ x, double* __restrict__ r,
+                                             double* __restrict__ z, const double* __restrict__ p,
+                                             const double* __restrict__ ap, const double* __restrict__ invd,
+                                             MixState* st, double* part, int mode) {
+  __shared__ double sh[32];
+  if (mode == 0 && st->status != MIX_RUNNING) return;
+  const double alpha = mode ? 0.0 : st->alpha;
+  double rr = 0.0, rz = 0.0;
+  const int64_t n2 = n >> 1;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n2; i += stride) {
+    double2 rv = reinterpret_cast<const double2*>(r)[i];
+    const double2 iv = reinterpret_cast<const double2*>(invd)[i];
+    if (mode == 0) {
+      double2 xv = reinterpret_cast<const double2*>(x)[i];
+      const double2 pv = reinterpret_cast<const double2*>(p)[i];
+      const double2 av = reinterpret_cast<const double2*>(ap)[i];
+      xv.x = fma(alpha, pv.x, xv.x);
+      xv.y = fma(alpha, pv.y, xv.y);
+      rv.x = fma(-alpha, av.x, rv.x);
+      rv.y = fma(-alpha, av.y, rv.y);
+      reinterpret_cast<double2*>(x)[i] = xv;
+      reinterpret_cast<double2*>(r)[i] = rv;
+    }
+    const double2 zv = make_double2(rv.x * iv.x, rv.y * iv.y);
+    reinterpret_cast<double2*>(z)[i] = zv;
+    rr += rv.x * rv.x + rv.y * rv.y;
+    rz += rv.x * zv.x + rv.y * zv.y;
+  }
+  xr_tail(rr, rz, st, part, mode, sh);
+}
+
+// x += alpha p, r -= alpha Ap, z = r invD; partials of r.r and r.z (FP64). mode 0: CG step; 1: residual
+// replacement (z, rho from the new r; beta = rho_new / rho_old); 2: start (z, rho; next step starts p = z).
+__global__ void __launch_bounds__(kT) k_xr32(int64_t n, float* __restrict__ x, float* __restrict__ r,
+                                             float* __restrict__ z, const float* __restrict__ p,
+                                             const float* __restrict__ ap, const float* __restrict__ invd,
+                                             MixState* st, double* part, int mode) {
+  __shared__ double sh[32];
+  if (mode == 0 && st->status != MIX_RUNNING) return;
+  const float alpha = mode ? 0.f : (float)st->alpha;
+  double rr = 0.0, rz = 0.0;
+  const int64_t n4 = n >> 2;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n4; i += stride) {
+    float4 rv = reinterpret_cast<const float4*>(r)[i];
+    float4 iv = reinterpret_cast<const float4*>(invd)[i];
+    if (mode == 0) {
+      float4 xv = reinterpret_cast<const float4*>(x)[i];
+      float4 pv = reinterpret_cast<const float4*>(p)[i];
+      float4 av = reinterpret_cast<const float4*>(ap)[i];
+      xv.x = fmaf(alpha, pv.x, xv.x); xv.y = fmaf(alpha, pv.y, xv.y);
+      xv.z = fmaf(alpha, pv.z, xv.z); xv.w = fmaf(alpha, pv.w, xv.w);
+      rv.x = fmaf(-alpha, av.x, rv.x); rv.y = fmaf(-alpha, av.y, rv.y);
+      rv.z = fmaf(-alpha, av.z, rv.z); rv.w = fmaf(-alpha, av.w, rv.w);
+      reinterpret_cast<float4*>(x)[i] = xv;
+      reinterpret_cast<float4*>(r)[i] = rv;
+    }
+    float4 zv = make_float4(rv.x * iv.x, rv.y * iv.y, rv.z * iv.z, rv.w * iv.w);
+    reinterpret_cast<float4*>(z)[i] = zv;
+    rr += (double)rv.x * rv.x + (double)rv.y * rv.y + (double)rv.z * rv.z + (double)rv.w * rv.w;
+    rz += (double)rv.x * zv.x + (double)rv.y * zv.y + (double)rv.z * zv.z + (double)rv.w * zv.w;
+  }
+  if (blockIdx.x == 0) {  // tail (n not a multiple of 4)
+    for (int64_t i = 4 * n4 + threadIdx.x; i < n; i += blockDim.x) {
+      float rv = r[i];
+      if (mode == 0) {
+        x[i] = fmaf(alpha, p[i], x[i]);
+        rv = fmaf(-alpha, ap[i], rv);
+        r[i] = rv;
+      }
+      float zv = rv * invd[i];
+      z[i] = zv;
+      rr += (double)rv * rv;
+      rz += (double)rv * zv;
+    }
+  }
+  xr_tail(rr, rz, st, part, mode, sh);
+}
+
+// Conversions between box-ordered FP64 DOF vectors and the padded FP32 / FP64 layouts walk node rows: row
+// q = j + ny1 k holds DOFs [3 nx1 q, 3 nx1 (q + 1)) in the box layout and [pitch q, pitch q + 3 nx1) in the
+// padded one (pitch rp for float, rp64 for double). CTA b takes rows b, b + gridDim.x, ...; its threads the
+// DOFs of a row.
+template <class T>
+__device__ __forceinline__ int64_t pad_pitch(const GridDims& g) {
+  return sizeof(T) == 4 ? (int64_t)g.rp : (int64_t)g.rp64;
+}
+
+// refinement: u += x, x = 0
+template <class T>
+__global__ void k_flush_u(GridDims g, double* __restrict__ u, T* __restrict__ xw) {
   const int rl = 3 * g.nx1;
   for (int64_t q = blockIdx.x; q < (int64_t)g.ny1 * g.nz1; q += gridDim.x)
     for (int t = threadIdx.x; t < rl; t += blockDim.x) {
-      const int64_t f = (int64_t)g.rp * q + t;
-      u[(int64_t)rl * q + t] += (double)x32[f];
-      x32[f] = 0.f;
+      const int64_t f = pad_pitch<T>(g) * q + t;
+      u[(int64_t)rl * q + t] += (double)xw[f];
+      xw[f] = (T)0;
     }
 }
 
-// after A u: r64 = P(b - A u), r32 = (float) r64, CTA partials of r64^2
+// after A u: r64 = P(b - A u), r_work = (T) r64, CTA partials of r64^2
+template <class T>
 __global__ void k_resid64(GridDims g, const uint8_t* __restrict__ nf, const double* __restrict__ b,
-                          const double* __restrict__ au, float* __restrict__ r32, double* part) {
+                          const double* __restrict__ au, T* __restrict__ rw, double* part) {
   __shared__ double sh[32];
   double s = 0.0;
   const int rl = 3 * g.nx1;
@@ -1285,7 +1604,7 @@ __global__ void k_resid64(GridDims g, const uint8_t* __restrict__ nf, const doub
       const int64_t i = (int64_t)rl * q + t;
       const bool con = nf[i / 3] & (1 << (t % 3));
       const double v = con ? 0.0 : (b[i] - au[i]);
-      r32[(int64_t)g.rp * q + t] = (float)v;
+      rw[pad_pitch<T>(g) * q + t] = (T)v;
       s += v * v;
     }
   double bs = bsum(s, sh);
@@ -1298,15 +1617,17 @@ __global__ void k_sum_part(const double* part, int nb, double* out) {
   if (threadIdx.x == 0) *out = s;
 }
 
-__global__ void k_to_f32(GridDims g, const double* __restrict__ a, float* __restrict__ b) {
+template <class T>
+__global__ void k_to_pad(GridDims g, const double* __restrict__ a, T* __restrict__ b) {
   const int rl = 3 * g.nx1;
   for (int64_t q = blockIdx.x; q < (int64_t)g.ny1 * g.nz1; q += gridDim.x)
-    for (int t = threadIdx.x; t < rl; t += blockDim.x) b[(int64_t)g.rp * q + t] = (float)a[(int64_t)rl * q + t];
+    for (int t = threadIdx.x; t < rl; t += blockDim.x) b[pad_pitch<T>(g) * q + t] = (T)a[(int64_t)rl * q + t];
 }
-__global__ void k_to_f64(GridDims g, const float* __restrict__ a, double* __restrict__ b) {
+template <class T>
+__global__ void k_from_pad(GridDims g, const T* __restrict__ a, double* __restrict__ b) {
   const int rl = 3 * g.nx1;
   for (int64_t q = blockIdx.x; q < (int64_t)g.ny1 * g.nz1; q += gridDim.x)
-    for (int t = threadIdx.x; t < rl; t += blockDim.x) b[(int64_t)rl * q + t] = (double)a[(int64_t)g.rp * q + t];
+    for (int t = threadIdx.x; t < rl; t += blockDim.x) b[(int64_t)rl * q + t] = (double)a[pad_pitch<T>(g) * q + t];
 }
 
 // grid for the streaming kernels: fixed by n (deterministic reductions), at most 8 CTAs per SM
@@ -1343,7 +1664,7 @@ static int32_t ensure_mixed(mycel_problem* p) {
   if (e != cudaSuccess) return set_error(p->ctx, MYCEL_E_OOM, "out of device memory for the mixed-precision workspace");
   float* mapped[4] = {p->f_r, p->f_z, p->f_p0, p->f_p1};
   for (int q = 0; q < 4; ++q) {
-    int32_t st = encode_plane_map(p, mapped[q], &p->f_tmap[q]);
+    int32_t st = encode_plane_map(p, mapped[q], false, &p->f_tmap[q]);
     if (st) return st;
   }
   return MYCEL_OK;
@@ -1354,9 +1675,51 @@ int32_t mixed_apply_k_f64io(mycel_problem* p, const double* x, double* y, int pr
   int32_t st = ensure_mixed(p);
   if (st) return st;
   cudaStream_t s = p->ctx->stream;
-  k_to_f32<<<stream_blocks(p), kT, 0, s>>>(p->g, x, p->f_r);
+  k_to_pad<float><<<stream_blocks(p), kT, 0, s>>>(p->g, x, p->f_r);
   launch_mv32_variant<0>(p, s, p->f_r, nullptr, nullptr, nullptr, p->f_ap, projected, nullptr, nullptr);
-  k_to_f64<<<stream_blocks(p), kT, 0, s>>>(p->g, p->f_ap, y);
+  k_from_pad<float><<<stream_blocks(p), kT, 0, s>>>(p->g, p->f_ap, y);
+  p->ctx->launches += 3;
+  return MYCEL_OK;
+}
+
+// FP64 work vectors of the fast FP64 form (padded layout, pads zero), their TMA descriptors, and the FP64
+// matvec's shared memory above the 48 KB default (once per process, before any launch or capture)
+static int32_t ensure_f64f(mycel_problem* p) {
+  static std::once_flag smem_once;
+  static cudaError_t smem_err = cudaSuccess;
+  std::call_once(smem_once, [] {
+    cudaError_t a = cudaFuncSetAttribute(k_mv64f<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fac64_smem_bytes(0));
+    cudaError_t b = cudaFuncSetAttribute(k_mv64f<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fac64_smem_bytes(1));
+    smem_err = a != cudaSuccess ? a : b;
+  });
+  if (smem_err != cudaSuccess)
+    return set_error(p->ctx, MYCEL_E_DEVICE, std::string("FP64 matvec shared memory: ") + cudaGetErrorString(smem_err));
+  if (p->g_x) return MYCEL_OK;
+  const size_t fb = sizeof(double) * (size_t)p->g.n64 + 64;
+  cudaError_t e = cudaSuccess;
+  double** bufs[] = {&p->g_x, &p->g_r, &p->g_z, &p->g_p0, &p->g_p1, &p->g_ap, &p->g_invd};
+  for (double** b : bufs) {
+    if ((e = cudaMallocAsync((void**)b, fb, p->ctx->stream)) != cudaSuccess) break;
+    p->device_bytes += (int64_t)fb;
+    cudaMemsetAsync(*b, 0, fb, p->ctx->stream);
+  }
+  if (e != cudaSuccess) return set_error(p->ctx, MYCEL_E_OOM, "out of device memory for the fast FP64 workspace");
+  double* mapped[4] = {p->g_r, p->g_z, p->g_p0, p->g_p1};
+  for (int q = 0; q < 4; ++q) {
+    int32_t st = encode_plane_map(p, mapped[q], true, &p->g_tmap[q]);
+    if (st) return st;
+  }
+  return MYCEL_OK;
+}
+
+// y = K x (projected: ApplyA form) through the factorised FP64 operator; x, y box-ordered FP64 device vectors
+int32_t fast64_apply_k(mycel_problem* p, const double* x, double* y, int projected) {
+  int32_t st = ensure_f64f(p);
+  if (st) return st;
+  cudaStream_t s = p->ctx->stream;
+  k_to_pad<double><<<stream_blocks(p), kT, 0, s>>>(p->g, x, p->g_r);
+  launch_mv64f<0>(p, s, p->g_r, nullptr, nullptr, nullptr, p->g_ap, projected, nullptr, nullptr);
+  k_from_pad<double><<<stream_blocks(p), kT, 0, s>>>(p->g, p->g_ap, y);
   p->ctx->launches += 3;
   return MYCEL_OK;
 }
@@ -1375,63 +1738,101 @@ __global__ void k_mix_init(MixState* st, double target, int max_iter, double flu
 
 __global__ void k_mix_set(MixState* st, int status) { st->status = status; }
 
+// The refined inner PCG runs in one of two forms: FP32 work vectors and the FP32 matvec (mixed form), or FP64
+// work vectors and the factorised FP64 matvec (fast FP64 form). Both use the same device state machine.
+struct InnerForm {
+  bool f64;
+  void *x, *r, *z, *p0, *p1, *ap;
+  const void* invd;
+  int64_t n;        // padded length
+  size_t es;        // element size
+  cudaGraphExec_t* graph;
+  int* graph_profiled;
+  cudaEvent_t (*ev)[2];
+  int prof_slot;
+  double flush_factor;
+};
+
+static InnerForm inner_form(mycel_problem* p, bool f64) {
+  if (f64)
+    return {true, p->g_x, p->g_r, p->g_z, p->g_p0, p->g_p1, p->g_ap, p->g_invd, p->g.n64, sizeof(double),
+            p->pcg64f_graph, &p->pcg64f_graph_profiled, p->prof64f_ev, 2, 1e-4};
+  return {false, p->f_x, p->f_r, p->f_z, p->f_p0, p->f_p1, p->f_ap, p->d_invdf, p->g.n32, sizeof(float),
+          p->pcg32_graph, &p->pcg32_graph_profiled, p->prof_ev, 0, kFlushFactor};
+}
+
+static void launch_inner_mv(mycel_problem* p, const InnerForm& F, cudaStream_t s, void* pold, void* pcur) {
+  if (F.f64)
+    launch_mv64f<1>(p, s, nullptr, (const double*)F.z, (const double*)pold, (double*)pcur, (double*)F.ap, 1,
+                    mix_state(p), p->d_part2);
+  else
+    launch_mv32_variant<1>(p, s, nullptr, (const float*)F.z, (const float*)pold, (float*)pcur, (float*)F.ap, 1,
+                           mix_state(p), p->d_part2);
+}
+
+static void launch_inner_xr(mycel_problem* p, const InnerForm& F, cudaStream_t s, void* pcur, int mode) {
+  const int sb = stream_blocks(p);
+  if (F.f64)
+    k_xr64<<<sb, kT, 0, s>>>(F.n, (double*)F.x, (double*)F.r, (double*)F.z, (const double*)pcur, (const double*)F.ap,
+                             (const double*)F.invd, mix_state(p), p->d_part2, mode);
+  else
+    k_xr32<<<sb, kT, 0, s>>>(F.n, (float*)F.x, (float*)F.r, (float*)F.z, (const float*)pcur, (const float*)F.ap,
+                             (const float*)F.invd, mix_state(p), p->d_part2, mode);
+}
+
 // Chunk of inner iterations as a graph; p alternates between two buffers (even chunk length, each chunk starts
-// from the direction held in f_p1). When the context profiles, the first matvec of a chunk is launched directly
+// from the direction held in p1). When the context profiles, the first matvec of a chunk is launched directly
 // between two stream events (outside the graph) and the graph holds the rest of the chunk.
-static int32_t capture_mixed_graph(mycel_problem* p, int chunk) {
+static int32_t capture_inner_graph(mycel_problem* p, const InnerForm& F, int chunk) {
   mycel_ctx* c = p->ctx;
-  if (p->pcg32_graph[0] && p->pcg32_graph_profiled == c->profile) return MYCEL_OK;
+  if (F.graph[0] && *F.graph_profiled == c->profile) return MYCEL_OK;
   for (int k = 0; k < 2; ++k) {
-    if (p->pcg32_graph[k]) cudaGraphExecDestroy(p->pcg32_graph[k]);
-    p->pcg32_graph[k] = nullptr;
+    if (F.graph[k]) cudaGraphExecDestroy(F.graph[k]);
+    F.graph[k] = nullptr;
     for (int j = 0; j < 2; ++j)
-      if (!p->prof_ev[k][j]) cudaEventCreate(&p->prof_ev[k][j]);
+      if (!F.ev[k][j]) cudaEventCreate(&F.ev[k][j]);
   }
   cudaStream_t s = c->stream;
-  MixState* st = mix_state(p);
-  double* part = p->d_part2;
-  int sb = stream_blocks(p);
   int64_t before = c->launches;
   for (int k = 0; k < 2; ++k) {
     cudaGraph_t graph;
     MYCEL_CUDA(c, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     for (int t = 0; t < chunk; ++t) {
-      float* pcur = (t & 1) ? p->f_p1 : p->f_p0;
-      float* pprev = (t & 1) ? p->f_p0 : p->f_p1;
-      if (!(c->profile && t == 0))
-        launch_mv32_variant<1>(p, s, nullptr, p->f_z, pprev, pcur, p->f_ap, 1, st, part);
-      k_xr32<<<sb, kT, 0, s>>>(p->g.n32, p->f_x, p->f_r, p->f_z, pcur, p->f_ap, p->d_invdf, st, part, 0);
+      void* pcur = (t & 1) ? F.p1 : F.p0;
+      void* pprev = (t & 1) ? F.p0 : F.p1;
+      if (!(c->profile && t == 0)) launch_inner_mv(p, F, s, pprev, pcur);
+      launch_inner_xr(p, F, s, pcur, 0);
     }
     MYCEL_CUDA(c, cudaStreamEndCapture(s, &graph));
-    MYCEL_CUDA(c, cudaGraphInstantiate(&p->pcg32_graph[k], graph, 0));
+    MYCEL_CUDA(c, cudaGraphInstantiate(&F.graph[k], graph, 0));
     cudaGraphDestroy(graph);
   }
   c->launches = before;
-  p->pcg32_graph_chunk = chunk;
-  p->pcg32_graph_profiled = c->profile;
+  *F.graph_profiled = c->profile;
   return MYCEL_OK;
 }
 
-static void launch_chunk(mycel_problem* p, int gi) {
+static void launch_inner_chunk(mycel_problem* p, const InnerForm& F, int gi) {
   mycel_ctx* c = p->ctx;
   cudaStream_t s = c->stream;
-  if (p->pcg32_graph_profiled) {
-    cudaEventRecord(p->prof_ev[gi][0], s);
-    launch_mv32_variant<1>(p, s, nullptr, p->f_z, p->f_p1, p->f_p0, p->f_ap, 1, mix_state(p), p->d_part2);
-    cudaEventRecord(p->prof_ev[gi][1], s);
+  if (*F.graph_profiled) {
+    cudaEventRecord(F.ev[gi][0], s);
+    launch_inner_mv(p, F, s, F.p1, F.p0);
+    cudaEventRecord(F.ev[gi][1], s);
   }
-  cudaGraphLaunch(p->pcg32_graph[gi], s);
+  cudaGraphLaunch(F.graph[gi], s);
 }
 
-// r32 = P(b - A u) in FP64, returns ||r|| (synchronises)
-static int32_t true_residual(mycel_problem* p, const double* d_b, const double* d_u, double* rn) {
+// r_work = P(b - A u) in FP64 (then rounded to the form's type), returns ||r|| (synchronises)
+static int32_t true_residual(mycel_problem* p, const InnerForm& F, const double* d_b, const double* d_u, double* rn) {
   mycel_ctx* c = p->ctx;
   cudaStream_t s = c->stream;
   int sb = stream_blocks(p);
   double* part = p->d_part2;
   double* scal = p->d_part2 + p->n_part2 - 128;
   launch_matvec64(p, d_u, p->d_ap, 1, nullptr);
-  k_resid64<<<sb, kT, 0, s>>>(p->g, p->d_nflags, d_b, p->d_ap, p->f_r, part);
+  if (F.f64) k_resid64<double><<<sb, kT, 0, s>>>(p->g, p->d_nflags, d_b, p->d_ap, (double*)F.r, part);
+  else k_resid64<float><<<sb, kT, 0, s>>>(p->g, p->d_nflags, d_b, p->d_ap, (float*)F.r, part);
   k_sum_part<<<1, 32, 0, s>>>(part, sb, scal);
   c->launches += 2;
   double* h = (double*)((char*)c->pinned + 1024);
@@ -1441,9 +1842,134 @@ static int32_t true_residual(mycel_problem* p, const double* d_b, const double* 
   return MYCEL_OK;
 }
 
-// Mixed solve of A u = b (A = P K P + I - P) to ||P(b - A u)|| / ||P b|| <= tol, measured in FP64.
-int32_t mixed_solve_entry(mycel_problem* p, const double* d_b, const int32_t* d_nz, int32_t n_nz, double* d_u,
-                          double tol, int max_iter, const volatile int32_t* cancel, mycel_pcg_result* res) {
+struct LoopOut {
+  int iterations = 0, flushes = 0;
+  double rel = 0.0;
+  bool ok = false, stalled = false;
+};
+
+// Refined inner PCG from the current u: the device state machine runs chunks of iterations; whenever the
+// recursive residual has dropped by the form's flush factor (or reached the target) the correction is added
+// to u in FP64 and the true residual P(b - A u) replaces the recursive one (the direction is kept).
+// Convergence is decided on the true residual. watch_stall ends the loop when a cycle stalls (mixed form).
+static int32_t refined_loop(mycel_problem* p, const InnerForm& F, const double* d_b, double* d_u, double bnorm,
+                            double tol, int max_iter, const volatile int32_t* cancel, bool watch_stall, bool verbose,
+                            LoopOut* out) {
+  mycel_ctx* c = p->ctx;
+  cudaStream_t s = c->stream;
+  const int chunk = 16;
+  const char* name = F.f64 ? "fast FP64" : "mixed";
+  MixState* ms = mix_state(p);
+  int32_t st;
+  if (F.f64) {
+    k_to_pad<double><<<stream_blocks(p), kT, 0, s>>>(p->g, p->d_invd, p->g_invd);
+    c->launches++;
+  }
+  if ((st = capture_inner_graph(p, F, chunk))) return st;
+  double rn = 0.0;
+  if ((st = true_residual(p, F, d_b, d_u, &rn))) return st;
+  out->rel = rn / bnorm;
+  out->ok = out->rel <= tol;
+  if (out->ok) return MYCEL_OK;
+  MixState* slot[2] = {(MixState*)((char*)c->pinned + 2048), (MixState*)((char*)c->pinned + 3072)};
+  cudaEvent_t evs[2];
+  cudaEventCreateWithFlags(&evs[0], cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&evs[1], cudaEventDisableTiming);
+  struct EvGuard { cudaEvent_t* e; ~EvGuard() { cudaEventDestroy(e[0]); cudaEventDestroy(e[1]); } } evg{evs};
+  cudaMemsetAsync(F.x, 0, F.es * F.n, s);
+  k_mix_init<<<1, 1, 0, s>>>(ms, 0.5 * tol * bnorm, max_iter, F.flush_factor);
+  launch_inner_xr(p, F, s, F.p0, 2);
+  c->launches += 2;
+  int64_t launched = 0;
+  const int64_t cap = (int64_t)max_iter + 64 * chunk + 4096;
+  int iter_at_resume = 0;
+  // stall watch: a refinement cycle gains log10(1/flush factor) orders of the true residual; after two
+  // cycles, one that runs 4x longer than the average iterations per order so far (and at least 500
+  // iterations) has stalled (FP32 CG on a badly conditioned system)
+  const double rel_start = out->rel;
+  int64_t cycle_limit = INT64_MAX;
+  for (;;) {
+    // pipeline: chunk k is queued while the status after chunk k-1 is read
+    int64_t k = 0;
+    int status = MIX_RUNNING;
+    for (;; ++k) {
+      if (cancel && *cancel) {
+        cudaStreamSynchronize(s);
+        return set_error(c, MYCEL_E_CANCELLED, "The operation was canceled.");
+      }
+      if (launched > cap) {
+        cudaStreamSynchronize(s);
+        return set_error(c, MYCEL_E_TIMEOUT, "inner PCG device state did not reach a final status");
+      }
+      int gi = (int)(k & 1);
+      launch_inner_chunk(p, F, gi);
+      MYCEL_CUDA(c, cudaGetLastError());
+      launched += chunk;
+      c->launches += 2 * chunk;
+      MYCEL_CUDA(c, cudaMemcpyAsync(slot[gi], ms, sizeof(MixState), cudaMemcpyDeviceToHost, s));
+      MYCEL_CUDA(c, cudaEventRecord(evs[gi], s));
+      if (k == 0) continue;
+      int pi = (int)((k - 1) & 1);
+      MYCEL_CUDA(c, cudaEventSynchronize(evs[pi]));
+      status = slot[pi]->status;
+      if (status != MIX_RUNNING) break;
+      if (watch_stall && slot[pi]->iter - iter_at_resume > cycle_limit) {
+        out->stalled = true;
+        k_mix_set<<<1, 1, 0, s>>>(ms, MIX_FLUSH);  // the queued chunk and what follows skip their work
+        c->launches++;
+        break;
+      }
+      if (c->profile) {  // every iteration of chunk k-1 ran: its first matvec is a full launch
+        float ms_ = 0.f;
+        if (cudaEventElapsedTime(&ms_, F.ev[pi][0], F.ev[pi][1]) == cudaSuccess) {
+          c->prof_ms[F.prof_slot] += ms_;
+          c->prof_n[F.prof_slot] += 1;
+          c->prof_nodes[F.prof_slot] += p->g.nn;
+          c->prof_elems[F.prof_slot] += p->n_active;
+        }
+      }
+    }
+    MYCEL_CUDA(c, cudaStreamSynchronize(s));
+    MixState* h = slot[0];
+    MYCEL_CUDA(c, cudaMemcpyAsync(h, ms, sizeof(MixState), cudaMemcpyDeviceToHost, s));
+    MYCEL_CUDA(c, cudaStreamSynchronize(s));
+    out->iterations = h->iter;
+    status = h->status;
+    // the latest direction is in p{(m-1)&1} after m iterations since the chunks restarted
+    int m = out->iterations - iter_at_resume;
+    if (m > 0 && (m & 1)) MYCEL_CUDA(c, cudaMemcpyAsync(F.p1, F.p0, F.es * F.n, cudaMemcpyDeviceToDevice, s));
+    // reliable update: u += x; r = P(b - A u) in FP64
+    if (F.f64) k_flush_u<double><<<stream_blocks(p), kT, 0, s>>>(p->g, d_u, (double*)F.x);
+    else k_flush_u<float><<<stream_blocks(p), kT, 0, s>>>(p->g, d_u, (float*)F.x);
+    c->launches++;
+    ++out->flushes;
+    if ((st = true_residual(p, F, d_b, d_u, &rn))) return st;
+    out->rel = rn / bnorm;
+    if (verbose)
+      std::fprintf(stderr, "mycel: %s refinement %d: inner %d, status %d, recursive %.3e, true %.3e (tol %.1e)\n", name,
+                   out->flushes, out->iterations, status, h->rn / bnorm, out->rel, tol);
+    if (out->rel <= tol) {
+      out->ok = true;
+      break;
+    }
+    const double orders = std::log10(rel_start / out->rel);
+    if (out->flushes >= 2 && orders > 0.0)
+      cycle_limit = std::max<int64_t>(500, (int64_t)(4.0 * std::log10(1.0 / F.flush_factor) * out->iterations / orders));
+    if (out->stalled || status != MIX_FLUSH || out->iterations >= max_iter) break;
+    launch_inner_xr(p, F, s, F.p0, 1);
+    c->launches++;
+    iter_at_resume = out->iterations;
+  }
+  return MYCEL_OK;
+}
+
+// Refined solve of A u = b (A = P K P + I - P) to ||P(b - A u)|| / ||P b|| <= tol, measured in FP64.
+// MYCEL_PRECISION_MIXED: FP32 inner PCG; if it stalls, breaks down or runs out of iterations the solve goes on
+// in the fast FP64 form from the refined u, and finally (should that fail too) in the plain FP64 PCG.
+// MYCEL_PRECISION_FP64_FACTORED: the fast FP64 form, then the plain FP64 PCG if it does not converge.
+int32_t refined_solve_entry(mycel_problem* p, const double* d_b, const int32_t* d_nz, int32_t n_nz, double* d_u,
+                            double tol, int max_iter, const volatile int32_t* cancel, int precision,
+                            mycel_pcg_result* res) {
   mycel_ctx* c = p->ctx;
   cudaStream_t s = c->stream;
   auto t0 = std::chrono::steady_clock::now();
@@ -1455,11 +1981,8 @@ int32_t mixed_solve_entry(mycel_problem* p, const double* d_b, const int32_t* d_
                          "). At least 6 fixed DOFs are required to prevent rigid body modes in 3D.");
   int32_t st = ensure_pcg_workspace(p);
   if (st) return st;
-  if ((st = ensure_mixed(p))) return st;
-  const int64_t n = p->g.nd;
-  const int sb = stream_blocks(p);
-  double* part = p->d_part2;
-  MixState* ms = mix_state(p);
+  const bool mixed = precision == MYCEL_PRECISION_MIXED;
+  if (mixed && (st = ensure_mixed(p))) return st;
   double* saved_b = p->d_b;
   int32_t* saved_nz = p->d_bnz;
   int32_t saved_n = p->n_bnz;
@@ -1479,133 +2002,64 @@ int32_t mixed_solve_entry(mycel_problem* p, const double* d_b, const int32_t* d_
   MYCEL_CUDA(c, cudaStreamSynchronize(s));
   const double bnorm = hs->bnorm;
   if (bnorm <= 1e-30) {
-    MYCEL_CUDA(c, cudaMemsetAsync(d_u, 0, sizeof(double) * n, s));
+    MYCEL_CUDA(c, cudaMemsetAsync(d_u, 0, sizeof(double) * p->g.nd, s));
     MYCEL_CUDA(c, cudaStreamSynchronize(s));
     res->converged = 1;
     std::snprintf(res->message, sizeof res->message, "RHS is zero. Solution is zero.");
     return MYCEL_OK;
   }
-  const int chunk = 16;
   const bool verbose = std::getenv("MYCEL_VERBOSE") != nullptr;
   MYCEL_CUDA(c, cudaMemsetAsync(p->d_err, 0, sizeof(int), s));  // bounded-wait failures of this solve only
-  if ((st = resolve_mv32(p))) return st;
-  if ((st = capture_mixed_graph(p, chunk))) return st;
-  double rn = 0.0;
-  if ((st = true_residual(p, d_b, d_u, &rn))) return st;
-  double rel = rn / bnorm;
-  int flushes = 0;
-  bool ok = rel <= tol;
-  if (ok) std::snprintf(res->message, sizeof res->message, "Initial guess already converged.");
-  MixState* slot[2] = {(MixState*)((char*)c->pinned + 2048), (MixState*)((char*)c->pinned + 3072)};
-  cudaEvent_t evs[2];
-  cudaEventCreateWithFlags(&evs[0], cudaEventDisableTiming);
-  cudaEventCreateWithFlags(&evs[1], cudaEventDisableTiming);
-  struct EvGuard { cudaEvent_t* e; ~EvGuard() { cudaEventDestroy(e[0]); cudaEventDestroy(e[1]); } } evg{evs};
-  int total_iter = 0;
-  bool stalled = false;
-  if (!ok) {
-    cudaMemsetAsync(p->f_x, 0, sizeof(float) * p->g.n32, s);
-    k_mix_init<<<1, 1, 0, s>>>(ms, 0.5 * tol * bnorm, max_iter, kFlushFactor);
-    k_xr32<<<sb, kT, 0, s>>>(p->g.n32, p->f_x, p->f_r, p->f_z, p->f_p0, p->f_ap, p->d_invdf, ms, part, 2);
-    c->launches += 2;
-    int64_t launched = 0;
-    const int64_t cap = (int64_t)max_iter + 64 * chunk + 4096;
-    int iter_at_resume = 0;
-    // stall watch: a refinement cycle gains log10(1/kFlushFactor) orders of the true residual; after two
-    // cycles, one that runs 4x longer than the average iterations per order so far (and at least 500
-    // iterations) has stalled (FP32 CG on a badly conditioned system)
-    const double rel_start = rel;
-    int64_t cycle_limit = INT64_MAX;
-    for (;;) {
-      // pipeline: chunk k is queued while the status after chunk k-1 is read
-      int64_t k = 0;
-      int status = MIX_RUNNING;
-      for (;; ++k) {
-        if (cancel && *cancel) {
-          cudaStreamSynchronize(s);
-          return set_error(c, MYCEL_E_CANCELLED, "The operation was canceled.");
-        }
-        if (launched > cap) {
-          cudaStreamSynchronize(s);
-          return set_error(c, MYCEL_E_TIMEOUT, "inner PCG device state did not reach a final status");
-        }
-        int gi = (int)(k & 1);
-        launch_chunk(p, gi);
-        MYCEL_CUDA(c, cudaGetLastError());
-        launched += chunk;
-        c->launches += 2 * chunk;
-        MYCEL_CUDA(c, cudaMemcpyAsync(slot[gi], ms, sizeof(MixState), cudaMemcpyDeviceToHost, s));
-        MYCEL_CUDA(c, cudaEventRecord(evs[gi], s));
-        if (k == 0) continue;
-        int pi = (int)((k - 1) & 1);
-        MYCEL_CUDA(c, cudaEventSynchronize(evs[pi]));
-        status = slot[pi]->status;
-        if (status != MIX_RUNNING) break;
-        if (slot[pi]->iter - iter_at_resume > cycle_limit) {
-          stalled = true;
-          k_mix_set<<<1, 1, 0, s>>>(ms, MIX_FLUSH);  // the queued chunk and what follows skip their work
-          c->launches++;
-          break;
-        }
-        if (c->profile) {  // every iteration of chunk k-1 ran: its first matvec is a full launch
-          float ms_ = 0.f;
-          if (cudaEventElapsedTime(&ms_, p->prof_ev[pi][0], p->prof_ev[pi][1]) == cudaSuccess) {
-            c->prof_ms[0] += ms_;
-            c->prof_n[0] += 1;
-            c->prof_nodes[0] += p->g.nn;
-            c->prof_elems[0] += p->n_active;
-          }
-        }
-      }
-      MYCEL_CUDA(c, cudaStreamSynchronize(s));
-      MixState* h = slot[0];
-      MYCEL_CUDA(c, cudaMemcpyAsync(h, ms, sizeof(MixState), cudaMemcpyDeviceToHost, s));
-      MYCEL_CUDA(c, cudaStreamSynchronize(s));
-      total_iter = h->iter;
-      status = h->status;
-      // the latest direction is in f_p{(m-1)&1} after m iterations since the chunks restarted
-      int m = total_iter - iter_at_resume;
-      if (m > 0 && (m & 1))
-        MYCEL_CUDA(c, cudaMemcpyAsync(p->f_p1, p->f_p0, sizeof(float) * p->g.n32, cudaMemcpyDeviceToDevice, s));
-      // reliable update: u += x32; r = P(b - A u) in FP64
-      k_flush_u<<<sb, kT, 0, s>>>(p->g, d_u, p->f_x);
-      c->launches++;
-      ++flushes;
-      if ((st = true_residual(p, d_b, d_u, &rn))) return st;
-      rel = rn / bnorm;
-      if (verbose)
-        std::fprintf(stderr, "mycel: mixed refinement %d: inner %d, status %d, recursive %.3e, true %.3e (tol %.1e)\n",
-                     flushes, total_iter, status, h->rn / bnorm, rel, tol);
-      if (rel <= tol) {
-        ok = true;
-        break;
-      }
-      const double orders = std::log10(rel_start / rel);
-      if (flushes >= 2 && orders > 0.0)
-        cycle_limit = std::max<int64_t>(500, (int64_t)(4.0 * std::log10(1.0 / kFlushFactor) * total_iter / orders));
-      if (stalled || status != MIX_FLUSH || total_iter >= max_iter) break;
-      k_xr32<<<sb, kT, 0, s>>>(p->g.n32, p->f_x, p->f_r, p->f_z, p->f_p0, p->f_ap, p->d_invdf, ms, part, 1);
-      c->launches++;
-      iter_at_resume = total_iter;
-    }
+  LoopOut l32, l64;
+  bool ok = false;
+  double rel = 0.0;
+  // once a mixed solve of a problem has stalled (its designs have become badly conditioned, which in a SIMP
+  // run does not go away), its later mixed solves start in the fast FP64 form
+  const bool run32 = mixed && !p->mixed_prefers_f64f;
+  if (run32) {
+    if ((st = resolve_mv32(p))) return st;
+    if ((st = refined_loop(p, inner_form(p, false), d_b, d_u, bnorm, tol, max_iter, cancel, true, verbose, &l32)))
+      return st;
+    ok = l32.ok;
+    rel = l32.rel;
+    if (!ok) p->mixed_prefers_f64f = true;
+    if (ok && l32.iterations == 0 && l32.flushes == 0)
+      std::snprintf(res->message, sizeof res->message, "Initial guess already converged.");
   }
-  // FP32 inner iteration stalled, broke down or ran out of iterations: finish with the plain FP64 PCG,
-  // warm-started from the refined solution (on the device, like everything else)
-  int fb_iter = 0;
+  int remaining = std::max(1, max_iter - l32.iterations);
+  if (!ok) {
+    if ((st = ensure_f64f(p))) return st;
+    MYCEL_CUDA(c, cudaMemsetAsync(p->d_err, 0, sizeof(int), s));
+    if ((st = refined_loop(p, inner_form(p, true), d_b, d_u, bnorm, tol, run32 ? std::max(remaining, max_iter / 2)
+                                                                             : max_iter,
+                           cancel, false, verbose, &l64)))
+      return st;
+    ok = l64.ok;
+    rel = l64.rel;
+    if (verbose && run32)
+      std::fprintf(stderr, "mycel: mixed solve went on in fast FP64 (%s after %d inner iterations): %d iterations, %.3e\n",
+                   l32.stalled ? "stalled" : "not converged", l32.iterations, l64.iterations, rel);
+    if (!run32 && ok && l64.iterations == 0 && l64.flushes == 0)
+      std::snprintf(res->message, sizeof res->message, "Initial guess already converged.");
+  }
+  int plain_iter = 0;
   if (!ok) {
     mycel_pcg_result r64;
     if ((st = pcg_solve_fp64(p, d_b, d_nz, n_nz, d_u, tol, max_iter, cancel, &r64))) return st;
-    fb_iter = r64.iterations;
+    plain_iter = r64.iterations;
     ok = r64.converged != 0;
     rel = r64.final_residual;
-    if (verbose)
-      std::fprintf(stderr, "mycel: mixed solve finished in FP64 (%s after %d inner iterations): %d iterations, %.3e\n",
-                   stalled ? "stalled" : "not converged", total_iter, fb_iter, rel);
+    if (verbose) std::fprintf(stderr, "mycel: solve finished by the plain FP64 PCG: %d iterations, %.3e\n", plain_iter, rel);
   }
-  res->iterations = total_iter + fb_iter;
-  res->inner_iterations = total_iter;
-  res->refinement_steps = flushes;
-  res->fallback_iterations = fb_iter;
+  if (mixed) {
+    res->inner_iterations = l32.iterations;
+    res->fallback_iterations = l64.iterations + plain_iter;
+  } else {
+    res->inner_iterations = l64.iterations;
+    res->fallback_iterations = plain_iter;
+  }
+  res->iterations = res->inner_iterations + res->fallback_iterations;
+  res->refinement_steps = l32.flushes + l64.flushes;
   res->final_residual = rel;
   res->converged = ok ? 1 : 0;
   if (!ok)
@@ -1613,6 +2067,11 @@ int32_t mixed_solve_entry(mycel_problem* p, const double* d_b, const int32_t* d_
                   "PCG reached maximum iterations without converging. Is the model not sufficiently constrained?");
   res->elapsed_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   return MYCEL_OK;
+}
+
+int32_t mixed_solve_entry(mycel_problem* p, const double* d_b, const int32_t* d_nz, int32_t n_nz, double* d_u,
+                          double tol, int max_iter, const volatile int32_t* cancel, mycel_pcg_result* res) {
+  return refined_solve_entry(p, d_b, d_nz, n_nz, d_u, tol, max_iter, cancel, MYCEL_PRECISION_MIXED, res);
 }
 
 }  // namespace mycel

@@ -123,17 +123,27 @@ void split_ke_tf32(const double* ke, KeTf* out) {
 // C^T o = e, C^T e = 0. So K is diagonal per component (eigenvalues below) plus one coupling per pair of
 // components between basis functions whose parities on the two axes are swapped. Coefficients of an
 // element vector in that basis are its 8-point Walsh-Hadamard transform / 8; the h / 8 is folded in here.
-void build_hexop(double h, double nu, HexOpF* out) {
+void build_hexop64(double h, double nu, HexOpD* out) {
   const double lam = nu / ((1.0 + nu) * (1.0 - 2.0 * nu)), mu = 1.0 / (2.0 * (1.0 + nu));
   const double l2m = lam + 2.0 * mu, sc = h / 8.0;
   const double dcl[2][3] = {{0.0, mu / 2.0, mu / 3.0},
                             {l2m / 2.0, l2m / 6.0 + mu / 6.0, l2m / 18.0 + mu / 9.0}};
   for (int a = 0; a < 2; ++a)
-    for (int n = 0; n < 3; ++n) out->dcl[a][n] = (float)(dcl[a][n] * sc);
-  out->lam[0] = (float)(lam / 2.0 * sc);
-  out->lam[1] = (float)(lam / 6.0 * sc);
-  out->mu[0] = (float)(mu / 2.0 * sc);
-  out->mu[1] = (float)(mu / 6.0 * sc);
+    for (int n = 0; n < 3; ++n) out->dcl[a][n] = dcl[a][n] * sc;
+  out->lam[0] = lam / 2.0 * sc;
+  out->lam[1] = lam / 6.0 * sc;
+  out->mu[0] = mu / 2.0 * sc;
+  out->mu[1] = mu / 6.0 * sc;
+}
+
+void build_hexop(double h, double nu, HexOpF* out) {
+  HexOpD d;
+  build_hexop64(h, nu, &d);
+  for (int a = 0; a < 2; ++a) {
+    for (int n = 0; n < 3; ++n) out->dcl[a][n] = (float)d.dcl[a][n];
+    out->lam[a] = (float)d.lam[a];
+    out->mu[a] = (float)d.mu[a];
+  }
 }
 
 }  // namespace mycel

@@ -20,6 +20,9 @@ struct GridDims {
   // contiguously from a 16-byte aligned start, row pitch rp floats (multiple of 4); pads stay zero.
   int rp;
   int64_t n32;       // rp * ny1 * nz1
+  // FP64 work vectors of the fast FP64 form: the same layout with row pitch rp64 doubles (multiple of 2)
+  int rp64;
+  int64_t n64;       // rp64 * ny1 * nz1
 };
 
 inline GridDims make_dims(int nx, int ny, int nz) {
@@ -31,6 +34,8 @@ inline GridDims make_dims(int nx, int ny, int nz) {
   g.nd = 3 * g.nn;
   g.rp = (3 * g.nx1 + 3) & ~3;
   g.n32 = (int64_t)g.rp * g.ny1 * g.nz1;
+  g.rp64 = (3 * g.nx1 + 1) & ~1;
+  g.n64 = (int64_t)g.rp64 * g.ny1 * g.nz1;
   return g;
 }
 
@@ -49,6 +54,7 @@ struct KeTf { float hi[32 * 24]; float lo[32 * 24]; };
 // odd (1) and with n odd factors on the other two axes; lam[pk], mu[pk]: coupling constants lambda m(pk),
 // mu m(pk) of two different components, pk the parity on the third axis.
 struct HexOpF { float dcl[2][3]; float lam[2]; float mu[2]; };
+struct HexOpD { double dcl[2][3]; double lam[2]; double mu[2]; };  // the same constants in FP64
 
 // Node flag bits (one byte per node): bits 0-2 = DOF c constrained, bit 3 = node active.
 enum : uint8_t { NF_CX = 1, NF_CY = 2, NF_CZ = 4, NF_ACTIVE = 8 };
@@ -114,8 +120,10 @@ struct mycel_problem {
   mycel::KeF kef{};
   mycel::KeTf ketf{};
   mycel::HexOpF hexop{};
+  mycel::HexOpD hexop64{};
   int mv32 = -1;                  // FP32 matvec variant in use: -1 not chosen yet, else MYCEL_MV32_* (1..3)
   int tune_mv32 = 0;              // requested variant: 0 autotune, else MYCEL_MV32_*
+  bool mixed_prefers_f64f = false; // a mixed solve of this problem stalled: later ones start in fast FP64
   int* d_err = nullptr;           // device error word (bounded waits that gave up)
   double diag_ke[24];
   int64_t n_active = 0, n_active_nodes = 0, n_active_fixed = 0;
@@ -150,6 +158,13 @@ struct mycel_problem {
   // mixed-form workspace
   float *f_x = nullptr, *f_r = nullptr, *f_z = nullptr, *f_p0 = nullptr, *f_p1 = nullptr, *f_ap = nullptr;
   CUtensorMap f_tmap[4];          // TMA descriptors of f_r, f_z, f_p0, f_p1 (node-plane boxes of the FP32 matvec)
+  // fast FP64 form (factorised operator, FP64 recurrences): padded FP64 work vectors, TMA maps, graphs
+  double *g_x = nullptr, *g_r = nullptr, *g_z = nullptr, *g_p0 = nullptr, *g_p1 = nullptr, *g_ap = nullptr,
+         *g_invd = nullptr;
+  CUtensorMap g_tmap[4];          // g_r, g_z, g_p0, g_p1
+  cudaGraphExec_t pcg64f_graph[2] = {nullptr, nullptr};
+  int pcg64f_graph_profiled = 0;
+  cudaEvent_t prof64f_ev[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
   double* d_r64 = nullptr;        // refinement residual
   double* d_part2 = nullptr;      // [many] FP64 partials for mixed dots
   int64_t n_part2 = 0;
@@ -193,6 +208,7 @@ int32_t set_error(mycel_ctx* ctx, int32_t code, const std::string& msg);
 void build_ke(double h, double nu, double* ke);  // Hex8Element.CreateKe semantics
 void split_ke_tf32(const double* ke, KeTf* out);   // hi = tf32(KE), lo = tf32(KE - hi), rows padded to 32
 void build_hexop(double h, double nu, HexOpF* out);  // factorised form of KE(h, nu), FP32
+void build_hexop64(double h, double nu, HexOpD* out);  // the same in FP64
 int64_t num_blocks8192(int64_t n);
 
 // ---- FP64 plain-path launchers (fp64_kernels.cu, compiled with -fmad=false) ----
@@ -245,6 +261,10 @@ int32_t mixed_apply_k_f64io(mycel_problem* p, const double* x, double* y, int pr
 bool simp_session_converged(const mycel_simp_session* s);  // the SIMP stop rule fired
 int32_t mixed_solve_entry(mycel_problem* p, const double* d_b, const int32_t* d_nz, int32_t n_nz, double* d_u,
                           double tol, int max_iter, const volatile int32_t* cancel, mycel_pcg_result* res);
+int32_t refined_solve_entry(mycel_problem* p, const double* d_b, const int32_t* d_nz, int32_t n_nz, double* d_u,
+                            double tol, int max_iter, const volatile int32_t* cancel, int precision,
+                            mycel_pcg_result* res);
+int32_t fast64_apply_k(mycel_problem* p, const double* x, double* y, int projected);
 
 // ---- drivers (api.cu) ----
 int32_t pcg_solve_fp64(mycel_problem* p, const double* d_b, const int32_t* d_nz, int32_t n_nz, double* d_x,

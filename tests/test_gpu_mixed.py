@@ -98,3 +98,40 @@ def test_mixed_solve_finishes_in_fp64_when_inner_iterations_run_out(oracle, ctx)
     assert r.fallback_iterations > 0 and r.iterations == r.inner_iterations + r.fallback_iterations
     assert r.converged and r.final_residual <= 1e-8
     assert np.abs(u - ref).max() <= 1e-5 * np.abs(ref).max()
+
+
+# ---- fast FP64 form (factorised operator, FP64 recurrences) ----
+# Tolerances (stated): the factorised FP64 operator equals the Gauss KE product up to FP64 rounding, within
+# 1e-12 of max|K x|; a solve to relative residual 1e-10 agrees with the FP64 oracle in u to 1e-7 of max|u| and
+# needs no more than 1.2x the oracle's iterations (+10); SIMP compliance within 1e-7 per iteration.
+
+@pytest.mark.parametrize("shape", [(1, 1, 1), (5, 3, 2), (33, 17, 9), (70, 9, 20)])
+def test_fp64_factored_matvec_matches_oracle(oracle, ctx, shape):
+    m = carved_model(*shape, seed=3, frac=0.15) if shape[0] > 2 else tiny_test_model(*shape)
+    om, pr = oracle.Model(m), api.Problem(m, ctx)
+    x = np.random.default_rng(2).uniform(-1, 1, m.total_dofs)
+    y64 = om.apply_k(x)
+    assert np.abs(pr.apply_k(x, precision="fp64f") - y64).max() <= 1e-12 * np.abs(y64).max()
+    xp = x * (om.constrained() == 0)
+    assert np.abs(pr.apply_k(xp, True, "fp64f") - om.apply_a(xp)).max() <= 1e-12 * np.abs(y64).max()
+
+
+def test_fp64_factored_solve_matches_oracle(oracle, ctx):
+    m = carved_model(31, 12, 9, seed=8, emin_ratio=1e-9)
+    om, pr = oracle.Model(m), api.Problem(m, ctx)
+    b = om.forces() * (om.constrained() == 0)
+    ref, rref = om.pcg_solve(b, tol=1e-10, max_iter=20000)
+    u, r = pr.pcg_solve(b, tol=1e-10, max_iterations=20000, precision="fp64f")
+    assert r.converged and r.final_residual <= 1e-10 and r.fallback_iterations == 0
+    assert r.iterations <= 1.2 * rref.iterations + 10
+    assert np.abs(u - ref).max() <= 1e-7 * np.abs(ref).max()
+
+
+def test_fp64_factored_simp_cantilever(oracle, ctx):
+    m, o = W.simp_cantilever_40x20x10()
+    o = o.replace(max_iterations=8)
+    ref = oracle.topopt_run(m, o)
+    res = api.TopologyOptimizer.run(m, o.replace(precision="fp64f"), ctx=ctx)
+    assert res.total_iterations == ref.n_iters
+    for a, b in zip(res.snapshots, ref.records):
+        assert abs(a.compliance - b["compliance"]) <= 1e-7 * abs(b["compliance"])
