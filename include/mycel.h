@@ -79,7 +79,8 @@ typedef struct {
   int32_t inner_iterations; /* mixed form: FP32 PCG iterations summed over refinement steps */
   char message[256];
   /* mixed form: iterations of the FP64 PCG that finished a solve whose FP32 inner iteration stalled (a
-     refinement cycle 4x slower than the average so far), broke down or ran out of iterations: the solve goes
+     refinement cycle longer than 3x all earlier cycles together and than 2000 iterations), broke down or ran
+     out of iterations: the solve goes
      on in the fast FP64 form (MYCEL_PRECISION_FP64_FACTORED) from the refined u, then, should that fail too,
      in the plain FP64 PCG. After a stall, later mixed solves of the same problem start in the fast FP64 form
      (inner_iterations 0). For MYCEL_PRECISION_FP64_FACTORED: the plain FP64 PCG's iterations.

@@ -1883,10 +1883,9 @@ static int32_t refined_loop(mycel_problem* p, const InnerForm& F, const double* 
   int64_t launched = 0;
   const int64_t cap = (int64_t)max_iter + 64 * chunk + 4096;
   int iter_at_resume = 0;
-  // stall watch: a refinement cycle gains log10(1/flush factor) orders of the true residual; after two
-  // cycles, one that runs 4x longer than the average iterations per order so far (and at least 500
-  // iterations) has stalled (FP32 CG on a badly conditioned system)
-  const double rel_start = out->rel;
+  // stall watch: each refinement cycle gains log10(1/flush factor) orders of the true residual. CG's later
+  // orders cost more than its first ones, so a cycle counts as stalled (FP32 CG on a badly conditioned system)
+  // only once it has run longer than 3x all earlier cycles together, and at least 2000 iterations.
   int64_t cycle_limit = INT64_MAX;
   for (;;) {
     // pipeline: chunk k is queued while the status after chunk k-1 is read
@@ -1952,9 +1951,7 @@ static int32_t refined_loop(mycel_problem* p, const InnerForm& F, const double* 
       out->ok = true;
       break;
     }
-    const double orders = std::log10(rel_start / out->rel);
-    if (out->flushes >= 2 && orders > 0.0)
-      cycle_limit = std::max<int64_t>(500, (int64_t)(4.0 * std::log10(1.0 / F.flush_factor) * out->iterations / orders));
+    cycle_limit = std::max<int64_t>(2000, 3 * (int64_t)out->iterations);
     if (out->stalled || status != MIX_FLUSH || out->iterations >= max_iter) break;
     launch_inner_xr(p, F, s, F.p0, 1);
     c->launches++;
