@@ -174,14 +174,16 @@ def matvec_bytes_fp32(model):
     return 48 * nn + 5 * ne + nn
 
 
-def serve_stream(jobs, precision, slots, budget_bytes, tol, rate_scale=1.0):
+def serve_stream(jobs, precision, slots, budget_bytes, tol, rate_scale=1.0, device=0, ws=1):
     """Submit the jobs at their arrival times to a server and wait for all; returns the stats, per-job
     compliance histories and the wall time. Arrival times are the stream's (seconds from the first)."""
     from mycel_b200 import api
     from mycel_b200 import workloads as W
     specs = [W.served_job(nx, ny, nz, it, seed, precision=precision, tol=tol) for (_t, nx, ny, nz, it, seed) in jobs]
     hist = []
-    with api.Server(slots=slots, hbm_budget_bytes=int(budget_bytes)) as srv:
+    lat = []
+    with api.Server(slots=slots, hbm_budget_bytes=int(budget_bytes), device=device) as srv:
+        barrier(ws)
         t0 = time.perf_counter()
         ids = []
         for (arr, *_rest), (m, o) in zip(jobs, specs):
@@ -193,15 +195,19 @@ def serve_stream(jobs, precision, slots, budget_bytes, tol, rate_scale=1.0):
         wall = time.perf_counter() - t0
         st = srv.stats()
         for jid in ids:
-            r = srv.result(jid) if srv.info(jid)["state"] == "done" else None
+            info = srv.info(jid)
+            r = srv.result(jid) if info["state"] == "done" else None
             hist.append([h.compliance for h in r["history"]] if r else None)
+            if r:
+                lat.append(info["finish_s"] - info["submit_s"])
     elems = sum(nx * ny * nz for (_t, nx, ny, nz, _i, _s) in jobs)
     span = st["last_finish_s"] - st["first_submit_s"]
     return {"jobs": len(jobs), "completed": st["completed"], "failed": st["failed"],
             "simp_iterations": st["simp_iterations"], "simp_iter_s": st["simp_iterations"] / span if span > 0 else None,
             "p50_latency_s": st["p50_latency_s"], "p99_latency_s": st["p99_latency_s"],
             "mean_latency_s": st["mean_latency_s"], "p50_queue_s": st["p50_queue_s"], "p99_queue_s": st["p99_queue_s"],
-            "peak_admitted_gb": st["peak_admitted_bytes"] / 1e9, "elements_total": elems, "wall_s": wall}, hist
+            "peak_admitted_gb": st["peak_admitted_bytes"] / 1e9, "elements_total": elems, "wall_s": wall,
+            "_latencies": lat}, hist
 
 
 def compare_histories(h_mixed, h_fp64):
@@ -229,6 +235,7 @@ def serving_report(args, n_jobs, max_elems, rate, slots, budget_gb, precisions, 
     for prec in precisions:
         sel = jobs if (prec != "fp64" or fp64_jobs is None) else jobs[:fp64_jobs]
         out[prec], hists[prec] = serve_stream(sel, prec, slots, budget_gb * 1e9, args.job_tol)
+        out[prec].pop("_latencies", None)
     if "fp64f" in hists and "fp64" in hists:
         out["rel_compliance_err_fp64f_vs_fp64"] = compare_histories(hists["fp64f"], hists["fp64"])
         if out["fp64"]["simp_iter_s"]:
@@ -243,11 +250,36 @@ def serving_report(args, n_jobs, max_elems, rate, slots, budget_gb, precisions, 
 
 
 def run_serve(args):
+    """The served stream on this node's GPUs: one process per GPU (torchrun), rank r serves jobs r, r+N, ...
+    on its own GPU; the per-job results are merged once at the end (no collective while jobs run)."""
+    from mycel_b200 import replicas
+    from mycel_b200 import workloads as W
+    ws, rank, local = dist_init()
     precisions = [p for p in args.serve_precisions.split(",") if p]
-    out = {"metric": "served SIMP job stream: p50/p99 job latency and aggregate SIMP iter/s",
-           **serving_report(args, args.serve_jobs, args.serve_max_elems, args.serve_rate, args.serve_slots,
-                            args.serve_budget_gb, precisions, args.serve_fp64_jobs)}
-    print(json.dumps(out), flush=True)
+    jobs = W.job_stream(n_jobs=args.serve_jobs, rate=args.serve_rate, seed=11, max_elems=args.serve_max_elems)
+    if ws == 1:
+        out = {"metric": "served SIMP job stream: p50/p99 job latency and aggregate SIMP iter/s",
+               **serving_report(args, args.serve_jobs, args.serve_max_elems, args.serve_rate, args.serve_slots,
+                                args.serve_budget_gb, precisions, args.serve_fp64_jobs)}
+        for prec in precisions:
+            out.get(prec, {}).pop("_latencies", None)
+        print(json.dumps(out), flush=True)
+        return
+    mine = replicas.partition(jobs, rank, ws)
+    out = {"metric": "served SIMP job stream: p50/p99 job latency and aggregate SIMP iter/s", "n_gpus": ws,
+           "scaling": "strong", "stream": {"jobs": args.serve_jobs, "rate_jobs_s": args.serve_rate,
+                                           "pcg_tol": args.job_tol, "slots_per_gpu": args.serve_slots}}
+    for prec in precisions:
+        r, _h = serve_stream(mine, prec, args.serve_slots, args.serve_budget_gb * 1e9, args.job_tol, device=local,
+                             ws=ws)
+        out[prec] = replicas.merge({"latencies": r["_latencies"], "simp_iterations": r["simp_iterations"],
+                                    "first_submit_s": 0.0, "last_finish_s": r["wall_s"]})
+    if "mixed" in out and "fp64" in out and out["fp64"]["simp_iter_s"]:
+        out["speedup_mixed_vs_fp64"] = out["mixed"]["simp_iter_s"] / out["fp64"]["simp_iter_s"]
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    import torch.distributed as dist
+    dist.destroy_process_group()
 
 
 def run_batched(args):
