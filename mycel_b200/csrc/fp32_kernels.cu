@@ -2019,7 +2019,7 @@ int32_t refined_solve_entry(mycel_problem* p, const double* d_b, const int32_t* 
       return st;
     ok = l32.ok;
     rel = l32.rel;
-    if (!ok) p->mixed_prefers_f64f = true;
+    if (l32.stalled) p->mixed_prefers_f64f = true;
     if (ok && l32.iterations == 0 && l32.flushes == 0)
       std::snprintf(res->message, sizeof res->message, "Initial guess already converged.");
   }
