@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--probe-variant", type=int, default=0,
                     help="FP32 matvec variant for --probe mixed (0 autotune, 1 dense, 2 tensor, 3 factored)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving sample of the default run")
+    ap.add_argument("--mv32-variant", type=int, default=0,
+                    help="FP32 matvec variant of the timed mixed run (0 autotune; for profiler runs)")
     ap.add_argument("--serve-sample-jobs", type=int, default=12)
     ap.add_argument("--serve-sample-max-elems", type=int, default=250_000)
     ap.add_argument("--serve", action="store_true",
@@ -319,6 +321,8 @@ def run_mycel(args):
 
     # ---------------- value: device-resident SIMP iterations ----------------
     prob = api.Problem(model, ctx)
+    if args.mv32_variant:
+        prob.set_matvec32(args.mv32_variant)
     sess = api.SimpSession(prob, mixed)
     for _ in range(args.warmup):
         sess.step()

@@ -245,6 +245,19 @@ int32_t mycel_simp_read(mycel_simp_session* s, double* u_out, float* physical_de
                         double* rho_phys_active_out, double* rho_design_active_out, double* lambda_out);
 int32_t mycel_simp_end(mycel_simp_session* s);
 
+/* RunWriter snapshot frames (Persistence/RunWriter.cs:132-160 WriteSnapshotAsync, :199-245 the it_NNNNNN
+   frame, :344-356 ComputeQuantizedChecksum) of the last completed iteration, without stalling the loop:
+   frame_begin quantises the physical density to one byte per box element on the device
+   (round(clamp(rho, 0, 1) * 255f), half away from zero) and starts its copy to pinned host memory; it returns a
+   slot (two alternate, so one frame can be in flight while the next iteration runs). frame_end waits for that
+   copy and returns the bytes (box-sized), the 72-byte little-endian header and the FNV-1a checksum of the
+   bytes (computed on the host: FNV-1a is sequential). The stream checksum of RunWriter is then
+   rolling = (rolling ^ checksum) * 16777619, starting from 2166136261. Brotli compression and file writing
+   stay with the host. Any output may be NULL. */
+int32_t mycel_simp_frame_begin(mycel_simp_session* s, int32_t* slot_out);
+int32_t mycel_simp_frame_end(mycel_simp_session* s, int32_t slot, uint8_t* frame_out, uint8_t* header_out,
+                             uint32_t* checksum_out);
+
 /* ---- serving: continuous batching of SIMP jobs on one GPU ----
    No counterpart in the reference, whose App runs one optimisation at a time (OptimizationCoordinator.cs:229
    through the FemWorkTeam lock, FemWorkTeam.cs:109). A server runs `slots` jobs at once, each on its own CUDA

@@ -125,6 +125,8 @@ SIGNATURES = {
     "mycel_simp_step": (i32, [P, C.POINTER(IterRecord), C.POINTER(i32)]),
     "mycel_simp_read": (i32, [P, P, P, P, P, P, C.POINTER(dbl)]),
     "mycel_simp_end": (i32, [P]),
+    "mycel_simp_frame_begin": (i32, [P, C.POINTER(i32)]),
+    "mycel_simp_frame_end": (i32, [P, i32, P, P, C.POINTER(C.c_uint32)]),
     "mycel_server_create": (i32, [C.POINTER(ServerOptions), C.POINTER(P)]),
     "mycel_server_submit": (i32, [P, C.POINTER(JobSpec), C.POINTER(i64)]),
     "mycel_server_job_info": (i32, [P, i64, C.POINTER(JobInfo)]),

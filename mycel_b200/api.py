@@ -431,6 +431,22 @@ class SimpSession:
                                         C.byref(lam)), self.problem.ctx)
         return dict(u=uu, physical=ph, design=de, rho_phys_active=rpa, rho_design_active=rda, lam=lam.value)
 
+    def frame_begin(self) -> int:
+        """Start the RunWriter frame of the last iteration (quantised on the device, copied without waiting)."""
+        slot = C.c_int32(-1)
+        _check(L.load().mycel_simp_frame_begin(self.handle, C.byref(slot)), self.problem.ctx)
+        return slot.value
+
+    def frame_end(self, slot: int):
+        """(frame bytes [box], 72-byte header, FNV-1a checksum) of a frame started by frame_begin."""
+        m = self.problem.model
+        fr = np.zeros(m.total_elements, dtype=np.uint8)
+        hd = np.zeros(72, dtype=np.uint8)
+        ck = C.c_uint32(0)
+        _check(L.load().mycel_simp_frame_end(self.handle, slot, fr.ctypes.data, hd.ctypes.data, C.byref(ck)),
+               self.problem.ctx)
+        return fr, bytes(hd), ck.value
+
     def close(self):
         if getattr(self, "handle", None):
             if getattr(self.problem, "handle", None):  # a destroyed problem has ended its sessions already

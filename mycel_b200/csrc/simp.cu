@@ -36,6 +36,14 @@ struct mycel_simp_session {
   int count = 0;
   cudaEvent_t ev[5] = {};
   std::vector<float> h_phys, h_des;
+  mycel_iter_record last{};        // record of the last completed iteration (frame headers)
+  // RunWriter frames: two device byte frames and pinned host copies, filled without waiting
+  uint8_t* d_frame[2] = {nullptr, nullptr};
+  uint8_t* h_frame[2] = {nullptr, nullptr};
+  cudaEvent_t frame_ev[2] = {nullptr, nullptr};
+  mycel_iter_record frame_rec[2] = {};
+  bool frame_busy[2] = {false, false};
+  int frame_next = 0;
 };
 
 namespace {
@@ -65,6 +73,15 @@ __global__ void k_heaviside_chain(int64_t na, const int32_t* __restrict__ act, c
   double d = beta * (1.0 - th * th) * inv;
   d = d > 1e-12 ? d : 1e-12;
   dct[e] = dcb[e] * d;
+}
+
+// RunWriter's 8-bit quantisation (Persistence/RunWriter.cs:211-217): round(clamp(v, 0, 1) * 255f), half away
+// from zero, in FP32
+__global__ void k_quantize(int64_t ne, const float* __restrict__ v, uint8_t* __restrict__ q) {
+  int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= ne) return;
+  const float c = fminf(fmaxf(v[e], 0.0f), 1.0f);
+  q[e] = (uint8_t)roundf(__fmul_rn(c, 255.0f));
 }
 
 __global__ void k_snapshot(int64_t ne, const uint8_t* __restrict__ dom, const double* __restrict__ rb,
@@ -321,6 +338,7 @@ static int32_t simp_step_impl(mycel_simp_session* s, mycel_iter_record* rec, int
   r.update_ms = ms;
   r.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   if (rec) *rec = r;
+  s->last = r;
   s->count++;
   // stop rule (:374-390)
   s->chist.push_back(r.compliance);
@@ -379,6 +397,79 @@ extern "C" int32_t mycel_simp_read(mycel_simp_session* s, double* u, float* phys
   return MYCEL_OK;
 }
 
+// ---- RunWriter frames (Persistence/RunWriter.cs:132-160, 199-245, 344-356) ----
+extern "C" int32_t mycel_simp_frame_begin(mycel_simp_session* s, int32_t* slot_out) {
+  if (!s || !slot_out) return set_error(s ? s->p->ctx : nullptr, MYCEL_E_ARG, "NULL argument");
+  mycel_problem* p = s->p;
+  mycel_ctx* c = p->ctx;
+  cudaSetDevice(c->device);
+  if (s->count == 0) return set_error(c, MYCEL_E_INVALID_OPERATION, "no iteration has been run yet");
+  const int slot = s->frame_next;
+  if (s->frame_busy[slot])
+    return set_error(c, MYCEL_E_INVALID_OPERATION, "both frame slots are pending: end one first");
+  const int64_t ne = p->g.ne;
+  if (!s->d_frame[slot]) {
+    MYCEL_CUDA(c, cudaMallocAsync((void**)&s->d_frame[slot], (size_t)ne, c->stream));
+    MYCEL_CUDA(c, cudaMallocHost((void**)&s->h_frame[slot], (size_t)ne));
+    MYCEL_CUDA(c, cudaEventCreateWithFlags(&s->frame_ev[slot], cudaEventDisableTiming));
+  }
+  snapshot(s);
+  k_quantize<<<(unsigned)((ne + 255) / 256), 256, 0, c->stream>>>(ne, s->d_phys_f, s->d_frame[slot]);
+  c->launches++;
+  MYCEL_CUDA(c, cudaMemcpyAsync(s->h_frame[slot], s->d_frame[slot], (size_t)ne, cudaMemcpyDeviceToHost, c->stream));
+  MYCEL_CUDA(c, cudaEventRecord(s->frame_ev[slot], c->stream));
+  s->frame_rec[slot] = s->last;
+  s->frame_busy[slot] = true;
+  s->frame_next = slot ^ 1;
+  *slot_out = slot;
+  return MYCEL_OK;
+}
+
+extern "C" int32_t mycel_simp_frame_end(mycel_simp_session* s, int32_t slot, uint8_t* frame_out, uint8_t* header_out,
+                                        uint32_t* checksum_out) {
+  if (!s) return set_error(nullptr, MYCEL_E_ARG, "NULL session");
+  mycel_problem* p = s->p;
+  mycel_ctx* c = p->ctx;
+  if (slot < 0 || slot > 1 || !s->frame_busy[slot])
+    return set_error(c, MYCEL_E_ARG, "frame slot is not pending");
+  cudaSetDevice(c->device);
+  MYCEL_CUDA(c, cudaEventSynchronize(s->frame_ev[slot]));
+  s->frame_busy[slot] = false;
+  const int64_t ne = p->g.ne;
+  const uint8_t* q = s->h_frame[slot];
+  // ComputeQuantizedChecksum (:344-356): FNV-1a over the bytes in order (sequential by definition)
+  uint32_t h = 2166136261u;
+  for (int64_t i = 0; i < ne; ++i) h = (h ^ q[i]) * 16777619u;
+  if (frame_out) std::memcpy(frame_out, q, (size_t)ne);
+  if (checksum_out) *checksum_out = h;
+  if (header_out) {
+    // WriteIterationFileAtomic header (:223-235): little-endian fields at fixed offsets
+    const mycel_iter_record& r = s->frame_rec[slot];
+    uint8_t hd[72] = {};
+    auto put32 = [&](int o, uint32_t v) { for (int b = 0; b < 4; ++b) hd[o + b] = (uint8_t)(v >> (8 * b)); };
+    auto putd = [&](int o, double v) {
+      uint64_t u;
+      std::memcpy(&u, &v, 8);
+      for (int b = 0; b < 8; ++b) hd[o + b] = (uint8_t)(u >> (8 * b));
+    };
+    hd[0] = 'T'; hd[1] = 'O'; hd[2] = 'P'; hd[3] = 'O';
+    put32(4, 1u);
+    put32(8, (uint32_t)p->g.nx);
+    put32(12, (uint32_t)p->g.ny);
+    put32(16, (uint32_t)p->g.nz);
+    put32(20, (uint32_t)r.iteration);
+    putd(24, r.compliance);
+    putd(32, r.volume_fraction);
+    putd(40, r.max_change);
+    putd(48, r.grey_level);
+    put32(56, (uint32_t)r.solver_iterations);
+    putd(60, r.total_ms);
+    put32(68, h);
+    std::memcpy(header_out, hd, 72);
+  }
+  return MYCEL_OK;
+}
+
 extern "C" int32_t mycel_simp_end(mycel_simp_session* s) {
   if (!s) return MYCEL_OK;
   auto& live = s->p->sessions;
@@ -400,6 +491,11 @@ extern "C" int32_t mycel_simp_end(mycel_simp_session* s) {
   if (s->d_des_f) cudaFreeAsync(s->d_des_f, st);
   for (auto& e : s->ev)
     if (e) cudaEventDestroy(e);
+  for (int k = 0; k < 2; ++k) {
+    if (s->d_frame[k]) cudaFreeAsync(s->d_frame[k], st);
+    if (s->h_frame[k]) cudaFreeHost(s->h_frame[k]);
+    if (s->frame_ev[k]) cudaEventDestroy(s->frame_ev[k]);
+  }
   delete s;
   return MYCEL_OK;
 }

@@ -1258,3 +1258,20 @@ extern "C" int orc_get_threads(void) {
   return 1;
 #endif
 }
+
+// ---------------------------------------------------------------------------------------------------------
+// RunWriter.ComputeQuantizedChecksum (src/Mycel.Core/Persistence/RunWriter.cs:344-356) and the quantisation of
+// WriteIterationFileAtomic (:211-217): q = (byte)MathF.Round(Math.Clamp(v, 0, 1) * 255f, AwayFromZero); FNV-1a
+// 32-bit over the bytes in order (offset basis 2166136261, prime 16777619). Writes q when out is non-NULL.
+extern "C" uint32_t orc_quantized_checksum(const float* v, int64_t n, uint8_t* out) {
+  uint32_t h = 2166136261u;
+  for (int64_t i = 0; i < n; ++i) {
+    float c = v[i] < 0.0f ? 0.0f : (v[i] > 1.0f ? 1.0f : v[i]);
+    float x = c * 255.0f;
+    uint8_t q = (uint8_t)std::round(x);  // std::round: half away from zero, like MidpointRounding.AwayFromZero
+    if (out) out[i] = q;
+    h ^= q;
+    h *= 16777619u;
+  }
+  return h;
+}

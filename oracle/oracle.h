@@ -34,6 +34,9 @@ void orc_set_lane_mode(int mode);
 void orc_set_pow_mode(int mode);
 void orc_set_threads(int n);
 int orc_get_threads(void);
+/* RunWriter.ComputeQuantizedChecksum and the 8-bit frame quantisation (Persistence/RunWriter.cs:211-217,
+   344-356); out (n bytes) may be NULL. */
+uint32_t orc_quantized_checksum(const float* v, int64_t n, uint8_t* out);
 
 /* Hex8Element.CreateKe(h, nu) -> ke[576] row-major. */
 int orc_create_ke(double h, double nu, double* ke);

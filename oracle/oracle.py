@@ -69,6 +69,8 @@ class IterRec(C.Structure):
 
 
 def _setup(L):
+    L.orc_quantized_checksum.restype = C.c_uint32
+    L.orc_quantized_checksum.argtypes = [np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS"), C.c_int64, P]
     L.orc_create_ke.argtypes = [C.c_double, C.c_double, dp]
     L.orc_model_create.restype = P
     L.orc_model_create.argtypes = [C.c_int, C.c_int, C.c_int, C.c_float, bp, C.c_double, C.c_double, C.c_double, ip,
@@ -308,6 +310,14 @@ def oc_update(rho, dc, s, passive, f, move=0.2, rho_min=1e-3, lambda_guess=1.0, 
                               None if pas is None else pas.ctypes.data, out, rho.size, f, move, rho_min, lambda_guess,
                               max_bisect, vol_tol)
     return out, lam
+
+
+def quantized_frame(v):
+    """RunWriter's 8-bit frame of a float density array and its FNV-1a checksum: (bytes, checksum)."""
+    v = np.ascontiguousarray(v, dtype=np.float32)
+    out = np.zeros(v.size, dtype=np.uint8)
+    ck = lib().orc_quantized_checksum(v, v.size, out.ctypes.data)
+    return out, int(ck)
 
 
 def passive_region(grid, nodes, radius=2):

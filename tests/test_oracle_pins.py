@@ -299,3 +299,32 @@ def test_passive_region_build(oracle):
     assert out.sum() == 8
     out = oracle.passive_region(g, [g.node_index(0, 0, 0)], radius=1)
     assert out.sum() == 1 and out[0] == 1
+
+
+# ---- RunWriter frames: FNV-1a 32-bit (published test vectors) and the 8-bit quantisation ----
+def _frame_of_bytes(bs):
+    # densities that quantise to the given byte values (v = b / 255 rounds back to b)
+    return np.array([b / 255.0 for b in bs], dtype=np.float32)
+
+
+def test_quantized_checksum_fnv1a_known_answers():
+    from oracle import oracle as O
+    assert O.quantized_frame(np.zeros(0, dtype=np.float32))[1] == 0x811C9DC5
+    q, ck = O.quantized_frame(_frame_of_bytes(b"a"))
+    assert list(q) == [97] and ck == 0xE40C292C
+    q, ck = O.quantized_frame(_frame_of_bytes(b"foobar"))
+    assert bytes(q) == b"foobar" and ck == 0xBF9CF968
+
+
+def test_quantization_rounds_half_away_and_clamps():
+    from oracle import oracle as O
+    v = np.array([-0.5, 0.0, 1.0, 2.0, np.float32(0.5) / np.float32(255.0), 1.5 / 255.0, 0.5, 0.25],
+                 dtype=np.float32)
+    q, _ = O.quantized_frame(v)
+    assert q[6] == 128  # 0.5 * 255 = 127.5 exactly: half away from zero
+    expect = [0, 0, 255, 255]
+    for x in v[4:]:
+        c = np.float32(min(max(float(x), 0.0), 1.0)) * np.float32(255.0)
+        f = np.floor(np.float64(c))
+        expect.append(int(f + 1 if np.float64(c) - f >= 0.5 else f))
+    assert list(q) == expect
