@@ -68,7 +68,7 @@ def test_admission_respects_budget_and_rejects_oversize():
                 srv.result(big)
 
 
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed", "fp64f"])
 def test_admission_estimate_bounds_job_memory(ctx, precision):
     m, o = W.served_job(30, 14, 10, 2, seed=5, precision=precision)
     est = api.Server.device_bytes(m, o)
@@ -78,7 +78,10 @@ def test_admission_estimate_bounds_job_memory(ctx, precision):
     held = pr.info()["device_bytes"]
     sess.close()
     pr.close()
-    assert held <= est <= 1.25 * held
+    # the estimate also holds the fast FP64 workspace that a mixed solve allocates only if it escalates
+    g = m.grid
+    fast64 = 7 * (8 * ((3 * (g.nx + 1) + 1) // 2 * 2) * (g.ny + 1) * (g.nz + 1) + 64) if precision == "mixed" else 0
+    assert held <= est <= 1.25 * held + fast64
 
 
 def test_unknown_job_is_an_argument_error():
