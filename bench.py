@@ -34,6 +34,11 @@ sys.path.insert(0, ROOT)
 # the FP64 path reproduces the reference's iteration counts bit for bit). Used only to scale the CPU sample.
 FP64_PCG_PER_SIMP_ITER = None
 
+# DRAM bytes per launch of the dominant kernel, from one ncu capture (dram__bytes_read.sum +
+# dram__bytes_write.sum; `--probe mixed --probe-grid 192x96x96 --probe-variant 3`): 53.47 MB read, 5.53 MB
+# written (K p and p_t mostly stay in the 126 MB L2 during the launch). Keyed by (matvec variant, workload).
+NCU_DRAM_BYTES = {(3, "bridge_192x96x96"): 53.47e6 + 5.53e6}
+
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -46,7 +51,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-sample-iters", type=int, default=6)
-    ap.add_argument("--probe", choices=["mixed", "fp64"], default=None,
+    ap.add_argument("--probe", choices=["mixed", "fp64", "fp64f"], default=None,
                     help="kernel probe for profilers: one PCG solve of --probe-iters iterations on a bridge grid")
     ap.add_argument("--probe-grid", default="96x48x48")
     ap.add_argument("--probe-iters", type=int, default=40)
@@ -66,6 +71,9 @@ def parse():
     ap.add_argument("--serve-budget-gb", type=float, default=150.0)
     ap.add_argument("--serve-precisions", default="mixed,fp64")
     ap.add_argument("--serve-fp64-jobs", type=int, default=None, help="prefix of the stream run in FP64 (default all)")
+    ap.add_argument("--static", action="store_true",
+                    help="static solve of the sphere-carved 96x48x24 box (about 98k active elements) to 1e-8: plain "
+                         "FP64, mixed and fast FP64 paths, and the CPU oracle")
     ap.add_argument("--batched", action="store_true", help="48 independent problems submitted at once")
     ap.add_argument("--batched-count", type=int, default=48)
     ap.add_argument("--batched-iters", type=int, default=4)
@@ -284,6 +292,57 @@ def run_serve(args):
     dist.destroy_process_group()
 
 
+def run_static(args):
+    """Static solve to relative residual 1e-8 on the sphere-carved 96x48x24 box: PCG solve time (median of three
+    solves from u = 0 on a prepared problem, CUDA events), iterations and the stiffness matvec time per path,
+    u and compliance against the plain FP64 result; the CPU oracle (all host threads) on the same solve."""
+    import torch
+    from mycel_b200 import api
+    from mycel_b200 import workloads as W
+    model = W.sphere_carved_box()
+    ctx = api.Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", 0))
+    out = {"metric": "static solve to 1e-8 (sphere-carved 96x48x24 box)", "active_elements": model.active_element_count,
+           "dofs": model.total_dofs}
+    ref = None
+    for prec, slot in (("fp64", 1), ("mixed", 0), ("fp64f", 2)):
+        pr = api.Problem(model, ctx)
+        b = pr.forces()
+        pr.pcg_solve(b, tol=1e-8, max_iterations=20000, precision=prec)  # set-up, autotune, graph capture
+        times = []
+        for rep in range(3):
+            ctx.set_profiling(rep == 2)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            u, r = pr.pcg_solve(b, tol=1e-8, max_iterations=20000, precision=prec)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+        tm = ctx.kernel_timing(slot)
+        ctx.set_profiling(False)
+        comp = float(np.dot(b, u))
+        entry = {"solve_ms": statistics.median(times), "pcg_iterations": r.iterations,
+                 "fallback_iterations": r.fallback_iterations, "final_residual": r.final_residual,
+                 "matvec_us": 1000.0 * tm["total_ms"] / tm["launches"] if tm["launches"] else None,
+                 "compliance": comp}
+        if ref is None:
+            ref = (u, comp)
+        else:
+            entry["rel_compliance_err_vs_fp64"] = abs(comp - ref[1]) / abs(ref[1])
+            entry["rel_u_err_vs_fp64"] = float(np.abs(u - ref[0]).max() / np.abs(ref[0]).max())
+        out[prec] = entry
+        pr.close()
+    if not args.no_cpu:
+        from oracle import oracle as O
+        O.set_modes(0, 0, threads=os.cpu_count() or 1)
+        t0 = time.perf_counter()
+        cres = O.static_run(model, 1e-8, 20000)
+        out["cpu_baseline"] = {"solve_ms": (time.perf_counter() - t0) * 1000.0, "cores": os.cpu_count() or 1,
+                               "kind": "port", "pcg_iterations": cres.solver_info.iterations,
+                               "note": "oracle StaticAnalysis.Run (set-up, solve, post-processing)"}
+    print(json.dumps(out), flush=True)
+
+
 def run_batched(args):
     """Batched instances: all problems submitted at once; aggregate SIMP iter/s, mixed vs FP64."""
     from mycel_b200 import api
@@ -359,9 +418,12 @@ def run_mycel(args):
     hbm = (pk or {}).get("hbm_gbs") or 6650.0
     kname = {1: "k_mv32 (dense KE rows, FMA pipe)", 2: "k_mv32tc (dense KE, tcgen05 3xTF32)",
              3: "k_mv32f (factorised Hex8 operator, TMA-fed)"}.get(mv_variant, "FP32 matvec")
+    traffic = NCU_DRAM_BYTES.get((mv_variant, args.workload))
     roof = {"kernel": kname + ": FP32 Hex8 K.p with fused p update + p.Ap partials", "bound": "hbm",
             "achieved": achieved, "peak": hbm, "unit": "GB/s",
-            "frac": (achieved / hbm) if achieved else None, "traffic": None,
+            "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one MODE-1 launch of this kernel on "
+                              "this workload (192x96x96)" if traffic else None,
             "peak_source": "measured" if pk else "fallback", "avg_launch_us": per_launch_ms * 1000.0,
             "timed_launches": timing["launches"], "algorithmic_bytes_per_launch": mv_bytes,
             "flops_per_launch": 1152 * model.active_element_count, "flops_note": "dense-KE equivalent",
@@ -568,6 +630,8 @@ if __name__ == "__main__":
         run_serve(a)
     elif a.batched and a.impl != "reference":
         run_batched(a)
+    elif a.static and a.impl != "reference":
+        run_static(a)
     elif a.impl == "reference":
         run_reference(a)
     else:

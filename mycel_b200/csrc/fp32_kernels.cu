@@ -795,7 +795,7 @@ constexpr size_t fac64_smem_bytes(int mode) {
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(FX * FY, 1) k_mv64f(GridDims g, const __grid_constant__ HexOpD op,
+__global__ void __launch_bounds__(FX * FY, 2) k_mv64f(GridDims g, const __grid_constant__ HexOpD op,
                                                       const __grid_constant__ CUtensorMap tm_a,
                                                       const __grid_constant__ CUtensorMap tm_b,
                                                       double* __restrict__ pnew, double* __restrict__ y,
