@@ -34,7 +34,11 @@ extern "C" {
 #define MYCEL_E_INVALID_OPERATION 9 /* InvalidOperationException (FeModel.AssembleForces: empty patch with force) */
 
 #define MYCEL_PRECISION_FP64 0  /* plain method: FP64 throughout, reproduces the reference's arithmetic */
-#define MYCEL_PRECISION_MIXED 1 /* FP32 inner PCG (K·u, Jacobi) inside FP64 iterative refinement */
+/* FP32 inner PCG (K·u, Jacobi) inside FP64 iterative refinement. Per problem, a mixed solve may instead run
+   the fast FP64 form below: after an FP32 stall, or when the problem's solves have shown the FP32 form needing
+   more than 1.5x the fast FP64 form's iterations per decade of residual (second solve probes it, every 16th
+   solve re-probes; decided on iteration counts, so deterministic). */
+#define MYCEL_PRECISION_MIXED 1
 /* FP64 throughout with the factorised cube-element operator (same tolerance test on the exact FP64 residual,
    not bit-exact with the reference's colour-ordered product); also what a stalled mixed solve goes on in */
 #define MYCEL_PRECISION_FP64_FACTORED 2

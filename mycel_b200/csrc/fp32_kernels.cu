@@ -1844,7 +1844,7 @@ static int32_t true_residual(mycel_problem* p, const InnerForm& F, const double*
 
 struct LoopOut {
   int iterations = 0, flushes = 0;
-  double rel = 0.0;
+  double rel = 0.0, rel0 = 0.0;  // relative true residual at the end and at the start of the loop
   bool ok = false, stalled = false;
 };
 
@@ -1868,7 +1868,7 @@ static int32_t refined_loop(mycel_problem* p, const InnerForm& F, const double* 
   if ((st = capture_inner_graph(p, F, chunk))) return st;
   double rn = 0.0;
   if ((st = true_residual(p, F, d_b, d_u, &rn))) return st;
-  out->rel = rn / bnorm;
+  out->rel = out->rel0 = rn / bnorm;
   out->ok = out->rel <= tol;
   if (out->ok) return MYCEL_OK;
   MixState* slot[2] = {(MixState*)((char*)c->pinned + 2048), (MixState*)((char*)c->pinned + 3072)};
@@ -2010,9 +2010,21 @@ int32_t refined_solve_entry(mycel_problem* p, const double* d_b, const int32_t* 
   LoopOut l32, l64;
   bool ok = false;
   double rel = 0.0;
-  // once a mixed solve of a problem has stalled (its designs have become badly conditioned, which in a SIMP
-  // run does not go away), its later mixed solves start in the fast FP64 form
-  const bool run32 = mixed && !p->mixed_prefers_f64f;
+  // Which inner form a mixed solve starts in. Once a mixed solve of a problem has stalled (its designs have
+  // become badly conditioned, which in a SIMP run does not go away), its later mixed solves start in the fast
+  // FP64 form. Otherwise the FP32 form runs unless the last solves showed it needing more than kCost64 times the
+  // fast FP64 form's iterations per decade of residual (kCost64: the cost of a fast FP64 iteration relative to
+  // an FP32 one); the second solve of a problem probes the fast FP64 form, and every 16th solve re-probes the
+  // form not in use. The choice rests on iteration counts only, so it is the same whatever else runs.
+  constexpr double kCost64 = 1.5;
+  bool use32 = true;
+  if (mixed && !p->mixed_prefers_f64f) {
+    const int n = p->mix_solves++;
+    if (p->it32_per_dec > 0.0 && p->it64_per_dec > 0.0) use32 = p->it32_per_dec <= kCost64 * p->it64_per_dec;
+    if (n == 1) use32 = false;
+    else if (n >= 16 && n % 16 == 0) use32 = !use32;
+  }
+  const bool run32 = mixed && !p->mixed_prefers_f64f && use32;
   if (run32) {
     if ((st = resolve_mv32(p))) return st;
     if ((st = refined_loop(p, inner_form(p, false), d_b, d_u, bnorm, tol, max_iter, cancel, true, verbose, &l32)))
@@ -2020,6 +2032,8 @@ int32_t refined_solve_entry(mycel_problem* p, const double* d_b, const int32_t* 
     ok = l32.ok;
     rel = l32.rel;
     if (l32.stalled) p->mixed_prefers_f64f = true;
+    if (ok && l32.iterations > 0 && l32.rel0 > l32.rel)
+      p->it32_per_dec = l32.iterations / std::max(0.1, std::log10(l32.rel0 / l32.rel));
     if (ok && l32.iterations == 0 && l32.flushes == 0)
       std::snprintf(res->message, sizeof res->message, "Initial guess already converged.");
   }
@@ -2033,6 +2047,8 @@ int32_t refined_solve_entry(mycel_problem* p, const double* d_b, const int32_t* 
       return st;
     ok = l64.ok;
     rel = l64.rel;
+    if (mixed && !run32 && ok && l64.iterations > 0 && l64.rel0 > l64.rel)
+      p->it64_per_dec = l64.iterations / std::max(0.1, std::log10(l64.rel0 / l64.rel));
     if (verbose && run32)
       std::fprintf(stderr, "mycel: mixed solve went on in fast FP64 (%s after %d inner iterations): %d iterations, %.3e\n",
                    l32.stalled ? "stalled" : "not converged", l32.iterations, l64.iterations, rel);

@@ -124,6 +124,10 @@ struct mycel_problem {
   int mv32 = -1;                  // FP32 matvec variant in use: -1 not chosen yet, else MYCEL_MV32_* (1..3)
   int tune_mv32 = 0;              // requested variant: 0 autotune, else MYCEL_MV32_*
   bool mixed_prefers_f64f = false; // a mixed solve of this problem stalled: later ones start in fast FP64
+  // mixed form's choice between its FP32 and fast FP64 inner forms: solves so far and the latest iterations
+  // per decade of residual reduction of each (deterministic: counts, not timings)
+  int mix_solves = 0;
+  double it32_per_dec = -1.0, it64_per_dec = -1.0;
   int* d_err = nullptr;           // device error word (bounded waits that gave up)
   double diag_ke[24];
   int64_t n_active = 0, n_active_nodes = 0, n_active_fixed = 0;

@@ -93,7 +93,8 @@ def test_mixed_solve_finishes_in_fp64_when_inner_iterations_run_out(oracle, ctx)
     _u0, r0 = pr.pcg_solve(b, tol=1e-8, max_iterations=20000, precision="mixed")
     assert r0.converged and r0.fallback_iterations == 0
     budget = int(r0.inner_iterations * 0.75)
-    u, r = pr.pcg_solve(b, tol=1e-8, max_iterations=budget, precision="mixed")
+    pr2 = api.Problem(m, ctx)  # a fresh problem: its first mixed solve runs the FP32 form
+    u, r = pr2.pcg_solve(b, tol=1e-8, max_iterations=budget, precision="mixed")
     assert r.inner_iterations <= budget
     assert r.fallback_iterations > 0 and r.iterations == r.inner_iterations + r.fallback_iterations
     assert r.converged and r.final_residual <= 1e-8
@@ -160,3 +161,22 @@ def test_runwriter_frames_match_oracle(oracle, ctx):
     assert rolling != 2166136261
     sess.close()
     pr.close()
+
+
+def test_mixed_form_choice_is_per_problem_and_deterministic(oracle, ctx):
+    """Second mixed solve of a problem probes the fast FP64 form; the choice after that rests on iteration
+    counts, so two identical problems make the same choices and give the same bits."""
+    m = carved_model(31, 12, 9, seed=8, emin_ratio=1e-9)
+    runs = []
+    for _ in range(2):
+        pr = api.Problem(m, ctx)
+        b = pr.forces()
+        out = []
+        for k in range(4):
+            u, r = pr.pcg_solve(b, tol=1e-8, max_iterations=20000, precision="mixed")
+            out.append((r.inner_iterations, r.fallback_iterations, u))
+        runs.append(out)
+        pr.close()
+    assert runs[0][1][0] == 0 and runs[0][1][1] > 0  # the probe ran in fast FP64
+    for a, b in zip(runs[0], runs[1]):
+        assert a[0] == b[0] and a[1] == b[1] and np.array_equal(a[2], b[2])
