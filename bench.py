@@ -305,7 +305,7 @@ def run_static(args):
     out = {"metric": "static solve to 1e-8 (sphere-carved 96x48x24 box)", "active_elements": model.active_element_count,
            "dofs": model.total_dofs}
     ref = None
-    for prec, slot in (("fp64", 1), ("mixed", 0), ("fp64f", 2)):
+    for prec, slot in (("fp64", 1), ("mixed", 0), ("fp64f", 2), ("mg", 2)):
         pr = api.Problem(model, ctx)
         b = pr.forces()
         pr.pcg_solve(b, tol=1e-8, max_iterations=20000, precision=prec)  # set-up, autotune, graph capture
@@ -476,28 +476,32 @@ def run_mycel(args):
                        "matvec_gbs": (48 * model.total_nodes + 9 * model.total_elements) / (per64 / 1000.0) / 1e9 if tm64["launches"] else None,
                        "mixed_vs_fp64_rel_compliance_err": errs, "max_rel_compliance_err": max(errs) if errs else None}
         out["speedup_mixed_vs_fp64"] = (value / ws) / out["fp64"]["simp_iter_s"] if out["fp64"]["simp_iter_s"] else None
-        # fast FP64 form (factorised FP64 operator, FP64 recurrences) on the same iterations
-        prob = api.Problem(model, ctx)
-        sess = api.SimpSession(prob, opts.replace(precision="fp64f"))
-        ctx.set_profiling(True)
-        q_recs, tq = [], []
-        for i in range(args.warmup + args.fp64_steps):
-            f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            f0.record(stream)
-            q_recs.append(sess.step())
-            f1.record(stream)
-            torch.cuda.synchronize(local)
-            if i >= args.warmup:
-                tq.append(f0.elapsed_time(f1))
-        tmq = ctx.kernel_timing(2)
-        ctx.set_profiling(False)
-        sess.close()
-        prob.close()
-        perq = tmq["total_ms"] / max(1, tmq["launches"])
-        qerr = [abs(a.compliance - b.compliance) / abs(b.compliance) for a, b in zip(q_recs, f_recs)]
-        out["fp64_factored"] = {"simp_iter_s": 1000.0 * len(tq) / sum(tq) if tq else None,
-                                "pcg_iters_per_step": [r.solver_iterations for r in q_recs[args.warmup:]],
-                                "matvec_us": perq * 1000.0, "max_rel_compliance_err_vs_fp64": max(qerr) if qerr else None}
+        # fast FP64 form (factorised FP64 operator, FP64 recurrences) and the multigrid form (FP64 flexible CG
+        # preconditioned by an FP32 V-cycle) on the same iterations
+        for prec, key in (("fp64f", "fp64_factored"), ("mg", "fp64_multigrid")):
+            prob = api.Problem(model, ctx)
+            sess = api.SimpSession(prob, opts.replace(precision=prec))
+            ctx.set_profiling(True)
+            q_recs, tq = [], []
+            for i in range(args.warmup + args.fp64_steps):
+                f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                f0.record(stream)
+                q_recs.append(sess.step())
+                f1.record(stream)
+                torch.cuda.synchronize(local)
+                if i >= args.warmup:
+                    tq.append(f0.elapsed_time(f1))
+            tmq = ctx.kernel_timing(2)
+            ctx.set_profiling(False)
+            sess.close()
+            prob.close()
+            perq = tmq["total_ms"] / max(1, tmq["launches"])
+            qerr = [abs(a.compliance - b.compliance) / abs(b.compliance) for a, b in zip(q_recs, f_recs)]
+            out[key] = {"simp_iter_s": 1000.0 * len(tq) / sum(tq) if tq else None,
+                        "ms_per_step": statistics.mean(tq) if tq else None,
+                        "pcg_iters_per_step": [r.solver_iterations for r in q_recs[args.warmup:]],
+                        "matvec_us": perq * 1000.0, "max_rel_compliance_err_vs_fp64": max(qerr) if qerr else None,
+                        "rel_compliance_err_vs_fp64": qerr}
 
     # ---------------- e2e: whole job through the C ABI from host buffers ----------------
     if not args.no_e2e:

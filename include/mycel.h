@@ -42,6 +42,11 @@ extern "C" {
 /* FP64 throughout with the factorised cube-element operator (same tolerance test on the exact FP64 residual,
    not bit-exact with the reference's colour-ordered product); also what a stalled mixed solve goes on in */
 #define MYCEL_PRECISION_FP64_FACTORED 2
+/* FP64 flexible CG on the factorised operator, preconditioned by a geometric multigrid V-cycle in FP32
+   (Galerkin coarse operators rebuilt from E at each solve, damped Jacobi smoothing, dense coarsest solve);
+   same tolerance test on the exact FP64 residual. Falls back to MYCEL_PRECISION_FP64_FACTORED on a grid
+   that does not coarsen (a 1x1x1 grid) or when it does not converge. */
+#define MYCEL_PRECISION_FP64_MG 3
 
 typedef struct mycel_ctx mycel_ctx;
 typedef struct mycel_problem mycel_problem;

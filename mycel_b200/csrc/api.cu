@@ -589,6 +589,7 @@ extern "C" int32_t mycel_problem_destroy(mycel_problem* p) {
       if (p->prof64f_ev[k][j]) cudaEventDestroy(p->prof64f_ev[k][j]);
     }
   }
+  mg_release(p);
   void* ptrs[] = {p->d_domain, p->d_nflags, p->d_fixed, p->d_err, p->d_active, p->d_e2a, p->d_F, p->d_b, p->d_fnz, p->d_bnz, p->d_rho_box,
                   p->d_E, p->d_Ef, p->d_diag, p->d_invd, p->d_invdf, p->d_r, p->d_z, p->d_p, p->d_ap, p->d_x,
                   p->d_part, p->d_state, p->f_x, p->f_r, p->f_z, p->f_p0, p->f_p1, p->f_ap, p->d_r64, p->d_part2,
@@ -677,7 +678,7 @@ extern "C" int32_t mycel_apply_k(mycel_problem* p, const double* x, double* y, i
     launch_E_to_f32(p);
     // FP32 operator on the FP32-rounded input
     if ((st = mixed_apply_k_f64io(p, p->d_tmp0, p->d_tmp1, projected))) return st;
-  } else if (precision == MYCEL_PRECISION_FP64_FACTORED) {
+  } else if (precision == MYCEL_PRECISION_FP64_FACTORED || precision == MYCEL_PRECISION_FP64_MG) {
     int32_t st = fast64_apply_k(p, p->d_tmp0, p->d_tmp1, projected);
     if (st) return st;
   } else {
@@ -700,7 +701,8 @@ extern "C" int32_t mycel_pcg_solve(mycel_problem* p, const double* b, double* x,
   int32_t* nz = (int32_t*)p->d_tmp0;
   int32_t cnt = 0;
   if ((st = build_nz_list(p, p->d_tmp1, nz, &cnt))) return st;
-  if (precision == MYCEL_PRECISION_MIXED || precision == MYCEL_PRECISION_FP64_FACTORED) {
+  if (precision == MYCEL_PRECISION_MIXED || precision == MYCEL_PRECISION_FP64_FACTORED ||
+      precision == MYCEL_PRECISION_FP64_MG) {
     st = refined_solve_entry(p, p->d_tmp1, nz, cnt, p->d_x, tol, max_iter, nullptr, precision, res);
   } else {
     st = pcg_solve_fp64(p, p->d_tmp1, nz, cnt, p->d_x, tol, max_iter, nullptr, res);
@@ -714,7 +716,8 @@ extern "C" int32_t mycel_pcg_solve(mycel_problem* p, const double* b, double* x,
 namespace mycel {
 int32_t solve_dispatch(mycel_problem* p, double* d_u, double tol, int max_iter, int precision,
                        const volatile int32_t* cancel, mycel_pcg_result* res) {
-  if (precision == MYCEL_PRECISION_MIXED || precision == MYCEL_PRECISION_FP64_FACTORED) {
+  if (precision == MYCEL_PRECISION_MIXED || precision == MYCEL_PRECISION_FP64_FACTORED ||
+      precision == MYCEL_PRECISION_FP64_MG) {
     return refined_solve_entry(p, p->d_b, p->d_bnz, p->n_bnz, d_u, tol, max_iter, cancel, precision, res);
   }
   return pcg_solve_fp64(p, p->d_b, p->d_bnz, p->n_bnz, d_u, tol, max_iter, cancel, res);

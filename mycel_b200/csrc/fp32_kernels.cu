@@ -531,7 +531,7 @@ __global__ void __launch_bounds__(FX * FY, 2) k_mv32f(GridDims g, const __grid_c
   float* yb = reinterpret_cast<float*>(fac_smem + (size_t)FNST * kFacStagePitch * (MODE == 1 ? 2 : 1));
   __shared__ __align__(8) unsigned long long full[FNST];
   __shared__ double sh[32];
-  if (MODE == 1 && st->status != MIX_RUNNING) return;
+  if (st && st->status != MIX_RUNNING) return;  // MODE 0 gets a state only inside the multigrid cycle
   const float beta = MODE == 1 ? (float)st->beta : 0.0f;
   const bool two = MODE == 1 && st->first == 0;  // p_t = z + beta p_{t-1} (else p_t = z)
   const int l = threadIdx.x, w = threadIdx.y, tid = w * FX + l;
@@ -1630,6 +1630,545 @@ __global__ void k_from_pad(GridDims g, const T* __restrict__ a, double* __restri
     for (int t = threadIdx.x; t < rl; t += blockDim.x) b[(int64_t)rl * q + t] = (double)a[pad_pitch<T>(g) * q + t];
 }
 
+// ---------------------------------------------------------------------------------------------------------
+// Geometric multigrid preconditioner (MYCEL_PRECISION_FP64_MG): flexible CG in FP64 on the factorised FP64
+// operator, preconditioned by one FP32 V-cycle per iteration.
+// Levels: each level halves the element counts of the one above, rounding up (vertex-centred: even fine nodes
+// coincide with coarse nodes, odd ones lie midway; with an odd count the last fine element alone forms the last
+// coarse element), down to a coarsest level of at most kMgCoarseMax DOFs. Coarse operators are Galerkin
+// products built element by element: a coarse element's 24 x 24 matrix is the sum over its (up to 8) fine
+// sub-elements s of W_s^T T_s W_s, where T_s is the finer level's element matrix (E_e KE on the voxel grid,
+// with the rows and columns of constrained DOFs zeroed) and W_s the trilinear interpolation from the coarse
+// element's 8 nodes to the sub-element's 8 nodes. Each coarse level is then stored assembled, as a 27-point
+// node stencil of 3 x 3 blocks. Everything is rebuilt at the start of each solve from the current E.
+// Smoothing: damped Jacobi, the same sweeps before and after the coarse correction, so the V-cycle is a
+// symmetric operator; the coarsest level is solved by a dense inverse (FP64 Gauss-Jordan in shared memory).
+// Outer iteration (FCG with one-term orthogonalisation): alpha = (z, r) / (p, A p) as in PCG, and
+// beta = -alpha (z_new, A p) / (z, r), which equals PCG's beta for a fixed SPD preconditioner and stays
+// correct when FP32 rounding makes the V-cycle vary slightly from one application to the next.
+// Element matrices use the voxel operator's local node order (0,0,0),(1,0,0),(1,1,0),(0,1,0), then the same at
+// z = 1, DOF 3 a + c, like KE.
+// ---------------------------------------------------------------------------------------------------------
+constexpr int kMgMaxLevels = 12;
+constexpr int kMgCoarseMax = 144;  // DOFs of the coarsest level (its dense FP64 inverse fits in shared memory)
+// Damping of the Jacobi sweeps, per level: omega = kMgOmegaScale / lambda, lambda the largest eigenvalue of
+// D^-1 A estimated by kMgPowerIters power iterations at each set-up (from below, hence the margin to 2).
+constexpr float kMgOmegaScale = 4.0f / 3.0f;
+constexpr int kMgPowerIters = 8;
+constexpr size_t kMgCoarseSmem = (size_t)kMgCoarseMax * kMgCoarseMax * 8 + kMgCoarseMax * 8;
+
+struct MgDims {
+  int nx, ny, nz;  // elements per axis (nodes: one more)
+};
+
+__host__ __device__ __forceinline__ int64_t mg_nn(const MgDims& d) {
+  return (int64_t)(d.nx + 1) * (d.ny + 1) * (d.nz + 1);
+}
+
+// per-axis interpolation weight of coarse node c at fine node f, for a fine axis of n elements
+__device__ __forceinline__ float mg_pw(int f, int c, int n) {
+  if (!(f & 1)) return c == (f >> 1) ? 1.0f : 0.0f;
+  if (f == n) return c == ((n + 1) >> 1) ? 1.0f : 0.0f;  // last node of an odd count
+  return (c == (f >> 1) || c == (f >> 1) + 1) ? 0.5f : 0.0f;
+}
+
+// local node index from its offsets inside the element, and back
+__device__ __forceinline__ int mg_lidx(int bx, int by, int bz) { return 4 * bz + (by ? (bx ? 2 : 3) : bx); }
+__device__ __forceinline__ int mg_bx(int a) { return (a ^ (a >> 1)) & 1; }
+__device__ __forceinline__ int mg_by(int a) { return (a >> 1) & 1; }
+__device__ __forceinline__ int mg_bz(int a) { return a >> 2; }
+
+__device__ __forceinline__ bool mg_running(const MixState* st) { return !st || st->status == MIX_RUNNING; }
+
+// Galerkin element matrices of a coarse level, one CTA per coarse element. FROM_FINE: the finer level is the
+// voxel grid (T = E_e KE, masked by the node flags); otherwise its element matrices Kf.
+template <bool FROM_FINE>
+__global__ void __launch_bounds__(64) k_mg_build(MgDims c, MgDims f, const __grid_constant__ KeF ke,
+                                                 const float* __restrict__ Ef, const uint8_t* __restrict__ nf,
+                                                 const float* __restrict__ Kf, float* __restrict__ Kc) {
+  __shared__ float T[576], U[576], W[64];
+  __shared__ uint8_t fr[24];
+  const int64_t e = blockIdx.x;
+  const int ex = (int)(e % c.nx), ey = (int)((e / c.nx) % c.ny), ez = (int)(e / ((int64_t)c.nx * c.ny));
+  const int tid = threadIdx.x;
+  float acc[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) acc[k] = 0.f;
+  for (int s = 0; s < 8; ++s) {
+    const int fx = 2 * ex + (s & 1), fy = 2 * ey + ((s >> 1) & 1), fz = 2 * ez + (s >> 2);
+    if (fx >= f.nx || fy >= f.ny || fz >= f.nz) continue;  // uniform over the CTA
+    const int64_t fe = fx + (int64_t)f.nx * (fy + (int64_t)f.ny * fz);
+    float ee = 1.0f;
+    if (FROM_FINE) {
+      ee = Ef[fe];
+      if (ee == 0.0f) continue;  // inactive element
+    }
+    {  // W[a][C]: weight of coarse local node C at the sub-element's local node a
+      const int a = tid >> 3, C = tid & 7;
+      W[tid] = mg_pw(fx + mg_bx(a), ex + mg_bx(C), f.nx) * mg_pw(fy + mg_by(a), ey + mg_by(C), f.ny) *
+               mg_pw(fz + mg_bz(a), ez + mg_bz(C), f.nz);
+    }
+    if (FROM_FINE && tid < 24) {
+      const int a = tid / 3, cc = tid % 3;
+      const int64_t n = (fx + mg_bx(a)) + (int64_t)(f.nx + 1) * ((fy + mg_by(a)) + (int64_t)(f.ny + 1) * (fz + mg_bz(a)));
+      fr[tid] = !(nf[n] & (1 << cc));
+    }
+    __syncthreads();
+    for (int o = tid; o < 576; o += 64) {
+      if (FROM_FINE) {
+        const int row = o / 24, col = o % 24;
+        T[o] = (fr[row] && fr[col]) ? ee * ke.v[o] : 0.0f;
+      } else {
+        T[o] = Kf[fe * 576 + o];
+      }
+    }
+    __syncthreads();
+    // U[(a,c),(C',c')] = sum_b T[(a,c),(b,c')] W[b][C']
+    for (int o = tid; o < 576; o += 64) {
+      const int row = o / 24, Cp = (o % 24) / 3, cp = o % 3;
+      float u = 0.f;
+#pragma unroll
+      for (int b = 0; b < 8; ++b) u = fmaf(T[row * 24 + 3 * b + cp], W[b * 8 + Cp], u);
+      U[o] = u;
+    }
+    __syncthreads();
+    // Kc[(C,c),(C',c')] += sum_a W[a][C] U[(a,c),(C',c')]
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      const int o = tid + 64 * k;
+      const int C = o / 72, cc = (o / 24) % 3, col = o % 24;
+      float v = 0.f;
+#pragma unroll
+      for (int a = 0; a < 8; ++a) v = fmaf(W[a * 8 + C], U[(3 * a + cc) * 24 + col], v);
+      acc[k] += v;
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int k = 0; k < 9; ++k) Kc[e * 576 + tid + 64 * k] = acc[k];
+}
+
+// Assembled 27-point stencil of a level from its element matrices: S[(nb * 9 + 3 ci + cj) * nn + n] is the
+// block entry (DOF ci of node n, DOF cj of neighbour nb), nb = (dx+1) + 3 (dy+1) + 9 (dz+1); also 1/diag
+// (0 where the diagonal is 0: DOFs no free fine DOF reaches)
+__global__ void k_mg_stencil(MgDims d, const float* __restrict__ K, float* __restrict__ S, float* __restrict__ invd) {
+  const int64_t nn = mg_nn(d);
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= 27 * nn) return;
+  const int nb = (int)(t / nn);
+  const int64_t n = t - nb * nn;
+  const int nx1 = d.nx + 1, ny1 = d.ny + 1;
+  const int i = (int)(n % nx1), j = (int)((n / nx1) % ny1), k = (int)(n / ((int64_t)nx1 * ny1));
+  const int dx = nb % 3 - 1, dy = (nb / 3) % 3 - 1, dz = nb / 9 - 1;
+  float v[9];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) v[q] = 0.f;
+  const int mi = i + dx, mj = j + dy, mk = k + dz;
+  if (mi >= 0 && mj >= 0 && mk >= 0 && mi <= d.nx && mj <= d.ny && mk <= d.nz) {
+    for (int ez = max(max(k, mk) - 1, 0); ez <= min(min(k, mk), d.nz - 1); ++ez)
+      for (int ey = max(max(j, mj) - 1, 0); ey <= min(min(j, mj), d.ny - 1); ++ey)
+        for (int ex = max(max(i, mi) - 1, 0); ex <= min(min(i, mi), d.nx - 1); ++ex) {
+          const int a = mg_lidx(i - ex, j - ey, k - ez), b = mg_lidx(mi - ex, mj - ey, mk - ez);
+          const float* Ke = K + (ex + (int64_t)d.nx * (ey + (int64_t)d.ny * ez)) * 576;
+#pragma unroll
+          for (int ci = 0; ci < 3; ++ci)
+#pragma unroll
+            for (int cj = 0; cj < 3; ++cj) v[3 * ci + cj] += Ke[(3 * a + ci) * 24 + 3 * b + cj];
+        }
+  }
+#pragma unroll
+  for (int q = 0; q < 9; ++q) S[(nb * 9 + q) * nn + n] = v[q];
+  if (nb == 13)
+#pragma unroll
+    for (int ci = 0; ci < 3; ++ci) invd[3 * n + ci] = v[4 * ci] > 0.f ? 1.0f / v[4 * ci] : 0.0f;
+}
+
+// coarse-level product by node gather. mode 0: y = A x; 1: y = x + omega invd (r - A x) (one Jacobi sweep);
+// 2: y = r - A x on DOFs with a nonzero diagonal, 0 elsewhere
+__global__ void __launch_bounds__(256) k_mg_apply(MgDims d, const float* __restrict__ S, const float* __restrict__ x,
+                                                  const float* __restrict__ r, const float* __restrict__ invd,
+                                                  float* __restrict__ y, int mode, const float* __restrict__ om,
+                                                  const MixState* st) {
+  if (!mg_running(st)) return;
+  const float omega = mode == 1 ? *om : 0.0f;
+  const int64_t nn = mg_nn(d);
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= nn) return;
+  const int nx1 = d.nx + 1, ny1 = d.ny + 1;
+  const int i = (int)(n % nx1), j = (int)((n / nx1) % ny1), k = (int)(n / ((int64_t)nx1 * ny1));
+  float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+#pragma unroll 1
+  for (int nb = 0; nb < 27; ++nb) {
+    const int mi = i + nb % 3 - 1, mj = j + (nb / 3) % 3 - 1, mk = k + nb / 9 - 1;
+    if (mi < 0 || mj < 0 || mk < 0 || mi > d.nx || mj > d.ny || mk > d.nz) continue;
+    const int64_t m = mi + (int64_t)nx1 * (mj + (int64_t)ny1 * mk);
+    const float x0 = x[3 * m], x1 = x[3 * m + 1], x2 = x[3 * m + 2];
+    const float* s = S + (int64_t)nb * 9 * nn + n;
+    a0 = fmaf(s[0], x0, fmaf(s[nn], x1, fmaf(s[2 * nn], x2, a0)));
+    a1 = fmaf(s[3 * nn], x0, fmaf(s[4 * nn], x1, fmaf(s[5 * nn], x2, a1)));
+    a2 = fmaf(s[6 * nn], x0, fmaf(s[7 * nn], x1, fmaf(s[8 * nn], x2, a2)));
+  }
+  const float acc[3] = {a0, a1, a2};
+#pragma unroll
+  for (int cc = 0; cc < 3; ++cc) {
+    const int64_t q = 3 * n + cc;
+    if (mode == 0) y[q] = acc[cc];
+    else if (mode == 1) y[q] = fmaf(omega * invd[q], r[q] - acc[cc], x[q]);
+    else y[q] = invd[q] != 0.0f ? r[q] - acc[cc] : 0.0f;
+  }
+}
+
+// first sweep from x = 0 on a coarse level: x = omega invd r
+__global__ void k_mg_jacobi0(int64_t nd, const float* __restrict__ r, const float* __restrict__ invd,
+                             float* __restrict__ x, const float* __restrict__ om, const MixState* st) {
+  if (!mg_running(st)) return;
+  const float omega = *om;
+  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q < nd) x[q] = omega * invd[q] * r[q];
+}
+
+// a further sweep on the voxel grid (padded FP32 layout, t = A x): x += omega invd (r - t)
+__global__ void k_mg_jacobi_fine(int64_t n, const float* __restrict__ r, const float* __restrict__ t,
+                                 const float* __restrict__ invd, float* __restrict__ x, const float* __restrict__ om,
+                                 const MixState* st) {
+  if (!mg_running(st)) return;
+  const float omega = *om;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
+    x[q] = fmaf(omega * invd[q], r[q] - t[q], x[q]);
+}
+
+// restriction r_c = W^T res of a level's residual. PAD: the voxel grid in the padded FP32 layout (row pitch
+// pitch), res = r - t; otherwise box layout, res = t. Coarse DOFs with a zero diagonal get 0.
+template <bool PAD>
+__global__ void k_mg_restrict(MgDims f, int pitch, const float* __restrict__ rf, const float* __restrict__ tf,
+                              MgDims c, const float* __restrict__ invdc, float* __restrict__ rc, const MixState* st) {
+  if (!mg_running(st)) return;
+  const int64_t nn = mg_nn(c);
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= nn) return;
+  const int cx1 = c.nx + 1, cy1 = c.ny + 1;
+  const int I = (int)(n % cx1), J = (int)((n / cx1) % cy1), K = (int)(n / ((int64_t)cx1 * cy1));
+  const int pi = min(2 * I, f.nx), pj = min(2 * J, f.ny), pk = min(2 * K, f.nz);
+  float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+  for (int k = max(pk - 1, 0); k <= min(pk + 1, f.nz); ++k) {
+    const float wz = mg_pw(k, K, f.nz);
+    if (wz == 0.f) continue;
+    for (int j = max(pj - 1, 0); j <= min(pj + 1, f.ny); ++j) {
+      const float wy = wz * mg_pw(j, J, f.ny);
+      if (wy == 0.f) continue;
+      for (int i = max(pi - 1, 0); i <= min(pi + 1, f.nx); ++i) {
+        const float w = wy * mg_pw(i, I, f.nx);
+        if (w == 0.f) continue;
+        const int64_t row = j + (int64_t)(f.ny + 1) * k;
+        const int64_t b = PAD ? (int64_t)pitch * row + 3 * i : 3 * (i + (int64_t)(f.nx + 1) * row);
+        if (PAD) {
+          a0 = fmaf(w, rf[b] - tf[b], a0);
+          a1 = fmaf(w, rf[b + 1] - tf[b + 1], a1);
+          a2 = fmaf(w, rf[b + 2] - tf[b + 2], a2);
+        } else {
+          a0 = fmaf(w, tf[b], a0);
+          a1 = fmaf(w, tf[b + 1], a1);
+          a2 = fmaf(w, tf[b + 2], a2);
+        }
+      }
+    }
+  }
+  rc[3 * n] = invdc[3 * n] != 0.f ? a0 : 0.f;
+  rc[3 * n + 1] = invdc[3 * n + 1] != 0.f ? a1 : 0.f;
+  rc[3 * n + 2] = invdc[3 * n + 2] != 0.f ? a2 : 0.f;
+}
+
+// prolongation x_f += W x_c on the finer level's free DOFs. PAD: the voxel grid (padded FP32 layout, free =
+// node flag bit clear); otherwise box layout, free = nonzero diagonal.
+template <bool PAD>
+__global__ void k_mg_prolong(MgDims f, int pitch, const uint8_t* __restrict__ nf, const float* __restrict__ invdf,
+                             float* __restrict__ xf, MgDims c, const float* __restrict__ xc, const MixState* st) {
+  if (!mg_running(st)) return;
+  const int64_t nn = mg_nn(f);
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= nn) return;
+  const int fx1 = f.nx + 1, fy1 = f.ny + 1;
+  const int i = (int)(n % fx1), j = (int)((n / fx1) % fy1), k = (int)(n / ((int64_t)fx1 * fy1));
+  // per axis: up to two coarse nodes with their weights
+  int ci[2], cj[2], ck[2];
+  float wi[2], wj[2], wk[2];
+  int ni, nj, nk;
+  auto axis = [](int f_, int n_, int* cc, float* ww) {
+    if (!(f_ & 1)) { cc[0] = f_ >> 1; ww[0] = 1.f; return 1; }
+    if (f_ == n_) { cc[0] = (n_ + 1) >> 1; ww[0] = 1.f; return 1; }
+    cc[0] = f_ >> 1; cc[1] = (f_ >> 1) + 1; ww[0] = ww[1] = 0.5f; return 2;
+  };
+  ni = axis(i, f.nx, ci, wi);
+  nj = axis(j, f.ny, cj, wj);
+  nk = axis(k, f.nz, ck, wk);
+  const int cx1 = c.nx + 1, cy1 = c.ny + 1;
+  float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+  for (int qz = 0; qz < nk; ++qz)
+    for (int qy = 0; qy < nj; ++qy)
+      for (int qx = 0; qx < ni; ++qx) {
+        const float w = wi[qx] * wj[qy] * wk[qz];
+        const int64_t m = ci[qx] + (int64_t)cx1 * (cj[qy] + (int64_t)cy1 * ck[qz]);
+        a0 = fmaf(w, xc[3 * m], a0);
+        a1 = fmaf(w, xc[3 * m + 1], a1);
+        a2 = fmaf(w, xc[3 * m + 2], a2);
+      }
+  const float acc[3] = {a0, a1, a2};
+  const int64_t b = PAD ? (int64_t)pitch * (j + (int64_t)fy1 * k) + 3 * i : 3 * n;
+#pragma unroll
+  for (int cc = 0; cc < 3; ++cc) {
+    const bool fr = PAD ? !(nf[n] & (1 << cc)) : (invdf[3 * n + cc] != 0.0f);
+    if (fr) xf[b + cc] += acc[cc];
+  }
+}
+
+// coarsest level set-up (one CTA): the dense matrix from the level's stencil, inverted in place by Gauss-Jordan
+// elimination without pivoting (SPD) in FP64 shared memory. A pivot that has lost all but 1e-12 of its
+// original diagonal (round-off on a nearly singular block) drops its DOF: row and column become 0, as do those
+// of DOFs whose diagonal is 0.
+__global__ void __launch_bounds__(1024) k_mg_coarse_setup(MgDims d, const float* __restrict__ S,
+                                                          double* __restrict__ ainv) {
+  extern __shared__ __align__(16) unsigned char mg_smem[];
+  const int64_t nn = mg_nn(d);
+  const int n = (int)(3 * nn);
+  double* A = reinterpret_cast<double*>(mg_smem);
+  double* dg = A + (size_t)n * n;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int nx1 = d.nx + 1, ny1 = d.ny + 1;
+  for (int o = tid; o < n * n; o += nt) {
+    const int row = o / n, col = o % n;
+    const int a = row / 3, ci = row % 3, b = col / 3, cj = col % 3;
+    const int dx = b % nx1 - a % nx1, dy = (b / nx1) % ny1 - (a / nx1) % ny1, dz = b / (nx1 * ny1) - a / (nx1 * ny1);
+    double v = 0.0;
+    if (dx >= -1 && dx <= 1 && dy >= -1 && dy <= 1 && dz >= -1 && dz <= 1) {
+      const int nb = (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1);
+      v = (double)S[(nb * 9 + 3 * ci + cj) * nn + a];
+    }
+    A[o] = v;
+  }
+  __syncthreads();
+  for (int q = tid; q < n; q += nt) {
+    dg[q] = A[q * n + q];
+    if (!(dg[q] > 0.0)) {  // no free DOF behind it: an identity row for the elimination, zeroed at the end
+      dg[q] = 0.0;
+      for (int o = 0; o < n; ++o) A[q * n + o] = 0.0;
+    }
+  }
+  __syncthreads();
+  for (int q = tid; q < n; q += nt)
+    if (dg[q] == 0.0) {
+      for (int o = 0; o < n; ++o) A[o * n + q] = 0.0;
+      A[q * n + q] = 1.0;
+    }
+  __syncthreads();
+  for (int k = 0; k < n; ++k) {
+    const double piv = A[k * n + k];
+    const bool keep = piv > 0.0 && (dg[k] == 0.0 || piv > 1e-12 * dg[k]);
+    __syncthreads();
+    if (!keep) {
+      for (int o = tid; o < n; o += nt) {
+        A[k * n + o] = 0.0;
+        A[o * n + k] = 0.0;
+      }
+      __syncthreads();
+      continue;
+    }
+    const double ip = 1.0 / piv;
+    for (int o = tid; o < n * n; o += nt) {
+      const int i = o / n, j = o % n;
+      if (i != k && j != k) A[o] = fma(-A[i * n + k] * ip, A[k * n + j], A[o]);
+    }
+    __syncthreads();
+    for (int o = tid; o < n; o += nt) {
+      if (o != k) {
+        A[k * n + o] *= ip;
+        A[o * n + k] = -A[o * n + k] * ip;
+      }
+    }
+    if (tid == 0) A[k * n + k] = ip;
+    __syncthreads();
+  }
+  for (int o = tid; o < n * n; o += nt) {
+    const int i = o / n, j = o % n;
+    ainv[o] = (dg[i] == 0.0 || dg[j] == 0.0) ? 0.0 : A[o];
+  }
+}
+
+// coarsest solve x = A^-1 r (one warp per row)
+__global__ void k_mg_coarse_solve(int n, const double* __restrict__ ainv, const float* __restrict__ r,
+                                  float* __restrict__ x, const MixState* st) {
+  if (!mg_running(st)) return;
+  const int lane = threadIdx.x & 31;
+  for (int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < n; row += (gridDim.x * blockDim.x) >> 5) {
+    double s = 0.0;
+    for (int col = lane; col < n; col += 32) s = fma(ainv[(int64_t)row * n + col], (double)r[col], s);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) x[row] = (float)s;
+  }
+}
+
+// Outer step, part 1. mode 0: x += alpha p, r -= alpha q (FP64, padded layout), ||r|| against the stop and
+// replacement thresholds. All modes: the voxel level's FP32 residual rf = r and its first Jacobi sweep
+// xf = omega invd rf (padded FP32 layout).
+__global__ void __launch_bounds__(kT) k_mg_enter(GridDims g, double* __restrict__ x, double* __restrict__ r,
+                                                 const double* __restrict__ p, const double* __restrict__ q,
+                                                 const float* __restrict__ invdf, float* __restrict__ rf,
+                                                 float* __restrict__ xf, const float* __restrict__ om, MixState* st,
+                                                 double* part, int mode) {
+  __shared__ double sh[32];
+  if (!mg_running(st)) return;
+  const double alpha = st->alpha;
+  const float omega = *om;
+  const int rl = 3 * g.nx1;
+  const int64_t total = (int64_t)g.ny1 * g.nz1 * rl;
+  double rr = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t row = i / rl;
+    const int t = (int)(i - row * rl);
+    const int64_t a = (int64_t)g.rp64 * row + t, b = (int64_t)g.rp * row + t;
+    double rv = r[a];
+    if (mode == 0) {
+      x[a] = fma(alpha, p[a], x[a]);
+      rv = fma(-alpha, q[a], rv);
+      r[a] = rv;
+      rr += rv * rv;
+    }
+    const float rfv = (float)rv;
+    rf[b] = rfv;
+    xf[b] = omega * invdf[b] * rfv;
+  }
+  if (mode != 0) return;
+  const double br = bsum(rr, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = br;
+  if (!elect_last32(&st->counter)) return;
+  if (threadIdx.x >= 32) return;
+  const double s = warp_sum_parts(part, gridDim.x);
+  if (threadIdx.x != 0) return;
+  st->counter = 0;
+  const double rn = sqrt(s);
+  st->rn = rn;
+  st->iter += 1;
+  if (rn <= st->target || rn <= st->flush_at) st->status = MIX_FLUSH;
+  else if (st->iter >= st->max_iter) st->status = MIX_MAXITER;
+}
+
+// Outer step, part 2: the voxel level's last Jacobi sweep written as the FP64 preconditioned residual
+// z = xf + omega invd (rf - tf) (tf = A xf), then (z, r), (z, A p) and (r, r) with fixed-order sums.
+// mode 0: beta = -alpha (z, A p) / rho, rho = (z, r). mode 1 (after a true-residual replacement, direction
+// kept): the same beta, new replacement threshold. mode 2 (start): rho, next direction p = z.
+__global__ void __launch_bounds__(kT) k_mg_exit(GridDims g, const float* __restrict__ rf, const float* __restrict__ tf,
+                                                const float* __restrict__ xf, const float* __restrict__ invdf,
+                                                const double* __restrict__ r, const double* __restrict__ q,
+                                                double* __restrict__ z, const float* __restrict__ om, MixState* st,
+                                                double* part, int mode) {
+  __shared__ double sh[32];
+  if (!mg_running(st)) return;
+  const float omega = *om;
+  const int rl = 3 * g.nx1;
+  const int64_t total = (int64_t)g.ny1 * g.nz1 * rl;
+  double zr = 0.0, zq = 0.0, rr = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t row = i / rl;
+    const int t = (int)(i - row * rl);
+    const int64_t a = (int64_t)g.rp64 * row + t, b = (int64_t)g.rp * row + t;
+    const double zv = (double)fmaf(omega * invdf[b], rf[b] - tf[b], xf[b]);
+    const double rv = r[a];
+    z[a] = zv;
+    zr += zv * rv;
+    zq += zv * q[a];
+    rr += rv * rv;
+  }
+  const double b1 = bsum(zr, sh);
+  const double b2 = bsum(zq, sh);
+  const double b3 = bsum(rr, sh);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = b1;
+    part[gridDim.x + blockIdx.x] = b2;
+    part[2 * gridDim.x + blockIdx.x] = b3;
+  }
+  if (!elect_last32(&st->counter)) return;
+  if (threadIdx.x >= 32) return;
+  const double szr = warp_sum_parts(part, gridDim.x);
+  const double szq = warp_sum_parts(part + gridDim.x, gridDim.x);
+  const double srr = warp_sum_parts(part + 2 * gridDim.x, gridDim.x);
+  if (threadIdx.x != 0) return;
+  st->counter = 0;
+  if (!(szr > 0.0) || !isfinite(szr)) {  // (z, r) > 0 for an SPD preconditioner and r != 0
+    st->status = MIX_BREAKDOWN;
+    return;
+  }
+  if (mode != 0) {
+    const double rn = sqrt(srr);
+    st->rn = rn;
+    st->flush_at = rn * st->flush_factor;
+  }
+  if (mode == 2) {
+    st->first = 1;
+    st->status = st->rn <= st->target ? MIX_FLUSH : MIX_RUNNING;
+  } else if (mode == 1 && (st->iter == 0 || !(st->rho0 > 0.0))) {
+    st->first = 1;
+  } else {
+    const double beta = -st->alpha * szq / st->rho0;
+    if (isfinite(beta)) {
+      st->beta = beta;
+      st->first = 0;
+    } else {
+      st->first = 1;
+    }
+  }
+  st->rho0 = szr;
+}
+
+// Power iteration for lambda_max(D^-1 A) of a level: a fixed pseudo-random start on DOFs with a nonzero
+// inverse diagonal, then y = A x, x = D^-1 y / ||D^-1 y||; after the last product lambda ~ ||D^-1 A x||.
+__device__ __forceinline__ float mg_start_value(int64_t q) {
+  uint32_t h = (uint32_t)q * 2654435761u;
+  h ^= h >> 16;
+  h *= 2246822519u;
+  h ^= h >> 13;
+  const float u = (float)(h & 0xffffffu) * (1.0f / 16777216.0f);
+  return (h & 0x80000000u) ? -(0.5f + u) : (0.5f + u);
+}
+
+__global__ void k_mg_pow_init(int64_t n, const float* __restrict__ invd, float* __restrict__ x) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
+    x[q] = invd[q] != 0.0f ? mg_start_value(q) : 0.0f;
+}
+
+struct MgScratch {
+  float omega[kMgMaxLevels];
+  float norm;
+  unsigned int counter;
+};
+
+// ||D^-1 y|| by fixed-order sums into sc->norm; with `omega_level` >= 0 also that level's damping
+__global__ void __launch_bounds__(kT) k_mg_pow_norm(int64_t n, const float* __restrict__ y, const float* __restrict__ invd,
+                                                    double* part, MgScratch* sc, int omega_level) {
+  __shared__ double sh[32];
+  double s = 0.0;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+    const double v = (double)invd[q] * y[q];
+    s += v * v;
+  }
+  const double b = bsum(s, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = b;
+  if (!elect_last32(&sc->counter)) return;
+  if (threadIdx.x >= 32) return;
+  const double t = warp_sum_parts(part, gridDim.x);
+  if (threadIdx.x != 0) return;
+  sc->counter = 0;
+  const float nrm = (float)sqrt(t);
+  sc->norm = nrm;
+  if (omega_level >= 0) sc->omega[omega_level] = (nrm > 0.0f && isfinite(nrm)) ? kMgOmegaScale / nrm : 0.5f;
+}
+
+__global__ void k_mg_pow_scale(int64_t n, const float* __restrict__ y, const float* __restrict__ invd,
+                               const MgScratch* __restrict__ sc, float* __restrict__ x) {
+  const float inv = 1.0f / fmaxf(sc->norm, 1e-30f);
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
+    x[q] = invd[q] * y[q] * inv;
+}
+
 // grid for the streaming kernels: fixed by n (deterministic reductions), at most 8 CTAs per SM
 static int stream_blocks(mycel_problem* p) {
   int64_t want = (p->g.nd / 4 + (int64_t)kT * 4 - 1) / ((int64_t)kT * 4);
@@ -1738,10 +2277,261 @@ __global__ void k_mix_init(MixState* st, double target, int max_iter, double flu
 
 __global__ void k_mix_set(MixState* st, int status) { st->status = status; }
 
-// The refined inner PCG runs in one of two forms: FP32 work vectors and the FP32 matvec (mixed form), or FP64
-// work vectors and the factorised FP64 matvec (fast FP64 form). Both use the same device state machine.
+// Multigrid hierarchy of a problem (MYCEL_PRECISION_FP64_MG). Level 0 is the voxel grid, whose vectors are the
+// mixed form's FP32 work vectors (padded layout): residual f_r, smoothed correction f_p0 (a mapped matvec
+// input), its product f_ap. Coarse levels hold box-ordered FP32 vectors and their assembled stencil.
+struct MgLevel {
+  MgDims d{};
+  int64_t nn = 0, nd = 0;
+  float *S = nullptr, *invd = nullptr, *xa = nullptr, *xb = nullptr, *r = nullptr, *t = nullptr;
+};
+
+struct MgHier {
+  int L = 0;  // levels 0 .. L-1; level L-1 is solved by its dense inverse
+  MgLevel lv[kMgMaxLevels];
+  float* em[2] = {nullptr, nullptr};  // element matrices of alternate coarse levels (rebuilt at each solve)
+  double* ainv = nullptr;
+  MgScratch* sc = nullptr;  // per-level damping, power-iteration norm and counter (device)
+  int sweeps = 1;
+  int per_iter = 0;  // kernel launches per outer iteration
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  int graph_profiled = 0;
+  cudaEvent_t ev[2][2] = {};
+  std::vector<void*> bufs;
+};
+
+// Level element counts; 0 when the grid cannot be coarsened to a coarsest level of at most kMgCoarseMax DOFs
+// with at least one coarse level.
+static int mg_levels(int nx, int ny, int nz, MgDims* out) {
+  MgDims d{nx, ny, nz};
+  int L = 0;
+  out[L++] = d;
+  while (L < kMgMaxLevels) {
+    if (L >= 2 && 3 * mg_nn(d) <= kMgCoarseMax) break;
+    if (d.nx == 1 && d.ny == 1 && d.nz == 1) break;
+    d = {(d.nx + 1) / 2, (d.ny + 1) / 2, (d.nz + 1) / 2};
+    out[L++] = d;
+  }
+  return (L >= 2 && 3 * mg_nn(out[L - 1]) <= kMgCoarseMax) ? L : 0;
+}
+
+int64_t mg_device_bytes(int nx, int ny, int nz) {
+  MgDims lv[kMgMaxLevels];
+  const int L = mg_levels(nx, ny, nz, lv);
+  if (!L) return 0;
+  int64_t b = 0;
+  for (int l = 1; l < L; ++l) b += 4 * (243 + 15) * mg_nn(lv[l]) + 6 * 64;
+  b += sizeof(MgScratch) + 64;
+  b += 4 * 576 * (int64_t)lv[1].nx * lv[1].ny * lv[1].nz + 64;
+  if (L > 2) b += 4 * 576 * (int64_t)lv[2].nx * lv[2].ny * lv[2].nz + 64;
+  b += 8 * 9 * mg_nn(lv[L - 1]) * mg_nn(lv[L - 1]) + 64;
+  return b;
+}
+
+void mg_release(mycel_problem* p) {
+  MgHier* mg = p->mg;
+  if (!mg) return;
+  for (int k = 0; k < 2; ++k) {
+    if (mg->graph[k]) cudaGraphExecDestroy(mg->graph[k]);
+    for (int j = 0; j < 2; ++j)
+      if (mg->ev[k][j]) cudaEventDestroy(mg->ev[k][j]);
+  }
+  for (void* b : mg->bufs) cudaFreeAsync(b, p->ctx->stream);
+  delete mg;
+  p->mg = nullptr;
+}
+
+static int32_t mg_ensure(mycel_problem* p, bool* available) {
+  static std::once_flag smem_once;
+  static cudaError_t smem_err = cudaSuccess;
+  std::call_once(smem_once, [] {
+    smem_err = cudaFuncSetAttribute(k_mg_coarse_setup, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMgCoarseSmem);
+  });
+  if (smem_err != cudaSuccess)
+    return set_error(p->ctx, MYCEL_E_DEVICE, std::string("multigrid shared memory: ") + cudaGetErrorString(smem_err));
+  *available = false;
+  if (p->mg) {
+    *available = true;
+    return MYCEL_OK;
+  }
+  MgDims dims[kMgMaxLevels];
+  const int L = mg_levels(p->g.nx, p->g.ny, p->g.nz, dims);
+  if (!L) return MYCEL_OK;
+  MgHier* mg = new MgHier();
+  mg->L = L;
+  if (const char* e = std::getenv("MYCEL_MG_SWEEPS")) mg->sweeps = std::max(1, std::atoi(e));
+  cudaStream_t s = p->ctx->stream;
+  bool oom = false;
+  auto alloc = [&](size_t bytes) -> void* {
+    void* ptr = nullptr;
+    if (oom || cudaMallocAsync(&ptr, bytes + 64, s) != cudaSuccess) {
+      oom = true;
+      return nullptr;
+    }
+    cudaMemsetAsync(ptr, 0, bytes + 64, s);
+    p->device_bytes += (int64_t)bytes + 64;
+    mg->bufs.push_back(ptr);
+    return ptr;
+  };
+  for (int l = 0; l < L; ++l) {
+    MgLevel& v = mg->lv[l];
+    v.d = dims[l];
+    v.nn = mg_nn(v.d);
+    v.nd = 3 * v.nn;
+    if (l == 0) continue;
+    v.S = (float*)alloc(sizeof(float) * 243 * v.nn);
+    float** vecs[] = {&v.invd, &v.xa, &v.xb, &v.r, &v.t};
+    for (float** q : vecs) *q = (float*)alloc(sizeof(float) * v.nd);
+  }
+  for (int k = 0; k < 2 && k + 1 < L; ++k) {
+    const MgDims& d = mg->lv[k + 1].d;
+    mg->em[k] = (float*)alloc(sizeof(float) * 576 * (size_t)d.nx * d.ny * d.nz);
+  }
+  const int64_t nc = mg->lv[L - 1].nd;
+  mg->ainv = (double*)alloc(sizeof(double) * nc * nc);
+  mg->sc = (MgScratch*)alloc(sizeof(MgScratch));
+  // launches per outer iteration: matvec, k_mg_enter, the V-cycle (as issued by mg_vcycle), k_mg_exit
+  const int sw = mg->sweeps;
+  const int cycle = 4 * (sw - 1) + 2 + (L - 2) * (2 + sw) + 1 + (L - 2) * (1 + sw) + 1 + 1;
+  mg->per_iter = 3 + cycle;
+  p->mg = mg;
+  if (oom) return set_error(p->ctx, MYCEL_E_OOM, "out of device memory for the multigrid hierarchy");
+  *available = true;
+  return MYCEL_OK;
+}
+
+static unsigned mg_blocks(int64_t n) { return (unsigned)((n + 255) / 256); }
+
+// Coarse operators from the current E: Galerkin element matrices level by level, their stencils, and the
+// coarsest level's dense inverse.
+static void mg_setup(mycel_problem* p) {
+  MgHier* mg = p->mg;
+  cudaStream_t s = p->ctx->stream;
+  MgLevel* lv = mg->lv;
+  const MgDims& d1 = lv[1].d;
+  k_mg_build<true><<<(unsigned)((int64_t)d1.nx * d1.ny * d1.nz), 64, 0, s>>>(d1, lv[0].d, p->kef, p->d_Ef,
+                                                                           p->d_nflags, nullptr, mg->em[0]);
+  k_mg_stencil<<<mg_blocks(27 * lv[1].nn), 256, 0, s>>>(d1, mg->em[0], lv[1].S, lv[1].invd);
+  for (int l = 2; l < mg->L; ++l) {
+    const MgDims& d = lv[l].d;
+    float* src = mg->em[(l - 2) & 1];
+    float* dst = mg->em[(l - 1) & 1];
+    k_mg_build<false><<<(unsigned)((int64_t)d.nx * d.ny * d.nz), 64, 0, s>>>(d, lv[l - 1].d, p->kef, nullptr,
+                                                                           nullptr, src, dst);
+    k_mg_stencil<<<mg_blocks(27 * lv[l].nn), 256, 0, s>>>(d, dst, lv[l].S, lv[l].invd);
+  }
+  k_mg_coarse_setup<<<1, 1024, kMgCoarseSmem, s>>>(lv[mg->L - 1].d, lv[mg->L - 1].S, mg->ainv);
+  int nl = 2 * (mg->L - 1) + 1;
+  // damping of every smoothed level (all but the coarsest) from its power iteration
+  const int sb = stream_blocks(p);
+  for (int l = 0; l < mg->L - 1; ++l) {
+    MgLevel& v = lv[l];
+    const int64_t n = l ? v.nd : p->g.n32;
+    const float* invd = l ? v.invd : p->d_invdf;
+    float* x = l ? v.xa : p->f_p0;
+    float* y = l ? v.t : p->f_ap;
+    const unsigned nb = l ? std::min<unsigned>(mg_blocks(n), (unsigned)sb) : (unsigned)sb;
+    k_mg_pow_init<<<nb, 256, 0, s>>>(n, invd, x);
+    for (int it = 0; it < kMgPowerIters; ++it) {
+      if (l) k_mg_apply<<<mg_blocks(v.nn), 256, 0, s>>>(v.d, v.S, x, nullptr, invd, y, 0, nullptr, nullptr);
+      else launch_mv32_variant<0>(p, s, p->f_p0, nullptr, nullptr, nullptr, p->f_ap, 1, nullptr, nullptr);
+      const bool last = it == kMgPowerIters - 1;
+      k_mg_pow_norm<<<nb, kT, 0, s>>>(n, y, invd, p->d_part2, mg->sc, last ? l : -1);
+      if (!last) k_mg_pow_scale<<<nb, 256, 0, s>>>(n, y, invd, mg->sc, x);
+      nl += last ? 2 : 3;
+    }
+    nl++;
+  }
+  p->ctx->launches += nl;
+}
+
+// One V-cycle from the voxel level's residual f_r and first sweep f_p0 (written by k_mg_enter) up to
+// f_ap = A f_p0 before the last sweep (done by k_mg_exit). Returns the kernels launched.
+static int mg_vcycle(mycel_problem* p, cudaStream_t s, MixState* st) {
+  MgHier* mg = p->mg;
+  MgLevel* lv = mg->lv;
+  const GridDims& g = p->g;
+  const float* om = mg->sc->omega;  // device: damping of level l at om + l
+  const int sb = stream_blocks(p);
+  int nl = 0;
+  auto fine_mv = [&] { launch_mv32_variant<0>(p, s, p->f_p0, nullptr, nullptr, nullptr, p->f_ap, 1, st, nullptr); };
+  for (int k = 1; k < mg->sweeps; ++k) {
+    fine_mv();
+    k_mg_jacobi_fine<<<sb, kT, 0, s>>>(g.n32, p->f_r, p->f_ap, p->d_invdf, p->f_p0, om, st);
+    nl += 2;
+  }
+  fine_mv();
+  k_mg_restrict<true><<<mg_blocks(lv[1].nn), 256, 0, s>>>(lv[0].d, g.rp, p->f_r, p->f_ap, lv[1].d, lv[1].invd,
+                                                          lv[1].r, st);
+  nl += 2;
+  float* xc[kMgMaxLevels] = {};
+  for (int l = 1; l < mg->L - 1; ++l) {
+    MgLevel& v = lv[l];
+    float *x = v.xa, *o = v.xb;
+    k_mg_jacobi0<<<mg_blocks(v.nd), 256, 0, s>>>(v.nd, v.r, v.invd, x, om + l, st);
+    for (int k = 1; k < mg->sweeps; ++k) {
+      k_mg_apply<<<mg_blocks(v.nn), 256, 0, s>>>(v.d, v.S, x, v.r, v.invd, o, 1, om + l, st);
+      std::swap(x, o);
+    }
+    k_mg_apply<<<mg_blocks(v.nn), 256, 0, s>>>(v.d, v.S, x, v.r, v.invd, v.t, 2, om + l, st);
+    k_mg_restrict<false><<<mg_blocks(lv[l + 1].nn), 256, 0, s>>>(v.d, 0, nullptr, v.t, lv[l + 1].d, lv[l + 1].invd,
+                                                                 lv[l + 1].r, st);
+    xc[l] = x;
+    nl += 2 + mg->sweeps;
+  }
+  MgLevel& cl = lv[mg->L - 1];
+  k_mg_coarse_solve<<<mg_blocks(32 * cl.nd), 256, 0, s>>>((int)cl.nd, mg->ainv, cl.r, cl.xa, st);
+  xc[mg->L - 1] = cl.xa;
+  nl++;
+  for (int l = mg->L - 2; l >= 1; --l) {
+    MgLevel& v = lv[l];
+    float* x = xc[l];
+    float* o = x == v.xa ? v.xb : v.xa;
+    k_mg_prolong<false><<<mg_blocks(v.nn), 256, 0, s>>>(v.d, 0, nullptr, v.invd, x, lv[l + 1].d, xc[l + 1], st);
+    for (int k = 0; k < mg->sweeps; ++k) {
+      k_mg_apply<<<mg_blocks(v.nn), 256, 0, s>>>(v.d, v.S, x, v.r, v.invd, o, 1, om + l, st);
+      std::swap(x, o);
+    }
+    xc[l] = x;
+    nl += 1 + mg->sweeps;
+  }
+  k_mg_prolong<true><<<mg_blocks(lv[0].nn), 256, 0, s>>>(lv[0].d, g.rp, p->d_nflags, nullptr, p->f_p0, lv[1].d,
+                                                         xc[1], st);
+  nl++;
+  for (int k = 1; k < mg->sweeps; ++k) {
+    fine_mv();
+    k_mg_jacobi_fine<<<sb, kT, 0, s>>>(g.n32, p->f_r, p->f_ap, p->d_invdf, p->f_p0, om, st);
+    nl += 2;
+  }
+  fine_mv();
+  return nl + 1;
+}
+
+// The outer step after the matvec (mode 0), or the preconditioned residual after a start (2) or a true-residual
+// replacement (1): k_mg_enter, the V-cycle, k_mg_exit. Returns the kernels launched.
+static int launch_mg_step(mycel_problem* p, cudaStream_t s, const double* pcur, int mode) {
+  MgHier* mg = p->mg;
+  MixState* st = mix_state(p);
+  const int sb = stream_blocks(p);
+  int nl = 0;
+  if (mode == 1) {
+    k_mix_set<<<1, 1, 0, s>>>(st, MIX_RUNNING);
+    nl++;
+  }
+  k_mg_enter<<<sb, kT, 0, s>>>(p->g, p->g_x, p->g_r, pcur, p->g_ap, p->d_invdf, p->f_r, p->f_p0, mg->sc->omega, st,
+                               p->d_part2, mode);
+  nl += 1 + mg_vcycle(p, s, st);
+  k_mg_exit<<<sb, kT, 0, s>>>(p->g, p->f_r, p->f_ap, p->f_p0, p->d_invdf, p->g_r, p->g_ap, p->g_z, mg->sc->omega, st,
+                              p->d_part2, mode);
+  return nl + 1;
+}
+
+// The refined inner PCG runs in one of three forms: FP32 work vectors and the FP32 matvec (mixed form), FP64
+// work vectors and the factorised FP64 matvec (fast FP64 form), or the latter preconditioned by a multigrid
+// V-cycle (multigrid form). All use the same device state machine.
 struct InnerForm {
   bool f64;
+  bool mg;
   void *x, *r, *z, *p0, *p1, *ap;
   const void* invd;
   int64_t n;        // padded length
@@ -1751,14 +2541,24 @@ struct InnerForm {
   cudaEvent_t (*ev)[2];
   int prof_slot;
   double flush_factor;
+  int chunk;     // iterations per graph (even)
+  int per_iter;  // kernel launches per iteration
 };
 
 static InnerForm inner_form(mycel_problem* p, bool f64) {
   if (f64)
-    return {true, p->g_x, p->g_r, p->g_z, p->g_p0, p->g_p1, p->g_ap, p->g_invd, p->g.n64, sizeof(double),
-            p->pcg64f_graph, &p->pcg64f_graph_profiled, p->prof64f_ev, 2, 1e-4};
-  return {false, p->f_x, p->f_r, p->f_z, p->f_p0, p->f_p1, p->f_ap, p->d_invdf, p->g.n32, sizeof(float),
-          p->pcg32_graph, &p->pcg32_graph_profiled, p->prof_ev, 0, kFlushFactor};
+    return {true, false, p->g_x, p->g_r, p->g_z, p->g_p0, p->g_p1, p->g_ap, p->g_invd, p->g.n64, sizeof(double),
+            p->pcg64f_graph, &p->pcg64f_graph_profiled, p->prof64f_ev, 2, 1e-4, 16, 2};
+  return {false, false, p->f_x, p->f_r, p->f_z, p->f_p0, p->f_p1, p->f_ap, p->d_invdf, p->g.n32, sizeof(float),
+          p->pcg32_graph, &p->pcg32_graph_profiled, p->prof_ev, 0, kFlushFactor, 16, 2};
+}
+
+// multigrid form: the fast FP64 form's vectors and matvec; short chunks, since an iteration past convergence
+// still launches its whole V-cycle (whose kernels then return at once)
+static InnerForm inner_form_mg(mycel_problem* p) {
+  MgHier* mg = p->mg;
+  return {true, true, p->g_x, p->g_r, p->g_z, p->g_p0, p->g_p1, p->g_ap, p->g_invd, p->g.n64, sizeof(double),
+          mg->graph, &mg->graph_profiled, mg->ev, 2, 1e-4, 4, mg->per_iter};
 }
 
 static void launch_inner_mv(mycel_problem* p, const InnerForm& F, cudaStream_t s, void* pold, void* pcur) {
@@ -1770,14 +2570,16 @@ static void launch_inner_mv(mycel_problem* p, const InnerForm& F, cudaStream_t s
                            mix_state(p), p->d_part2);
 }
 
-static void launch_inner_xr(mycel_problem* p, const InnerForm& F, cudaStream_t s, void* pcur, int mode) {
+static int launch_inner_xr(mycel_problem* p, const InnerForm& F, cudaStream_t s, void* pcur, int mode) {
   const int sb = stream_blocks(p);
+  if (F.mg) return launch_mg_step(p, s, (const double*)pcur, mode);
   if (F.f64)
     k_xr64<<<sb, kT, 0, s>>>(F.n, (double*)F.x, (double*)F.r, (double*)F.z, (const double*)pcur, (const double*)F.ap,
                              (const double*)F.invd, mix_state(p), p->d_part2, mode);
   else
     k_xr32<<<sb, kT, 0, s>>>(F.n, (float*)F.x, (float*)F.r, (float*)F.z, (const float*)pcur, (const float*)F.ap,
                              (const float*)F.invd, mix_state(p), p->d_part2, mode);
+  return 1;
 }
 
 // Chunk of inner iterations as a graph; p alternates between two buffers (even chunk length, each chunk starts
@@ -1857,8 +2659,8 @@ static int32_t refined_loop(mycel_problem* p, const InnerForm& F, const double* 
                             LoopOut* out) {
   mycel_ctx* c = p->ctx;
   cudaStream_t s = c->stream;
-  const int chunk = 16;
-  const char* name = F.f64 ? "fast FP64" : "mixed";
+  const int chunk = F.chunk;
+  const char* name = F.mg ? "multigrid" : (F.f64 ? "fast FP64" : "mixed");
   MixState* ms = mix_state(p);
   int32_t st;
   if (F.f64) {
@@ -1878,8 +2680,7 @@ static int32_t refined_loop(mycel_problem* p, const InnerForm& F, const double* 
   struct EvGuard { cudaEvent_t* e; ~EvGuard() { cudaEventDestroy(e[0]); cudaEventDestroy(e[1]); } } evg{evs};
   cudaMemsetAsync(F.x, 0, F.es * F.n, s);
   k_mix_init<<<1, 1, 0, s>>>(ms, 0.5 * tol * bnorm, max_iter, F.flush_factor);
-  launch_inner_xr(p, F, s, F.p0, 2);
-  c->launches += 2;
+  c->launches += 1 + launch_inner_xr(p, F, s, F.p0, 2);
   int64_t launched = 0;
   const int64_t cap = (int64_t)max_iter + 64 * chunk + 4096;
   int iter_at_resume = 0;
@@ -1904,7 +2705,7 @@ static int32_t refined_loop(mycel_problem* p, const InnerForm& F, const double* 
       launch_inner_chunk(p, F, gi);
       MYCEL_CUDA(c, cudaGetLastError());
       launched += chunk;
-      c->launches += 2 * chunk;
+      c->launches += (int64_t)F.per_iter * chunk;
       MYCEL_CUDA(c, cudaMemcpyAsync(slot[gi], ms, sizeof(MixState), cudaMemcpyDeviceToHost, s));
       MYCEL_CUDA(c, cudaEventRecord(evs[gi], s));
       if (k == 0) continue;
@@ -1953,8 +2754,7 @@ static int32_t refined_loop(mycel_problem* p, const InnerForm& F, const double* 
     }
     cycle_limit = std::max<int64_t>(2000, 3 * (int64_t)out->iterations);
     if (out->stalled || status != MIX_FLUSH || out->iterations >= max_iter) break;
-    launch_inner_xr(p, F, s, F.p0, 1);
-    c->launches++;
+    c->launches += launch_inner_xr(p, F, s, F.p0, 1);
     iter_at_resume = out->iterations;
   }
   return MYCEL_OK;
@@ -1964,6 +2764,7 @@ static int32_t refined_loop(mycel_problem* p, const InnerForm& F, const double* 
 // MYCEL_PRECISION_MIXED: FP32 inner PCG; if it stalls, breaks down or runs out of iterations the solve goes on
 // in the fast FP64 form from the refined u, and finally (should that fail too) in the plain FP64 PCG.
 // MYCEL_PRECISION_FP64_FACTORED: the fast FP64 form, then the plain FP64 PCG if it does not converge.
+// MYCEL_PRECISION_FP64_MG: the multigrid form (where the grid coarsens), then as MYCEL_PRECISION_FP64_FACTORED.
 int32_t refined_solve_entry(mycel_problem* p, const double* d_b, const int32_t* d_nz, int32_t n_nz, double* d_u,
                             double tol, int max_iter, const volatile int32_t* cancel, int precision,
                             mycel_pcg_result* res) {
@@ -1979,7 +2780,8 @@ int32_t refined_solve_entry(mycel_problem* p, const double* d_b, const int32_t* 
   int32_t st = ensure_pcg_workspace(p);
   if (st) return st;
   const bool mixed = precision == MYCEL_PRECISION_MIXED;
-  if (mixed && (st = ensure_mixed(p))) return st;
+  const bool mgp = precision == MYCEL_PRECISION_FP64_MG;
+  if ((mixed || mgp) && (st = ensure_mixed(p))) return st;
   double* saved_b = p->d_b;
   int32_t* saved_nz = p->d_bnz;
   int32_t saved_n = p->n_bnz;
@@ -2007,9 +2809,24 @@ int32_t refined_solve_entry(mycel_problem* p, const double* d_b, const int32_t* 
   }
   const bool verbose = std::getenv("MYCEL_VERBOSE") != nullptr;
   MYCEL_CUDA(c, cudaMemsetAsync(p->d_err, 0, sizeof(int), s));  // bounded-wait failures of this solve only
-  LoopOut l32, l64;
+  LoopOut l32, l64, lmg;
   bool ok = false;
   double rel = 0.0;
+  bool ran_mg = false;
+  if (mgp) {
+    bool avail = false;
+    if ((st = ensure_f64f(p)) || (st = resolve_mv32(p)) || (st = mg_ensure(p, &avail))) return st;
+    if (avail) {
+      ran_mg = true;
+      mg_setup(p);
+      if ((st = refined_loop(p, inner_form_mg(p), d_b, d_u, bnorm, tol, max_iter, cancel, false, verbose, &lmg)))
+        return st;
+      ok = lmg.ok;
+      rel = lmg.rel;
+      if (ok && lmg.iterations == 0 && lmg.flushes == 0)
+        std::snprintf(res->message, sizeof res->message, "Initial guess already converged.");
+    }
+  }
   // Which inner form a mixed solve starts in. Once a mixed solve of a problem has stalled (its designs have
   // become badly conditioned, which in a SIMP run does not go away), its later mixed solves start in the fast
   // FP64 form. Otherwise the FP32 form runs unless the last solves showed it needing more than kCost64 times the
@@ -2038,6 +2855,9 @@ int32_t refined_solve_entry(mycel_problem* p, const double* d_b, const int32_t* 
       std::snprintf(res->message, sizeof res->message, "Initial guess already converged.");
   }
   int remaining = std::max(1, max_iter - l32.iterations);
+  if (!ok && ran_mg && verbose)
+    std::fprintf(stderr, "mycel: multigrid solve not converged after %d iterations (%.3e); fast FP64 form next\n",
+                 lmg.iterations, lmg.rel);
   if (!ok) {
     if ((st = ensure_f64f(p))) return st;
     MYCEL_CUDA(c, cudaMemsetAsync(p->d_err, 0, sizeof(int), s));
@@ -2052,7 +2872,7 @@ int32_t refined_solve_entry(mycel_problem* p, const double* d_b, const int32_t* 
     if (verbose && run32)
       std::fprintf(stderr, "mycel: mixed solve went on in fast FP64 (%s after %d inner iterations): %d iterations, %.3e\n",
                    l32.stalled ? "stalled" : "not converged", l32.iterations, l64.iterations, rel);
-    if (!run32 && ok && l64.iterations == 0 && l64.flushes == 0)
+    if (!run32 && !ran_mg && ok && l64.iterations == 0 && l64.flushes == 0)
       std::snprintf(res->message, sizeof res->message, "Initial guess already converged.");
   }
   int plain_iter = 0;
@@ -2067,12 +2887,15 @@ int32_t refined_solve_entry(mycel_problem* p, const double* d_b, const int32_t* 
   if (mixed) {
     res->inner_iterations = l32.iterations;
     res->fallback_iterations = l64.iterations + plain_iter;
+  } else if (mgp) {
+    res->inner_iterations = lmg.iterations;
+    res->fallback_iterations = l64.iterations + plain_iter;
   } else {
     res->inner_iterations = l64.iterations;
     res->fallback_iterations = plain_iter;
   }
   res->iterations = res->inner_iterations + res->fallback_iterations;
-  res->refinement_steps = l32.flushes + l64.flushes;
+  res->refinement_steps = l32.flushes + l64.flushes + lmg.flushes;
   res->final_residual = rel;
   res->converged = ok ? 1 : 0;
   if (!ok)

@@ -92,6 +92,7 @@ struct DevBuf {
   size_t bytes = 0;
 };
 
+struct MgHier;  // multigrid hierarchy of a problem (fp32_kernels.cu)
 }  // namespace mycel
 
 // ---- opaque handles of the C ABI ----
@@ -169,6 +170,7 @@ struct mycel_problem {
   cudaGraphExec_t pcg64f_graph[2] = {nullptr, nullptr};
   int pcg64f_graph_profiled = 0;
   cudaEvent_t prof64f_ev[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+  mycel::MgHier* mg = nullptr;     // multigrid hierarchy (MYCEL_PRECISION_FP64_MG), built on first use
   double* d_r64 = nullptr;        // refinement residual
   double* d_part2 = nullptr;      // [many] FP64 partials for mixed dots
   int64_t n_part2 = 0;
@@ -269,6 +271,8 @@ int32_t refined_solve_entry(mycel_problem* p, const double* d_b, const int32_t* 
                             double tol, int max_iter, const volatile int32_t* cancel, int precision,
                             mycel_pcg_result* res);
 int32_t fast64_apply_k(mycel_problem* p, const double* x, double* y, int projected);
+void mg_release(mycel_problem* p);
+int64_t mg_device_bytes(int nx, int ny, int nz);  // hierarchy of a grid; 0 when it does not coarsen
 
 // ---- drivers (api.cu) ----
 int32_t pcg_solve_fp64(mycel_problem* p, const double* d_b, const int32_t* d_nz, int32_t n_nz, double* d_x,

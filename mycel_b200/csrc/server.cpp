@@ -110,8 +110,11 @@ static int64_t job_bytes(const mycel_grid& gr, int64_t n_active, int64_t n_fixed
   const int64_t nb = (nd + 8191) / 8192;
   b += 5 * al16(8 * nd) + al16(8 * (2 * nb + 64)) + al16(sizeof(mycel::PcgState));
   // mixed workspace (6 FP32 vectors) and the fast FP64 workspace (7 FP64 vectors) a mixed solve escalates to
-  if (o.precision == MYCEL_PRECISION_MIXED) b += 6 * (4 * g.n32 + 64);
-  if (o.precision == MYCEL_PRECISION_MIXED || o.precision == MYCEL_PRECISION_FP64_FACTORED) b += 7 * (8 * g.n64 + 64);
+  const bool mg = o.precision == MYCEL_PRECISION_FP64_MG;
+  if (o.precision == MYCEL_PRECISION_MIXED || mg) b += 6 * (4 * g.n32 + 64);
+  if (o.precision == MYCEL_PRECISION_MIXED || o.precision == MYCEL_PRECISION_FP64_FACTORED || mg)
+    b += 7 * (8 * g.n64 + 64);
+  if (mg) b += mycel::mg_device_bytes(g.nx, g.ny, g.nz);
   // filter (stencil offsets and weights of radius ceil(rmin) <= max(filter radius, 1.5) / h, plus invHs, S)
   double rmin = o.filter_radius_mm / std::max(1e-30, (double)gr.h);
   if (o.enforce_minimum_filter_radius && rmin < 1.5) rmin = 1.5;
