@@ -1592,18 +1592,20 @@ __global__ void k_flush_u(GridDims g, double* __restrict__ u, T* __restrict__ xw
     }
 }
 
-// after A u: r64 = P(b - A u), r_work = (T) r64, CTA partials of r64^2
+// after A u (padded FP64 layout, factorised FP64 operator): r64 = P(b - A u), r_work = (T) r64, CTA partials of
+// r64^2; zero_au clears A u after reading
 template <class T>
-__global__ void k_resid64(GridDims g, const uint8_t* __restrict__ nf, const double* __restrict__ b,
-                          const double* __restrict__ au, T* __restrict__ rw, double* part) {
+__global__ void k_resid64p(GridDims g, const uint8_t* __restrict__ nf, const double* __restrict__ b,
+                           double* __restrict__ au, T* __restrict__ rw, double* part, int zero_au) {
   __shared__ double sh[32];
   double s = 0.0;
   const int rl = 3 * g.nx1;
   for (int64_t q = blockIdx.x; q < (int64_t)g.ny1 * g.nz1; q += gridDim.x)
     for (int t = threadIdx.x; t < rl; t += blockDim.x) {
-      const int64_t i = (int64_t)rl * q + t;
+      const int64_t i = (int64_t)rl * q + t, a = (int64_t)g.rp64 * q + t;
       const bool con = nf[i / 3] & (1 << (t % 3));
-      const double v = con ? 0.0 : (b[i] - au[i]);
+      const double v = con ? 0.0 : (b[i] - au[a]);
+      if (zero_au) au[a] = 0.0;
       rw[pad_pitch<T>(g) * q + t] = (T)v;
       s += v * v;
     }
@@ -1685,10 +1687,12 @@ __device__ __forceinline__ bool mg_running(const MixState* st) { return !st || s
 template <bool FROM_FINE>
 __global__ void __launch_bounds__(64) k_mg_build(MgDims c, MgDims f, const __grid_constant__ KeF ke,
                                                  const float* __restrict__ Ef, const uint8_t* __restrict__ nf,
-                                                 const float* __restrict__ Kf, float* __restrict__ Kc) {
+                                                 const float* __restrict__ Kf, float* __restrict__ Kc,
+                                                 const uint8_t* __restrict__ only) {
   __shared__ float T[576], U[576], W[64];
   __shared__ uint8_t fr[24];
   const int64_t e = blockIdx.x;
+  if (only && !only[e]) return;  // done by k_mg_build1
   const int ex = (int)(e % c.nx), ey = (int)((e / c.nx) % c.ny), ez = (int)(e / ((int64_t)c.nx * c.ny));
   const int tid = threadIdx.x;
   float acc[9];
@@ -1748,6 +1752,60 @@ __global__ void __launch_bounds__(64) k_mg_build(MgDims c, MgDims f, const __gri
   for (int k = 0; k < 9; ++k) Kc[e * 576 + tid + 64 * k] = acc[k];
 }
 
+// Level-1 element matrices from the voxel grid, fast path: when all 8 sub-elements of a coarse element exist and
+// none of its 27 fine nodes has a constrained DOF, K_c = sum_s E_s G_s with G_s = W_s^T KE W_s (precomputed,
+// [8][576]). Other coarse elements (an odd last layer, supports) are marked for k_mg_build<true>. Four coarse
+// elements per CTA, 64 threads each.
+__global__ void __launch_bounds__(256) k_mg_build1(MgDims c, MgDims f, const float* __restrict__ G,
+                                                   const float* __restrict__ Ef, const uint8_t* __restrict__ nf,
+                                                   float* __restrict__ Kc, uint8_t* __restrict__ special) {
+  __shared__ float Gs[8 * 576];
+  __shared__ float Es[4][8];
+  __shared__ int sp[4];
+  for (int o = threadIdx.x; o < 8 * 576; o += blockDim.x) Gs[o] = G[o];
+  const int grp = threadIdx.x >> 6, lt = threadIdx.x & 63;
+  const int64_t ne = (int64_t)c.nx * c.ny * c.nz;
+  for (int64_t base = (int64_t)blockIdx.x * 4; base < ne; base += (int64_t)gridDim.x * 4) {
+    const int64_t e = base + grp;
+    const bool valid = e < ne;
+    if (lt == 0) sp[grp] = 0;
+    __syncthreads();
+    if (valid) {
+      const int ex = (int)(e % c.nx), ey = (int)((e / c.nx) % c.ny), ez = (int)(e / ((int64_t)c.nx * c.ny));
+      if (lt < 8) {
+        const int fx = 2 * ex + (lt & 1), fy = 2 * ey + ((lt >> 1) & 1), fz = 2 * ez + (lt >> 2);
+        if (fx < f.nx && fy < f.ny && fz < f.nz) Es[grp][lt] = Ef[fx + (int64_t)f.nx * (fy + (int64_t)f.ny * fz)];
+        else sp[grp] = 1;
+      } else if (lt >= 32 && lt < 59) {
+        const int q = lt - 32;
+        const int i = 2 * ex + q % 3, j = 2 * ey + (q / 3) % 3, k = 2 * ez + q / 9;
+        if (i <= f.nx && j <= f.ny && k <= f.nz) {
+          const uint8_t fl = nf[i + (int64_t)(f.nx + 1) * (j + (int64_t)(f.ny + 1) * k)];
+          if ((fl & (NF_CX | NF_CY | NF_CZ)) && (fl & NF_ACTIVE)) sp[grp] = 1;
+        } else {
+          sp[grp] = 1;
+        }
+      }
+    }
+    __syncthreads();
+    if (valid && !sp[grp]) {
+      float es[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) es[q] = Es[grp][q];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) {
+        const int o = lt + 64 * k;
+        float v = 0.f;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v = fmaf(es[q], Gs[q * 576 + o], v);
+        Kc[e * 576 + o] = v;
+      }
+    }
+    if (valid && lt == 0) special[e] = (uint8_t)sp[grp];
+    __syncthreads();
+  }
+}
+
 // Assembled 27-point stencil of a level from its element matrices: S[(nb * 9 + 3 ci + cj) * nn + n] is the
 // block entry (DOF ci of node n, DOF cj of neighbour nb), nb = (dx+1) + 3 (dy+1) + 9 (dz+1); also 1/diag
 // (0 where the diagonal is 0: DOFs no free fine DOF reaches)
@@ -1797,10 +1855,12 @@ __global__ void __launch_bounds__(256) k_mg_apply(MgDims d, const float* __restr
   const int nx1 = d.nx + 1, ny1 = d.ny + 1;
   const int i = (int)(n % nx1), j = (int)((n / nx1) % ny1), k = (int)(n / ((int64_t)nx1 * ny1));
   float a0 = 0.f, a1 = 0.f, a2 = 0.f;
-#pragma unroll 1
+  // all 27 blocks without branches: a neighbour outside the grid has a zero stencil block, so its x is read
+  // at a clamped (valid) node
+#pragma unroll
   for (int nb = 0; nb < 27; ++nb) {
-    const int mi = i + nb % 3 - 1, mj = j + (nb / 3) % 3 - 1, mk = k + nb / 9 - 1;
-    if (mi < 0 || mj < 0 || mk < 0 || mi > d.nx || mj > d.ny || mk > d.nz) continue;
+    const int mi = min(max(i + nb % 3 - 1, 0), d.nx), mj = min(max(j + (nb / 3) % 3 - 1, 0), d.ny),
+              mk = min(max(k + nb / 9 - 1, 0), d.nz);
     const int64_t m = mi + (int64_t)nx1 * (mj + (int64_t)ny1 * mk);
     const float x0 = x[3 * m], x1 = x[3 * m + 1], x2 = x[3 * m + 2];
     const float* s = S + (int64_t)nb * 9 * nn + n;
@@ -1850,15 +1910,20 @@ __global__ void k_mg_restrict(MgDims f, int pitch, const float* __restrict__ rf,
   const int I = (int)(n % cx1), J = (int)((n / cx1) % cy1), K = (int)(n / ((int64_t)cx1 * cy1));
   const int pi = min(2 * I, f.nx), pj = min(2 * J, f.ny), pk = min(2 * K, f.nz);
   float a0 = 0.f, a1 = 0.f, a2 = 0.f;
-  for (int k = max(pk - 1, 0); k <= min(pk + 1, f.nz); ++k) {
-    const float wz = mg_pw(k, K, f.nz);
-    if (wz == 0.f) continue;
-    for (int j = max(pj - 1, 0); j <= min(pj + 1, f.ny); ++j) {
-      const float wy = wz * mg_pw(j, J, f.ny);
-      if (wy == 0.f) continue;
-      for (int i = max(pi - 1, 0); i <= min(pi + 1, f.nx); ++i) {
-        const float w = wy * mg_pw(i, I, f.nx);
-        if (w == 0.f) continue;
+  // the 27 candidate fine nodes around the coarse node's position, without branches: a candidate outside the
+  // grid gets weight 0 and a clamped (valid) read
+#pragma unroll
+  for (int dk = -1; dk <= 1; ++dk) {
+    const int k0 = pk + dk, k = min(max(k0, 0), f.nz);
+    const float wz = (k0 == k) ? mg_pw(k, K, f.nz) : 0.f;
+#pragma unroll
+    for (int dj = -1; dj <= 1; ++dj) {
+      const int j0 = pj + dj, j = min(max(j0, 0), f.ny);
+      const float wy = (j0 == j) ? wz * mg_pw(j, J, f.ny) : 0.f;
+#pragma unroll
+      for (int di = -1; di <= 1; ++di) {
+        const int i0 = pi + di, i = min(max(i0, 0), f.nx);
+        const float w = (i0 == i) ? wy * mg_pw(i, I, f.nx) : 0.f;
         const int64_t row = j + (int64_t)(f.ny + 1) * k;
         const int64_t b = PAD ? (int64_t)pitch * row + 3 * i : 3 * (i + (int64_t)(f.nx + 1) * row);
         if (PAD) {
@@ -1889,23 +1954,27 @@ __global__ void k_mg_prolong(MgDims f, int pitch, const uint8_t* __restrict__ nf
   if (n >= nn) return;
   const int fx1 = f.nx + 1, fy1 = f.ny + 1;
   const int i = (int)(n % fx1), j = (int)((n / fx1) % fy1), k = (int)(n / ((int64_t)fx1 * fy1));
-  // per axis: up to two coarse nodes with their weights
+  // per axis: two coarse nodes with their weights (the second with weight 0 unless the fine node lies midway)
   int ci[2], cj[2], ck[2];
   float wi[2], wj[2], wk[2];
-  int ni, nj, nk;
-  auto axis = [](int f_, int n_, int* cc, float* ww) {
-    if (!(f_ & 1)) { cc[0] = f_ >> 1; ww[0] = 1.f; return 1; }
-    if (f_ == n_) { cc[0] = (n_ + 1) >> 1; ww[0] = 1.f; return 1; }
-    cc[0] = f_ >> 1; cc[1] = (f_ >> 1) + 1; ww[0] = ww[1] = 0.5f; return 2;
+  auto axis = [](int f_, int n_, int nc_, int* cc, float* ww) {
+    const bool mid = (f_ & 1) && f_ != n_;
+    cc[0] = ((f_ & 1) && f_ == n_) ? nc_ : (f_ >> 1);
+    cc[1] = min(cc[0] + 1, nc_);
+    ww[0] = mid ? 0.5f : 1.0f;
+    ww[1] = mid ? 0.5f : 0.0f;
   };
-  ni = axis(i, f.nx, ci, wi);
-  nj = axis(j, f.ny, cj, wj);
-  nk = axis(k, f.nz, ck, wk);
+  axis(i, f.nx, c.nx, ci, wi);
+  axis(j, f.ny, c.ny, cj, wj);
+  axis(k, f.nz, c.nz, ck, wk);
   const int cx1 = c.nx + 1, cy1 = c.ny + 1;
   float a0 = 0.f, a1 = 0.f, a2 = 0.f;
-  for (int qz = 0; qz < nk; ++qz)
-    for (int qy = 0; qy < nj; ++qy)
-      for (int qx = 0; qx < ni; ++qx) {
+#pragma unroll
+  for (int qz = 0; qz < 2; ++qz)
+#pragma unroll
+    for (int qy = 0; qy < 2; ++qy)
+#pragma unroll
+      for (int qx = 0; qx < 2; ++qx) {
         const float w = wi[qx] * wj[qy] * wk[qz];
         const int64_t m = ci[qx] + (int64_t)cx1 * (cj[qy] + (int64_t)cy1 * ck[qz]);
         a0 = fmaf(w, xc[3 * m], a0);
@@ -2290,6 +2359,8 @@ struct MgHier {
   int L = 0;  // levels 0 .. L-1; level L-1 is solved by its dense inverse
   MgLevel lv[kMgMaxLevels];
   float* em[2] = {nullptr, nullptr};  // element matrices of alternate coarse levels (rebuilt at each solve)
+  float* G = nullptr;                 // [8][576] W_s^T KE W_s of the 8 sub-element positions (level-1 fast path)
+  uint8_t* special = nullptr;         // [level-1 elements] built by the general path
   double* ainv = nullptr;
   MgScratch* sc = nullptr;  // per-level damping, power-iteration norm and counter (device)
   int sweeps = 1;
@@ -2321,7 +2392,7 @@ int64_t mg_device_bytes(int nx, int ny, int nz) {
   if (!L) return 0;
   int64_t b = 0;
   for (int l = 1; l < L; ++l) b += 4 * (243 + 15) * mg_nn(lv[l]) + 6 * 64;
-  b += sizeof(MgScratch) + 64;
+  b += sizeof(MgScratch) + 64 + 4 * 8 * 576 + 64 + (int64_t)lv[1].nx * lv[1].ny * lv[1].nz + 64;
   b += 4 * 576 * (int64_t)lv[1].nx * lv[1].ny * lv[1].nz + 64;
   if (L > 2) b += 4 * 576 * (int64_t)lv[2].nx * lv[2].ny * lv[2].nz + 64;
   b += 8 * 9 * mg_nn(lv[L - 1]) * mg_nn(lv[L - 1]) + 64;
@@ -2390,6 +2461,32 @@ static int32_t mg_ensure(mycel_problem* p, bool* available) {
   const int64_t nc = mg->lv[L - 1].nd;
   mg->ainv = (double*)alloc(sizeof(double) * nc * nc);
   mg->sc = (MgScratch*)alloc(sizeof(MgScratch));
+  mg->G = (float*)alloc(sizeof(float) * 8 * 576);
+  mg->special = (uint8_t*)alloc((size_t)dims[1].nx * dims[1].ny * dims[1].nz);
+  if (!oom) {  // G_s = W_s^T KE W_s for an interior coarse element (all sub-elements present), in FP64
+    auto w1 = [](int f, int c) { return f == 1 ? 0.5 : ((f == 0) == (c == 0) ? 1.0 : 0.0); };
+    auto bx = [](int a) { return (a ^ (a >> 1)) & 1; };
+    auto by = [](int a) { return (a >> 1) & 1; };
+    auto bz = [](int a) { return a >> 2; };
+    std::vector<float> G(8 * 576);
+    for (int sub = 0; sub < 8; ++sub) {
+      const int sx = sub & 1, sy = (sub >> 1) & 1, sz = sub >> 2;
+      double W[8][8];
+      for (int a = 0; a < 8; ++a)
+        for (int C = 0; C < 8; ++C)
+          W[a][C] = w1(sx + bx(a), bx(C)) * w1(sy + by(a), by(C)) * w1(sz + bz(a), bz(C));
+      for (int row = 0; row < 24; ++row)
+        for (int col = 0; col < 24; ++col) {
+          const int C = row / 3, cc = row % 3, Cp = col / 3, cp = col % 3;
+          double v = 0.0;
+          for (int a = 0; a < 8; ++a)
+            for (int b = 0; b < 8; ++b) v += W[a][C] * p->ke.v[(3 * a + cc) * 24 + 3 * b + cp] * W[b][Cp];
+          G[sub * 576 + row * 24 + col] = (float)v;
+        }
+    }
+    cudaMemcpyAsync(mg->G, G.data(), sizeof(float) * G.size(), cudaMemcpyHostToDevice, s);
+    cudaStreamSynchronize(s);
+  }
   // launches per outer iteration: matvec, k_mg_enter, the V-cycle (as issued by mg_vcycle), k_mg_exit
   const int sw = mg->sweeps;
   const int cycle = 4 * (sw - 1) + 2 + (L - 2) * (2 + sw) + 1 + (L - 2) * (1 + sw) + 1 + 1;
@@ -2409,19 +2506,22 @@ static void mg_setup(mycel_problem* p) {
   cudaStream_t s = p->ctx->stream;
   MgLevel* lv = mg->lv;
   const MgDims& d1 = lv[1].d;
-  k_mg_build<true><<<(unsigned)((int64_t)d1.nx * d1.ny * d1.nz), 64, 0, s>>>(d1, lv[0].d, p->kef, p->d_Ef,
-                                                                           p->d_nflags, nullptr, mg->em[0]);
+  const int64_t ne1 = (int64_t)d1.nx * d1.ny * d1.nz;
+  k_mg_build1<<<(unsigned)std::min<int64_t>((ne1 + 3) / 4, 8 * (int64_t)p->ctx->num_sms), 256, 0, s>>>(
+      d1, lv[0].d, mg->G, p->d_Ef, p->d_nflags, mg->em[0], mg->special);
+  k_mg_build<true><<<(unsigned)ne1, 64, 0, s>>>(d1, lv[0].d, p->kef, p->d_Ef, p->d_nflags, nullptr, mg->em[0],
+                                                mg->special);
   k_mg_stencil<<<mg_blocks(27 * lv[1].nn), 256, 0, s>>>(d1, mg->em[0], lv[1].S, lv[1].invd);
   for (int l = 2; l < mg->L; ++l) {
     const MgDims& d = lv[l].d;
     float* src = mg->em[(l - 2) & 1];
     float* dst = mg->em[(l - 1) & 1];
     k_mg_build<false><<<(unsigned)((int64_t)d.nx * d.ny * d.nz), 64, 0, s>>>(d, lv[l - 1].d, p->kef, nullptr,
-                                                                           nullptr, src, dst);
+                                                                           nullptr, src, dst, nullptr);
     k_mg_stencil<<<mg_blocks(27 * lv[l].nn), 256, 0, s>>>(d, dst, lv[l].S, lv[l].invd);
   }
   k_mg_coarse_setup<<<1, 1024, kMgCoarseSmem, s>>>(lv[mg->L - 1].d, lv[mg->L - 1].S, mg->ainv);
-  int nl = 2 * (mg->L - 1) + 1;
+  int nl = 2 * (mg->L - 1) + 2;
   // damping of every smoothed level (all but the coarsest) from its power iteration
   const int sb = stream_blocks(p);
   for (int l = 0; l < mg->L - 1; ++l) {
@@ -2625,18 +2725,24 @@ static void launch_inner_chunk(mycel_problem* p, const InnerForm& F, int gi) {
   cudaGraphLaunch(F.graph[gi], s);
 }
 
-// r_work = P(b - A u) in FP64 (then rounded to the form's type), returns ||r|| (synchronises)
+// r_work = P(b - A u) in FP64 (then rounded to the form's type), returns ||r|| (synchronises). A u comes from
+// the factorised FP64 operator (equal to the reference's product up to FP64 rounding): u goes to g_r (a mapped
+// input; the fast FP64 forms' own residual, overwritten here anyway), A u to a vector free at this point (g_x,
+// the fast FP64 forms' correction, already added to u and cleared again here; g_ap in the mixed form, whose
+// vectors are FP32).
 static int32_t true_residual(mycel_problem* p, const InnerForm& F, const double* d_b, const double* d_u, double* rn) {
   mycel_ctx* c = p->ctx;
   cudaStream_t s = c->stream;
   int sb = stream_blocks(p);
   double* part = p->d_part2;
   double* scal = p->d_part2 + p->n_part2 - 128;
-  launch_matvec64(p, d_u, p->d_ap, 1, nullptr);
-  if (F.f64) k_resid64<double><<<sb, kT, 0, s>>>(p->g, p->d_nflags, d_b, p->d_ap, (double*)F.r, part);
-  else k_resid64<float><<<sb, kT, 0, s>>>(p->g, p->d_nflags, d_b, p->d_ap, (float*)F.r, part);
+  double* au = F.f64 ? p->g_x : p->g_ap;
+  k_to_pad<double><<<sb, kT, 0, s>>>(p->g, d_u, p->g_r);
+  launch_mv64f<0>(p, s, p->g_r, nullptr, nullptr, nullptr, au, 1, nullptr, nullptr);
+  if (F.f64) k_resid64p<double><<<sb, kT, 0, s>>>(p->g, p->d_nflags, d_b, au, (double*)F.r, part, 1);
+  else k_resid64p<float><<<sb, kT, 0, s>>>(p->g, p->d_nflags, d_b, au, (float*)F.r, part, 0);
   k_sum_part<<<1, 32, 0, s>>>(part, sb, scal);
-  c->launches += 2;
+  c->launches += 4;
   double* h = (double*)((char*)c->pinned + 1024);
   MYCEL_CUDA(c, cudaMemcpyAsync(h, scal, sizeof(double), cudaMemcpyDeviceToHost, s));
   MYCEL_CUDA(c, cudaStreamSynchronize(s));
@@ -2782,6 +2888,7 @@ int32_t refined_solve_entry(mycel_problem* p, const double* d_b, const int32_t* 
   const bool mixed = precision == MYCEL_PRECISION_MIXED;
   const bool mgp = precision == MYCEL_PRECISION_FP64_MG;
   if ((mixed || mgp) && (st = ensure_mixed(p))) return st;
+  if ((st = ensure_f64f(p))) return st;  // every refined form measures its true residual with the FP64 operator
   double* saved_b = p->d_b;
   int32_t* saved_nz = p->d_bnz;
   int32_t saved_n = p->n_bnz;
