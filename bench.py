@@ -1,6 +1,11 @@
 #!/usr/bin/env python
 """SIMP iterations/s of the mixed-precision path on the 192x96x96 bridge (1,769,472 Hex8 elements, 5.4M DOFs).
 
+The timed path (--precision, default "mixed-mg") is the mixed-precision form with the multigrid preconditioner:
+FP32 inner flexible CG (FP32 K.u and FP32 V-cycle) inside FP64 iterative refinement, FP64 dot products. The
+other solver forms run beside it on the same iterations: the plain FP64 path (reference arithmetic), "mixed"
+(FP32 inner Jacobi-PCG, the reference's preconditioner), "fp64f" and "mg".
+
 One step = one SIMP iteration (filter, E/DiagA, warm-started PCG to the tolerance, compliance, sensitivities,
 adjoint filter, OC bisection) on the device-resident state. Prints one JSON line.
 
@@ -8,7 +13,7 @@ adjoint filter, OC bisection) on the device-resident state. Prints one JSON line
   e2e        the same metric for a whole job through the C ABI from host buffers: problem upload, W+K
              iterations each followed by the density snapshot read-back (what the App consumes), final u
   roofline   the FP32 stiffness matvec (the dominant kernel), timed live by events captured in the PCG graph
-  fp64       the plain FP64 path (bit-exact drop-in) on the same workload, and the mixed-vs-FP64 compliance error
+  fp64       the plain FP64 path (bit-exact drop-in) on the same workload, and the timed path's compliance error
   cpu_baseline  the CPU oracle (C++ restatement, all host threads) on a bounded sample of the same iteration
 
 --impl reference runs only the CPU restatement of the reference path (rank 0) on the same workload.
@@ -28,16 +33,19 @@ import time
 import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
+# the headline metric (the same for both arms)
+METRIC = "SIMP iter/s (mixed FP32-inner/FP64-refined, 192x96x96 bridge)"
 sys.path.insert(0, ROOT)
 
 # PCG iterations per SIMP iteration of the plain FP64 path on this workload (iterations 4-13, measured on B200;
 # the FP64 path reproduces the reference's iteration counts bit for bit). Used only to scale the CPU sample.
 FP64_PCG_PER_SIMP_ITER = None
 
-# DRAM bytes per launch of the dominant kernel, from one ncu capture (dram__bytes_read.sum +
-# dram__bytes_write.sum; `--probe mixed --probe-grid 192x96x96 --probe-variant 3`): 53.47 MB read, 5.53 MB
-# written (K p and p_t mostly stay in the 126 MB L2 during the launch). Keyed by (matvec variant, workload).
-NCU_DRAM_BYTES = {(3, "bridge_192x96x96"): 53.47e6 + 5.53e6}
+# DRAM bytes per launch of the FP32 matvec (MODE 1) from one ncu capture (dram__bytes_read.sum +
+# dram__bytes_write.sum), keyed by (solver form, matvec variant, workload). Jacobi-PCG form (`--probe mixed
+# --probe-grid 192x96x96 --probe-variant 3`): 53.47 MB read, 5.53 MB written (K p and p_t mostly stay in the
+# 126 MB L2 during the launch).
+NCU_DRAM_BYTES = {("mixed", 3, "bridge_192x96x96"): 53.47e6 + 5.53e6}
 
 
 def parse():
@@ -51,7 +59,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-sample-iters", type=int, default=6)
-    ap.add_argument("--probe", choices=["mixed", "fp64", "fp64f"], default=None,
+    ap.add_argument("--precision", choices=["mixed-mg", "mixed", "mg", "fp64f"], default="mixed-mg",
+                    help="solver form of the timed path (value, e2e, roofline, serving sample, batched)")
+    ap.add_argument("--probe", choices=["mixed", "fp64", "fp64f", "mg", "mixed-mg"], default=None,
                     help="kernel probe for profilers: one PCG solve of --probe-iters iterations on a bridge grid")
     ap.add_argument("--probe-grid", default="96x48x48")
     ap.add_argument("--probe-iters", type=int, default=40)
@@ -69,7 +79,7 @@ def parse():
     ap.add_argument("--serve-max-elems", type=int, default=1_000_000)
     ap.add_argument("--serve-slots", type=int, default=6)
     ap.add_argument("--serve-budget-gb", type=float, default=150.0)
-    ap.add_argument("--serve-precisions", default="mixed,fp64")
+    ap.add_argument("--serve-precisions", default="mixed-mg,fp64")
     ap.add_argument("--serve-fp64-jobs", type=int, default=None, help="prefix of the stream run in FP64 (default all)")
     ap.add_argument("--static", action="store_true",
                     help="static solve of the sphere-carved 96x48x24 box (about 98k active elements) to 1e-8: plain "
@@ -250,12 +260,13 @@ def serving_report(args, n_jobs, max_elems, rate, slots, budget_gb, precisions, 
         out["rel_compliance_err_fp64f_vs_fp64"] = compare_histories(hists["fp64f"], hists["fp64"])
         if out["fp64"]["simp_iter_s"]:
             out["speedup_fp64f_vs_fp64"] = out["fp64f"]["simp_iter_s"] / out["fp64"]["simp_iter_s"]
-    if "mixed" in hists and "fp64" in hists:
-        out["rel_compliance_err_mixed_vs_fp64"] = compare_histories(hists["mixed"], hists["fp64"])
-        n = min(len(hists["mixed"]), len(hists["fp64"]))
-        if out["fp64"]["simp_iter_s"]:
-            out["speedup_mixed_vs_fp64"] = out["mixed"]["simp_iter_s"] / out["fp64"]["simp_iter_s"] \
-                if n == len(hists["mixed"]) else None
+    for prec in ("mixed", "mixed-mg", "mg"):
+        if prec in hists and "fp64" in hists:
+            out[f"rel_compliance_err_{prec}_vs_fp64"] = compare_histories(hists[prec], hists["fp64"])
+            n = min(len(hists[prec]), len(hists["fp64"]))
+            if out["fp64"]["simp_iter_s"]:
+                out[f"speedup_{prec}_vs_fp64"] = out[prec]["simp_iter_s"] / out["fp64"]["simp_iter_s"] \
+                    if n == len(hists[prec]) else None
     return out
 
 
@@ -284,8 +295,9 @@ def run_serve(args):
                              ws=ws)
         out[prec] = replicas.merge({"latencies": r["_latencies"], "simp_iterations": r["simp_iterations"],
                                     "first_submit_s": 0.0, "last_finish_s": r["wall_s"]})
-    if "mixed" in out and "fp64" in out and out["fp64"]["simp_iter_s"]:
-        out["speedup_mixed_vs_fp64"] = out["mixed"]["simp_iter_s"] / out["fp64"]["simp_iter_s"]
+    for prec in precisions:
+        if prec != "fp64" and "fp64" in out and out["fp64"]["simp_iter_s"]:
+            out[f"speedup_{prec}_vs_fp64"] = out[prec]["simp_iter_s"] / out["fp64"]["simp_iter_s"]
     if rank == 0:
         print(json.dumps(out), flush=True)
     import torch.distributed as dist
@@ -305,7 +317,7 @@ def run_static(args):
     out = {"metric": "static solve to 1e-8 (sphere-carved 96x48x24 box)", "active_elements": model.active_element_count,
            "dofs": model.total_dofs}
     ref = None
-    for prec, slot in (("fp64", 1), ("mixed", 0), ("fp64f", 2), ("mg", 2)):
+    for prec, slot in (("fp64", 1), ("mixed", 0), ("fp64f", 2), ("mg", 2), ("mixed-mg", 0)):
         pr = api.Problem(model, ctx)
         b = pr.forces()
         pr.pcg_solve(b, tol=1e-8, max_iterations=20000, precision=prec)  # set-up, autotune, graph capture
@@ -344,7 +356,7 @@ def run_static(args):
 
 
 def run_batched(args):
-    """Batched instances: all problems submitted at once; aggregate SIMP iter/s, mixed vs FP64."""
+    """Batched instances: all problems submitted at once; aggregate SIMP iter/s, the timed form vs FP64."""
     from mycel_b200 import api
     from mycel_b200 import workloads as W
     probs = W.batched_instances(count=args.batched_count)
@@ -352,7 +364,8 @@ def run_batched(args):
            "iterations_each": args.batched_iters, "pcg_tol": args.job_tol,
            "elements_total": int(sum(bp.model.total_elements for bp in probs))}
     hists = {}
-    for prec in ("mixed", "fp64"):
+    head = args.precision
+    for prec in (head, "fp64"):
         with api.Server(slots=args.serve_slots, hbm_budget_bytes=int(args.serve_budget_gb * 1e9)) as srv:
             ids = [srv.submit(bp.model, bp.options.replace(max_iterations=args.batched_iters, precision=prec,
                                                           solver_tolerance_initial=args.job_tol,
@@ -364,8 +377,8 @@ def run_batched(args):
         span = st["last_finish_s"] - st["first_submit_s"]
         out[prec] = {"simp_iter_s": st["simp_iterations"] / span, "wall_s": span, "completed": st["completed"],
                      "p50_latency_s": st["p50_latency_s"], "p99_latency_s": st["p99_latency_s"]}
-    out["speedup_mixed_vs_fp64"] = out["mixed"]["simp_iter_s"] / out["fp64"]["simp_iter_s"]
-    out["rel_compliance_err_mixed_vs_fp64"] = compare_histories(hists["mixed"], hists["fp64"])
+    out[f"speedup_{head}_vs_fp64"] = out[head]["simp_iter_s"] / out["fp64"]["simp_iter_s"]
+    out[f"rel_compliance_err_{head}_vs_fp64"] = compare_histories(hists[head], hists["fp64"])
     print(json.dumps(out), flush=True)
 
 
@@ -375,14 +388,14 @@ def run_mycel(args):
     ws, rank, local = dist_init()
     ctx = api.Context(local)
     model, opts = workload(args.workload)
-    mixed = opts.replace(precision="mixed")
+    head = opts.replace(precision=args.precision)
     stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
 
     # ---------------- value: device-resident SIMP iterations ----------------
     prob = api.Problem(model, ctx)
     if args.mv32_variant:
         prob.set_matvec32(args.mv32_variant)
-    sess = api.SimpSession(prob, mixed)
+    sess = api.SimpSession(prob, head)
     for _ in range(args.warmup):
         sess.step()
     launches0 = ctx.launch_count
@@ -405,7 +418,7 @@ def run_mycel(args):
     t_max = max_over_ranks(ws, t_ms)
     value = ws * args.steps / (t_max / 1000.0)
     pcg_inner = [r.solver_iterations for r in recs]
-    comp_mixed = [r.compliance for r in recs]
+    comp_head = [r.compliance for r in recs]
     mv_variant = prob.matvec32()
     sess.close()
     prob.close()
@@ -418,7 +431,7 @@ def run_mycel(args):
     hbm = (pk or {}).get("hbm_gbs") or 6650.0
     kname = {1: "k_mv32 (dense KE rows, FMA pipe)", 2: "k_mv32tc (dense KE, tcgen05 3xTF32)",
              3: "k_mv32f (factorised Hex8 operator, TMA-fed)"}.get(mv_variant, "FP32 matvec")
-    traffic = NCU_DRAM_BYTES.get((mv_variant, args.workload))
+    traffic = NCU_DRAM_BYTES.get((args.precision, mv_variant, args.workload))
     roof = {"kernel": kname + ": FP32 Hex8 K.p with fused p update + p.Ap partials", "bound": "hbm",
             "achieved": achieved, "peak": hbm, "unit": "GB/s",
             "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
@@ -429,17 +442,17 @@ def run_mycel(args):
             "flops_per_launch": 1152 * model.active_element_count, "flops_note": "dense-KE equivalent",
             "tflops": 1152 * model.active_element_count / (per_launch_ms / 1000.0) / 1e12 if timing["launches"] else None}
 
-    out = {"metric": "SIMP iter/s (mixed FP32-inner/FP64-refined, 192x96x96 bridge)", "value": value,
+    out = {"metric": METRIC, "value": value,
            "unit": "SIMP iter/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "f32 inner PCG + f64 refinement/reductions", "data": "synthetic",
            "config": {"workload": args.workload, "elements": model.total_elements, "dofs": model.total_dofs,
-                      "precision": "mixed", "volfrac": opts.volume_fraction, "rmin": opts.filter_radius_mm,
+                      "precision": args.precision, "volfrac": opts.volume_fraction, "rmin": opts.filter_radius_mm,
                       "penal": opts.penal, "emin_ratio": model.material.emin_ratio,
                       "pcg_tol": opts.solver_tolerance_final, "inputs_vs_l2": "inputs > L2 (126 MB); no flush",
                       "parallelism": f"replicas x{ws}"},
            "roofline": roof, "gpu_launches": gpu_launches, "clocks": clk,
-           "pcg_inner_iters_per_step": pcg_inner, "compliance_mixed": comp_mixed}
+           "pcg_inner_iters_per_step": pcg_inner, "compliance": comp_head}
 
     # ---------------- plain FP64 path on the same iterations ----------------
     if args.fp64_steps > 0 and rank == 0:
@@ -461,9 +474,9 @@ def run_mycel(args):
         ctx.set_profiling(False)
         sess.close()
         prob.close()
-        # compliance of the same iterations (1..W+fp64_steps) in the mixed run: rerun them from the start
+        # compliance of the same iterations (1..W+fp64_steps) in the timed form: rerun them from the start
         prob = api.Problem(model, ctx)
-        sess = api.SimpSession(prob, mixed)
+        sess = api.SimpSession(prob, head)
         m_recs = [sess.step() for _ in range(args.warmup + args.fp64_steps)]
         sess.close()
         prob.close()
@@ -474,11 +487,14 @@ def run_mycel(args):
                        "pcg_iters_per_step": [r.solver_iterations for r in f_recs[args.warmup:]],
                        "matvec_us": per64 * 1000.0,
                        "matvec_gbs": (48 * model.total_nodes + 9 * model.total_elements) / (per64 / 1000.0) / 1e9 if tm64["launches"] else None,
-                       "mixed_vs_fp64_rel_compliance_err": errs, "max_rel_compliance_err": max(errs) if errs else None}
-        out["speedup_mixed_vs_fp64"] = (value / ws) / out["fp64"]["simp_iter_s"] if out["fp64"]["simp_iter_s"] else None
+                       "timed_form_vs_fp64_rel_compliance_err": errs,
+                       "max_rel_compliance_err": max(errs) if errs else None}
+        out["speedup_vs_fp64"] = (value / ws) / out["fp64"]["simp_iter_s"] if out["fp64"]["simp_iter_s"] else None
         # fast FP64 form (factorised FP64 operator, FP64 recurrences) and the multigrid form (FP64 flexible CG
         # preconditioned by an FP32 V-cycle) on the same iterations
-        for prec, key in (("fp64f", "fp64_factored"), ("mg", "fp64_multigrid")):
+        others = [("fp64f", "fp64_factored"), ("mg", "fp64_multigrid"), ("mixed", "mixed_jacobi"),
+                  ("mixed-mg", "mixed_multigrid")]
+        for prec, key in [o for o in others if o[0] != args.precision]:
             prob = api.Problem(model, ctx)
             sess = api.SimpSession(prob, opts.replace(precision=prec))
             ctx.set_profiling(True)
@@ -513,7 +529,7 @@ def run_mycel(args):
         d2h_step = 2 * 4 * model.total_elements + 112
         t0 = time.perf_counter()
         prob = api.Problem(model, ctx)
-        sess = api.SimpSession(prob, mixed.replace(max_iterations=n_it))
+        sess = api.SimpSession(prob, head.replace(max_iterations=n_it))
         for _ in range(n_it):
             sess.step()
             sess.read(u=False, densities=True)
@@ -537,7 +553,7 @@ def run_mycel(args):
     # ---------------- serving sample (rank 0): Poisson job stream through the serving loop ----------------
     if rank == 0 and not args.no_serve:
         out["serving"] = serving_report(args, args.serve_sample_jobs, args.serve_sample_max_elems, 20.0,
-                                        args.serve_slots, 150.0, ["mixed", "fp64"])
+                                        args.serve_slots, 150.0, [args.precision, "fp64"])
         out["serving"]["note"] = ("bounded sample of the served stream: first jobs of the Poisson(20/s) stream, "
                                   "sizes log-uniform up to serve_sample_max_elems; full stream: bench.py --serve")
 
@@ -602,7 +618,7 @@ def run_reference(args):
         if i >= args.warmup:
             vals.append(r["value"])
     v = statistics.mean(vals)
-    out = {"impl": "reference", "metric": "SIMP iter/s (mixed FP32-inner/FP64-refined, 192x96x96 bridge)",
+    out = {"impl": "reference", "metric": METRIC,
            "value": v, "unit": "SIMP iter/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
            "config": {"workload": args.workload},
@@ -618,12 +634,12 @@ def run_probe(args):
     nx, ny, nz = (int(v) for v in args.probe_grid.split("x"))
     ctx = api.Context(0)
     pr = api.Problem(W.bridge(nx, ny, nz), ctx)
-    if args.probe == "mixed" and args.probe_variant:
+    if args.probe in ("mixed", "mixed-mg", "mg") and args.probe_variant:
         pr.set_matvec32(args.probe_variant)
     u, r = pr.pcg_solve(pr.forces(), tol=1e-30, max_iterations=args.probe_iters, precision=args.probe)
     print(json.dumps({"probe": args.probe, "grid": args.probe_grid, "iterations": r.iterations,
                       "elapsed_ms": r.elapsed_ms, "final_residual": r.final_residual,
-                      "matvec32": pr.matvec32() if args.probe == "mixed" else None}))
+                      "matvec32": pr.matvec32() if args.probe in ("mixed", "mixed-mg", "mg") else None}))
 
 
 if __name__ == "__main__":

@@ -47,6 +47,11 @@ extern "C" {
    same tolerance test on the exact FP64 residual. Falls back to MYCEL_PRECISION_FP64_FACTORED on a grid
    that does not coarsen (a 1x1x1 grid) or when it does not converge. */
 #define MYCEL_PRECISION_FP64_MG 3
+/* The multigrid form with the inner iteration in FP32: FP32 flexible CG (FP32 K·u and V-cycle, FP64 dot
+   products) wrapped in FP64 iterative refinement (true residual f - K u in FP64 after each 1e-3 drop of the
+   recursive one). Goes on in MYCEL_PRECISION_FP64_MG if it stalls or does not converge (and starts there for
+   the rest of the problem's solves after a stall), then as MYCEL_PRECISION_FP64_FACTORED. */
+#define MYCEL_PRECISION_MIXED_MG 4
 
 typedef struct mycel_ctx mycel_ctx;
 typedef struct mycel_problem mycel_problem;

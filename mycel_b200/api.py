@@ -24,8 +24,9 @@ FP64 = 0
 MIXED = 1
 FP64_FACTORED = 2
 FP64_MG = 3
-_PREC = {"fp64": FP64, "mixed": MIXED, "fp64f": FP64_FACTORED, "mg": FP64_MG, FP64: FP64, MIXED: MIXED,
-         FP64_FACTORED: FP64_FACTORED, FP64_MG: FP64_MG}
+MIXED_MG = 4
+_PREC = {"fp64": FP64, "mixed": MIXED, "fp64f": FP64_FACTORED, "mg": FP64_MG, "mixed-mg": MIXED_MG, FP64: FP64,
+         MIXED: MIXED, FP64_FACTORED: FP64_FACTORED, FP64_MG: FP64_MG, MIXED_MG: MIXED_MG}
 
 _ERRORS = {1: ArgumentError, 2: InvalidOperationError, 3: InvalidOperationError, 4: InvalidOperationError,
            5: CancelledError, 6: TimeoutError_, 7: DeviceError, 8: OutOfMemoryError, 9: InvalidOperationError}

@@ -672,7 +672,7 @@ extern "C" int32_t mycel_apply_k(mycel_problem* p, const double* x, double* y, i
   cudaSetDevice(p->ctx->device);
   cudaStream_t s = p->ctx->stream;
   MYCEL_CUDA(p->ctx, cudaMemcpyAsync(p->d_tmp0, x, sizeof(double) * p->g.nd, cudaMemcpyHostToDevice, s));
-  if (precision == MYCEL_PRECISION_MIXED) {
+  if (precision == MYCEL_PRECISION_MIXED || precision == MYCEL_PRECISION_MIXED_MG) {
     int32_t st = ensure_pcg_workspace(p);
     if (st) return st;
     launch_E_to_f32(p);
@@ -702,7 +702,7 @@ extern "C" int32_t mycel_pcg_solve(mycel_problem* p, const double* b, double* x,
   int32_t cnt = 0;
   if ((st = build_nz_list(p, p->d_tmp1, nz, &cnt))) return st;
   if (precision == MYCEL_PRECISION_MIXED || precision == MYCEL_PRECISION_FP64_FACTORED ||
-      precision == MYCEL_PRECISION_FP64_MG) {
+      precision == MYCEL_PRECISION_FP64_MG || precision == MYCEL_PRECISION_MIXED_MG) {
     st = refined_solve_entry(p, p->d_tmp1, nz, cnt, p->d_x, tol, max_iter, nullptr, precision, res);
   } else {
     st = pcg_solve_fp64(p, p->d_tmp1, nz, cnt, p->d_x, tol, max_iter, nullptr, res);
@@ -717,7 +717,7 @@ namespace mycel {
 int32_t solve_dispatch(mycel_problem* p, double* d_u, double tol, int max_iter, int precision,
                        const volatile int32_t* cancel, mycel_pcg_result* res) {
   if (precision == MYCEL_PRECISION_MIXED || precision == MYCEL_PRECISION_FP64_FACTORED ||
-      precision == MYCEL_PRECISION_FP64_MG) {
+      precision == MYCEL_PRECISION_FP64_MG || precision == MYCEL_PRECISION_MIXED_MG) {
     return refined_solve_entry(p, p->d_b, p->d_bnz, p->n_bnz, d_u, tol, max_iter, cancel, precision, res);
   }
   return pcg_solve_fp64(p, p->d_b, p->d_bnz, p->n_bnz, d_u, tol, max_iter, cancel, res);

@@ -1841,17 +1841,12 @@ __global__ void k_mg_stencil(MgDims d, const float* __restrict__ K, float* __res
     for (int ci = 0; ci < 3; ++ci) invd[3 * n + ci] = v[4 * ci] > 0.f ? 1.0f / v[4 * ci] : 0.0f;
 }
 
-// coarse-level product by node gather. mode 0: y = A x; 1: y = x + omega invd (r - A x) (one Jacobi sweep);
-// 2: y = r - A x on DOFs with a nonzero diagonal, 0 elsewhere
-__global__ void __launch_bounds__(256) k_mg_apply(MgDims d, const float* __restrict__ S, const float* __restrict__ x,
-                                                  const float* __restrict__ r, const float* __restrict__ invd,
-                                                  float* __restrict__ y, int mode, const float* __restrict__ om,
-                                                  const MixState* st) {
-  if (!mg_running(st)) return;
-  const float omega = mode == 1 ? *om : 0.0f;
-  const int64_t nn = mg_nn(d);
-  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (n >= nn) return;
+// coarse-level product at node n by gather. mode 0: y = A x; 1: y = x + omega invd (r - A x) (one Jacobi
+// sweep); 2: y = r - A x on DOFs with a nonzero diagonal, 0 elsewhere
+__device__ __forceinline__ void mg_apply_node(const MgDims& d, int64_t nn, int64_t n, const float* __restrict__ S,
+                                              const float* __restrict__ x, const float* __restrict__ r,
+                                              const float* __restrict__ invd, float* __restrict__ y, int mode,
+                                              float omega) {
   const int nx1 = d.nx + 1, ny1 = d.ny + 1;
   const int i = (int)(n % nx1), j = (int)((n / nx1) % ny1), k = (int)(n / ((int64_t)nx1 * ny1));
   float a0 = 0.f, a1 = 0.f, a2 = 0.f;
@@ -1878,6 +1873,16 @@ __global__ void __launch_bounds__(256) k_mg_apply(MgDims d, const float* __restr
   }
 }
 
+__global__ void __launch_bounds__(256) k_mg_apply(MgDims d, const float* __restrict__ S, const float* __restrict__ x,
+                                                  const float* __restrict__ r, const float* __restrict__ invd,
+                                                  float* __restrict__ y, int mode, const float* __restrict__ om,
+                                                  const MixState* st) {
+  if (!mg_running(st)) return;
+  const int64_t nn = mg_nn(d);
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n < nn) mg_apply_node(d, nn, n, S, x, r, invd, y, mode, mode == 1 ? *om : 0.0f);
+}
+
 // first sweep from x = 0 on a coarse level: x = omega invd r
 __global__ void k_mg_jacobi0(int64_t nd, const float* __restrict__ r, const float* __restrict__ invd,
                              float* __restrict__ x, const float* __restrict__ om, const MixState* st) {
@@ -1897,15 +1902,12 @@ __global__ void k_mg_jacobi_fine(int64_t n, const float* __restrict__ r, const f
     x[q] = fmaf(omega * invd[q], r[q] - t[q], x[q]);
 }
 
-// restriction r_c = W^T res of a level's residual. PAD: the voxel grid in the padded FP32 layout (row pitch
-// pitch), res = r - t; otherwise box layout, res = t. Coarse DOFs with a zero diagonal get 0.
+// restriction r_c = W^T res of a level's residual at coarse node n. PAD: the voxel grid in the padded FP32
+// layout (row pitch pitch), res = r - t; otherwise box layout, res = t. Coarse DOFs with a zero diagonal get 0.
 template <bool PAD>
-__global__ void k_mg_restrict(MgDims f, int pitch, const float* __restrict__ rf, const float* __restrict__ tf,
-                              MgDims c, const float* __restrict__ invdc, float* __restrict__ rc, const MixState* st) {
-  if (!mg_running(st)) return;
-  const int64_t nn = mg_nn(c);
-  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (n >= nn) return;
+__device__ __forceinline__ void mg_restrict_node(const MgDims& f, int pitch, const float* __restrict__ rf,
+                                                 const float* __restrict__ tf, const MgDims& c,
+                                                 const float* __restrict__ invdc, float* __restrict__ rc, int64_t n) {
   const int cx1 = c.nx + 1, cy1 = c.ny + 1;
   const int I = (int)(n % cx1), J = (int)((n / cx1) % cy1), K = (int)(n / ((int64_t)cx1 * cy1));
   const int pi = min(2 * I, f.nx), pj = min(2 * J, f.ny), pk = min(2 * K, f.nz);
@@ -1943,15 +1945,20 @@ __global__ void k_mg_restrict(MgDims f, int pitch, const float* __restrict__ rf,
   rc[3 * n + 2] = invdc[3 * n + 2] != 0.f ? a2 : 0.f;
 }
 
-// prolongation x_f += W x_c on the finer level's free DOFs. PAD: the voxel grid (padded FP32 layout, free =
-// node flag bit clear); otherwise box layout, free = nonzero diagonal.
 template <bool PAD>
-__global__ void k_mg_prolong(MgDims f, int pitch, const uint8_t* __restrict__ nf, const float* __restrict__ invdf,
-                             float* __restrict__ xf, MgDims c, const float* __restrict__ xc, const MixState* st) {
+__global__ void k_mg_restrict(MgDims f, int pitch, const float* __restrict__ rf, const float* __restrict__ tf,
+                              MgDims c, const float* __restrict__ invdc, float* __restrict__ rc, const MixState* st) {
   if (!mg_running(st)) return;
-  const int64_t nn = mg_nn(f);
   const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (n >= nn) return;
+  if (n < mg_nn(c)) mg_restrict_node<PAD>(f, pitch, rf, tf, c, invdc, rc, n);
+}
+
+// prolongation x_f += W x_c at fine node n, on the finer level's free DOFs. PAD: the voxel grid (padded FP32
+// layout, free = node flag bit clear); otherwise box layout, free = nonzero diagonal.
+template <bool PAD>
+__device__ __forceinline__ void mg_prolong_node(const MgDims& f, int pitch, const uint8_t* __restrict__ nf,
+                                                const float* __restrict__ invdf, float* __restrict__ xf,
+                                                const MgDims& c, const float* __restrict__ xc, int64_t n) {
   const int fx1 = f.nx + 1, fy1 = f.ny + 1;
   const int i = (int)(n % fx1), j = (int)((n / fx1) % fy1), k = (int)(n / ((int64_t)fx1 * fy1));
   // per axis: two coarse nodes with their weights (the second with weight 0 unless the fine node lies midway)
@@ -1988,6 +1995,14 @@ __global__ void k_mg_prolong(MgDims f, int pitch, const uint8_t* __restrict__ nf
     const bool fr = PAD ? !(nf[n] & (1 << cc)) : (invdf[3 * n + cc] != 0.0f);
     if (fr) xf[b + cc] += acc[cc];
   }
+}
+
+template <bool PAD>
+__global__ void k_mg_prolong(MgDims f, int pitch, const uint8_t* __restrict__ nf, const float* __restrict__ invdf,
+                             float* __restrict__ xf, MgDims c, const float* __restrict__ xc, const MixState* st) {
+  if (!mg_running(st)) return;
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n < mg_nn(f)) mg_prolong_node<PAD>(f, pitch, nf, invdf, xf, c, xc, n);
 }
 
 // coarsest level set-up (one CTA): the dense matrix from the level's stencil, inverted in place by Gauss-Jordan
@@ -2062,18 +2077,89 @@ __global__ void __launch_bounds__(1024) k_mg_coarse_setup(MgDims d, const float*
   }
 }
 
-// coarsest solve x = A^-1 r (one warp per row)
-__global__ void k_mg_coarse_solve(int n, const double* __restrict__ ainv, const float* __restrict__ r,
-                                  float* __restrict__ x, const MixState* st) {
+// The coarse levels from T down to the coarsest and back in one launch of one thread-block cluster: levels
+// this small cost more in separate launches than in work. The cluster's CTAs are co-scheduled, so a cluster
+// barrier separates the phases; all vectors stay in global memory (L2).
+constexpr int kMgTailCtas = 8, kMgTailThreads = 512;
+constexpr int64_t kMgTailMaxNodes = 2 * kMgTailCtas * kMgTailThreads;  // at most two nodes per thread
+
+struct MgTailLevel {
+  MgDims d;
+  int64_t nn;
+  const float* S;
+  const float* invd;
+  float *xa, *xb, *r, *t;
+};
+struct MgTail {
+  int T, L, sweeps, nc;
+  const double* ainv;
+  MgTailLevel lv[kMgMaxLevels];
+};
+
+__device__ __forceinline__ void mg_cluster_sync() {
+  asm volatile("barrier.cluster.arrive.release;\n" ::: "memory");
+  asm volatile("barrier.cluster.wait.acquire;\n" ::: "memory");
+}
+
+// Levels T .. L-1 of the V-cycle: from r of level T (restricted by the caller) to the smoothed correction of
+// level T, left in its xa.
+__global__ void __cluster_dims__(kMgTailCtas, 1, 1) __launch_bounds__(kMgTailThreads)
+    k_mg_tail(const __grid_constant__ MgTail tl, const float* __restrict__ om, const MixState* st) {
   if (!mg_running(st)) return;
-  const int lane = threadIdx.x & 31;
-  for (int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < n; row += (gridDim.x * blockDim.x) >> 5) {
-    double s = 0.0;
-    for (int col = lane; col < n; col += 32) s = fma(ainv[(int64_t)row * n + col], (double)r[col], s);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) x[row] = (float)s;
+  const int64_t gt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x, gs = (int64_t)gridDim.x * blockDim.x;
+  float* xc[kMgMaxLevels];
+  for (int l = tl.T; l < tl.L - 1; ++l) {
+    const MgTailLevel& v = tl.lv[l];
+    const MgTailLevel& cv = tl.lv[l + 1];
+    const float w = om[l];
+    float *x = v.xa, *o = v.xb;
+    for (int64_t q = gt; q < 3 * v.nn; q += gs) x[q] = w * v.invd[q] * v.r[q];
+    mg_cluster_sync();
+    for (int k = 1; k < tl.sweeps; ++k) {
+      for (int64_t n = gt; n < v.nn; n += gs) mg_apply_node(v.d, v.nn, n, v.S, x, v.r, v.invd, o, 1, w);
+      mg_cluster_sync();
+      float* tmp = x;
+      x = o;
+      o = tmp;
+    }
+    for (int64_t n = gt; n < v.nn; n += gs) mg_apply_node(v.d, v.nn, n, v.S, x, v.r, v.invd, v.t, 2, 0.0f);
+    mg_cluster_sync();
+    for (int64_t n = gt; n < cv.nn; n += gs) mg_restrict_node<false>(v.d, 0, nullptr, v.t, cv.d, cv.invd, cv.r, n);
+    mg_cluster_sync();
+    xc[l] = x;
   }
+  {  // coarsest level: x = A^-1 r, one warp per row
+    const MgTailLevel& v = tl.lv[tl.L - 1];
+    const int lane = threadIdx.x & 31;
+    for (int64_t row = gt >> 5; row < tl.nc; row += gs >> 5) {
+      double acc = 0.0;
+      for (int col = lane; col < tl.nc; col += 32) acc = fma(tl.ainv[row * tl.nc + col], (double)v.r[col], acc);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+      if (lane == 0) v.xa[row] = (float)acc;
+    }
+    mg_cluster_sync();
+    xc[tl.L - 1] = v.xa;
+  }
+  for (int l = tl.L - 2; l >= tl.T; --l) {
+    const MgTailLevel& v = tl.lv[l];
+    const float w = om[l];
+    float* x = xc[l];
+    float* o = x == v.xa ? v.xb : v.xa;
+    for (int64_t n = gt; n < v.nn; n += gs) mg_prolong_node<false>(v.d, 0, nullptr, v.invd, x, tl.lv[l + 1].d, xc[l + 1], n);
+    mg_cluster_sync();
+    for (int k = 0; k < tl.sweeps; ++k) {
+      for (int64_t n = gt; n < v.nn; n += gs) mg_apply_node(v.d, v.nn, n, v.S, x, v.r, v.invd, o, 1, w);
+      mg_cluster_sync();
+      float* tmp = x;
+      x = o;
+      o = tmp;
+    }
+    xc[l] = x;
+  }
+  const MgTailLevel& vt = tl.lv[tl.T];
+  if (xc[tl.T] != vt.xa)
+    for (int64_t q = gt; q < 3 * vt.nn; q += gs) vt.xa[q] = xc[tl.T][q];
 }
 
 // Outer step, part 1. mode 0: x += alpha p, r -= alpha q (FP64, padded layout), ||r|| against the stop and
@@ -2121,35 +2207,11 @@ __global__ void __launch_bounds__(kT) k_mg_enter(GridDims g, double* __restrict_
   else if (st->iter >= st->max_iter) st->status = MIX_MAXITER;
 }
 
-// Outer step, part 2: the voxel level's last Jacobi sweep written as the FP64 preconditioned residual
-// z = xf + omega invd (rf - tf) (tf = A xf), then (z, r), (z, A p) and (r, r) with fixed-order sums.
-// mode 0: beta = -alpha (z, A p) / rho, rho = (z, r). mode 1 (after a true-residual replacement, direction
-// kept): the same beta, new replacement threshold. mode 2 (start): rho, next direction p = z.
-__global__ void __launch_bounds__(kT) k_mg_exit(GridDims g, const float* __restrict__ rf, const float* __restrict__ tf,
-                                                const float* __restrict__ xf, const float* __restrict__ invdf,
-                                                const double* __restrict__ r, const double* __restrict__ q,
-                                                double* __restrict__ z, const float* __restrict__ om, MixState* st,
-                                                double* part, int mode) {
-  __shared__ double sh[32];
-  if (!mg_running(st)) return;
-  const float omega = *om;
-  const int rl = 3 * g.nx1;
-  const int64_t total = (int64_t)g.ny1 * g.nz1 * rl;
-  double zr = 0.0, zq = 0.0, rr = 0.0;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t row = i / rl;
-    const int t = (int)(i - row * rl);
-    const int64_t a = (int64_t)g.rp64 * row + t, b = (int64_t)g.rp * row + t;
-    const double zv = (double)fmaf(omega * invdf[b], rf[b] - tf[b], xf[b]);
-    const double rv = r[a];
-    z[a] = zv;
-    zr += zv * rv;
-    zq += zv * q[a];
-    rr += rv * rv;
-  }
-  const double b1 = bsum(zr, sh);
-  const double b2 = bsum(zq, sh);
-  const double b3 = bsum(rr, sh);
+// End of an outer step (CTA partials of (z, r), (z, A p), (r, r) in b1..b3, valid in thread 0): fixed-order
+// sums by the last CTA. mode 0: beta = -alpha (z, A p) / rho, rho = (z, r). mode 1 (after a true-residual
+// replacement, direction kept): the same beta, new replacement threshold. mode 2 (start): rho, next direction
+// p = z.
+__device__ __forceinline__ void mg_exit_tail(double b1, double b2, double b3, MixState* st, double* part, int mode) {
   if (threadIdx.x == 0) {
     part[blockIdx.x] = b1;
     part[gridDim.x + blockIdx.x] = b2;
@@ -2186,6 +2248,112 @@ __global__ void __launch_bounds__(kT) k_mg_exit(GridDims g, const float* __restr
     }
   }
   st->rho0 = szr;
+}
+
+// Outer step, part 2: the voxel level's last Jacobi sweep written as the FP64 preconditioned residual
+// z = xf + omega invd (rf - tf) (tf = A xf), then (z, r), (z, A p) and (r, r) (mg_exit_tail).
+__global__ void __launch_bounds__(kT) k_mg_exit(GridDims g, const float* __restrict__ rf, const float* __restrict__ tf,
+                                                const float* __restrict__ xf, const float* __restrict__ invdf,
+                                                const double* __restrict__ r, const double* __restrict__ q,
+                                                double* __restrict__ z, const float* __restrict__ om, MixState* st,
+                                                double* part, int mode) {
+  __shared__ double sh[32];
+  if (!mg_running(st)) return;
+  const float omega = *om;
+  const int rl = 3 * g.nx1;
+  const int64_t total = (int64_t)g.ny1 * g.nz1 * rl;
+  double zr = 0.0, zq = 0.0, rr = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t row = i / rl;
+    const int t = (int)(i - row * rl);
+    const int64_t a = (int64_t)g.rp64 * row + t, b = (int64_t)g.rp * row + t;
+    const double zv = (double)fmaf(omega * invdf[b], rf[b] - tf[b], xf[b]);
+    const double rv = r[a];
+    z[a] = zv;
+    zr += zv * rv;
+    zq += zv * q[a];
+    rr += rv * rv;
+  }
+  const double b1 = bsum(zr, sh);
+  const double b2 = bsum(zq, sh);
+  const double b3 = bsum(rr, sh);
+  mg_exit_tail(b1, b2, b3, st, part, mode);
+}
+
+// The same two parts for the FP32 outer iteration (mixed multigrid form): all vectors in the padded FP32 layout,
+// the voxel level's residual is the outer residual r itself and its smoothed correction is built in place in z
+// (a mapped matvec input). Dots accumulate in FP64.
+__global__ void __launch_bounds__(kT) k_mg_enter32(int64_t n, float* __restrict__ x, float* __restrict__ r,
+                                                   const float* __restrict__ p, const float* __restrict__ q,
+                                                   const float* __restrict__ invd, float* __restrict__ xf,
+                                                   const float* __restrict__ om, MixState* st, double* part, int mode) {
+  __shared__ double sh[32];
+  if (!mg_running(st)) return;
+  const float alpha = (float)st->alpha;
+  const float omega = *om;
+  double rr = 0.0;
+  const int64_t n4 = n >> 2;  // n is a multiple of 4 (row pitch)
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n4; i += (int64_t)gridDim.x * blockDim.x) {
+    float4 rv = reinterpret_cast<const float4*>(r)[i];
+    const float4 iv = reinterpret_cast<const float4*>(invd)[i];
+    if (mode == 0) {
+      float4 xv = reinterpret_cast<const float4*>(x)[i];
+      const float4 pv = reinterpret_cast<const float4*>(p)[i];
+      const float4 qv = reinterpret_cast<const float4*>(q)[i];
+      xv.x = fmaf(alpha, pv.x, xv.x); xv.y = fmaf(alpha, pv.y, xv.y);
+      xv.z = fmaf(alpha, pv.z, xv.z); xv.w = fmaf(alpha, pv.w, xv.w);
+      rv.x = fmaf(-alpha, qv.x, rv.x); rv.y = fmaf(-alpha, qv.y, rv.y);
+      rv.z = fmaf(-alpha, qv.z, rv.z); rv.w = fmaf(-alpha, qv.w, rv.w);
+      reinterpret_cast<float4*>(x)[i] = xv;
+      reinterpret_cast<float4*>(r)[i] = rv;
+      rr += (double)rv.x * rv.x + (double)rv.y * rv.y + (double)rv.z * rv.z + (double)rv.w * rv.w;
+    }
+    reinterpret_cast<float4*>(xf)[i] =
+        make_float4(omega * iv.x * rv.x, omega * iv.y * rv.y, omega * iv.z * rv.z, omega * iv.w * rv.w);
+  }
+  if (mode != 0) return;
+  const double br = bsum(rr, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = br;
+  if (!elect_last32(&st->counter)) return;
+  if (threadIdx.x >= 32) return;
+  const double s = warp_sum_parts(part, gridDim.x);
+  if (threadIdx.x != 0) return;
+  st->counter = 0;
+  const double rn = sqrt(s);
+  st->rn = rn;
+  st->iter += 1;
+  if (rn <= st->target || rn <= st->flush_at) st->status = MIX_FLUSH;
+  else if (st->iter >= st->max_iter) st->status = MIX_MAXITER;
+}
+
+__global__ void __launch_bounds__(kT) k_mg_exit32(int64_t n, const float* __restrict__ r, const float* __restrict__ tf,
+                                                  float* __restrict__ z, const float* __restrict__ invd,
+                                                  const float* __restrict__ q, const float* __restrict__ om,
+                                                  MixState* st, double* part, int mode) {
+  __shared__ double sh[32];
+  if (!mg_running(st)) return;
+  const float omega = *om;
+  double zr = 0.0, zq = 0.0, rr = 0.0;
+  const int64_t n4 = n >> 2;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n4; i += (int64_t)gridDim.x * blockDim.x) {
+    const float4 rv = reinterpret_cast<const float4*>(r)[i];
+    const float4 tv = reinterpret_cast<const float4*>(tf)[i];
+    const float4 iv = reinterpret_cast<const float4*>(invd)[i];
+    const float4 qv = reinterpret_cast<const float4*>(q)[i];
+    float4 zv = reinterpret_cast<const float4*>(z)[i];
+    zv.x = fmaf(omega * iv.x, rv.x - tv.x, zv.x);
+    zv.y = fmaf(omega * iv.y, rv.y - tv.y, zv.y);
+    zv.z = fmaf(omega * iv.z, rv.z - tv.z, zv.z);
+    zv.w = fmaf(omega * iv.w, rv.w - tv.w, zv.w);
+    reinterpret_cast<float4*>(z)[i] = zv;
+    zr += (double)zv.x * rv.x + (double)zv.y * rv.y + (double)zv.z * rv.z + (double)zv.w * rv.w;
+    zq += (double)zv.x * qv.x + (double)zv.y * qv.y + (double)zv.z * qv.z + (double)zv.w * qv.w;
+    rr += (double)rv.x * rv.x + (double)rv.y * rv.y + (double)rv.z * rv.z + (double)rv.w * rv.w;
+  }
+  const double b1 = bsum(zr, sh);
+  const double b2 = bsum(zq, sh);
+  const double b3 = bsum(rr, sh);
+  mg_exit_tail(b1, b2, b3, st, part, mode);
 }
 
 // Power iteration for lambda_max(D^-1 A) of a level: a fixed pseudo-random start on DOFs with a nonzero
@@ -2365,9 +2533,16 @@ struct MgHier {
   MgScratch* sc = nullptr;  // per-level damping, power-iteration norm and counter (device)
   int sweeps = 1;
   int per_iter = 0;  // kernel launches per outer iteration
-  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};    // FP64 outer iteration chunks
   int graph_profiled = 0;
   cudaEvent_t ev[2][2] = {};
+  cudaGraphExec_t graph32[2] = {nullptr, nullptr};  // FP32 outer iteration chunks (mixed multigrid form)
+  int graph32_profiled = 0;
+  cudaEvent_t ev32[2][2] = {};
+  float* f_t = nullptr;  // FP32 outer form: A x of the voxel level's smoothing (padded FP32 layout)
+  int T = 1;             // first level handled by the cluster kernel k_mg_tail
+  MgTail tail{};
+  bool prefers_f64 = false;  // an FP32 outer solve of this problem stalled: later ones start in FP64
   std::vector<void*> bufs;
 };
 
@@ -2393,6 +2568,8 @@ int64_t mg_device_bytes(int nx, int ny, int nz) {
   int64_t b = 0;
   for (int l = 1; l < L; ++l) b += 4 * (243 + 15) * mg_nn(lv[l]) + 6 * 64;
   b += sizeof(MgScratch) + 64 + 4 * 8 * 576 + 64 + (int64_t)lv[1].nx * lv[1].ny * lv[1].nz + 64;
+  const int64_t rp = (3 * (int64_t)(nx + 1) + 3) & ~int64_t(3);  // FP32 row pitch of the voxel level
+  b += 4 * rp * (ny + 1) * (nz + 1) + 64;                         // f_t
   b += 4 * 576 * (int64_t)lv[1].nx * lv[1].ny * lv[1].nz + 64;
   if (L > 2) b += 4 * 576 * (int64_t)lv[2].nx * lv[2].ny * lv[2].nz + 64;
   b += 8 * 9 * mg_nn(lv[L - 1]) * mg_nn(lv[L - 1]) + 64;
@@ -2404,8 +2581,11 @@ void mg_release(mycel_problem* p) {
   if (!mg) return;
   for (int k = 0; k < 2; ++k) {
     if (mg->graph[k]) cudaGraphExecDestroy(mg->graph[k]);
-    for (int j = 0; j < 2; ++j)
+    if (mg->graph32[k]) cudaGraphExecDestroy(mg->graph32[k]);
+    for (int j = 0; j < 2; ++j) {
       if (mg->ev[k][j]) cudaEventDestroy(mg->ev[k][j]);
+      if (mg->ev32[k][j]) cudaEventDestroy(mg->ev32[k][j]);
+    }
   }
   for (void* b : mg->bufs) cudaFreeAsync(b, p->ctx->stream);
   delete mg;
@@ -2461,6 +2641,7 @@ static int32_t mg_ensure(mycel_problem* p, bool* available) {
   const int64_t nc = mg->lv[L - 1].nd;
   mg->ainv = (double*)alloc(sizeof(double) * nc * nc);
   mg->sc = (MgScratch*)alloc(sizeof(MgScratch));
+  mg->f_t = (float*)alloc(sizeof(float) * (size_t)p->g.n32);
   mg->G = (float*)alloc(sizeof(float) * 8 * 576);
   mg->special = (uint8_t*)alloc((size_t)dims[1].nx * dims[1].ny * dims[1].nz);
   if (!oom) {  // G_s = W_s^T KE W_s for an interior coarse element (all sub-elements present), in FP64
@@ -2487,9 +2668,35 @@ static int32_t mg_ensure(mycel_problem* p, bool* available) {
     cudaMemcpyAsync(mg->G, G.data(), sizeof(float) * G.size(), cudaMemcpyHostToDevice, s);
     cudaStreamSynchronize(s);
   }
-  // launches per outer iteration: matvec, k_mg_enter, the V-cycle (as issued by mg_vcycle), k_mg_exit
-  const int sw = mg->sweeps;
-  const int cycle = 4 * (sw - 1) + 2 + (L - 2) * (2 + sw) + 1 + (L - 2) * (1 + sw) + 1 + 1;
+  {  // the cluster kernel must fit: kMgTailCtas CTAs of kMgTailThreads threads co-resident
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(kMgTailCtas);
+    cfg.blockDim = dim3(kMgTailThreads);
+    int nclusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&nclusters, k_mg_tail, &cfg) != cudaSuccess || nclusters < 1) {
+      cudaGetLastError();
+      return set_error(p->ctx, MYCEL_E_DEVICE, "multigrid: the coarse-level cluster kernel cannot be scheduled");
+    }
+  }
+  // levels T .. L-1 in one cluster launch: T is the first coarse level of at most kMgTailMaxNodes nodes
+  mg->T = L - 1;
+  for (int l = 1; l < L; ++l)
+    if (mg->lv[l].nn <= kMgTailMaxNodes) {
+      mg->T = l;
+      break;
+    }
+  mg->tail.T = mg->T;
+  mg->tail.L = L;
+  mg->tail.sweeps = mg->sweeps;
+  mg->tail.nc = (int)nc;
+  mg->tail.ainv = mg->ainv;
+  for (int l = 1; l < L; ++l) {
+    const MgLevel& v = mg->lv[l];
+    mg->tail.lv[l] = {v.d, v.nn, v.S, v.invd, v.xa, v.xb, v.r, v.t};
+  }
+  // launches per outer iteration: matvec, k_mg_enter*, the V-cycle (as issued by mg_vcycle), k_mg_exit*
+  const int sw = mg->sweeps, T = mg->T;
+  const int cycle = 4 * (sw - 1) + 2 + (T - 1) * (2 + sw) + 1 + (T - 1) * (1 + sw) + 1 + 1;
   mg->per_iter = 3 + cycle;
   p->mg = mg;
   if (oom) return set_error(p->ctx, MYCEL_E_OOM, "out of device memory for the multigrid hierarchy");
@@ -2545,27 +2752,26 @@ static void mg_setup(mycel_problem* p) {
   p->ctx->launches += nl;
 }
 
-// One V-cycle from the voxel level's residual f_r and first sweep f_p0 (written by k_mg_enter) up to
-// f_ap = A f_p0 before the last sweep (done by k_mg_exit). Returns the kernels launched.
-static int mg_vcycle(mycel_problem* p, cudaStream_t s, MixState* st) {
+// One V-cycle from the voxel level's residual rf and first sweep xf (written by k_mg_enter*) up to tf = A xf
+// before the last sweep (done by k_mg_exit*). xf is a mapped FP32 matvec input. Returns the kernels launched.
+static int mg_vcycle(mycel_problem* p, cudaStream_t s, MixState* st, float* rf, float* xf, float* tf) {
   MgHier* mg = p->mg;
   MgLevel* lv = mg->lv;
   const GridDims& g = p->g;
   const float* om = mg->sc->omega;  // device: damping of level l at om + l
   const int sb = stream_blocks(p);
   int nl = 0;
-  auto fine_mv = [&] { launch_mv32_variant<0>(p, s, p->f_p0, nullptr, nullptr, nullptr, p->f_ap, 1, st, nullptr); };
+  auto fine_mv = [&] { launch_mv32_variant<0>(p, s, xf, nullptr, nullptr, nullptr, tf, 1, st, nullptr); };
   for (int k = 1; k < mg->sweeps; ++k) {
     fine_mv();
-    k_mg_jacobi_fine<<<sb, kT, 0, s>>>(g.n32, p->f_r, p->f_ap, p->d_invdf, p->f_p0, om, st);
+    k_mg_jacobi_fine<<<sb, kT, 0, s>>>(g.n32, rf, tf, p->d_invdf, xf, om, st);
     nl += 2;
   }
   fine_mv();
-  k_mg_restrict<true><<<mg_blocks(lv[1].nn), 256, 0, s>>>(lv[0].d, g.rp, p->f_r, p->f_ap, lv[1].d, lv[1].invd,
-                                                          lv[1].r, st);
+  k_mg_restrict<true><<<mg_blocks(lv[1].nn), 256, 0, s>>>(lv[0].d, g.rp, rf, tf, lv[1].d, lv[1].invd, lv[1].r, st);
   nl += 2;
   float* xc[kMgMaxLevels] = {};
-  for (int l = 1; l < mg->L - 1; ++l) {
+  for (int l = 1; l < mg->T; ++l) {
     MgLevel& v = lv[l];
     float *x = v.xa, *o = v.xb;
     k_mg_jacobi0<<<mg_blocks(v.nd), 256, 0, s>>>(v.nd, v.r, v.invd, x, om + l, st);
@@ -2579,11 +2785,10 @@ static int mg_vcycle(mycel_problem* p, cudaStream_t s, MixState* st) {
     xc[l] = x;
     nl += 2 + mg->sweeps;
   }
-  MgLevel& cl = lv[mg->L - 1];
-  k_mg_coarse_solve<<<mg_blocks(32 * cl.nd), 256, 0, s>>>((int)cl.nd, mg->ainv, cl.r, cl.xa, st);
-  xc[mg->L - 1] = cl.xa;
+  k_mg_tail<<<kMgTailCtas, kMgTailThreads, 0, s>>>(mg->tail, om, st);
+  xc[mg->T] = lv[mg->T].xa;
   nl++;
-  for (int l = mg->L - 2; l >= 1; --l) {
+  for (int l = mg->T - 1; l >= 1; --l) {
     MgLevel& v = lv[l];
     float* x = xc[l];
     float* o = x == v.xa ? v.xb : v.xa;
@@ -2595,12 +2800,11 @@ static int mg_vcycle(mycel_problem* p, cudaStream_t s, MixState* st) {
     xc[l] = x;
     nl += 1 + mg->sweeps;
   }
-  k_mg_prolong<true><<<mg_blocks(lv[0].nn), 256, 0, s>>>(lv[0].d, g.rp, p->d_nflags, nullptr, p->f_p0, lv[1].d,
-                                                         xc[1], st);
+  k_mg_prolong<true><<<mg_blocks(lv[0].nn), 256, 0, s>>>(lv[0].d, g.rp, p->d_nflags, nullptr, xf, lv[1].d, xc[1], st);
   nl++;
   for (int k = 1; k < mg->sweeps; ++k) {
     fine_mv();
-    k_mg_jacobi_fine<<<sb, kT, 0, s>>>(g.n32, p->f_r, p->f_ap, p->d_invdf, p->f_p0, om, st);
+    k_mg_jacobi_fine<<<sb, kT, 0, s>>>(g.n32, rf, tf, p->d_invdf, xf, om, st);
     nl += 2;
   }
   fine_mv();
@@ -2608,21 +2812,30 @@ static int mg_vcycle(mycel_problem* p, cudaStream_t s, MixState* st) {
 }
 
 // The outer step after the matvec (mode 0), or the preconditioned residual after a start (2) or a true-residual
-// replacement (1): k_mg_enter, the V-cycle, k_mg_exit. Returns the kernels launched.
-static int launch_mg_step(mycel_problem* p, cudaStream_t s, const double* pcur, int mode) {
+// replacement (1): k_mg_enter*, the V-cycle, k_mg_exit*. FP64 outer iteration: the voxel level works on f_r,
+// f_p0, f_ap; FP32 outer iteration: on the outer r (f_r) and z (f_z) and f_t. Returns the kernels launched.
+static int launch_mg_step(mycel_problem* p, cudaStream_t s, const void* pcur, int mode, bool f64) {
   MgHier* mg = p->mg;
   MixState* st = mix_state(p);
   const int sb = stream_blocks(p);
+  const float* om = mg->sc->omega;
   int nl = 0;
   if (mode == 1) {
     k_mix_set<<<1, 1, 0, s>>>(st, MIX_RUNNING);
     nl++;
   }
-  k_mg_enter<<<sb, kT, 0, s>>>(p->g, p->g_x, p->g_r, pcur, p->g_ap, p->d_invdf, p->f_r, p->f_p0, mg->sc->omega, st,
-                               p->d_part2, mode);
-  nl += 1 + mg_vcycle(p, s, st);
-  k_mg_exit<<<sb, kT, 0, s>>>(p->g, p->f_r, p->f_ap, p->f_p0, p->d_invdf, p->g_r, p->g_ap, p->g_z, mg->sc->omega, st,
-                              p->d_part2, mode);
+  if (f64) {
+    k_mg_enter<<<sb, kT, 0, s>>>(p->g, p->g_x, p->g_r, (const double*)pcur, p->g_ap, p->d_invdf, p->f_r, p->f_p0, om,
+                                 st, p->d_part2, mode);
+    nl += 1 + mg_vcycle(p, s, st, p->f_r, p->f_p0, p->f_ap);
+    k_mg_exit<<<sb, kT, 0, s>>>(p->g, p->f_r, p->f_ap, p->f_p0, p->d_invdf, p->g_r, p->g_ap, p->g_z, om, st,
+                                p->d_part2, mode);
+  } else {
+    k_mg_enter32<<<sb, kT, 0, s>>>(p->g.n32, p->f_x, p->f_r, (const float*)pcur, p->f_ap, p->d_invdf, p->f_z, om, st,
+                                   p->d_part2, mode);
+    nl += 1 + mg_vcycle(p, s, st, p->f_r, p->f_z, mg->f_t);
+    k_mg_exit32<<<sb, kT, 0, s>>>(p->g.n32, p->f_r, mg->f_t, p->f_z, p->d_invdf, p->f_ap, om, st, p->d_part2, mode);
+  }
   return nl + 1;
 }
 
@@ -2653,12 +2866,17 @@ static InnerForm inner_form(mycel_problem* p, bool f64) {
           p->pcg32_graph, &p->pcg32_graph_profiled, p->prof_ev, 0, kFlushFactor, 16, 2};
 }
 
-// multigrid form: the fast FP64 form's vectors and matvec; short chunks, since an iteration past convergence
-// still launches its whole V-cycle (whose kernels then return at once)
-static InnerForm inner_form_mg(mycel_problem* p) {
+// multigrid forms: the fast FP64 form's vectors and matvec (f64), or the mixed form's (FP32, replacement after
+// a 1e-3 drop of the recursive residual: a multigrid-preconditioned FP32 recurrence stays close to the true
+// residual that far); short chunks, since an iteration past convergence still launches its whole V-cycle
+// (whose kernels then return at once)
+static InnerForm inner_form_mg(mycel_problem* p, bool f64) {
   MgHier* mg = p->mg;
-  return {true, true, p->g_x, p->g_r, p->g_z, p->g_p0, p->g_p1, p->g_ap, p->g_invd, p->g.n64, sizeof(double),
-          mg->graph, &mg->graph_profiled, mg->ev, 2, 1e-4, 4, mg->per_iter};
+  if (f64)
+    return {true, true, p->g_x, p->g_r, p->g_z, p->g_p0, p->g_p1, p->g_ap, p->g_invd, p->g.n64, sizeof(double),
+            mg->graph, &mg->graph_profiled, mg->ev, 2, 1e-4, 2, mg->per_iter};
+  return {false, true, p->f_x, p->f_r, p->f_z, p->f_p0, p->f_p1, p->f_ap, p->d_invdf, p->g.n32, sizeof(float),
+          mg->graph32, &mg->graph32_profiled, mg->ev32, 0, 1e-3, 2, mg->per_iter};
 }
 
 static void launch_inner_mv(mycel_problem* p, const InnerForm& F, cudaStream_t s, void* pold, void* pcur) {
@@ -2672,7 +2890,7 @@ static void launch_inner_mv(mycel_problem* p, const InnerForm& F, cudaStream_t s
 
 static int launch_inner_xr(mycel_problem* p, const InnerForm& F, cudaStream_t s, void* pcur, int mode) {
   const int sb = stream_blocks(p);
-  if (F.mg) return launch_mg_step(p, s, (const double*)pcur, mode);
+  if (F.mg) return launch_mg_step(p, s, pcur, mode, F.f64);
   if (F.f64)
     k_xr64<<<sb, kT, 0, s>>>(F.n, (double*)F.x, (double*)F.r, (double*)F.z, (const double*)pcur, (const double*)F.ap,
                              (const double*)F.invd, mix_state(p), p->d_part2, mode);
@@ -2792,8 +3010,10 @@ static int32_t refined_loop(mycel_problem* p, const InnerForm& F, const double* 
   int iter_at_resume = 0;
   // stall watch: each refinement cycle gains log10(1/flush factor) orders of the true residual. CG's later
   // orders cost more than its first ones, so a cycle counts as stalled (FP32 CG on a badly conditioned system)
-  // only once it has run longer than 3x all earlier cycles together, and at least 2000 iterations.
-  int64_t cycle_limit = INT64_MAX;
+  // only once it has run longer than 3x all earlier cycles together, and at least 2000 iterations. A multigrid
+  // form gains its orders in tens of iterations: there the floor is 300, and it also bounds the first cycle.
+  const int64_t stall_floor = F.mg ? 300 : 2000;
+  int64_t cycle_limit = F.mg ? stall_floor : INT64_MAX;
   for (;;) {
     // pipeline: chunk k is queued while the status after chunk k-1 is read
     int64_t k = 0;
@@ -2858,7 +3078,7 @@ static int32_t refined_loop(mycel_problem* p, const InnerForm& F, const double* 
       out->ok = true;
       break;
     }
-    cycle_limit = std::max<int64_t>(2000, 3 * (int64_t)out->iterations);
+    cycle_limit = std::max<int64_t>(stall_floor, 3 * (int64_t)out->iterations);
     if (out->stalled || status != MIX_FLUSH || out->iterations >= max_iter) break;
     c->launches += launch_inner_xr(p, F, s, F.p0, 1);
     iter_at_resume = out->iterations;
@@ -2871,6 +3091,8 @@ static int32_t refined_loop(mycel_problem* p, const InnerForm& F, const double* 
 // in the fast FP64 form from the refined u, and finally (should that fail too) in the plain FP64 PCG.
 // MYCEL_PRECISION_FP64_FACTORED: the fast FP64 form, then the plain FP64 PCG if it does not converge.
 // MYCEL_PRECISION_FP64_MG: the multigrid form (where the grid coarsens), then as MYCEL_PRECISION_FP64_FACTORED.
+// MYCEL_PRECISION_MIXED_MG: the multigrid form with FP32 outer iteration and FP64 refinement, then as
+// MYCEL_PRECISION_FP64_MG.
 int32_t refined_solve_entry(mycel_problem* p, const double* d_b, const int32_t* d_nz, int32_t n_nz, double* d_u,
                             double tol, int max_iter, const volatile int32_t* cancel, int precision,
                             mycel_pcg_result* res) {
@@ -2886,7 +3108,7 @@ int32_t refined_solve_entry(mycel_problem* p, const double* d_b, const int32_t* 
   int32_t st = ensure_pcg_workspace(p);
   if (st) return st;
   const bool mixed = precision == MYCEL_PRECISION_MIXED;
-  const bool mgp = precision == MYCEL_PRECISION_FP64_MG;
+  const bool mgp = precision == MYCEL_PRECISION_FP64_MG || precision == MYCEL_PRECISION_MIXED_MG;
   if ((mixed || mgp) && (st = ensure_mixed(p))) return st;
   if ((st = ensure_f64f(p))) return st;  // every refined form measures its true residual with the FP64 operator
   double* saved_b = p->d_b;
@@ -2916,21 +3138,37 @@ int32_t refined_solve_entry(mycel_problem* p, const double* d_b, const int32_t* 
   }
   const bool verbose = std::getenv("MYCEL_VERBOSE") != nullptr;
   MYCEL_CUDA(c, cudaMemsetAsync(p->d_err, 0, sizeof(int), s));  // bounded-wait failures of this solve only
-  LoopOut l32, l64, lmg;
+  LoopOut l32, l64, lmg, lmg32;
   bool ok = false;
   double rel = 0.0;
   bool ran_mg = false;
   if (mgp) {
     bool avail = false;
-    if ((st = ensure_f64f(p)) || (st = resolve_mv32(p)) || (st = mg_ensure(p, &avail))) return st;
+    if ((st = resolve_mv32(p)) || (st = mg_ensure(p, &avail))) return st;
     if (avail) {
       ran_mg = true;
       mg_setup(p);
-      if ((st = refined_loop(p, inner_form_mg(p), d_b, d_u, bnorm, tol, max_iter, cancel, false, verbose, &lmg)))
-        return st;
-      ok = lmg.ok;
-      rel = lmg.rel;
-      if (ok && lmg.iterations == 0 && lmg.flushes == 0)
+      // MYCEL_PRECISION_MIXED_MG: the FP32 outer iteration first (unless one of this problem's solves stalled
+      // in it), then the FP64 outer iteration from the refined u
+      if (precision == MYCEL_PRECISION_MIXED_MG && !p->mg->prefers_f64) {
+        if ((st = refined_loop(p, inner_form_mg(p, false), d_b, d_u, bnorm, tol, max_iter, cancel, true, verbose,
+                               &lmg32)))
+          return st;
+        ok = lmg32.ok;
+        rel = lmg32.rel;
+        if (lmg32.stalled) p->mg->prefers_f64 = true;
+        if (!ok && verbose)
+          std::fprintf(stderr, "mycel: FP32 multigrid solve %s after %d iterations (%.3e); FP64 multigrid next\n",
+                       lmg32.stalled ? "stalled" : "not converged", lmg32.iterations, lmg32.rel);
+      }
+      if (!ok) {
+        const int budget = lmg32.iterations ? std::max(max_iter - lmg32.iterations, max_iter / 2) : max_iter;
+        if ((st = refined_loop(p, inner_form_mg(p, true), d_b, d_u, bnorm, tol, budget, cancel, false, verbose, &lmg)))
+          return st;
+        ok = lmg.ok;
+        rel = lmg.rel;
+      }
+      if (ok && lmg.iterations + lmg32.iterations == 0 && lmg.flushes + lmg32.flushes == 0)
         std::snprintf(res->message, sizeof res->message, "Initial guess already converged.");
     }
   }
@@ -2994,6 +3232,9 @@ int32_t refined_solve_entry(mycel_problem* p, const double* d_b, const int32_t* 
   if (mixed) {
     res->inner_iterations = l32.iterations;
     res->fallback_iterations = l64.iterations + plain_iter;
+  } else if (precision == MYCEL_PRECISION_MIXED_MG) {
+    res->inner_iterations = lmg32.iterations;
+    res->fallback_iterations = lmg.iterations + l64.iterations + plain_iter;
   } else if (mgp) {
     res->inner_iterations = lmg.iterations;
     res->fallback_iterations = l64.iterations + plain_iter;
@@ -3002,7 +3243,7 @@ int32_t refined_solve_entry(mycel_problem* p, const double* d_b, const int32_t* 
     res->fallback_iterations = plain_iter;
   }
   res->iterations = res->inner_iterations + res->fallback_iterations;
-  res->refinement_steps = l32.flushes + l64.flushes + lmg.flushes;
+  res->refinement_steps = l32.flushes + l64.flushes + lmg.flushes + lmg32.flushes;
   res->final_residual = rel;
   res->converged = ok ? 1 : 0;
   if (!ok)

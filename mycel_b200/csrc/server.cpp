@@ -110,7 +110,7 @@ static int64_t job_bytes(const mycel_grid& gr, int64_t n_active, int64_t n_fixed
   const int64_t nb = (nd + 8191) / 8192;
   b += 5 * al16(8 * nd) + al16(8 * (2 * nb + 64)) + al16(sizeof(mycel::PcgState));
   // mixed workspace (6 FP32 vectors) and the fast FP64 workspace (7 FP64 vectors) a mixed solve escalates to
-  const bool mg = o.precision == MYCEL_PRECISION_FP64_MG;
+  const bool mg = o.precision == MYCEL_PRECISION_FP64_MG || o.precision == MYCEL_PRECISION_MIXED_MG;
   if (o.precision == MYCEL_PRECISION_MIXED || mg) b += 6 * (4 * g.n32 + 64);
   if (o.precision == MYCEL_PRECISION_MIXED || o.precision == MYCEL_PRECISION_FP64_FACTORED || mg)
     b += 7 * (8 * g.n64 + 64);

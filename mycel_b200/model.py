@@ -217,7 +217,10 @@ class StaticAnalysisOptions:
     max_iterations: int = 5000
     warm_start_displacements: Optional[np.ndarray] = None
     throw_on_non_convergence: bool = True
-    precision: str = "fp64"  # "fp64" (the plain drop-in) or "mixed" (FP32 inner PCG + FP64 refinement)
+    # "fp64" (the plain drop-in), "mixed" (FP32 inner Jacobi-PCG + FP64 refinement), "fp64f" (factorised FP64
+    # operator), "mg" (FP64 flexible CG with an FP32 multigrid V-cycle), "mixed-mg" (that iteration in FP32 inside
+    # FP64 refinement)
+    precision: str = "fp64"
 
 
 @dataclass
@@ -263,7 +266,7 @@ class OptimizerOptions:
     start_iteration: int = 1
     warm_start_displacements: Optional[np.ndarray] = None
     enforce_minimum_filter_radius: bool = True
-    precision: str = "fp64"
+    precision: str = "fp64"  # solver form, as for StaticAnalysisOptions.precision
 
     def replace(self, **kw) -> "OptimizerOptions":
         return dataclasses.replace(self, **kw)

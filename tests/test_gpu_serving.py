@@ -21,7 +21,7 @@ def _jobs(precision, n=5, iters=4):
             for i, (nx, ny, nz) in enumerate(shapes[:n])]
 
 
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed", "mixed-mg"])
 def test_results_same_alone_and_in_mix(ctx, precision):
     jobs = _jobs(precision)
     alone = [api.TopologyOptimizer.run(m, o, ctx=ctx) for m, o in jobs]
@@ -68,7 +68,7 @@ def test_admission_respects_budget_and_rejects_oversize():
                 srv.result(big)
 
 
-@pytest.mark.parametrize("precision", ["fp64", "mixed", "fp64f"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed", "fp64f", "mg", "mixed-mg"])
 def test_admission_estimate_bounds_job_memory(ctx, precision):
     m, o = W.served_job(30, 14, 10, 2, seed=5, precision=precision)
     est = api.Server.device_bytes(m, o)
