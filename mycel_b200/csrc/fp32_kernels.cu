@@ -1806,15 +1806,19 @@ __global__ void __launch_bounds__(256) k_mg_build1(MgDims c, MgDims f, const flo
   }
 }
 
-// Assembled 27-point stencil of a level from its element matrices: S[(nb * 9 + 3 ci + cj) * nn + n] is the
-// block entry (DOF ci of node n, DOF cj of neighbour nb), nb = (dx+1) + 3 (dy+1) + 9 (dz+1); also 1/diag
-// (0 where the diagonal is 0: DOFs no free fine DOF reaches)
+// Assembled 27-point stencil of a level from its element matrices, in symmetric half storage: node n keeps the
+// blocks of its neighbours nb = 13 .. 26 (itself and the 13 neighbours later in node order), nb = (dx+1) +
+// 3 (dy+1) + 9 (dz+1); S[((nb - 13) * 9 + 3 ci + cj) * nn + n] is the entry (DOF ci of node n, DOF cj of
+// neighbour nb). The block of an earlier neighbour m is the transpose of m's block for offset 26 - nb. Also
+// 1/diag (0 where the diagonal is 0: DOFs no free fine DOF reaches).
+constexpr int kMgHalf = 14;  // stored blocks per node
 __global__ void k_mg_stencil(MgDims d, const float* __restrict__ K, float* __restrict__ S, float* __restrict__ invd) {
   const int64_t nn = mg_nn(d);
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (t >= 27 * nn) return;
-  const int nb = (int)(t / nn);
-  const int64_t n = t - nb * nn;
+  if (t >= kMgHalf * nn) return;
+  const int hb = (int)(t / nn);
+  const int nb = 13 + hb;
+  const int64_t n = t - hb * nn;
   const int nx1 = d.nx + 1, ny1 = d.ny + 1;
   const int i = (int)(n % nx1), j = (int)((n / nx1) % ny1), k = (int)(n / ((int64_t)nx1 * ny1));
   const int dx = nb % 3 - 1, dy = (nb / 3) % 3 - 1, dz = nb / 9 - 1;
@@ -1835,11 +1839,19 @@ __global__ void k_mg_stencil(MgDims d, const float* __restrict__ K, float* __res
         }
   }
 #pragma unroll
-  for (int q = 0; q < 9; ++q) S[(nb * 9 + q) * nn + n] = v[q];
-  if (nb == 13)
+  for (int q = 0; q < 9; ++q) S[(hb * 9 + q) * nn + n] = v[q];
+  if (hb == 0)
 #pragma unroll
     for (int ci = 0; ci < 3; ++ci) invd[3 * n + ci] = v[4 * ci] > 0.f ? 1.0f / v[4 * ci] : 0.0f;
 }
+
+// Kernels over nodes of the levels below the voxel grid run a thread per DOF: CTAs of 3 x 64 threads, warps
+// 0-1 take component 0 of 64 consecutive nodes, warps 2-3 component 1, warps 4-5 component 2 (coalesced loads,
+// three times the threads in flight of a thread per node).
+constexpr int kMgDofThreads = 192;
+__device__ __forceinline__ int64_t mg_dof_node() { return blockIdx.x * (int64_t)64 + (threadIdx.x & 63); }
+__device__ __forceinline__ int mg_dof_comp() { return threadIdx.x >> 6; }
+static inline unsigned mg_dof_blocks(int64_t nn) { return (unsigned)((nn + 63) / 64); }
 
 // coarse-level product at node n by gather. mode 0: y = A x; 1: y = x + omega invd (r - A x) (one Jacobi
 // sweep); 2: y = r - A x on DOFs with a nonzero diagonal, 0 elsewhere
@@ -1850,18 +1862,27 @@ __device__ __forceinline__ void mg_apply_node(const MgDims& d, int64_t nn, int64
   const int nx1 = d.nx + 1, ny1 = d.ny + 1;
   const int i = (int)(n % nx1), j = (int)((n / nx1) % ny1), k = (int)(n / ((int64_t)nx1 * ny1));
   float a0 = 0.f, a1 = 0.f, a2 = 0.f;
-  // all 27 blocks without branches: a neighbour outside the grid has a zero stencil block, so its x is read
-  // at a clamped (valid) node
+  // all 27 blocks without branches: a neighbour outside the grid is read at a clamped (valid) node with x
+  // taken as 0. Later neighbours' blocks are n's own (row ci at entries 3 ci + cj), earlier ones the transposed
+  // blocks stored at the neighbour (row ci at entries 3 cj + ci).
 #pragma unroll
   for (int nb = 0; nb < 27; ++nb) {
-    const int mi = min(max(i + nb % 3 - 1, 0), d.nx), mj = min(max(j + (nb / 3) % 3 - 1, 0), d.ny),
-              mk = min(max(k + nb / 9 - 1, 0), d.nz);
+    const int ui = i + nb % 3 - 1, uj = j + (nb / 3) % 3 - 1, uk = k + nb / 9 - 1;
+    const int mi = min(max(ui, 0), d.nx), mj = min(max(uj, 0), d.ny), mk = min(max(uk, 0), d.nz);
+    const bool in = mi == ui && mj == uj && mk == uk;
     const int64_t m = mi + (int64_t)nx1 * (mj + (int64_t)ny1 * mk);
-    const float x0 = x[3 * m], x1 = x[3 * m + 1], x2 = x[3 * m + 2];
-    const float* s = S + (int64_t)nb * 9 * nn + n;
-    a0 = fmaf(s[0], x0, fmaf(s[nn], x1, fmaf(s[2 * nn], x2, a0)));
-    a1 = fmaf(s[3 * nn], x0, fmaf(s[4 * nn], x1, fmaf(s[5 * nn], x2, a1)));
-    a2 = fmaf(s[6 * nn], x0, fmaf(s[7 * nn], x1, fmaf(s[8 * nn], x2, a2)));
+    const float x0 = in ? x[3 * m] : 0.f, x1 = in ? x[3 * m + 1] : 0.f, x2 = in ? x[3 * m + 2] : 0.f;
+    if (nb >= 13) {
+      const float* s = S + (int64_t)(nb - 13) * 9 * nn + n;
+      a0 = fmaf(s[0], x0, fmaf(s[nn], x1, fmaf(s[2 * nn], x2, a0)));
+      a1 = fmaf(s[3 * nn], x0, fmaf(s[4 * nn], x1, fmaf(s[5 * nn], x2, a1)));
+      a2 = fmaf(s[6 * nn], x0, fmaf(s[7 * nn], x1, fmaf(s[8 * nn], x2, a2)));
+    } else {
+      const float* s = S + (int64_t)(13 - nb) * 9 * nn + m;
+      a0 = fmaf(s[0], x0, fmaf(s[3 * nn], x1, fmaf(s[6 * nn], x2, a0)));
+      a1 = fmaf(s[nn], x0, fmaf(s[4 * nn], x1, fmaf(s[7 * nn], x2, a1)));
+      a2 = fmaf(s[2 * nn], x0, fmaf(s[5 * nn], x1, fmaf(s[8 * nn], x2, a2)));
+    }
   }
   const float acc[3] = {a0, a1, a2};
 #pragma unroll
@@ -1873,14 +1894,56 @@ __device__ __forceinline__ void mg_apply_node(const MgDims& d, int64_t nn, int64
   }
 }
 
-__global__ void __launch_bounds__(256) k_mg_apply(MgDims d, const float* __restrict__ S, const float* __restrict__ x,
-                                                  const float* __restrict__ r, const float* __restrict__ invd,
-                                                  float* __restrict__ y, int mode, const float* __restrict__ om,
-                                                  const MixState* st) {
+// the same for one row (DOF ci of node n): a third of the loads of a node
+__device__ __forceinline__ void mg_apply_row(const MgDims& d, int64_t nn, int64_t n, int ci,
+                                             const float* __restrict__ S, const float* __restrict__ x,
+                                             const float* __restrict__ r, const float* __restrict__ invd,
+                                             float* __restrict__ y, int mode, float omega) {
+  const int nx1 = d.nx + 1, ny1 = d.ny + 1;
+  const int i = (int)(n % nx1), j = (int)((n / nx1) % ny1), k = (int)(n / ((int64_t)nx1 * ny1));
+  float a = 0.f;
+#pragma unroll
+  for (int nb = 0; nb < 27; ++nb) {
+    const int ui = i + nb % 3 - 1, uj = j + (nb / 3) % 3 - 1, uk = k + nb / 9 - 1;
+    const int mi = min(max(ui, 0), d.nx), mj = min(max(uj, 0), d.ny), mk = min(max(uk, 0), d.nz);
+    const bool in = mi == ui && mj == uj && mk == uk;
+    const int64_t m = mi + (int64_t)nx1 * (mj + (int64_t)ny1 * mk);
+    const float x0 = in ? x[3 * m] : 0.f, x1 = in ? x[3 * m + 1] : 0.f, x2 = in ? x[3 * m + 2] : 0.f;
+    if (nb >= 13) {
+      const float* s = S + ((int64_t)(nb - 13) * 9 + 3 * ci) * nn + n;
+      a = fmaf(s[0], x0, fmaf(s[nn], x1, fmaf(s[2 * nn], x2, a)));
+    } else {
+      const float* s = S + ((int64_t)(13 - nb) * 9 + ci) * nn + m;
+      a = fmaf(s[0], x0, fmaf(s[3 * nn], x1, fmaf(s[6 * nn], x2, a)));
+    }
+  }
+  const int64_t q = 3 * n + ci;
+  if (mode == 0) y[q] = a;
+  else if (mode == 1) y[q] = fmaf(omega * invd[q], r[q] - a, x[q]);
+  else y[q] = invd[q] != 0.0f ? r[q] - a : 0.0f;
+}
+
+// coarse-level product kernels: a thread per node (large levels: the three rows share their x loads) or a
+// thread per DOF (smaller levels: three times the threads in flight); mg_apply_kernel picks by size
+__global__ void __launch_bounds__(256) k_mg_apply_nodes(MgDims d, const float* __restrict__ S,
+                                                        const float* __restrict__ x, const float* __restrict__ r,
+                                                        const float* __restrict__ invd, float* __restrict__ y,
+                                                        int mode, const float* __restrict__ om, const MixState* st) {
   if (!mg_running(st)) return;
   const int64_t nn = mg_nn(d);
   const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (n < nn) mg_apply_node(d, nn, n, S, x, r, invd, y, mode, mode == 1 ? *om : 0.0f);
+}
+
+__global__ void __launch_bounds__(kMgDofThreads) k_mg_apply(MgDims d, const float* __restrict__ S,
+                                                            const float* __restrict__ x, const float* __restrict__ r,
+                                                            const float* __restrict__ invd, float* __restrict__ y,
+                                                            int mode, const float* __restrict__ om,
+                                                            const MixState* st) {
+  if (!mg_running(st)) return;
+  const int64_t nn = mg_nn(d);
+  const int64_t n = mg_dof_node();
+  if (n < nn) mg_apply_row(d, nn, n, mg_dof_comp(), S, x, r, invd, y, mode, mode == 1 ? *om : 0.0f);
 }
 
 // first sweep from x = 0 on a coarse level: x = omega invd r
@@ -1902,6 +1965,79 @@ __global__ void k_mg_jacobi_fine(int64_t n, const float* __restrict__ r, const f
     x[q] = fmaf(omega * invd[q], r[q] - t[q], x[q]);
 }
 
+// restriction r_c = W^T res of a level's residual, component cc at coarse node n. PAD: the voxel grid in the
+// padded FP32 layout (row pitch pitch), res = r - t; otherwise box layout, res = t. Coarse DOFs with a zero
+// diagonal get 0.
+template <bool PAD>
+__device__ __forceinline__ void mg_restrict_comp(const MgDims& f, int pitch, const float* __restrict__ rf,
+                                                 const float* __restrict__ tf, const MgDims& c,
+                                                 const float* __restrict__ invdc, float* __restrict__ rc, int64_t n,
+                                                 int cc) {
+  const int cx1 = c.nx + 1, cy1 = c.ny + 1;
+  const int I = (int)(n % cx1), J = (int)((n / cx1) % cy1), K = (int)(n / ((int64_t)cx1 * cy1));
+  const int pi = min(2 * I, f.nx), pj = min(2 * J, f.ny), pk = min(2 * K, f.nz);
+  float a = 0.f;
+  // the 27 candidate fine nodes around the coarse node's position, without branches: a candidate outside the
+  // grid gets weight 0 and a clamped (valid) read
+#pragma unroll
+  for (int dk = -1; dk <= 1; ++dk) {
+    const int k0 = pk + dk, k = min(max(k0, 0), f.nz);
+    const float wz = (k0 == k) ? mg_pw(k, K, f.nz) : 0.f;
+#pragma unroll
+    for (int dj = -1; dj <= 1; ++dj) {
+      const int j0 = pj + dj, j = min(max(j0, 0), f.ny);
+      const float wy = (j0 == j) ? wz * mg_pw(j, J, f.ny) : 0.f;
+#pragma unroll
+      for (int di = -1; di <= 1; ++di) {
+        const int i0 = pi + di, i = min(max(i0, 0), f.nx);
+        const float w = (i0 == i) ? wy * mg_pw(i, I, f.nx) : 0.f;
+        const int64_t row = j + (int64_t)(f.ny + 1) * k;
+        const int64_t b = (PAD ? (int64_t)pitch * row + 3 * i : 3 * (i + (int64_t)(f.nx + 1) * row)) + cc;
+        a = fmaf(w, PAD ? rf[b] - tf[b] : tf[b], a);
+      }
+    }
+  }
+  rc[3 * n + cc] = invdc[3 * n + cc] != 0.f ? a : 0.f;
+}
+
+
+// prolongation x_f += W x_c, component cc at fine node n, on the finer level's free DOFs. PAD: the voxel grid
+// (padded FP32 layout, free = node flag bit clear); otherwise box layout, free = nonzero diagonal.
+template <bool PAD>
+__device__ __forceinline__ void mg_prolong_comp(const MgDims& f, int pitch, const uint8_t* __restrict__ nf,
+                                                const float* __restrict__ invdf, float* __restrict__ xf,
+                                                const MgDims& c, const float* __restrict__ xc, int64_t n, int cc) {
+  const int fx1 = f.nx + 1, fy1 = f.ny + 1;
+  const int i = (int)(n % fx1), j = (int)((n / fx1) % fy1), k = (int)(n / ((int64_t)fx1 * fy1));
+  // per axis: two coarse nodes with their weights (the second with weight 0 unless the fine node lies midway)
+  int ci[2], cj[2], ck[2];
+  float wi[2], wj[2], wk[2];
+  auto axis = [](int f_, int n_, int nc_, int* c_, float* ww) {
+    const bool mid = (f_ & 1) && f_ != n_;
+    c_[0] = ((f_ & 1) && f_ == n_) ? nc_ : (f_ >> 1);
+    c_[1] = min(c_[0] + 1, nc_);
+    ww[0] = mid ? 0.5f : 1.0f;
+    ww[1] = mid ? 0.5f : 0.0f;
+  };
+  axis(i, f.nx, c.nx, ci, wi);
+  axis(j, f.ny, c.ny, cj, wj);
+  axis(k, f.nz, c.nz, ck, wk);
+  const int cx1 = c.nx + 1, cy1 = c.ny + 1;
+  float a = 0.f;
+#pragma unroll
+  for (int qz = 0; qz < 2; ++qz)
+#pragma unroll
+    for (int qy = 0; qy < 2; ++qy)
+#pragma unroll
+      for (int qx = 0; qx < 2; ++qx) {
+        const int64_t m = ci[qx] + (int64_t)cx1 * (cj[qy] + (int64_t)cy1 * ck[qz]);
+        a = fmaf(wi[qx] * wj[qy] * wk[qz], xc[3 * m + cc], a);
+      }
+  const bool fr = PAD ? !(nf[n] & (1 << cc)) : (invdf[3 * n + cc] != 0.0f);
+  if (fr) xf[(PAD ? (int64_t)pitch * (j + (int64_t)fy1 * k) + 3 * i : 3 * n) + cc] += a;
+}
+
+// the same transfers for all three components of a node in one pass (the per-level kernels):
 // restriction r_c = W^T res of a level's residual at coarse node n. PAD: the voxel grid in the padded FP32
 // layout (row pitch pitch), res = r - t; otherwise box layout, res = t. Coarse DOFs with a zero diagonal get 0.
 template <bool PAD>
@@ -2005,6 +2141,7 @@ __global__ void k_mg_prolong(MgDims f, int pitch, const uint8_t* __restrict__ nf
   if (n < mg_nn(f)) mg_prolong_node<PAD>(f, pitch, nf, invdf, xf, c, xc, n);
 }
 
+
 // coarsest level set-up (one CTA): the dense matrix from the level's stencil, inverted in place by Gauss-Jordan
 // elimination without pivoting (SPD) in FP64 shared memory. A pivot that has lost all but 1e-12 of its
 // original diagonal (round-off on a nearly singular block) drops its DOF: row and column become 0, as do those
@@ -2025,7 +2162,7 @@ __global__ void __launch_bounds__(1024) k_mg_coarse_setup(MgDims d, const float*
     double v = 0.0;
     if (dx >= -1 && dx <= 1 && dy >= -1 && dy <= 1 && dz >= -1 && dz <= 1) {
       const int nb = (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1);
-      v = (double)S[(nb * 9 + 3 * ci + cj) * nn + a];
+      v = nb >= 13 ? (double)S[((nb - 13) * 9 + 3 * ci + cj) * nn + a] : (double)S[((13 - nb) * 9 + 3 * cj + ci) * nn + b];
     }
     A[o] = v;
   }
@@ -2057,9 +2194,11 @@ __global__ void __launch_bounds__(1024) k_mg_coarse_setup(MgDims d, const float*
       continue;
     }
     const double ip = 1.0 / piv;
-    for (int o = tid; o < n * n; o += nt) {
-      const int i = o / n, j = o % n;
-      if (i != k && j != k) A[o] = fma(-A[i * n + k] * ip, A[k * n + j], A[o]);
+    for (int i = tid >> 5; i < n; i += nt >> 5) {  // 32 x 32 thread tile: rows by warp, columns by lane
+      if (i == k) continue;
+      const double f = A[i * n + k] * ip;
+      for (int j = tid & 31; j < n; j += 32)
+        if (j != k) A[i * n + j] = fma(-f, A[k * n + j], A[i * n + j]);
     }
     __syncthreads();
     for (int o = tid; o < n; o += nt) {
@@ -2108,6 +2247,14 @@ __global__ void __cluster_dims__(kMgTailCtas, 1, 1) __launch_bounds__(kMgTailThr
   if (!mg_running(st)) return;
   const int64_t gt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x, gs = (int64_t)gridDim.x * blockDim.x;
   float* xc[kMgMaxLevels];
+  // a thread per row where the level's rows fit the cluster's threads, else a thread per node
+  auto apply = [&](const MgTailLevel& v, const float* x, float* y, int mode, float w) {
+    if (3 * v.nn <= gs) {
+      for (int64_t t = gt; t < 3 * v.nn; t += gs) mg_apply_row(v.d, v.nn, t / 3, (int)(t % 3), v.S, x, v.r, v.invd, y, mode, w);
+    } else {
+      for (int64_t n = gt; n < v.nn; n += gs) mg_apply_node(v.d, v.nn, n, v.S, x, v.r, v.invd, y, mode, w);
+    }
+  };
   for (int l = tl.T; l < tl.L - 1; ++l) {
     const MgTailLevel& v = tl.lv[l];
     const MgTailLevel& cv = tl.lv[l + 1];
@@ -2116,15 +2263,16 @@ __global__ void __cluster_dims__(kMgTailCtas, 1, 1) __launch_bounds__(kMgTailThr
     for (int64_t q = gt; q < 3 * v.nn; q += gs) x[q] = w * v.invd[q] * v.r[q];
     mg_cluster_sync();
     for (int k = 1; k < tl.sweeps; ++k) {
-      for (int64_t n = gt; n < v.nn; n += gs) mg_apply_node(v.d, v.nn, n, v.S, x, v.r, v.invd, o, 1, w);
+      apply(v, x, o, 1, w);
       mg_cluster_sync();
       float* tmp = x;
       x = o;
       o = tmp;
     }
-    for (int64_t n = gt; n < v.nn; n += gs) mg_apply_node(v.d, v.nn, n, v.S, x, v.r, v.invd, v.t, 2, 0.0f);
+    apply(v, x, v.t, 2, 0.0f);
     mg_cluster_sync();
-    for (int64_t n = gt; n < cv.nn; n += gs) mg_restrict_node<false>(v.d, 0, nullptr, v.t, cv.d, cv.invd, cv.r, n);
+    for (int64_t q = gt; q < 3 * cv.nn; q += gs)
+      mg_restrict_comp<false>(v.d, 0, nullptr, v.t, cv.d, cv.invd, cv.r, q / 3, (int)(q % 3));
     mg_cluster_sync();
     xc[l] = x;
   }
@@ -2146,10 +2294,11 @@ __global__ void __cluster_dims__(kMgTailCtas, 1, 1) __launch_bounds__(kMgTailThr
     const float w = om[l];
     float* x = xc[l];
     float* o = x == v.xa ? v.xb : v.xa;
-    for (int64_t n = gt; n < v.nn; n += gs) mg_prolong_node<false>(v.d, 0, nullptr, v.invd, x, tl.lv[l + 1].d, xc[l + 1], n);
+    for (int64_t q = gt; q < 3 * v.nn; q += gs)
+      mg_prolong_comp<false>(v.d, 0, nullptr, v.invd, x, tl.lv[l + 1].d, xc[l + 1], q / 3, (int)(q % 3));
     mg_cluster_sync();
     for (int k = 0; k < tl.sweeps; ++k) {
-      for (int64_t n = gt; n < v.nn; n += gs) mg_apply_node(v.d, v.nn, n, v.S, x, v.r, v.invd, o, 1, w);
+      apply(v, x, o, 1, w);
       mg_cluster_sync();
       float* tmp = x;
       x = o;
@@ -2566,7 +2715,7 @@ int64_t mg_device_bytes(int nx, int ny, int nz) {
   const int L = mg_levels(nx, ny, nz, lv);
   if (!L) return 0;
   int64_t b = 0;
-  for (int l = 1; l < L; ++l) b += 4 * (243 + 15) * mg_nn(lv[l]) + 6 * 64;
+  for (int l = 1; l < L; ++l) b += 4 * (9 * kMgHalf + 15) * mg_nn(lv[l]) + 6 * 64;
   b += sizeof(MgScratch) + 64 + 4 * 8 * 576 + 64 + (int64_t)lv[1].nx * lv[1].ny * lv[1].nz + 64;
   const int64_t rp = (3 * (int64_t)(nx + 1) + 3) & ~int64_t(3);  // FP32 row pitch of the voxel level
   b += 4 * rp * (ny + 1) * (nz + 1) + 64;                         // f_t
@@ -2630,7 +2779,7 @@ static int32_t mg_ensure(mycel_problem* p, bool* available) {
     v.nn = mg_nn(v.d);
     v.nd = 3 * v.nn;
     if (l == 0) continue;
-    v.S = (float*)alloc(sizeof(float) * 243 * v.nn);
+    v.S = (float*)alloc(sizeof(float) * 9 * kMgHalf * v.nn);
     float** vecs[] = {&v.invd, &v.xa, &v.xb, &v.r, &v.t};
     for (float** q : vecs) *q = (float*)alloc(sizeof(float) * v.nd);
   }
@@ -2706,6 +2855,16 @@ static int32_t mg_ensure(mycel_problem* p, bool* available) {
 
 static unsigned mg_blocks(int64_t n) { return (unsigned)((n + 255) / 256); }
 
+// coarse-level product on the stream: a thread per DOF up to 64k nodes, a thread per node above (measured on
+// the bridge: level 2, 31k nodes, 9.6 vs 14.5 us; level 1, 233k nodes, 43 vs 51 us)
+static void launch_mg_apply(cudaStream_t s, const MgLevel& v, const float* x, const float* r, const float* invd,
+                            float* y, int mode, const float* om, const MixState* st) {
+  if (v.nn <= 65536)
+    k_mg_apply<<<mg_dof_blocks(v.nn), kMgDofThreads, 0, s>>>(v.d, v.S, x, r, invd, y, mode, om, st);
+  else
+    k_mg_apply_nodes<<<mg_blocks(v.nn), 256, 0, s>>>(v.d, v.S, x, r, invd, y, mode, om, st);
+}
+
 // Coarse operators from the current E: Galerkin element matrices level by level, their stencils, and the
 // coarsest level's dense inverse.
 static void mg_setup(mycel_problem* p) {
@@ -2718,14 +2877,14 @@ static void mg_setup(mycel_problem* p) {
       d1, lv[0].d, mg->G, p->d_Ef, p->d_nflags, mg->em[0], mg->special);
   k_mg_build<true><<<(unsigned)ne1, 64, 0, s>>>(d1, lv[0].d, p->kef, p->d_Ef, p->d_nflags, nullptr, mg->em[0],
                                                 mg->special);
-  k_mg_stencil<<<mg_blocks(27 * lv[1].nn), 256, 0, s>>>(d1, mg->em[0], lv[1].S, lv[1].invd);
+  k_mg_stencil<<<mg_blocks(kMgHalf * lv[1].nn), 256, 0, s>>>(d1, mg->em[0], lv[1].S, lv[1].invd);
   for (int l = 2; l < mg->L; ++l) {
     const MgDims& d = lv[l].d;
     float* src = mg->em[(l - 2) & 1];
     float* dst = mg->em[(l - 1) & 1];
     k_mg_build<false><<<(unsigned)((int64_t)d.nx * d.ny * d.nz), 64, 0, s>>>(d, lv[l - 1].d, p->kef, nullptr,
                                                                            nullptr, src, dst, nullptr);
-    k_mg_stencil<<<mg_blocks(27 * lv[l].nn), 256, 0, s>>>(d, dst, lv[l].S, lv[l].invd);
+    k_mg_stencil<<<mg_blocks(kMgHalf * lv[l].nn), 256, 0, s>>>(d, dst, lv[l].S, lv[l].invd);
   }
   k_mg_coarse_setup<<<1, 1024, kMgCoarseSmem, s>>>(lv[mg->L - 1].d, lv[mg->L - 1].S, mg->ainv);
   int nl = 2 * (mg->L - 1) + 2;
@@ -2740,7 +2899,7 @@ static void mg_setup(mycel_problem* p) {
     const unsigned nb = l ? std::min<unsigned>(mg_blocks(n), (unsigned)sb) : (unsigned)sb;
     k_mg_pow_init<<<nb, 256, 0, s>>>(n, invd, x);
     for (int it = 0; it < kMgPowerIters; ++it) {
-      if (l) k_mg_apply<<<mg_blocks(v.nn), 256, 0, s>>>(v.d, v.S, x, nullptr, invd, y, 0, nullptr, nullptr);
+      if (l) launch_mg_apply(s, v, x, nullptr, invd, y, 0, nullptr, nullptr);
       else launch_mv32_variant<0>(p, s, p->f_p0, nullptr, nullptr, nullptr, p->f_ap, 1, nullptr, nullptr);
       const bool last = it == kMgPowerIters - 1;
       k_mg_pow_norm<<<nb, kT, 0, s>>>(n, y, invd, p->d_part2, mg->sc, last ? l : -1);
@@ -2776,10 +2935,10 @@ static int mg_vcycle(mycel_problem* p, cudaStream_t s, MixState* st, float* rf, 
     float *x = v.xa, *o = v.xb;
     k_mg_jacobi0<<<mg_blocks(v.nd), 256, 0, s>>>(v.nd, v.r, v.invd, x, om + l, st);
     for (int k = 1; k < mg->sweeps; ++k) {
-      k_mg_apply<<<mg_blocks(v.nn), 256, 0, s>>>(v.d, v.S, x, v.r, v.invd, o, 1, om + l, st);
+      launch_mg_apply(s, v, x, v.r, v.invd, o, 1, om + l, st);
       std::swap(x, o);
     }
-    k_mg_apply<<<mg_blocks(v.nn), 256, 0, s>>>(v.d, v.S, x, v.r, v.invd, v.t, 2, om + l, st);
+    launch_mg_apply(s, v, x, v.r, v.invd, v.t, 2, om + l, st);
     k_mg_restrict<false><<<mg_blocks(lv[l + 1].nn), 256, 0, s>>>(v.d, 0, nullptr, v.t, lv[l + 1].d, lv[l + 1].invd,
                                                                  lv[l + 1].r, st);
     xc[l] = x;
@@ -2794,7 +2953,7 @@ static int mg_vcycle(mycel_problem* p, cudaStream_t s, MixState* st, float* rf, 
     float* o = x == v.xa ? v.xb : v.xa;
     k_mg_prolong<false><<<mg_blocks(v.nn), 256, 0, s>>>(v.d, 0, nullptr, v.invd, x, lv[l + 1].d, xc[l + 1], st);
     for (int k = 0; k < mg->sweeps; ++k) {
-      k_mg_apply<<<mg_blocks(v.nn), 256, 0, s>>>(v.d, v.S, x, v.r, v.invd, o, 1, om + l, st);
+      launch_mg_apply(s, v, x, v.r, v.invd, o, 1, om + l, st);
       std::swap(x, o);
     }
     xc[l] = x;
