@@ -45,7 +45,10 @@ FP64_PCG_PER_SIMP_ITER = None
 # dram__bytes_write.sum), keyed by (solver form, matvec variant, workload). Jacobi-PCG form (`--probe mixed
 # --probe-grid 192x96x96 --probe-variant 3`): 53.47 MB read, 5.53 MB written (K p and p_t mostly stay in the
 # 126 MB L2 during the launch).
-NCU_DRAM_BYTES = {("mixed", 3, "bridge_192x96x96"): 53.47e6 + 5.53e6}
+# Mixed multigrid form (`--probe mixed-mg --probe-grid 192x96x96 --probe-variant 3`, third MODE-1 launch):
+# 53.52 MB read, 4.88 MB written.
+NCU_DRAM_BYTES = {("mixed", 3, "bridge_192x96x96"): 53.47e6 + 5.53e6,
+                  ("mixed-mg", 3, "bridge_192x96x96"): 53.52e6 + 4.88e6}
 
 
 def parse():
@@ -435,8 +438,8 @@ def run_mycel(args):
     roof = {"kernel": kname + ": FP32 Hex8 K.p with fused p update + p.Ap partials", "bound": "hbm",
             "achieved": achieved, "peak": hbm, "unit": "GB/s",
             "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
-            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one MODE-1 launch of this kernel on "
-                              "this workload (192x96x96)" if traffic else None,
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one MODE-1 launch of this kernel in "
+                              "this solver form on this workload (192x96x96)" if traffic else None,
             "peak_source": "measured" if pk else "fallback", "avg_launch_us": per_launch_ms * 1000.0,
             "timed_launches": timing["launches"], "algorithmic_bytes_per_launch": mv_bytes,
             "flops_per_launch": 1152 * model.active_element_count, "flops_note": "dense-KE equivalent",
