@@ -272,6 +272,23 @@ int32_t mycel_simp_frame_begin(mycel_simp_session* s, int32_t* slot_out);
 int32_t mycel_simp_frame_end(mycel_simp_session* s, int32_t slot, uint8_t* frame_out, uint8_t* header_out,
                              uint32_t* checksum_out);
 
+/* ---- iso-surface: SurfaceNetsExtractor.Extract (PostProcessing/SurfaceNetsExtractor.cs:31-312) ----
+   Closed 2-manifold triangle mesh of the level set density >= threshold of a box-sized float density field
+   (element order x fastest) on a grid with spacing h and the given origin, by constrained Surface Nets with a
+   1-voxel zero border: the reference's well-composedness passes, one vertex per dual cell with mixed corners,
+   two triangles per sign-changing grid edge. Vertices, triangles and their orders are the reference's
+   (sequential semantics, float arithmetic rounded per operation). density_len shorter than nx*ny*nz is
+   MYCEL_E_ARG with the reference's message. The mesh (IndexedMesh: positions, 3 floats per vertex; indices, 3
+   per triangle) is returned in host memory; mycel_mesh_info also gives the well-composedness passes run and
+   the voxels' saddle/corner-kiss resolutions made. */
+typedef struct mycel_mesh mycel_mesh;
+int32_t mycel_surface_nets(mycel_ctx* ctx, int32_t nx, int32_t ny, int32_t nz, float h, const float* origin,
+                           const float* density, int64_t density_len, float threshold, mycel_mesh** out);
+int32_t mycel_mesh_info(const mycel_mesh* m, int64_t* n_vertices, int64_t* n_indices, int32_t* passes,
+                        int64_t* changes);
+int32_t mycel_mesh_copy(const mycel_mesh* m, float* positions, int32_t* indices);
+void mycel_mesh_destroy(mycel_mesh* m);
+
 /* ---- serving: continuous batching of SIMP jobs on one GPU ----
    No counterpart in the reference, whose App runs one optimisation at a time (OptimizationCoordinator.cs:229
    through the FemWorkTeam lock, FemWorkTeam.cs:109). A server runs `slots` jobs at once, each on its own CUDA

@@ -11,6 +11,7 @@ from __future__ import annotations
 import ctypes as C
 import threading
 import weakref
+from dataclasses import dataclass
 from typing import Callable, Optional
 
 import numpy as np
@@ -570,3 +571,44 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+@dataclass
+class IndexedMesh:
+    """Triangle mesh (Geometry/IndexedMesh.cs): positions [V, 3] float32, indices [3T] int32 (counter-clockwise
+    seen from outside), plus the well-composedness passes and resolutions of the extraction."""
+    positions: np.ndarray
+    indices: np.ndarray
+    passes: int = 0
+    changes: int = 0
+
+    @property
+    def vertex_count(self) -> int:
+        return int(self.positions.shape[0])
+
+    @property
+    def triangle_count(self) -> int:
+        return int(self.indices.size // 3)
+
+
+class SurfaceNetsExtractor:
+    """SurfaceNetsExtractor.Extract (PostProcessing/SurfaceNetsExtractor.cs:31-312) on the device."""
+
+    @staticmethod
+    def extract(grid, physical_density, threshold: float = 0.5, ctx: Context = None) -> IndexedMesh:
+        ctx = ctx or default_context()
+        d = np.ascontiguousarray(physical_density, dtype=np.float32).reshape(-1)
+        o = np.ascontiguousarray(getattr(grid, "origin", (0.0, 0.0, 0.0)), dtype=np.float32)
+        lib = L.load()
+        h = C.c_void_p()
+        _check(lib.mycel_surface_nets(ctx.handle, grid.nx, grid.ny, grid.nz, float(grid.h), o.ctypes.data,
+                                      d.ctypes.data, d.size, float(threshold), C.byref(h)), ctx)
+        try:
+            nv, ni, passes, changes = C.c_int64(0), C.c_int64(0), C.c_int32(0), C.c_int64(0)
+            _check(lib.mycel_mesh_info(h, C.byref(nv), C.byref(ni), C.byref(passes), C.byref(changes)))
+            pos = np.zeros((nv.value, 3), dtype=np.float32)
+            idx = np.zeros(ni.value, dtype=np.int32)
+            _check(lib.mycel_mesh_copy(h, pos.ctypes.data, idx.ctypes.data))
+        finally:
+            lib.mycel_mesh_destroy(h)
+        return IndexedMesh(pos, idx, int(passes.value), int(changes.value))

@@ -25,6 +25,7 @@ UNITS = [
     ("simp.cu", ["-fmad=true"]),
     ("hex8.cpp", []),
     ("server.cpp", []),
+    ("surface_nets.cu", ["-fmad=false"]),
 ]
 
 

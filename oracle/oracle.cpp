@@ -1275,3 +1275,185 @@ extern "C" uint32_t orc_quantized_checksum(const float* v, int64_t n, uint8_t* o
   }
   return h;
 }
+
+// ---------------------------------------------------------------------------------------------------------
+// SurfaceNetsExtractor.Extract (src/Mycel.Core/PostProcessing/SurfaceNetsExtractor.cs:31-312), with
+// MakeWellComposed (:352-435), Resolve2x2Saddle (:437-451), Resolve3DCornerKiss (:453-476) and EmitQuad
+// (:314-346). Sequential, in the reference's loop orders; float arithmetic with every operation rounded
+// (no contraction), as RyuJIT evaluates the Vector3 expressions. Vector3.DistanceSquared is taken as
+// (dx*dx + dy*dy) + dz*dz and Vector3 / float as a component-wise division.
+// ---------------------------------------------------------------------------------------------------------
+struct orc_mesh {
+  std::vector<float> pos;     // 3 per vertex
+  std::vector<int32_t> idx;   // 3 per triangle
+  int32_t passes = 0;         // well-composedness passes run
+  int64_t changes = 0;        // saddle and corner-kiss resolutions made
+};
+
+namespace {
+
+bool sn_saddle(std::vector<uint8_t>& s, std::vector<float>& rho, float thr, int64_t i00, int64_t i10, int64_t i01,
+               int64_t i11) {
+  const bool s00 = s[i00], s10 = s[i10], s01 = s[i01], s11 = s[i11];
+  if (!(s00 == s11 && s10 == s01 && s00 != s10)) return false;
+  const int64_t a = s00 ? i10 : i00, b = s00 ? i01 : i11;  // the two empty voxels of the diagonal pair
+  const int64_t pick = rho[a] >= rho[b] ? a : b;
+  s[pick] = 1;
+  if (rho[pick] < thr) rho[pick] = thr;
+  return true;
+}
+
+bool sn_kiss(std::vector<uint8_t>& s, std::vector<float>& rho, float thr, int64_t dA, int64_t dB, int64_t a1,
+             int64_t a2, int64_t a3, int64_t b1, int64_t b2, int64_t b3) {
+  if (!(s[dA] && s[dB])) return false;
+  const bool linked = (s[a1] && (s[b1] || s[b2])) || (s[a2] && (s[b1] || s[b3])) || (s[a3] && (s[b2] || s[b3]));
+  if (linked) return false;
+  s[a1] = 1;
+  s[b1] = 1;
+  if (rho[a1] < thr) rho[a1] = thr;
+  if (rho[b1] < thr) rho[b1] = thr;
+  return true;
+}
+
+}  // namespace
+
+extern "C" orc_mesh* orc_surface_nets(int nx, int ny, int nz, float h, const float* origin, const float* density,
+                                      float thr) {
+  orc_mesh* m = new orc_mesh();
+  const int64_t PX = nx + 2, PY = ny + 2, PZ = nz + 2, SY = PX, SZ = PX * PY;
+  std::vector<float> rho((size_t)(PX * PY * PZ), 0.0f);
+  std::vector<uint8_t> sol((size_t)(PX * PY * PZ), 0);
+  for (int z = 0; z < nz; ++z)
+    for (int y = 0; y < ny; ++y)
+      for (int x = 0; x < nx; ++x) {
+        const float v = density[x + (int64_t)nx * (y + (int64_t)ny * z)];
+        const int64_t p = (x + 1) + SY * (y + 1) + SZ * (z + 1);
+        rho[p] = v;
+        sol[p] = v >= thr;
+      }
+  // well-composedness: face saddles, then corner kisses, until a pass changes nothing (at most 8 passes)
+  bool changed = true;
+  while (changed && m->passes < 8) {
+    changed = false;
+    m->passes++;
+    for (int64_t z = 1; z <= nz; ++z)
+      for (int64_t y = 1; y <= ny; ++y)
+        for (int64_t x = 1; x <= nx; ++x) {
+          const int64_t b = x + y * SY + z * SZ;
+          if (x < nx && y < ny && sn_saddle(sol, rho, thr, b, b + 1, b + SY, b + SY + 1)) changed = true, m->changes++;
+          if (x < nx && z < nz && sn_saddle(sol, rho, thr, b, b + 1, b + SZ, b + SZ + 1)) changed = true, m->changes++;
+          if (y < ny && z < nz && sn_saddle(sol, rho, thr, b, b + SY, b + SZ, b + SZ + SY)) changed = true, m->changes++;
+        }
+    for (int64_t z = 1; z < nz; ++z)
+      for (int64_t y = 1; y < ny; ++y)
+        for (int64_t x = 1; x < nx; ++x) {
+          const int64_t c000 = x + y * SY + z * SZ, c100 = c000 + 1, c010 = c000 + SY, c110 = c000 + SY + 1;
+          const int64_t c001 = c000 + SZ, c101 = c001 + 1, c011 = c001 + SY, c111 = c001 + SY + 1;
+          if (sn_kiss(sol, rho, thr, c000, c111, c100, c010, c001, c110, c101, c011) ||
+              sn_kiss(sol, rho, thr, c100, c011, c000, c110, c101, c010, c001, c111) ||
+              sn_kiss(sol, rho, thr, c010, c101, c000, c110, c011, c100, c001, c111) ||
+              sn_kiss(sol, rho, thr, c001, c110, c000, c101, c011, c100, c010, c111))
+            changed = true, m->changes++;
+        }
+  }
+  // one vertex per dual cell with mixed corners, in cell order (cz, cy, cx)
+  static const int edges[12][2] = {{0, 1}, {2, 3}, {4, 5}, {6, 7}, {0, 2}, {1, 3},
+                                   {4, 6}, {5, 7}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
+  const int64_t CX = nx + 1, CY = ny + 1, CZ = nz + 1;
+  std::vector<int32_t> vidx((size_t)(CX * CY * CZ), -1);
+  for (int64_t cz = 0; cz < CZ; ++cz)
+    for (int64_t cy = 0; cy < CY; ++cy)
+      for (int64_t cx = 0; cx < CX; ++cx) {
+        float cr[8];
+        bool cs[8];
+        int mask = 0;
+        for (int c = 0; c < 8; ++c) {
+          const int64_t p = (cx + (c & 1)) + SY * (cy + ((c >> 1) & 1)) + SZ * (cz + (c >> 2));
+          cr[c] = rho[p];
+          cs[c] = sol[p];
+          if (cs[c]) mask |= 1 << c;
+        }
+        if (mask == 0 || mask == 255) continue;
+        float sx = 0.f, sy = 0.f, sz = 0.f;
+        int cnt = 0;
+        for (int e = 0; e < 12; ++e) {
+          const int a = edges[e][0], b = edges[e][1];
+          if (cs[a] == cs[b]) continue;
+          const float va = cr[a], vb = cr[b];
+          const float den = vb - va;
+          float al = 0.5f;
+          if (std::fabs(den) > 1e-12f) {
+            al = (thr - va) / den;
+            al = al < 0.05f ? 0.05f : (al > 0.95f ? 0.95f : al);
+          }
+          const float oa[3] = {(a & 1) - 0.5f, ((a >> 1) & 1) - 0.5f, (a >> 2) - 0.5f};
+          const float ob[3] = {(b & 1) - 0.5f, ((b >> 1) & 1) - 0.5f, (b >> 2) - 0.5f};
+          const float px = oa[0] + al * (ob[0] - oa[0]);
+          const float py = oa[1] + al * (ob[1] - oa[1]);
+          const float pz = oa[2] + al * (ob[2] - oa[2]);
+          sx = sx + px;
+          sy = sy + py;
+          sz = sz + pz;
+          cnt++;
+        }
+        float ox = 0.f, oy = 0.f, oz = 0.f;
+        if (cnt > 0) {
+          const float fc = (float)cnt;
+          ox = sx / fc;
+          oy = sy / fc;
+          oz = sz / fc;
+        }
+        vidx[(size_t)(cx + CX * (cy + CY * cz))] = (int32_t)(m->pos.size() / 3);
+        m->pos.push_back(origin[0] + ((float)cx + ox) * h);
+        m->pos.push_back(origin[1] + ((float)cy + oy) * h);
+        m->pos.push_back(origin[2] + ((float)cz + oz) * h);
+      }
+  if (m->pos.empty()) return m;
+  auto cell = [&](int64_t x, int64_t y, int64_t z) { return vidx[(size_t)(x + CX * (y + CY * z))]; };
+  auto d2 = [&](int32_t i, int32_t j) {
+    const float dx = m->pos[3 * i] - m->pos[3 * j], dy = m->pos[3 * i + 1] - m->pos[3 * j + 1],
+                dz = m->pos[3 * i + 2] - m->pos[3 * j + 2];
+    const float xx = dx * dx, yy = dy * dy, zz = dz * dz;
+    return (xx + yy) + zz;
+  };
+  auto quad = [&](int32_t v0, int32_t v1, int32_t v2, int32_t v3, bool flip) {
+    if (v0 < 0 || v1 < 0 || v2 < 0 || v3 < 0) return;
+    if (flip) std::swap(v1, v3);
+    if (d2(v0, v2) <= d2(v1, v3)) {
+      m->idx.insert(m->idx.end(), {v0, v1, v2, v0, v2, v3});
+    } else {
+      m->idx.insert(m->idx.end(), {v0, v1, v3, v1, v2, v3});
+    }
+  };
+  for (int64_t z = 1; z <= nz; ++z)  // x-directed grid edges
+    for (int64_t y = 1; y <= ny; ++y)
+      for (int64_t x = 0; x <= nx; ++x) {
+        const bool s0 = sol[x + y * SY + z * SZ], s1 = sol[x + 1 + y * SY + z * SZ];
+        if (s0 != s1) quad(cell(x, y - 1, z - 1), cell(x, y, z - 1), cell(x, y, z), cell(x, y - 1, z), !s0);
+      }
+  for (int64_t z = 1; z <= nz; ++z)  // y-directed
+    for (int64_t y = 0; y <= ny; ++y)
+      for (int64_t x = 1; x <= nx; ++x) {
+        const bool s0 = sol[x + y * SY + z * SZ], s1 = sol[x + (y + 1) * SY + z * SZ];
+        if (s0 != s1) quad(cell(x - 1, y, z - 1), cell(x - 1, y, z), cell(x, y, z), cell(x, y, z - 1), !s0);
+      }
+  for (int64_t z = 0; z <= nz; ++z)  // z-directed
+    for (int64_t y = 1; y <= ny; ++y)
+      for (int64_t x = 1; x <= nx; ++x) {
+        const bool s0 = sol[x + y * SY + z * SZ], s1 = sol[x + y * SY + (z + 1) * SZ];
+        if (s0 != s1) quad(cell(x - 1, y - 1, z), cell(x, y - 1, z), cell(x, y, z), cell(x - 1, y, z), !s0);
+      }
+  return m;
+}
+
+extern "C" void orc_mesh_info(const orc_mesh* m, int64_t* out) {
+  out[0] = (int64_t)(m->pos.size() / 3);
+  out[1] = (int64_t)m->idx.size();
+  out[2] = m->passes;
+  out[3] = m->changes;
+}
+extern "C" void orc_mesh_copy(const orc_mesh* m, float* pos, int32_t* idx) {
+  std::copy(m->pos.begin(), m->pos.end(), pos);
+  std::copy(m->idx.begin(), m->idx.end(), idx);
+}
+extern "C" void orc_mesh_free(orc_mesh* m) { delete m; }

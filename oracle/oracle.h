@@ -143,6 +143,14 @@ int orc_topopt_run(orc_model* m, const orc_simp_options* o, orc_iter_record* his
                    int32_t* n_iters, int32_t* converged, double* u_out, float* phys_out, float* design_out,
                    double* rho_phys_active, double* rho_design_active, double* lambda_out, char* msg, int msglen);
 
+/* SurfaceNetsExtractor.Extract: padded threshold field, well-composedness passes, one vertex per mixed dual
+   cell, two triangles per sign-changing grid edge. orc_mesh_info: {vertices, indices, passes, changes}. */
+typedef struct orc_mesh orc_mesh;
+orc_mesh* orc_surface_nets(int nx, int ny, int nz, float h, const float* origin, const float* density, float thr);
+void orc_mesh_info(const orc_mesh* m, int64_t* out);
+void orc_mesh_copy(const orc_mesh* m, float* pos, int32_t* idx);
+void orc_mesh_free(orc_mesh* m);
+
 #ifdef __cplusplus
 }
 #endif

@@ -320,6 +320,26 @@ def quantized_frame(v):
     return out, int(ck)
 
 
+def surface_nets(nx, ny, nz, density, h=1.0, origin=(0.0, 0.0, 0.0), threshold=0.5):
+    """SurfaceNetsExtractor.Extract: (positions float32 [V,3], indices int32 [3T], info {passes, changes})."""
+    L = lib()
+    d = np.ascontiguousarray(density, dtype=np.float32)
+    o = np.ascontiguousarray(origin, dtype=np.float32)
+    L.orc_surface_nets.restype = C.c_void_p
+    L.orc_surface_nets.argtypes = [C.c_int, C.c_int, C.c_int, C.c_float, C.c_void_p, C.c_void_p, C.c_float]
+    L.orc_mesh_info.argtypes = [C.c_void_p, C.c_void_p]
+    L.orc_mesh_copy.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    L.orc_mesh_free.argtypes = [C.c_void_p]
+    m = L.orc_surface_nets(nx, ny, nz, h, o.ctypes.data, d.ctypes.data, threshold)
+    info = np.zeros(4, dtype=np.int64)
+    L.orc_mesh_info(m, info.ctypes.data)
+    pos = np.zeros((int(info[0]), 3), dtype=np.float32)
+    idx = np.zeros(int(info[1]), dtype=np.int32)
+    L.orc_mesh_copy(m, pos.ctypes.data, idx.ctypes.data)
+    L.orc_mesh_free(m)
+    return pos, idx, {"passes": int(info[2]), "changes": int(info[3])}
+
+
 def passive_region(grid, nodes, radius=2):
     out = np.zeros(grid.total_elements, dtype=np.uint8)
     nodes = np.ascontiguousarray(nodes, dtype=np.int32)

@@ -1,0 +1,55 @@
+"""Surface Nets on the device (mycel_surface_nets) against the oracle's sequential restatement of
+SurfaceNetsExtractor.Extract: identical vertex positions (bit for bit), identical triangle indices and order,
+and the same well-composedness passes and resolutions, on the reference tests' fields, border and degenerate
+cases, and saddle-rich fields that drive several passes of the wavefront-scheduled well-composedness kernel."""
+import numpy as np
+import pytest
+
+from mycel_b200 import api
+from mycel_b200.model import ArgumentError, GridSpec
+from meshtools import saddle_field, sphere_field, topology
+
+pytestmark = pytest.mark.gpu
+
+
+def _same(oracle, ctx, nx, ny, nz, dens, h=1.0, origin=(0.0, 0.0, 0.0), thr=0.5):
+    ref_pos, ref_idx, info = oracle.surface_nets(nx, ny, nz, dens, h=h, origin=origin, threshold=thr)
+    m = api.SurfaceNetsExtractor.extract(GridSpec(nx, ny, nz, h, origin), dens, thr, ctx=ctx)
+    assert m.positions.shape == ref_pos.shape and m.indices.shape == ref_idx.shape
+    assert np.array_equal(m.positions.view(np.uint32), ref_pos.view(np.uint32))
+    assert np.array_equal(m.indices, ref_idx)
+    assert (m.passes, m.changes) == (info["passes"], info["changes"])
+    return m
+
+
+def test_sphere_matches_oracle(oracle, ctx):
+    m = _same(oracle, ctx, 32, 32, 32, sphere_field(32, 32, 32, [(16, 16, 16)], 12.0))
+    op, nm, ne, comps = topology(m.indices)
+    assert (op, nm, comps) == (0, 0, 1) and m.vertex_count - ne + m.triangle_count == 2
+
+
+def test_two_spheres_and_border_cube_match_oracle(oracle, ctx):
+    _same(oracle, ctx, 40, 20, 20, sphere_field(40, 20, 20, [(10, 10, 10), (30, 10, 10)], 6.0))
+    _same(oracle, ctx, 10, 10, 10, np.ones(1000, dtype=np.float32), h=2.0, origin=(10.0, 20.0, 30.0))
+
+
+@pytest.mark.parametrize("shape,seed", [((14, 11, 9), 3), ((33, 17, 9), 5), ((1, 7, 5), 1), ((20, 1, 6), 2),
+                                        ((9, 8, 1), 4), ((64, 40, 24), 7)])
+def test_saddle_fields_match_oracle(oracle, ctx, shape, seed):
+    nx, ny, nz = shape
+    m = _same(oracle, ctx, nx, ny, nz, saddle_field(nx, ny, nz, seed=seed), thr=0.5)
+    if min(shape) > 1:
+        assert m.changes > 0
+
+
+def test_threshold_and_empty_fields(oracle, ctx):
+    d = sphere_field(24, 20, 16, [(12, 10, 8)], 6.5)
+    _same(oracle, ctx, 24, 20, 16, d, thr=0.3)
+    _same(oracle, ctx, 24, 20, 16, d, thr=0.8)
+    m = _same(oracle, ctx, 6, 5, 4, np.zeros(120, dtype=np.float32))
+    assert m.vertex_count == 0 and m.triangle_count == 0
+
+
+def test_short_density_is_an_argument_error(ctx):
+    with pytest.raises(ArgumentError, match="smaller than grid element count"):
+        api.SurfaceNetsExtractor.extract(GridSpec(4, 4, 4), np.zeros(63, dtype=np.float32), ctx=ctx)
