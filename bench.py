@@ -88,6 +88,10 @@ def parse():
                     help="static solve of the sphere-carved 96x48x24 box (about 98k active elements) to 1e-8: plain "
                          "FP64, mixed and fast FP64 paths, and the CPU oracle")
     ap.add_argument("--batched", action="store_true", help="48 independent problems submitted at once")
+    ap.add_argument("--surface", action="store_true",
+                    help="iso-surface (Surface Nets) of the bridge's physical density after --surface-iters SIMP "
+                         "iterations: device time vs the CPU oracle, identical meshes")
+    ap.add_argument("--surface-iters", type=int, default=20)
     ap.add_argument("--batched-count", type=int, default=48)
     ap.add_argument("--batched-iters", type=int, default=4)
     ap.add_argument("--job-tol", type=float, default=1e-8,
@@ -355,6 +359,66 @@ def run_static(args):
         out["cpu_baseline"] = {"solve_ms": (time.perf_counter() - t0) * 1000.0, "cores": os.cpu_count() or 1,
                                "kind": "port", "pcg_iterations": cres.solver_info.iterations,
                                "note": "oracle StaticAnalysis.Run (set-up, solve, post-processing)"}
+    print(json.dumps(out), flush=True)
+
+
+def run_surface(args):
+    """Surface Nets of a SIMP design: the 192x96x96 bridge's physical density after --surface-iters iterations of
+    the timed form, extracted at threshold 0.5 on the device (median of 3 calls through the C ABI from host
+    buffers) and by the CPU oracle (the reference's sequential algorithm, one thread); meshes compared."""
+    import torch
+    from mycel_b200 import api
+    from mycel_b200 import workloads as W
+    from mycel_b200.model import GridSpec
+    model, opts = W.bridge_192x96x96()
+    ctx = api.Context(0)
+    prob = api.Problem(model, ctx)
+    sess = api.SimpSession(prob, opts.replace(precision=args.precision, max_iterations=args.surface_iters))
+    for _ in range(args.surface_iters):
+        sess.step()
+    rho = sess.read(u=False, densities=True)["physical"]
+    sess.close()
+    prob.close()
+    g = model.grid
+    grid = GridSpec(g.nx, g.ny, g.nz, g.h)
+    api.SurfaceNetsExtractor.extract(grid, rho, 0.5, ctx=ctx)  # warm-up
+    ts = []
+    for _ in range(3):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        m = api.SurfaceNetsExtractor.extract(grid, rho, 0.5, ctx=ctx)
+        ts.append((time.perf_counter() - t0) * 1000.0)
+    out = {"metric": "Surface Nets iso-surface of the bridge design (192x96x96, threshold 0.5)",
+           "simp_iterations": args.surface_iters, "vertices": m.vertex_count, "triangles": m.triangle_count,
+           "well_composed_passes": m.passes, "resolutions": m.changes,
+           "device_ms": statistics.median(ts), "includes": "host density upload, all kernels, mesh read-back"}
+    if not args.no_cpu:
+        from oracle import oracle as O
+        t0 = time.perf_counter()
+        pos, idx, info = O.surface_nets(g.nx, g.ny, g.nz, rho, h=float(g.h), threshold=0.5)
+        out["cpu_baseline"] = {"ms": (time.perf_counter() - t0) * 1000.0, "cores": 1, "kind": "port",
+                               "sample": "the same extraction, oracle restatement of the reference's sequential code"}
+        out["identical_to_oracle"] = bool(np.array_equal(pos.view(np.uint32), m.positions.view(np.uint32)) and
+                                          np.array_equal(idx, m.indices) and info["passes"] == m.passes)
+        out["speedup_vs_cpu"] = out["cpu_baseline"]["ms"] / out["device_ms"]
+    # the same grid with a saddle-rich density: every pass of the well-composedness sweep runs
+    sd = W.saddle_density(g.nx, g.ny, g.nz, seed=1)
+    api.SurfaceNetsExtractor.extract(grid, sd, 0.5, ctx=ctx)
+    ts = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        ms = api.SurfaceNetsExtractor.extract(grid, sd, 0.5, ctx=ctx)
+        ts.append((time.perf_counter() - t0) * 1000.0)
+    sad = {"vertices": ms.vertex_count, "triangles": ms.triangle_count, "well_composed_passes": ms.passes,
+           "resolutions": ms.changes, "device_ms": statistics.median(ts)}
+    if not args.no_cpu:
+        t0 = time.perf_counter()
+        pos, idx, info = O.surface_nets(g.nx, g.ny, g.nz, sd, h=float(g.h), threshold=0.5)
+        sad["cpu_ms"] = (time.perf_counter() - t0) * 1000.0
+        sad["identical_to_oracle"] = bool(np.array_equal(pos.view(np.uint32), ms.positions.view(np.uint32)) and
+                                          np.array_equal(idx, ms.indices) and info["passes"] == ms.passes and
+                                          info["changes"] == ms.changes)
+    out["saddle_field"] = sad
     print(json.dumps(out), flush=True)
 
 
@@ -655,6 +719,8 @@ if __name__ == "__main__":
         run_batched(a)
     elif a.static and a.impl != "reference":
         run_static(a)
+    elif a.surface and a.impl != "reference":
+        run_surface(a)
     elif a.impl == "reference":
         run_reference(a)
     else:

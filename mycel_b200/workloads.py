@@ -256,3 +256,11 @@ def served_job(nx: int, ny: int, nz: int, n_iters: int, seed: int, precision: st
                             penal=3.0, move_limit=0.2, max_iterations=int(n_iters), solver_tolerance_initial=tol,
                             solver_tolerance_final=tol, solver_max_iterations=20000, precision=precision)
     return model, opts
+
+
+def saddle_density(nx, ny, nz, seed=0, p=0.45):
+    """Seeded float32 density whose 0.5-level set is full of face saddles and corner kisses (the hard case of
+    the iso-surface's well-composedness passes): uniform values, a fraction p of them above 0.5."""
+    rng = np.random.default_rng(seed)
+    v = rng.random(nx * ny * nz).astype(np.float32)
+    return np.where(rng.random(nx * ny * nz) < p, 0.5 + 0.5 * v, 0.5 * v).astype(np.float32)
