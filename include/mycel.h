@@ -209,6 +209,11 @@ int32_t mycel_pcg_solve(mycel_problem* p, const double* b, double* x, double tol
 int32_t mycel_static_solve(mycel_problem* p, const mycel_static_options* opt, const double* warm_start,
                            int64_t warm_start_len, double* u_out, double* reactions_out, double* von_mises_out,
                            double* compliance_out, double* max_displacement_out, mycel_pcg_result* res);
+/* StaticAnalysis.AverageElementToNode (Fem/StaticAnalysis.cs:222-268): nodal_out[node] = mean of
+   element_scalar over the problem's active elements meeting at the node (0 where none does), summed in the
+   reference's element order. len must equal the element count (else MYCEL_E_ARG with the reference's text). */
+int32_t mycel_average_element_to_node(mycel_problem* p, const double* element_scalar, int64_t len,
+                                      double* nodal_out);
 
 /* DensityFilter (Optimization/DensityFilter.cs:34-199) over the problem's active elements, radius in elements. */
 int32_t mycel_filter_create(mycel_problem* p, double rmin, mycel_filter** out);

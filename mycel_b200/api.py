@@ -294,6 +294,21 @@ class StaticAnalysis:
         finally:
             prob.close()
 
+    @staticmethod
+    def average_element_to_node(model: FeModel, element_scalar, ctx: Optional[Context] = None,
+                                problem: Optional["Problem"] = None) -> np.ndarray:
+        """StaticAnalysis.AverageElementToNode: nodal means of an element scalar over the active elements."""
+        prob = problem or Problem(model, ctx)
+        try:
+            es = np.ascontiguousarray(element_scalar, dtype=np.float64).reshape(-1)
+            out = np.zeros(model.total_nodes)
+            _check(L.load().mycel_average_element_to_node(prob.handle, es.ctypes.data, es.size, out.ctypes.data),
+                   prob.ctx)
+            return out
+        finally:
+            if problem is None:
+                prob.close()
+
 
 class IterationController:
     """Cooperative pause / resume / stop between SIMP iterations (IterationController.cs:9-65)."""

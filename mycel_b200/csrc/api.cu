@@ -724,6 +724,19 @@ int32_t solve_dispatch(mycel_problem* p, double* d_u, double tol, int max_iter, 
 }
 }  // namespace mycel
 
+extern "C" int32_t mycel_average_element_to_node(mycel_problem* p, const double* element_scalar, int64_t len,
+                                                 double* nodal_out) {
+  if (!p || !element_scalar || !nodal_out) return set_error(p ? p->ctx : nullptr, MYCEL_E_ARG, "NULL argument");
+  if (len != p->g.ne) return set_error(p->ctx, MYCEL_E_ARG, "elementScalar length must equal TotalElements.");
+  cudaSetDevice(p->ctx->device);
+  cudaStream_t s = p->ctx->stream;
+  MYCEL_CUDA(p->ctx, cudaMemcpyAsync(p->d_tmp0, element_scalar, sizeof(double) * p->g.ne, cudaMemcpyHostToDevice, s));
+  launch_average_e2n(p, p->d_tmp0, p->d_tmp1);
+  MYCEL_CUDA(p->ctx, cudaMemcpyAsync(nodal_out, p->d_tmp1, sizeof(double) * p->g.nn, cudaMemcpyDeviceToHost, s));
+  MYCEL_CUDA(p->ctx, cudaStreamSynchronize(s));
+  return MYCEL_OK;
+}
+
 extern "C" int32_t mycel_static_solve(mycel_problem* p, const mycel_static_options* opt, const double* warm,
                                       int64_t warm_len, double* u_out, double* reactions_out, double* vm_out,
                                       double* compliance_out, double* maxdisp_out, mycel_pcg_result* res) {

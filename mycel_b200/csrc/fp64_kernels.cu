@@ -798,6 +798,33 @@ void launch_von_mises(mycel_problem* p, const double* u, double* vm) {
   p->ctx->launches++;
 }
 
+// StaticAnalysis.AverageElementToNode (Fem/StaticAnalysis.cs:222-268): per node, the mean of the scalars of the
+// active elements meeting there, 0 where none does. A node gathers its (up to 8) elements in increasing element
+// index, the order in which the reference's element loop adds to the node's sum, so the sums are bit-identical.
+__global__ void k_avg_e2n(GridDims g, const double* __restrict__ es, const uint8_t* __restrict__ dom,
+                          double* __restrict__ out) {
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= g.nn) return;
+  const int i = (int)(n % g.nx1), j = (int)((n / g.nx1) % g.ny1), k = (int)(n / ((int64_t)g.nx1 * g.ny1));
+  double sum = 0.0;
+  int cnt = 0;
+  for (int ez = k - 1; ez <= k; ++ez)
+    for (int ey = j - 1; ey <= j; ++ey)
+      for (int ex = i - 1; ex <= i; ++ex) {
+        if (ex < 0 || ey < 0 || ez < 0 || ex >= g.nx || ey >= g.ny || ez >= g.nz) continue;
+        const int64_t e = ex + (int64_t)g.nx * (ey + (int64_t)g.ny * ez);
+        if (!dom[e]) continue;
+        sum = sum + es[e];
+        cnt++;
+      }
+  out[n] = cnt > 0 ? sum / (double)cnt : 0.0;
+}
+
+void launch_average_e2n(mycel_problem* p, const double* es, double* out) {
+  k_avg_e2n<<<(unsigned)((p->g.nn + 255) / 256), 256, 0, p->ctx->stream>>>(p->g, es, p->d_domain, out);
+  p->ctx->launches++;
+}
+
 // active <-> box index maps
 __global__ void k_scatter_active(int64_t na, const int32_t* __restrict__ act, const double* __restrict__ src,
                                  double* __restrict__ dst) {

@@ -232,6 +232,7 @@ void launch_compliance(mycel_problem* p, const double* u, double* d_out);
 void launch_max_disp(mycel_problem* p, const double* u, double* d_out);
 void launch_reactions(mycel_problem* p, const double* ku, double* out, const int32_t* d_fixed, int32_t n_fixed);
 void launch_von_mises(mycel_problem* p, const double* u, double* vm);
+void launch_average_e2n(mycel_problem* p, const double* es, double* out);
 void launch_scatter_active(mycel_problem* p, const double* src_active, double* dst_box, double fill);
 void launch_gather_active(mycel_problem* p, const double* src_box, double* dst_active);
 

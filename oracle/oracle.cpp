@@ -1457,3 +1457,22 @@ extern "C" void orc_mesh_copy(const orc_mesh* m, float* pos, int32_t* idx) {
   std::copy(m->idx.begin(), m->idx.end(), idx);
 }
 extern "C" void orc_mesh_free(orc_mesh* m) { delete m; }
+
+// StaticAnalysis.AverageElementToNode (src/Mycel.Core/Fem/StaticAnalysis.cs:222-268): node sums in the active
+// element order, then sum / count.
+extern "C" void orc_average_element_to_node(const orc_model* m, const double* es, double* out) {
+  const int64_t nx1 = m->nx + 1, ny1 = m->ny + 1;
+  std::vector<double> sum((size_t)m->total_nodes, 0.0);
+  std::vector<int> cnt((size_t)m->total_nodes, 0);
+  for (int32_t e : m->active_elements) {
+    const int64_t ix = e % m->nx, iy = (e / m->nx) % m->ny, iz = e / ((int64_t)m->nx * m->ny);
+    const int64_t n0 = ix + nx1 * (iy + ny1 * iz), n1 = n0 + 1, n3 = n0 + nx1, n2 = n3 + 1;
+    const int64_t n4 = n0 + nx1 * ny1, n5 = n4 + 1, n7 = n4 + nx1, n6 = n7 + 1;
+    const int64_t ns[8] = {n0, n1, n2, n3, n4, n5, n6, n7};
+    for (int64_t q : ns) {
+      sum[(size_t)q] += es[e];
+      cnt[(size_t)q]++;
+    }
+  }
+  for (int64_t q = 0; q < m->total_nodes; ++q) out[q] = cnt[(size_t)q] > 0 ? sum[(size_t)q] / cnt[(size_t)q] : 0.0;
+}

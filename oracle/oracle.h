@@ -145,6 +145,8 @@ int orc_topopt_run(orc_model* m, const orc_simp_options* o, orc_iter_record* his
 
 /* SurfaceNetsExtractor.Extract: padded threshold field, well-composedness passes, one vertex per mixed dual
    cell, two triangles per sign-changing grid edge. orc_mesh_info: {vertices, indices, passes, changes}. */
+/* StaticAnalysis.AverageElementToNode: nodal means of an element scalar over the active elements. */
+void orc_average_element_to_node(const orc_model* m, const double* element_scalar, double* nodal_out);
 typedef struct orc_mesh orc_mesh;
 orc_mesh* orc_surface_nets(int nx, int ny, int nz, float h, const float* origin, const float* density, float thr);
 void orc_mesh_info(const orc_mesh* m, int64_t* out);

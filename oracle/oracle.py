@@ -180,6 +180,15 @@ class Model:
         return dict(active_elements=int(o[0]), active_nodes=int(o[1]), active_fixed=int(o[2]), dofs=int(o[3]),
                     elements=int(o[4]), nodes=int(o[5]))
 
+    def average_element_to_node(self, element_scalar):
+        """StaticAnalysis.AverageElementToNode."""
+        es = np.ascontiguousarray(element_scalar, dtype=np.float64)
+        out = np.zeros(self.fe.total_nodes)
+        L = lib()
+        L.orc_average_element_to_node.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_average_element_to_node(self.h, es.ctypes.data, out.ctypes.data)
+        return out
+
     def constrained(self):
         out = np.zeros(self.fe.total_dofs, dtype=np.uint8)
         lib().orc_model_constrained(self.h, out)

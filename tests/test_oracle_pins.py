@@ -328,3 +328,14 @@ def test_quantization_rounds_half_away_and_clamps():
         f = np.floor(np.float64(c))
         expect.append(int(f + 1 if np.float64(c) - f >= 0.5 else f))
     assert list(q) == expect
+
+
+def test_average_element_to_node_reference_case(oracle):
+    """StaticAnalysisTests.AverageElementToNode_AveragesSharedElementsCorrectly: 2x2x1 grid, scalars 10..40,
+    centre node (1,1,0) = 25, corner node (0,0,0) = 10."""
+    from mycel_b200.model import FeMaterial, FeModel, GridSpec
+    g = GridSpec(2, 2, 1, 1.0)
+    m = FeModel(g, np.ones(4, dtype=np.uint8), FeMaterial(1000.0, 0.3), [0, 1, 2, 3, 4, 5])
+    out = oracle.Model(m).average_element_to_node(np.array([10.0, 20.0, 30.0, 40.0]))
+    assert abs(out[g.node_index(1, 1, 0)] - 25.0) < 1e-10
+    assert abs(out[g.node_index(0, 0, 0)] - 10.0) < 1e-10
