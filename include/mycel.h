@@ -293,6 +293,13 @@ int32_t mycel_mesh_info(const mycel_mesh* m, int64_t* n_vertices, int64_t* n_ind
                         int64_t* changes);
 int32_t mycel_mesh_copy(const mycel_mesh* m, float* positions, int32_t* indices);
 void mycel_mesh_destroy(mycel_mesh* m);
+/* TaubinSmoother.Smooth (PostProcessing/TaubinSmoother.cs:15-134): positions (3 floats per vertex, host) are
+   replaced by the smoothed ones; per vertex the sorted de-duplicated triangle neighbours, then `iterations`
+   times a lambda and a mu Laplacian step (reference defaults 3, 0.5, -0.53), bit-identical to the sequential
+   code. iterations <= 0 or an empty mesh leaves positions unchanged; an index outside the vertex array is
+   MYCEL_E_ARG. */
+int32_t mycel_taubin_smooth(mycel_ctx* ctx, float* positions, int64_t n_vertices, const int32_t* indices,
+                            int64_t n_indices, int32_t iterations, float lambda, float mu);
 
 /* ---- serving: continuous batching of SIMP jobs on one GPU ----
    No counterpart in the reference, whose App runs one optimisation at a time (OptimizationCoordinator.cs:229

@@ -141,6 +141,7 @@ SIGNATURES = {
     "mycel_mesh_info": (i32, [P, C.POINTER(i64), C.POINTER(i64), C.POINTER(i32), C.POINTER(i64)]),
     "mycel_mesh_copy": (i32, [P, P, P]),
     "mycel_mesh_destroy": (None, [P]),
+    "mycel_taubin_smooth": (i32, [P, P, i64, P, i64, i32, C.c_float, C.c_float]),
 }
 
 _lib = None

@@ -627,3 +627,17 @@ class SurfaceNetsExtractor:
         finally:
             lib.mycel_mesh_destroy(h)
         return IndexedMesh(pos, idx, int(passes.value), int(changes.value))
+
+
+class TaubinSmoother:
+    """TaubinSmoother.Smooth (PostProcessing/TaubinSmoother.cs:15-134) on the device."""
+
+    @staticmethod
+    def smooth(mesh: IndexedMesh, iterations: int = 3, lam: float = 0.50, mu: float = -0.53,
+               ctx: Context = None) -> IndexedMesh:
+        ctx = ctx or default_context()
+        pos = np.array(mesh.positions, dtype=np.float32, copy=True, order="C")
+        idx = np.ascontiguousarray(mesh.indices, dtype=np.int32)
+        _check(L.load().mycel_taubin_smooth(ctx.handle, pos.ctypes.data, pos.shape[0], idx.ctypes.data, idx.size,
+                                            int(iterations), float(lam), float(mu)), ctx)
+        return IndexedMesh(pos, idx.copy(), mesh.passes, mesh.changes)

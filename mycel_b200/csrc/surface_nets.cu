@@ -402,6 +402,87 @@ __global__ void k_sn_quads(SnGrid g, int64_t E, const uint8_t* __restrict__ s, c
   }
 }
 
+// ---- TaubinSmoother.Smooth (PostProcessing/TaubinSmoother.cs:15-134) ----
+// Neighbour lists: each triangle adds (i1, i2) to i0, (i2, i0) to i1, (i0, i1) to i2 (slots taken with atomics;
+// the order does not matter because each list is then sorted), then sorted and de-duplicated per vertex, the
+// vertex itself dropped except as the first entry, as in the reference.
+__global__ void k_tb_check(int64_t ni, const int32_t* __restrict__ idx, int64_t nv, int* bad) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < ni; i += (int64_t)gridDim.x * blockDim.x)
+    if (idx[i] < 0 || idx[i] >= nv) *bad = 1;
+}
+
+__global__ void k_tb_degree(int64_t nt, const int32_t* __restrict__ idx, int32_t* deg) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nt; t += (int64_t)gridDim.x * blockDim.x) {
+    atomicAdd(&deg[idx[3 * t]], 2);
+    atomicAdd(&deg[idx[3 * t + 1]], 2);
+    atomicAdd(&deg[idx[3 * t + 2]], 2);
+  }
+}
+
+__global__ void k_tb_fill(int64_t nt, const int32_t* __restrict__ idx, int32_t* cursor, int32_t* __restrict__ nb) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nt; t += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t a = idx[3 * t], b = idx[3 * t + 1], c = idx[3 * t + 2];
+    int32_t k = atomicAdd(&cursor[a], 2);
+    nb[k] = b; nb[k + 1] = c;
+    k = atomicAdd(&cursor[b], 2);
+    nb[k] = c; nb[k + 1] = a;
+    k = atomicAdd(&cursor[c], 2);
+    nb[k] = a; nb[k + 1] = b;
+  }
+}
+
+// sort (insertion: lists are short) and de-duplicate each vertex's list in place; cnt[v] = unique count
+__global__ void k_tb_sort(int64_t nv, const int32_t* __restrict__ off, const int32_t* __restrict__ deg,
+                          int32_t* __restrict__ nb, int32_t* __restrict__ cnt) {
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nv; v += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t s0 = off[v], len = deg[v];
+    if (len == 0) {
+      cnt[v] = 0;
+      continue;
+    }
+    int32_t* l = nb + s0;
+    for (int32_t i = 1; i < len; ++i) {
+      const int32_t x = l[i];
+      int32_t j = i - 1;
+      while (j >= 0 && l[j] > x) {
+        l[j + 1] = l[j];
+        --j;
+      }
+      l[j + 1] = x;
+    }
+    int32_t d = 1;
+    for (int32_t k = 1; k < len; ++k)
+      if (l[k] != l[d - 1] && l[k] != (int32_t)v) l[d++] = l[k];
+    cnt[v] = d;
+  }
+}
+
+// dst[v] = p + (factor / count) * sum over the sorted neighbours q of (q - p), every operation rounded
+__global__ void k_tb_step(int64_t nv, const float* __restrict__ src, float* __restrict__ dst,
+                          const int32_t* __restrict__ off, const int32_t* __restrict__ cnt,
+                          const int32_t* __restrict__ nb, float factor) {
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nv; v += (int64_t)gridDim.x * blockDim.x) {
+    const float px = src[3 * v], py = src[3 * v + 1], pz = src[3 * v + 2];
+    const int32_t c = cnt[v];
+    if (c == 0) {
+      dst[3 * v] = px; dst[3 * v + 1] = py; dst[3 * v + 2] = pz;
+      continue;
+    }
+    const int32_t* l = nb + off[v];
+    float sx = 0.f, sy = 0.f, sz = 0.f;
+    for (int32_t k = 0; k < c; ++k) {
+      const int64_t q = l[k];
+      sx = __fadd_rn(sx, __fsub_rn(src[3 * q], px));
+      sy = __fadd_rn(sy, __fsub_rn(src[3 * q + 1], py));
+      sz = __fadd_rn(sz, __fsub_rn(src[3 * q + 2], pz));
+    }
+    const float w = __fdiv_rn(factor, (float)c);
+    dst[3 * v] = __fadd_rn(px, __fmul_rn(w, sx));
+    dst[3 * v + 1] = __fadd_rn(py, __fmul_rn(w, sy));
+    dst[3 * v + 2] = __fadd_rn(pz, __fmul_rn(w, sz));
+  }
+}
+
 int sn_grid_blocks(int64_t n, int num_sms) {
   return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)num_sms * 16));
 }
@@ -553,3 +634,73 @@ extern "C" int32_t mycel_mesh_copy(const mycel_mesh* m, float* positions, int32_
 }
 
 extern "C" void mycel_mesh_destroy(mycel_mesh* m) { delete m; }
+
+extern "C" int32_t mycel_taubin_smooth(mycel_ctx* ctx, float* positions, int64_t n_vertices, const int32_t* indices,
+                                       int64_t n_indices, int32_t iterations, float lambda, float mu) {
+  if (!ctx || (!positions && n_vertices) || (!indices && n_indices)) return set_error(ctx, MYCEL_E_ARG, "NULL argument");
+  if (n_vertices < 0 || n_indices < 0 || n_indices % 3) return set_error(ctx, MYCEL_E_ARG, "indices must hold whole triangles");
+  if (iterations <= 0 || n_vertices == 0 || n_indices == 0) return MYCEL_OK;  // the mesh is returned unchanged
+  if (n_indices >= INT32_MAX / 2 || n_vertices >= INT32_MAX)
+    return set_error(ctx, MYCEL_E_ARG, "mesh too large for the smoother (index count beyond 2^30)");
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->stream;
+  const int64_t nv = n_vertices, ni = n_indices, nt = ni / 3;
+  std::vector<void*> bufs;
+  bool oom = false;
+  auto alloc = [&](size_t bytes) -> void* {
+    void* p = nullptr;
+    if (oom || cudaMallocAsync(&p, bytes + 16, s) != cudaSuccess) {
+      oom = true;
+      return nullptr;
+    }
+    bufs.push_back(p);
+    return p;
+  };
+  struct Free {
+    std::vector<void*>* b;
+    cudaStream_t s;
+    ~Free() {
+      for (void* p : *b) cudaFreeAsync(p, s);
+    }
+  } guard{&bufs, s};
+  int32_t* d_idx = (int32_t*)alloc(sizeof(int32_t) * ni);
+  float* d_a = (float*)alloc(sizeof(float) * 3 * nv);
+  float* d_b = (float*)alloc(sizeof(float) * 3 * nv);
+  int32_t* d_deg = (int32_t*)alloc(sizeof(int32_t) * nv);
+  int32_t* d_off = (int32_t*)alloc(sizeof(int32_t) * nv);
+  int32_t* d_cur = (int32_t*)alloc(sizeof(int32_t) * nv);
+  int32_t* d_cnt = (int32_t*)alloc(sizeof(int32_t) * nv);
+  int32_t* d_nb = (int32_t*)alloc(sizeof(int32_t) * 2 * ni);
+  int32_t* d_sums = (int32_t*)alloc(sizeof(int32_t) * ((nv + kScanBlock - 1) / kScanBlock + 1));
+  long long* d_tot = (long long*)alloc(sizeof(long long) * 2);
+  int* d_bad = (int*)alloc(sizeof(int));
+  if (oom) return set_error(ctx, MYCEL_E_OOM, "out of device memory for the mesh smoother");
+  int* h_bad = (int*)ctx->pinned;
+  const int nsm = ctx->num_sms;
+  MYCEL_CUDA(ctx, cudaMemcpyAsync(d_idx, indices, sizeof(int32_t) * ni, cudaMemcpyHostToDevice, s));
+  MYCEL_CUDA(ctx, cudaMemcpyAsync(d_a, positions, sizeof(float) * 3 * nv, cudaMemcpyHostToDevice, s));
+  MYCEL_CUDA(ctx, cudaMemsetAsync(d_bad, 0, sizeof(int), s));
+  MYCEL_CUDA(ctx, cudaMemsetAsync(d_deg, 0, sizeof(int32_t) * nv, s));
+  k_tb_check<<<sn_grid_blocks(ni, nsm), 256, 0, s>>>(ni, d_idx, nv, d_bad);
+  MYCEL_CUDA(ctx, cudaMemcpyAsync(h_bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+  MYCEL_CUDA(ctx, cudaStreamSynchronize(s));
+  ctx->launches++;
+  if (*h_bad) return set_error(ctx, MYCEL_E_ARG, "triangle index out of range of the vertex array");
+  k_tb_degree<<<sn_grid_blocks(nt, nsm), 256, 0, s>>>(nt, d_idx, d_deg);
+  MYCEL_CUDA(ctx, cudaMemcpyAsync(d_off, d_deg, sizeof(int32_t) * nv, cudaMemcpyDeviceToDevice, s));
+  ctx->launches++;
+  if (int32_t st = sn_scan(ctx, d_off, nv, d_sums, d_tot)) return st;
+  MYCEL_CUDA(ctx, cudaMemcpyAsync(d_cur, d_off, sizeof(int32_t) * nv, cudaMemcpyDeviceToDevice, s));
+  k_tb_fill<<<sn_grid_blocks(nt, nsm), 256, 0, s>>>(nt, d_idx, d_cur, d_nb);
+  k_tb_sort<<<sn_grid_blocks(nv, nsm), 256, 0, s>>>(nv, d_off, d_deg, d_nb, d_cnt);
+  ctx->launches += 2;
+  for (int it = 0; it < iterations; ++it) {
+    k_tb_step<<<sn_grid_blocks(nv, nsm), 256, 0, s>>>(nv, d_a, d_b, d_off, d_cnt, d_nb, lambda);
+    k_tb_step<<<sn_grid_blocks(nv, nsm), 256, 0, s>>>(nv, d_b, d_a, d_off, d_cnt, d_nb, mu);
+    ctx->launches += 2;
+  }
+  MYCEL_CUDA(ctx, cudaGetLastError());
+  MYCEL_CUDA(ctx, cudaMemcpyAsync(positions, d_a, sizeof(float) * 3 * nv, cudaMemcpyDeviceToHost, s));
+  MYCEL_CUDA(ctx, cudaStreamSynchronize(s));
+  return MYCEL_OK;
+}

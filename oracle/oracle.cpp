@@ -1476,3 +1476,54 @@ extern "C" void orc_average_element_to_node(const orc_model* m, const double* es
   }
   for (int64_t q = 0; q < m->total_nodes; ++q) out[q] = cnt[(size_t)q] > 0 ? sum[(size_t)q] / cnt[(size_t)q] : 0.0;
 }
+
+// TaubinSmoother.Smooth (src/Mycel.Core/PostProcessing/TaubinSmoother.cs:15-101, ApplyLaplacianStep :103-134):
+// per vertex the sorted, de-duplicated neighbours over all triangles; each iteration a +lambda then a mu
+// Laplacian step, p + (factor / count) * sum(q - p) with every Vector3 operation rounded per component.
+extern "C" void orc_taubin_smooth(float* pos, int64_t nv, const int32_t* idx, int64_t ni, int iterations, float lambda,
+                                  float mu) {
+  if (iterations <= 0 || nv == 0 || ni < 3) return;
+  std::vector<std::vector<int32_t>> nb((size_t)nv);
+  for (int64_t t = 0; t + 2 < ni; t += 3) {
+    const int32_t a = idx[t], b = idx[t + 1], c = idx[t + 2];
+    nb[a].push_back(b); nb[a].push_back(c);
+    nb[b].push_back(c); nb[b].push_back(a);
+    nb[c].push_back(a); nb[c].push_back(b);
+  }
+  for (int64_t v = 0; v < nv; ++v) {
+    auto& l = nb[(size_t)v];
+    if (l.empty()) continue;
+    std::sort(l.begin(), l.end());
+    std::vector<int32_t> u;
+    u.push_back(l[0]);
+    for (size_t k = 1; k < l.size(); ++k)
+      if (l[k] != u.back() && l[k] != (int32_t)v) u.push_back(l[k]);
+    l.swap(u);
+  }
+  std::vector<float> cur(pos, pos + 3 * nv), tmp((size_t)(3 * nv));
+  auto step = [&](const std::vector<float>& src, std::vector<float>& dst, float factor) {
+    for (int64_t v = 0; v < nv; ++v) {
+      const auto& l = nb[(size_t)v];
+      const float px = src[3 * v], py = src[3 * v + 1], pz = src[3 * v + 2];
+      if (l.empty()) {
+        dst[3 * v] = px; dst[3 * v + 1] = py; dst[3 * v + 2] = pz;
+        continue;
+      }
+      float sx = 0.f, sy = 0.f, sz = 0.f;
+      for (int32_t q : l) {
+        sx = sx + (src[3 * (size_t)q] - px);
+        sy = sy + (src[3 * (size_t)q + 1] - py);
+        sz = sz + (src[3 * (size_t)q + 2] - pz);
+      }
+      const float w = factor / (float)l.size();
+      dst[3 * v] = px + w * sx;
+      dst[3 * v + 1] = py + w * sy;
+      dst[3 * v + 2] = pz + w * sz;
+    }
+  };
+  for (int it = 0; it < iterations; ++it) {
+    step(cur, tmp, lambda);
+    step(tmp, cur, mu);
+  }
+  std::copy(cur.begin(), cur.end(), pos);
+}

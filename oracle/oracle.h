@@ -148,6 +148,8 @@ int orc_topopt_run(orc_model* m, const orc_simp_options* o, orc_iter_record* his
 /* StaticAnalysis.AverageElementToNode: nodal means of an element scalar over the active elements. */
 void orc_average_element_to_node(const orc_model* m, const double* element_scalar, double* nodal_out);
 typedef struct orc_mesh orc_mesh;
+/* TaubinSmoother.Smooth on positions (3 floats per vertex) in place. */
+void orc_taubin_smooth(float* pos, int64_t nv, const int32_t* idx, int64_t ni, int iterations, float lambda, float mu);
 orc_mesh* orc_surface_nets(int nx, int ny, int nz, float h, const float* origin, const float* density, float thr);
 void orc_mesh_info(const orc_mesh* m, int64_t* out);
 void orc_mesh_copy(const orc_mesh* m, float* pos, int32_t* idx);

@@ -349,6 +349,16 @@ def surface_nets(nx, ny, nz, density, h=1.0, origin=(0.0, 0.0, 0.0), threshold=0
     return pos, idx, {"passes": int(info[2]), "changes": int(info[3])}
 
 
+def taubin_smooth(positions, indices, iterations=3, lam=0.5, mu=-0.53):
+    """TaubinSmoother.Smooth: smoothed copy of positions [V, 3] float32."""
+    L = lib()
+    p = np.array(positions, dtype=np.float32, copy=True, order="C")
+    i = np.ascontiguousarray(indices, dtype=np.int32)
+    L.orc_taubin_smooth.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int, C.c_float, C.c_float]
+    L.orc_taubin_smooth(p.ctypes.data, p.shape[0], i.ctypes.data, i.size, iterations, lam, mu)
+    return p
+
+
 def passive_region(grid, nodes, radius=2):
     out = np.zeros(grid.total_elements, dtype=np.uint8)
     nodes = np.ascontiguousarray(nodes, dtype=np.int32)

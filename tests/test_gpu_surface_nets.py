@@ -53,3 +53,23 @@ def test_threshold_and_empty_fields(oracle, ctx):
 def test_short_density_is_an_argument_error(ctx):
     with pytest.raises(ArgumentError, match="smaller than grid element count"):
         api.SurfaceNetsExtractor.extract(GridSpec(4, 4, 4), np.zeros(63, dtype=np.float32), ctx=ctx)
+
+
+@pytest.mark.parametrize("iters", [1, 3, 7])
+def test_taubin_matches_oracle(oracle, ctx, iters):
+    d = sphere_field(40, 20, 20, [(10, 10, 10), (30, 10, 10)], 6.0)
+    m = api.SurfaceNetsExtractor.extract(GridSpec(40, 20, 20), d, 0.5, ctx=ctx)
+    sm = api.TaubinSmoother.smooth(m, iters, ctx=ctx)
+    ref = oracle.taubin_smooth(m.positions, m.indices, iters)
+    assert np.array_equal(sm.positions.view(np.uint32), ref.view(np.uint32))
+    assert np.array_equal(sm.indices, m.indices)
+
+
+def test_taubin_on_saddle_mesh_and_bad_index(oracle, ctx):
+    d = saddle_field(20, 14, 10, seed=9)
+    m = api.SurfaceNetsExtractor.extract(GridSpec(20, 14, 10), d, 0.5, ctx=ctx)
+    sm = api.TaubinSmoother.smooth(m, 3, ctx=ctx)
+    assert np.array_equal(sm.positions.view(np.uint32), oracle.taubin_smooth(m.positions, m.indices, 3).view(np.uint32))
+    bad = api.IndexedMesh(m.positions, np.concatenate([m.indices[:-3], [0, 1, m.vertex_count]]).astype(np.int32))
+    with pytest.raises(ArgumentError, match="out of range"):
+        api.TaubinSmoother.smooth(bad, 3, ctx=ctx)

@@ -46,3 +46,19 @@ def test_saddle_field_is_made_well_composed(oracle):
     assert info["changes"] > 0 and info["passes"] >= 2
     op, nm, _, _ = topology(idx)
     assert op == 0
+
+
+def test_taubin_keeps_topology_and_volume(oracle):
+    """The reference's export test (Step6Tests T3) smooths the extracted sphere with 3 Taubin iterations and
+    requires a watertight result whose volume is kept: topology unchanged, volume within 1 %, and the
+    staircase reduced (radial spread of the vertices shrinks)."""
+    n = 24
+    pos, idx, _ = oracle.surface_nets(n, n, n, sphere_field(n, n, n, [(12, 12, 12)], 8.0))
+    sm = oracle.taubin_smooth(pos, idx, 3)
+    assert sm.shape == pos.shape and not np.array_equal(sm, pos)
+    v0, v1 = signed_volume(pos, idx), signed_volume(sm, idx)
+    assert abs(v1 - v0) / abs(v0) < 0.01
+    r0 = np.linalg.norm(pos - 12.0, axis=1)
+    r1 = np.linalg.norm(sm - 12.0, axis=1)
+    assert r1.std() < r0.std()
+    assert np.array_equal(oracle.taubin_smooth(pos, idx, 0), pos)
