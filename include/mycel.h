@@ -289,6 +289,10 @@ int32_t mycel_simp_frame_end(mycel_simp_session* s, int32_t slot, uint8_t* frame
 typedef struct mycel_mesh mycel_mesh;
 int32_t mycel_surface_nets(mycel_ctx* ctx, int32_t nx, int32_t ny, int32_t nz, float h, const float* origin,
                            const float* density, int64_t density_len, float threshold, mycel_mesh** out);
+/* The same extraction from a SIMP session's physical density of its last iteration, which stays on the device
+   (the float field the snapshots read), for a per-iteration preview without copying the density to the host.
+   origin may be NULL (0, 0, 0). */
+int32_t mycel_simp_surface_nets(mycel_simp_session* s, const float* origin, float threshold, mycel_mesh** out);
 int32_t mycel_mesh_info(const mycel_mesh* m, int64_t* n_vertices, int64_t* n_indices, int32_t* passes,
                         int64_t* changes);
 int32_t mycel_mesh_copy(const mycel_mesh* m, float* positions, int32_t* indices);

@@ -138,6 +138,7 @@ SIGNATURES = {
     "mycel_job_device_bytes": (i64, [C.POINTER(JobSpec)]),
     "mycel_average_element_to_node": (i32, [P, P, i64, P]),
     "mycel_surface_nets": (i32, [P, i32, i32, i32, C.c_float, P, P, i64, C.c_float, C.POINTER(P)]),
+    "mycel_simp_surface_nets": (i32, [P, P, C.c_float, C.POINTER(P)]),
     "mycel_mesh_info": (i32, [P, C.POINTER(i64), C.POINTER(i64), C.POINTER(i32), C.POINTER(i64)]),
     "mycel_mesh_copy": (i32, [P, P, P]),
     "mycel_mesh_destroy": (None, [P]),

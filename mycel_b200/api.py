@@ -450,6 +450,23 @@ class SimpSession:
                                         C.byref(lam)), self.problem.ctx)
         return dict(u=uu, physical=ph, design=de, rho_phys_active=rpa, rho_design_active=rda, lam=lam.value)
 
+    def surface_mesh(self, threshold: float = 0.5, origin=(0.0, 0.0, 0.0)):
+        """Iso-surface (SurfaceNetsExtractor.Extract) of the last iteration's physical density, extracted from
+        the device-resident field (no host copy of the density)."""
+        o = np.ascontiguousarray(origin, dtype=np.float32)
+        lib = L.load()
+        h = C.c_void_p()
+        _check(lib.mycel_simp_surface_nets(self.handle, o.ctypes.data, float(threshold), C.byref(h)), self.problem.ctx)
+        try:
+            nv, ni, passes, changes = C.c_int64(0), C.c_int64(0), C.c_int32(0), C.c_int64(0)
+            _check(lib.mycel_mesh_info(h, C.byref(nv), C.byref(ni), C.byref(passes), C.byref(changes)))
+            pos = np.zeros((nv.value, 3), dtype=np.float32)
+            idx = np.zeros(ni.value, dtype=np.int32)
+            _check(lib.mycel_mesh_copy(h, pos.ctypes.data, idx.ctypes.data))
+        finally:
+            lib.mycel_mesh_destroy(h)
+        return IndexedMesh(pos, idx, int(passes.value), int(changes.value))
+
     def frame_begin(self) -> int:
         """Start the RunWriter frame of the last iteration (quantised on the device, copied without waiting)."""
         slot = C.c_int32(-1)

@@ -233,6 +233,8 @@ void launch_max_disp(mycel_problem* p, const double* u, double* d_out);
 void launch_reactions(mycel_problem* p, const double* ku, double* out, const int32_t* d_fixed, int32_t n_fixed);
 void launch_von_mises(mycel_problem* p, const double* u, double* vm);
 void launch_average_e2n(mycel_problem* p, const double* es, double* out);
+int32_t surface_nets_core(mycel_ctx* ctx, int32_t nx, int32_t ny, int32_t nz, float h, const float* origin,
+                          const float* h_density, const float* d_density, float threshold, mycel_mesh** out);
 void launch_scatter_active(mycel_problem* p, const double* src_active, double* dst_box, double fill);
 void launch_gather_active(mycel_problem* p, const double* src_box, double* dst_active);
 

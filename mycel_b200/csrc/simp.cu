@@ -552,3 +552,16 @@ extern "C" int32_t mycel_simp_run(mycel_problem* p, const mycel_simp_options* op
 namespace mycel {
 bool simp_session_converged(const mycel_simp_session* s) { return s && s->converged; }
 }  // namespace mycel
+
+extern "C" int32_t mycel_simp_surface_nets(mycel_simp_session* s, const float* origin, float threshold,
+                                           mycel_mesh** out) {
+  if (!s || !out) return set_error(s ? s->p->ctx : nullptr, MYCEL_E_ARG, "NULL argument");
+  mycel_problem* p = s->p;
+  mycel_ctx* c = p->ctx;
+  cudaSetDevice(c->device);
+  if (s->count == 0) return set_error(c, MYCEL_E_INVALID_OPERATION, "no iteration has been run yet");
+  const float zero[3] = {0.0f, 0.0f, 0.0f};
+  snapshot(s);  // the float physical density of the last iteration, on the device
+  return surface_nets_core(c, p->g.nx, p->g.ny, p->g.nz, p->h, origin ? origin : zero, nullptr, s->d_phys_f,
+                           threshold, out);
+}

@@ -503,15 +503,13 @@ int32_t sn_scan(mycel_ctx* c, int32_t* a, int64_t n, int32_t* sums, long long* t
 
 using namespace mycel;
 
-extern "C" int32_t mycel_surface_nets(mycel_ctx* ctx, int32_t nx, int32_t ny, int32_t nz, float h, const float* origin,
-                                      const float* density, int64_t density_len, float threshold, mycel_mesh** out) {
-  if (!ctx || !density || !origin || !out) return set_error(ctx, MYCEL_E_ARG, "NULL argument");
+namespace mycel {
+// The extraction from a density already in device memory (d_density: nx*ny*nz floats, box order), or from
+// host memory (h_density, copied in first).
+int32_t surface_nets_core(mycel_ctx* ctx, int32_t nx, int32_t ny, int32_t nz, float h, const float* origin,
+                          const float* h_density, const float* d_density, float threshold, mycel_mesh** out) {
   *out = nullptr;
-  if (nx < 1 || ny < 1 || nz < 1) return set_error(ctx, MYCEL_E_ARG, "Grid dimensions must be positive.");
   const int64_t n = (int64_t)nx * ny * nz;
-  if (density_len < n)
-    return set_error(ctx, MYCEL_E_ARG, "physicalDensity length (" + std::to_string(density_len) +
-                                           ") is smaller than grid element count (" + std::to_string(n) + ").");
   const int64_t CX = nx + 1, CY = ny + 1, CZ = nz + 1, C = CX * CY * CZ;
   const int64_t P = (int64_t)(nx + 2) * (ny + 2) * (nz + 2);
   const int64_t E = (int64_t)nz * ny * (nx + 1) + (int64_t)nz * (ny + 1) * nx + (int64_t)(nz + 1) * ny * nx;
@@ -539,7 +537,7 @@ extern "C" int32_t mycel_surface_nets(mycel_ctx* ctx, int32_t nx, int32_t ny, in
       for (void* p : *b) cudaFreeAsync(p, s);
     }
   } guard{&bufs, s};
-  float* d_in = (float*)alloc(sizeof(float) * n);
+  float* d_in = h_density ? (float*)alloc(sizeof(float) * n) : const_cast<float*>(d_density);
   float* d_rho = (float*)alloc(sizeof(float) * P);
   uint8_t* d_s = (uint8_t*)alloc(P);
   int32_t* d_cflag = (int32_t*)alloc(sizeof(int32_t) * C);
@@ -554,7 +552,7 @@ extern "C" int32_t mycel_surface_nets(mycel_ctx* ctx, int32_t nx, int32_t ny, in
   int* d_flags = (int*)alloc(sizeof(int) * 8);
   if (oom) return set_error(ctx, MYCEL_E_OOM, "out of device memory for the iso-surface");
   long long* h_scal = (long long*)ctx->pinned;  // at least 64 bytes of pinned scratch
-  MYCEL_CUDA(ctx, cudaMemcpyAsync(d_in, density, sizeof(float) * n, cudaMemcpyHostToDevice, s));
+  if (h_density) MYCEL_CUDA(ctx, cudaMemcpyAsync(d_in, h_density, sizeof(float) * n, cudaMemcpyHostToDevice, s));
   MYCEL_CUDA(ctx, cudaMemsetAsync(d_scal, 0, sizeof(long long) * 8, s));
   MYCEL_CUDA(ctx, cudaMemsetAsync(d_flags, 0, sizeof(int) * 8, s));
   const int nsm = ctx->num_sms;
@@ -614,6 +612,19 @@ extern "C" int32_t mycel_surface_nets(mycel_ctx* ctx, int32_t nx, int32_t ny, in
   *out = m;
   m = nullptr;
   return MYCEL_OK;
+}
+}  // namespace mycel
+
+extern "C" int32_t mycel_surface_nets(mycel_ctx* ctx, int32_t nx, int32_t ny, int32_t nz, float h, const float* origin,
+                                      const float* density, int64_t density_len, float threshold, mycel_mesh** out) {
+  if (!ctx || !density || !origin || !out) return set_error(ctx, MYCEL_E_ARG, "NULL argument");
+  *out = nullptr;
+  if (nx < 1 || ny < 1 || nz < 1) return set_error(ctx, MYCEL_E_ARG, "Grid dimensions must be positive.");
+  const int64_t n = (int64_t)nx * ny * nz;
+  if (density_len < n)
+    return set_error(ctx, MYCEL_E_ARG, "physicalDensity length (" + std::to_string(density_len) +
+                                           ") is smaller than grid element count (" + std::to_string(n) + ").");
+  return surface_nets_core(ctx, nx, ny, nz, h, origin, density, nullptr, threshold, out);
 }
 
 extern "C" int32_t mycel_mesh_info(const mycel_mesh* m, int64_t* n_vertices, int64_t* n_indices, int32_t* passes,

@@ -73,3 +73,22 @@ def test_taubin_on_saddle_mesh_and_bad_index(oracle, ctx):
     bad = api.IndexedMesh(m.positions, np.concatenate([m.indices[:-3], [0, 1, m.vertex_count]]).astype(np.int32))
     with pytest.raises(ArgumentError, match="out of range"):
         api.TaubinSmoother.smooth(bad, 3, ctx=ctx)
+
+
+def test_session_mesh_equals_host_extraction(oracle, ctx):
+    """The preview path: a SIMP session's iso-surface from its device-resident density equals the extraction
+    of the density it reads back (and the oracle's)."""
+    from mycel_b200 import workloads as W
+    m, o = W.simp_cantilever_40x20x10()
+    pr = api.Problem(m, ctx)
+    s = api.SimpSession(pr, o.replace(max_iterations=6))
+    for _ in range(6):
+        s.step()
+    mesh = s.surface_mesh(0.5)
+    rho = s.read(u=False, densities=True)["physical"]
+    g = m.grid
+    ref = _same(oracle, ctx, g.nx, g.ny, g.nz, rho, h=float(g.h))
+    assert np.array_equal(mesh.positions.view(np.uint32), ref.positions.view(np.uint32))
+    assert np.array_equal(mesh.indices, ref.indices) and mesh.triangle_count > 0
+    s.close()
+    pr.close()
