@@ -1657,6 +1657,9 @@ constexpr int kMgCoarseMax = 144;  // DOFs of the coarsest level (its dense FP64
 // D^-1 A estimated by kMgPowerIters power iterations at each set-up (from below, hence the margin to 2).
 constexpr float kMgOmegaScale = 4.0f / 3.0f;
 constexpr int kMgPowerIters = 8;
+// Later set-ups of the same problem start from the previous set-up's eigenvector estimate (the design changes
+// little from one solve to the next) and take kMgPowerItersWarm iterations.
+constexpr int kMgPowerItersWarm = 3;
 constexpr size_t kMgCoarseSmem = (size_t)kMgCoarseMax * kMgCoarseMax * 8 + kMgCoarseMax * 8;
 
 struct MgDims {
@@ -2689,6 +2692,8 @@ struct MgHier {
   int graph32_profiled = 0;
   cudaEvent_t ev32[2][2] = {};
   float* f_t = nullptr;  // FP32 outer form: A x of the voxel level's smoothing (padded FP32 layout)
+  float* eig[kMgMaxLevels] = {};  // last eigenvector estimate of D^-1 A per smoothed level (warm start)
+  bool eig_valid = false;
   int T = 1;             // first level handled by the cluster kernel k_mg_tail
   MgTail tail{};
   bool prefers_f64 = false;  // an FP32 outer solve of this problem stalled: later ones start in FP64
@@ -2719,6 +2724,8 @@ int64_t mg_device_bytes(int nx, int ny, int nz) {
   b += sizeof(MgScratch) + 64 + 4 * 8 * 576 + 64 + (int64_t)lv[1].nx * lv[1].ny * lv[1].nz + 64;
   const int64_t rp = (3 * (int64_t)(nx + 1) + 3) & ~int64_t(3);  // FP32 row pitch of the voxel level
   b += 4 * rp * (ny + 1) * (nz + 1) + 64;                         // f_t
+  b += 4 * rp * (ny + 1) * (nz + 1) + 64;                         // eigenvector estimate of the voxel level
+  for (int l = 1; l < L - 1; ++l) b += 4 * 3 * mg_nn(lv[l]) + 64; // and of the coarse smoothed levels
   b += 4 * 576 * (int64_t)lv[1].nx * lv[1].ny * lv[1].nz + 64;
   if (L > 2) b += 4 * 576 * (int64_t)lv[2].nx * lv[2].ny * lv[2].nz + 64;
   b += 8 * 9 * mg_nn(lv[L - 1]) * mg_nn(lv[L - 1]) + 64;
@@ -2791,6 +2798,7 @@ static int32_t mg_ensure(mycel_problem* p, bool* available) {
   mg->ainv = (double*)alloc(sizeof(double) * nc * nc);
   mg->sc = (MgScratch*)alloc(sizeof(MgScratch));
   mg->f_t = (float*)alloc(sizeof(float) * (size_t)p->g.n32);
+  for (int l = 0; l < L - 1; ++l) mg->eig[l] = (float*)alloc(sizeof(float) * (size_t)(l ? mg->lv[l].nd : p->g.n32));
   mg->G = (float*)alloc(sizeof(float) * 8 * 576);
   mg->special = (uint8_t*)alloc((size_t)dims[1].nx * dims[1].ny * dims[1].nz);
   if (!oom) {  // G_s = W_s^T KE W_s for an interior coarse element (all sub-elements present), in FP64
@@ -2897,17 +2905,23 @@ static void mg_setup(mycel_problem* p) {
     float* x = l ? v.xa : p->f_p0;
     float* y = l ? v.t : p->f_ap;
     const unsigned nb = l ? std::min<unsigned>(mg_blocks(n), (unsigned)sb) : (unsigned)sb;
-    k_mg_pow_init<<<nb, 256, 0, s>>>(n, invd, x);
-    for (int it = 0; it < kMgPowerIters; ++it) {
+    if (mg->eig_valid) {
+      cudaMemcpyAsync(x, mg->eig[l], sizeof(float) * (size_t)n, cudaMemcpyDeviceToDevice, s);
+    } else {
+      k_mg_pow_init<<<nb, 256, 0, s>>>(n, invd, x);
+      nl++;
+    }
+    const int iters = mg->eig_valid ? kMgPowerItersWarm : kMgPowerIters;
+    for (int it = 0; it < iters; ++it) {
       if (l) launch_mg_apply(s, v, x, nullptr, invd, y, 0, nullptr, nullptr);
       else launch_mv32_variant<0>(p, s, p->f_p0, nullptr, nullptr, nullptr, p->f_ap, 1, nullptr, nullptr);
-      const bool last = it == kMgPowerIters - 1;
+      const bool last = it == iters - 1;
       k_mg_pow_norm<<<nb, kT, 0, s>>>(n, y, invd, p->d_part2, mg->sc, last ? l : -1);
-      if (!last) k_mg_pow_scale<<<nb, 256, 0, s>>>(n, y, invd, mg->sc, x);
-      nl += last ? 2 : 3;
+      k_mg_pow_scale<<<nb, 256, 0, s>>>(n, y, invd, mg->sc, last ? mg->eig[l] : x);
+      nl += 3;
     }
-    nl++;
   }
+  mg->eig_valid = true;
   p->ctx->launches += nl;
 }
 
