@@ -909,6 +909,103 @@ __global__ void k_filter_apply(GridDims g, const uint8_t* __restrict__ dom, cons
   out[e] = s;
 }
 
+// The same sums as a shared-memory stencil: a CTA stages a 32 x 8 x 2 element tile with an rc-element halo
+// (the input, the element flags and, for the adjoint, 1/Hs; outside the grid or inactive: flag 0) and the
+// offset list, then each thread forms its elements' sums from shared memory in the reference's neighbour order
+// with the same operations, so the results are those of k_filter_apply bit for bit.
+constexpr int kFtX = 32, kFtY = 8, kFtZ = 2;
+
+__host__ __device__ inline size_t filter_tile_smem(int rc, int noff, bool adj) {
+  const size_t nt = (size_t)(kFtX + 2 * rc) * (kFtY + 2 * rc) * (kFtZ + 2 * rc);
+  size_t b = nt * 8 * (adj ? 2 : 1);
+  b = (b + 15) & ~(size_t)15;
+  b += (size_t)noff * 16 + (size_t)noff * 8 + nt;
+  return b;
+}
+
+template <int ADJ>
+__global__ void __launch_bounds__(256) k_filter_tile(GridDims g, int rc, const uint8_t* __restrict__ dom,
+                                                     const int4* __restrict__ off, const double* __restrict__ w,
+                                                     int noff, const double* __restrict__ invhs,
+                                                     const double* __restrict__ in, double* __restrict__ out,
+                                                     int ones) {
+  extern __shared__ __align__(16) unsigned char ftile[];
+  const int PX = kFtX + 2 * rc, PY = kFtY + 2 * rc, PZ = kFtZ + 2 * rc, nt = PX * PY * PZ;
+  double* sv = reinterpret_cast<double*>(ftile);
+  double* sh = sv + nt;  // adjoint only
+  size_t ob = (size_t)nt * 8 * (ADJ ? 2 : 1);
+  ob = (ob + 15) & ~(size_t)15;
+  int4* so = reinterpret_cast<int4*>(ftile + ob);
+  double* sw = reinterpret_cast<double*>(so + noff);
+  uint8_t* sd = reinterpret_cast<uint8_t*>(sw + noff);
+  const int tid = threadIdx.x;
+  const int x0 = blockIdx.x * kFtX - rc, y0 = blockIdx.y * kFtY - rc, z0 = blockIdx.z * kFtZ - rc;
+  for (int i = tid; i < nt; i += blockDim.x) {
+    const int gx = x0 + i % PX, gy = y0 + (i / PX) % PY, gz = z0 + i / (PX * PY);
+    uint8_t d = 0;
+    double v = 0.0, h = 0.0;
+    if (gx >= 0 && gx < g.nx && gy >= 0 && gy < g.ny && gz >= 0 && gz < g.nz) {
+      const int64_t j = gx + (int64_t)g.nx * (gy + (int64_t)g.ny * gz);
+      d = dom[j];
+      if (d) {
+        if (!ones) v = in[j];
+        if (ADJ) h = invhs[j];
+      }
+    }
+    sd[i] = d;
+    sv[i] = v;
+    if (ADJ) sh[i] = h;
+  }
+  for (int q = tid; q < noff; q += blockDim.x) {
+    so[q] = off[q];
+    sw[q] = w[q];
+  }
+  __syncthreads();
+  const int tx = tid % kFtX, ty = tid / kFtX;
+  for (int tz = 0; tz < kFtZ; ++tz) {
+    const int ex = blockIdx.x * kFtX + tx, ey = blockIdx.y * kFtY + ty, ez = blockIdx.z * kFtZ + tz;
+    if (ex >= g.nx || ey >= g.ny || ez >= g.nz) continue;
+    const int li = (tx + rc) + PX * ((ty + rc) + PY * (tz + rc));
+    if (!sd[li]) continue;
+    const int64_t e = ex + (int64_t)g.nx * (ey + (int64_t)g.ny * ez);
+    double s = 0.0;
+    const double ih = ADJ ? 0.0 : invhs[e];
+    for (int q = 0; q < noff; ++q) {
+      const int4 o = so[q];
+      const int lj = li + o.x + PX * (o.y + PY * o.z);
+      if (!sd[lj]) continue;
+      if (ADJ) {
+        const double wt = sw[q] * sh[lj];
+        s = s + (ones ? wt : wt * sv[lj]);
+      } else {
+        s = s + (sw[q] * ih) * sv[lj];
+      }
+    }
+    out[e] = s;
+  }
+}
+
+// largest shared-memory tile a CTA may use; beyond it (large filter radii) the per-element kernel runs
+constexpr size_t kFilterTileMax = 200 * 1024;
+
+static bool filter_tiled(mycel_filter* f, bool adj) {
+  static std::once_flag once;
+  static bool ok = false;
+  std::call_once(once, [] {
+    ok = cudaFuncSetAttribute(k_filter_tile<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFilterTileMax) ==
+             cudaSuccess &&
+         cudaFuncSetAttribute(k_filter_tile<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFilterTileMax) ==
+             cudaSuccess;
+    cudaGetLastError();
+  });
+  return ok && filter_tile_smem(f->rc, f->n_off, adj) <= kFilterTileMax;
+}
+
+static dim3 filter_tile_grid(const GridDims& g) {
+  return dim3((unsigned)((g.nx + kFtX - 1) / kFtX), (unsigned)((g.ny + kFtY - 1) / kFtY),
+              (unsigned)((g.nz + kFtZ - 1) / kFtZ));
+}
+
 int filter_setup(mycel_filter* f) {
   mycel_problem* p = f->p;
   double rmin = f->rmin;
@@ -927,6 +1024,7 @@ int filter_setup(mycel_filter* f) {
         ws.push_back(rmin - dist);
       }
   f->n_off = (int)offs.size();
+  f->rc = rc;
   cudaStream_t s = p->ctx->stream;
   if (cudaMallocAsync(&f->d_off, sizeof(int4) * offs.size(), s) != cudaSuccess) return MYCEL_E_OOM;
   if (cudaMallocAsync(&f->d_w, sizeof(double) * ws.size(), s) != cudaSuccess) return MYCEL_E_OOM;
@@ -953,15 +1051,23 @@ int filter_setup(mycel_filter* f) {
 
 void launch_filter_fwd(mycel_filter* f, const double* in_box, double* out_box) {
   mycel_problem* p = f->p;
-  k_filter_apply<0><<<(unsigned)((p->g.ne + 127) / 128), 128, 0, p->ctx->stream>>>(
-      p->g, p->d_domain, f->d_off, f->d_w, f->n_off, f->d_invhs, in_box, out_box, 0);
+  if (filter_tiled(f, false))
+    k_filter_tile<0><<<filter_tile_grid(p->g), 256, filter_tile_smem(f->rc, f->n_off, false), p->ctx->stream>>>(
+        p->g, f->rc, p->d_domain, f->d_off, f->d_w, f->n_off, f->d_invhs, in_box, out_box, 0);
+  else
+    k_filter_apply<0><<<(unsigned)((p->g.ne + 127) / 128), 128, 0, p->ctx->stream>>>(
+        p->g, p->d_domain, f->d_off, f->d_w, f->n_off, f->d_invhs, in_box, out_box, 0);
   p->ctx->launches++;
 }
 
 void launch_filter_adj(mycel_filter* f, const double* in_box, double* out_box) {
   mycel_problem* p = f->p;
-  k_filter_apply<1><<<(unsigned)((p->g.ne + 127) / 128), 128, 0, p->ctx->stream>>>(
-      p->g, p->d_domain, f->d_off, f->d_w, f->n_off, f->d_invhs, in_box, out_box, 0);
+  if (filter_tiled(f, true))
+    k_filter_tile<1><<<filter_tile_grid(p->g), 256, filter_tile_smem(f->rc, f->n_off, true), p->ctx->stream>>>(
+        p->g, f->rc, p->d_domain, f->d_off, f->d_w, f->n_off, f->d_invhs, in_box, out_box, 0);
+  else
+    k_filter_apply<1><<<(unsigned)((p->g.ne + 127) / 128), 128, 0, p->ctx->stream>>>(
+        p->g, p->d_domain, f->d_off, f->d_w, f->n_off, f->d_invhs, in_box, out_box, 0);
   p->ctx->launches++;
 }
 

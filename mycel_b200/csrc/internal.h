@@ -193,6 +193,7 @@ struct mycel_filter {
   mycel_problem* p = nullptr;
   double rmin = 1.5;
   int n_off = 0;
+  int rc = 0;                   // offset radius ceil(rmin), in elements
   int4* d_off = nullptr;        // (dx, dy, dz, unused) in the reference's loop order
   double* d_w = nullptr;        // rmin - dist per offset
   double* d_invhs = nullptr;    // [ne]

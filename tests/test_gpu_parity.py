@@ -125,9 +125,12 @@ def test_static_errors_match_reference(ctx):
         api.StaticAnalysis.run(m, None, ctx)
 
 
-@pytest.mark.parametrize("rmin", [1.5, 1.8, 2.5, 3.0])
-def test_filter_bit_exact(oracle, ctx, rmin):
-    g, dom = l_shape_domain(9, 7, 6)
+@pytest.mark.parametrize("rmin,shape", [(1.5, (9, 7, 6)), (1.8, (9, 7, 6)), (2.5, (9, 7, 6)), (3.0, (9, 7, 6)),
+                                        (2.5, (70, 19, 9)), (4.2, (37, 12, 11)), (8.5, (30, 12, 10))])
+def test_filter_bit_exact(oracle, ctx, rmin, shape):
+    """Shared-memory tiles (several tiles and partial ones; rmin 8.5 exceeds the tile limit and runs the
+    per-element kernel): the same bits as the oracle."""
+    g, dom = l_shape_domain(*shape)
     act = np.nonzero(dom)[0].astype(np.int32)
     m = FeModel(g, dom, FeMaterial(1.0, 0.3), FeModel.fix_dofs(range(3)))
     pr = api.Problem(m, ctx)
