@@ -909,55 +909,51 @@ __global__ void k_filter_apply(GridDims g, const uint8_t* __restrict__ dom, cons
   out[e] = s;
 }
 
-// The same sums as a shared-memory stencil: a CTA stages a 32 x 8 x 2 element tile with an rc-element halo
-// (the input, the element flags and, for the adjoint, 1/Hs; outside the grid or inactive: flag 0) and the
-// offset list, then each thread forms its elements' sums from shared memory in the reference's neighbour order
-// with the same operations, so the results are those of k_filter_apply bit for bit.
+// The forward filter as a shared-memory stencil: a CTA stages a 32 x 8 x 2 element tile with an rc-element halo
+// (the input and the element flags; outside the grid or inactive: flag 0) and the offset list as index steps,
+// then each thread forms its elements' sums from shared memory in the reference's neighbour order with the same
+// operations, so the results are those of k_filter_apply<0> bit for bit (206 -> 147 us on the 192x96x96
+// bridge). The adjoint stays per element: staged with 1/Hs its tile needs 74 KB, and at the occupancy that
+// leaves it ran slower (237 against 201 us).
 constexpr int kFtX = 32, kFtY = 8, kFtZ = 2;
 
-__host__ __device__ inline size_t filter_tile_smem(int rc, int noff, bool adj) {
+__host__ __device__ inline size_t filter_tile_smem(int rc, int noff) {
   const size_t nt = (size_t)(kFtX + 2 * rc) * (kFtY + 2 * rc) * (kFtZ + 2 * rc);
-  size_t b = nt * 8 * (adj ? 2 : 1);
+  size_t b = nt * 8;
   b = (b + 15) & ~(size_t)15;
-  b += (size_t)noff * 16 + (size_t)noff * 8 + nt;
+  b += (size_t)noff * 8 + (size_t)noff * 4 + nt;
   return b;
 }
 
-template <int ADJ>
 __global__ void __launch_bounds__(256) k_filter_tile(GridDims g, int rc, const uint8_t* __restrict__ dom,
                                                      const int4* __restrict__ off, const double* __restrict__ w,
                                                      int noff, const double* __restrict__ invhs,
-                                                     const double* __restrict__ in, double* __restrict__ out,
-                                                     int ones) {
+                                                     const double* __restrict__ in, double* __restrict__ out) {
   extern __shared__ __align__(16) unsigned char ftile[];
   const int PX = kFtX + 2 * rc, PY = kFtY + 2 * rc, PZ = kFtZ + 2 * rc, nt = PX * PY * PZ;
   double* sv = reinterpret_cast<double*>(ftile);
-  double* sh = sv + nt;  // adjoint only
-  size_t ob = (size_t)nt * 8 * (ADJ ? 2 : 1);
+  size_t ob = (size_t)nt * 8;
   ob = (ob + 15) & ~(size_t)15;
-  int4* so = reinterpret_cast<int4*>(ftile + ob);
-  double* sw = reinterpret_cast<double*>(so + noff);
-  uint8_t* sd = reinterpret_cast<uint8_t*>(sw + noff);
+  double* sw = reinterpret_cast<double*>(ftile + ob);
+  int* so = reinterpret_cast<int*>(sw + noff);  // offsets as shared-memory index steps
+  uint8_t* sd = reinterpret_cast<uint8_t*>(so + noff);
   const int tid = threadIdx.x;
   const int x0 = blockIdx.x * kFtX - rc, y0 = blockIdx.y * kFtY - rc, z0 = blockIdx.z * kFtZ - rc;
   for (int i = tid; i < nt; i += blockDim.x) {
     const int gx = x0 + i % PX, gy = y0 + (i / PX) % PY, gz = z0 + i / (PX * PY);
     uint8_t d = 0;
-    double v = 0.0, h = 0.0;
+    double v = 0.0;
     if (gx >= 0 && gx < g.nx && gy >= 0 && gy < g.ny && gz >= 0 && gz < g.nz) {
       const int64_t j = gx + (int64_t)g.nx * (gy + (int64_t)g.ny * gz);
       d = dom[j];
-      if (d) {
-        if (!ones) v = in[j];
-        if (ADJ) h = invhs[j];
-      }
+      if (d) v = in[j];
     }
     sd[i] = d;
     sv[i] = v;
-    if (ADJ) sh[i] = h;
   }
   for (int q = tid; q < noff; q += blockDim.x) {
-    so[q] = off[q];
+    const int4 o = off[q];
+    so[q] = o.x + PX * (o.y + PY * o.z);
     sw[q] = w[q];
   }
   __syncthreads();
@@ -969,17 +965,12 @@ __global__ void __launch_bounds__(256) k_filter_tile(GridDims g, int rc, const u
     if (!sd[li]) continue;
     const int64_t e = ex + (int64_t)g.nx * (ey + (int64_t)g.ny * ez);
     double s = 0.0;
-    const double ih = ADJ ? 0.0 : invhs[e];
+    const double ih = invhs[e];
+#pragma unroll 4
     for (int q = 0; q < noff; ++q) {
-      const int4 o = so[q];
-      const int lj = li + o.x + PX * (o.y + PY * o.z);
+      const int lj = li + so[q];
       if (!sd[lj]) continue;
-      if (ADJ) {
-        const double wt = sw[q] * sh[lj];
-        s = s + (ones ? wt : wt * sv[lj]);
-      } else {
-        s = s + (sw[q] * ih) * sv[lj];
-      }
+      s = s + (sw[q] * ih) * sv[lj];
     }
     out[e] = s;
   }
@@ -988,17 +979,15 @@ __global__ void __launch_bounds__(256) k_filter_tile(GridDims g, int rc, const u
 // largest shared-memory tile a CTA may use; beyond it (large filter radii) the per-element kernel runs
 constexpr size_t kFilterTileMax = 200 * 1024;
 
-static bool filter_tiled(mycel_filter* f, bool adj) {
+static bool filter_tiled(mycel_filter* f) {
   static std::once_flag once;
   static bool ok = false;
   std::call_once(once, [] {
-    ok = cudaFuncSetAttribute(k_filter_tile<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFilterTileMax) ==
-             cudaSuccess &&
-         cudaFuncSetAttribute(k_filter_tile<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFilterTileMax) ==
-             cudaSuccess;
+    ok = cudaFuncSetAttribute(k_filter_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFilterTileMax) ==
+         cudaSuccess;
     cudaGetLastError();
   });
-  return ok && filter_tile_smem(f->rc, f->n_off, adj) <= kFilterTileMax;
+  return ok && filter_tile_smem(f->rc, f->n_off) <= kFilterTileMax;
 }
 
 static dim3 filter_tile_grid(const GridDims& g) {
@@ -1051,9 +1040,9 @@ int filter_setup(mycel_filter* f) {
 
 void launch_filter_fwd(mycel_filter* f, const double* in_box, double* out_box) {
   mycel_problem* p = f->p;
-  if (filter_tiled(f, false))
-    k_filter_tile<0><<<filter_tile_grid(p->g), 256, filter_tile_smem(f->rc, f->n_off, false), p->ctx->stream>>>(
-        p->g, f->rc, p->d_domain, f->d_off, f->d_w, f->n_off, f->d_invhs, in_box, out_box, 0);
+  if (filter_tiled(f))
+    k_filter_tile<<<filter_tile_grid(p->g), 256, filter_tile_smem(f->rc, f->n_off), p->ctx->stream>>>(
+        p->g, f->rc, p->d_domain, f->d_off, f->d_w, f->n_off, f->d_invhs, in_box, out_box);
   else
     k_filter_apply<0><<<(unsigned)((p->g.ne + 127) / 128), 128, 0, p->ctx->stream>>>(
         p->g, p->d_domain, f->d_off, f->d_w, f->n_off, f->d_invhs, in_box, out_box, 0);
@@ -1062,12 +1051,8 @@ void launch_filter_fwd(mycel_filter* f, const double* in_box, double* out_box) {
 
 void launch_filter_adj(mycel_filter* f, const double* in_box, double* out_box) {
   mycel_problem* p = f->p;
-  if (filter_tiled(f, true))
-    k_filter_tile<1><<<filter_tile_grid(p->g), 256, filter_tile_smem(f->rc, f->n_off, true), p->ctx->stream>>>(
-        p->g, f->rc, p->d_domain, f->d_off, f->d_w, f->n_off, f->d_invhs, in_box, out_box, 0);
-  else
-    k_filter_apply<1><<<(unsigned)((p->g.ne + 127) / 128), 128, 0, p->ctx->stream>>>(
-        p->g, p->d_domain, f->d_off, f->d_w, f->n_off, f->d_invhs, in_box, out_box, 0);
+  k_filter_apply<1><<<(unsigned)((p->g.ne + 127) / 128), 128, 0, p->ctx->stream>>>(
+      p->g, p->d_domain, f->d_off, f->d_w, f->n_off, f->d_invhs, in_box, out_box, 0);
   p->ctx->launches++;
 }
 
