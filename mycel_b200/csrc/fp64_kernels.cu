@@ -1188,9 +1188,14 @@ __device__ double grid_total(double mine, const OcArgs& a, int slot, double* sh,
     *ok = false;
     return 0.0;
   }
+  // warp 0 adds the block partials: lane l takes blocks l, l + 32, ... in order, then a fixed shuffle tree
+  // (the same order in every block, so every block gets the same bits; one load round instead of gridDim.x
+  // dependent loads)
   double t = 0.0;
-  if (threadIdx.x == 0)
-    for (unsigned k = 0; k < gridDim.x; ++k) t = t + ld_volatile(part + k);
+  if (threadIdx.x < 32) {
+    for (unsigned k = threadIdx.x; k < gridDim.x; k += 32) t = t + ld_volatile(part + k);
+    for (int o = 16; o > 0; o >>= 1) t = t + __shfl_xor_sync(0xffffffffu, t, o);
+  }
   return t;
 }
 
