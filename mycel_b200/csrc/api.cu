@@ -359,6 +359,15 @@ extern "C" int32_t mycel_ctx_create(int32_t device, mycel_ctx** out) {
     return set_error(nullptr, MYCEL_E_DEVICE, m);
   }
   c->pinned_bytes = 1 << 16;
+  // Device memory freed by a problem stays in the device's stream-ordered pool for the next problem instead of
+  // going back to the driver at the next synchronisation (re-mapping gigabytes for every job cost up to a few
+  // hundred ms per job). A host that needs it released calls cudaMemPoolTrimTo on the default pool.
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  cudaGetLastError();
   *out = c;
   return MYCEL_OK;
 }
