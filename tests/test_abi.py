@@ -59,3 +59,17 @@ def test_job_device_bytes_needs_no_device():
     assert b_mixed > b_small
     # at least the problem's own FP64 vectors (F, b, diag, invD, 2 temporaries, 5 PCG vectors, u): 12 x 8 B/DOF
     assert b_small >= 12 * 8 * small[0].total_dofs
+
+
+def test_job_device_bytes_counts_the_multigrid_hierarchy():
+    """The multigrid forms' estimate adds the hierarchy (coarse stencils, element matrices, vectors) to the
+    mixed and fast FP64 workspaces; it scales with the grid."""
+    from mycel_b200 import api, workloads as W
+    est = {p: api.Server.device_bytes(*W.served_job(32, 16, 16, 2, seed=1, precision=p))
+           for p in ("fp64", "mixed", "fp64f", "mg", "mixed-mg")}
+    assert est["mixed-mg"] == est["mg"] > est["mixed"] > est["fp64"]
+    assert est["mg"] > est["fp64f"]
+    # level 1 of a 32x16x16 grid alone: 576 FP32 element-matrix entries per coarse element (16x8x8)
+    assert est["mg"] - est["mixed"] >= 4 * 576 * 16 * 8 * 8
+    big = api.Server.device_bytes(*W.served_job(64, 32, 32, 2, seed=1, precision="mg"))
+    assert big > 6 * est["mg"]
