@@ -73,3 +73,22 @@ def test_mg_simp_cantilever(oracle, ctx, prec):
     assert res.total_iterations == ref.n_iters
     for a, b in zip(res.snapshots, ref.records):
         assert abs(a.compliance - b["compliance"]) <= 1e-6 * abs(b["compliance"])
+
+
+@pytest.mark.parametrize("prec", ["mg", "mixed-mg"])
+def test_mg_pitch_poisson_thin_plate_and_bridge(oracle, ctx, prec):
+    """Voxel pitch h = 2.5 with nu = 0.28 (KE scaled and changed), a thin 48x40x2 plate (an axis that stops
+    coarsening at one element), and a small bridge with corner supports: converged in the multigrid form itself,
+    u within 1e-7 of the oracle's."""
+    cases = [W.cantilever(24, 10, 6, h=2.5, nu=0.28, e0=1.0, emin_ratio=1e-9, force=-1.0),
+             W.cantilever(48, 40, 2, e0=1.0, emin_ratio=1e-9, force=-1.0),
+             W.bridge(48, 24, 24, support=4, load_patch=6)]
+    for m in cases:
+        om, pr = oracle.Model(m), api.Problem(m, ctx)
+        b = om.forces() * (om.constrained() == 0)
+        ref, rref = om.pcg_solve(b, tol=1e-10, max_iter=40000)
+        u, r = pr.pcg_solve(b, tol=1e-10, max_iterations=40000, precision=prec)
+        assert r.converged and r.final_residual <= 1e-10 and r.fallback_iterations == 0
+        assert r.iterations < rref.iterations
+        assert np.abs(u - ref).max() <= 1e-7 * np.abs(ref).max()
+        pr.close()
