@@ -1816,37 +1816,45 @@ __global__ void __launch_bounds__(256) k_mg_build1(MgDims c, MgDims f, const flo
 // neighbour nb). The block of an earlier neighbour m is the transpose of m's block for offset 26 - nb. Also
 // 1/diag (0 where the diagonal is 0: DOFs no free fine DOF reaches).
 constexpr int kMgHalf = 14;  // stored blocks per node
-__global__ void k_mg_stencil(MgDims d, const float* __restrict__ K, float* __restrict__ S, float* __restrict__ invd) {
+__global__ void __launch_bounds__(256) k_mg_stencil(MgDims d, const float* __restrict__ K, float* __restrict__ S,
+                                                    float* __restrict__ invd) {
+  // a thread per (node, row ci): it reads row 3a + ci of each of the node's (up to 8) elements once (24
+  // contiguous floats) and adds the entries that belong to the node's own 14 blocks; the elements are taken in
+  // ascending index, so every block entry is the same ordered sum as an element-by-element assembly
   const int64_t nn = mg_nn(d);
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (t >= kMgHalf * nn) return;
-  const int hb = (int)(t / nn);
-  const int nb = 13 + hb;
-  const int64_t n = t - hb * nn;
+  if (t >= 3 * nn) return;
+  const int ci = (int)(t / nn);
+  const int64_t n = t - ci * nn;
   const int nx1 = d.nx + 1, ny1 = d.ny + 1;
   const int i = (int)(n % nx1), j = (int)((n / nx1) % ny1), k = (int)(n / ((int64_t)nx1 * ny1));
-  const int dx = nb % 3 - 1, dy = (nb / 3) % 3 - 1, dz = nb / 9 - 1;
-  float v[9];
+  float acc[kMgHalf][3];
 #pragma unroll
-  for (int q = 0; q < 9; ++q) v[q] = 0.f;
-  const int mi = i + dx, mj = j + dy, mk = k + dz;
-  if (mi >= 0 && mj >= 0 && mk >= 0 && mi <= d.nx && mj <= d.ny && mk <= d.nz) {
-    for (int ez = max(max(k, mk) - 1, 0); ez <= min(min(k, mk), d.nz - 1); ++ez)
-      for (int ey = max(max(j, mj) - 1, 0); ey <= min(min(j, mj), d.ny - 1); ++ey)
-        for (int ex = max(max(i, mi) - 1, 0); ex <= min(min(i, mi), d.nx - 1); ++ex) {
-          const int a = mg_lidx(i - ex, j - ey, k - ez), b = mg_lidx(mi - ex, mj - ey, mk - ez);
-          const float* Ke = K + (ex + (int64_t)d.nx * (ey + (int64_t)d.ny * ez)) * 576;
+  for (int h = 0; h < kMgHalf; ++h) acc[h][0] = acc[h][1] = acc[h][2] = 0.f;
 #pragma unroll
-          for (int ci = 0; ci < 3; ++ci)
+  for (int q = 0; q < 8; ++q) {  // element (i - ox, j - oy, k - oz), ascending element index
+    const int ox = 1 - (q & 1), oy = 1 - ((q >> 1) & 1), oz = 1 - (q >> 2);
+    const int ex = i - ox, ey = j - oy, ez = k - oz;
+    const bool have = ex >= 0 && ey >= 0 && ez >= 0 && ex < d.nx && ey < d.ny && ez < d.nz;
+    const int a = mg_lidx(ox, oy, oz);
+    const float* row =
+        K + (have ? (ex + (int64_t)d.nx * (ey + (int64_t)d.ny * ez)) * 576 + (3 * a + ci) * 24 : 0);
 #pragma unroll
-            for (int cj = 0; cj < 3; ++cj) v[3 * ci + cj] += Ke[(3 * a + ci) * 24 + 3 * b + cj];
-        }
+    for (int b = 0; b < 8; ++b) {
+      const int dx = mg_bx(b) - ox, dy = mg_by(b) - oy, dz = mg_bz(b) - oz;
+      const int nb = (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1);
+      if (nb < 13) continue;  // stored (transposed) at the earlier neighbour
+#pragma unroll
+      for (int cj = 0; cj < 3; ++cj)
+        if (have) acc[nb - 13][cj] += row[3 * b + cj];
+    }
   }
 #pragma unroll
-  for (int q = 0; q < 9; ++q) S[(hb * 9 + q) * nn + n] = v[q];
-  if (hb == 0)
+  for (int h = 0; h < kMgHalf; ++h)
 #pragma unroll
-    for (int ci = 0; ci < 3; ++ci) invd[3 * n + ci] = v[4 * ci] > 0.f ? 1.0f / v[4 * ci] : 0.0f;
+    for (int cj = 0; cj < 3; ++cj) S[((int64_t)h * 9 + 3 * ci + cj) * nn + n] = acc[h][cj];
+  const float dg = ci == 0 ? acc[0][0] : (ci == 1 ? acc[0][1] : acc[0][2]);  // keeps acc in registers
+  invd[3 * n + ci] = dg > 0.f ? 1.0f / dg : 0.0f;
 }
 
 // Kernels over nodes of the levels below the voxel grid run a thread per DOF: CTAs of 3 x 64 threads, warps
@@ -2888,14 +2896,14 @@ static void mg_setup(mycel_problem* p) {
       d1, lv[0].d, mg->G, p->d_Ef, p->d_nflags, mg->em[0], mg->special);
   k_mg_build<true><<<(unsigned)ne1, 64, 0, s>>>(d1, lv[0].d, p->kef, p->d_Ef, p->d_nflags, nullptr, mg->em[0],
                                                 mg->special);
-  k_mg_stencil<<<mg_blocks(kMgHalf * lv[1].nn), 256, 0, s>>>(d1, mg->em[0], lv[1].S, lv[1].invd);
+  k_mg_stencil<<<mg_blocks(3 * lv[1].nn), 256, 0, s>>>(d1, mg->em[0], lv[1].S, lv[1].invd);
   for (int l = 2; l < mg->L; ++l) {
     const MgDims& d = lv[l].d;
     float* src = mg->em[(l - 2) & 1];
     float* dst = mg->em[(l - 1) & 1];
     k_mg_build<false><<<(unsigned)((int64_t)d.nx * d.ny * d.nz), 64, 0, s>>>(d, lv[l - 1].d, p->kef, nullptr,
                                                                            nullptr, src, dst, nullptr);
-    k_mg_stencil<<<mg_blocks(kMgHalf * lv[l].nn), 256, 0, s>>>(d, dst, lv[l].S, lv[l].invd);
+    k_mg_stencil<<<mg_blocks(3 * lv[l].nn), 256, 0, s>>>(d, dst, lv[l].S, lv[l].invd);
   }
   k_mg_coarse_setup<<<1, 1024, kMgCoarseSmem, s>>>(lv[mg->L - 1].d, lv[mg->L - 1].S, mg->ainv);
   int nl = 2 * (mg->L - 1) + 2;
