@@ -94,6 +94,9 @@ def parse():
     ap.add_argument("--surface-iters", type=int, default=20)
     ap.add_argument("--batched-count", type=int, default=48)
     ap.add_argument("--batched-iters", type=int, default=4)
+    ap.add_argument("--batched-cases", choices=("separate", "summed"), default="separate",
+                    help="load cases of a batched problem: one solve per case on the shared stiffness (objective "
+                         "the sum of the cases' compliances), or summed into one right-hand side as the reference")
     ap.add_argument("--job-tol", type=float, default=1e-8,
                     help="PCG relative residual of the served and batched jobs (every SIMP iteration)")
     return ap.parse_args()
@@ -427,8 +430,10 @@ def run_batched(args):
     from mycel_b200 import api
     from mycel_b200 import workloads as W
     probs = W.batched_instances(count=args.batched_count)
+    sep = args.batched_cases == "separate"
     out = {"metric": "batched instances: aggregate SIMP iter/s", "problems": len(probs),
-           "iterations_each": args.batched_iters, "pcg_tol": args.job_tol,
+           "iterations_each": args.batched_iters, "pcg_tol": args.job_tol, "load_cases": args.batched_cases,
+           "load_cases_total": int(sum(len(bp.load_cases) for bp in probs)),
            "elements_total": int(sum(bp.model.total_elements for bp in probs))}
     hists = {}
     head = args.precision
@@ -436,7 +441,8 @@ def run_batched(args):
         with api.Server(slots=args.serve_slots, hbm_budget_bytes=int(args.serve_budget_gb * 1e9)) as srv:
             ids = [srv.submit(bp.model, bp.options.replace(max_iterations=args.batched_iters, precision=prec,
                                                           solver_tolerance_initial=args.job_tol,
-                                                          solver_tolerance_final=args.job_tol))
+                                                          solver_tolerance_final=args.job_tol,
+                                                          separate_load_cases=sep))
                    for bp in probs]
             srv.wait()
             st = srv.stats()

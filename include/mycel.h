@@ -133,6 +133,14 @@ typedef struct {
   int64_t warm_start_len;
   int32_t enforce_minimum_filter_radius; /* 1 */
   int32_t precision;                     /* MYCEL_PRECISION_* */
+  /* 0: the load cases are summed into one right-hand side (FeModel.AssembleForces, FeModel.cs:263-321; the
+     reference's behaviour). 1: load cases kept apart (no counterpart in the reference): each case is solved on
+     the shared stiffness from its own warm start, the objective is the sum of the cases' compliances (the
+     record's compliance), the sensitivities are summed over the cases in case order, max_displacement is the
+     largest over the cases, u is the sum of the cases' displacements, solver_iterations the sum and
+     solver_residual the largest over the cases; warm_start_displacements is not used (every case starts from
+     zero). With one load case both modes give the same results. */
+  int32_t separate_load_cases;
 } mycel_simp_options;
 
 /* IterationSnapshot scalars + IterationTimings (Optimization/IterationSnapshot.cs:5-31). */
@@ -191,6 +199,18 @@ int32_t mycel_problem_set_tuning(mycel_problem* p, int32_t key, int32_t value);
 int32_t mycel_problem_get_tuning(mycel_problem* p, int32_t key, int32_t* value);
 /* FeModel.AssembleForces (Fem/FeModel.cs:263-321): box-sized nodal forces. */
 int32_t mycel_problem_forces(mycel_problem* p, double* f_out);
+/* Load cases kept apart (multi-RHS over the shared stiffness; the reference sums its cases, FeModel.cs:267-318).
+   mycel_problem_load_cases: the number of load cases given to mycel_problem_create. mycel_problem_case_forces:
+   the nodal forces of case k alone (the same arithmetic as AssembleForces on a zero vector). */
+int32_t mycel_problem_load_cases(mycel_problem* p, int32_t* n_cases);
+int32_t mycel_problem_case_forces(mycel_problem* p, int32_t k, double* f_out);
+/* StaticAnalysis.Run (Fem/StaticAnalysis.cs:35-142) for every load case apart, on one stiffness: E, DiagA and
+   the solver set-up (the multigrid hierarchy of the MG precisions) are formed once and shared by the cases;
+   case k equals mycel_static_solve on the problem holding case k alone. Each case starts from zero.
+   u_out: n_cases * total_dofs (case-major); compliance_out, max_displacement_out, res: n_cases each, may be
+   NULL. opt->throw_on_non_convergence reports the first case that does not converge. */
+int32_t mycel_static_solve_cases(mycel_problem* p, const mycel_static_options* opt, double* u_out,
+                                 double* compliance_out, double* max_displacement_out, mycel_pcg_result* res);
 
 /* ---- kernel-level entry points ---- */
 /* FemOperator.UpdateDensities (Fem/FemOperator.cs:114-138): E_e = Emin + rho^p (E0-Emin) and DiagA. */

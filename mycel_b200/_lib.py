@@ -53,7 +53,7 @@ class SimpOptions(C.Structure):
                 ("passive_mask", P), ("passive_mask_len", i64), ("protect_boundary_hinges", i32),
                 ("initial_density", P), ("initial_density_len", i64), ("start_iteration", i32),
                 ("warm_start_displacements", P), ("warm_start_len", i64), ("enforce_minimum_filter_radius", i32),
-                ("precision", i32)]
+                ("precision", i32), ("separate_load_cases", i32)]
 
 
 class IterRecord(C.Structure):
@@ -103,6 +103,8 @@ SIGNATURES = {
     "mycel_problem_destroy": (i32, [P]),
     "mycel_problem_info_get": (i32, [P, C.POINTER(ProblemInfo)]),
     "mycel_problem_forces": (i32, [P, P]),
+    "mycel_problem_load_cases": (i32, [P, C.POINTER(i32)]),
+    "mycel_problem_case_forces": (i32, [P, i32, P]),
     "mycel_problem_set_tuning": (i32, [P, i32, i32]),
     "mycel_problem_get_tuning": (i32, [P, i32, C.POINTER(i32)]),
     "mycel_update_densities": (i32, [P, P, dbl]),
@@ -111,6 +113,7 @@ SIGNATURES = {
     "mycel_pcg_solve": (i32, [P, P, P, dbl, i32, i32, C.POINTER(PcgResultC)]),
     "mycel_static_solve": (i32, [P, C.POINTER(StaticOptions), P, i64, P, P, P, C.POINTER(dbl), C.POINTER(dbl),
                                  C.POINTER(PcgResultC)]),
+    "mycel_static_solve_cases": (i32, [P, C.POINTER(StaticOptions), P, P, P, P]),
     "mycel_filter_create": (i32, [P, dbl, C.POINTER(P)]),
     "mycel_filter_destroy": (i32, [P]),
     "mycel_filter_apply": (i32, [P, P, P]),

@@ -12,7 +12,7 @@ import ctypes as C
 import threading
 import weakref
 from dataclasses import dataclass
-from typing import Callable, Optional
+from typing import Callable, List, Optional
 
 import numpy as np
 
@@ -168,6 +168,17 @@ class Problem:
         _check(L.load().mycel_problem_forces(self.handle, f.ctypes.data), self.ctx)
         return f
 
+    def load_case_count(self) -> int:
+        n = C.c_int32(0)
+        _check(L.load().mycel_problem_load_cases(self.handle, C.byref(n)), self.ctx)
+        return n.value
+
+    def case_forces(self, k: int) -> np.ndarray:
+        """Nodal forces of load case k alone (the right-hand side of case k when load cases are kept apart)."""
+        f = np.zeros(self.n_dofs)
+        _check(L.load().mycel_problem_case_forces(self.handle, int(k), f.ctypes.data), self.ctx)
+        return f
+
     # ---- FemOperator ----
     def update_densities(self, density_box, penal: float):
         d = L.f64(density_box)
@@ -295,6 +306,30 @@ class StaticAnalysis:
             prob.close()
 
     @staticmethod
+    def run_cases(model: FeModel, options: Optional[StaticAnalysisOptions] = None,
+                  ctx: Optional[Context] = None) -> List[StaticAnalysisResult]:
+        """StaticAnalysis.Run for every load case apart on one stiffness (multi-RHS; the reference sums its load
+        cases). Case k equals StaticAnalysis.Run on the model holding case k alone; E, DiagA and the solver's
+        set-up are formed once. Each case starts from zero; reactions and von Mises are not formed."""
+        options = options or StaticAnalysisOptions()
+        prob = Problem(model, ctx)
+        try:
+            m = prob.load_case_count()
+            n = model.total_dofs
+            u = np.zeros((m, n))
+            c = np.zeros(m)
+            md = np.zeros(m)
+            rs = (L.PcgResultC * max(m, 1))()
+            o = L.StaticOptions(options.tolerance, options.max_iterations, int(options.throw_on_non_convergence),
+                                _PREC[options.precision])
+            _check(L.load().mycel_static_solve_cases(prob.handle, C.byref(o), u.ctypes.data, c.ctypes.data,
+                                                     md.ctypes.data, rs), prob.ctx)
+            return [StaticAnalysisResult(u[k], float(c[k]), None, float(md[k]), _pcg_result(rs[k]), None)
+                    for k in range(m)]
+        finally:
+            prob.close()
+
+    @staticmethod
     def average_element_to_node(model: FeModel, element_scalar, ctx: Optional[Context] = None,
                                 problem: Optional["Problem"] = None) -> np.ndarray:
         """StaticAnalysis.AverageElementToNode: nodal means of an element scalar over the active elements."""
@@ -355,7 +390,7 @@ def _simp_options(o: OptimizerOptions, keep: list) -> L.SimpOptions:
                          o.solver_tolerance_initial, o.solver_tolerance_final, o.solver_max_iterations,
                          int(o.continuation), int(o.enable_heaviside), o.rho_min, pm, pl,
                          int(o.protect_boundary_hinges), idp, idl, o.start_iteration, wp, wl,
-                         int(o.enforce_minimum_filter_radius), _PREC[o.precision])
+                         int(o.enforce_minimum_filter_radius), _PREC[o.precision], int(o.separate_load_cases))
 
 
 def _snapshot(r: L.IterRecord, phys=None, design=None) -> IterationSnapshot:

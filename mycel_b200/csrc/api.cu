@@ -447,8 +447,11 @@ extern "C" int32_t mycel_problem_create(mycel_ctx* c, const mycel_grid* grid, co
   // FeModel.AssembleForces (FeModel.cs:263-321): descriptor marshalling of the load patches, O(patch nodes).
   p->forces_host.assign(g.nd, 0.0);
   std::unordered_set<int32_t> seen;
+  p->n_cases = std::max<int32_t>(n_loads, 0);
+  p->case_terms.assign((size_t)p->n_cases, {});
   for (int32_t li = 0; li < n_loads && !p->assemble_status; ++li) {
     const mycel_load_case& L = loads[li];
+    auto& terms = p->case_terms[(size_t)li];
     for (int32_t q = 0; q < L.n_nodes; ++q)
       if (seen.insert(L.nodes[q]).second) p->load_nodes_host.push_back(L.nodes[q]);
     if (L.n_nodes == 0) {
@@ -475,6 +478,9 @@ extern "C" int32_t mycel_problem_create(mycel_ctx* c, const mycel_grid* grid, co
         p->forces_host[3 * n] += fx;
         p->forces_host[3 * n + 1] += fy;
         p->forces_host[3 * n + 2] += fz;
+        terms.push_back({3 * n, fx});
+        terms.push_back({3 * n + 1, fy});
+        terms.push_back({3 * n + 2, fz});
       }
     } else {
       double inv = 1.0 / total;
@@ -484,6 +490,9 @@ extern "C" int32_t mycel_problem_create(mycel_ctx* c, const mycel_grid* grid, co
         p->forces_host[3 * n] += (double)L.force[0] * w;
         p->forces_host[3 * n + 1] += (double)L.force[1] * w;
         p->forces_host[3 * n + 2] += (double)L.force[2] * w;
+        terms.push_back({3 * n, (double)L.force[0] * w});
+        terms.push_back({3 * n + 1, (double)L.force[1] * w});
+        terms.push_back({3 * n + 2, (double)L.force[2] * w});
       }
     }
   }
@@ -600,6 +609,7 @@ extern "C" int32_t mycel_problem_destroy(mycel_problem* p) {
   }
   mg_release(p);
   void* ptrs[] = {p->d_domain, p->d_nflags, p->d_fixed, p->d_err, p->d_active, p->d_e2a, p->d_F, p->d_b, p->d_fnz, p->d_bnz, p->d_rho_box,
+                  p->d_case_F, p->d_case_b, p->d_case_nz,
                   p->d_E, p->d_Ef, p->d_diag, p->d_invd, p->d_invdf, p->d_r, p->d_z, p->d_p, p->d_ap, p->d_x,
                   p->d_part, p->d_state, p->f_x, p->f_r, p->f_z, p->f_p0, p->f_p1, p->f_ap, p->d_r64, p->d_part2,
                   p->d_tmp0, p->d_tmp1, p->g_x, p->g_r, p->g_z, p->g_p0, p->g_p1, p->g_ap, p->g_invd};
@@ -652,6 +662,88 @@ extern "C" int32_t mycel_problem_forces(mycel_problem* p, double* f) {
   std::memcpy(f, p->forces_host.data(), sizeof(double) * p->g.nd);
   return MYCEL_OK;
 }
+
+// ---- load cases apart (multi-RHS over one stiffness; the reference sums its cases, FeModel.cs:267-318) ----
+static void case_forces_host(const mycel_problem* p, int k, double* f) {
+  std::fill(f, f + p->g.nd, 0.0);
+  for (const auto& t : p->case_terms[(size_t)k]) f[t.first] += t.second;  // assembly order, as the summed F
+}
+
+extern "C" int32_t mycel_problem_load_cases(mycel_problem* p, int32_t* n) {
+  if (!p || !n) return set_error(p ? p->ctx : nullptr, MYCEL_E_ARG, "NULL argument");
+  *n = p->n_cases;
+  return MYCEL_OK;
+}
+
+extern "C" int32_t mycel_problem_case_forces(mycel_problem* p, int32_t k, double* f) {
+  if (!p || !f) return set_error(p ? p->ctx : nullptr, MYCEL_E_ARG, "NULL argument");
+  if (p->assemble_status) return set_error(p->ctx, p->assemble_status, p->assemble_msg);
+  if (k < 0 || k >= p->n_cases)
+    return set_error(p->ctx, MYCEL_E_ARG, "Load case index " + std::to_string(k) + " is out of range [0, " +
+                                              std::to_string(p->n_cases) + ").");
+  case_forces_host(p, k, f);
+  return MYCEL_OK;
+}
+
+namespace mycel {
+// Device right-hand sides of every load case (first use): F_k, P F_k, and the ascending non-zero lists of F_k
+// (compliance F_k . u_k, as k_compliance sums F . u) and of P F_k (the PCG's ||P b||), at case_nz_off[2k] and
+// case_nz_off[2k + 1].
+int32_t ensure_cases(mycel_problem* p) {
+  if (p->d_case_F || p->n_cases <= 0) return MYCEL_OK;
+  if (p->assemble_status) return set_error(p->ctx, p->assemble_status, p->assemble_msg);
+  mycel_ctx* c = p->ctx;
+  cudaStream_t s = c->stream;
+  const int64_t nd = p->g.nd;
+  const int m = p->n_cases;
+  std::vector<uint8_t> nf((size_t)p->g.nn);
+  MYCEL_CUDA(c, cudaMemcpyAsync(nf.data(), p->d_nflags, p->g.nn, cudaMemcpyDeviceToHost, s));
+  MYCEL_CUDA(c, cudaStreamSynchronize(s));
+  std::vector<double> f((size_t)nd), b((size_t)nd);
+  std::vector<int32_t> lists;
+  p->case_nz_off.assign(2 * (size_t)m, 0);
+  p->case_nz_cnt.assign(2 * (size_t)m, 0);
+  if (dalloc(p, &p->d_case_F, (size_t)(m * nd)) || dalloc(p, &p->d_case_b, (size_t)(m * nd))) {
+    dfree(s, p->d_case_F);
+    p->d_case_F = nullptr;
+    return set_error(c, MYCEL_E_OOM, "out of device memory for the load cases");
+  }
+  for (int k = 0; k < m; ++k) {
+    case_forces_host(p, k, f.data());
+    p->case_nz_off[2 * k] = (int32_t)lists.size();
+    for (int64_t i = 0; i < nd; ++i)
+      if (f[i] != 0.0) lists.push_back((int32_t)i);
+    p->case_nz_cnt[2 * k] = (int32_t)lists.size() - p->case_nz_off[2 * k];
+    p->case_nz_off[2 * k + 1] = (int32_t)lists.size();
+    for (int64_t i = 0; i < nd; ++i) {
+      b[i] = (nf[i / 3] & (1 << (i % 3))) ? 0.0 : f[i];
+      if (b[i] != 0.0) lists.push_back((int32_t)i);
+    }
+    p->case_nz_cnt[2 * k + 1] = (int32_t)lists.size() - p->case_nz_off[2 * k + 1];
+    MYCEL_CUDA(c, cudaMemcpyAsync(p->d_case_F + k * nd, f.data(), sizeof(double) * nd, cudaMemcpyHostToDevice, s));
+    MYCEL_CUDA(c, cudaMemcpyAsync(p->d_case_b + k * nd, b.data(), sizeof(double) * nd, cudaMemcpyHostToDevice, s));
+    MYCEL_CUDA(c, cudaStreamSynchronize(s));  // f and b are refilled for the next case
+  }
+  if (dalloc(p, &p->d_case_nz, std::max<size_t>(lists.size(), 1)))
+    return set_error(c, MYCEL_E_OOM, "out of device memory for the load cases");
+  if (!lists.empty())
+    MYCEL_CUDA(c, cudaMemcpyAsync(p->d_case_nz, lists.data(), sizeof(int32_t) * lists.size(), cudaMemcpyHostToDevice, s));
+  MYCEL_CUDA(c, cudaStreamSynchronize(s));
+  return MYCEL_OK;
+}
+
+// PCG solve of load case k (right-hand side P F_k) into d_u, in the given precision
+int32_t solve_case(mycel_problem* p, int k, double* d_u, double tol, int max_iter, int precision,
+                   const volatile int32_t* cancel, mycel_pcg_result* res) {
+  const double* b = p->d_case_b + (int64_t)k * p->g.nd;
+  const int32_t* nz = p->d_case_nz + p->case_nz_off[2 * k + 1];
+  const int32_t cnt = p->case_nz_cnt[2 * k + 1];
+  if (precision == MYCEL_PRECISION_MIXED || precision == MYCEL_PRECISION_FP64_FACTORED ||
+      precision == MYCEL_PRECISION_FP64_MG || precision == MYCEL_PRECISION_MIXED_MG)
+    return refined_solve_entry(p, b, nz, cnt, d_u, tol, max_iter, cancel, precision, res);
+  return pcg_solve_fp64(p, b, nz, cnt, d_u, tol, max_iter, cancel, res);
+}
+}  // namespace mycel
 
 // ======================================================================================================
 // kernel-level entry points
@@ -792,6 +884,46 @@ extern "C" int32_t mycel_static_solve(mycel_problem* p, const mycel_static_optio
   MYCEL_CUDA(c, cudaStreamSynchronize(s));
   if (compliance_out) *compliance_out = hsc[0];
   if (maxdisp_out) *maxdisp_out = hsc[1];
+  return MYCEL_OK;
+}
+
+extern "C" int32_t mycel_static_solve_cases(mycel_problem* p, const mycel_static_options* opt, double* u_out,
+                                            double* compliance_out, double* maxdisp_out, mycel_pcg_result* res) {
+  if (!p || !u_out) return set_error(p ? p->ctx : nullptr, MYCEL_E_ARG, "NULL argument");
+  mycel_ctx* c = p->ctx;
+  cudaSetDevice(c->device);
+  cudaStream_t s = c->stream;
+  mycel_static_options o = opt ? *opt : mycel_static_options{1e-6, 5000, 1, MYCEL_PRECISION_FP64};
+  if (p->n_active_fixed < 6) return set_error(c, MYCEL_E_UNDERCONSTRAINED, underconstrained_msg(p->n_active_fixed));
+  if (p->assemble_status) return set_error(c, p->assemble_status, p->assemble_msg);
+  int32_t st = ensure_pcg_workspace(p);
+  if (st || (st = ensure_cases(p))) return st;
+  // one stiffness for all cases: E and DiagA here, the solver's own set-up (multigrid hierarchy) on the first
+  // case's solve, reused by the others while E is unchanged
+  launch_update_E(p, p->d_rho_box, p->penal);
+  launch_diag(p);
+  const int64_t nd = p->g.nd;
+  double* d_sc = p->d_part2;  // [0] compliance, [1] max disp
+  double* hsc = (double*)c->pinned;
+  for (int k = 0; k < p->n_cases; ++k) {
+    mycel_pcg_result local;
+    mycel_pcg_result* r = res ? res + k : &local;
+    MYCEL_CUDA(c, cudaMemsetAsync(p->d_x, 0, sizeof(double) * nd, s));
+    if ((st = solve_case(p, k, p->d_x, o.tolerance, o.max_iterations, o.precision, nullptr, r))) return st;
+    if (o.throw_on_non_convergence && !r->converged)
+      return set_error(c, MYCEL_E_NOT_CONVERGED,
+                       "FEM solver did not converge in " + std::to_string(r->iterations) + " iterations (" +
+                           r->message + ") for load case " + std::to_string(k) +
+                           ". Is the model not sufficiently constrained?");
+    launch_compliance(p, p->d_case_F + k * nd, p->d_case_nz + p->case_nz_off[2 * k], p->case_nz_cnt[2 * k], p->d_x,
+                      d_sc);
+    launch_max_disp(p, p->d_x, d_sc + 1);
+    MYCEL_CUDA(c, cudaMemcpyAsync(hsc, d_sc, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    MYCEL_CUDA(c, cudaMemcpyAsync(u_out + k * nd, p->d_x, sizeof(double) * nd, cudaMemcpyDeviceToHost, s));
+    MYCEL_CUDA(c, cudaStreamSynchronize(s));
+    if (compliance_out) compliance_out[k] = hsc[0];
+    if (maxdisp_out) maxdisp_out[k] = hsc[1];
+  }
   return MYCEL_OK;
 }
 

@@ -1642,7 +1642,8 @@ __global__ void k_from_pad(GridDims g, const T* __restrict__ a, double* __restri
 // sub-elements s of W_s^T T_s W_s, where T_s is the finer level's element matrix (E_e KE on the voxel grid,
 // with the rows and columns of constrained DOFs zeroed) and W_s the trilinear interpolation from the coarse
 // element's 8 nodes to the sub-element's 8 nodes. Each coarse level is then stored assembled, as a 27-point
-// node stencil of 3 x 3 blocks. Everything is rebuilt at the start of each solve from the current E.
+// node stencil of 3 x 3 blocks. Everything is rebuilt from the current E at the start of a solve, unless E is
+// unchanged since the last build (the load cases of one stiffness share it).
 // Smoothing: damped Jacobi, the same sweeps before and after the coarse correction, so the V-cycle is a
 // symmetric operator; the coarsest level is solved by a dense inverse (FP64 Gauss-Jordan in shared memory).
 // Outer iteration (FCG with one-term orthogonalisation): alpha = (z, r) / (p, A p) as in PCG, and
@@ -2688,6 +2689,7 @@ struct MgLevel {
 
 struct MgHier {
   int L = 0;  // levels 0 .. L-1; level L-1 is solved by its dense inverse
+  uint64_t setup_version = ~0ull;  // the problem's E version the coarse operators were built from
   MgLevel lv[kMgMaxLevels];
   float* em[2] = {nullptr, nullptr};  // element matrices of alternate coarse levels (rebuilt at each solve)
   float* G = nullptr;                 // [8][576] W_s^T KE W_s of the 8 sub-element positions (level-1 fast path)
@@ -3331,7 +3333,10 @@ int32_t refined_solve_entry(mycel_problem* p, const double* d_b, const int32_t* 
     if ((st = resolve_mv32(p)) || (st = mg_ensure(p, &avail))) return st;
     if (avail) {
       ran_mg = true;
-      mg_setup(p);
+      if (p->mg->setup_version != p->e_version) {  // solves on an unchanged E (load cases) share the set-up
+        mg_setup(p);
+        p->mg->setup_version = p->e_version;
+      }
       // MYCEL_PRECISION_MIXED_MG: the FP32 outer iteration first (unless one of this problem's solves stalled
       // in it), then the FP64 outer iteration from the refined u
       if (precision == MYCEL_PRECISION_MIXED_MG && !p->mg->prefers_f64) {

@@ -181,6 +181,7 @@ __global__ void k_update_E(int64_t na, const int32_t* __restrict__ active, const
 }
 
 void launch_update_E(mycel_problem* p, const double* d_rho_box, double penal) {
+  p->e_version++;
   if (p->n_active == 0) return;
   k_update_E<<<(unsigned)((p->n_active + 255) / 256), 256, 0, p->ctx->stream>>>(
       p->n_active, p->d_active, d_rho_box, p->emin, p->e0, penal, p->d_E, p->d_Ef);
@@ -682,7 +683,12 @@ __global__ void k_compliance(const double* __restrict__ F, const double* __restr
 }
 
 void launch_compliance(mycel_problem* p, const double* u, double* d_out) {
-  k_compliance<<<1, 32, 0, p->ctx->stream>>>(p->d_F, u, p->d_fnz, p->n_fnz, d_out);
+  launch_compliance(p, p->d_F, p->d_fnz, p->n_fnz, u, d_out);
+}
+
+void launch_compliance(mycel_problem* p, const double* F, const int32_t* fnz, int32_t n_fnz, const double* u,
+                       double* d_out) {
+  k_compliance<<<1, 32, 0, p->ctx->stream>>>(F, u, fnz, n_fnz, d_out);
   p->ctx->launches++;
 }
 
@@ -712,12 +718,17 @@ __global__ void k_sqrt_inplace(unsigned long long* v) {
   *(double*)v = sqrt(d);
 }
 
-void launch_max_disp(mycel_problem* p, const double* u, double* d_out) {
+void launch_max_disp(mycel_problem* p, const double* u, double* d_out) { launch_max_disp(p, &u, 1, 0, d_out); }
+
+// largest |u| over the active nodes of m displacement vectors, u[k] at us[k] + k * stride
+void launch_max_disp(mycel_problem* p, const double* const* us, int m, int64_t stride, double* d_out) {
   cudaMemsetAsync(d_out, 0, sizeof(double), p->ctx->stream);
   int blocks = std::max(1, std::min<int>((int)((p->g.nn + 255) / 256), p->ctx->num_sms * 8));
-  k_max_disp<<<blocks, 256, 0, p->ctx->stream>>>(p->g, p->d_nflags, u, (unsigned long long*)d_out);
+  for (int k = 0; k < m; ++k)
+    k_max_disp<<<blocks, 256, 0, p->ctx->stream>>>(p->g, p->d_nflags, stride ? us[0] + k * stride : us[k],
+                                                   (unsigned long long*)d_out);
   k_sqrt_inplace<<<1, 1, 0, p->ctx->stream>>>((unsigned long long*)d_out);
-  p->ctx->launches += 2;
+  p->ctx->launches += 1 + m;
 }
 
 __global__ void k_reactions(const double* __restrict__ ku, double* out, const int32_t* __restrict__ fixed, int32_t nf) {
@@ -1061,7 +1072,7 @@ void launch_filter_adj(mycel_filter* f, const double* in_box, double* out_box) {
 // ---------------------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(128) k_sens(GridDims g, const __grid_constant__ KeD ke, const double* __restrict__ u,
                                               const double* __restrict__ rho, const uint8_t* __restrict__ dom,
-                                              double penal, double dE, double* __restrict__ dc) {
+                                              double penal, double dE, double* __restrict__ dc, int accumulate) {
   int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (e >= g.ne || !dom[e]) return;
   int ix = (int)(e % g.nx);
@@ -1084,12 +1095,14 @@ __global__ void __launch_bounds__(128) k_sens(GridDims g, const __grid_constant_
     se = se + ue[rr] * s;
   }
   double dEdr = penal * path_pow(rho[e], penal - 1.0) * dE;
-  dc[e] = -dEdr * se;
+  const double v = -dEdr * se;
+  dc[e] = accumulate ? dc[e] + v : v;  // load cases apart: summed over the cases in case order
 }
 
-void launch_sens(mycel_problem* p, const double* u, const double* rho_box, double penal, double* dc_box) {
+void launch_sens(mycel_problem* p, const double* u, const double* rho_box, double penal, double* dc_box,
+                 bool accumulate) {
   k_sens<<<(unsigned)((p->g.ne + 127) / 128), 128, 0, p->ctx->stream>>>(p->g, p->ke, u, rho_box, p->d_domain, penal,
-                                                                        p->e0 - p->emin, dc_box);
+                                                                        p->e0 - p->emin, dc_box, accumulate ? 1 : 0);
   p->ctx->launches++;
 }
 

@@ -136,6 +136,15 @@ struct mycel_problem {
   std::vector<int32_t> fixed_host;        // FixedDofs as given (may repeat)
   std::vector<int32_t> load_nodes_host;   // union of load patch nodes (hinge shell)
   std::vector<double> forces_host;        // AssembleForces result (box DOF vector)
+  // load cases kept apart (multi-RHS solves over the shared stiffness): each case's nodal forces alone, as
+  // (DOF, value) contributions in assembly order; device right-hand sides built on first use
+  std::vector<std::vector<std::pair<int64_t, double>>> case_terms;
+  int32_t n_cases = 0;
+  double* d_case_F = nullptr;             // [n_cases * nd] F_k
+  double* d_case_b = nullptr;             // [n_cases * nd] P F_k
+  int32_t* d_case_nz = nullptr;           // non-zero lists of F_k (ascending), concatenated
+  std::vector<int32_t> case_nz_off, case_nz_cnt;
+  uint64_t e_version = 0;                 // bumped whenever E changes (shared set-ups compare it)
   int assemble_status = 0;
   std::string assemble_msg;
   // device arrays
@@ -230,7 +239,10 @@ void launch_pcg_dot_rr(mycel_problem* p);
 void launch_pcg_init_z(mycel_problem* p);
 void launch_pcg_iteration(mycel_problem* p, bool skip_matvec = false);
 void launch_compliance(mycel_problem* p, const double* u, double* d_out);
+void launch_compliance(mycel_problem* p, const double* F, const int32_t* fnz, int32_t n_fnz, const double* u,
+                       double* d_out);
 void launch_max_disp(mycel_problem* p, const double* u, double* d_out);
+void launch_max_disp(mycel_problem* p, const double* const* us, int m, int64_t stride, double* d_out);
 void launch_reactions(mycel_problem* p, const double* ku, double* out, const int32_t* d_fixed, int32_t n_fixed);
 void launch_von_mises(mycel_problem* p, const double* u, double* vm);
 void launch_average_e2n(mycel_problem* p, const double* es, double* out);
@@ -243,7 +255,8 @@ void launch_gather_active(mycel_problem* p, const double* src_box, double* dst_a
 int filter_setup(mycel_filter* f);
 void launch_filter_fwd(mycel_filter* f, const double* in_box, double* out_box);
 void launch_filter_adj(mycel_filter* f, const double* in_box, double* out_box);
-void launch_sens(mycel_problem* p, const double* u, const double* rho_box, double penal, double* dc_box);
+void launch_sens(mycel_problem* p, const double* u, const double* rho_box, double penal, double* dc_box,
+                 bool accumulate = false);
 
 // OC (persistent cooperative kernel); returns 0 or MYCEL_E_TIMEOUT / MYCEL_E_DEVICE
 struct OcParams {
@@ -281,6 +294,10 @@ int64_t mg_device_bytes(int nx, int ny, int nz);  // hierarchy of a grid; 0 when
 // ---- drivers (api.cu) ----
 int32_t pcg_solve_fp64(mycel_problem* p, const double* d_b, const int32_t* d_nz, int32_t n_nz, double* d_x,
                        double tol, int max_iter, const volatile int32_t* cancel, mycel_pcg_result* res);
+// load cases apart: device right-hand sides of every case (built on first use) and a solve of one of them
+int32_t ensure_cases(mycel_problem* p);
+int32_t solve_case(mycel_problem* p, int k, double* d_u, double tol, int max_iter, int precision,
+                   const volatile int32_t* cancel, mycel_pcg_result* res);
 int32_t solve_dispatch(mycel_problem* p, double* d_u, double tol, int max_iter, int precision,
                        const volatile int32_t* cancel, mycel_pcg_result* res);
 int32_t ensure_pcg_workspace(mycel_problem* p);

@@ -96,7 +96,7 @@ struct mycel_server {
 // Device memory of one job, allocation by allocation as problem_create, ensure_pcg_workspace, ensure_mixed,
 // filter_create and simp_begin make them (each rounded to 16 bytes as they count it).
 static int64_t job_bytes(const mycel_grid& gr, int64_t n_active, int64_t n_fixed, int64_t n_load_nodes,
-                         const mycel_simp_options& o, int num_sms) {
+                         int32_t n_loads, const mycel_simp_options& o, int num_sms) {
   const mycel::GridDims g = mycel::make_dims(gr.nx, gr.ny, gr.nz);
   const int64_t ne = g.ne, nn = g.nn, nd = g.nd, na = std::max<int64_t>(n_active, 1);
   const int64_t nfnz = std::max<int64_t>(std::min<int64_t>(3 * n_load_nodes, nd), 1);
@@ -124,6 +124,9 @@ static int64_t job_bytes(const mycel_grid& gr, int64_t n_active, int64_t n_fixed
   b += 5 * al16(8 * ne) + al16(8 * nd) + al16(8 * 16) + al16(8 * ((int64_t)num_sms * 16 + 64)) +
        al16(sizeof(mycel::OcOut)) + al16(ne) + 2 * al16(4 * ne);
   if (o.enable_heaviside) b += 2 * al16(8 * ne);
+  // load cases apart: F_k and P F_k, their non-zero lists, each case's u, the per-case compliances
+  if (o.separate_load_cases && n_loads > 1)
+    b += 3 * al16(8 * (int64_t)n_loads * nd) + al16(4 * std::max<int64_t>(6 * n_load_nodes, 1)) + al16(8 * n_loads);
   return b;
 }
 
@@ -134,7 +137,7 @@ static int64_t spec_bytes(const mycel_job_spec* j, int num_sms) {
     for (int64_t e = 0; e < g.ne; ++e) na += j->domain[e] != 0;
   int64_t nl = 0;
   for (int32_t q = 0; q < j->n_loads; ++q) nl += j->loads[q].n_nodes;
-  return job_bytes(j->grid, na, j->n_fixed, nl, j->options, num_sms);
+  return job_bytes(j->grid, na, j->n_fixed, nl, j->n_loads, j->options, num_sms);
 }
 
 extern "C" int64_t mycel_job_device_bytes(const mycel_job_spec* job) {

@@ -29,6 +29,8 @@ struct mycel_simp_session {
   OcOut* d_oc = nullptr;
   uint8_t* d_pas = nullptr;
   float *d_phys_f = nullptr, *d_des_f = nullptr;
+  int ncase = 1;               // load cases solved apart (separate_load_cases with more than one case), else 1
+  double* d_uc = nullptr;      // [ncase * nd] each case's displacements (its warm start)
   int iter = 1, start = 1, maxit = 200;
   double lambda = 1.0, max_change = 1.0, beta = 1.0;
   std::deque<double> chist;
@@ -82,6 +84,19 @@ __global__ void k_quantize(int64_t ne, const float* __restrict__ v, uint8_t* __r
   if (e >= ne) return;
   const float c = fminf(fmaxf(v[e], 0.0f), 1.0f);
   q[e] = (uint8_t)roundf(__fmul_rn(c, 255.0f));
+}
+
+// u += v (the superposition of the load cases' displacements, added in case order)
+__global__ void k_add_into(int64_t n, double* __restrict__ u, const double* __restrict__ v) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) u[i] = u[i] + v[i];
+}
+
+// out = 0 + c[0] + c[1] + ... in case order (the objective: the sum of the cases' compliances)
+__global__ void k_sum_in_order(const double* __restrict__ c, int m, double* out) {
+  double t = 0.0;
+  for (int k = 0; k < m; ++k) t = t + c[k];
+  *out = t;
 }
 
 __global__ void k_snapshot(int64_t ne, const uint8_t* __restrict__ dom, const double* __restrict__ rb,
@@ -192,12 +207,19 @@ extern "C" int32_t mycel_simp_begin(mycel_problem* p, const mycel_simp_options* 
     delete s;
     return rc;
   }
+  s->ncase = o.separate_load_cases && p->n_cases > 1 ? p->n_cases : 1;
+  if (s->ncase > 1 && (rc = ensure_cases(p))) {
+    delete s;
+    return rc;
+  }
   bool ok = !salloc(s, &s->d_rho, g.ne) && !salloc(s, &s->d_rho_new, g.ne) && !salloc(s, &s->d_rt, g.ne) &&
             !salloc(s, &s->d_dcb, g.ne) && !salloc(s, &s->d_dc, g.ne) && !salloc(s, &s->d_u, g.nd) &&
-            !salloc(s, &s->d_scal, 16) && !salloc(s, &s->d_oc_scr, (size_t)c->num_sms * 2 * 8 + 64) &&
+            !salloc(s, &s->d_scal, 16 + (s->ncase > 1 ? s->ncase : 0)) &&
+            !salloc(s, &s->d_oc_scr, (size_t)c->num_sms * 2 * 8 + 64) &&
             !salloc(s, &s->d_oc, 1) && !salloc(s, &s->d_pas, g.ne) && !salloc(s, &s->d_phys_f, g.ne) &&
             !salloc(s, &s->d_des_f, g.ne);
   if (ok && o.enable_heaviside) ok = !salloc(s, &s->d_rb, g.ne) && !salloc(s, &s->d_dct, g.ne);
+  if (ok && s->ncase > 1) ok = !salloc(s, &s->d_uc, (size_t)(s->ncase * g.nd));
   if (!ok) {
     mycel_simp_end(s);
     return set_error(c, MYCEL_E_OOM, "out of device memory for the SIMP state");
@@ -209,10 +231,11 @@ extern "C" int32_t mycel_simp_begin(mycel_problem* p, const mycel_simp_options* 
   cudaMemsetAsync(s->d_rt, 0, sizeof(double) * g.ne, st);
   cudaMemsetAsync(s->d_dcb, 0, sizeof(double) * g.ne, st);
   cudaMemsetAsync(s->d_dc, 0, sizeof(double) * g.ne, st);
-  if (o.warm_start_displacements && o.warm_start_len == g.nd)
+  if (o.warm_start_displacements && o.warm_start_len == g.nd && s->ncase == 1)
     cudaMemcpyAsync(s->d_u, o.warm_start_displacements, sizeof(double) * g.nd, cudaMemcpyHostToDevice, st);
   else
     cudaMemsetAsync(s->d_u, 0, sizeof(double) * g.nd, st);
+  if (s->d_uc) cudaMemsetAsync(s->d_uc, 0, sizeof(double) * s->ncase * g.nd, st);
   for (auto& e : s->ev) cudaEventCreate(&e);
   cudaError_t pe = cudaGetLastError();
   if (pe != cudaSuccess) {
@@ -278,20 +301,58 @@ static int32_t simp_step_impl(mycel_simp_session* s, mycel_iter_record* rec, int
     double lt = lf + ta * (li - lf);
     tol = std::pow(10.0, lt);
   }
-  // 4. warm-started PCG (:226-253)
+  // 4. warm-started PCG (:226-253); with the load cases apart one solve per case from its own warm start, all
+  // on this iteration's stiffness (the solver set-up is shared)
   mycel_pcg_result pr;
-  int32_t rc = solve_dispatch(p, s->d_u, tol, o.solver_max_iterations, o.precision, cancel, &pr);
-  if (rc) return rc;
+  int32_t rc;
+  const int64_t nd = p->g.nd;
+  if (s->ncase == 1) {
+    rc = solve_dispatch(p, s->d_u, tol, o.solver_max_iterations, o.precision, cancel, &pr);
+    if (rc) return rc;
+  } else {
+    std::memset(&pr, 0, sizeof pr);
+    pr.converged = 1;
+    for (int k = 0; k < s->ncase && pr.converged; ++k) {
+      mycel_pcg_result rk;
+      if ((rc = solve_case(p, k, s->d_uc + k * nd, tol, o.solver_max_iterations, o.precision, cancel, &rk)))
+        return rc;
+      pr.iterations += rk.iterations;
+      pr.inner_iterations += rk.inner_iterations;
+      pr.fallback_iterations += rk.fallback_iterations;
+      pr.refinement_steps += rk.refinement_steps;
+      pr.elapsed_ms += rk.elapsed_ms;
+      pr.final_residual = std::max(pr.final_residual, rk.final_residual);
+      pr.converged = rk.converged;
+      std::memcpy(pr.message, rk.message, sizeof pr.message);
+    }
+  }
   cudaEventRecord(s->ev[2], st);
   if (!pr.converged)
     return set_error(c, MYCEL_E_NOT_CONVERGED,
                      "FEM solver did not converge in " + std::to_string(pr.iterations) + " iterations (" + pr.message +
                          "). Is the model not sufficiently constrained?");
-  // compliance and max |u| (:255-276)
-  launch_compliance(p, s->d_u, s->d_scal);
-  launch_max_disp(p, s->d_u, s->d_scal + 1);
-  // 5. sensitivities and adjoint filter (:278-294)
-  launch_sens(p, s->d_u, s->d_rb, penal, s->d_dcb);
+  if (s->ncase == 1) {
+    // compliance and max |u| (:255-276)
+    launch_compliance(p, s->d_u, s->d_scal);
+    launch_max_disp(p, s->d_u, s->d_scal + 1);
+    // 5. sensitivities and adjoint filter (:278-294)
+    launch_sens(p, s->d_u, s->d_rb, penal, s->d_dcb);
+  } else {
+    // objective sum_k F_k . u_k, the largest |u| over the cases, sensitivities summed in case order, and the
+    // reported u = sum_k u_k
+    for (int k = 0; k < s->ncase; ++k) {
+      launch_compliance(p, p->d_case_F + k * nd, p->d_case_nz + p->case_nz_off[2 * k], p->case_nz_cnt[2 * k],
+                        s->d_uc + k * nd, s->d_scal + 16 + k);
+      launch_sens(p, s->d_uc + k * nd, s->d_rb, penal, s->d_dcb, k > 0);
+    }
+    k_sum_in_order<<<1, 1, 0, st>>>(s->d_scal + 16, s->ncase, s->d_scal);
+    const double* uc = s->d_uc;
+    launch_max_disp(p, &uc, s->ncase, nd, s->d_scal + 1);
+    MYCEL_CUDA(c, cudaMemcpyAsync(s->d_u, s->d_uc, sizeof(double) * nd, cudaMemcpyDeviceToDevice, st));
+    for (int k = 1; k < s->ncase; ++k)
+      k_add_into<<<(unsigned)((nd + 255) / 256), 256, 0, st>>>(nd, s->d_u, s->d_uc + k * nd);
+    c->launches += s->ncase;
+  }
   if (o.enable_heaviside) {
     k_heaviside_chain<<<(unsigned)((p->n_active + 255) / 256), 256, 0, st>>>(p->n_active, p->d_active, s->d_rt,
                                                                             s->d_dcb, s->d_dct, s->beta, 0.5);
@@ -478,7 +539,7 @@ extern "C" int32_t mycel_simp_end(mycel_simp_session* s) {
   cudaStreamSynchronize(s->p->ctx->stream);
   if (s->filt) mycel_filter_destroy(s->filt);
   cudaStream_t st = s->p->ctx->stream;
-  double* dptr[] = {s->d_rho, s->d_rho_new, s->d_rt, s->d_dcb, s->d_dc, s->d_u, s->d_scal, s->d_oc_scr};
+  double* dptr[] = {s->d_rho, s->d_rho_new, s->d_rt, s->d_dcb, s->d_dc, s->d_u, s->d_scal, s->d_oc_scr, s->d_uc};
   for (double* q : dptr)
     if (q) cudaFreeAsync(q, st);
   if (s->o.enable_heaviside) {

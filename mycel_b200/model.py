@@ -267,6 +267,11 @@ class OptimizerOptions:
     warm_start_displacements: Optional[np.ndarray] = None
     enforce_minimum_filter_radius: bool = True
     precision: str = "fp64"  # solver form, as for StaticAnalysisOptions.precision
+    # Load cases: False sums them into one right-hand side (FeModel.AssembleForces, the reference's behaviour);
+    # True solves each case on the shared stiffness (its own warm start), minimises the sum of the cases'
+    # compliances, sums the sensitivities over the cases in case order and reports u as the sum of the cases'
+    # displacements. An extension: the reference has no multi-load objective.
+    separate_load_cases: bool = False
 
     def replace(self, **kw) -> "OptimizerOptions":
         return dataclasses.replace(self, **kw)

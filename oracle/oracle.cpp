@@ -276,45 +276,65 @@ extern "C" void orc_model_set_density(orc_model* m, const double* d, double pena
   m->penal = penal;
 }
 
-// FeModel.AssembleForces (FeModel.cs:263-321)
-extern "C" int orc_model_assemble_forces(const orc_model* m, double* f, char* msg, int msglen) {
-  for (int64_t i = 0; i < m->total_dofs; ++i) f[i] = 0.0;
-  for (const orc_load& l : m->loads) {
-    int n = (int)l.nodes.size();
-    if (n == 0) {
-      if (l.f[0] != 0.0f || l.f[1] != 0.0f || l.f[2] != 0.0f) {
-        set_msg(msg, msglen, "Cannot assemble load case: surface patch contains 0 nodes.");
-        return ORC_E_INVALID_OPERATION;
-      }
-      continue;
+// One load case's nodal forces added into f (the body of FeModel.AssembleForces' loop, FeModel.cs:267-318)
+static int add_load_case(const orc_model* m, const orc_load& l, double* f, char* msg, int msglen) {
+  int n = (int)l.nodes.size();
+  if (n == 0) {
+    if (l.f[0] != 0.0f || l.f[1] != 0.0f || l.f[2] != 0.0f) {
+      set_msg(msg, msglen, "Cannot assemble load case: surface patch contains 0 nodes.");
+      return ORC_E_INVALID_OPERATION;
     }
-    double total = 0.0;
-    for (int i = 0; i < n; ++i) total += l.areas[i];
-    for (int i = 0; i < n; ++i)
-      if ((uint64_t)(uint32_t)l.nodes[i] >= (uint64_t)m->total_nodes || l.nodes[i] < 0) {
-        set_msg(msg, msglen, "Patch node index is out of bounds.");
-        return ORC_E_INVALID_OPERATION;
-      }
-    if (total <= 0.0) {
-      double inv = 1.0 / n;
-      double fx = (double)l.f[0] * inv, fy = (double)l.f[1] * inv, fz = (double)l.f[2] * inv;
-      for (int i = 0; i < n; ++i) {
-        int64_t nd = l.nodes[i];
-        f[3 * nd] += fx; f[3 * nd + 1] += fy; f[3 * nd + 2] += fz;
-      }
-    } else {
-      double inv = 1.0 / total;
-      for (int i = 0; i < n; ++i) {
-        int64_t nd = l.nodes[i];
-        double w = l.areas[i] * inv;
-        f[3 * nd] += (double)l.f[0] * w;
-        f[3 * nd + 1] += (double)l.f[1] * w;
-        f[3 * nd + 2] += (double)l.f[2] * w;
-      }
+    return ORC_OK;
+  }
+  double total = 0.0;
+  for (int i = 0; i < n; ++i) total += l.areas[i];
+  for (int i = 0; i < n; ++i)
+    if ((uint64_t)(uint32_t)l.nodes[i] >= (uint64_t)m->total_nodes || l.nodes[i] < 0) {
+      set_msg(msg, msglen, "Patch node index is out of bounds.");
+      return ORC_E_INVALID_OPERATION;
+    }
+  if (total <= 0.0) {
+    double inv = 1.0 / n;
+    double fx = (double)l.f[0] * inv, fy = (double)l.f[1] * inv, fz = (double)l.f[2] * inv;
+    for (int i = 0; i < n; ++i) {
+      int64_t nd = l.nodes[i];
+      f[3 * nd] += fx; f[3 * nd + 1] += fy; f[3 * nd + 2] += fz;
+    }
+  } else {
+    double inv = 1.0 / total;
+    for (int i = 0; i < n; ++i) {
+      int64_t nd = l.nodes[i];
+      double w = l.areas[i] * inv;
+      f[3 * nd] += (double)l.f[0] * w;
+      f[3 * nd + 1] += (double)l.f[1] * w;
+      f[3 * nd + 2] += (double)l.f[2] * w;
     }
   }
   return ORC_OK;
 }
+
+// FeModel.AssembleForces (FeModel.cs:263-321): all load cases summed into one vector, in case order
+extern "C" int orc_model_assemble_forces(const orc_model* m, double* f, char* msg, int msglen) {
+  for (int64_t i = 0; i < m->total_dofs; ++i) f[i] = 0.0;
+  for (const orc_load& l : m->loads) {
+    int st = add_load_case(m, l, f, msg, msglen);
+    if (st) return st;
+  }
+  return ORC_OK;
+}
+
+// Load case k alone (the same arithmetic on a zero vector): the right-hand side of case k when load cases are
+// kept separate (no counterpart in the reference, which sums them)
+extern "C" int orc_model_assemble_case_forces(const orc_model* m, int32_t k, double* f, char* msg, int msglen) {
+  if (k < 0 || k >= (int32_t)m->loads.size()) {
+    set_msg(msg, msglen, "Load case index is out of range.");
+    return ORC_E_ARG;
+  }
+  for (int64_t i = 0; i < m->total_dofs; ++i) f[i] = 0.0;
+  return add_load_case(m, m->loads[k], f, msg, msglen);
+}
+
+extern "C" int32_t orc_model_load_case_count(const orc_model* m) { return (int32_t)m->loads.size(); }
 
 // ---------------------------------------------------------------------------------------------------------
 // FemOperator — src/Mycel.Core/Fem/FemOperator.cs:33-294, 379-439
@@ -1118,14 +1138,25 @@ extern "C" int orc_topopt_run(orc_model* m, const orc_simp_options* o, orc_iter_
   std::vector<double> u(nd, 0.0);
   if (o->warm_start && o->warm_start_len == nd) std::copy(o->warm_start, o->warm_start + nd, u.begin());
   orc_op* op = orc_op_create(m);
-  std::vector<double> F(nd), b(nd);
-  int st = orc_model_assemble_forces(m, F.data(), msg, msglen);
+  // Load cases: summed into one right-hand side as the reference does, or (separate_load_cases) kept apart:
+  // one solve per case with its own warm start, compliance sum_k F_k.u_k and sensitivities summed over the
+  // cases in case order (objective sum_k c_k, an extension: the reference has no multi-load objective)
+  const int ncase = o->separate_load_cases ? std::max<int>(1, (int)m->loads.size()) : 1;
+  std::vector<std::vector<double>> Fk(ncase, std::vector<double>(nd)), bk(ncase, std::vector<double>(nd));
+  std::vector<std::vector<double>> uk;
+  int st = ORC_OK;
+  for (int k = 0; k < ncase && !st; ++k)
+    st = o->separate_load_cases && !m->loads.empty() ? orc_model_assemble_case_forces(m, k, Fk[k].data(), msg, msglen)
+                                                     : orc_model_assemble_forces(m, Fk[k].data(), msg, msglen);
   if (st) {
     orc_op_free(op);
     orc_filter_free(filt);
     return st;
   }
-  for (int64_t i = 0; i < nd; ++i) b[i] = m->constrained[i] ? 0.0 : F[i];
+  for (int k = 0; k < ncase; ++k)
+    for (int64_t i = 0; i < nd; ++i) bk[k][i] = m->constrained[i] ? 0.0 : Fk[k][i];
+  if (o->separate_load_cases) uk.assign(ncase, std::vector<double>(nd, 0.0));
+  std::vector<double> dck(o->separate_load_cases ? na : 0);
   double lambda = 1.0, maxChange = 1.0, beta = 1.0;
   int conv = 0;
   std::vector<double> chist;
@@ -1157,28 +1188,46 @@ extern "C" int orc_topopt_run(orc_model* m, const orc_simp_options* o, orc_iter_
       tol = std::pow(10.0, lt);
     }
     orc_pcg_result pr;
-    st = orc_pcg_solve(op, b.data(), u.data(), tol, o->solver_max_iterations, &pr, msg, msglen);
-    if (st) break;
-    if (!pr.converged) {
-      char buf[400];
-      std::snprintf(buf, sizeof buf,
-                    "FEM solver did not converge in %d iterations (%s). Is the model not sufficiently constrained?",
-                    pr.iterations, pr.message);
-      set_msg(msg, msglen, buf);
-      st = ORC_E_NOT_CONVERGED;
-      break;
-    }
-    double c = 0.0;
-    for (int64_t i = 0; i < nd; ++i) c += F[i] * u[i];
-    double md = 0.0;
-    for (int64_t q = 0; q < m->total_nodes; ++q)
-      if (m->active_nodes[q]) {
-        double ux = u[3 * q], uy = u[3 * q + 1], uz = u[3 * q + 2];
-        double sq = ux * ux + uy * uy + uz * uz;
-        if (sq > md) md = sq;
+    int iters = 0;
+    double resid = 0.0, c = 0.0, md = 0.0;
+    for (int k = 0; k < ncase; ++k) {
+      std::vector<double>& uc = o->separate_load_cases ? uk[k] : u;
+      st = orc_pcg_solve(op, bk[k].data(), uc.data(), tol, o->solver_max_iterations, &pr, msg, msglen);
+      if (st) break;
+      if (!pr.converged) {
+        char buf[400];
+        std::snprintf(buf, sizeof buf,
+                      "FEM solver did not converge in %d iterations (%s). Is the model not sufficiently constrained?",
+                      pr.iterations, pr.message);
+        set_msg(msg, msglen, buf);
+        st = ORC_E_NOT_CONVERGED;
+        break;
       }
+      iters += pr.iterations;
+      resid = std::max(resid, pr.final_residual);
+      double ck = 0.0;
+      for (int64_t i = 0; i < nd; ++i) ck += Fk[k][i] * uc[i];
+      c += ck;
+      for (int64_t q = 0; q < m->total_nodes; ++q)
+        if (m->active_nodes[q]) {
+          double ux = uc[3 * q], uy = uc[3 * q + 1], uz = uc[3 * q + 2];
+          double sq = ux * ux + uy * uy + uz * uz;
+          if (sq > md) md = sq;
+        }
+      if (k == 0) {
+        orc_sensitivities(op, uc.data(), rb.data(), dcb.data(), penal);
+      } else {
+        orc_sensitivities(op, uc.data(), rb.data(), dck.data(), penal);
+        for (int32_t i = 0; i < na; ++i) dcb[i] = dcb[i] + dck[i];
+      }
+    }
+    if (st) break;
     md = std::sqrt(md);
-    orc_sensitivities(op, u.data(), rb.data(), dcb.data(), penal);
+    if (o->separate_load_cases) {  // u reported: the superposition sum_k u_k, in case order
+      for (int64_t i = 0; i < nd; ++i) u[i] = uk[0][i];
+      for (int k = 1; k < ncase; ++k)
+        for (int64_t i = 0; i < nd; ++i) u[i] = u[i] + uk[k][i];
+    }
     if (o->enable_heaviside) {
       orc_heaviside_derivative(rt.data(), dd.data(), na, beta, 0.5);
       for (int32_t i = 0; i < na; ++i) dct[i] = dcb[i] * dd[i];
@@ -1206,8 +1255,8 @@ extern "C" int orc_topopt_run(orc_model* m, const orc_simp_options* o, orc_iter_
       rec.volume_fraction = cv / na;
       rec.max_change = maxChange;
       rec.grey_level = (4.0 * gs / na) * 100.0;
-      rec.solver_iterations = pr.iterations;
-      rec.solver_residual = pr.final_residual;
+      rec.solver_iterations = iters;
+      rec.solver_residual = resid;
       rec.max_displacement = md;
       rec.total_ms = 0;
     }

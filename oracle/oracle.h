@@ -54,6 +54,9 @@ void orc_model_counts(const orc_model* m, int64_t* out6);
 void orc_model_active_elements(const orc_model* m, int32_t* out);
 void orc_model_constrained(const orc_model* m, uint8_t* out);
 int orc_model_assemble_forces(const orc_model* m, double* f, char* msg, int msglen);
+/* load case k alone, and the number of load cases */
+int orc_model_assemble_case_forces(const orc_model* m, int32_t k, double* f, char* msg, int msglen);
+int32_t orc_model_load_case_count(const orc_model* m);
 void orc_model_set_density(orc_model* m, const double* density_box, double penal);
 
 /* FemOperator */
@@ -126,6 +129,9 @@ typedef struct {
   const double* warm_start;
   int64_t warm_start_len;
   int32_t enforce_min_filter_radius;
+  /* 0: load cases summed into one right-hand side (the reference); 1: one solve per load case, objective the
+     sum of the cases' compliances, sensitivities summed in case order, u reported as the sum of the cases' u */
+  int32_t separate_load_cases;
 } orc_simp_options;
 
 typedef struct {

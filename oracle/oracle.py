@@ -59,7 +59,8 @@ class SimpOpts(C.Structure):
                 ("enable_heaviside", C.c_int32), ("rho_min", C.c_double), ("passive_mask", P),
                 ("passive_len", C.c_int64), ("protect_boundary_hinges", C.c_int32), ("initial_density", P),
                 ("initial_density_len", C.c_int64), ("start_iteration", C.c_int32), ("warm_start", P),
-                ("warm_start_len", C.c_int64), ("enforce_min_filter_radius", C.c_int32)]
+                ("warm_start_len", C.c_int64), ("enforce_min_filter_radius", C.c_int32),
+                ("separate_load_cases", C.c_int32)]
 
 
 class IterRec(C.Structure):
@@ -81,6 +82,9 @@ def _setup(L):
     L.orc_model_active_elements.argtypes = [P, ip]
     L.orc_model_constrained.argtypes = [P, bp]
     L.orc_model_assemble_forces.argtypes = [P, dp, C.c_char_p, C.c_int]
+    L.orc_model_assemble_case_forces.argtypes = [P, C.c_int32, dp, C.c_char_p, C.c_int]
+    L.orc_model_load_case_count.restype = C.c_int32
+    L.orc_model_load_case_count.argtypes = [P]
     L.orc_model_set_density.argtypes = [P, dp, C.c_double]
     L.orc_op_create.restype = P
     L.orc_op_create.argtypes = [P]
@@ -206,6 +210,18 @@ class Model:
         if st:
             _raise(st, msg)
         return f
+
+    def case_forces(self, k):
+        """Load case k alone (the right-hand side of case k when load cases are kept separate)."""
+        f = np.zeros(self.fe.total_dofs)
+        msg = C.create_string_buffer(512)
+        st = lib().orc_model_assemble_case_forces(self.h, int(k), f, msg, 512)
+        if st:
+            _raise(st, msg)
+        return f
+
+    def load_case_count(self):
+        return int(lib().orc_model_load_case_count(self.h))
 
     def update_densities(self, dens_box, penal):
         lib().orc_op_update_densities(self.op, np.ascontiguousarray(dens_box, dtype=np.float64), float(penal))
@@ -396,7 +412,7 @@ def topopt_run(fe: FeModel, o: OptimizerOptions) -> OracleSimpResult:
     so = SimpOpts(o.volume_fraction, o.filter_radius_mm, o.penal, o.move_limit, o.max_iterations,
                   o.solver_tolerance_initial, o.solver_tolerance_final, o.solver_max_iterations, int(o.continuation),
                   int(o.enable_heaviside), o.rho_min, pm, pl, int(o.protect_boundary_hinges), idp, idl,
-                  o.start_iteration, wp, wl, int(o.enforce_minimum_filter_radius))
+                  o.start_iteration, wp, wl, int(o.enforce_minimum_filter_radius), int(o.separate_load_cases))
     cap = max(1, o.max_iterations - o.start_iteration + 1)
     recs = (IterRec * cap)()
     ni = C.c_int32(0)

@@ -88,3 +88,30 @@ def test_unknown_job_is_an_argument_error():
     with api.Server(slots=1, hbm_budget_bytes=10**9) as srv:
         with pytest.raises(ArgumentError):
             srv.info(12345)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed-mg"])
+def test_separate_load_cases_served(ctx, precision):
+    """Jobs whose load cases are kept apart: same results alone and in the mix, estimate bounds their memory."""
+    jobs = [(m, o.replace(separate_load_cases=True)) for m, o in _jobs(precision, n=4, iters=3)]
+    assert sum(len(m.loads) > 1 for m, _ in jobs) >= 3
+    alone = [api.TopologyOptimizer.run(m, o, ctx=ctx) for m, o in jobs]
+    with api.Server(slots=3, hbm_budget_bytes=8 * 10**9) as srv:
+        ids = [srv.submit(m, o) for m, o in jobs]
+        srv.wait()
+        for jid, ref in zip(ids, alone):
+            r = srv.result(jid)
+            assert r["info"]["state"] == "done", r["info"]["message"]
+            for a, b in zip(r["history"], ref.snapshots):
+                assert abs(a.compliance - b.compliance) <= (0.0 if precision == "fp64" else 1e-12) * abs(b.compliance)
+    m, o = W.served_job(30, 14, 10, 2, seed=2, precision=precision)
+    o = o.replace(separate_load_cases=True)
+    assert len(m.loads) == 3
+    est = api.Server.device_bytes(m, o)
+    pr = api.Problem(m, ctx)
+    sess = api.SimpSession(pr, o)
+    sess.step()
+    held = pr.info()["device_bytes"]
+    sess.close()
+    pr.close()
+    assert held <= est <= 1.25 * held
