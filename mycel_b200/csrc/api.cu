@@ -144,6 +144,13 @@ __global__ void k_state_rel_from_b(PcgState* st) {
 }
 
 // ordered list of indices i with b[i] != 0 and DOF i unconstrained (P b non-zeros, ascending)
+// b = P F: F with the constrained DOFs zeroed
+__global__ void k_project_rhs(int64_t n, const double* __restrict__ F, const uint8_t* __restrict__ nf,
+                              double* __restrict__ b) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) b[i] = (nf[i / 3] & (1 << (i % 3))) ? 0.0 : F[i];
+}
+
 __global__ void k_nz_count(int64_t n, const double* __restrict__ b, const uint8_t* __restrict__ nf, int32_t* cnt) {
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   int v = 0;
@@ -544,10 +551,8 @@ extern "C" int32_t mycel_problem_create(mycel_ctx* c, const mycel_grid* grid, co
   launch_setup_nodes(p, p->d_fixed, n_fixed, d_cnt);
   // b = P F and its ordered non-zero list
   int32_t nb_cnt = 0;
-  {
-    // d_b = F masked by the constrained flags: reuse the non-zero list builder on F itself
-    cudaMemcpyAsync(p->d_b, p->d_F, sizeof(double) * g.nd, cudaMemcpyDeviceToDevice, s);
-  }
+  k_project_rhs<<<(unsigned)((g.nd + 255) / 256), 256, 0, s>>>(g.nd, p->d_F, p->d_nflags, p->d_b);
+  c->launches++;
   int32_t st = build_nz_list(p, p->d_F, p->d_bnz, &nb_cnt);
   if (st) {
     dfree(c->stream, d_cnt);
@@ -571,14 +576,6 @@ extern "C" int32_t mycel_problem_create(mycel_ctx* c, const mycel_grid* grid, co
   for (int64_t n = 0; n < g.nn; ++n) an += (nf[n] & NF_ACTIVE) ? 1 : 0;
   p->n_active_nodes = an;
   p->n_active_fixed = hcnt;
-  // b = P F on device
-  {
-    std::vector<double> b(p->forces_host);
-    for (int64_t i = 0; i < g.nd; ++i)
-      if (nf[i / 3] & (1 << (i % 3))) b[i] = 0.0;
-    cudaMemcpyAsync(p->d_b, b.data(), sizeof(double) * g.nd, cudaMemcpyHostToDevice, s);
-    cudaStreamSynchronize(s);
-  }
   launch_update_E(p, p->d_rho_box, penal);
   launch_diag(p);
   if ((e = cudaGetLastError()) != cudaSuccess || (e = cudaStreamSynchronize(s)) != cudaSuccess) {
