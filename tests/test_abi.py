@@ -73,3 +73,17 @@ def test_job_device_bytes_counts_the_multigrid_hierarchy():
     assert est["mg"] - est["mixed"] >= 4 * 576 * 16 * 8 * 8
     big = api.Server.device_bytes(*W.served_job(64, 32, 32, 2, seed=1, precision="mg"))
     assert big > 6 * est["mg"]
+
+
+def test_job_device_bytes_counts_separate_load_cases():
+    """Load cases kept apart add each case's F, P F and u (3 x 8 B per DOF per case) to the estimate; with one
+    load case the option changes nothing."""
+    from mycel_b200 import api, workloads as W
+    m, o = W.served_job(30, 14, 10, 2, seed=2, precision="mixed-mg")
+    assert len(m.loads) == 3
+    summed = api.Server.device_bytes(m, o)
+    apart = api.Server.device_bytes(m, o.replace(separate_load_cases=True))
+    assert apart - summed >= 3 * 8 * 3 * m.total_dofs
+    m1, o1 = W.served_job(30, 14, 10, 2, seed=1, precision="mixed-mg")
+    assert len(m1.loads) == 1
+    assert api.Server.device_bytes(m1, o1) == api.Server.device_bytes(m1, o1.replace(separate_load_cases=True))
