@@ -1959,15 +1959,6 @@ __global__ void __launch_bounds__(kMgDofThreads) k_mg_apply(MgDims d, const floa
   if (n < nn) mg_apply_row(d, nn, n, mg_dof_comp(), S, x, r, invd, y, mode, mode == 1 ? *om : 0.0f);
 }
 
-// first sweep from x = 0 on a coarse level: x = omega invd r
-__global__ void k_mg_jacobi0(int64_t nd, const float* __restrict__ r, const float* __restrict__ invd,
-                             float* __restrict__ x, const float* __restrict__ om, const MixState* st) {
-  if (!mg_running(st)) return;
-  const float omega = *om;
-  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (q < nd) x[q] = omega * invd[q] * r[q];
-}
-
 // a further sweep on the voxel grid (padded FP32 layout, t = A x): x += omega invd (r - t)
 __global__ void k_mg_jacobi_fine(int64_t n, const float* __restrict__ r, const float* __restrict__ t,
                                  const float* __restrict__ invd, float* __restrict__ x, const float* __restrict__ om,
@@ -2056,7 +2047,8 @@ __device__ __forceinline__ void mg_prolong_comp(const MgDims& f, int pitch, cons
 template <bool PAD>
 __device__ __forceinline__ void mg_restrict_node(const MgDims& f, int pitch, const float* __restrict__ rf,
                                                  const float* __restrict__ tf, const MgDims& c,
-                                                 const float* __restrict__ invdc, float* __restrict__ rc, int64_t n) {
+                                                 const float* __restrict__ invdc, float* __restrict__ rc, int64_t n,
+                                                 float* __restrict__ xc, float omega) {
   const int cx1 = c.nx + 1, cy1 = c.ny + 1;
   const int I = (int)(n % cx1), J = (int)((n / cx1) % cy1), K = (int)(n / ((int64_t)cx1 * cy1));
   const int pi = min(2 * I, f.nx), pj = min(2 * J, f.ny), pk = min(2 * K, f.nz);
@@ -2089,17 +2081,26 @@ __device__ __forceinline__ void mg_restrict_node(const MgDims& f, int pitch, con
       }
     }
   }
-  rc[3 * n] = invdc[3 * n] != 0.f ? a0 : 0.f;
-  rc[3 * n + 1] = invdc[3 * n + 1] != 0.f ? a1 : 0.f;
-  rc[3 * n + 2] = invdc[3 * n + 2] != 0.f ? a2 : 0.f;
+  const float d0 = invdc[3 * n], d1 = invdc[3 * n + 1], d2 = invdc[3 * n + 2];
+  const float r0 = d0 != 0.f ? a0 : 0.f, r1 = d1 != 0.f ? a1 : 0.f, r2 = d2 != 0.f ? a2 : 0.f;
+  rc[3 * n] = r0;
+  rc[3 * n + 1] = r1;
+  rc[3 * n + 2] = r2;
+  if (xc) {  // the coarse level's first Jacobi sweep from x = 0: x = omega invd r
+    xc[3 * n] = omega * d0 * r0;
+    xc[3 * n + 1] = omega * d1 * r1;
+    xc[3 * n + 2] = omega * d2 * r2;
+  }
 }
 
 template <bool PAD>
 __global__ void k_mg_restrict(MgDims f, int pitch, const float* __restrict__ rf, const float* __restrict__ tf,
-                              MgDims c, const float* __restrict__ invdc, float* __restrict__ rc, const MixState* st) {
+                              MgDims c, const float* __restrict__ invdc, float* __restrict__ rc, const MixState* st,
+                              float* __restrict__ xc, const float* __restrict__ om) {
   if (!mg_running(st)) return;
+  const float omega = xc ? *om : 0.f;
   const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (n < mg_nn(c)) mg_restrict_node<PAD>(f, pitch, rf, tf, c, invdc, rc, n);
+  if (n < mg_nn(c)) mg_restrict_node<PAD>(f, pitch, rf, tf, c, invdc, rc, n, xc, omega);
 }
 
 // prolongation x_f += W x_c at fine node n, on the finer level's free DOFs. PAD: the voxel grid (padded FP32
@@ -2866,7 +2867,7 @@ static int32_t mg_ensure(mycel_problem* p, bool* available) {
   }
   // launches per outer iteration: matvec, k_mg_enter*, the V-cycle (as issued by mg_vcycle), k_mg_exit*
   const int sw = mg->sweeps, T = mg->T;
-  const int cycle = 4 * (sw - 1) + 2 + (T - 1) * (2 + sw) + 1 + (T - 1) * (1 + sw) + 1 + 1;
+  const int cycle = 4 * (sw - 1) + 2 + (T - 1) * (1 + sw) + 1 + (T - 1) * (1 + sw) + 1 + 1;
   mg->per_iter = 3 + cycle;
   p->mg = mg;
   if (oom) return set_error(p->ctx, MYCEL_E_OOM, "out of device memory for the multigrid hierarchy");
@@ -2954,22 +2955,24 @@ static int mg_vcycle(mycel_problem* p, cudaStream_t s, MixState* st, float* rf, 
     nl += 2;
   }
   fine_mv();
-  k_mg_restrict<true><<<mg_blocks(lv[1].nn), 256, 0, s>>>(lv[0].d, g.rp, rf, tf, lv[1].d, lv[1].invd, lv[1].r, st);
+  // restriction to level 1, with level 1's first sweep (unless level 1 is the cluster kernel's)
+  k_mg_restrict<true><<<mg_blocks(lv[1].nn), 256, 0, s>>>(lv[0].d, g.rp, rf, tf, lv[1].d, lv[1].invd, lv[1].r, st,
+                                                          mg->T > 1 ? lv[1].xa : nullptr, om + 1);
   nl += 2;
   float* xc[kMgMaxLevels] = {};
   for (int l = 1; l < mg->T; ++l) {
     MgLevel& v = lv[l];
     float *x = v.xa, *o = v.xb;
-    k_mg_jacobi0<<<mg_blocks(v.nd), 256, 0, s>>>(v.nd, v.r, v.invd, x, om + l, st);
     for (int k = 1; k < mg->sweeps; ++k) {
       launch_mg_apply(s, v, x, v.r, v.invd, o, 1, om + l, st);
       std::swap(x, o);
     }
     launch_mg_apply(s, v, x, v.r, v.invd, v.t, 2, om + l, st);
     k_mg_restrict<false><<<mg_blocks(lv[l + 1].nn), 256, 0, s>>>(v.d, 0, nullptr, v.t, lv[l + 1].d, lv[l + 1].invd,
-                                                                 lv[l + 1].r, st);
+                                                                 lv[l + 1].r, st,
+                                                                 l + 1 < mg->T ? lv[l + 1].xa : nullptr, om + l + 1);
     xc[l] = x;
-    nl += 2 + mg->sweeps;
+    nl += 1 + mg->sweeps;
   }
   k_mg_tail<<<kMgTailCtas, kMgTailThreads, 0, s>>>(mg->tail, om, st);
   xc[mg->T] = lv[mg->T].xa;
