@@ -1221,12 +1221,26 @@ __global__ void __launch_bounds__(256) k_oc(OcArgs a, OcParams prm) {
   int slot = 0;
   auto element = [&](int64_t i) -> int64_t { return a.idx ? (int64_t)a.idx[i] : i; };
   auto volume = [&](double lam) -> double {
+    // the thread's elements t0, t0 + stride, ... summed in that order; the loads of 8 of them are issued before
+    // their terms are added, so the index -> data load chains overlap
+    constexpr int kB = 8;
     double v = 0.0;
-    for (int64_t i = t0; i < a.n; i += stride) {
-      int64_t e = element(i);
-      bool pas = a.pas && a.pas[e];
-      double si = a.s[e];
-      v = v + si * (pas ? 1.0 : oc_new_rho(a.rho[e], a.dc[e], si, false, lam, prm.move, prm.rho_min));
+    for (int64_t base = t0; base < a.n; base += kB * stride) {
+      double si[kB], rr[kB], dd[kB];
+      bool pp[kB];
+#pragma unroll
+      for (int k = 0; k < kB; ++k) {
+        const int64_t i = base + k * stride;
+        const int64_t e = i < a.n ? element(i) : 0;
+        pp[k] = i < a.n && a.pas && a.pas[e];
+        si[k] = i < a.n ? a.s[e] : 0.0;
+        rr[k] = i < a.n ? a.rho[e] : 0.0;
+        dd[k] = i < a.n ? a.dc[e] : 0.0;
+      }
+#pragma unroll
+      for (int k = 0; k < kB; ++k)
+        if (base + k * stride < a.n)
+          v = v + si[k] * (pp[k] ? 1.0 : oc_new_rho(rr[k], dd[k], si[k], false, lam, prm.move, prm.rho_min));
     }
     double tot = grid_total(v, a, slot, sh, &ok);
     slot ^= 1;
