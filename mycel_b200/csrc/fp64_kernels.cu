@@ -610,9 +610,14 @@ __global__ void k_bnorm_list(const double* __restrict__ b, const int32_t* __rest
                              PcgState* st) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   double s = 0.0;
-  for (int32_t q = 0; q < cnt; ++q) {
-    double v = b[idx[q]];
-    s = s + v * v;
+  constexpr int kB = 16;  // loads of 16 entries issued before they are added, in list order
+  for (int32_t q0 = 0; q0 < cnt; q0 += kB) {
+    double v[kB];
+#pragma unroll
+    for (int k = 0; k < kB; ++k) v[k] = q0 + k < cnt ? b[idx[q0 + k]] : 0.0;
+#pragma unroll
+    for (int k = 0; k < kB; ++k)
+      if (q0 + k < cnt) s = s + v[k] * v[k];
   }
   st->bn2 = s;
   st->bnorm = sqrt(s);
@@ -678,7 +683,19 @@ __global__ void k_compliance(const double* __restrict__ F, const double* __restr
                              const int32_t* __restrict__ idx, int32_t cnt, double* out) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   double c = 0.0;
-  for (int32_t q = 0; q < cnt; ++q) c = c + F[idx[q]] * u[idx[q]];
+  constexpr int kB = 16;  // loads of 16 terms issued before they are added, in list order
+  for (int32_t q0 = 0; q0 < cnt; q0 += kB) {
+    double fv[kB], uv[kB];
+#pragma unroll
+    for (int k = 0; k < kB; ++k) {
+      const int32_t j = q0 + k < cnt ? idx[q0 + k] : 0;
+      fv[k] = q0 + k < cnt ? F[j] : 0.0;
+      uv[k] = q0 + k < cnt ? u[j] : 0.0;
+    }
+#pragma unroll
+    for (int k = 0; k < kB; ++k)
+      if (q0 + k < cnt) c = c + fv[k] * uv[k];
+  }
   *out = c;
 }
 
