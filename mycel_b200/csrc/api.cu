@@ -687,7 +687,7 @@ namespace mycel {
 // (compliance F_k . u_k, as k_compliance sums F . u) and of P F_k (the PCG's ||P b||), at case_nz_off[2k] and
 // case_nz_off[2k + 1].
 int32_t ensure_cases(mycel_problem* p) {
-  if (p->d_case_F || p->n_cases <= 0) return MYCEL_OK;
+  if (p->d_case_nz || p->n_cases <= 0) return MYCEL_OK;  // the non-zero lists are written last
   if (p->assemble_status) return set_error(p->ctx, p->assemble_status, p->assemble_msg);
   mycel_ctx* c = p->ctx;
   cudaStream_t s = c->stream;
@@ -700,9 +700,17 @@ int32_t ensure_cases(mycel_problem* p) {
   std::vector<int32_t> lists;
   p->case_nz_off.assign(2 * (size_t)m, 0);
   p->case_nz_cnt.assign(2 * (size_t)m, 0);
-  if (dalloc(p, &p->d_case_F, (size_t)(m * nd)) || dalloc(p, &p->d_case_b, (size_t)(m * nd))) {
+  auto release = [&] {  // after a failure nothing is kept, so a later call starts over
+    const int64_t fb = ((int64_t)(8 * m * nd) + 15) & ~int64_t(15);
+    if (p->d_case_F) p->device_bytes -= fb;
+    if (p->d_case_b) p->device_bytes -= fb;
     dfree(s, p->d_case_F);
-    p->d_case_F = nullptr;
+    dfree(s, p->d_case_b);
+    p->d_case_F = p->d_case_b = nullptr;
+  };
+  if ((!p->d_case_F && dalloc(p, &p->d_case_F, (size_t)(m * nd))) ||
+      (!p->d_case_b && dalloc(p, &p->d_case_b, (size_t)(m * nd)))) {
+    release();
     return set_error(c, MYCEL_E_OOM, "out of device memory for the load cases");
   }
   for (int k = 0; k < m; ++k) {
@@ -721,8 +729,11 @@ int32_t ensure_cases(mycel_problem* p) {
     MYCEL_CUDA(c, cudaMemcpyAsync(p->d_case_b + k * nd, b.data(), sizeof(double) * nd, cudaMemcpyHostToDevice, s));
     MYCEL_CUDA(c, cudaStreamSynchronize(s));  // f and b are refilled for the next case
   }
-  if (dalloc(p, &p->d_case_nz, std::max<size_t>(lists.size(), 1)))
+  if (dalloc(p, &p->d_case_nz, std::max<size_t>(lists.size(), 1))) {
+    p->d_case_nz = nullptr;
+    release();
     return set_error(c, MYCEL_E_OOM, "out of device memory for the load cases");
+  }
   if (!lists.empty())
     MYCEL_CUDA(c, cudaMemcpyAsync(p->d_case_nz, lists.data(), sizeof(int32_t) * lists.size(), cudaMemcpyHostToDevice, s));
   MYCEL_CUDA(c, cudaStreamSynchronize(s));
