@@ -2,7 +2,7 @@
 
 Tolerances (stated): FP32 matvec within 2e-6 of max|K x| (FP32 accumulation of 24-term rows over 8 elements);
 solves to the same FP64 residual tolerance agree in compliance to 1e-8 relative and in u to 1e-6 of max|u|;
-the SIMP loop agrees in compliance to 1e-6 relative per iteration.
+the SIMP loop agrees in compliance to 1e-6 relative per iteration (the accuracy the mixed form is specified to).
 """
 import numpy as np
 import pytest
