@@ -1976,7 +1976,7 @@ template <bool PAD>
 __device__ __forceinline__ void mg_restrict_comp(const MgDims& f, int pitch, const float* __restrict__ rf,
                                                  const float* __restrict__ tf, const MgDims& c,
                                                  const float* __restrict__ invdc, float* __restrict__ rc, int64_t n,
-                                                 int cc) {
+                                                 int cc, float* __restrict__ xc, float omega) {
   const int cx1 = c.nx + 1, cy1 = c.ny + 1;
   const int I = (int)(n % cx1), J = (int)((n / cx1) % cy1), K = (int)(n / ((int64_t)cx1 * cy1));
   const int pi = min(2 * I, f.nx), pj = min(2 * J, f.ny), pk = min(2 * K, f.nz);
@@ -2001,7 +2001,9 @@ __device__ __forceinline__ void mg_restrict_comp(const MgDims& f, int pitch, con
       }
     }
   }
-  rc[3 * n + cc] = invdc[3 * n + cc] != 0.f ? a : 0.f;
+  const float d = invdc[3 * n + cc], rv = d != 0.f ? a : 0.f;
+  rc[3 * n + cc] = rv;
+  if (xc) xc[3 * n + cc] = omega * d * rv;  // the coarse level's first Jacobi sweep from x = 0
 }
 
 
@@ -2275,9 +2277,7 @@ __global__ void __cluster_dims__(kMgTailCtas, 1, 1) __launch_bounds__(kMgTailThr
     const MgTailLevel& v = tl.lv[l];
     const MgTailLevel& cv = tl.lv[l + 1];
     const float w = om[l];
-    float *x = v.xa, *o = v.xb;
-    for (int64_t q = gt; q < 3 * v.nn; q += gs) x[q] = w * v.invd[q] * v.r[q];
-    mg_cluster_sync();
+    float *x = v.xa, *o = v.xb;  // x = omega invd r, written with r by the restriction into this level
     for (int k = 1; k < tl.sweeps; ++k) {
       apply(v, x, o, 1, w);
       mg_cluster_sync();
@@ -2287,8 +2287,11 @@ __global__ void __cluster_dims__(kMgTailCtas, 1, 1) __launch_bounds__(kMgTailThr
     }
     apply(v, x, v.t, 2, 0.0f);
     mg_cluster_sync();
+    const bool smoothed = l + 1 < tl.L - 1;  // the coarsest level is solved, not smoothed
+    const float wc = smoothed ? om[l + 1] : 0.0f;
     for (int64_t q = gt; q < 3 * cv.nn; q += gs)
-      mg_restrict_comp<false>(v.d, 0, nullptr, v.t, cv.d, cv.invd, cv.r, q / 3, (int)(q % 3));
+      mg_restrict_comp<false>(v.d, 0, nullptr, v.t, cv.d, cv.invd, cv.r, q / 3, (int)(q % 3),
+                              smoothed ? cv.xa : nullptr, wc);
     mg_cluster_sync();
     xc[l] = x;
   }
@@ -2955,9 +2958,9 @@ static int mg_vcycle(mycel_problem* p, cudaStream_t s, MixState* st, float* rf, 
     nl += 2;
   }
   fine_mv();
-  // restriction to level 1, with level 1's first sweep (unless level 1 is the cluster kernel's)
+  // restriction to level 1, with level 1's first sweep (unless level 1 is the coarsest)
   k_mg_restrict<true><<<mg_blocks(lv[1].nn), 256, 0, s>>>(lv[0].d, g.rp, rf, tf, lv[1].d, lv[1].invd, lv[1].r, st,
-                                                          mg->T > 1 ? lv[1].xa : nullptr, om + 1);
+                                                          1 < mg->L - 1 ? lv[1].xa : nullptr, om + 1);
   nl += 2;
   float* xc[kMgMaxLevels] = {};
   for (int l = 1; l < mg->T; ++l) {
@@ -2970,7 +2973,8 @@ static int mg_vcycle(mycel_problem* p, cudaStream_t s, MixState* st, float* rf, 
     launch_mg_apply(s, v, x, v.r, v.invd, v.t, 2, om + l, st);
     k_mg_restrict<false><<<mg_blocks(lv[l + 1].nn), 256, 0, s>>>(v.d, 0, nullptr, v.t, lv[l + 1].d, lv[l + 1].invd,
                                                                  lv[l + 1].r, st,
-                                                                 l + 1 < mg->T ? lv[l + 1].xa : nullptr, om + l + 1);
+                                                                 l + 1 < mg->L - 1 ? lv[l + 1].xa : nullptr,
+                                                                 om + l + 1);
     xc[l] = x;
     nl += 1 + mg->sweeps;
   }
