@@ -11,6 +11,7 @@
 #include <deque>
 #include <string>
 #include <thread>
+#include <unordered_map>
 #include <unordered_set>
 #include <vector>
 
@@ -144,6 +145,13 @@ __global__ void k_state_rel_from_b(PcgState* st) {
 }
 
 // ordered list of indices i with b[i] != 0 and DOF i unconstrained (P b non-zeros, ascending)
+// F[idx[q]] = val[q]: the assembled forces' non-zero entries
+__global__ void k_scatter_forces(int32_t n, const int32_t* __restrict__ idx, const double* __restrict__ val,
+                                 double* __restrict__ F) {
+  const int32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < n) F[idx[q]] = val[q];
+}
+
 // b = P F: F with the constrained DOFs zeroed
 __global__ void k_project_rhs(int64_t n, const double* __restrict__ F, const uint8_t* __restrict__ nf,
                               double* __restrict__ b) {
@@ -452,7 +460,8 @@ extern "C" int32_t mycel_problem_create(mycel_ctx* c, const mycel_grid* grid, co
   p->fixed_host.assign(fixed, fixed + n_fixed);
 
   // FeModel.AssembleForces (FeModel.cs:263-321): descriptor marshalling of the load patches, O(patch nodes).
-  p->forces_host.assign(g.nd, 0.0);
+  // per DOF the terms are added in assembly order from 0.0, as into the reference's zeroed vector
+  std::unordered_map<int64_t, double> facc;
   std::unordered_set<int32_t> seen;
   p->n_cases = std::max<int32_t>(n_loads, 0);
   p->case_terms.assign((size_t)p->n_cases, {});
@@ -482,9 +491,9 @@ extern "C" int32_t mycel_problem_create(mycel_ctx* c, const mycel_grid* grid, co
       double fx = (double)L.force[0] * inv, fy = (double)L.force[1] * inv, fz = (double)L.force[2] * inv;
       for (int32_t q = 0; q < L.n_nodes; ++q) {
         int64_t n = L.nodes[q];
-        p->forces_host[3 * n] += fx;
-        p->forces_host[3 * n + 1] += fy;
-        p->forces_host[3 * n + 2] += fz;
+        facc[3 * n] += fx;
+        facc[3 * n + 1] += fy;
+        facc[3 * n + 2] += fz;
         terms.push_back({3 * n, fx});
         terms.push_back({3 * n + 1, fy});
         terms.push_back({3 * n + 2, fz});
@@ -494,9 +503,9 @@ extern "C" int32_t mycel_problem_create(mycel_ctx* c, const mycel_grid* grid, co
       for (int32_t q = 0; q < L.n_nodes; ++q) {
         int64_t n = L.nodes[q];
         double w = L.node_area[q] * inv;
-        p->forces_host[3 * n] += (double)L.force[0] * w;
-        p->forces_host[3 * n + 1] += (double)L.force[1] * w;
-        p->forces_host[3 * n + 2] += (double)L.force[2] * w;
+        facc[3 * n] += (double)L.force[0] * w;
+        facc[3 * n + 1] += (double)L.force[1] * w;
+        facc[3 * n + 2] += (double)L.force[2] * w;
         terms.push_back({3 * n, (double)L.force[0] * w});
         terms.push_back({3 * n + 1, (double)L.force[1] * w});
         terms.push_back({3 * n + 2, (double)L.force[2] * w});
@@ -508,9 +517,12 @@ extern "C" int32_t mycel_problem_create(mycel_ctx* c, const mycel_grid* grid, co
   for (int64_t e = 0; e < g.ne; ++e)
     if (domain[e]) active.push_back((int32_t)e);
   p->n_active = (int64_t)active.size();
-  std::vector<int32_t> fnz;
-  for (int64_t i = 0; i < g.nd; ++i)
-    if (p->forces_host[i] != 0.0) fnz.push_back((int32_t)i);
+  for (const auto& kv : facc)
+    if (kv.second != 0.0) p->f_idx.push_back((int32_t)kv.first);
+  std::sort(p->f_idx.begin(), p->f_idx.end());
+  p->f_val.resize(p->f_idx.size());
+  for (size_t q = 0; q < p->f_idx.size(); ++q) p->f_val[q] = facc[p->f_idx[q]];
+  const std::vector<int32_t>& fnz = p->f_idx;
   p->n_fnz = (int32_t)fnz.size();
 
   cudaStream_t s = c->stream;
@@ -534,8 +546,14 @@ extern "C" int32_t mycel_problem_create(mycel_ctx* c, const mycel_grid* grid, co
   cudaMemsetAsync(p->d_invdf, 0, sizeof(float) * g.n32, s);  // pads of the padded FP32 layout stay zero
   cudaMemcpyAsync(p->d_domain, domain, g.ne, cudaMemcpyHostToDevice, s);
   if (p->n_active) cudaMemcpyAsync(p->d_active, active.data(), sizeof(int32_t) * p->n_active, cudaMemcpyHostToDevice, s);
-  cudaMemcpyAsync(p->d_F, p->forces_host.data(), sizeof(double) * g.nd, cudaMemcpyHostToDevice, s);
-  if (p->n_fnz) cudaMemcpyAsync(p->d_fnz, fnz.data(), sizeof(int32_t) * p->n_fnz, cudaMemcpyHostToDevice, s);
+  // F: zero, then its non-zero entries scattered (their values staged in tmp0)
+  cudaMemsetAsync(p->d_F, 0, sizeof(double) * g.nd, s);
+  if (p->n_fnz) {
+    cudaMemcpyAsync(p->d_fnz, fnz.data(), sizeof(int32_t) * p->n_fnz, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(p->d_tmp0, p->f_val.data(), sizeof(double) * p->n_fnz, cudaMemcpyHostToDevice, s);
+    k_scatter_forces<<<(unsigned)((p->n_fnz + 255) / 256), 256, 0, s>>>(p->n_fnz, p->d_fnz, p->d_tmp0, p->d_F);
+    c->launches++;
+  }
   if (n_fixed) cudaMemcpyAsync(p->d_fixed, fixed, sizeof(int32_t) * n_fixed, cudaMemcpyHostToDevice, s);
   if (density) {
     cudaMemcpyAsync(p->d_rho_box, density, sizeof(double) * g.ne, cudaMemcpyHostToDevice, s);
@@ -656,7 +674,8 @@ extern "C" int32_t mycel_problem_get_tuning(mycel_problem* p, int32_t key, int32
 extern "C" int32_t mycel_problem_forces(mycel_problem* p, double* f) {
   if (!p || !f) return set_error(p ? p->ctx : nullptr, MYCEL_E_ARG, "NULL argument");
   if (p->assemble_status) return set_error(p->ctx, p->assemble_status, p->assemble_msg);
-  std::memcpy(f, p->forces_host.data(), sizeof(double) * p->g.nd);
+  std::fill(f, f + p->g.nd, 0.0);
+  for (size_t q = 0; q < p->f_idx.size(); ++q) f[p->f_idx[q]] = p->f_val[q];
   return MYCEL_OK;
 }
 

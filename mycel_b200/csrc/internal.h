@@ -135,7 +135,8 @@ struct mycel_problem {
   std::vector<mycel_simp_session*> sessions;  // live SIMP sessions on this problem (ended by problem_destroy)
   std::vector<int32_t> fixed_host;        // FixedDofs as given (may repeat)
   std::vector<int32_t> load_nodes_host;   // union of load patch nodes (hinge shell)
-  std::vector<double> forces_host;        // AssembleForces result (box DOF vector)
+  std::vector<int32_t> f_idx;             // AssembleForces result: DOFs with a non-zero force, ascending
+  std::vector<double> f_val;              //   and their forces
   // load cases kept apart (multi-RHS solves over the shared stiffness): each case's nodal forces alone, as
   // (DOF, value) contributions in assembly order; device right-hand sides built on first use
   std::vector<std::vector<std::pair<int64_t, double>>> case_terms;
