@@ -136,3 +136,21 @@ def test_simp_separate_cases_mixed_within_tolerance(ctx, precision):
     for a, b in zip(res.snapshots, ref.snapshots):
         assert abs(a.compliance - b.compliance) <= 1e-6 * abs(b.compliance)
     assert np.abs(res.final_design_density - ref.final_design_density).max() <= 1e-4
+
+
+def test_simp_separate_cases_with_an_empty_case(oracle_cr, ctx):
+    """A load case without nodes and force adds a zero right-hand side (the solvers' zero-RHS branch): the run
+    equals the oracle's and the run without that case."""
+    from mycel_b200.model import LoadCase, SurfacePatch
+    m = _multi_case_models()[0]
+    m2 = FeModel(m.grid, m.domain, m.material, m.fixed_dofs,
+                 list(m.loads) + [LoadCase(SurfacePatch([], []), (0.0, 0.0, 0.0))])
+    o = _opts(max_iterations=3)
+    ref = oracle_cr.topopt_run(m2, o)
+    for prec in ("fp64", "mixed-mg"):
+        a = api.TopologyOptimizer.run(m, o.replace(precision=prec), ctx=ctx)
+        b = api.TopologyOptimizer.run(m2, o.replace(precision=prec), ctx=ctx)
+        assert [s.compliance for s in a.snapshots] == [s.compliance for s in b.snapshots]
+        if prec == "fp64":
+            assert [s.compliance for s in b.snapshots] == [r["compliance"] for r in ref.records]
+            assert np.array_equal(b.final_physical_density, ref.phys)

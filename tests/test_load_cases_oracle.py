@@ -92,3 +92,19 @@ def test_separate_cases_objective_decreases(oracle):
     c = [x["compliance"] for x in r.records]
     assert c[-1] < c[0]
     assert abs(r.records[-1]["volume_fraction"] - 0.4) < 1e-3
+
+
+def test_separate_cases_with_an_empty_case(oracle):
+    """A load case with no nodes and zero force (allowed by AssembleForces) adds a zero right-hand side: its
+    solve returns u = 0 and the run equals the one without it."""
+    from mycel_b200.model import LoadCase, SurfacePatch
+    m = tiny_test_model()
+    empty = LoadCase(SurfacePatch([], []), (0.0, 0.0, 0.0))
+    m2 = FeModel(m.grid, m.domain, m.material, m.fixed_dofs, list(m.loads) + [empty])
+    o = _opts(max_iterations=3, solver_tolerance_initial=1e-8, solver_tolerance_final=1e-8, separate_load_cases=True)
+    a = oracle.topopt_run(m, o)
+    b = oracle.topopt_run(m2, o)
+    assert oracle.Model(m2).load_case_count() == 3
+    assert not oracle.Model(m2).case_forces(2).any()
+    assert [x["compliance"] for x in a.records] == [x["compliance"] for x in b.records]
+    assert np.array_equal(a.phys, b.phys) and np.array_equal(a.u, b.u)
