@@ -37,9 +37,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 METRIC = "SIMP iter/s (mixed FP32-inner/FP64-refined, 192x96x96 bridge)"
 sys.path.insert(0, ROOT)
 
-# PCG iterations per SIMP iteration of the plain FP64 path on this workload (iterations 4-13, measured on B200;
-# the FP64 path reproduces the reference's iteration counts bit for bit). Used only to scale the CPU sample.
-FP64_PCG_PER_SIMP_ITER = None
+# PCG iterations per SIMP iteration of the plain FP64 path on this workload (mean of iterations 4 and 5: 2,619
+# and 2,499, measured on B200 by the default run's fp64 arm; the FP64 path reproduces the reference's iteration
+# counts). Used only to scale the CPU sample of the reference arm; the default run uses its own fp64 counts.
+FP64_PCG_PER_SIMP_ITER = {"bridge_192x96x96": 2559}
 
 # DRAM bytes per launch of the FP32 matvec (MODE 1) from one ncu capture (dram__bytes_read.sum +
 # dram__bytes_write.sum), keyed by (solver form, matvec variant, workload). Jacobi-PCG form (`--probe mixed
@@ -620,7 +621,7 @@ def run_mycel(args):
     # ---------------- CPU baseline (rank 0, bounded sample) ----------------
     if rank == 0 and not args.no_cpu:
         pcg_per_it = (statistics.mean(out["fp64"]["pcg_iters_per_step"]) if "fp64" in out else
-                      FP64_PCG_PER_SIMP_ITER or statistics.mean(pcg_inner))
+                      FP64_PCG_PER_SIMP_ITER.get(args.workload) or statistics.mean(pcg_inner))
         out["cpu_baseline"] = cpu_sample(model, opts, pcg_per_it, args.cpu_sample_iters)
 
     # ---------------- serving sample (rank 0): Poisson job stream through the serving loop ----------------
@@ -683,7 +684,7 @@ def run_reference(args):
     if rank != 0:
         return
     model, opts = workload(args.workload)
-    pcg_per_it = FP64_PCG_PER_SIMP_ITER or 1000
+    pcg_per_it = FP64_PCG_PER_SIMP_ITER.get(args.workload, 1000)
     vals = []
     for i in range(args.warmup + args.steps):
         t = time.perf_counter()
