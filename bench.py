@@ -357,7 +357,7 @@ def run_static(args):
         pr.close()
     if not args.no_cpu:
         from oracle import oracle as O
-        O.set_modes(0, 0, threads=os.cpu_count() or 1)
+        O.set_modes(0, threads=os.cpu_count() or 1)
         t0 = time.perf_counter()
         cres = O.static_run(model, 1e-8, 20000)
         out["cpu_baseline"] = {"solve_ms": (time.perf_counter() - t0) * 1000.0, "cores": os.cpu_count() or 1,
@@ -644,7 +644,7 @@ def cpu_sample(model, opts, pcg_per_simp_iter, sample_iters):
     One SIMP iteration is estimated as the non-PCG part + pcg_per_simp_iter * (time per PCG iteration)."""
     from oracle import oracle as O
     threads = os.cpu_count() or 1
-    O.set_modes(0, 0, threads=threads)
+    O.set_modes(0, threads=threads)
     m = O.Model(model)
     act = model.active_elements
     t = time.perf_counter()

@@ -175,6 +175,13 @@ int64_t mycel_ctx_launch_count(mycel_ctx* ctx);
 int32_t mycel_ctx_set_profiling(mycel_ctx* ctx, int32_t enable);
 int32_t mycel_ctx_kernel_timing(mycel_ctx* ctx, int32_t which, double* total_ms, int64_t* launches, int64_t* nodes,
                                 int64_t* active_elements);
+/* Bounded waits of the OC kernel (no counterpart in the reference, whose OC runs on the host). The OC update is
+   one persistent kernel whose blocks meet at grid barriers; each wait polls at most max_polls times (about
+   64 ns each) and then gives up, the kernel returns and the call reports MYCEL_E_TIMEOUT with the device still
+   usable. max_polls = 0 restores the default (about 1 s plus 4 polls per element). unreachable = 1 is for
+   testing that failure path: every barrier then waits for one block more than the grid holds, so each wait
+   runs out. */
+int32_t mycel_ctx_set_oc_wait(mycel_ctx* ctx, int64_t max_polls, int32_t unreachable);
 
 /* ---- problem: FeModel + FemOperator (Fem/FeModel.cs:43-184, Fem/FemOperator.cs:33-108) ----
    element_density: box-sized (default 1.0 when NULL); penal: FeModel.Penal. */
@@ -235,6 +242,12 @@ int32_t mycel_static_solve(mycel_problem* p, const mycel_static_options* opt, co
 int32_t mycel_average_element_to_node(mycel_problem* p, const double* element_scalar, int64_t len,
                                       double* nodal_out);
 
+/* Math.Pow as the kernels evaluate it (FemOperator.cs:100,133 E_e = Emin + Math.Pow(rho, p)(E0 - Emin);
+   SensitivityAnalysis.cs:93-95 p Math.Pow(rho, p - 1) dE): the host C library's pow (GNU libc 2.28+ algorithm)
+   with its rounding sequence, so the device returns the library's bits. out[i] = x[i]^y[i] (y_len == n) or
+   x[i]^y[0] (y_len == 1); host buffers. */
+int32_t mycel_pow(mycel_ctx* ctx, int64_t n, const double* x, const double* y, int64_t y_len, double* out);
+
 /* DensityFilter (Optimization/DensityFilter.cs:34-199) over the problem's active elements, radius in elements. */
 int32_t mycel_filter_create(mycel_problem* p, double rmin, mycel_filter** out);
 int32_t mycel_filter_destroy(mycel_filter* f);
@@ -257,14 +270,24 @@ int32_t mycel_oc_update(mycel_ctx* ctx, int32_t n, const double* rho, const doub
    allocate device memory when they run this step (a host whose device memory is all reserved by another
    allocator in the process, or a loop that must not take the synchronisation of a cudaMalloc/cudaFree).
    rho, dc, s, passive (may be NULL) and rho_new are device pointers owned by the caller; lambda_out is a host
-   pointer. The kernel's scratch is a fixed 65.7 KB array inside the library, held by every GPU that loads it
+   pointer. The kernel's scratch is a fixed 65.6 KB array inside the library, held by every GPU that loads it
    until the process exits, sized for 1024 persistent blocks (devices that need more return MYCEL_E_ARG).
    The first call on a device looks up that array's device address, so make it before any stream capture.
+   The work runs on the context's stream, which is not ordered after the caller's streams: the caller's writes
+   to rho, dc, s and passive must be complete (e.g. their stream synchronised) before the call. Each call
+   synchronises the context's stream to read lambda, so rho_new is ready when it returns.
    All calls share the array: calls that overlap on the GPU (other streams, other threads) race. */
 int32_t mycel_oc_update_noalloc(mycel_ctx* ctx, int32_t n, const double* rho, const double* dc, const double* s,
                                 const uint8_t* passive, double* rho_new, double target_volume_fraction,
                                 double move_limit, double rho_min, double lambda_guess, int32_t max_bisection_steps,
                                 double volume_tolerance, double* lambda_out);
+
+/* HeavisideProjection.Project / Derivative (Optimization/HeavisideProjection.cs:12-37), host arrays of n values;
+   the reference's default eta is 0.5. */
+int32_t mycel_heaviside_project(mycel_ctx* ctx, int64_t n, const double* rho_tilde, double* rho_bar, double beta,
+                                double eta);
+int32_t mycel_heaviside_derivative(mycel_ctx* ctx, int64_t n, const double* rho_tilde, double* deriv, double beta,
+                                   double eta);
 
 /* ---- SIMP loop: TopologyOptimizer.Run (Optimization/TopologyOptimizer.cs:16-407) ----
    cancel / pause: polled between iterations (CancellationToken, IterationController.CheckAndBlock);

@@ -97,6 +97,7 @@ SIGNATURES = {
     "mycel_last_error": (C.c_char_p, [P]),
     "mycel_ctx_launch_count": (i64, [P]),
     "mycel_ctx_set_profiling": (i32, [P, i32]),
+    "mycel_ctx_set_oc_wait": (i32, [P, i64, i32]),
     "mycel_ctx_kernel_timing": (i32, [P, i32, C.POINTER(dbl), C.POINTER(i64), C.POINTER(i64), C.POINTER(i64)]),
     "mycel_problem_create": (i32, [P, C.POINTER(Grid), P, C.POINTER(Material), P, i32, P, i32, P, dbl,
                                    C.POINTER(P)]),
@@ -121,7 +122,10 @@ SIGNATURES = {
     "mycel_filter_s": (i32, [P, P]),
     "mycel_sensitivities": (i32, [P, P, P, dbl, P]),
     "mycel_oc_update": (i32, [P, i32, P, P, P, P, P, dbl, dbl, dbl, dbl, i32, dbl, C.POINTER(dbl)]),
+    "mycel_pow": (i32, [P, i64, P, P, i64, P]),
     "mycel_oc_update_noalloc": (i32, [P, i32, P, P, P, P, P, dbl, dbl, dbl, dbl, i32, dbl, C.POINTER(dbl)]),
+    "mycel_heaviside_project": (i32, [P, i64, P, P, dbl, dbl]),
+    "mycel_heaviside_derivative": (i32, [P, i64, P, P, dbl, dbl]),
     "mycel_simp_run": (i32, [P, C.POINTER(SimpOptions), PROGRESS_FN, P, P, P, C.POINTER(IterRecord), i32,
                              C.POINTER(i32), C.POINTER(i32), P, P, P]),
     "mycel_simp_begin": (i32, [P, C.POINTER(SimpOptions), C.POINTER(P)]),

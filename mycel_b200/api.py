@@ -74,6 +74,11 @@ class Context:
     def set_profiling(self, on: bool = True):
         _check(L.load().mycel_ctx_set_profiling(self.handle, int(on)), self)
 
+    def set_oc_wait(self, max_polls: int = 0, unreachable: bool = False):
+        """Bounded waits of the OC kernel's grid barrier (0: default); unreachable=True makes every wait run out
+        (for testing the MYCEL_E_TIMEOUT path)."""
+        _check(L.load().mycel_ctx_set_oc_wait(self.handle, int(max_polls), int(unreachable)), self)
+
     def kernel_timing(self, which: int = 0) -> dict:
         ms, n, nodes, els = C.c_double(0), C.c_int64(0), C.c_int64(0), C.c_int64(0)
         _check(L.load().mycel_ctx_kernel_timing(self.handle, which, C.byref(ms), C.byref(n), C.byref(nodes),
@@ -279,6 +284,38 @@ def oc_update(rho, dc, s, passive, target_volume_fraction, move_limit=0.2, rho_m
                                     out.ctypes.data, target_volume_fraction, move_limit, rho_min, lambda_guess,
                                     max_bisection_steps, volume_tolerance, C.byref(lam)), ctx)
     return out, lam.value
+
+
+class HeavisideProjection:
+    """HeavisideProjection.Project / Derivative (HeavisideProjection.cs:12-37) on the device."""
+
+    @staticmethod
+    def project(rho_tilde, beta: float, eta: float = 0.5, ctx: Optional[Context] = None) -> np.ndarray:
+        ctx = ctx or default_context()
+        x = L.f64(rho_tilde).ravel()
+        out = np.empty(x.size)
+        _check(L.load().mycel_heaviside_project(ctx.handle, x.size, x.ctypes.data, out.ctypes.data, beta, eta), ctx)
+        return out
+
+    @staticmethod
+    def derivative(rho_tilde, beta: float, eta: float = 0.5, ctx: Optional[Context] = None) -> np.ndarray:
+        ctx = ctx or default_context()
+        x = L.f64(rho_tilde).ravel()
+        out = np.empty(x.size)
+        _check(L.load().mycel_heaviside_derivative(ctx.handle, x.size, x.ctypes.data, out.ctypes.data, beta, eta),
+               ctx)
+        return out
+
+
+def math_pow(x, y, ctx: Optional[Context] = None) -> np.ndarray:
+    """Math.Pow as the kernels evaluate it on the device (the host C library's pow, bit for bit):
+    x**y elementwise, y an array of x's length or a scalar."""
+    ctx = ctx or default_context()
+    x = L.f64(x).ravel()
+    y = L.f64(np.atleast_1d(y)).ravel()
+    out = np.empty(x.size)
+    _check(L.load().mycel_pow(ctx.handle, x.size, x.ctypes.data, y.ctypes.data, y.size, out.ctypes.data), ctx)
+    return out
 
 
 class StaticAnalysis:

@@ -45,7 +45,8 @@ def _stale(out: str, deps) -> bool:
 
 def build(verbose: bool = False, force: bool = False, extra=None) -> str:
     os.makedirs(BUILD, exist_ok=True)
-    headers = [os.path.join(CSRC, "internal.h"), os.path.join(HERE, "..", "include", "mycel.h")]
+    headers = [os.path.join(CSRC, h) for h in ("internal.h", "libm_pow.h", "libm_pow_tables.h")]
+    headers.append(os.path.join(HERE, "..", "include", "mycel.h"))
     objs = []
     for src, flags in UNITS:
         path = os.path.join(CSRC, src)

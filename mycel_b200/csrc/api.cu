@@ -374,6 +374,14 @@ extern "C" int32_t mycel_ctx_create(int32_t device, mycel_ctx** out) {
     return set_error(nullptr, MYCEL_E_DEVICE, m);
   }
   c->pinned_bytes = 1 << 16;
+  int oc_bpsm = 0;
+  if (oc_blocks_per_sm(&oc_bpsm) != MYCEL_OK) {
+    cudaFreeHost(c->pinned);
+    cudaStreamDestroy(c->stream);
+    delete c;
+    return set_error(nullptr, MYCEL_E_DEVICE, "occupancy query of the OC kernel failed");
+  }
+  c->oc_grid = c->num_sms * oc_bpsm;
   // Device memory freed by a problem stays in the device's stream-ordered pool for the next problem instead of
   // going back to the driver at the next synchronisation (re-mapping gigabytes for every job cost up to a few
   // hundred ms per job). A host that needs it released calls cudaMemPoolTrimTo on the default pool.
@@ -407,6 +415,13 @@ extern "C" int32_t mycel_ctx_set_profiling(mycel_ctx* c, int32_t enable) {
   if (!c) return set_error(nullptr, MYCEL_E_ARG, "NULL context");
   c->profile = enable ? 1 : 0;
   for (int k = 0; k < 4; ++k) c->prof_ms[k] = 0, c->prof_n[k] = 0, c->prof_nodes[k] = 0, c->prof_elems[k] = 0;
+  return MYCEL_OK;
+}
+
+extern "C" int32_t mycel_ctx_set_oc_wait(mycel_ctx* c, int64_t max_polls, int32_t unreachable) {
+  if (!c || max_polls < 0) return set_error(c, MYCEL_E_ARG, "invalid argument");
+  c->oc_wait_polls = max_polls;
+  c->oc_wait_unreachable = unreachable ? 1 : 0;
   return MYCEL_OK;
 }
 
@@ -1044,7 +1059,7 @@ extern "C" int32_t mycel_oc_update(mycel_ctx* c, int32_t n, const double* rho, c
   double *d_rho, *d_dc, *d_s, *d_new, *d_scr;
   uint8_t* d_pas = nullptr;
   OcOut* d_out;
-  size_t scr = (size_t)c->num_sms * 2 * 8 + 64;
+  size_t scr = oc_scratch_doubles(c->oc_grid);
   MYCEL_CUDA(c, cudaMallocAsync((void**)&d_rho, nn * 8, s));
   MYCEL_CUDA(c, cudaMallocAsync((void**)&d_dc, nn * 8, s));
   MYCEL_CUDA(c, cudaMallocAsync((void**)&d_s, nn * 8, s));
@@ -1060,7 +1075,7 @@ extern "C" int32_t mycel_oc_update(mycel_ctx* c, int32_t n, const double* rho, c
     if (passive) cudaMemcpyAsync(d_pas, passive, n, cudaMemcpyHostToDevice, s);
   }
   OcParams prm{f, move, rho_min, lambda_guess, vol_tol, max_bisect, 0};
-  int st = launch_oc(c, n, nullptr, d_rho, d_dc, d_s, d_pas, d_new, nullptr, nullptr, prm, d_scr, d_out);
+  int st = launch_oc(c, n, nullptr, d_rho, d_dc, d_s, d_pas, d_new, nullptr, nullptr, prm, d_scr, scr, d_out);
   OcOut* ho = (OcOut*)c->pinned;
   std::memset(ho, 0, sizeof(OcOut));
   if (!st) {

@@ -27,6 +27,7 @@
 #include <stdint.h>
 
 #include "internal.h"
+#include "libm_pow.h"
 
 namespace mycel {
 
@@ -44,29 +45,10 @@ __device__ __forceinline__ double lane_sum(int mode, double a0, double a1, doubl
   return (a0 + a1) + (a2 + a3);
 }
 
-// Correctly rounded x^n (n small, >= 0): exact power carried as a double-double, rounded once.
-__device__ __forceinline__ double pow_int_cr(double x, int n) {
-  if (n == 0) return 1.0;
-  if (n == 1) return x;
-  double hi = x, lo = 0.0;
-  for (int k = 1; k < n; ++k) {
-    double ph = __dmul_rn(hi, x);
-    double pl = __fma_rn(hi, x, -ph);
-    pl = __dadd_rn(pl, __dmul_rn(lo, x));
-    double s = __dadd_rn(ph, pl);
-    lo = __dsub_rn(pl, __dsub_rn(s, ph));
-    hi = s;
-  }
-  return hi;
-}
-
-// Math.Pow on the path: integer exponents (the SIMP penalty p = 1, 2, 3 and p - 1) are correctly rounded;
-// other exponents use CUDA's pow.
-__device__ __forceinline__ double path_pow(double x, double y) {
-  double r = rint(y);
-  if (r == y && r >= 0.0 && r <= 16.0 && x >= 0.0 && isfinite(x)) return pow_int_cr(x, (int)r);
-  return pow(x, y);
-}
+// Math.Pow on the path (FemOperator.cs:100,133; SensitivityAnalysis.cs:93-95): the host C library's pow,
+// restated with its rounding sequence (libm_pow.h), so E_e and dE/drho carry the reference's bits for every
+// exponent.
+__device__ __forceinline__ double path_pow(double x, double y) { return libm_pow::pow(x, y); }
 
 __device__ __forceinline__ int local_index(int ox, int oy, int oz) {
   // Hex8 local node order (Hex8Element.cs:8-16): (0,0,0),(1,0,0),(1,1,0),(0,1,0), then the same at z=1
@@ -1124,25 +1106,66 @@ void launch_sens(mycel_problem* p, const double* u, const double* rho_box, doubl
 }
 
 // ---------------------------------------------------------------------------------------------------------
+// HeavisideProjection (Optimization/HeavisideProjection.cs:12-37), an option of TopologyOptimizer.Run
+// (:192-199, :279-290): the reference's expression order, every operation rounded once (this unit is built
+// without contraction); Math.Clamp lets NaN through and Math.Max propagates it, as here. tanh is CUDA's, which
+// can differ from the C library's in the last bit.
+// ---------------------------------------------------------------------------------------------------------
+__global__ void k_heaviside(int64_t n, const int32_t* __restrict__ idx, const double* __restrict__ rt,
+                            const double* __restrict__ dcb, double* __restrict__ out, double beta, double eta,
+                            int mode) {
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int64_t e = idx ? (int64_t)idx[t] : t;
+  const double den = tanh(beta * eta) + tanh(beta * (1.0 - eta));
+  const double inv = 1.0 / den;
+  if (mode == 0) {
+    const double tbe = tanh(beta * eta);
+    const double v = (tbe + tanh(beta * (rt[e] - eta))) * inv;
+    out[e] = v < 0.0 ? 0.0 : (v > 1.0 ? 1.0 : v);  // Math.Clamp(v, 0, 1)
+    return;
+  }
+  const double th = tanh(beta * (rt[e] - eta));
+  double d = beta * (1.0 - th * th) * inv;
+  d = isnan(d) ? d : (d > 1e-12 ? d : 1e-12);  // Math.Max(d, 1e-12)
+  out[e] = mode == 1 ? dcb[e] * d : d;
+}
+
+void launch_heaviside(mycel_ctx* ctx, int64_t n, const int32_t* idx, const double* rt, const double* dcb,
+                      double* out, double beta, double eta, int mode) {
+  if (n <= 0) return;
+  k_heaviside<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(n, idx, rt, dcb, out, beta, eta, mode);
+  ctx->launches++;
+}
+
+// Math.Pow over arrays, evaluated by the kernels' own path_pow (out[i] = x[i]^y[i], or x[i]^y[0] when y_len
+// is 1): lets a host check the device's bits against its C library's pow.
+__global__ void k_pow(int64_t n, const double* __restrict__ x, const double* __restrict__ y, int y_scalar,
+                      double* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = path_pow(x[i], y[y_scalar ? 0 : i]);
+}
+
+// ---------------------------------------------------------------------------------------------------------
 // OC update: persistent cooperative kernel with a bounded grid barrier
 // ---------------------------------------------------------------------------------------------------------
-constexpr long long kBarrierSpinLimit = 1ll << 24;  // ~1 s of __nanosleep(64) polling before giving up
-
-__device__ bool grid_sync_bounded(unsigned int* bar, int* err) {
+// Every wait gives up after OcArgs::max_polls polls of __nanosleep(64) (about 1 s by default, longer for large
+// n, see launch_oc) and sets the error flag, so a grid that cannot meet ends with MYCEL_E_TIMEOUT on the host.
+__device__ bool grid_sync_bounded(unsigned int* bar, int* err, long long max_polls, unsigned int extra) {
   __syncthreads();
   if (threadIdx.x == 0) {
     volatile unsigned int* vgen = bar + 1;
     unsigned int gen = *vgen;
     __threadfence();
     unsigned int arrived = atomicAdd(bar, 1u);
-    if (arrived == gridDim.x - 1) {
+    if (arrived == gridDim.x - 1 + extra) {
       bar[0] = 0;
       __threadfence();
       atomicAdd(bar + 1, 1u);
     } else {
       long long spins = 0;
       while (*vgen == gen) {
-        if (++spins > kBarrierSpinLimit || *(volatile int*)err) {
+        if (++spins > max_polls || *(volatile int*)err) {
           atomicExch(err, 1);
           break;
         }
@@ -1203,31 +1226,54 @@ struct OcArgs {
   double* rho_new;
   const double* rho_phys;
   const double* rho_grey;
-  double* scratch;  // 2 * gridDim.x * 3 doubles
+  double* scratch;  // oc_scratch_doubles(gridDim.x) doubles, layout below
   unsigned int* bar;
   int* err;
   OcOut* out;
+  long long max_polls;    // polls of each wait before it gives up
+  unsigned int extra;     // arrivals a barrier waits for beyond the grid (0; 1 only to test the time-out path)
 };
+// scratch layout (grid = gridDim.x): [0, 4 grid) two alternating pairs of per-block partial sums (value, sum of
+// magnitudes) of the volume trials; [4 grid, 7 grid) per-block max change, volume and grey sums;
+// [7 grid, 7 grid + 4) two alternating broadcast cells of sequential sums; then the barrier words.
 
-// Grid-wide deterministic sum of per-thread values; every block returns the same total (thread 0 valid).
-__device__ double grid_total(double mine, const OcArgs& a, int slot, double* sh, bool* ok) {
-  double bs = block_sum(mine, sh);
-  double* part = a.scratch + (size_t)slot * gridDim.x;
-  if (threadIdx.x == 0) part[blockIdx.x] = bs;
-  if (!grid_sync_bounded(a.bar, a.err)) {
+// Grid-wide deterministic sums of two per-thread values; every block gets the same totals (thread 0 valid).
+__device__ void grid_total2(double m0, double m1, const OcArgs& a, int slot, double* sh, bool* ok, double* t0,
+                            double* t1) {
+  double b0 = block_sum(m0, sh);
+  double b1 = block_sum(m1, sh);
+  double* part = a.scratch + (size_t)slot * 2 * gridDim.x;
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = b0;
+    part[gridDim.x + blockIdx.x] = b1;
+  }
+  if (!grid_sync_bounded(a.bar, a.err, a.max_polls, a.extra)) {
     *ok = false;
-    return 0.0;
+    return;
   }
   // warp 0 adds the block partials: lane l takes blocks l, l + 32, ... in order, then a fixed shuffle tree
-  // (the same order in every block, so every block gets the same bits; one load round instead of gridDim.x
-  // dependent loads)
-  double t = 0.0;
+  // (the same order in every block, so every block gets the same bits)
+  double s0 = 0.0, s1 = 0.0;
   if (threadIdx.x < 32) {
-    for (unsigned k = threadIdx.x; k < gridDim.x; k += 32) t = t + ld_volatile(part + k);
-    for (int o = 16; o > 0; o >>= 1) t = t + __shfl_xor_sync(0xffffffffu, t, o);
+    for (unsigned k = threadIdx.x; k < gridDim.x; k += 32) {
+      s0 = s0 + ld_volatile(part + k);
+      s1 = s1 + ld_volatile(part + gridDim.x + k);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      s0 = s0 + __shfl_xor_sync(0xffffffffu, s0, o);
+      s1 = s1 + __shfl_xor_sync(0xffffffffu, s1, o);
+    }
   }
-  return t;
+  *t0 = s0;
+  *t1 = s1;
 }
+
+// A volume V(lambda) of the bisection: the grid's tree sum, with an error bound against any other order of the
+// same terms, or (exact) the sum in the reference's element order.
+struct OcVol {
+  double v, bound;
+  bool exact;
+};
 
 __global__ void __launch_bounds__(256) k_oc(OcArgs a, OcParams prm) {
   __shared__ double sh[32];
@@ -1235,13 +1281,41 @@ __global__ void __launch_bounds__(256) k_oc(OcArgs a, OcParams prm) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   const int64_t t0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   bool ok = true;
-  int slot = 0;
+  int slot = 0, cell = 0;
   auto element = [&](int64_t i) -> int64_t { return a.idx ? (int64_t)a.idx[i] : i; };
-  auto volume = [&](double lam) -> double {
+  auto term = [&](int64_t e, double lam) -> double {
+    const double si = a.s[e];
+    return si * ((a.pas && a.pas[e]) ? 1.0 : oc_new_rho(a.rho[e], a.dc[e], si, false, lam, prm.move, prm.rho_min));
+  };
+  // Sum of f(i) over i = 0 .. n-1 in that order (the reference's sequential loops), by warp 0 of block 0: its
+  // lanes evaluate 32 consecutive terms, then every lane adds them one by one in index order. The other blocks
+  // wait at the grid barrier; the result is broadcast through a scratch cell.
+  auto sequential_sum = [&](auto f) -> double {
+    double* c = a.scratch + (size_t)7 * gridDim.x + 2 * cell;
+    cell ^= 1;
+    if (blockIdx.x == 0 && threadIdx.x < 32) {
+      double acc = 0.0;
+      for (int64_t base = 0; base < a.n; base += 32) {
+        const int64_t i = base + threadIdx.x;
+        const double t = i < a.n ? f(i) : 0.0;
+        const int cnt = (int)min((int64_t)32, a.n - base);
+        for (int k = 0; k < cnt; ++k) acc = acc + __shfl_sync(0xffffffffu, t, k);
+      }
+      if (threadIdx.x == 0) *(volatile double*)c = acc;
+    }
+    if (!grid_sync_bounded(a.bar, a.err, a.max_polls, a.extra)) {
+      ok = false;
+      return 0.0;
+    }
+    return ld_volatile(c);
+  };
+  // tree depth of a grid total: the per-thread chain, the warp and block steps, the lane-strided block partials
+  const double depth = (double)((a.n + stride - 1) / stride) + 5.0 + 8.0 + (double)((gridDim.x + 31) / 32) + 5.0;
+  auto volume = [&](double lam) -> OcVol {
     // the thread's elements t0, t0 + stride, ... summed in that order; the loads of 8 of them are issued before
     // their terms are added, so the index -> data load chains overlap
     constexpr int kB = 8;
-    double v = 0.0;
+    double v = 0.0, va = 0.0;
     for (int64_t base = t0; base < a.n; base += kB * stride) {
       double si[kB], rr[kB], dd[kB];
       bool pp[kB];
@@ -1256,25 +1330,73 @@ __global__ void __launch_bounds__(256) k_oc(OcArgs a, OcParams prm) {
       }
 #pragma unroll
       for (int k = 0; k < kB; ++k)
-        if (base + k * stride < a.n)
-          v = v + si[k] * (pp[k] ? 1.0 : oc_new_rho(rr[k], dd[k], si[k], false, lam, prm.move, prm.rho_min));
+        if (base + k * stride < a.n) {
+          const double t = si[k] * (pp[k] ? 1.0 : oc_new_rho(rr[k], dd[k], si[k], false, lam, prm.move, prm.rho_min));
+          v = v + t;
+          va = va + fabs(t);
+        }
     }
-    double tot = grid_total(v, a, slot, sh, &ok);
+    double tv = 0.0, ta = 0.0;
+    grid_total2(v, va, a, slot, sh, &ok, &tv, &ta);
     slot ^= 1;
-    if (threadIdx.x == 0) bc[0] = tot;
+    if (threadIdx.x == 0) {
+      bc[0] = tv;
+      bc[1] = ta;
+    }
     __syncthreads();
-    return bc[0];
+    OcVol r;
+    r.v = bc[0];
+    // |tree - exact| <= gamma_depth sum|t| and |sequential - exact| <= gamma_(n-1) sum|t|, gamma_k = k u / (1 - k u);
+    // doubled for the rounding of the computed sum of magnitudes and of the bound itself
+    r.bound = 2.0 * ((double)a.n + depth) * 0x1p-53 * bc[1] * 1.0000001;
+    r.exact = false;
+    __syncthreads();
+    return r;
   };
-  // total S (OcOptimizer.cs:177-182)
-  double sv = 0.0;
-  for (int64_t i = t0; i < a.n; i += stride) sv = sv + a.s[element(i)];
-  double ts = grid_total(sv, a, slot, sh, &ok);
-  slot ^= 1;
-  if (threadIdx.x == 0) bc[0] = ts;
-  __syncthreads();
-  ts = bc[0];
+  // the volume at lam in the reference's order, when a decision needs it
+  auto make_exact = [&](OcVol& x, double lam) {
+    if (x.exact) return;
+    x.v = sequential_sum([&](int64_t i) { return term(element(i), lam); });
+    x.bound = 0.0;
+    x.exact = true;
+  };
+  // total S (OcOptimizer.cs:28-33): sequential in element order, or the value the caller has cached
+  double ts;
+  if (prm.total_s >= 0.0) {
+    ts = prm.total_s;
+  } else if (prm.exact) {
+    ts = sequential_sum([&](int64_t i) { return a.s[element(i)]; });
+  } else {
+    double sv = 0.0;
+    for (int64_t i = t0; i < a.n; i += stride) sv = sv + a.s[element(i)];
+    double t1 = 0.0;
+    grid_total2(sv, 0.0, a, slot, sh, &ok, &ts, &t1);
+    slot ^= 1;
+    if (threadIdx.x == 0) bc[0] = ts;
+    __syncthreads();
+    ts = bc[0];
+    __syncthreads();
+  }
   if (!ok) return;
   const double tv = prm.f * ts;
+  // the comparisons of the reference (v < target, v > target, relErr <= tolerance) taken on the tree sum unless
+  // it is within its error bound of the threshold; then on the sequential sum (exact mode)
+  auto less_than_target = [&](OcVol& x, double lam) -> bool {
+    if (prm.exact && !x.exact && fabs(x.v - tv) <= x.bound) make_exact(x, lam);
+    return x.v < tv;
+  };
+  auto greater_than_target = [&](OcVol& x, double lam) -> bool {
+    if (prm.exact && !x.exact && fabs(x.v - tv) <= x.bound) make_exact(x, lam);
+    return x.v > tv;
+  };
+  const double denom = maxd(tv, 1e-12);
+  auto within_tolerance = [&](OcVol& x, double lam) -> bool {
+    if (prm.exact && !x.exact) {
+      const double d = fabs(x.v - tv), lim = prm.vol_tol * denom;
+      if (fabs(d - lim) <= x.bound + 0x1p-50 * (d + lim)) make_exact(x, lam);
+    }
+    return fabs(x.v - tv) / denom <= prm.vol_tol;
+  };
   const double lg = prm.lambda_guess;
   bool gok = lg > 0.0 && !isinf(lg) && !isnan(lg);
   double l1 = gok ? lg * 0.5 : 1e-12;
@@ -1282,12 +1404,13 @@ __global__ void __launch_bounds__(256) k_oc(OcArgs a, OcParams prm) {
   if (l1 <= 1e-50) l1 = 1e-12;
   if (l2 <= l1) l2 = l1 * 10.0;
   int trials = 0;
-  double v1 = volume(l1);
-  double v2 = volume(l2);
+  OcVol v1 = volume(l1);
+  OcVol v2 = volume(l2);
   trials += 2;
   if (!ok) return;
   int ex = 0;
-  while (v1 < tv && l1 > 1e-50 && ex++ < 50) {
+  while (less_than_target(v1, l1) && l1 > 1e-50 && ex++ < 50) {
+    if (!ok) return;
     l2 = l1;
     v2 = v1;
     l1 *= 0.1;
@@ -1295,8 +1418,10 @@ __global__ void __launch_bounds__(256) k_oc(OcArgs a, OcParams prm) {
     ++trials;
     if (!ok) return;
   }
+  if (!ok) return;
   ex = 0;
-  while (v2 > tv && l2 < 1e50 && ex++ < 50) {
+  while (greater_than_target(v2, l2) && l2 < 1e50 && ex++ < 50) {
+    if (!ok) return;
     l1 = l2;
     v1 = v2;
     l2 *= 10.0;
@@ -1304,15 +1429,19 @@ __global__ void __launch_bounds__(256) k_oc(OcArgs a, OcParams prm) {
     ++trials;
     if (!ok) return;
   }
+  if (!ok) return;
   double lm = sqrt(l1 * l2);
   for (int st = 0; st < prm.max_bisect; ++st) {
     lm = sqrt(l1 * l2);
-    double vm = volume(lm);
+    OcVol vm = volume(lm);
     ++trials;
     if (!ok) return;
-    double re = fabs(vm - tv) / maxd(tv, 1e-12);
-    if (re <= prm.vol_tol) break;
-    if (vm > tv) l1 = lm;
+    const bool done = within_tolerance(vm, lm);
+    if (!ok) return;
+    if (done) break;
+    const bool high = greater_than_target(vm, lm);
+    if (!ok) return;
+    if (high) l1 = lm;
     else l2 = lm;
     if (fabs(l2 - l1) <= 1e-15 * lm) break;
   }
@@ -1326,7 +1455,7 @@ __global__ void __launch_bounds__(256) k_oc(OcArgs a, OcParams prm) {
     a.rho_new[e] = nr;
     double d = fabs(nr - r);
     if (d > mc) mc = d;
-    if (a.rho_phys) {
+    if (a.rho_phys && !prm.exact) {
       vs = vs + a.rho_phys[e];
       double rb = a.rho_grey[e];
       gs = gs + rb * (1.0 - rb);
@@ -1343,7 +1472,7 @@ __global__ void __launch_bounds__(256) k_oc(OcArgs a, OcParams prm) {
     for (int k = 0; k < (int)(blockDim.x >> 5); ++k)
       if (sh[k] > mc) mc = sh[k];
   }
-  double* part = a.scratch + (size_t)2 * 2 * gridDim.x;  // slots 4..6
+  double* part = a.scratch + (size_t)4 * gridDim.x;
   double bvs = block_sum(vs, sh);
   double bgs = block_sum(gs, sh);
   if (threadIdx.x == 0) {
@@ -1351,7 +1480,17 @@ __global__ void __launch_bounds__(256) k_oc(OcArgs a, OcParams prm) {
     part[gridDim.x + blockIdx.x] = bvs;
     part[2 * gridDim.x + blockIdx.x] = bgs;
   }
-  if (!grid_sync_bounded(a.bar, a.err)) return;
+  if (!grid_sync_bounded(a.bar, a.err, a.max_polls, a.extra)) return;
+  // exact mode: the volume and grey sums in the reference's element order (:328-335)
+  double svol = 0.0, sgrey = 0.0;
+  if (prm.exact && a.rho_phys) {
+    svol = sequential_sum([&](int64_t i) { return a.rho_phys[element(i)]; });
+    sgrey = sequential_sum([&](int64_t i) {
+      const double rb = a.rho_grey[element(i)];
+      return rb * (1.0 - rb);
+    });
+    if (!ok) return;
+  }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     double m = 0.0, v = 0.0, gg = 0.0;
     for (unsigned k = 0; k < gridDim.x; ++k) {
@@ -1362,29 +1501,36 @@ __global__ void __launch_bounds__(256) k_oc(OcArgs a, OcParams prm) {
     }
     a.out->lambda = lm;
     a.out->max_change = m;
-    a.out->vol_sum = v;
-    a.out->grey_sum = gg;
+    a.out->vol_sum = prm.exact ? svol : v;
+    a.out->grey_sum = prm.exact ? sgrey : gg;
+    a.out->total_s = ts;
     a.out->err = 0;
     a.out->trials = trials;
   }
 }
 
+int oc_blocks_per_sm(int* out) {
+  int b = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_oc, 256, 0);
+  if (e != cudaSuccess) return MYCEL_E_DEVICE;
+  *out = std::max(1, std::min(b, 2));
+  return MYCEL_OK;
+}
+
 int launch_oc(mycel_ctx* ctx, int64_t n, const int32_t* d_index, const double* rho, const double* dc, const double* s,
               const uint8_t* passive, double* rho_new, const double* rho_phys_for_metrics,
-              const double* rho_tilde_for_grey, const OcParams& prm, double* d_scratch, OcOut* d_out) {
-  static int blocks_per_sm = -1;
-  if (blocks_per_sm < 0) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_oc, 256, 0);
-    if (blocks_per_sm < 1) blocks_per_sm = 1;
-    if (blocks_per_sm > 2) blocks_per_sm = 2;
-  }
-  int grid = ctx->num_sms * blocks_per_sm;
-  // scratch layout: [7 * grid] doubles of partials, then barrier words + error flag
-  unsigned int* bar = (unsigned int*)(d_scratch + 8 * grid);
+              const double* rho_tilde_for_grey, const OcParams& prm, double* d_scratch, size_t scratch_doubles,
+              OcOut* d_out) {
+  const int grid = ctx->oc_grid;  // fixed when the context was created
+  if (grid < 1 || oc_scratch_doubles(grid) > scratch_doubles) return MYCEL_E_ARG;
+  unsigned int* bar = (unsigned int*)(d_scratch + 7 * (size_t)grid + 4);
   int* err = (int*)(bar + 4);
-  cudaMemsetAsync(bar, 0, 8 * sizeof(unsigned int), ctx->stream);
+  if (cudaMemsetAsync(bar, 0, 8 * sizeof(unsigned int), ctx->stream) != cudaSuccess) return MYCEL_E_DEVICE;
+  // each wait: about 1 s of polling, plus room for the sequential sums of the exact mode (about 20 ns per term)
+  long long polls = ctx->oc_wait_polls > 0 ? ctx->oc_wait_polls : (1ll << 24) + 4 * (long long)n;
   OcArgs a{n, d_index, rho, dc, s, passive, rho_new, rho_phys_for_metrics,
-           rho_tilde_for_grey ? rho_tilde_for_grey : rho_phys_for_metrics, d_scratch, bar, err, d_out};
+           rho_tilde_for_grey ? rho_tilde_for_grey : rho_phys_for_metrics, d_scratch, bar, err, d_out,
+           polls, ctx->oc_wait_unreachable ? 1u : 0u};
   OcParams pp = prm;
   void* args[] = {&a, &pp};
   cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_oc, dim3(grid), dim3(256), args, 0, ctx->stream);
@@ -1439,12 +1585,8 @@ extern "C" int32_t mycel_oc_update_noalloc(mycel_ctx* ctx, int32_t n, const doub
     }
     base = g_oc_noalloc_addr[ctx->device];
   }
-  int blocks_per_sm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_oc, 256, 0);
-  if (e != cudaSuccess) return set_error(ctx, MYCEL_E_DEVICE, std::string("occupancy query: ") + cudaGetErrorString(e));
-  blocks_per_sm = std::max(1, std::min(blocks_per_sm, 2));
-  const int grid = ctx->num_sms * blocks_per_sm;  // the grid launch_oc uses
-  if (grid > kOcNoAllocMaxBlocks)
+  const int grid = ctx->oc_grid;  // the grid launch_oc uses, fixed when the context was created
+  if (oc_scratch_doubles(grid) > (size_t)kOcNoAllocScratch)
     return set_error(ctx, MYCEL_E_ARG, "OC without allocation: this device needs " + std::to_string(grid) +
                                            " persistent blocks, the static scratch holds " +
                                            std::to_string(kOcNoAllocMaxBlocks));
@@ -1454,7 +1596,8 @@ extern "C" int32_t mycel_oc_update_noalloc(mycel_ctx* ctx, int32_t n, const doub
   e = cudaMemsetAsync(out, 0, sizeof(OcOut), ctx->stream);
   if (e != cudaSuccess) return set_error(ctx, MYCEL_E_DEVICE, std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));
   OcParams prm{target_volume_fraction, move_limit, rho_min, lambda_guess, volume_tolerance, max_bisection_steps, 0};
-  if (launch_oc(ctx, n, nullptr, rho, dc, s, passive, rho_new, nullptr, nullptr, prm, scratch, out))
+  if (launch_oc(ctx, n, nullptr, rho, dc, s, passive, rho_new, nullptr, nullptr, prm, scratch, kOcNoAllocScratch,
+                out))
     return set_error(ctx, MYCEL_E_DEVICE, std::string("OC kernel launch: ") + cudaGetErrorString(cudaGetLastError()));
   OcOut* h = reinterpret_cast<OcOut*>(ctx->pinned);
   e = cudaMemcpyAsync(h, out, sizeof(OcOut), cudaMemcpyDeviceToHost, ctx->stream);
@@ -1463,4 +1606,69 @@ extern "C" int32_t mycel_oc_update_noalloc(mycel_ctx* ctx, int32_t n, const doub
   if (h->trials == 0) return set_error(ctx, MYCEL_E_TIMEOUT, "OC grid barrier timed out");
   *lambda_out = h->lambda;
   return MYCEL_OK;
+}
+
+extern "C" int32_t mycel_pow(mycel_ctx* ctx, int64_t n, const double* x, const double* y, int64_t y_len,
+                             double* out) {
+  using namespace mycel;
+  if (!ctx) return set_error(nullptr, MYCEL_E_ARG, "NULL context");
+  if (n < 0 || (n > 0 && (!x || !y || !out)) || (n > 0 && y_len != 1 && y_len != n))
+    return set_error(ctx, MYCEL_E_ARG, "pow: x and out need n values, y 1 or n");
+  if (n == 0) return MYCEL_OK;
+  MYCEL_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  double *dx = nullptr, *dy = nullptr, *dout = nullptr;
+  MYCEL_CUDA(ctx, cudaMallocAsync((void**)&dx, sizeof(double) * n, st));
+  MYCEL_CUDA(ctx, cudaMallocAsync((void**)&dy, sizeof(double) * y_len, st));
+  MYCEL_CUDA(ctx, cudaMallocAsync((void**)&dout, sizeof(double) * n, st));
+  cudaError_t e = cudaMemcpyAsync(dx, x, sizeof(double) * n, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dy, y, sizeof(double) * y_len, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) {
+    const int blocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)ctx->num_sms * 8);
+    k_pow<<<blocks, 256, 0, st>>>(n, dx, dy, y_len == 1 ? 1 : 0, dout);
+    ctx->launches++;
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, dout, sizeof(double) * n, cudaMemcpyDeviceToHost, st);
+  cudaFreeAsync(dx, st);
+  cudaFreeAsync(dy, st);
+  cudaFreeAsync(dout, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return set_error(ctx, MYCEL_E_DEVICE, std::string("pow: ") + cudaGetErrorString(e));
+  return MYCEL_OK;
+}
+
+// HeavisideProjection.Project / Derivative over host arrays (kernel-level entry points).
+static int32_t heaviside_entry(mycel_ctx* ctx, int64_t n, const double* rt, double* out, double beta, double eta,
+                               int mode) {
+  using namespace mycel;
+  if (!ctx) return set_error(nullptr, MYCEL_E_ARG, "NULL context");
+  if (n < 0 || (n > 0 && (!rt || !out))) return set_error(ctx, MYCEL_E_ARG, "NULL argument");
+  if (n == 0) return MYCEL_OK;
+  MYCEL_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  double *din = nullptr, *dout = nullptr;
+  MYCEL_CUDA(ctx, cudaMallocAsync((void**)&din, sizeof(double) * n, st));
+  MYCEL_CUDA(ctx, cudaMallocAsync((void**)&dout, sizeof(double) * n, st));
+  cudaError_t e = cudaMemcpyAsync(din, rt, sizeof(double) * n, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) {
+    launch_heaviside(ctx, n, nullptr, din, nullptr, dout, beta, eta, mode);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, dout, sizeof(double) * n, cudaMemcpyDeviceToHost, st);
+  cudaFreeAsync(din, st);
+  cudaFreeAsync(dout, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return set_error(ctx, MYCEL_E_DEVICE, std::string("Heaviside: ") + cudaGetErrorString(e));
+  return MYCEL_OK;
+}
+
+extern "C" int32_t mycel_heaviside_project(mycel_ctx* ctx, int64_t n, const double* rho_tilde, double* rho_bar,
+                                           double beta, double eta) {
+  return heaviside_entry(ctx, n, rho_tilde, rho_bar, beta, eta, 0);
+}
+
+extern "C" int32_t mycel_heaviside_derivative(mycel_ctx* ctx, int64_t n, const double* rho_tilde, double* deriv,
+                                              double beta, double eta) {
+  return heaviside_entry(ctx, n, rho_tilde, deriv, beta, eta, 2);
 }

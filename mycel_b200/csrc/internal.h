@@ -100,6 +100,9 @@ struct mycel_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   int num_sms = 148;
+  int oc_grid = 0;                  // blocks of the persistent OC kernel: num_sms x oc_blocks_per_sm(), set at creation
+  int64_t oc_wait_polls = 0;        // polls of each OC grid-barrier wait before it gives up (0: the default)
+  int oc_wait_unreachable = 0;      // test switch: the OC barrier waits for one block more than the grid holds
   int64_t launches = 0;
   std::string last_error;
   void* pinned = nullptr;  // small pinned scratch for scalar readbacks
@@ -264,6 +267,11 @@ struct OcParams {
   double f, move, rho_min, lambda_guess, vol_tol;
   int max_bisect;
   int heaviside;
+  // 1: every decision of the bisection is the one the reference's sequential sums give (the tree sums are used
+  // where they are farther from the threshold than their error bound, the sequential sum otherwise), and the
+  // total S and the volume and grey metrics are summed in element order. 0: tree sums throughout.
+  int exact = 1;
+  double total_s = -1.0;  // >= 0: sum of S in element order, known from an earlier call; < 0: computed here
 };
 struct OcOut {
   double lambda;
@@ -271,12 +279,22 @@ struct OcOut {
   double vol_sum;
   double grey_sum;
   int err;
-  int trials;
+  int trials;  // volume evaluations; 0 when a grid barrier timed out
+  double total_s;
 };
+// HeavisideProjection (HeavisideProjection.cs:12-37) over the elements idx[0..n) (all n when idx is null):
+// mode 0 out = Project(rt); mode 1 out = dcb * Derivative(rt) (TopologyOptimizer.cs:283-287); mode 2
+// out = Derivative(rt).
+void launch_heaviside(mycel_ctx* ctx, int64_t n, const int32_t* idx, const double* rt, const double* dcb,
+                      double* out, double beta, double eta, int mode);
+// Blocks of the persistent OC kernel per SM on the current device (occupancy, clamped to [1, 2]).
+int oc_blocks_per_sm(int* out);
+// Scratch the OC kernel needs for a grid of `grid` blocks: partial sums, broadcast cells, barrier words.
+inline size_t oc_scratch_doubles(int grid) { return (size_t)7 * grid + 4 + 4; }
 int launch_oc(mycel_ctx* ctx, int64_t n, const int32_t* d_index /*box index of element i or null*/,
               const double* rho, const double* dc, const double* s, const uint8_t* passive, double* rho_new,
               const double* rho_phys_for_metrics, const double* rho_tilde_for_grey, const OcParams& prm,
-              double* d_scratch, OcOut* d_out);
+              double* d_scratch, size_t scratch_doubles, OcOut* d_out);
 
 // ---- mixed form (fp32_kernels.cu) ----
 void launch_E_to_f32(mycel_problem* p);

@@ -33,6 +33,7 @@ struct mycel_simp_session {
   double* d_uc = nullptr;      // [ncase * nd] each case's displacements (its warm start)
   int iter = 1, start = 1, maxit = 200;
   double lambda = 1.0, max_change = 1.0, beta = 1.0;
+  double total_s = -1.0;       // sum of the filter's S over the active elements (fixed per filter), once known
   std::deque<double> chist;
   bool converged = false, done = false;
   int count = 0;
@@ -49,33 +50,6 @@ struct mycel_simp_session {
 };
 
 namespace {
-
-__global__ void k_heaviside_project(int64_t na, const int32_t* __restrict__ act, const double* __restrict__ rt,
-                                    double* __restrict__ rb, double beta, double eta) {
-  // HeavisideProjection.Project (HeavisideProjection.cs:12-24)
-  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (t >= na) return;
-  int32_t e = act[t];
-  double den = tanh(beta * eta) + tanh(beta * (1.0 - eta));
-  double inv = 1.0 / den;
-  double tbe = tanh(beta * eta);
-  double v = (tbe + tanh(beta * (rt[e] - eta))) * inv;
-  rb[e] = v < 0.0 ? 0.0 : (v > 1.0 ? 1.0 : v);
-}
-
-__global__ void k_heaviside_chain(int64_t na, const int32_t* __restrict__ act, const double* __restrict__ rt,
-                                  const double* __restrict__ dcb, double* __restrict__ dct, double beta, double eta) {
-  // HeavisideProjection.Derivative (:26-37) times dc/drhoBar (TopologyOptimizer.cs:283-287)
-  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (t >= na) return;
-  int32_t e = act[t];
-  double den = tanh(beta * eta) + tanh(beta * (1.0 - eta));
-  double inv = 1.0 / den;
-  double th = tanh(beta * (rt[e] - eta));
-  double d = beta * (1.0 - th * th) * inv;
-  d = d > 1e-12 ? d : 1e-12;
-  dct[e] = dcb[e] * d;
-}
 
 // RunWriter's 8-bit quantisation (Persistence/RunWriter.cs:211-217): round(clamp(v, 0, 1) * 255f), half away
 // from zero, in FP32
@@ -215,7 +189,7 @@ extern "C" int32_t mycel_simp_begin(mycel_problem* p, const mycel_simp_options* 
   bool ok = !salloc(s, &s->d_rho, g.ne) && !salloc(s, &s->d_rho_new, g.ne) && !salloc(s, &s->d_rt, g.ne) &&
             !salloc(s, &s->d_dcb, g.ne) && !salloc(s, &s->d_dc, g.ne) && !salloc(s, &s->d_u, g.nd) &&
             !salloc(s, &s->d_scal, 16 + (s->ncase > 1 ? s->ncase : 0)) &&
-            !salloc(s, &s->d_oc_scr, (size_t)c->num_sms * 2 * 8 + 64) &&
+            !salloc(s, &s->d_oc_scr, oc_scratch_doubles(c->oc_grid)) &&
             !salloc(s, &s->d_oc, 1) && !salloc(s, &s->d_pas, g.ne) && !salloc(s, &s->d_phys_f, g.ne) &&
             !salloc(s, &s->d_des_f, g.ne);
   if (ok && o.enable_heaviside) ok = !salloc(s, &s->d_rb, g.ne) && !salloc(s, &s->d_dct, g.ne);
@@ -282,9 +256,7 @@ static int32_t simp_step_impl(mycel_simp_session* s, mycel_iter_record* rec, int
   // 2. filter (:191-202); passive elements are kept at 1 by the OC kernel and the initial design
   launch_filter_fwd(s->filt, s->d_rho, s->d_rt);
   if (o.enable_heaviside) {
-    k_heaviside_project<<<(unsigned)((p->n_active + 255) / 256), 256, 0, st>>>(p->n_active, p->d_active, s->d_rt,
-                                                                              s->d_rb, s->beta, 0.5);
-    c->launches++;
+    launch_heaviside(c, p->n_active, p->d_active, s->d_rt, nullptr, s->d_rb, s->beta, 0.5, 0);
   }
   cudaEventRecord(s->ev[1], st);
   // E_e and DiagA from the physical densities (:204-209)
@@ -354,18 +326,20 @@ static int32_t simp_step_impl(mycel_simp_session* s, mycel_iter_record* rec, int
     c->launches += s->ncase;
   }
   if (o.enable_heaviside) {
-    k_heaviside_chain<<<(unsigned)((p->n_active + 255) / 256), 256, 0, st>>>(p->n_active, p->d_active, s->d_rt,
-                                                                            s->d_dcb, s->d_dct, s->beta, 0.5);
-    c->launches++;
+    launch_heaviside(c, p->n_active, p->d_active, s->d_rt, s->d_dcb, s->d_dct, s->beta, 0.5, 1);
     launch_filter_adj(s->filt, s->d_dct, s->d_dc);
   } else {
     launch_filter_adj(s->filt, s->d_dcb, s->d_dc);
   }
   cudaEventRecord(s->ev[3], st);
   // 6. OC update with lambda carried over (:296-311) + metrics (:322-338)
+  // the plain method takes every bisection decision as the reference's sequential sums do; the other forms
+  // (not bit-exact anyway) decide on the grid's tree sums
   OcParams prm{o.volume_fraction, o.move_limit, o.rho_min, s->lambda, 1e-8, 60, o.enable_heaviside};
+  prm.exact = o.precision == MYCEL_PRECISION_FP64 ? 1 : 0;
+  prm.total_s = s->total_s;
   rc = launch_oc(c, p->n_active, p->d_active, s->d_rho, s->d_dc, s->filt->d_s, s->d_pas, s->d_rho_new, s->d_rb,
-                 o.enable_heaviside ? s->d_rt : s->d_rb, prm, s->d_oc_scr, s->d_oc);
+                 o.enable_heaviside ? s->d_rt : s->d_rb, prm, s->d_oc_scr, oc_scratch_doubles(c->oc_grid), s->d_oc);
   if (rc) return set_error(c, rc, "OC kernel launch failed");
   cudaEventRecord(s->ev[4], st);
   double* hsc = (double*)c->pinned;
@@ -376,6 +350,7 @@ static int32_t simp_step_impl(mycel_simp_session* s, mycel_iter_record* rec, int
   if (ho->trials == 0) return set_error(c, MYCEL_E_TIMEOUT, "OC grid barrier timed out");
   std::swap(s->d_rho, s->d_rho_new);
   s->lambda = ho->lambda;
+  s->total_s = ho->total_s;
   if (o.enable_heaviside && iter % 25 == 0 && s->beta < 8.0) s->beta = std::min(8.0, s->beta * 2.0);
   s->max_change = ho->max_change;
   double na = (double)p->n_active;

@@ -17,7 +17,6 @@
 namespace {
 
 int g_lane_mode = 0;
-int g_pow_mode = 0;
 
 void set_msg(char* msg, int len, const char* s) {
   if (msg && len > 0) {
@@ -34,30 +33,11 @@ inline double lane_sum(const double a[4]) {
   }
 }
 
-// Correctly rounded x^n for a small non-negative integer n: the exact power is carried as a double-double
-// (error-free products by fma) and rounded once. Same algorithm as the device code.
-double pow_int_cr(double x, int n) {
-  if (n == 0) return 1.0;
-  if (n == 1) return x;
-  double hi = x, lo = 0.0;
-  for (int k = 1; k < n; ++k) {
-    double ph = hi * x;
-    double pl = std::fma(hi, x, -ph);
-    pl = pl + lo * x;
-    hi = ph + pl;
-    lo = pl - (hi - ph);
-  }
-  return hi;
-}
-
-// Math.Pow as used on the path (E_e = Emin + rho^p (E0-Emin), dE/drho = p rho^(p-1) dE).
-double mpow(double x, double y) {
-  if (g_pow_mode == 1) {
-    double r = std::nearbyint(y);
-    if (r == y && r >= 0.0 && r <= 16.0 && x >= 0.0 && std::isfinite(x)) return pow_int_cr(x, (int)r);
-  }
-  return std::pow(x, y);
-}
+// Math.Pow as used on the path (E_e = Emin + rho^p (E0-Emin), dE/drho = p rho^(p-1) dE): .NET on Linux calls
+// the C runtime's pow. Called through a volatile pointer so the compiler cannot replace a call whose exponent
+// it can see (pow(x, 2.0) -> x * x) by its own arithmetic.
+double (*volatile g_libm_pow)(double, double) = ::pow;
+double mpow(double x, double y) { return g_libm_pow(x, y); }
 
 }  // namespace
 
@@ -990,37 +970,47 @@ double eval_volume(const double* rho, const double* dc, const double* s, const u
 }
 }  // namespace
 
-extern "C" double orc_oc_update(const double* rho, const double* dc, const double* s, const uint8_t* pas,
-                                double* rho_new, int32_t n, double f, double move, double rmin, double lg,
-                                int32_t maxb, double voltol) {
+namespace {
+// OcOptimizer.Update; trace (optional) records each volume evaluation's lambda and V(lambda) in order.
+double oc_update_impl(const double* rho, const double* dc, const double* s, const uint8_t* pas, double* rho_new,
+                      int32_t n, double f, double move, double rmin, double lg, int32_t maxb, double voltol,
+                      std::vector<double>* trace) {
   double ts = 0.0;
   for (int32_t i = 0; i < n; ++i) ts += s[i];
   double tv = f * ts;
+  auto vol = [&](double lam) {
+    double v = eval_volume(rho, dc, s, pas, n, lam, move, rmin);
+    if (trace) {
+      trace->push_back(lam);
+      trace->push_back(v);
+    }
+    return v;
+  };
   bool ok = lg > 0.0 && !std::isinf(lg) && !std::isnan(lg);
   double l1 = ok ? lg * 0.5 : 1e-12;
   double l2 = ok ? lg * 2.0 : 1e12;
   if (l1 <= 1e-50) l1 = 1e-12;
   if (l2 <= l1) l2 = l1 * 10.0;
-  double v1 = eval_volume(rho, dc, s, pas, n, l1, move, rmin);
-  double v2 = eval_volume(rho, dc, s, pas, n, l2, move, rmin);
+  double v1 = vol(l1);
+  double v2 = vol(l2);
   int ex = 0;
   while (v1 < tv && l1 > 1e-50 && ex++ < 50) {
     l2 = l1;
     v2 = v1;
     l1 *= 0.1;
-    v1 = eval_volume(rho, dc, s, pas, n, l1, move, rmin);
+    v1 = vol(l1);
   }
   ex = 0;
   while (v2 > tv && l2 < 1e50 && ex++ < 50) {
     l1 = l2;
     v1 = v2;
     l2 *= 10.0;
-    v2 = eval_volume(rho, dc, s, pas, n, l2, move, rmin);
+    v2 = vol(l2);
   }
   double lm = std::sqrt(l1 * l2);
   for (int32_t st = 0; st < maxb; ++st) {
     lm = std::sqrt(l1 * l2);
-    double vm = eval_volume(rho, dc, s, pas, n, lm, move, rmin);
+    double vm = vol(lm);
     double re = std::fabs(vm - tv) / maxd(tv, 1e-12);
     if (re <= voltol) break;
     if (vm > tv) l1 = lm;
@@ -1042,6 +1032,29 @@ extern "C" double orc_oc_update(const double* rho, const double* dc, const doubl
     }
   }
   return lm;
+}
+}  // namespace
+
+extern "C" double orc_oc_update(const double* rho, const double* dc, const double* s, const uint8_t* pas,
+                                double* rho_new, int32_t n, double f, double move, double rmin, double lg,
+                                int32_t maxb, double voltol) {
+  return oc_update_impl(rho, dc, s, pas, rho_new, n, f, move, rmin, lg, maxb, voltol, nullptr);
+}
+
+extern "C" int32_t orc_oc_trace(const double* rho, const double* dc, const double* s, const uint8_t* pas, int32_t n,
+                                double f, double move, double rmin, double lg, int32_t maxb, double voltol,
+                                double* lam_out, double* vol_out, int32_t cap, double* total_s_out) {
+  std::vector<double> rn((size_t)std::max(n, 1)), tr;
+  oc_update_impl(rho, dc, s, pas, rn.data(), n, f, move, rmin, lg, maxb, voltol, &tr);
+  double ts = 0.0;
+  for (int32_t i = 0; i < n; ++i) ts += s[i];
+  if (total_s_out) *total_s_out = ts;
+  int32_t cnt = (int32_t)(tr.size() / 2);
+  for (int32_t k = 0; k < cnt && k < cap; ++k) {
+    lam_out[k] = tr[2 * k];
+    vol_out[k] = tr[2 * k + 1];
+  }
+  return cnt;
 }
 
 // HeavisideProjection (HeavisideProjection.cs:12-37)
@@ -1292,7 +1305,9 @@ extern "C" int orc_topopt_run(orc_model* m, const orc_simp_options* o, orc_iter_
 
 // ---------------------------------------------------------------------------------------------------------
 extern "C" void orc_set_lane_mode(int mode) { g_lane_mode = mode; }
-extern "C" void orc_set_pow_mode(int mode) { g_pow_mode = mode; }
+extern "C" void orc_math_pow(int64_t n, const double* x, const double* y, int64_t y_len, double* out) {
+  for (int64_t i = 0; i < n; ++i) out[i] = mpow(x[i], y[y_len == 1 ? 0 : i]);
+}
 extern "C" void orc_set_threads(int n) {
 #ifdef _OPENMP
   omp_set_num_threads(n > 0 ? n : 1);

@@ -9,11 +9,10 @@
  * against the reference's own known-answer tests and published numbers (Hex8 patch tests, V1 axial bar,
  * V3 cantilever deflections, E_min ablation compliances) — see tests/test_oracle_*.py.
  *
- * Two details of the reference cannot be observed here and are runtime switches:
+ * One detail of the reference cannot be observed here and is a runtime switch:
  *   lane mode  — how Vector256<double>.Sum combines its four lanes
  *                (0: (l0+l1)+(l2+l3) [.NET 8+ Sum(lower)+Sum(upper)], 1: (l0+l2)+(l1+l3), 2: ((l0+l1)+l2)+l3)
- *   pow mode   — 0: glibc pow (what .NET's Math.Pow calls on Linux), 1: correctly rounded integer power
- *                (what the CUDA kernels compute; equals glibc pow except for ~0.1% 1-ulp cases of x^3).
+ * Math.Pow is the C library's pow, as .NET calls it on Linux.
  */
 #ifndef MYCEL_ORACLE_H
 #define MYCEL_ORACLE_H
@@ -31,7 +30,8 @@ extern "C" {
 #define ORC_E_INVALID_OPERATION 9
 
 void orc_set_lane_mode(int mode);
-void orc_set_pow_mode(int mode);
+/* Math.Pow as the restatement evaluates it (the C library's pow): out[i] = x[i]^y[y_len == 1 ? 0 : i]. */
+void orc_math_pow(int64_t n, const double* x, const double* y, int64_t y_len, double* out);
 void orc_set_threads(int n);
 int orc_get_threads(void);
 /* RunWriter.ComputeQuantizedChecksum and the 8-bit frame quantisation (Persistence/RunWriter.cs:211-217,
@@ -104,6 +104,11 @@ void orc_sensitivities(orc_op* op, const double* u, const double* rho_phys, doub
 double orc_oc_update(const double* rho, const double* dc, const double* s, const uint8_t* passive, double* rho_new,
                      int32_t n, double f, double move, double rho_min, double lambda_guess, int32_t max_bisect,
                      double vol_tol);
+/* The same update, recording each volume evaluation in order: lam_out[k], vol_out[k] (up to cap of them);
+   returns the number of evaluations; total_s_out: the sum of s in element order. */
+int32_t orc_oc_trace(const double* rho, const double* dc, const double* s, const uint8_t* pas, int32_t n, double f,
+                     double move, double rmin, double lg, int32_t maxb, double voltol, double* lam_out,
+                     double* vol_out, int32_t cap, double* total_s_out);
 
 /* HeavisideProjection */
 void orc_heaviside_project(const double* rt, double* rb, int32_t n, double beta, double eta);

@@ -111,23 +111,36 @@ def _setup(L):
     L.orc_oc_update.restype = C.c_double
     L.orc_oc_update.argtypes = [dp, dp, dp, P, dp, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double,
                                 C.c_int32, C.c_double]
+    L.orc_oc_trace.restype = C.c_int32
+    L.orc_oc_trace.argtypes = [dp, dp, dp, P, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int32,
+                               C.c_double, dp, dp, C.c_int32, C.POINTER(C.c_double)]
     L.orc_heaviside_project.argtypes = [dp, dp, C.c_int32, C.c_double, C.c_double]
     L.orc_heaviside_derivative.argtypes = [dp, dp, C.c_int32, C.c_double, C.c_double]
     L.orc_passive_region.argtypes = [C.c_int, C.c_int, C.c_int, ip, C.c_int32, C.c_int, bp]
     L.orc_topopt_run.argtypes = [P, C.POINTER(SimpOpts), C.POINTER(IterRec), C.c_int32, C.POINTER(C.c_int32),
                                  C.POINTER(C.c_int32), dp, fp, fp, dp, dp, C.POINTER(C.c_double), C.c_char_p, C.c_int]
     L.orc_set_lane_mode.argtypes = [C.c_int]
-    L.orc_set_pow_mode.argtypes = [C.c_int]
+    L.orc_math_pow.argtypes = [C.c_int64, dp, dp, C.c_int64, dp]
     L.orc_set_threads.argtypes = [C.c_int]
     L.orc_get_threads.restype = C.c_int
 
 
-def set_modes(lane_mode: int = 0, pow_mode: int = 0, threads: int | None = None):
+def set_modes(lane_mode: int = 0, threads: int | None = None):
     L = lib()
     L.orc_set_lane_mode(lane_mode)
-    L.orc_set_pow_mode(pow_mode)
     if threads is not None:
         L.orc_set_threads(threads)
+
+
+def math_pow(x, y) -> np.ndarray:
+    """Math.Pow as the restatement evaluates it (the C library's pow), elementwise; y an array or a scalar."""
+    x = np.ascontiguousarray(x, dtype=np.float64).ravel()
+    y = np.ascontiguousarray(np.atleast_1d(y), dtype=np.float64).ravel()
+    if y.size not in (1, x.size):
+        raise ValueError("y needs 1 or len(x) values")
+    out = np.empty(x.size)
+    lib().orc_math_pow(x.size, x, y, y.size, out)
+    return out
 
 
 def create_ke(h: float, nu: float) -> np.ndarray:
@@ -335,6 +348,36 @@ def oc_update(rho, dc, s, passive, f, move=0.2, rho_min=1e-3, lambda_guess=1.0, 
                               None if pas is None else pas.ctypes.data, out, rho.size, f, move, rho_min, lambda_guess,
                               max_bisect, vol_tol)
     return out, lam
+
+
+def oc_trace(rho, dc, s, passive, f, move=0.2, rho_min=1e-3, lambda_guess=1.0, max_bisect=60, vol_tol=1e-8):
+    """The volume evaluations of OcOptimizer.Update in order: (lambdas, volumes, sum of s in element order)."""
+    rho = np.ascontiguousarray(rho, dtype=np.float64)
+    pas = None if passive is None else np.ascontiguousarray(passive, dtype=np.uint8)
+    cap = 512
+    lam = np.zeros(cap)
+    vol = np.zeros(cap)
+    ts = C.c_double(0)
+    k = lib().orc_oc_trace(rho, np.ascontiguousarray(dc, dtype=np.float64), np.ascontiguousarray(s, dtype=np.float64),
+                           None if pas is None else pas.ctypes.data, rho.size, f, move, rho_min, lambda_guess,
+                           max_bisect, vol_tol, lam, vol, cap, C.byref(ts))
+    return lam[:k].copy(), vol[:k].copy(), ts.value
+
+
+def heaviside_project(rho_tilde, beta, eta=0.5):
+    """HeavisideProjection.Project (HeavisideProjection.cs:12-24)."""
+    x = np.ascontiguousarray(rho_tilde, dtype=np.float64)
+    out = np.empty_like(x)
+    lib().orc_heaviside_project(x, out, x.size, beta, eta)
+    return out
+
+
+def heaviside_derivative(rho_tilde, beta, eta=0.5):
+    """HeavisideProjection.Derivative (HeavisideProjection.cs:26-37)."""
+    x = np.ascontiguousarray(rho_tilde, dtype=np.float64)
+    out = np.empty_like(x)
+    lib().orc_heaviside_derivative(x, out, x.size, beta, eta)
+    return out
 
 
 def quantized_frame(v):

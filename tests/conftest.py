@@ -16,7 +16,7 @@ def pytest_configure(config):
 def oracle():
     from oracle import oracle as O
     O.lib()
-    O.set_modes(0, 0)
+    O.set_modes(0)
     return O
 
 

@@ -20,9 +20,9 @@ pytestmark = pytest.mark.gpu
 def oracle_cr(oracle):
     """The oracle with correctly rounded integer powers in E = Emin + rho^p (E0 - Emin), as the device computes
     them (glibc pow, the oracle's default, is off by an ulp for a few random densities)."""
-    oracle.set_modes(0, 1)
+    oracle.set_modes(0)
     yield oracle
-    oracle.set_modes(0, 0)
+    oracle.set_modes(0)
 
 
 def _single(m, k):

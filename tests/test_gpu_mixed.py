@@ -17,9 +17,9 @@ pytestmark = pytest.mark.gpu
 
 @pytest.fixture(autouse=True)
 def exact_oracle(oracle):
-    oracle.set_modes(0, 1, threads=8)
+    oracle.set_modes(0, threads=8)
     yield
-    oracle.set_modes(0, 0)
+    oracle.set_modes(0)
 
 
 @pytest.mark.parametrize("variant", [1, 2, 3], ids=["dense", "tensor", "factored"])

@@ -115,3 +115,20 @@ def test_separate_load_cases_served(ctx, precision):
     sess.close()
     pr.close()
     assert held <= est <= 1.25 * held
+
+
+def test_six_slots_started_together(ctx):
+    """Six jobs admitted at once into six slots: their contexts' first OC launches overlap on the device; every
+    job's results are still bit-identical to the job run alone (plain method)."""
+    shapes = [(24, 12, 8), (32, 16, 8), (20, 10, 10), (28, 14, 6), (36, 12, 8), (16, 8, 8)]
+    jobs = [W.served_job(nx, ny, nz, 3, seed=300 + i, precision="fp64") for i, (nx, ny, nz) in enumerate(shapes)]
+    alone = [api.TopologyOptimizer.run(m, o, ctx=ctx) for m, o in jobs]
+    with api.Server(slots=6, hbm_budget_bytes=8 * 10**9) as srv:
+        ids = [srv.submit(m, o, keep_u=True) for m, o in jobs]
+        srv.wait()
+        for jid, ref in zip(ids, alone):
+            r = srv.result(jid, u=True)
+            assert r["info"]["state"] == "done", r["info"]["message"]
+            assert [a.compliance for a in r["history"]] == [b.compliance for b in ref.snapshots]
+            assert np.array_equal(r["physical"], ref.final_physical_density)
+            assert np.array_equal(r["u"], ref.final_displacements)

@@ -280,9 +280,9 @@ def test_t5_bridge_mirror_symmetry(oracle):
 def test_t7_determinism_and_thread_independence(oracle):
     m = W.cantilever(20, 8, 4)
     o = _cantilever_opts(max_iterations=10)
-    oracle.set_modes(0, 0, threads=1)
+    oracle.set_modes(0, threads=1)
     r1 = oracle.topopt_run(m, o)
-    oracle.set_modes(0, 0, threads=8)
+    oracle.set_modes(0, threads=8)
     r2 = oracle.topopt_run(m, o)
     assert [x["compliance"] for x in r1.records] == [x["compliance"] for x in r2.records]
     assert np.array_equal(r1.phys, r2.phys) and np.array_equal(r1.u, r2.u)
@@ -339,3 +339,28 @@ def test_average_element_to_node_reference_case(oracle):
     out = oracle.Model(m).average_element_to_node(np.array([10.0, 20.0, 30.0, 40.0]))
     assert abs(out[g.node_index(1, 1, 0)] - 25.0) < 1e-10
     assert abs(out[g.node_index(0, 0, 0)] - 10.0) < 1e-10
+
+
+# Published PCG iteration counts of the reference's V10 scaling benchmark (docs/STEP3_BENCH.md:25-28), model
+# of FemValidationTests.cs:633-726: cold solve to 1e-4 (rho = 1), warm solve to 1e-4 of the 2 % perturbed model
+# (rho = 0.98) from the cold u, cold solve of the perturbed model, cold solve to 1e-6.
+V10_PUBLISHED = {53_240: (436, 410, 436, 481), 98_415: (535, 503, 535, 591)}
+
+
+def v10_counts(oracle, target):
+    m0 = W.v10_cantilever(target)
+    mp = W.v10_cantilever(target, 0.98)
+    c4 = oracle.static_run(m0, 1e-4)
+    w4 = oracle.static_run(mp, 1e-4, warm_start=c4.u)
+    cp = oracle.static_run(mp, 1e-4)
+    c6 = oracle.static_run(m0, 1e-6)
+    return m0, (c4, w4, cp, c6)
+
+
+def test_v10_published_pcg_counts_53k(oracle):
+    # the whole PCG path (KE, forces, colour-ordered products, 8192-block reductions, stopping rule) reproduces
+    # the reference's own published iteration counts
+    oracle.set_modes(0, threads=8)
+    m0, runs = v10_counts(oracle, 50_000)
+    assert m0.total_elements == 53_240 and m0.total_dofs == 176_157
+    assert tuple(r.solver_info.iterations for r in runs) == V10_PUBLISHED[53_240]
