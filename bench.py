@@ -59,7 +59,11 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mycel", choices=["mycel", "reference"])
     ap.add_argument("--workload", default="bridge_192x96x96", choices=["bridge_192x96x96", "cantilever_40x20x10"])
-    ap.add_argument("--fp64-steps", type=int, default=2)
+    ap.add_argument("--fp64-steps", type=int, default=-1,
+                    help="iterations after the warm-up of the plain FP64 arm run beside the timed form (-1: --steps, "
+                         "0: none)")
+    ap.add_argument("--others-steps", type=int, default=2,
+                    help="iterations after the warm-up of the other solver forms (fp64f, mg, mixed)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-sample-iters", type=int, default=6)
@@ -487,6 +491,7 @@ def run_mycel(args):
     barrier(ws)
     t_ms = e0.elapsed_time(e1)
     timing = ctx.kernel_timing(0)
+    timing_l1 = ctx.kernel_timing(3)
     ctx.set_profiling(False)
     gpu_launches = ctx.launch_count - launches0
     t_max = max_over_ranks(ws, t_ms)
@@ -516,6 +521,21 @@ def run_mycel(args):
             "flops_per_launch": 1152 * model.active_element_count, "flops_note": "dense-KE equivalent",
             "tflops": 1152 * model.active_element_count / (per_launch_ms / 1000.0) / 1e12 if timing["launches"] else None}
 
+    # the multigrid level-1 residual product (y = r - A x on the 96x48x48 level, 27-point stencil of 3x3 blocks in
+    # half storage): 14 blocks x 9 floats of the node's own rows + x, r, 1/diag read + y written = 552 B per node
+    roof_l1 = None
+    if timing_l1["launches"]:
+        l1_ms = timing_l1["total_ms"] / timing_l1["launches"]
+        l1_nodes = timing_l1["nodes"] / timing_l1["launches"]
+        l1_bytes = 552.0 * l1_nodes
+        l1_ach = l1_bytes / (l1_ms / 1000.0) / 1e9
+        roof_l1 = {"kernel": "k_mg_apply_nodes (multigrid level-1 residual product, thread per node)", "bound": "hbm",
+                   "achieved": l1_ach, "peak": hbm, "unit": "GB/s", "frac": l1_ach / hbm,
+                   "traffic": NCU_DRAM_BYTES.get(("mg-level1", args.precision, args.workload)),
+                   "peak_source": "measured" if pk else "fallback", "avg_launch_us": l1_ms * 1000.0,
+                   "timed_launches": timing_l1["launches"], "nodes_per_launch": l1_nodes,
+                   "algorithmic_bytes_per_launch": l1_bytes, "bytes_per_node": 552}
+
     out = {"metric": METRIC, "value": value,
            "unit": "SIMP iter/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -525,55 +545,63 @@ def run_mycel(args):
                       "penal": opts.penal, "emin_ratio": model.material.emin_ratio,
                       "pcg_tol": opts.solver_tolerance_final, "inputs_vs_l2": "inputs > L2 (126 MB); no flush",
                       "parallelism": f"replicas x{ws}"},
-           "roofline": roof, "gpu_launches": gpu_launches, "clocks": clk,
+           "roofline": roof, "roofline_mg_level1": roof_l1, "gpu_launches": gpu_launches, "clocks": clk,
            "pcg_inner_iters_per_step": pcg_inner, "compliance": comp_head}
 
-    # ---------------- plain FP64 path on the same iterations ----------------
-    if args.fp64_steps > 0 and rank == 0:
-        prob = api.Problem(model, ctx)
-        sess = api.SimpSession(prob, opts.replace(precision="fp64"))
+    # ---------------- plain FP64 path over the same iterations; the timed form's errors against it ----------------
+    # Both forms run from iteration 1 side by side for the timed run's W + K iterations (or W + --fp64-steps):
+    # per iteration the relative compliance error, the max-norm relative error of u and the largest absolute
+    # difference of the physical densities (values in [0, 1]) of the timed form against the plain FP64 path.
+    if args.fp64_steps != 0 and rank == 0:
+        n_acc = args.warmup + (args.steps if args.fp64_steps < 0 else args.fp64_steps)
+        pa, pb = api.Problem(model, ctx), api.Problem(model, ctx)
+        if args.mv32_variant:
+            pa.set_matvec32(args.mv32_variant)
+        sa = api.SimpSession(pa, head)
+        sb = api.SimpSession(pb, opts.replace(precision="fp64"))
         ctx.set_profiling(True)
-        f_recs = []
-        t64 = []
-        for i in range(args.warmup + args.fp64_steps):
+        f_recs, t64, err_c, err_u, err_d = [], [], [], [], []
+        for i in range(n_acc):
+            ra = sa.step()
             f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             f0.record(stream)
-            r = sess.step()
+            rb = sb.step()
             f1.record(stream)
             torch.cuda.synchronize(local)
-            f_recs.append(r)
+            f_recs.append(rb)
             if i >= args.warmup:
                 t64.append(f0.elapsed_time(f1))
+            xa = sa.read(u=True, densities=False, active=True)
+            xb = sb.read(u=True, densities=False, active=True)
+            err_c.append(abs(ra.compliance - rb.compliance) / abs(rb.compliance))
+            err_u.append(float(np.abs(xa["u"] - xb["u"]).max() / np.abs(xb["u"]).max()))
+            err_d.append(float(np.abs(xa["rho_phys_active"] - xb["rho_phys_active"]).max()))
         tm64 = ctx.kernel_timing(1)
         ctx.set_profiling(False)
-        sess.close()
-        prob.close()
-        # compliance of the same iterations (1..W+fp64_steps) in the timed form: rerun them from the start
-        prob = api.Problem(model, ctx)
-        sess = api.SimpSession(prob, head)
-        m_recs = [sess.step() for _ in range(args.warmup + args.fp64_steps)]
-        sess.close()
-        prob.close()
-        errs = [abs(a.compliance - b.compliance) / abs(b.compliance) for a, b in zip(m_recs, f_recs)]
+        for q in (sa, sb, pa, pb):
+            q.close()
         per64 = tm64["total_ms"] / max(1, tm64["launches"])
         out["fp64"] = {"simp_iter_s": 1000.0 * len(t64) / sum(t64) if t64 else None,
                        "ms_per_step": statistics.mean(t64) if t64 else None,
+                       "iterations_timed": f"{args.warmup + 1}..{n_acc}",
                        "pcg_iters_per_step": [r.solver_iterations for r in f_recs[args.warmup:]],
                        "matvec_us": per64 * 1000.0,
-                       "matvec_gbs": (48 * model.total_nodes + 9 * model.total_elements) / (per64 / 1000.0) / 1e9 if tm64["launches"] else None,
-                       "timed_form_vs_fp64_rel_compliance_err": errs,
-                       "max_rel_compliance_err": max(errs) if errs else None}
+                       "matvec_gbs": (48 * model.total_nodes + 9 * model.total_elements) / (per64 / 1000.0) / 1e9 if tm64["launches"] else None}
+        out["rel_err_vs_fp64"] = {"iterations": list(range(1, n_acc + 1)), "compliance": err_c, "u": err_u,
+                                  "density": err_d, "max_compliance": max(err_c), "max_u": max(err_u),
+                                  "max_density": max(err_d),
+                                  "definition": "per SIMP iteration from 1, timed form vs plain FP64 run side by side: "
+                                                "|C - C64|/|C64|, max|u - u64|/max|u64|, max|rho_phys - rho_phys64|"}
         out["speedup_vs_fp64"] = (value / ws) / out["fp64"]["simp_iter_s"] if out["fp64"]["simp_iter_s"] else None
-        # fast FP64 form (factorised FP64 operator, FP64 recurrences) and the multigrid form (FP64 flexible CG
-        # preconditioned by an FP32 V-cycle) on the same iterations
+        # the other solver forms on the first W + --others-steps iterations: speed and compliance error
         others = [("fp64f", "fp64_factored"), ("mg", "fp64_multigrid"), ("mixed", "mixed_jacobi"),
                   ("mixed-mg", "mixed_multigrid")]
-        for prec, key in [o for o in others if o[0] != args.precision]:
+        n_oth = min(n_acc, args.warmup + args.others_steps)
+        for prec, key in [o for o in others if o[0] != args.precision and args.others_steps > 0]:
             prob = api.Problem(model, ctx)
             sess = api.SimpSession(prob, opts.replace(precision=prec))
-            ctx.set_profiling(True)
             q_recs, tq = [], []
-            for i in range(args.warmup + args.fp64_steps):
+            for i in range(n_oth):
                 f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 f0.record(stream)
                 q_recs.append(sess.step())
@@ -581,16 +609,13 @@ def run_mycel(args):
                 torch.cuda.synchronize(local)
                 if i >= args.warmup:
                     tq.append(f0.elapsed_time(f1))
-            tmq = ctx.kernel_timing(2)
-            ctx.set_profiling(False)
             sess.close()
             prob.close()
-            perq = tmq["total_ms"] / max(1, tmq["launches"])
             qerr = [abs(a.compliance - b.compliance) / abs(b.compliance) for a, b in zip(q_recs, f_recs)]
             out[key] = {"simp_iter_s": 1000.0 * len(tq) / sum(tq) if tq else None,
                         "ms_per_step": statistics.mean(tq) if tq else None,
                         "pcg_iters_per_step": [r.solver_iterations for r in q_recs[args.warmup:]],
-                        "matvec_us": perq * 1000.0, "max_rel_compliance_err_vs_fp64": max(qerr) if qerr else None,
+                        "max_rel_compliance_err_vs_fp64": max(qerr) if qerr else None,
                         "rel_compliance_err_vs_fp64": qerr}
 
     # ---------------- e2e: whole job through the C ABI from host buffers ----------------

@@ -169,9 +169,11 @@ void* mycel_ctx_stream(mycel_ctx* ctx);
 const char* mycel_last_error(mycel_ctx* ctx);
 /* Kernel launches issued by this context since creation (all of them are this library's own kernels). */
 int64_t mycel_ctx_launch_count(mycel_ctx* ctx);
-/* Live timing of the dominant kernel: when enabled, PCG chunks record CUDA events around one stiffness matvec
-   launch per chunk (on the context stream). which = 0: FP32 matvec of the mixed form, 1: FP64 matvec.
-   Returns the summed device time, the number of timed launches and the nodes / active elements they covered. */
+/* Live timing of the dominant kernels: when enabled, PCG chunks record CUDA events around one stiffness matvec
+   launch per chunk (on the context stream). which = 0: FP32 matvec of the mixed form, 1: FP64 matvec,
+   2: FP64 matvec of the fast FP64 and multigrid forms, 3: the multigrid forms' level-1 residual product
+   (event-record nodes inside the chunk graph; nodes = that level's nodes). Returns the summed device time, the
+   number of timed launches and the nodes / active elements they covered. */
 int32_t mycel_ctx_set_profiling(mycel_ctx* ctx, int32_t enable);
 int32_t mycel_ctx_kernel_timing(mycel_ctx* ctx, int32_t which, double* total_ms, int64_t* launches, int64_t* nodes,
                                 int64_t* active_elements);

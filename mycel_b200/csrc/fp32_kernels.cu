@@ -2708,6 +2708,10 @@ struct MgHier {
   cudaGraphExec_t graph32[2] = {nullptr, nullptr};  // FP32 outer iteration chunks (mixed multigrid form)
   int graph32_profiled = 0;
   cudaEvent_t ev32[2][2] = {};
+  // live timing of the level-1 residual product (the form's largest coarse-level kernel): event-record nodes
+  // around it in the first iteration of each chunk graph, captured only while the context profiles
+  cudaEvent_t l1ev[2][2] = {};
+  cudaEvent_t* l1_timing = nullptr;  // the pair of the graph being captured (iteration 0 only), else null
   float* f_t = nullptr;  // FP32 outer form: A x of the voxel level's smoothing (padded FP32 layout)
   float* eig[kMgMaxLevels] = {};  // last eigenvector estimate of D^-1 A per smoothed level (warm start)
   bool eig_valid = false;
@@ -2758,6 +2762,7 @@ void mg_release(mycel_problem* p) {
     for (int j = 0; j < 2; ++j) {
       if (mg->ev[k][j]) cudaEventDestroy(mg->ev[k][j]);
       if (mg->ev32[k][j]) cudaEventDestroy(mg->ev32[k][j]);
+      if (mg->l1ev[k][j]) cudaEventDestroy(mg->l1ev[k][j]);
     }
   }
   for (void* b : mg->bufs) cudaFreeAsync(b, p->ctx->stream);
@@ -2970,7 +2975,9 @@ static int mg_vcycle(mycel_problem* p, cudaStream_t s, MixState* st, float* rf, 
       launch_mg_apply(s, v, x, v.r, v.invd, o, 1, om + l, st);
       std::swap(x, o);
     }
+    if (l == 1 && mg->l1_timing) cudaEventRecordWithFlags(mg->l1_timing[0], s, cudaEventRecordExternal);
     launch_mg_apply(s, v, x, v.r, v.invd, v.t, 2, om + l, st);
+    if (l == 1 && mg->l1_timing) cudaEventRecordWithFlags(mg->l1_timing[1], s, cudaEventRecordExternal);
     k_mg_restrict<false><<<mg_blocks(lv[l + 1].nn), 256, 0, s>>>(v.d, 0, nullptr, v.t, lv[l + 1].d, lv[l + 1].invd,
                                                                  lv[l + 1].r, st,
                                                                  l + 1 < mg->L - 1 ? lv[l + 1].xa : nullptr,
@@ -3107,6 +3114,11 @@ static int32_t capture_inner_graph(mycel_problem* p, const InnerForm& F, int chu
   }
   cudaStream_t s = c->stream;
   int64_t before = c->launches;
+  MgHier* mg = F.mg ? p->mg : nullptr;
+  if (mg)
+    for (int k = 0; k < 2; ++k)
+      for (int j = 0; j < 2; ++j)
+        if (!mg->l1ev[k][j]) cudaEventCreate(&mg->l1ev[k][j]);
   for (int k = 0; k < 2; ++k) {
     cudaGraph_t graph;
     MYCEL_CUDA(c, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
@@ -3114,7 +3126,9 @@ static int32_t capture_inner_graph(mycel_problem* p, const InnerForm& F, int chu
       void* pcur = (t & 1) ? F.p1 : F.p0;
       void* pprev = (t & 1) ? F.p0 : F.p1;
       if (!(c->profile && t == 0)) launch_inner_mv(p, F, s, pprev, pcur);
+      if (mg) mg->l1_timing = (c->profile && t == 0 && mg->T > 1) ? mg->l1ev[k] : nullptr;
       launch_inner_xr(p, F, s, pcur, 0);
+      if (mg) mg->l1_timing = nullptr;
     }
     MYCEL_CUDA(c, cudaStreamEndCapture(s, &graph));
     MYCEL_CUDA(c, cudaGraphInstantiate(&F.graph[k], graph, 0));
@@ -3245,6 +3259,12 @@ static int32_t refined_loop(mycel_problem* p, const InnerForm& F, const double* 
           c->prof_n[F.prof_slot] += 1;
           c->prof_nodes[F.prof_slot] += p->g.nn;
           c->prof_elems[F.prof_slot] += p->n_active;
+        }
+        if (F.mg && p->mg->T > 1 &&
+            cudaEventElapsedTime(&ms_, p->mg->l1ev[pi][0], p->mg->l1ev[pi][1]) == cudaSuccess) {
+          c->prof_ms[3] += ms_;
+          c->prof_n[3] += 1;
+          c->prof_nodes[3] += p->mg->lv[1].nn;
         }
       }
     }
