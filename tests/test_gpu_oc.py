@@ -28,40 +28,57 @@ def _rel(v, tv):
     return abs(v - tv) / max(tv, 1e-12)
 
 
-def _late_record_trial(rels):
-    # a late bisection trial whose relative error is below every earlier one's: with the tolerance set to it, the
-    # reference stops exactly there
-    k = len(rels) - 1
-    while k > 0 and not (0 < rels[k] < min(rels[:k])):
-        k -= 1
-    assert k > 2
-    return k
+def _bisection_start(lam):
+    # the bracket's two trials, then its expansions (lambda x 0.1 or x 10), then the bisection
+    b = 2
+    while b < len(lam) and (lam[b] == lam[b - 1] * 0.1 or lam[b] == lam[b - 1] * 10.0):
+        b += 1
+    return b
 
 
+def _late_record_trial(lam, rels):
+    # a late bisection trial whose relative error is below every earlier bisection trial's: with the tolerance
+    # set to it, the reference stops exactly there
+    b = _bisection_start(lam)
+    for k in range(len(rels) - 1, b + 2, -1):
+        if 0 < rels[k] < min(rels[b:k]):
+            return k
+    raise AssertionError("no record trial")
+
+
+# f = 0.5: the target lies between the volumes at the largest and the smallest multiplier, so the bracket is
+# found and the bisection runs
 @pytest.mark.parametrize("n", [5000, 120_001, 1_769_472])
 def test_tolerance_tie(oracle, ctx, n):
     rho, dc, s, pas = _inputs(n, 7 + n % 11)
-    f = 0.35
+    f = 0.5
     lam, vol, ts = oracle.oc_trace(rho, dc, s, pas, f, vol_tol=0.0)
     tv = f * ts
     rels = [_rel(v, tv) for v in vol]
-    k = _late_record_trial(rels)
-    for tol in (rels[k], float(np.nextafter(rels[k], 0.0)), float(np.nextafter(rels[k], 1.0))):
-        oo, ol = oracle.oc_update(rho, dc, s, pas, f, 0.2, 1e-3, 1.0, 60, tol)
-        go, gl = api.oc_update(rho, dc, s, pas, f, 0.2, 1e-3, 1.0, 60, tol, ctx=ctx)
-        assert gl == ol, (k, tol)
-        assert np.array_equal(go, oo)
-    # at exactly the trial's relative error the reference stops on that trial
-    assert oracle.oc_update(rho, dc, s, pas, f, 0.2, 1e-3, 1.0, 60, rels[k])[1] == lam[k]
+    # the last record trial (relative error near 1e-16: decided in the last bits) and the first record below
+    # 1e-7 (the range of the SIMP loop's 1e-8 tolerance)
+    b = _bisection_start(lam)
+    k_late = _late_record_trial(lam, rels)
+    k_mid = next(k for k in range(b + 1, len(rels)) if rels[k] < 1e-7 and rels[k] < min(rels[b:k]))
+    for k in (k_late, k_mid):
+        for tol in (rels[k], float(np.nextafter(rels[k], 0.0)), float(np.nextafter(rels[k], 1.0))):
+            oo, ol = oracle.oc_update(rho, dc, s, pas, f, 0.2, 1e-3, 1.0, 60, tol)
+            go, gl = api.oc_update(rho, dc, s, pas, f, 0.2, 1e-3, 1.0, 60, tol, ctx=ctx)
+            assert gl == ol, (k, tol)
+            assert np.array_equal(go, oo)
+        # at exactly the trial's relative error the reference stops on that trial
+        assert oracle.oc_update(rho, dc, s, pas, f, 0.2, 1e-3, 1.0, 60, rels[k])[1] == lam[k]
 
 
 @pytest.mark.parametrize("n", [5000, 120_001])
 def test_equality_tie(oracle, ctx, n):
-    # zero tolerance and a target equal to the reference's V(lambda) of a late trial: the reference stops there
+    # zero tolerance and a target equal to the reference's V(lambda) of a late bisection trial: the reference
+    # stops there
     rho, dc, s, pas = _inputs(n, 3 + n % 7)
-    lam, vol, ts = oracle.oc_trace(rho, dc, s, pas, 0.3, vol_tol=0.0)
+    lam, vol, ts = oracle.oc_trace(rho, dc, s, pas, 0.5, vol_tol=0.0)
+    b = _bisection_start(lam)
     found = False
-    for k in range(len(vol) - 1, 2, -1):
+    for k in range(len(vol) - 1, b + 2, -1):
         f = vol[k] / ts
         for _ in range(8):
             if f * ts == vol[k]:
