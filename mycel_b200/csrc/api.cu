@@ -947,11 +947,30 @@ extern "C" int32_t mycel_static_solve_cases(mycel_problem* p, const mycel_static
   const int64_t nd = p->g.nd;
   double* d_sc = p->d_part2;  // [0] compliance, [1] max disp
   double* hsc = (double*)c->pinned;
+  // the mixed multigrid form solves the cases together (one V-cycle's coarse levels for all of them)
+  const bool together = o.precision == MYCEL_PRECISION_MIXED_MG && p->n_cases > 1 &&
+                        p->n_cases <= kMaxBatchedCases && cases_together_enabled();
+  double* d_ucs = nullptr;
+  std::vector<mycel_pcg_result> rs((size_t)std::max(p->n_cases, 1));
+  struct Free {
+    double*& q; cudaStream_t s;
+    ~Free() { if (q) cudaFreeAsync(q, s); }
+  } free_ucs{d_ucs, s};
+  if (together) {
+    MYCEL_CUDA(c, cudaMallocAsync((void**)&d_ucs, sizeof(double) * nd * p->n_cases, s));
+    MYCEL_CUDA(c, cudaMemsetAsync(d_ucs, 0, sizeof(double) * nd * p->n_cases, s));
+    if ((st = mg_solve_cases(p, p->n_cases, d_ucs, o.tolerance, o.max_iterations, nullptr, rs.data()))) return st;
+  }
   for (int k = 0; k < p->n_cases; ++k) {
     mycel_pcg_result local;
     mycel_pcg_result* r = res ? res + k : &local;
-    MYCEL_CUDA(c, cudaMemsetAsync(p->d_x, 0, sizeof(double) * nd, s));
-    if ((st = solve_case(p, k, p->d_x, o.tolerance, o.max_iterations, o.precision, nullptr, r))) return st;
+    if (together) {
+      *r = rs[(size_t)k];
+      MYCEL_CUDA(c, cudaMemcpyAsync(p->d_x, d_ucs + k * nd, sizeof(double) * nd, cudaMemcpyDeviceToDevice, s));
+    } else {
+      MYCEL_CUDA(c, cudaMemsetAsync(p->d_x, 0, sizeof(double) * nd, s));
+      if ((st = solve_case(p, k, p->d_x, o.tolerance, o.max_iterations, o.precision, nullptr, r))) return st;
+    }
     if (o.throw_on_non_convergence && !r->converged)
       return set_error(c, MYCEL_E_NOT_CONVERGED,
                        "FEM solver did not converge in " + std::to_string(r->iterations) + " iterations (" +

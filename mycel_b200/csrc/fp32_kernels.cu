@@ -35,7 +35,7 @@
 
 namespace mycel {
 
-enum MixStatus : int { MIX_RUNNING = 0, MIX_FLUSH = 1, MIX_BREAKDOWN = 2, MIX_MAXITER = 3 };
+enum MixStatus : int { MIX_RUNNING = 0, MIX_FLUSH = 1, MIX_BREAKDOWN = 2, MIX_MAXITER = 3, MIX_DONE = 4 };
 
 struct MixState {
   int status;
@@ -1297,6 +1297,8 @@ static const CUtensorMap* tmap_of(mycel_problem* p, const float* ptr) {
   const float* bufs[4] = {p->f_r, p->f_z, p->f_p0, p->f_p1};
   for (int q = 0; q < 4; ++q)
     if (ptr == bufs[q]) return &p->f_tmap[q];
+  for (int q = 0; q < p->n_case_tmaps; ++q)
+    if (ptr == p->case_tmap_ptr[q]) return p->case_tmap[q];
   return nullptr;
 }
 
@@ -1668,6 +1670,20 @@ struct MgDims {
   int nx, ny, nz;  // elements per axis (nodes: one more)
 };
 
+// Load cases kept apart are advanced together: the coarse-level kernels of one V-cycle take the vectors of up
+// to kMgMaxCases cases (the cases share K, so each stencil entry is loaded once per node for all of them).
+// Threads are numbered with the case fastest, so the lanes of a node read the same stencil words. Case c's
+// vector of a level is p[c]; a single solve is the case set {1 case}.
+constexpr int kMgMaxCases = 8;
+struct MgPtrs {
+  float* p[kMgMaxCases];
+};
+__host__ __device__ __forceinline__ MgPtrs mg_one(float* v) {
+  MgPtrs r{};
+  r.p[0] = v;
+  return r;
+}
+
 __host__ __device__ __forceinline__ int64_t mg_nn(const MgDims& d) {
   return (int64_t)(d.nx + 1) * (d.ny + 1) * (d.nz + 1);
 }
@@ -1938,25 +1954,34 @@ __device__ __forceinline__ void mg_apply_row(const MgDims& d, int64_t nn, int64_
 
 // coarse-level product kernels: a thread per node (large levels: the three rows share their x loads) or a
 // thread per DOF (smaller levels: three times the threads in flight); mg_apply_kernel picks by size
+// (st: the cases' states, one per case, or null; a case whose state is not running is skipped)
 __global__ void __launch_bounds__(256) k_mg_apply_nodes(MgDims d, const float* __restrict__ S,
-                                                        const float* __restrict__ x, const float* __restrict__ r,
-                                                        const float* __restrict__ invd, float* __restrict__ y,
-                                                        int mode, const float* __restrict__ om, const MixState* st) {
-  if (!mg_running(st)) return;
+                                                        const __grid_constant__ MgPtrs x,
+                                                        const __grid_constant__ MgPtrs r,
+                                                        const float* __restrict__ invd,
+                                                        const __grid_constant__ MgPtrs y, int mode,
+                                                        const float* __restrict__ om, const MixState* st, int ncase) {
   const int64_t nn = mg_nn(d);
-  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (n < nn) mg_apply_node(d, nn, n, S, x, r, invd, y, mode, mode == 1 ? *om : 0.0f);
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t n = t / ncase;
+  const int c = (int)(t - n * ncase);
+  if (n >= nn || !mg_running(st ? st + c : nullptr)) return;
+  mg_apply_node(d, nn, n, S, x.p[c], r.p[c], invd, y.p[c], mode, mode == 1 ? *om : 0.0f);
 }
 
 __global__ void __launch_bounds__(kMgDofThreads) k_mg_apply(MgDims d, const float* __restrict__ S,
-                                                            const float* __restrict__ x, const float* __restrict__ r,
-                                                            const float* __restrict__ invd, float* __restrict__ y,
-                                                            int mode, const float* __restrict__ om,
-                                                            const MixState* st) {
-  if (!mg_running(st)) return;
+                                                            const __grid_constant__ MgPtrs x,
+                                                            const __grid_constant__ MgPtrs r,
+                                                            const float* __restrict__ invd,
+                                                            const __grid_constant__ MgPtrs y, int mode,
+                                                            const float* __restrict__ om, const MixState* st,
+                                                            int ncase) {
   const int64_t nn = mg_nn(d);
-  const int64_t n = mg_dof_node();
-  if (n < nn) mg_apply_row(d, nn, n, mg_dof_comp(), S, x, r, invd, y, mode, mode == 1 ? *om : 0.0f);
+  const int64_t i = mg_dof_node();  // (node, case) pair, the case fastest
+  const int64_t n = i / ncase;
+  const int c = (int)(i - n * ncase);
+  if (n >= nn || !mg_running(st ? st + c : nullptr)) return;
+  mg_apply_row(d, nn, n, mg_dof_comp(), S, x.p[c], r.p[c], invd, y.p[c], mode, mode == 1 ? *om : 0.0f);
 }
 
 // a further sweep on the voxel grid (padded FP32 layout, t = A x): x += omega invd (r - t)
@@ -2096,13 +2121,16 @@ __device__ __forceinline__ void mg_restrict_node(const MgDims& f, int pitch, con
 }
 
 template <bool PAD>
-__global__ void k_mg_restrict(MgDims f, int pitch, const float* __restrict__ rf, const float* __restrict__ tf,
-                              MgDims c, const float* __restrict__ invdc, float* __restrict__ rc, const MixState* st,
-                              float* __restrict__ xc, const float* __restrict__ om) {
-  if (!mg_running(st)) return;
-  const float omega = xc ? *om : 0.f;
-  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (n < mg_nn(c)) mg_restrict_node<PAD>(f, pitch, rf, tf, c, invdc, rc, n, xc, omega);
+__global__ void k_mg_restrict(MgDims f, int pitch, const __grid_constant__ MgPtrs rf, const __grid_constant__ MgPtrs tf,
+                              MgDims c, const float* __restrict__ invdc, const __grid_constant__ MgPtrs rc,
+                              const MixState* st, const __grid_constant__ MgPtrs xc, int first_sweep,
+                              const float* __restrict__ om, int ncase) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t n = t / ncase;
+  const int k = (int)(t - n * ncase);
+  if (n >= mg_nn(c) || !mg_running(st ? st + k : nullptr)) return;
+  const float omega = first_sweep ? *om : 0.f;
+  mg_restrict_node<PAD>(f, pitch, rf.p[k], tf.p[k], c, invdc, rc.p[k], n, first_sweep ? xc.p[k] : nullptr, omega);
 }
 
 // prolongation x_f += W x_c at fine node n, on the finer level's free DOFs. PAD: the voxel grid (padded FP32
@@ -2151,10 +2179,13 @@ __device__ __forceinline__ void mg_prolong_node(const MgDims& f, int pitch, cons
 
 template <bool PAD>
 __global__ void k_mg_prolong(MgDims f, int pitch, const uint8_t* __restrict__ nf, const float* __restrict__ invdf,
-                             float* __restrict__ xf, MgDims c, const float* __restrict__ xc, const MixState* st) {
-  if (!mg_running(st)) return;
-  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (n < mg_nn(f)) mg_prolong_node<PAD>(f, pitch, nf, invdf, xf, c, xc, n);
+                             const __grid_constant__ MgPtrs xf, MgDims c, const __grid_constant__ MgPtrs xc,
+                             const MixState* st, int ncase) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t n = t / ncase;
+  const int k = (int)(t - n * ncase);
+  if (n >= mg_nn(f) || !mg_running(st ? st + k : nullptr)) return;
+  mg_prolong_node<PAD>(f, pitch, nf, invdf, xf.p[k], c, xc.p[k], n);
 }
 
 
@@ -2245,7 +2276,7 @@ struct MgTailLevel {
   int64_t nn;
   const float* S;
   const float* invd;
-  float *xa, *xb, *r, *t;
+  float *xa, *xb, *r, *t;  // case 0's vectors; case k's at + k * 3 nn
 };
 struct MgTail {
   int T, L, sweeps, nc;
@@ -2258,24 +2289,39 @@ __device__ __forceinline__ void mg_cluster_sync() {
   asm volatile("barrier.cluster.wait.acquire;\n" ::: "memory");
 }
 
-// Levels T .. L-1 of the V-cycle: from r of level T (restricted by the caller) to the smoothed correction of
-// level T, left in its xa.
+// Levels T .. L-1 of the V-cycle for ncase load cases: from r of level T (restricted by the caller) to the
+// smoothed correction of level T, left in its xa. Work items are numbered with the case fastest; a case whose
+// state is not running is skipped, and the kernel returns at once (every thread alike) when none is.
 __global__ void __cluster_dims__(kMgTailCtas, 1, 1) __launch_bounds__(kMgTailThreads)
-    k_mg_tail(const __grid_constant__ MgTail tl, const float* __restrict__ om, const MixState* st) {
-  if (!mg_running(st)) return;
+    k_mg_tail(const __grid_constant__ MgTail tl, const float* __restrict__ om, const MixState* st, int ncase) {
+  bool any = false;
+  for (int k = 0; k < ncase; ++k) any = any || mg_running(st ? st + k : nullptr);
+  if (!any) return;
+  auto live = [&](int k) { return mg_running(st ? st + k : nullptr); };
   const int64_t gt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x, gs = (int64_t)gridDim.x * blockDim.x;
   float* xc[kMgMaxLevels];
-  // a thread per row where the level's rows fit the cluster's threads, else a thread per node
+  // a thread per (row, case) where the level's rows fit the cluster's threads, else a thread per (node, case)
   auto apply = [&](const MgTailLevel& v, const float* x, float* y, int mode, float w) {
-    if (3 * v.nn <= gs) {
-      for (int64_t t = gt; t < 3 * v.nn; t += gs) mg_apply_row(v.d, v.nn, t / 3, (int)(t % 3), v.S, x, v.r, v.invd, y, mode, w);
+    const int64_t nd = 3 * v.nn;
+    if (3 * v.nn * ncase <= gs) {
+      for (int64_t t = gt; t < nd * ncase; t += gs) {
+        const int64_t it = t / ncase;
+        const int k = (int)(t - it * ncase);
+        if (live(k))
+          mg_apply_row(v.d, v.nn, it / 3, (int)(it % 3), v.S, x + k * nd, v.r + k * nd, v.invd, y + k * nd, mode, w);
+      }
     } else {
-      for (int64_t n = gt; n < v.nn; n += gs) mg_apply_node(v.d, v.nn, n, v.S, x, v.r, v.invd, y, mode, w);
+      for (int64_t t = gt; t < v.nn * ncase; t += gs) {
+        const int64_t n = t / ncase;
+        const int k = (int)(t - n * ncase);
+        if (live(k)) mg_apply_node(v.d, v.nn, n, v.S, x + k * nd, v.r + k * nd, v.invd, y + k * nd, mode, w);
+      }
     }
   };
   for (int l = tl.T; l < tl.L - 1; ++l) {
     const MgTailLevel& v = tl.lv[l];
     const MgTailLevel& cv = tl.lv[l + 1];
+    const int64_t nd = 3 * v.nn, cnd = 3 * cv.nn;
     const float w = om[l];
     float *x = v.xa, *o = v.xb;  // x = omega invd r, written with r by the restriction into this level
     for (int k = 1; k < tl.sweeps; ++k) {
@@ -2289,32 +2335,47 @@ __global__ void __cluster_dims__(kMgTailCtas, 1, 1) __launch_bounds__(kMgTailThr
     mg_cluster_sync();
     const bool smoothed = l + 1 < tl.L - 1;  // the coarsest level is solved, not smoothed
     const float wc = smoothed ? om[l + 1] : 0.0f;
-    for (int64_t q = gt; q < 3 * cv.nn; q += gs)
-      mg_restrict_comp<false>(v.d, 0, nullptr, v.t, cv.d, cv.invd, cv.r, q / 3, (int)(q % 3),
-                              smoothed ? cv.xa : nullptr, wc);
+    for (int64_t q = gt; q < cnd * ncase; q += gs) {
+      const int64_t it = q / ncase;
+      const int k = (int)(q - it * ncase);
+      if (live(k))
+        mg_restrict_comp<false>(v.d, 0, nullptr, v.t + k * nd, cv.d, cv.invd, cv.r + k * cnd, it / 3, (int)(it % 3),
+                                smoothed ? cv.xa + k * cnd : nullptr, wc);
+    }
     mg_cluster_sync();
     xc[l] = x;
   }
-  {  // coarsest level: x = A^-1 r, one warp per row
+  {  // coarsest level: x = A^-1 r, one warp per (row, case)
     const MgTailLevel& v = tl.lv[tl.L - 1];
+    const int64_t nd = 3 * v.nn;
     const int lane = threadIdx.x & 31;
-    for (int64_t row = gt >> 5; row < tl.nc; row += gs >> 5) {
+    for (int64_t rc = gt >> 5; rc < (int64_t)tl.nc * ncase; rc += gs >> 5) {
+      const int64_t row = rc / ncase;
+      const int k = (int)(rc - row * ncase);
+      if (!live(k)) continue;
+      const float* r = v.r + k * nd;
       double acc = 0.0;
-      for (int col = lane; col < tl.nc; col += 32) acc = fma(tl.ainv[row * tl.nc + col], (double)v.r[col], acc);
+      for (int col = lane; col < tl.nc; col += 32) acc = fma(tl.ainv[row * tl.nc + col], (double)r[col], acc);
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-      if (lane == 0) v.xa[row] = (float)acc;
+      if (lane == 0) v.xa[k * nd + row] = (float)acc;
     }
     mg_cluster_sync();
     xc[tl.L - 1] = v.xa;
   }
   for (int l = tl.L - 2; l >= tl.T; --l) {
     const MgTailLevel& v = tl.lv[l];
+    const int64_t nd = 3 * v.nn, cnd = 3 * tl.lv[l + 1].nn;
     const float w = om[l];
     float* x = xc[l];
     float* o = x == v.xa ? v.xb : v.xa;
-    for (int64_t q = gt; q < 3 * v.nn; q += gs)
-      mg_prolong_comp<false>(v.d, 0, nullptr, v.invd, x, tl.lv[l + 1].d, xc[l + 1], q / 3, (int)(q % 3));
+    for (int64_t q = gt; q < nd * ncase; q += gs) {
+      const int64_t it = q / ncase;
+      const int k = (int)(q - it * ncase);
+      if (live(k))
+        mg_prolong_comp<false>(v.d, 0, nullptr, v.invd, x + k * nd, tl.lv[l + 1].d, xc[l + 1] + k * cnd, it / 3,
+                               (int)(it % 3));
+    }
     mg_cluster_sync();
     for (int k = 0; k < tl.sweeps; ++k) {
       apply(v, x, o, 1, w);
@@ -2326,8 +2387,14 @@ __global__ void __cluster_dims__(kMgTailCtas, 1, 1) __launch_bounds__(kMgTailThr
     xc[l] = x;
   }
   const MgTailLevel& vt = tl.lv[tl.T];
-  if (xc[tl.T] != vt.xa)
-    for (int64_t q = gt; q < 3 * vt.nn; q += gs) vt.xa[q] = xc[tl.T][q];
+  if (xc[tl.T] != vt.xa) {
+    const int64_t nd = 3 * vt.nn;
+    for (int64_t q = gt; q < nd * ncase; q += gs) {
+      const int64_t it = q / ncase;
+      const int k = (int)(q - it * ncase);
+      if (live(k)) vt.xa[k * nd + it] = xc[tl.T][k * nd + it];
+    }
+  }
 }
 
 // Outer step, part 1. mode 0: x += alpha p, r -= alpha q (FP64, padded layout), ||r|| against the stop and
@@ -2718,6 +2785,23 @@ struct MgHier {
   int T = 1;             // first level handled by the cluster kernel k_mg_tail
   MgTail tail{};
   bool prefers_f64 = false;  // an FP32 outer solve of this problem stalled: later ones start in FP64
+  // reuse of the coarse levels across solves on a changed E (see mg_needs_setup)
+  int fresh_iters = 0;   // outer iterations of the last solve right after a set-up
+  int last_iters = 0;    // outer iterations of the last solve
+  int reuses = 0;        // solves since the last set-up that kept an older hierarchy
+  int ncap = 1;          // load cases the level vectors have room for (case k at + k * nd)
+  // load cases solved together (mg_solve_cases): per case the FP32 work vectors x, r, z, p0, p1, ap, t of the
+  // voxel level, the TMA descriptors of r, z, p0, p1, one state per case, and the chunk graphs
+  struct CaseWork {
+    int n = 0;
+    float* v[kMgMaxCases][7] = {};
+    CUtensorMap tmap[kMgMaxCases][4];
+    MixState* st = nullptr;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int graph_profiled = -1;
+    int graph_n = 0;
+    int per_chunk = 0;  // kernel launches of one chunk graph
+  } cw;
   std::vector<void*> bufs;
 };
 
@@ -2736,12 +2820,13 @@ static int mg_levels(int nx, int ny, int nz, MgDims* out) {
   return (L >= 2 && 3 * mg_nn(out[L - 1]) <= kMgCoarseMax) ? L : 0;
 }
 
-int64_t mg_device_bytes(int nx, int ny, int nz) {
+int64_t mg_device_bytes(int nx, int ny, int nz, int n_cases, bool cases_together) {
   MgDims lv[kMgMaxLevels];
   const int L = mg_levels(nx, ny, nz, lv);
   if (!L) return 0;
+  const int nc = std::min(kMgMaxCases, std::max(1, n_cases));  // level vectors have room for the cases
   int64_t b = 0;
-  for (int l = 1; l < L; ++l) b += 4 * (9 * kMgHalf + 15) * mg_nn(lv[l]) + 6 * 64;
+  for (int l = 1; l < L; ++l) b += 4 * (9 * kMgHalf + 3 + 12 * nc) * mg_nn(lv[l]) + 6 * 64;
   b += sizeof(MgScratch) + 64 + 4 * 8 * 576 + 64 + (int64_t)lv[1].nx * lv[1].ny * lv[1].nz + 64;
   const int64_t rp = (3 * (int64_t)(nx + 1) + 3) & ~int64_t(3);  // FP32 row pitch of the voxel level
   b += 4 * rp * (ny + 1) * (nz + 1) + 64;                         // f_t
@@ -2750,6 +2835,8 @@ int64_t mg_device_bytes(int nx, int ny, int nz) {
   b += 4 * 576 * (int64_t)lv[1].nx * lv[1].ny * lv[1].nz + 64;
   if (L > 2) b += 4 * 576 * (int64_t)lv[2].nx * lv[2].ny * lv[2].nz + 64;
   b += 8 * 9 * mg_nn(lv[L - 1]) * mg_nn(lv[L - 1]) + 64;
+  if (cases_together && n_cases > 1 && n_cases <= kMgMaxCases)  // the cases' voxel-level vectors and states
+    b += (int64_t)n_cases * (7 * (4 * rp * (ny + 1) * (nz + 1) + 64) + (int64_t)sizeof(MixState));
   return b;
 }
 
@@ -2764,7 +2851,9 @@ void mg_release(mycel_problem* p) {
       if (mg->ev32[k][j]) cudaEventDestroy(mg->ev32[k][j]);
       if (mg->l1ev[k][j]) cudaEventDestroy(mg->l1ev[k][j]);
     }
+    if (mg->cw.graph[k]) cudaGraphExecDestroy(mg->cw.graph[k]);
   }
+  p->n_case_tmaps = 0;
   for (void* b : mg->bufs) cudaFreeAsync(b, p->ctx->stream);
   delete mg;
   p->mg = nullptr;
@@ -2788,6 +2877,7 @@ static int32_t mg_ensure(mycel_problem* p, bool* available) {
   if (!L) return MYCEL_OK;
   MgHier* mg = new MgHier();
   mg->L = L;
+  mg->ncap = std::min(kMgMaxCases, std::max(1, (int)p->n_cases));
   if (const char* e = std::getenv("MYCEL_MG_SWEEPS")) mg->sweeps = std::max(1, std::atoi(e));
   cudaStream_t s = p->ctx->stream;
   bool oom = false;
@@ -2809,8 +2899,9 @@ static int32_t mg_ensure(mycel_problem* p, bool* available) {
     v.nd = 3 * v.nn;
     if (l == 0) continue;
     v.S = (float*)alloc(sizeof(float) * 9 * kMgHalf * v.nn);
-    float** vecs[] = {&v.invd, &v.xa, &v.xb, &v.r, &v.t};
-    for (float** q : vecs) *q = (float*)alloc(sizeof(float) * v.nd);
+    v.invd = (float*)alloc(sizeof(float) * v.nd);
+    float** vecs[] = {&v.xa, &v.xb, &v.r, &v.t};
+    for (float** q : vecs) *q = (float*)alloc(sizeof(float) * v.nd * mg->ncap);
   }
   for (int k = 0; k < 2 && k + 1 < L; ++k) {
     const MgDims& d = mg->lv[k + 1].d;
@@ -2887,12 +2978,51 @@ static unsigned mg_blocks(int64_t n) { return (unsigned)((n + 255) / 256); }
 
 // coarse-level product on the stream: a thread per DOF up to 64k nodes, a thread per node above (measured on
 // the bridge: level 2, 31k nodes, 9.6 vs 14.5 us; level 1, 233k nodes, 43 vs 51 us)
-static void launch_mg_apply(cudaStream_t s, const MgLevel& v, const float* x, const float* r, const float* invd,
-                            float* y, int mode, const float* om, const MixState* st) {
-  if (v.nn <= 65536)
-    k_mg_apply<<<mg_dof_blocks(v.nn), kMgDofThreads, 0, s>>>(v.d, v.S, x, r, invd, y, mode, om, st);
+// case k's vector of a level whose case vectors follow one another (base + k * nd)
+static MgPtrs lv_ptrs(float* base, int64_t nd, int n) {
+  MgPtrs r{};
+  for (int k = 0; k < n; ++k) r.p[k] = base ? base + k * nd : nullptr;
+  return r;
+}
+
+static void launch_mg_apply(cudaStream_t s, const MgLevel& v, const MgPtrs& x, const MgPtrs& r, const float* invd,
+                            const MgPtrs& y, int mode, const float* om, const MixState* st, int nc) {
+  if (v.nn * nc <= 65536)
+    k_mg_apply<<<mg_dof_blocks(v.nn * nc), kMgDofThreads, 0, s>>>(v.d, v.S, x, r, invd, y, mode, om, st, nc);
   else
-    k_mg_apply_nodes<<<mg_blocks(v.nn), 256, 0, s>>>(v.d, v.S, x, r, invd, y, mode, om, st);
+    k_mg_apply_nodes<<<mg_blocks(v.nn * nc), 256, 0, s>>>(v.d, v.S, x, r, invd, y, mode, om, st, nc);
+}
+
+// The load cases one V-cycle advances: their states (one per case, contiguous) and their voxel-level vectors
+// (padded FP32 layout): residual rf, first sweep / correction xf (a mapped matvec input) and tf = A xf.
+struct MgRun {
+  int n = 1;
+  MixState* st = nullptr;
+  float* rf[kMgMaxCases] = {};
+  float* xf[kMgMaxCases] = {};
+  float* tf[kMgMaxCases] = {};
+};
+static MgPtrs mg_ptrs(float* const (&v)[kMgMaxCases], int n) {
+  MgPtrs r{};
+  for (int k = 0; k < n; ++k) r.p[k] = v[k];
+  return r;
+}
+
+// Whether a solve on a changed E rebuilds the coarse levels. The outer iteration is flexible CG on the current
+// operator, so a hierarchy built from an earlier E still gives the solution to the same tolerance, only the
+// iteration count can grow. A SIMP design changes a little from one solve to the next: the hierarchy is kept
+// while the last solve needed at most kMgReuseSlack times the iterations of the last solve right after a
+// set-up, for at most kMgMaxReuse solves in a row. Decided on iteration counts only (deterministic, the same
+// whatever else runs). MYCEL_MG_REUSE=0 rebuilds at every change of E.
+constexpr double kMgReuseSlack = 1.25;
+constexpr int kMgMaxReuse = 3;
+static bool mg_needs_setup(const MgHier* mg) {
+  static const bool allow = [] {
+    const char* e = std::getenv("MYCEL_MG_REUSE");
+    return !(e && e[0] == '0');
+  }();
+  if (!allow || mg->fresh_iters <= 0 || mg->reuses >= kMgMaxReuse) return true;
+  return (double)mg->last_iters > kMgReuseSlack * mg->fresh_iters;
 }
 
 // Coarse operators from the current E: Galerkin element matrices level by level, their stencils, and the
@@ -2935,7 +3065,7 @@ static void mg_setup(mycel_problem* p) {
     }
     const int iters = mg->eig_valid ? kMgPowerItersWarm : kMgPowerIters;
     for (int it = 0; it < iters; ++it) {
-      if (l) launch_mg_apply(s, v, x, nullptr, invd, y, 0, nullptr, nullptr);
+      if (l) launch_mg_apply(s, v, mg_one(x), mg_one(nullptr), invd, mg_one(y), 0, nullptr, nullptr, 1);
       else launch_mv32_variant<0>(p, s, p->f_p0, nullptr, nullptr, nullptr, p->f_ap, 1, nullptr, nullptr);
       const bool last = it == iters - 1;
       k_mg_pow_norm<<<nb, kT, 0, s>>>(n, y, invd, p->d_part2, mg->sc, last ? l : -1);
@@ -2947,68 +3077,85 @@ static void mg_setup(mycel_problem* p) {
   p->ctx->launches += nl;
 }
 
-// One V-cycle from the voxel level's residual rf and first sweep xf (written by k_mg_enter*) up to tf = A xf
-// before the last sweep (done by k_mg_exit*). xf is a mapped FP32 matvec input. Returns the kernels launched.
-static int mg_vcycle(mycel_problem* p, cudaStream_t s, MixState* st, float* rf, float* xf, float* tf) {
+// One V-cycle for the cases of R: from each case's voxel-level residual rf and first sweep xf (written by
+// k_mg_enter*) up to tf = A xf before the last sweep (done by k_mg_exit*). Voxel-level work runs per case; the
+// coarse levels run once for all cases. Returns the kernels launched.
+static int mg_vcycle(mycel_problem* p, cudaStream_t s, const MgRun& R) {
   MgHier* mg = p->mg;
   MgLevel* lv = mg->lv;
   const GridDims& g = p->g;
   const float* om = mg->sc->omega;  // device: damping of level l at om + l
   const int sb = stream_blocks(p);
+  const int nc = R.n;
+  MixState* st = R.st;
+  auto cst = [&](int k) { return st ? st + k : nullptr; };
   int nl = 0;
-  auto fine_mv = [&] { launch_mv32_variant<0>(p, s, xf, nullptr, nullptr, nullptr, tf, 1, st, nullptr); };
-  for (int k = 1; k < mg->sweeps; ++k) {
-    fine_mv();
-    k_mg_jacobi_fine<<<sb, kT, 0, s>>>(g.n32, rf, tf, p->d_invdf, xf, om, st);
-    nl += 2;
-  }
-  fine_mv();
+  auto fine_mv = [&](int k) {
+    launch_mv32_variant<0>(p, s, R.xf[k], nullptr, nullptr, nullptr, R.tf[k], 1, cst(k), nullptr);
+  };
+  for (int q = 1; q < mg->sweeps; ++q)
+    for (int k = 0; k < nc; ++k) {
+      fine_mv(k);
+      k_mg_jacobi_fine<<<sb, kT, 0, s>>>(g.n32, R.rf[k], R.tf[k], p->d_invdf, R.xf[k], om, cst(k));
+      nl += 2;
+    }
+  for (int k = 0; k < nc; ++k) fine_mv(k);
+  nl += nc;
   // restriction to level 1, with level 1's first sweep (unless level 1 is the coarsest)
-  k_mg_restrict<true><<<mg_blocks(lv[1].nn), 256, 0, s>>>(lv[0].d, g.rp, rf, tf, lv[1].d, lv[1].invd, lv[1].r, st,
-                                                          1 < mg->L - 1 ? lv[1].xa : nullptr, om + 1);
-  nl += 2;
+  k_mg_restrict<true><<<mg_blocks(lv[1].nn * nc), 256, 0, s>>>(lv[0].d, g.rp, mg_ptrs(R.rf, nc), mg_ptrs(R.tf, nc),
+                                                               lv[1].d, lv[1].invd, lv_ptrs(lv[1].r, lv[1].nd, nc), st,
+                                                               lv_ptrs(lv[1].xa, lv[1].nd, nc), 1 < mg->L - 1 ? 1 : 0,
+                                                               om + 1, nc);
+  nl++;
   float* xc[kMgMaxLevels] = {};
   for (int l = 1; l < mg->T; ++l) {
     MgLevel& v = lv[l];
     float *x = v.xa, *o = v.xb;
+    const MgPtrs r = lv_ptrs(v.r, v.nd, nc);
     for (int k = 1; k < mg->sweeps; ++k) {
-      launch_mg_apply(s, v, x, v.r, v.invd, o, 1, om + l, st);
+      launch_mg_apply(s, v, lv_ptrs(x, v.nd, nc), r, v.invd, lv_ptrs(o, v.nd, nc), 1, om + l, st, nc);
       std::swap(x, o);
     }
     if (l == 1 && mg->l1_timing) cudaEventRecordWithFlags(mg->l1_timing[0], s, cudaEventRecordExternal);
-    launch_mg_apply(s, v, x, v.r, v.invd, v.t, 2, om + l, st);
+    launch_mg_apply(s, v, lv_ptrs(x, v.nd, nc), r, v.invd, lv_ptrs(v.t, v.nd, nc), 2, om + l, st, nc);
     if (l == 1 && mg->l1_timing) cudaEventRecordWithFlags(mg->l1_timing[1], s, cudaEventRecordExternal);
-    k_mg_restrict<false><<<mg_blocks(lv[l + 1].nn), 256, 0, s>>>(v.d, 0, nullptr, v.t, lv[l + 1].d, lv[l + 1].invd,
-                                                                 lv[l + 1].r, st,
-                                                                 l + 1 < mg->L - 1 ? lv[l + 1].xa : nullptr,
-                                                                 om + l + 1);
+    MgLevel& cv = lv[l + 1];
+    k_mg_restrict<false><<<mg_blocks(cv.nn * nc), 256, 0, s>>>(v.d, 0, lv_ptrs(nullptr, 0, nc),
+                                                               lv_ptrs(v.t, v.nd, nc), cv.d, cv.invd,
+                                                               lv_ptrs(cv.r, cv.nd, nc), st,
+                                                               lv_ptrs(cv.xa, cv.nd, nc), l + 1 < mg->L - 1 ? 1 : 0,
+                                                               om + l + 1, nc);
     xc[l] = x;
     nl += 1 + mg->sweeps;
   }
-  k_mg_tail<<<kMgTailCtas, kMgTailThreads, 0, s>>>(mg->tail, om, st);
+  k_mg_tail<<<kMgTailCtas, kMgTailThreads, 0, s>>>(mg->tail, om, st, nc);
   xc[mg->T] = lv[mg->T].xa;
   nl++;
   for (int l = mg->T - 1; l >= 1; --l) {
     MgLevel& v = lv[l];
     float* x = xc[l];
     float* o = x == v.xa ? v.xb : v.xa;
-    k_mg_prolong<false><<<mg_blocks(v.nn), 256, 0, s>>>(v.d, 0, nullptr, v.invd, x, lv[l + 1].d, xc[l + 1], st);
+    k_mg_prolong<false><<<mg_blocks(v.nn * nc), 256, 0, s>>>(v.d, 0, nullptr, v.invd, lv_ptrs(x, v.nd, nc), lv[l + 1].d,
+                                                              lv_ptrs(xc[l + 1], lv[l + 1].nd, nc), st, nc);
+    const MgPtrs r = lv_ptrs(v.r, v.nd, nc);
     for (int k = 0; k < mg->sweeps; ++k) {
-      launch_mg_apply(s, v, x, v.r, v.invd, o, 1, om + l, st);
+      launch_mg_apply(s, v, lv_ptrs(x, v.nd, nc), r, v.invd, lv_ptrs(o, v.nd, nc), 1, om + l, st, nc);
       std::swap(x, o);
     }
     xc[l] = x;
     nl += 1 + mg->sweeps;
   }
-  k_mg_prolong<true><<<mg_blocks(lv[0].nn), 256, 0, s>>>(lv[0].d, g.rp, p->d_nflags, nullptr, xf, lv[1].d, xc[1], st);
+  k_mg_prolong<true><<<mg_blocks(lv[0].nn * nc), 256, 0, s>>>(lv[0].d, g.rp, p->d_nflags, nullptr, mg_ptrs(R.xf, nc),
+                                                              lv[1].d, lv_ptrs(xc[1], lv[1].nd, nc), st, nc);
   nl++;
-  for (int k = 1; k < mg->sweeps; ++k) {
-    fine_mv();
-    k_mg_jacobi_fine<<<sb, kT, 0, s>>>(g.n32, rf, tf, p->d_invdf, xf, om, st);
-    nl += 2;
-  }
-  fine_mv();
-  return nl + 1;
+  for (int q = 1; q < mg->sweeps; ++q)
+    for (int k = 0; k < nc; ++k) {
+      fine_mv(k);
+      k_mg_jacobi_fine<<<sb, kT, 0, s>>>(g.n32, R.rf[k], R.tf[k], p->d_invdf, R.xf[k], om, cst(k));
+      nl += 2;
+    }
+  for (int k = 0; k < nc; ++k) fine_mv(k);
+  return nl + nc;
 }
 
 // The outer step after the matvec (mode 0), or the preconditioned residual after a start (2) or a true-residual
@@ -3024,16 +3171,24 @@ static int launch_mg_step(mycel_problem* p, cudaStream_t s, const void* pcur, in
     k_mix_set<<<1, 1, 0, s>>>(st, MIX_RUNNING);
     nl++;
   }
+  MgRun R;
+  R.st = st;
   if (f64) {
     k_mg_enter<<<sb, kT, 0, s>>>(p->g, p->g_x, p->g_r, (const double*)pcur, p->g_ap, p->d_invdf, p->f_r, p->f_p0, om,
                                  st, p->d_part2, mode);
-    nl += 1 + mg_vcycle(p, s, st, p->f_r, p->f_p0, p->f_ap);
+    R.rf[0] = p->f_r;
+    R.xf[0] = p->f_p0;
+    R.tf[0] = p->f_ap;
+    nl += 1 + mg_vcycle(p, s, R);
     k_mg_exit<<<sb, kT, 0, s>>>(p->g, p->f_r, p->f_ap, p->f_p0, p->d_invdf, p->g_r, p->g_ap, p->g_z, om, st,
                                 p->d_part2, mode);
   } else {
     k_mg_enter32<<<sb, kT, 0, s>>>(p->g.n32, p->f_x, p->f_r, (const float*)pcur, p->f_ap, p->d_invdf, p->f_z, om, st,
                                    p->d_part2, mode);
-    nl += 1 + mg_vcycle(p, s, st, p->f_r, p->f_z, mg->f_t);
+    R.rf[0] = p->f_r;
+    R.xf[0] = p->f_z;
+    R.tf[0] = mg->f_t;
+    nl += 1 + mg_vcycle(p, s, R);
     k_mg_exit32<<<sb, kT, 0, s>>>(p->g.n32, p->f_r, mg->f_t, p->f_z, p->d_invdf, p->f_ap, om, st, p->d_part2, mode);
   }
   return nl + 1;
@@ -3101,8 +3256,9 @@ static int launch_inner_xr(mycel_problem* p, const InnerForm& F, cudaStream_t s,
 }
 
 // Chunk of inner iterations as a graph; p alternates between two buffers (even chunk length, each chunk starts
-// from the direction held in p1). When the context profiles, the first matvec of a chunk is launched directly
-// between two stream events (outside the graph) and the graph holds the rest of the chunk.
+// from the direction held in p1). When the context profiles, the graph also records events around the chunk's
+// first matvec (and, in the multigrid forms, around its first level-1 product), so the kernels are timed where
+// they run.
 static int32_t capture_inner_graph(mycel_problem* p, const InnerForm& F, int chunk) {
   mycel_ctx* c = p->ctx;
   if (F.graph[0] && *F.graph_profiled == c->profile) return MYCEL_OK;
@@ -3125,7 +3281,14 @@ static int32_t capture_inner_graph(mycel_problem* p, const InnerForm& F, int chu
     for (int t = 0; t < chunk; ++t) {
       void* pcur = (t & 1) ? F.p1 : F.p0;
       void* pprev = (t & 1) ? F.p0 : F.p1;
-      if (!(c->profile && t == 0)) launch_inner_mv(p, F, s, pprev, pcur);
+      if (c->profile && t == 0) {
+        // timed in place: event-record nodes around the chunk's first matvec, inside the graph
+        cudaEventRecordWithFlags(F.ev[k][0], s, cudaEventRecordExternal);
+        launch_inner_mv(p, F, s, pprev, pcur);
+        cudaEventRecordWithFlags(F.ev[k][1], s, cudaEventRecordExternal);
+      } else {
+        launch_inner_mv(p, F, s, pprev, pcur);
+      }
       if (mg) mg->l1_timing = (c->profile && t == 0 && mg->T > 1) ? mg->l1ev[k] : nullptr;
       launch_inner_xr(p, F, s, pcur, 0);
       if (mg) mg->l1_timing = nullptr;
@@ -3140,14 +3303,7 @@ static int32_t capture_inner_graph(mycel_problem* p, const InnerForm& F, int chu
 }
 
 static void launch_inner_chunk(mycel_problem* p, const InnerForm& F, int gi) {
-  mycel_ctx* c = p->ctx;
-  cudaStream_t s = c->stream;
-  if (*F.graph_profiled) {
-    cudaEventRecord(F.ev[gi][0], s);
-    launch_inner_mv(p, F, s, F.p1, F.p0);
-    cudaEventRecord(F.ev[gi][1], s);
-  }
-  cudaGraphLaunch(F.graph[gi], s);
+  cudaGraphLaunch(F.graph[gi], p->ctx->stream);
 }
 
 // r_work = P(b - A u) in FP64 (then rounded to the form's type), returns ||r|| (synchronises). A u comes from
@@ -3360,9 +3516,14 @@ int32_t refined_solve_entry(mycel_problem* p, const double* d_b, const int32_t* 
     if ((st = resolve_mv32(p)) || (st = mg_ensure(p, &avail))) return st;
     if (avail) {
       ran_mg = true;
-      if (p->mg->setup_version != p->e_version) {  // solves on an unchanged E (load cases) share the set-up
+      bool fresh = false;
+      if (p->mg->setup_version != p->e_version && mg_needs_setup(p->mg)) {
         mg_setup(p);
         p->mg->setup_version = p->e_version;
+        p->mg->reuses = 0;
+        fresh = true;
+      } else if (p->mg->setup_version != p->e_version) {
+        p->mg->reuses++;
       }
       // MYCEL_PRECISION_MIXED_MG: the FP32 outer iteration first (unless one of this problem's solves stalled
       // in it), then the FP64 outer iteration from the refined u
@@ -3386,6 +3547,8 @@ int32_t refined_solve_entry(mycel_problem* p, const double* d_b, const int32_t* 
       }
       if (ok && lmg.iterations + lmg32.iterations == 0 && lmg.flushes + lmg32.flushes == 0)
         std::snprintf(res->message, sizeof res->message, "Initial guess already converged.");
+      p->mg->last_iters = ok ? lmg32.iterations + lmg.iterations : INT32_MAX;
+      if (fresh) p->mg->fresh_iters = p->mg->last_iters;
     }
   }
   // Which inner form a mixed solve starts in. Once a mixed solve of a problem has stalled (its designs have
@@ -3466,6 +3629,363 @@ int32_t refined_solve_entry(mycel_problem* p, const double* d_b, const int32_t* 
     std::snprintf(res->message, sizeof res->message,
                   "PCG reached maximum iterations without converging. Is the model not sufficiently constrained?");
   res->elapsed_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  return MYCEL_OK;
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// Load cases kept apart, solved together (mixed multigrid form). The cases share K: their outer FP32
+// flexible CG iterations run side by side in the same chunk graphs, each with its own state (alpha, beta,
+// residual, status), and one V-cycle serves all of them: the voxel-level products run per case, the coarse
+// levels (restriction, stencil products, the cluster kernel, prolongation) once for all cases, loading each
+// stencil entry once per node. Every case's arithmetic is that of its solve alone.
+// A round runs the chunks until no case is running (each has reached its true-residual replacement point or a
+// final state); then every case is refined in FP64 (u += x, r = P(b - A u)) and those not yet converged
+// restart together. A case that stalls, breaks down or runs out of iterations is finished afterwards, alone,
+// by refined_solve_entry from its refined u (FP64 multigrid, then the fast FP64 and plain forms).
+// ---------------------------------------------------------------------------------------------------------
+static int32_t mg_ensure_cases(mycel_problem* p, int n) {
+  MgHier* mg = p->mg;
+  auto& cw = mg->cw;
+  if (cw.n >= n) return MYCEL_OK;
+  if (cw.n > 0 || n > mg->ncap) return set_error(p->ctx, MYCEL_E_ARG, "multigrid case workspace: too many cases");
+  cudaStream_t s = p->ctx->stream;
+  const size_t fb = sizeof(float) * (size_t)p->g.n32 + 64;
+  for (int k = 0; k < n; ++k)
+    for (int q = 0; q < 7; ++q) {
+      void* b = nullptr;
+      if (cudaMallocAsync(&b, fb, s) != cudaSuccess)
+        return set_error(p->ctx, MYCEL_E_OOM, "out of device memory for the load cases' multigrid workspace");
+      cudaMemsetAsync(b, 0, fb, s);
+      p->device_bytes += (int64_t)fb;
+      mg->bufs.push_back(b);
+      cw.v[k][q] = (float*)b;
+    }
+  void* st = nullptr;
+  if (cudaMallocAsync(&st, sizeof(MixState) * n, s) != cudaSuccess)
+    return set_error(p->ctx, MYCEL_E_OOM, "out of device memory for the load cases' multigrid workspace");
+  cudaMemsetAsync(st, 0, sizeof(MixState) * n, s);
+  p->device_bytes += (int64_t)(sizeof(MixState) * n);
+  mg->bufs.push_back(st);
+  cw.st = (MixState*)st;
+  for (int k = 0; k < n; ++k)
+    for (int q = 0; q < 4; ++q) {  // r, z, p0, p1 are matvec inputs
+      int32_t e = encode_plane_map(p, cw.v[k][1 + q], false, &cw.tmap[k][q]);
+      if (e) return e;
+      p->case_tmap_ptr[p->n_case_tmaps] = cw.v[k][1 + q];
+      p->case_tmap[p->n_case_tmaps] = &cw.tmap[k][q];
+      p->n_case_tmaps++;
+    }
+  cw.n = n;
+  return MYCEL_OK;
+}
+
+// vector q of case k: 0 x, 1 r, 2 z, 3 p0, 4 p1, 5 ap, 6 t
+static float* cwv(MgHier* mg, int k, int q) { return mg->cw.v[k][q]; }
+
+// One outer step of every case (mode 0: after the matvec; 1: after a replacement; 2: start): k_mg_enter32 per
+// case, one V-cycle for all, k_mg_exit32 per case. Returns the kernels launched.
+static int launch_mg_step_cases(mycel_problem* p, cudaStream_t s, int n, const int* pcur_sel, int mode) {
+  MgHier* mg = p->mg;
+  const int sb = stream_blocks(p);
+  const float* om = mg->sc->omega;
+  MgRun R;
+  R.n = n;
+  R.st = mg->cw.st;
+  int nl = 0;
+  for (int k = 0; k < n; ++k) {
+    float* pcur = cwv(mg, k, 3 + pcur_sel[k]);
+    k_mg_enter32<<<sb, kT, 0, s>>>(p->g.n32, cwv(mg, k, 0), cwv(mg, k, 1), pcur, cwv(mg, k, 5), p->d_invdf,
+                                   cwv(mg, k, 2), om, R.st + k, p->d_part2, mode);
+    R.rf[k] = cwv(mg, k, 1);
+    R.xf[k] = cwv(mg, k, 2);
+    R.tf[k] = cwv(mg, k, 6);
+    nl++;
+  }
+  nl += mg_vcycle(p, s, R);
+  for (int k = 0; k < n; ++k) {
+    k_mg_exit32<<<sb, kT, 0, s>>>(p->g.n32, cwv(mg, k, 1), cwv(mg, k, 6), cwv(mg, k, 2), p->d_invdf, cwv(mg, k, 5), om,
+                                  R.st + k, p->d_part2, mode);
+    nl++;
+  }
+  return nl;
+}
+
+// chunk graphs of the cases (two iterations each; p alternates between p0 and p1 as in the single solve)
+static int32_t capture_cases_graph(mycel_problem* p, int n) {
+  mycel_ctx* c = p->ctx;
+  MgHier* mg = p->mg;
+  auto& cw = mg->cw;
+  if (cw.graph[0] && cw.graph_profiled == c->profile && cw.graph_n == n) return MYCEL_OK;
+  for (int k = 0; k < 2; ++k) {
+    if (cw.graph[k]) cudaGraphExecDestroy(cw.graph[k]);
+    cw.graph[k] = nullptr;
+  }
+  cudaStream_t s = c->stream;
+  const int64_t before = c->launches;
+  for (int g = 0; g < 2; ++g) {
+    cudaGraph_t graph;
+    MYCEL_CUDA(c, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    int nl = 0;
+    for (int t = 0; t < 2; ++t) {
+      int sel[kMgMaxCases];
+      for (int k = 0; k < n; ++k) {
+        float* pcur = cwv(mg, k, (t & 1) ? 4 : 3);
+        float* pprev = cwv(mg, k, (t & 1) ? 3 : 4);
+        launch_mv32_variant<1>(p, s, nullptr, cwv(mg, k, 2), pprev, pcur, cwv(mg, k, 5), 1, cw.st + k, p->d_part2);
+        sel[k] = t & 1;
+        nl++;
+      }
+      nl += launch_mg_step_cases(p, s, n, sel, 0);
+    }
+    cw.per_chunk = nl;
+    MYCEL_CUDA(c, cudaStreamEndCapture(s, &graph));
+    MYCEL_CUDA(c, cudaGraphInstantiate(&cw.graph[g], graph, 0));
+    cudaGraphDestroy(graph);
+  }
+  c->launches = before;
+  cw.graph_profiled = c->profile;
+  cw.graph_n = n;
+  return MYCEL_OK;
+}
+
+__global__ void k_mix_set_if(MixState* st, int from, int to) {
+  if (st->status == from) st->status = to;
+}
+
+bool cases_together_enabled() {
+  const char* e = std::getenv("MYCEL_CASES_TOGETHER");  // "0": one case after another (for comparisons)
+  return !(e && e[0] == '0');
+}
+
+int32_t mg_solve_cases(mycel_problem* p, int ncase, double* d_u, double tol, int max_iter,
+                       const volatile int32_t* cancel, mycel_pcg_result* res) {
+  mycel_ctx* c = p->ctx;
+  cudaStream_t s = c->stream;
+  auto t0 = std::chrono::steady_clock::now();
+  const int64_t nd = p->g.nd;
+  for (int k = 0; k < ncase; ++k) std::memset(res + k, 0, sizeof(mycel_pcg_result));
+  if (p->n_active_fixed < 6)
+    return set_error(c, MYCEL_E_UNDERCONSTRAINED,
+                     "Model has fewer than 6 unique fixed DOFs on active nodes (found " +
+                         std::to_string(p->n_active_fixed) +
+                         "). At least 6 fixed DOFs are required to prevent rigid body modes in 3D.");
+  if (ncase < 1 || ncase > kMgMaxCases) return set_error(c, MYCEL_E_ARG, "batched multigrid solve: case count");
+  int32_t st = ensure_pcg_workspace(p);
+  if (st || (st = ensure_mixed(p)) || (st = ensure_f64f(p))) return st;
+  bool avail = false;
+  if ((st = resolve_mv32(p)) || (st = mg_ensure(p, &avail))) return st;
+  auto solve_alone = [&](int k, int budget, int precision) -> int32_t {
+    const double* b = p->d_case_b + (int64_t)k * nd;
+    const int32_t* nz = p->d_case_nz + p->case_nz_off[2 * k + 1];
+    return refined_solve_entry(p, b, nz, p->case_nz_cnt[2 * k + 1], d_u + k * nd, tol, budget, cancel, precision,
+                               res + k);
+  };
+  if (!avail || p->mg->prefers_f64 || ncase > p->mg->ncap) {  // no batched form here: one case after another
+    for (int k = 0; k < ncase; ++k)
+      if ((st = solve_alone(k, max_iter, MYCEL_PRECISION_MIXED_MG))) return st;
+    return MYCEL_OK;
+  }
+  MgHier* mg = p->mg;
+  if ((st = mg_ensure_cases(p, ncase))) return st;
+  // per case: project u, ||P b||, the true residual; cases with a zero right-hand side or already converged
+  // take no part
+  double bnorm[kMgMaxCases] = {}, rel[kMgMaxCases] = {};
+  bool active[kMgMaxCases] = {}, ok[kMgMaxCases] = {}, stalled[kMgMaxCases] = {};
+  int iters[kMgMaxCases] = {}, flushes[kMgMaxCases] = {}, resume[kMgMaxCases] = {};
+  double* saved_b = p->d_b;
+  int32_t* saved_nz = p->d_bnz;
+  int32_t saved_n = p->n_bnz;
+  struct Restore {
+    mycel_problem* p; double* b; int32_t* nz; int32_t n;
+    ~Restore() { p->d_b = b; p->d_bnz = nz; p->n_bnz = n; }
+  } restore{p, saved_b, saved_nz, saved_n};
+  auto bind = [&](int k) {
+    p->d_b = p->d_case_b + (int64_t)k * nd;
+    p->d_bnz = p->d_case_nz + p->case_nz_off[2 * k + 1];
+    p->n_bnz = p->case_nz_cnt[2 * k + 1];
+  };
+  auto form = [&](int k) {  // the single-solve form with case k's vectors (for the true residual)
+    InnerForm F = inner_form_mg(p, false);
+    F.x = cwv(mg, k, 0);
+    F.r = cwv(mg, k, 1);
+    F.z = cwv(mg, k, 2);
+    F.p0 = cwv(mg, k, 3);
+    F.p1 = cwv(mg, k, 4);
+    F.ap = cwv(mg, k, 5);
+    return F;
+  };
+  MYCEL_CUDA(c, cudaMemsetAsync(p->d_err, 0, sizeof(int), s));
+  // one stiffness: the hierarchy is rebuilt (or kept) as for a single solve
+  bool fresh = false;
+  if (mg->setup_version != p->e_version && mg_needs_setup(mg)) {
+    mg_setup(p);
+    mg->setup_version = p->e_version;
+    mg->reuses = 0;
+    fresh = true;
+  } else if (mg->setup_version != p->e_version) {
+    mg->reuses++;
+  }
+  PcgState* hs = (PcgState*)c->pinned;
+  int nact = 0;
+  for (int k = 0; k < ncase; ++k) {
+    bind(k);
+    double* u = d_u + k * nd;
+    cudaMemsetAsync(p->d_state, 0, sizeof(PcgState), s);
+    launch_project_x(p, u, &p->d_state->nonzero_x);
+    launch_pcg_bnorm(p);
+    MYCEL_CUDA(c, cudaMemcpyAsync(hs, p->d_state, sizeof(PcgState), cudaMemcpyDeviceToHost, s));
+    MYCEL_CUDA(c, cudaStreamSynchronize(s));
+    bnorm[k] = hs->bnorm;
+    if (bnorm[k] <= 1e-30) {
+      MYCEL_CUDA(c, cudaMemsetAsync(u, 0, sizeof(double) * nd, s));
+      res[k].converged = 1;
+      std::snprintf(res[k].message, sizeof res[k].message, "RHS is zero. Solution is zero.");
+      ok[k] = true;
+      continue;
+    }
+    double rn = 0.0;
+    if ((st = true_residual(p, form(k), p->d_b, u, &rn))) return st;
+    rel[k] = rn / bnorm[k];
+    if (rel[k] <= tol) {
+      ok[k] = true;
+      std::snprintf(res[k].message, sizeof res[k].message, "Initial guess already converged.");
+      continue;
+    }
+    cudaMemsetAsync(cwv(mg, k, 0), 0, sizeof(float) * (size_t)p->g.n32, s);
+    k_mix_init<<<1, 1, 0, s>>>(mg->cw.st + k, 0.5 * tol * bnorm[k], max_iter, 1e-3);
+    c->launches++;
+    active[k] = true;
+    ++nact;
+  }
+  for (int k = 0; k < ncase; ++k)
+    if (!active[k]) {  // not running: every batched kernel skips the case
+      k_mix_set<<<1, 1, 0, s>>>(mg->cw.st + k, MIX_DONE);
+      c->launches++;
+    }
+  if (nact > 0) {
+    if ((st = capture_cases_graph(p, ncase))) return st;
+    int sel[kMgMaxCases] = {};
+    c->launches += launch_mg_step_cases(p, s, ncase, sel, 2);
+  }
+  MixState* slot[2] = {(MixState*)((char*)c->pinned + 2048), (MixState*)((char*)c->pinned + 2048 + 2048)};
+  static_assert(sizeof(MixState) * kMgMaxCases <= 2048, "pinned state slots");
+  cudaEvent_t evs[2];
+  cudaEventCreateWithFlags(&evs[0], cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&evs[1], cudaEventDisableTiming);
+  struct EvGuard { cudaEvent_t* e; ~EvGuard() { cudaEventDestroy(e[0]); cudaEventDestroy(e[1]); } } evg{evs};
+  const int64_t stall_floor = 300;
+  int64_t cycle_limit[kMgMaxCases];
+  for (int k = 0; k < ncase; ++k) cycle_limit[k] = stall_floor;
+  const int64_t cap = (int64_t)max_iter + 64 * 2 + 4096;
+  int64_t launched = 0;
+  while (nact > 0) {
+    // chunks until no case runs (pipelined: chunk k is queued while the states after chunk k-1 are read)
+    for (int64_t k = 0;; ++k) {
+      if (cancel && *cancel) {
+        cudaStreamSynchronize(s);
+        return set_error(c, MYCEL_E_CANCELLED, "The operation was canceled.");
+      }
+      if (launched > cap) {
+        cudaStreamSynchronize(s);
+        return set_error(c, MYCEL_E_TIMEOUT, "batched inner PCG device state did not reach a final status");
+      }
+      const int gi = (int)(k & 1);
+      cudaGraphLaunch(mg->cw.graph[gi], s);
+      MYCEL_CUDA(c, cudaGetLastError());
+      launched += 2;
+      c->launches += mg->cw.per_chunk;
+      MYCEL_CUDA(c, cudaMemcpyAsync(slot[gi], mg->cw.st, sizeof(MixState) * ncase, cudaMemcpyDeviceToHost, s));
+      MYCEL_CUDA(c, cudaEventRecord(evs[gi], s));
+      if (k == 0) continue;
+      const int pi = (int)((k - 1) & 1);
+      MYCEL_CUDA(c, cudaEventSynchronize(evs[pi]));
+      bool running = false;
+      for (int q = 0; q < ncase; ++q) {
+        if (!active[q] || slot[pi][q].status != MIX_RUNNING) continue;
+        if (slot[pi][q].iter - resume[q] > cycle_limit[q]) {  // stalled: stop it (the queued chunk skips it)
+          stalled[q] = true;
+          k_mix_set_if<<<1, 1, 0, s>>>(mg->cw.st + q, MIX_RUNNING, MIX_FLUSH);
+          c->launches++;
+          continue;
+        }
+        running = true;
+      }
+      if (!running) break;
+    }
+    MYCEL_CUDA(c, cudaStreamSynchronize(s));
+    MixState* h = slot[0];
+    MYCEL_CUDA(c, cudaMemcpyAsync(h, mg->cw.st, sizeof(MixState) * ncase, cudaMemcpyDeviceToHost, s));
+    MYCEL_CUDA(c, cudaStreamSynchronize(s));
+    bool restart = false;
+    for (int k = 0; k < ncase; ++k) {
+      if (!active[k]) continue;
+      bind(k);
+      const int status = h[k].status;
+      iters[k] = h[k].iter;
+      const int m = iters[k] - resume[k];
+      if (m > 0 && (m & 1))
+        MYCEL_CUDA(c, cudaMemcpyAsync(cwv(mg, k, 4), cwv(mg, k, 3), sizeof(float) * (size_t)p->g.n32,
+                                      cudaMemcpyDeviceToDevice, s));
+      k_flush_u<float><<<stream_blocks(p), kT, 0, s>>>(p->g, d_u + k * nd, cwv(mg, k, 0));
+      c->launches++;
+      ++flushes[k];
+      double rn = 0.0;
+      if ((st = true_residual(p, form(k), p->d_b, d_u + k * nd, &rn))) return st;
+      rel[k] = rn / bnorm[k];
+      cycle_limit[k] = std::max<int64_t>(stall_floor, 3 * (int64_t)iters[k]);
+      if (rel[k] <= tol) {
+        ok[k] = true;
+        active[k] = false;
+        --nact;
+        k_mix_set<<<1, 1, 0, s>>>(mg->cw.st + k, MIX_DONE);
+        c->launches++;
+      } else if (stalled[k] || status != MIX_FLUSH || iters[k] >= max_iter) {
+        active[k] = false;  // finished alone below
+        --nact;
+        k_mix_set<<<1, 1, 0, s>>>(mg->cw.st + k, MIX_DONE);
+        c->launches++;
+      } else {
+        k_mix_set<<<1, 1, 0, s>>>(mg->cw.st + k, MIX_RUNNING);
+        c->launches++;
+        resume[k] = iters[k];
+        restart = true;
+      }
+    }
+    if (!restart) break;
+    // the restarting cases' preconditioned residual after the replacement (the others are not running)
+    int sel[kMgMaxCases] = {};
+    c->launches += launch_mg_step_cases(p, s, ncase, sel, 1);
+  }
+  {
+    int most = 0;
+    for (int k = 0; k < ncase; ++k) most = std::max(most, ok[k] ? iters[k] : INT32_MAX);
+    mg->last_iters = most;
+    if (fresh) mg->fresh_iters = most;
+  }
+  const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  for (int k = 0; k < ncase; ++k) {
+    if (res[k].message[0] && ok[k]) {  // zero right-hand side or converged at the start
+      res[k].elapsed_ms = ms;
+      continue;
+    }
+    if (!ok[k]) {  // finished alone from the refined u, as a single solve goes on after its FP32 iteration
+      if (stalled[k]) mg->prefers_f64 = true;
+      const int budget = std::max(max_iter - iters[k], max_iter / 2);
+      if ((st = solve_alone(k, budget, MYCEL_PRECISION_FP64_MG))) return st;
+      mycel_pcg_result& r = res[k];
+      r.fallback_iterations = r.iterations;
+      r.inner_iterations = iters[k];
+      r.iterations += iters[k];
+      r.refinement_steps += flushes[k];
+      continue;
+    }
+    res[k].inner_iterations = iters[k];
+    res[k].iterations = iters[k];
+    res[k].refinement_steps = flushes[k];
+    res[k].final_residual = rel[k];
+    res[k].converged = 1;
+    res[k].elapsed_ms = ms;
+  }
   return MYCEL_OK;
 }
 

@@ -184,6 +184,10 @@ struct mycel_problem {
   int pcg64f_graph_profiled = 0;
   cudaEvent_t prof64f_ev[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
   mycel::MgHier* mg = nullptr;     // multigrid hierarchy (MYCEL_PRECISION_FP64_MG), built on first use
+  // TMA descriptors of the per-case FP32 work vectors of batched multigrid solves (owned by the hierarchy)
+  int n_case_tmaps = 0;
+  const float* case_tmap_ptr[32] = {};
+  const CUtensorMap* case_tmap[32] = {};
   double* d_r64 = nullptr;        // refinement residual
   double* d_part2 = nullptr;      // [many] FP64 partials for mixed dots
   int64_t n_part2 = 0;
@@ -303,12 +307,18 @@ int32_t mixed_apply_k_f64io(mycel_problem* p, const double* x, double* y, int pr
 bool simp_session_converged(const mycel_simp_session* s);  // the SIMP stop rule fired
 int32_t mixed_solve_entry(mycel_problem* p, const double* d_b, const int32_t* d_nz, int32_t n_nz, double* d_u,
                           double tol, int max_iter, const volatile int32_t* cancel, mycel_pcg_result* res);
+// Load cases 0 .. ncase-1 of the problem solved together in the mixed multigrid form (one V-cycle's coarse
+// levels for all cases); d_u: ncase x total_dofs, case-major, warm starts in, solutions out; res: ncase.
+int32_t mg_solve_cases(mycel_problem* p, int ncase, double* d_u, double tol, int max_iter,
+                       const volatile int32_t* cancel, mycel_pcg_result* res);
+constexpr int kMaxBatchedCases = 8;
+bool cases_together_enabled();  // MYCEL_CASES_TOGETHER=0 turns the batched case solve off
 int32_t refined_solve_entry(mycel_problem* p, const double* d_b, const int32_t* d_nz, int32_t n_nz, double* d_u,
                             double tol, int max_iter, const volatile int32_t* cancel, int precision,
                             mycel_pcg_result* res);
 int32_t fast64_apply_k(mycel_problem* p, const double* x, double* y, int projected);
 void mg_release(mycel_problem* p);
-int64_t mg_device_bytes(int nx, int ny, int nz);  // hierarchy of a grid; 0 when it does not coarsen
+int64_t mg_device_bytes(int nx, int ny, int nz, int n_cases, bool cases_together);  // hierarchy of a grid; 0 when it does not coarsen
 
 // ---- drivers (api.cu) ----
 int32_t pcg_solve_fp64(mycel_problem* p, const double* d_b, const int32_t* d_nz, int32_t n_nz, double* d_x,

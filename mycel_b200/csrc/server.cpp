@@ -114,7 +114,9 @@ static int64_t job_bytes(const mycel_grid& gr, int64_t n_active, int64_t n_fixed
   if (o.precision == MYCEL_PRECISION_MIXED || mg) b += 6 * (4 * g.n32 + 64);
   if (o.precision == MYCEL_PRECISION_MIXED || o.precision == MYCEL_PRECISION_FP64_FACTORED || mg)
     b += 7 * (8 * g.n64 + 64);
-  if (mg) b += mycel::mg_device_bytes(g.nx, g.ny, g.nz);
+  if (mg)
+    b += mycel::mg_device_bytes(g.nx, g.ny, g.nz, n_loads,
+                                o.precision == MYCEL_PRECISION_MIXED_MG && o.separate_load_cases != 0);
   // filter (stencil offsets and weights of radius ceil(rmin) <= max(filter radius, 1.5) / h, plus invHs, S)
   double rmin = o.filter_radius_mm / std::max(1e-30, (double)gr.h);
   if (o.enforce_minimum_filter_radius && rmin < 1.5) rmin = 1.5;

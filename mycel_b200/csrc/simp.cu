@@ -284,9 +284,15 @@ static int32_t simp_step_impl(mycel_simp_session* s, mycel_iter_record* rec, int
   } else {
     std::memset(&pr, 0, sizeof pr);
     pr.converged = 1;
+    // the mixed multigrid form solves the cases together (one V-cycle's coarse levels for all of them)
+    const bool together =
+        o.precision == MYCEL_PRECISION_MIXED_MG && s->ncase <= kMaxBatchedCases && cases_together_enabled();
+    mycel_pcg_result rs[kMaxBatchedCases];
+    if (together && (rc = mg_solve_cases(p, s->ncase, s->d_uc, tol, o.solver_max_iterations, cancel, rs))) return rc;
     for (int k = 0; k < s->ncase && pr.converged; ++k) {
       mycel_pcg_result rk;
-      if ((rc = solve_case(p, k, s->d_uc + k * nd, tol, o.solver_max_iterations, o.precision, cancel, &rk)))
+      if (together) rk = rs[k];
+      else if ((rc = solve_case(p, k, s->d_uc + k * nd, tol, o.solver_max_iterations, o.precision, cancel, &rk)))
         return rc;
       pr.iterations += rk.iterations;
       pr.inner_iterations += rk.inner_iterations;

@@ -18,8 +18,7 @@ pytestmark = pytest.mark.gpu
 
 @pytest.fixture
 def oracle_cr(oracle):
-    """The oracle with correctly rounded integer powers in E = Emin + rho^p (E0 - Emin), as the device computes
-    them (glibc pow, the oracle's default, is off by an ulp for a few random densities)."""
+    """The reference-faithful oracle (the C library's pow, .NET 8+ lane order), as the device computes."""
     oracle.set_modes(0)
     yield oracle
     oracle.set_modes(0)
@@ -154,3 +153,37 @@ def test_simp_separate_cases_with_an_empty_case(oracle_cr, ctx):
         if prec == "fp64":
             assert [s.compliance for s in b.snapshots] == [r["compliance"] for r in ref.records]
             assert np.array_equal(b.final_physical_density, ref.phys)
+
+
+@pytest.mark.parametrize("which", [0, 1, 2])
+def test_static_cases_solved_together_equal_each_alone(ctx, which):
+    """Mixed multigrid form: the cases of one stiffness are solved together (their outer iterations side by side,
+    one V-cycle whose coarse levels advance every case per stencil read); each case gets the iterations and the
+    bits of its solve alone."""
+    m = _multi_case_models()[which]
+    rng = np.random.default_rng(10 + which)
+    m.element_density[:] = rng.uniform(0.1, 1.0, m.total_elements)
+    opt = StaticAnalysisOptions(tolerance=1e-8, max_iterations=20000, precision="mixed-mg")
+    got = api.StaticAnalysis.run_cases(m, opt, ctx=ctx)
+    assert len(got) == len(m.loads) >= 2
+    for k, g in enumerate(got):
+        one = api.StaticAnalysis.run(_single(m, k), opt, ctx=ctx, reactions=False, von_mises=False)
+        assert g.solver_info.converged and one.solver_info.converged
+        assert g.solver_info.iterations == one.solver_info.iterations
+        assert np.array_equal(g.u, one.u)
+        assert g.compliance == one.compliance
+
+
+def test_simp_cases_together_equal_one_after_another(ctx, monkeypatch):
+    """The SIMP loop with load cases apart in the mixed multigrid form: solving the cases together gives the
+    same iterates as solving them one after another (MYCEL_CASES_TOGETHER=0)."""
+    m = _multi_case_models()[1]
+    o = _opts(precision="mixed-mg", max_iterations=4)
+    together = api.TopologyOptimizer.run(m, o, ctx=ctx)
+    monkeypatch.setenv("MYCEL_CASES_TOGETHER", "0")
+    apart = api.TopologyOptimizer.run(m, o, ctx=ctx)
+    monkeypatch.delenv("MYCEL_CASES_TOGETHER")
+    assert [s.compliance for s in together.snapshots] == [s.compliance for s in apart.snapshots]
+    assert [s.solver_iterations for s in together.snapshots] == [s.solver_iterations for s in apart.snapshots]
+    assert np.array_equal(together.final_displacements, apart.final_displacements)
+    assert np.array_equal(together.final_design_density, apart.final_design_density)
