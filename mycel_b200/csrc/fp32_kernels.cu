@@ -2785,10 +2785,6 @@ struct MgHier {
   int T = 1;             // first level handled by the cluster kernel k_mg_tail
   MgTail tail{};
   bool prefers_f64 = false;  // an FP32 outer solve of this problem stalled: later ones start in FP64
-  // reuse of the coarse levels across solves on a changed E (see mg_needs_setup)
-  int fresh_iters = 0;   // outer iterations of the last solve right after a set-up
-  int last_iters = 0;    // outer iterations of the last solve
-  int reuses = 0;        // solves since the last set-up that kept an older hierarchy
   int ncap = 1;          // load cases the level vectors have room for (case k at + k * nd)
   // load cases solved together (mg_solve_cases): per case the FP32 work vectors x, r, z, p0, p1, ap, t of the
   // voxel level, the TMA descriptors of r, z, p0, p1, one state per case, and the chunk graphs
@@ -3006,23 +3002,6 @@ static MgPtrs mg_ptrs(float* const (&v)[kMgMaxCases], int n) {
   MgPtrs r{};
   for (int k = 0; k < n; ++k) r.p[k] = v[k];
   return r;
-}
-
-// Whether a solve on a changed E rebuilds the coarse levels. The outer iteration is flexible CG on the current
-// operator, so a hierarchy built from an earlier E still gives the solution to the same tolerance, only the
-// iteration count can grow. A SIMP design changes a little from one solve to the next: the hierarchy is kept
-// while the last solve needed at most kMgReuseSlack times the iterations of the last solve right after a
-// set-up, for at most kMgMaxReuse solves in a row. Decided on iteration counts only (deterministic, the same
-// whatever else runs). MYCEL_MG_REUSE=0 rebuilds at every change of E.
-constexpr double kMgReuseSlack = 1.25;
-constexpr int kMgMaxReuse = 3;
-static bool mg_needs_setup(const MgHier* mg) {
-  static const bool allow = [] {
-    const char* e = std::getenv("MYCEL_MG_REUSE");
-    return !(e && e[0] == '0');
-  }();
-  if (!allow || mg->fresh_iters <= 0 || mg->reuses >= kMgMaxReuse) return true;
-  return (double)mg->last_iters > kMgReuseSlack * mg->fresh_iters;
 }
 
 // Coarse operators from the current E: Galerkin element matrices level by level, their stencils, and the
@@ -3516,14 +3495,9 @@ int32_t refined_solve_entry(mycel_problem* p, const double* d_b, const int32_t* 
     if ((st = resolve_mv32(p)) || (st = mg_ensure(p, &avail))) return st;
     if (avail) {
       ran_mg = true;
-      bool fresh = false;
-      if (p->mg->setup_version != p->e_version && mg_needs_setup(p->mg)) {
+      if (p->mg->setup_version != p->e_version) {  // solves on an unchanged E (load cases) share the set-up
         mg_setup(p);
         p->mg->setup_version = p->e_version;
-        p->mg->reuses = 0;
-        fresh = true;
-      } else if (p->mg->setup_version != p->e_version) {
-        p->mg->reuses++;
       }
       // MYCEL_PRECISION_MIXED_MG: the FP32 outer iteration first (unless one of this problem's solves stalled
       // in it), then the FP64 outer iteration from the refined u
@@ -3547,8 +3521,6 @@ int32_t refined_solve_entry(mycel_problem* p, const double* d_b, const int32_t* 
       }
       if (ok && lmg.iterations + lmg32.iterations == 0 && lmg.flushes + lmg32.flushes == 0)
         std::snprintf(res->message, sizeof res->message, "Initial guess already converged.");
-      p->mg->last_iters = ok ? lmg32.iterations + lmg.iterations : INT32_MAX;
-      if (fresh) p->mg->fresh_iters = p->mg->last_iters;
     }
   }
   // Which inner form a mixed solve starts in. Once a mixed solve of a problem has stalled (its designs have
@@ -3815,15 +3787,10 @@ int32_t mg_solve_cases(mycel_problem* p, int ncase, double* d_u, double tol, int
     return F;
   };
   MYCEL_CUDA(c, cudaMemsetAsync(p->d_err, 0, sizeof(int), s));
-  // one stiffness: the hierarchy is rebuilt (or kept) as for a single solve
-  bool fresh = false;
-  if (mg->setup_version != p->e_version && mg_needs_setup(mg)) {
+  // one stiffness: the hierarchy is rebuilt when E has changed, once for all cases
+  if (mg->setup_version != p->e_version) {
     mg_setup(p);
     mg->setup_version = p->e_version;
-    mg->reuses = 0;
-    fresh = true;
-  } else if (mg->setup_version != p->e_version) {
-    mg->reuses++;
   }
   PcgState* hs = (PcgState*)c->pinned;
   int nact = 0;
@@ -3955,12 +3922,6 @@ int32_t mg_solve_cases(mycel_problem* p, int ncase, double* d_u, double tol, int
     // the restarting cases' preconditioned residual after the replacement (the others are not running)
     int sel[kMgMaxCases] = {};
     c->launches += launch_mg_step_cases(p, s, ncase, sel, 1);
-  }
-  {
-    int most = 0;
-    for (int k = 0; k < ncase; ++k) most = std::max(most, ok[k] ? iters[k] : INT32_MAX);
-    mg->last_iters = most;
-    if (fresh) mg->fresh_iters = most;
   }
   const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   for (int k = 0; k < ncase; ++k) {
