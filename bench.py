@@ -37,10 +37,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 METRIC = "SIMP iter/s (mixed FP32-inner/FP64-refined, 192x96x96 bridge)"
 sys.path.insert(0, ROOT)
 
-# PCG iterations per SIMP iteration of the plain FP64 path on this workload (mean of iterations 4 and 5: 2,619
-# and 2,499, measured on B200 by the default run's fp64 arm; the FP64 path reproduces the reference's iteration
-# counts). Used only to scale the CPU sample of the reference arm; the default run uses its own fp64 counts.
-FP64_PCG_PER_SIMP_ITER = {"bridge_192x96x96": 2559}
+# PCG iterations per SIMP iteration of the plain FP64 path on this workload: the mean over SIMP iterations
+# 6-25 (the timed iterations of a `--steps 20 --warmup 5` run), 1,810, measured on B200 by the default run's
+# fp64 arm, which runs those same iterations (the FP64 path reproduces the reference's iteration counts). Used
+# only to scale the CPU sample of the reference arm; the default run uses its own fp64 counts.
+FP64_PCG_PER_SIMP_ITER = {"bridge_192x96x96": 1810}
 
 # DRAM bytes per launch of the FP32 matvec (MODE 1) from one ncu capture (dram__bytes_read.sum +
 # dram__bytes_write.sum), keyed by (solver form, matvec variant, workload). Jacobi-PCG form (`--probe mixed
