@@ -49,8 +49,11 @@ FP64_PCG_PER_SIMP_ITER = {"bridge_192x96x96": 1810}
 # 126 MB L2 during the launch).
 # Mixed multigrid form (`--probe mixed-mg --probe-grid 192x96x96 --probe-variant 3`, third MODE-1 launch):
 # 53.52 MB read, 4.88 MB written.
+# Multigrid level-1 residual product (`--probe mixed-mg --probe-grid 192x96x96 --probe-variant 3`, fifth
+# k_mg_apply_nodes launch): 122.26 MB read, 4.54 MB written.
 NCU_DRAM_BYTES = {("mixed", 3, "bridge_192x96x96"): 53.47e6 + 5.53e6,
-                  ("mixed-mg", 3, "bridge_192x96x96"): 53.52e6 + 4.88e6}
+                  ("mixed-mg", 3, "bridge_192x96x96"): 53.52e6 + 4.88e6,
+                  ("mg-level1", "mixed-mg", "bridge_192x96x96"): 122.26e6 + 4.54e6}
 
 
 def parse():
@@ -63,6 +66,8 @@ def parse():
     ap.add_argument("--fp64-steps", type=int, default=-1,
                     help="iterations after the warm-up of the plain FP64 arm run beside the timed form (-1: --steps, "
                          "0: none)")
+    ap.add_argument("--profile-steps", type=int, default=5,
+                    help="SIMP iterations after the timed ones during which the roofline kernels are timed")
     ap.add_argument("--others-steps", type=int, default=2,
                     help="iterations after the warm-up of the other solver forms (fp64f, mg, mixed)")
     ap.add_argument("--no-e2e", action="store_true")
@@ -481,7 +486,6 @@ def run_mycel(args):
     for _ in range(args.warmup):
         sess.step()
     launches0 = ctx.launch_count
-    ctx.set_profiling(True)
     clocks = Clocks(local)
     barrier(ws)
     torch.cuda.synchronize(local)
@@ -494,12 +498,27 @@ def run_mycel(args):
     clk = clocks.stop()
     barrier(ws)
     t_ms = e0.elapsed_time(e1)
-    timing = ctx.kernel_timing(0)
-    timing_l1 = ctx.kernel_timing(3)
-    ctx.set_profiling(False)
     gpu_launches = ctx.launch_count - launches0
     t_max = max_over_ranks(ws, t_ms)
     value = ws * args.steps / (t_max / 1000.0)
+    # kernel timings for the roofline: the next --profile-steps iterations of the same session, with CUDA
+    # event-record nodes around one matvec and one level-1 product per chunk graph (kept out of the timed steps
+    # above, whose graphs carry no events)
+    ctx.set_profiling(True)
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record(stream)
+    n_prof = 0
+    for _ in range(args.profile_steps):
+        if sess.done:
+            break
+        sess.step()
+        n_prof += 1
+    p1.record(stream)
+    torch.cuda.synchronize(local)
+    timing = ctx.kernel_timing(0)
+    timing_l1 = ctx.kernel_timing(3)
+    ctx.set_profiling(False)
+    prof_window = {"iterations": n_prof, "simp_iter_s": 1000.0 * n_prof / p0.elapsed_time(p1) if n_prof else None}
     pcg_inner = [r.solver_iterations for r in recs]
     comp_head = [r.compliance for r in recs]
     mv_variant = prob.matvec32()
@@ -549,7 +568,8 @@ def run_mycel(args):
                       "penal": opts.penal, "emin_ratio": model.material.emin_ratio,
                       "pcg_tol": opts.solver_tolerance_final, "inputs_vs_l2": "inputs > L2 (126 MB); no flush",
                       "parallelism": f"replicas x{ws}"},
-           "roofline": roof, "roofline_mg_level1": roof_l1, "gpu_launches": gpu_launches, "clocks": clk,
+           "roofline": roof, "roofline_mg_level1": roof_l1, "roofline_window": prof_window,
+           "gpu_launches": gpu_launches, "clocks": clk,
            "pcg_inner_iters_per_step": pcg_inner, "compliance": comp_head}
 
     # ---------------- plain FP64 path over the same iterations; the timed form's errors against it ----------------

@@ -1678,6 +1678,20 @@ constexpr int kMgMaxCases = 8;
 struct MgPtrs {
   float* p[kMgMaxCases];
 };
+// (item, case) from a thread number with the case fastest; one case: the number itself (no division). The
+// kernels are instantiated for one case (MULTI false: the single solve's code, compile-time case 0) and for
+// several.
+template <bool MULTI>
+__device__ __forceinline__ void mg_item_case(int64_t t, int ncase, int64_t* item, int* c) {
+  if (!MULTI || ncase == 1) {
+    *item = t;
+    *c = 0;
+  } else {
+    const uint32_t q = (uint32_t)t / (uint32_t)ncase;  // items x cases < 2^32 on every level
+    *item = q;
+    *c = (int)((uint32_t)t - q * (uint32_t)ncase);
+  }
+}
 __host__ __device__ __forceinline__ MgPtrs mg_one(float* v) {
   MgPtrs r{};
   r.p[0] = v;
@@ -1955,6 +1969,7 @@ __device__ __forceinline__ void mg_apply_row(const MgDims& d, int64_t nn, int64_
 // coarse-level product kernels: a thread per node (large levels: the three rows share their x loads) or a
 // thread per DOF (smaller levels: three times the threads in flight); mg_apply_kernel picks by size
 // (st: the cases' states, one per case, or null; a case whose state is not running is skipped)
+template <bool MULTI>
 __global__ void __launch_bounds__(256) k_mg_apply_nodes(MgDims d, const float* __restrict__ S,
                                                         const __grid_constant__ MgPtrs x,
                                                         const __grid_constant__ MgPtrs r,
@@ -1962,13 +1977,14 @@ __global__ void __launch_bounds__(256) k_mg_apply_nodes(MgDims d, const float* _
                                                         const __grid_constant__ MgPtrs y, int mode,
                                                         const float* __restrict__ om, const MixState* st, int ncase) {
   const int64_t nn = mg_nn(d);
-  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  const int64_t n = t / ncase;
-  const int c = (int)(t - n * ncase);
+  int64_t n;
+  int c;
+  mg_item_case<MULTI>(blockIdx.x * (int64_t)blockDim.x + threadIdx.x, ncase, &n, &c);
   if (n >= nn || !mg_running(st ? st + c : nullptr)) return;
   mg_apply_node(d, nn, n, S, x.p[c], r.p[c], invd, y.p[c], mode, mode == 1 ? *om : 0.0f);
 }
 
+template <bool MULTI>
 __global__ void __launch_bounds__(kMgDofThreads) k_mg_apply(MgDims d, const float* __restrict__ S,
                                                             const __grid_constant__ MgPtrs x,
                                                             const __grid_constant__ MgPtrs r,
@@ -1977,9 +1993,9 @@ __global__ void __launch_bounds__(kMgDofThreads) k_mg_apply(MgDims d, const floa
                                                             const float* __restrict__ om, const MixState* st,
                                                             int ncase) {
   const int64_t nn = mg_nn(d);
-  const int64_t i = mg_dof_node();  // (node, case) pair, the case fastest
-  const int64_t n = i / ncase;
-  const int c = (int)(i - n * ncase);
+  int64_t n;  // (node, case) pair, the case fastest
+  int c;
+  mg_item_case<MULTI>(mg_dof_node(), ncase, &n, &c);
   if (n >= nn || !mg_running(st ? st + c : nullptr)) return;
   mg_apply_row(d, nn, n, mg_dof_comp(), S, x.p[c], r.p[c], invd, y.p[c], mode, mode == 1 ? *om : 0.0f);
 }
@@ -2120,14 +2136,14 @@ __device__ __forceinline__ void mg_restrict_node(const MgDims& f, int pitch, con
   }
 }
 
-template <bool PAD>
+template <bool PAD, bool MULTI>
 __global__ void k_mg_restrict(MgDims f, int pitch, const __grid_constant__ MgPtrs rf, const __grid_constant__ MgPtrs tf,
                               MgDims c, const float* __restrict__ invdc, const __grid_constant__ MgPtrs rc,
                               const MixState* st, const __grid_constant__ MgPtrs xc, int first_sweep,
                               const float* __restrict__ om, int ncase) {
-  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  const int64_t n = t / ncase;
-  const int k = (int)(t - n * ncase);
+  int64_t n;
+  int k;
+  mg_item_case<MULTI>(blockIdx.x * (int64_t)blockDim.x + threadIdx.x, ncase, &n, &k);
   if (n >= mg_nn(c) || !mg_running(st ? st + k : nullptr)) return;
   const float omega = first_sweep ? *om : 0.f;
   mg_restrict_node<PAD>(f, pitch, rf.p[k], tf.p[k], c, invdc, rc.p[k], n, first_sweep ? xc.p[k] : nullptr, omega);
@@ -2177,13 +2193,13 @@ __device__ __forceinline__ void mg_prolong_node(const MgDims& f, int pitch, cons
   }
 }
 
-template <bool PAD>
+template <bool PAD, bool MULTI>
 __global__ void k_mg_prolong(MgDims f, int pitch, const uint8_t* __restrict__ nf, const float* __restrict__ invdf,
                              const __grid_constant__ MgPtrs xf, MgDims c, const __grid_constant__ MgPtrs xc,
                              const MixState* st, int ncase) {
-  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  const int64_t n = t / ncase;
-  const int k = (int)(t - n * ncase);
+  int64_t n;
+  int k;
+  mg_item_case<MULTI>(blockIdx.x * (int64_t)blockDim.x + threadIdx.x, ncase, &n, &k);
   if (n >= mg_nn(f) || !mg_running(st ? st + k : nullptr)) return;
   mg_prolong_node<PAD>(f, pitch, nf, invdf, xf.p[k], c, xc.p[k], n);
 }
@@ -2292,6 +2308,7 @@ __device__ __forceinline__ void mg_cluster_sync() {
 // Levels T .. L-1 of the V-cycle for ncase load cases: from r of level T (restricted by the caller) to the
 // smoothed correction of level T, left in its xa. Work items are numbered with the case fastest; a case whose
 // state is not running is skipped, and the kernel returns at once (every thread alike) when none is.
+template <bool MULTI>
 __global__ void __cluster_dims__(kMgTailCtas, 1, 1) __launch_bounds__(kMgTailThreads)
     k_mg_tail(const __grid_constant__ MgTail tl, const float* __restrict__ om, const MixState* st, int ncase) {
   bool any = false;
@@ -2305,15 +2322,17 @@ __global__ void __cluster_dims__(kMgTailCtas, 1, 1) __launch_bounds__(kMgTailThr
     const int64_t nd = 3 * v.nn;
     if (3 * v.nn * ncase <= gs) {
       for (int64_t t = gt; t < nd * ncase; t += gs) {
-        const int64_t it = t / ncase;
-        const int k = (int)(t - it * ncase);
+        int64_t it;
+        int k;
+        mg_item_case<MULTI>(t, ncase, &it, &k);
         if (live(k))
           mg_apply_row(v.d, v.nn, it / 3, (int)(it % 3), v.S, x + k * nd, v.r + k * nd, v.invd, y + k * nd, mode, w);
       }
     } else {
       for (int64_t t = gt; t < v.nn * ncase; t += gs) {
-        const int64_t n = t / ncase;
-        const int k = (int)(t - n * ncase);
+        int64_t n;
+        int k;
+        mg_item_case<MULTI>(t, ncase, &n, &k);
         if (live(k)) mg_apply_node(v.d, v.nn, n, v.S, x + k * nd, v.r + k * nd, v.invd, y + k * nd, mode, w);
       }
     }
@@ -2336,8 +2355,9 @@ __global__ void __cluster_dims__(kMgTailCtas, 1, 1) __launch_bounds__(kMgTailThr
     const bool smoothed = l + 1 < tl.L - 1;  // the coarsest level is solved, not smoothed
     const float wc = smoothed ? om[l + 1] : 0.0f;
     for (int64_t q = gt; q < cnd * ncase; q += gs) {
-      const int64_t it = q / ncase;
-      const int k = (int)(q - it * ncase);
+      int64_t it;
+      int k;
+      mg_item_case<MULTI>(q, ncase, &it, &k);
       if (live(k))
         mg_restrict_comp<false>(v.d, 0, nullptr, v.t + k * nd, cv.d, cv.invd, cv.r + k * cnd, it / 3, (int)(it % 3),
                                 smoothed ? cv.xa + k * cnd : nullptr, wc);
@@ -2350,8 +2370,9 @@ __global__ void __cluster_dims__(kMgTailCtas, 1, 1) __launch_bounds__(kMgTailThr
     const int64_t nd = 3 * v.nn;
     const int lane = threadIdx.x & 31;
     for (int64_t rc = gt >> 5; rc < (int64_t)tl.nc * ncase; rc += gs >> 5) {
-      const int64_t row = rc / ncase;
-      const int k = (int)(rc - row * ncase);
+      int64_t row;
+      int k;
+      mg_item_case<MULTI>(rc, ncase, &row, &k);
       if (!live(k)) continue;
       const float* r = v.r + k * nd;
       double acc = 0.0;
@@ -2370,8 +2391,9 @@ __global__ void __cluster_dims__(kMgTailCtas, 1, 1) __launch_bounds__(kMgTailThr
     float* x = xc[l];
     float* o = x == v.xa ? v.xb : v.xa;
     for (int64_t q = gt; q < nd * ncase; q += gs) {
-      const int64_t it = q / ncase;
-      const int k = (int)(q - it * ncase);
+      int64_t it;
+      int k;
+      mg_item_case<MULTI>(q, ncase, &it, &k);
       if (live(k))
         mg_prolong_comp<false>(v.d, 0, nullptr, v.invd, x + k * nd, tl.lv[l + 1].d, xc[l + 1] + k * cnd, it / 3,
                                (int)(it % 3));
@@ -2390,8 +2412,9 @@ __global__ void __cluster_dims__(kMgTailCtas, 1, 1) __launch_bounds__(kMgTailThr
   if (xc[tl.T] != vt.xa) {
     const int64_t nd = 3 * vt.nn;
     for (int64_t q = gt; q < nd * ncase; q += gs) {
-      const int64_t it = q / ncase;
-      const int k = (int)(q - it * ncase);
+      int64_t it;
+      int k;
+      mg_item_case<MULTI>(q, ncase, &it, &k);
       if (live(k)) vt.xa[k * nd + it] = xc[tl.T][k * nd + it];
     }
   }
@@ -2939,7 +2962,9 @@ static int32_t mg_ensure(mycel_problem* p, bool* available) {
     cfg.gridDim = dim3(kMgTailCtas);
     cfg.blockDim = dim3(kMgTailThreads);
     int nclusters = 0;
-    if (cudaOccupancyMaxActiveClusters(&nclusters, k_mg_tail, &cfg) != cudaSuccess || nclusters < 1) {
+    int ncl2 = 0;
+    if (cudaOccupancyMaxActiveClusters(&nclusters, k_mg_tail<false>, &cfg) != cudaSuccess || nclusters < 1 ||
+        cudaOccupancyMaxActiveClusters(&ncl2, k_mg_tail<true>, &cfg) != cudaSuccess || ncl2 < 1) {
       cudaGetLastError();
       return set_error(p->ctx, MYCEL_E_DEVICE, "multigrid: the coarse-level cluster kernel cannot be scheduled");
     }
@@ -2984,9 +3009,11 @@ static MgPtrs lv_ptrs(float* base, int64_t nd, int n) {
 static void launch_mg_apply(cudaStream_t s, const MgLevel& v, const MgPtrs& x, const MgPtrs& r, const float* invd,
                             const MgPtrs& y, int mode, const float* om, const MixState* st, int nc) {
   if (v.nn * nc <= 65536)
-    k_mg_apply<<<mg_dof_blocks(v.nn * nc), kMgDofThreads, 0, s>>>(v.d, v.S, x, r, invd, y, mode, om, st, nc);
+    (nc == 1 ? k_mg_apply<false> : k_mg_apply<true>)<<<mg_dof_blocks(v.nn * nc), kMgDofThreads, 0, s>>>(
+        v.d, v.S, x, r, invd, y, mode, om, st, nc);
   else
-    k_mg_apply_nodes<<<mg_blocks(v.nn * nc), 256, 0, s>>>(v.d, v.S, x, r, invd, y, mode, om, st, nc);
+    (nc == 1 ? k_mg_apply_nodes<false> : k_mg_apply_nodes<true>)<<<mg_blocks(v.nn * nc), 256, 0, s>>>(
+        v.d, v.S, x, r, invd, y, mode, om, st, nc);
 }
 
 // The load cases one V-cycle advances: their states (one per case, contiguous) and their voxel-level vectors
@@ -3081,7 +3108,7 @@ static int mg_vcycle(mycel_problem* p, cudaStream_t s, const MgRun& R) {
   for (int k = 0; k < nc; ++k) fine_mv(k);
   nl += nc;
   // restriction to level 1, with level 1's first sweep (unless level 1 is the coarsest)
-  k_mg_restrict<true><<<mg_blocks(lv[1].nn * nc), 256, 0, s>>>(lv[0].d, g.rp, mg_ptrs(R.rf, nc), mg_ptrs(R.tf, nc),
+  (nc == 1 ? k_mg_restrict<true, false> : k_mg_restrict<true, true>)<<<mg_blocks(lv[1].nn * nc), 256, 0, s>>>(lv[0].d, g.rp, mg_ptrs(R.rf, nc), mg_ptrs(R.tf, nc),
                                                                lv[1].d, lv[1].invd, lv_ptrs(lv[1].r, lv[1].nd, nc), st,
                                                                lv_ptrs(lv[1].xa, lv[1].nd, nc), 1 < mg->L - 1 ? 1 : 0,
                                                                om + 1, nc);
@@ -3099,7 +3126,7 @@ static int mg_vcycle(mycel_problem* p, cudaStream_t s, const MgRun& R) {
     launch_mg_apply(s, v, lv_ptrs(x, v.nd, nc), r, v.invd, lv_ptrs(v.t, v.nd, nc), 2, om + l, st, nc);
     if (l == 1 && mg->l1_timing) cudaEventRecordWithFlags(mg->l1_timing[1], s, cudaEventRecordExternal);
     MgLevel& cv = lv[l + 1];
-    k_mg_restrict<false><<<mg_blocks(cv.nn * nc), 256, 0, s>>>(v.d, 0, lv_ptrs(nullptr, 0, nc),
+    (nc == 1 ? k_mg_restrict<false, false> : k_mg_restrict<false, true>)<<<mg_blocks(cv.nn * nc), 256, 0, s>>>(v.d, 0, lv_ptrs(nullptr, 0, nc),
                                                                lv_ptrs(v.t, v.nd, nc), cv.d, cv.invd,
                                                                lv_ptrs(cv.r, cv.nd, nc), st,
                                                                lv_ptrs(cv.xa, cv.nd, nc), l + 1 < mg->L - 1 ? 1 : 0,
@@ -3107,14 +3134,14 @@ static int mg_vcycle(mycel_problem* p, cudaStream_t s, const MgRun& R) {
     xc[l] = x;
     nl += 1 + mg->sweeps;
   }
-  k_mg_tail<<<kMgTailCtas, kMgTailThreads, 0, s>>>(mg->tail, om, st, nc);
+  (nc == 1 ? k_mg_tail<false> : k_mg_tail<true>)<<<kMgTailCtas, kMgTailThreads, 0, s>>>(mg->tail, om, st, nc);
   xc[mg->T] = lv[mg->T].xa;
   nl++;
   for (int l = mg->T - 1; l >= 1; --l) {
     MgLevel& v = lv[l];
     float* x = xc[l];
     float* o = x == v.xa ? v.xb : v.xa;
-    k_mg_prolong<false><<<mg_blocks(v.nn * nc), 256, 0, s>>>(v.d, 0, nullptr, v.invd, lv_ptrs(x, v.nd, nc), lv[l + 1].d,
+    (nc == 1 ? k_mg_prolong<false, false> : k_mg_prolong<false, true>)<<<mg_blocks(v.nn * nc), 256, 0, s>>>(v.d, 0, nullptr, v.invd, lv_ptrs(x, v.nd, nc), lv[l + 1].d,
                                                               lv_ptrs(xc[l + 1], lv[l + 1].nd, nc), st, nc);
     const MgPtrs r = lv_ptrs(v.r, v.nd, nc);
     for (int k = 0; k < mg->sweeps; ++k) {
@@ -3124,7 +3151,7 @@ static int mg_vcycle(mycel_problem* p, cudaStream_t s, const MgRun& R) {
     xc[l] = x;
     nl += 1 + mg->sweeps;
   }
-  k_mg_prolong<true><<<mg_blocks(lv[0].nn * nc), 256, 0, s>>>(lv[0].d, g.rp, p->d_nflags, nullptr, mg_ptrs(R.xf, nc),
+  (nc == 1 ? k_mg_prolong<true, false> : k_mg_prolong<true, true>)<<<mg_blocks(lv[0].nn * nc), 256, 0, s>>>(lv[0].d, g.rp, p->d_nflags, nullptr, mg_ptrs(R.xf, nc),
                                                               lv[1].d, lv_ptrs(xc[1], lv[1].nd, nc), st, nc);
   nl++;
   for (int q = 1; q < mg->sweeps; ++q)
