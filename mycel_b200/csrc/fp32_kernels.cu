@@ -2000,6 +2000,67 @@ __global__ void __launch_bounds__(kMgDofThreads) k_mg_apply(MgDims d, const floa
   mg_apply_row(d, nn, n, mg_dof_comp(), S, x.p[c], r.p[c], invd, y.p[c], mode, mode == 1 ? *om : 0.0f);
 }
 
+// The same product with the 27 neighbour blocks split by neighbour plane (dz = -1, 0, 1): three threads per
+// node (threadIdx.y = plane), each gathering 9 neighbours for all three rows; the partial sums are added in
+// plane order through shared memory. Three times the threads in flight of k_mg_apply_nodes without its loads
+// repeated (the per-DOF kernel loads each neighbour's x once per row).
+template <bool MULTI>
+__global__ void __launch_bounds__(192) k_mg_apply_planes(MgDims d, const float* __restrict__ S,
+                                                         const __grid_constant__ MgPtrs x,
+                                                         const __grid_constant__ MgPtrs r,
+                                                         const float* __restrict__ invd,
+                                                         const __grid_constant__ MgPtrs y, int mode,
+                                                         const float* __restrict__ om, const MixState* st, int ncase) {
+  __shared__ float part[3][3][64];
+  const int tx = threadIdx.x, pz = threadIdx.y;
+  const int64_t nn = mg_nn(d);
+  int64_t n;
+  int c;
+  mg_item_case<MULTI>(blockIdx.x * (int64_t)64 + tx, ncase, &n, &c);
+  const bool valid = n < nn && mg_running(st ? st + c : nullptr);
+  float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+  if (valid) {
+    const int nx1 = d.nx + 1, ny1 = d.ny + 1;
+    const int i = (int)(n % nx1), j = (int)((n / nx1) % ny1), k = (int)(n / ((int64_t)nx1 * ny1));
+    const float* xv = x.p[c];
+    const int uk = k + pz - 1;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+      const int nb = 9 * pz + q;
+      const int ui = i + q % 3 - 1, uj = j + q / 3 - 1;
+      const int mi = min(max(ui, 0), d.nx), mj = min(max(uj, 0), d.ny), mk = min(max(uk, 0), d.nz);
+      const bool in = mi == ui && mj == uj && mk == uk;
+      const int64_t m = mi + (int64_t)nx1 * (mj + (int64_t)ny1 * mk);
+      const float x0 = in ? xv[3 * m] : 0.f, x1 = in ? xv[3 * m + 1] : 0.f, x2 = in ? xv[3 * m + 2] : 0.f;
+      if (nb >= 13) {
+        const float* sp = S + (int64_t)(nb - 13) * 9 * nn + n;
+        a0 = fmaf(sp[0], x0, fmaf(sp[nn], x1, fmaf(sp[2 * nn], x2, a0)));
+        a1 = fmaf(sp[3 * nn], x0, fmaf(sp[4 * nn], x1, fmaf(sp[5 * nn], x2, a1)));
+        a2 = fmaf(sp[6 * nn], x0, fmaf(sp[7 * nn], x1, fmaf(sp[8 * nn], x2, a2)));
+      } else {
+        const float* sp = S + (int64_t)(13 - nb) * 9 * nn + m;
+        a0 = fmaf(sp[0], x0, fmaf(sp[3 * nn], x1, fmaf(sp[6 * nn], x2, a0)));
+        a1 = fmaf(sp[nn], x0, fmaf(sp[4 * nn], x1, fmaf(sp[7 * nn], x2, a1)));
+        a2 = fmaf(sp[2 * nn], x0, fmaf(sp[5 * nn], x1, fmaf(sp[8 * nn], x2, a2)));
+      }
+    }
+  }
+  part[pz][0][tx] = a0;
+  part[pz][1][tx] = a1;
+  part[pz][2][tx] = a2;
+  __syncthreads();
+  if (!valid || pz != 0) return;
+  const float omega = mode == 1 ? *om : 0.0f;
+#pragma unroll
+  for (int cc = 0; cc < 3; ++cc) {
+    const float acc = (part[0][cc][tx] + part[1][cc][tx]) + part[2][cc][tx];
+    const int64_t q = 3 * n + cc;
+    if (mode == 0) y.p[c][q] = acc;
+    else if (mode == 1) y.p[c][q] = fmaf(omega * invd[q], r.p[c][q] - acc, x.p[c][q]);
+    else y.p[c][q] = invd[q] != 0.0f ? r.p[c][q] - acc : 0.0f;
+  }
+}
+
 // a further sweep on the voxel grid (padded FP32 layout, t = A x): x += omega invd (r - t)
 __global__ void k_mg_jacobi_fine(int64_t n, const float* __restrict__ r, const float* __restrict__ t,
                                  const float* __restrict__ invd, float* __restrict__ x, const float* __restrict__ om,
@@ -3006,9 +3067,22 @@ static MgPtrs lv_ptrs(float* base, int64_t nd, int n) {
   return r;
 }
 
+// product kernel of the large levels: a thread per node (default) or three per node split by neighbour plane
+// (MYCEL_MG_APPLY=planes)
+static bool mg_apply_planes() {
+  static const bool planes = [] {
+    const char* e = std::getenv("MYCEL_MG_APPLY");
+    return e && std::string(e) == "planes";
+  }();
+  return planes;
+}
+
 static void launch_mg_apply(cudaStream_t s, const MgLevel& v, const MgPtrs& x, const MgPtrs& r, const float* invd,
                             const MgPtrs& y, int mode, const float* om, const MixState* st, int nc) {
-  if (v.nn * nc <= 65536)
+  if (v.nn * nc > 65536 && mg_apply_planes())
+    (nc == 1 ? k_mg_apply_planes<false> : k_mg_apply_planes<true>)<<<(unsigned)((v.nn * nc + 63) / 64), dim3(64, 3),
+                                                                     0, s>>>(v.d, v.S, x, r, invd, y, mode, om, st, nc);
+  else if (v.nn * nc <= 65536)
     (nc == 1 ? k_mg_apply<false> : k_mg_apply<true>)<<<mg_dof_blocks(v.nn * nc), kMgDofThreads, 0, s>>>(
         v.d, v.S, x, r, invd, y, mode, om, st, nc);
   else
