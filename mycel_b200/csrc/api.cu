@@ -367,6 +367,7 @@ extern "C" int32_t mycel_ctx_create(int32_t device, mycel_ctx** out) {
   c->device = device;
   if ((e = cudaSetDevice(device)) != cudaSuccess ||
       (e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+      (e = cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking)) != cudaSuccess ||
       (e = cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess ||
       (e = cudaMallocHost(&c->pinned, 1 << 16)) != cudaSuccess) {
     std::string m = cudaGetErrorString(e);
@@ -378,6 +379,7 @@ extern "C" int32_t mycel_ctx_create(int32_t device, mycel_ctx** out) {
   if (oc_blocks_per_sm(&oc_bpsm) != MYCEL_OK) {
     cudaFreeHost(c->pinned);
     cudaStreamDestroy(c->stream);
+    if (c->side) cudaStreamDestroy(c->side);
     delete c;
     return set_error(nullptr, MYCEL_E_DEVICE, "occupancy query of the OC kernel failed");
   }
@@ -401,6 +403,10 @@ extern "C" int32_t mycel_ctx_destroy(mycel_ctx* c) {
   if (c->stream) {
     cudaStreamSynchronize(c->stream);
     cudaStreamDestroy(c->stream);
+  }
+  if (c->side) {
+    cudaStreamSynchronize(c->side);
+    cudaStreamDestroy(c->side);
   }
   if (c->pinned) cudaFreeHost(c->pinned);
   delete c;

@@ -2697,9 +2697,9 @@ struct MgScratch {
   unsigned int counter;
 };
 
-// ||D^-1 y|| by fixed-order sums into sc->norm; with `omega_level` >= 0 also that level's damping
+// ||D^-1 y|| by fixed-order sums into sc->norm; with `omega_out` also that level's damping
 __global__ void __launch_bounds__(kT) k_mg_pow_norm(int64_t n, const float* __restrict__ y, const float* __restrict__ invd,
-                                                    double* part, MgScratch* sc, int omega_level) {
+                                                    double* part, MgScratch* sc, float* omega_out) {
   __shared__ double sh[32];
   double s = 0.0;
   for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
@@ -2715,7 +2715,7 @@ __global__ void __launch_bounds__(kT) k_mg_pow_norm(int64_t n, const float* __re
   sc->counter = 0;
   const float nrm = (float)sqrt(t);
   sc->norm = nrm;
-  if (omega_level >= 0) sc->omega[omega_level] = (nrm > 0.0f && isfinite(nrm)) ? kMgOmegaScale / nrm : 0.5f;
+  if (omega_out) *omega_out = (nrm > 0.0f && isfinite(nrm)) ? kMgOmegaScale / nrm : 0.5f;
 }
 
 __global__ void k_mg_pow_scale(int64_t n, const float* __restrict__ y, const float* __restrict__ invd,
@@ -2851,6 +2851,11 @@ struct MgHier {
   uint8_t* special = nullptr;         // [level-1 elements] built by the general path
   double* ainv = nullptr;
   MgScratch* sc = nullptr;  // per-level damping, power-iteration norm and counter (device)
+  // the voxel level's power iteration runs on the context's side stream beside the coarse-level builds: its
+  // own norm/counter and block partials, and the fork/join events
+  MgScratch* sc0 = nullptr;
+  double* part0 = nullptr;
+  cudaEvent_t fork_ev = nullptr, stencil_ev = nullptr, join_ev = nullptr;
   int sweeps = 1;
   int per_iter = 0;  // kernel launches per outer iteration
   cudaGraphExec_t graph[2] = {nullptr, nullptr};    // FP64 outer iteration chunks
@@ -2933,6 +2938,8 @@ void mg_release(mycel_problem* p) {
     }
     if (mg->cw.graph[k]) cudaGraphExecDestroy(mg->cw.graph[k]);
   }
+  for (cudaEvent_t e : {mg->fork_ev, mg->stencil_ev, mg->join_ev})
+    if (e) cudaEventDestroy(e);
   p->n_case_tmaps = 0;
   for (void* b : mg->bufs) cudaFreeAsync(b, p->ctx->stream);
   delete mg;
@@ -2990,6 +2997,11 @@ static int32_t mg_ensure(mycel_problem* p, bool* available) {
   const int64_t nc = mg->lv[L - 1].nd;
   mg->ainv = (double*)alloc(sizeof(double) * nc * nc);
   mg->sc = (MgScratch*)alloc(sizeof(MgScratch));
+  mg->sc0 = (MgScratch*)alloc(sizeof(MgScratch));
+  mg->part0 = (double*)alloc(sizeof(double) * 8 * (size_t)p->ctx->num_sms + 64);
+  cudaEventCreateWithFlags(&mg->fork_ev, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&mg->stencil_ev, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&mg->join_ev, cudaEventDisableTiming);
   mg->f_t = (float*)alloc(sizeof(float) * (size_t)p->g.n32);
   for (int l = 0; l < L - 1; ++l) mg->eig[l] = (float*)alloc(sizeof(float) * (size_t)(l ? mg->lv[l].nd : p->g.n32));
   mg->G = (float*)alloc(sizeof(float) * 8 * 576);
@@ -3109,8 +3121,39 @@ static MgPtrs mg_ptrs(float* const (&v)[kMgMaxCases], int n) {
 // coarsest level's dense inverse.
 static void mg_setup(mycel_problem* p) {
   MgHier* mg = p->mg;
-  cudaStream_t s = p->ctx->stream;
+  cudaStream_t s = p->ctx->stream, ss = p->ctx->side;
   MgLevel* lv = mg->lv;
+  const int sb = stream_blocks(p);
+  int nl = 0;
+  // power iteration for the damping of level l (all but the coarsest), on stream q
+  auto power = [&](int l, cudaStream_t q, MgScratch* sc, double* part) {
+    MgLevel& v = lv[l];
+    const int64_t n = l ? v.nd : p->g.n32;
+    const float* invd = l ? v.invd : p->d_invdf;
+    float* x = l ? v.xa : p->f_p0;
+    float* y = l ? v.t : p->f_ap;
+    const unsigned nb = l ? std::min<unsigned>(mg_blocks(n), (unsigned)sb) : (unsigned)sb;
+    if (mg->eig_valid) {
+      cudaMemcpyAsync(x, mg->eig[l], sizeof(float) * (size_t)n, cudaMemcpyDeviceToDevice, q);
+    } else {
+      k_mg_pow_init<<<nb, 256, 0, q>>>(n, invd, x);
+      nl++;
+    }
+    const int iters = mg->eig_valid ? kMgPowerItersWarm : kMgPowerIters;
+    for (int it = 0; it < iters; ++it) {
+      if (l) launch_mg_apply(q, v, mg_one(x), mg_one(nullptr), invd, mg_one(y), 0, nullptr, nullptr, 1);
+      else launch_mv32_variant<0>(p, q, p->f_p0, nullptr, nullptr, nullptr, p->f_ap, 1, nullptr, nullptr);
+      const bool last = it == iters - 1;
+      k_mg_pow_norm<<<nb, kT, 0, q>>>(n, y, invd, part, sc, last ? mg->sc->omega + l : nullptr);
+      k_mg_pow_scale<<<nb, 256, 0, q>>>(n, y, invd, sc, last ? mg->eig[l] : x);
+      nl += 3;
+    }
+  };
+  // the voxel level's power iteration needs only E and the diagonal (ready on s): it runs on the side stream
+  // while s builds the coarse levels
+  cudaEventRecord(mg->fork_ev, s);
+  cudaStreamWaitEvent(ss, mg->fork_ev, 0);
+  power(0, ss, mg->sc0, mg->part0);
   const MgDims& d1 = lv[1].d;
   const int64_t ne1 = (int64_t)d1.nx * d1.ny * d1.nz;
   k_mg_build1<<<(unsigned)std::min<int64_t>((ne1 + 3) / 4, 8 * (int64_t)p->ctx->num_sms), 256, 0, s>>>(
@@ -3126,33 +3169,15 @@ static void mg_setup(mycel_problem* p) {
                                                                            nullptr, src, dst, nullptr);
     k_mg_stencil<<<mg_blocks(3 * lv[l].nn), 256, 0, s>>>(d, dst, lv[l].S, lv[l].invd);
   }
-  k_mg_coarse_setup<<<1, 1024, kMgCoarseSmem, s>>>(lv[mg->L - 1].d, lv[mg->L - 1].S, mg->ainv);
-  int nl = 2 * (mg->L - 1) + 2;
-  // damping of every smoothed level (all but the coarsest) from its power iteration
-  const int sb = stream_blocks(p);
-  for (int l = 0; l < mg->L - 1; ++l) {
-    MgLevel& v = lv[l];
-    const int64_t n = l ? v.nd : p->g.n32;
-    const float* invd = l ? v.invd : p->d_invdf;
-    float* x = l ? v.xa : p->f_p0;
-    float* y = l ? v.t : p->f_ap;
-    const unsigned nb = l ? std::min<unsigned>(mg_blocks(n), (unsigned)sb) : (unsigned)sb;
-    if (mg->eig_valid) {
-      cudaMemcpyAsync(x, mg->eig[l], sizeof(float) * (size_t)n, cudaMemcpyDeviceToDevice, s);
-    } else {
-      k_mg_pow_init<<<nb, 256, 0, s>>>(n, invd, x);
-      nl++;
-    }
-    const int iters = mg->eig_valid ? kMgPowerItersWarm : kMgPowerIters;
-    for (int it = 0; it < iters; ++it) {
-      if (l) launch_mg_apply(s, v, mg_one(x), mg_one(nullptr), invd, mg_one(y), 0, nullptr, nullptr, 1);
-      else launch_mv32_variant<0>(p, s, p->f_p0, nullptr, nullptr, nullptr, p->f_ap, 1, nullptr, nullptr);
-      const bool last = it == iters - 1;
-      k_mg_pow_norm<<<nb, kT, 0, s>>>(n, y, invd, p->d_part2, mg->sc, last ? l : -1);
-      k_mg_pow_scale<<<nb, 256, 0, s>>>(n, y, invd, mg->sc, last ? mg->eig[l] : x);
-      nl += 3;
-    }
-  }
+  nl += 2 * (mg->L - 1) + 1;
+  // the coarsest level's dense inverse on the side stream too, beside the coarse levels' power iterations
+  cudaEventRecord(mg->stencil_ev, s);
+  cudaStreamWaitEvent(ss, mg->stencil_ev, 0);
+  k_mg_coarse_setup<<<1, 1024, kMgCoarseSmem, ss>>>(lv[mg->L - 1].d, lv[mg->L - 1].S, mg->ainv);
+  nl++;
+  for (int l = 1; l < mg->L - 1; ++l) power(l, s, mg->sc, p->d_part2);
+  cudaEventRecord(mg->join_ev, ss);
+  cudaStreamWaitEvent(s, mg->join_ev, 0);
   mg->eig_valid = true;
   p->ctx->launches += nl;
 }

@@ -99,6 +99,7 @@ struct MgHier;  // multigrid hierarchy of a problem (fp32_kernels.cu)
 struct mycel_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t side = nullptr;  // second stream for set-up work that can overlap the main stream's (joined back)
   int num_sms = 148;
   int oc_grid = 0;                  // blocks of the persistent OC kernel: num_sms x oc_blocks_per_sm(), set at creation
   int64_t oc_wait_polls = 0;        // polls of each OC grid-barrier wait before it gives up (0: the default)
