@@ -2000,67 +2000,6 @@ __global__ void __launch_bounds__(kMgDofThreads) k_mg_apply(MgDims d, const floa
   mg_apply_row(d, nn, n, mg_dof_comp(), S, x.p[c], r.p[c], invd, y.p[c], mode, mode == 1 ? *om : 0.0f);
 }
 
-// The same product with the 27 neighbour blocks split by neighbour plane (dz = -1, 0, 1): three threads per
-// node (threadIdx.y = plane), each gathering 9 neighbours for all three rows; the partial sums are added in
-// plane order through shared memory. Three times the threads in flight of k_mg_apply_nodes without its loads
-// repeated (the per-DOF kernel loads each neighbour's x once per row).
-template <bool MULTI>
-__global__ void __launch_bounds__(192) k_mg_apply_planes(MgDims d, const float* __restrict__ S,
-                                                         const __grid_constant__ MgPtrs x,
-                                                         const __grid_constant__ MgPtrs r,
-                                                         const float* __restrict__ invd,
-                                                         const __grid_constant__ MgPtrs y, int mode,
-                                                         const float* __restrict__ om, const MixState* st, int ncase) {
-  __shared__ float part[3][3][64];
-  const int tx = threadIdx.x, pz = threadIdx.y;
-  const int64_t nn = mg_nn(d);
-  int64_t n;
-  int c;
-  mg_item_case<MULTI>(blockIdx.x * (int64_t)64 + tx, ncase, &n, &c);
-  const bool valid = n < nn && mg_running(st ? st + c : nullptr);
-  float a0 = 0.f, a1 = 0.f, a2 = 0.f;
-  if (valid) {
-    const int nx1 = d.nx + 1, ny1 = d.ny + 1;
-    const int i = (int)(n % nx1), j = (int)((n / nx1) % ny1), k = (int)(n / ((int64_t)nx1 * ny1));
-    const float* xv = x.p[c];
-    const int uk = k + pz - 1;
-#pragma unroll
-    for (int q = 0; q < 9; ++q) {
-      const int nb = 9 * pz + q;
-      const int ui = i + q % 3 - 1, uj = j + q / 3 - 1;
-      const int mi = min(max(ui, 0), d.nx), mj = min(max(uj, 0), d.ny), mk = min(max(uk, 0), d.nz);
-      const bool in = mi == ui && mj == uj && mk == uk;
-      const int64_t m = mi + (int64_t)nx1 * (mj + (int64_t)ny1 * mk);
-      const float x0 = in ? xv[3 * m] : 0.f, x1 = in ? xv[3 * m + 1] : 0.f, x2 = in ? xv[3 * m + 2] : 0.f;
-      if (nb >= 13) {
-        const float* sp = S + (int64_t)(nb - 13) * 9 * nn + n;
-        a0 = fmaf(sp[0], x0, fmaf(sp[nn], x1, fmaf(sp[2 * nn], x2, a0)));
-        a1 = fmaf(sp[3 * nn], x0, fmaf(sp[4 * nn], x1, fmaf(sp[5 * nn], x2, a1)));
-        a2 = fmaf(sp[6 * nn], x0, fmaf(sp[7 * nn], x1, fmaf(sp[8 * nn], x2, a2)));
-      } else {
-        const float* sp = S + (int64_t)(13 - nb) * 9 * nn + m;
-        a0 = fmaf(sp[0], x0, fmaf(sp[3 * nn], x1, fmaf(sp[6 * nn], x2, a0)));
-        a1 = fmaf(sp[nn], x0, fmaf(sp[4 * nn], x1, fmaf(sp[7 * nn], x2, a1)));
-        a2 = fmaf(sp[2 * nn], x0, fmaf(sp[5 * nn], x1, fmaf(sp[8 * nn], x2, a2)));
-      }
-    }
-  }
-  part[pz][0][tx] = a0;
-  part[pz][1][tx] = a1;
-  part[pz][2][tx] = a2;
-  __syncthreads();
-  if (!valid || pz != 0) return;
-  const float omega = mode == 1 ? *om : 0.0f;
-#pragma unroll
-  for (int cc = 0; cc < 3; ++cc) {
-    const float acc = (part[0][cc][tx] + part[1][cc][tx]) + part[2][cc][tx];
-    const int64_t q = 3 * n + cc;
-    if (mode == 0) y.p[c][q] = acc;
-    else if (mode == 1) y.p[c][q] = fmaf(omega * invd[q], r.p[c][q] - acc, x.p[c][q]);
-    else y.p[c][q] = invd[q] != 0.0f ? r.p[c][q] - acc : 0.0f;
-  }
-}
-
 // a further sweep on the voxel grid (padded FP32 layout, t = A x): x += omega invd (r - t)
 __global__ void k_mg_jacobi_fine(int64_t n, const float* __restrict__ r, const float* __restrict__ t,
                                  const float* __restrict__ invd, float* __restrict__ x, const float* __restrict__ om,
@@ -2361,7 +2300,12 @@ struct MgTail {
   MgTailLevel lv[kMgMaxLevels];
 };
 
+// phase barrier of the tail kernel: the cluster's barrier, or the CTA's when it runs as one CTA
 __device__ __forceinline__ void mg_cluster_sync() {
+  if (gridDim.x == 1) {
+    __syncthreads();
+    return;
+  }
   asm volatile("barrier.cluster.arrive.release;\n" ::: "memory");
   asm volatile("barrier.cluster.wait.acquire;\n" ::: "memory");
 }
@@ -2370,7 +2314,7 @@ __device__ __forceinline__ void mg_cluster_sync() {
 // smoothed correction of level T, left in its xa. Work items are numbered with the case fastest; a case whose
 // state is not running is skipped, and the kernel returns at once (every thread alike) when none is.
 template <bool MULTI>
-__global__ void __cluster_dims__(kMgTailCtas, 1, 1) __launch_bounds__(kMgTailThreads)
+__global__ void __launch_bounds__(kMgTailThreads)
     k_mg_tail(const __grid_constant__ MgTail tl, const float* __restrict__ om, const MixState* st, int ncase) {
   bool any = false;
   for (int k = 0; k < ncase; ++k) any = any || mg_running(st ? st + k : nullptr);
@@ -3034,6 +2978,13 @@ static int32_t mg_ensure(mycel_problem* p, bool* available) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(kMgTailCtas);
     cfg.blockDim = dim3(kMgTailThreads);
+    cudaLaunchAttribute at{};
+    at.id = cudaLaunchAttributeClusterDimension;
+    at.val.clusterDim.x = kMgTailCtas;
+    at.val.clusterDim.y = 1;
+    at.val.clusterDim.z = 1;
+    cfg.attrs = &at;
+    cfg.numAttrs = 1;
     int nclusters = 0;
     int ncl2 = 0;
     if (cudaOccupancyMaxActiveClusters(&nclusters, k_mg_tail<false>, &cfg) != cudaSuccess || nclusters < 1 ||
@@ -3072,6 +3023,33 @@ static unsigned mg_blocks(int64_t n) { return (unsigned)((n + 255) / 256); }
 
 // coarse-level product on the stream: a thread per DOF up to 64k nodes, a thread per node above (measured on
 // the bridge: level 2, 31k nodes, 9.6 vs 14.5 us; level 1, 233k nodes, 43 vs 51 us)
+// the small levels' kernel: an 8-CTA cluster (cluster barriers between phases), or one CTA
+// (MYCEL_MG_TAIL_CTAS=1: CTA barriers)
+static int mg_tail_ctas() {
+  static const int ctas = [] {
+    const char* e = std::getenv("MYCEL_MG_TAIL_CTAS");
+    return (e && std::atoi(e) == 1) ? 1 : kMgTailCtas;
+  }();
+  return ctas;
+}
+
+static void launch_mg_tail(cudaStream_t s, MgHier* mg, const float* om, const MixState* st, int nc) {
+  const int ctas = mg_tail_ctas();
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(ctas);
+  cfg.blockDim = dim3(kMgTailThreads);
+  cfg.stream = s;
+  cudaLaunchAttribute at{};
+  at.id = cudaLaunchAttributeClusterDimension;
+  at.val.clusterDim.x = ctas;
+  at.val.clusterDim.y = 1;
+  at.val.clusterDim.z = 1;
+  cfg.attrs = &at;
+  cfg.numAttrs = ctas > 1 ? 1 : 0;
+  if (nc == 1) cudaLaunchKernelEx(&cfg, k_mg_tail<false>, mg->tail, om, st, nc);
+  else cudaLaunchKernelEx(&cfg, k_mg_tail<true>, mg->tail, om, st, nc);
+}
+
 // case k's vector of a level whose case vectors follow one another (base + k * nd)
 static MgPtrs lv_ptrs(float* base, int64_t nd, int n) {
   MgPtrs r{};
@@ -3079,22 +3057,9 @@ static MgPtrs lv_ptrs(float* base, int64_t nd, int n) {
   return r;
 }
 
-// product kernel of the large levels: a thread per node (default) or three per node split by neighbour plane
-// (MYCEL_MG_APPLY=planes)
-static bool mg_apply_planes() {
-  static const bool planes = [] {
-    const char* e = std::getenv("MYCEL_MG_APPLY");
-    return e && std::string(e) == "planes";
-  }();
-  return planes;
-}
-
 static void launch_mg_apply(cudaStream_t s, const MgLevel& v, const MgPtrs& x, const MgPtrs& r, const float* invd,
                             const MgPtrs& y, int mode, const float* om, const MixState* st, int nc) {
-  if (v.nn * nc > 65536 && mg_apply_planes())
-    (nc == 1 ? k_mg_apply_planes<false> : k_mg_apply_planes<true>)<<<(unsigned)((v.nn * nc + 63) / 64), dim3(64, 3),
-                                                                     0, s>>>(v.d, v.S, x, r, invd, y, mode, om, st, nc);
-  else if (v.nn * nc <= 65536)
+  if (v.nn * nc <= 65536)
     (nc == 1 ? k_mg_apply<false> : k_mg_apply<true>)<<<mg_dof_blocks(v.nn * nc), kMgDofThreads, 0, s>>>(
         v.d, v.S, x, r, invd, y, mode, om, st, nc);
   else
@@ -3233,7 +3198,7 @@ static int mg_vcycle(mycel_problem* p, cudaStream_t s, const MgRun& R) {
     xc[l] = x;
     nl += 1 + mg->sweeps;
   }
-  (nc == 1 ? k_mg_tail<false> : k_mg_tail<true>)<<<kMgTailCtas, kMgTailThreads, 0, s>>>(mg->tail, om, st, nc);
+  launch_mg_tail(s, mg, om, st, nc);
   xc[mg->T] = lv[mg->T].xa;
   nl++;
   for (int l = mg->T - 1; l >= 1; --l) {
