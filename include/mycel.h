@@ -175,6 +175,11 @@ int64_t mycel_ctx_launch_count(mycel_ctx* ctx);
    (event-record nodes inside the chunk graph; nodes = that level's nodes). Returns the summed device time, the
    number of timed launches and the nodes / active elements they covered. */
 int32_t mycel_ctx_set_profiling(mycel_ctx* ctx, int32_t enable);
+/* Device time of one launch of a solver kernel on this problem (no counterpart in the reference): `reps`
+   launches back to back in one CUDA graph, as the solver's chunk graphs issue them, timed by CUDA events on the
+   context stream after a warm-up launch; which = 0: the FP32 outer matvec of the mixed forms, 3: the multigrid
+   level-1 residual product. Uses only work vectors that hold nothing between solves. */
+int32_t mycel_problem_kernel_bench(mycel_problem* p, int32_t which, int32_t reps, double* avg_us);
 int32_t mycel_ctx_kernel_timing(mycel_ctx* ctx, int32_t which, double* total_ms, int64_t* launches, int64_t* nodes,
                                 int64_t* active_elements);
 /* Bounded waits of the OC kernel (no counterpart in the reference, whose OC runs on the host). The OC update is

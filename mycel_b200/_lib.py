@@ -98,6 +98,7 @@ SIGNATURES = {
     "mycel_ctx_launch_count": (i64, [P]),
     "mycel_ctx_set_profiling": (i32, [P, i32]),
     "mycel_ctx_set_oc_wait": (i32, [P, i64, i32]),
+    "mycel_problem_kernel_bench": (i32, [P, i32, i32, C.POINTER(dbl)]),
     "mycel_ctx_kernel_timing": (i32, [P, i32, C.POINTER(dbl), C.POINTER(i64), C.POINTER(i64), C.POINTER(i64)]),
     "mycel_problem_create": (i32, [P, C.POINTER(Grid), P, C.POINTER(Material), P, i32, P, i32, P, dbl,
                                    C.POINTER(P)]),

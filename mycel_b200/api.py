@@ -163,6 +163,13 @@ class Problem:
         the tensor cores, 3 factorised cube-element operator."""
         _check(L.load().mycel_problem_set_tuning(self.handle, 1, int(variant)), self.ctx)
 
+    def kernel_bench(self, which: int, reps: int = 20) -> float:
+        """Device microseconds of one launch of a solver kernel (0: FP32 outer matvec, 3: multigrid level-1
+        product), from `reps` launches back to back in one CUDA graph timed by CUDA events."""
+        us = C.c_double(0)
+        _check(L.load().mycel_problem_kernel_bench(self.handle, int(which), int(reps), C.byref(us)), self.ctx)
+        return us.value
+
     def matvec32(self) -> int:
         v = C.c_int32(0)
         _check(L.load().mycel_problem_get_tuning(self.handle, 1, C.byref(v)), self.ctx)

@@ -431,6 +431,12 @@ extern "C" int32_t mycel_ctx_set_oc_wait(mycel_ctx* c, int64_t max_polls, int32_
   return MYCEL_OK;
 }
 
+extern "C" int32_t mycel_problem_kernel_bench(mycel_problem* p, int32_t which, int32_t reps, double* avg_us) {
+  if (!p || !avg_us) return set_error(p ? p->ctx : nullptr, MYCEL_E_ARG, "NULL argument");
+  cudaSetDevice(p->ctx->device);
+  return kernel_bench(p, which, reps, avg_us);
+}
+
 extern "C" int32_t mycel_ctx_kernel_timing(mycel_ctx* c, int32_t which, double* total_ms, int64_t* launches,
                                            int64_t* nodes, int64_t* elems) {
   if (!c || which < 0 || which > 3) return set_error(c, MYCEL_E_ARG, "invalid argument");

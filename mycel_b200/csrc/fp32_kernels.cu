@@ -3815,6 +3815,80 @@ __global__ void k_mix_set_if(MixState* st, int from, int to) {
   if (st->status == from) st->status = to;
 }
 
+// Device time of one launch of a solver kernel, measured in place: `reps` launches back to back in one CUDA
+// graph (as the chunk graphs issue them), bracketed by CUDA events on the context stream after a warm-up
+// launch of the same graph. which 0: the FP32 outer matvec k_mv32f (MODE 1: p = z + beta p_old, K p, p.Ap)
+// on the problem's FP32 work vectors with a scratch state; 3: the multigrid level-1 residual product
+// (r - A x on level 1). Uses only work vectors that hold nothing between solves.
+int32_t kernel_bench(mycel_problem* p, int which, int reps, double* avg_us) {
+  mycel_ctx* c = p->ctx;
+  cudaStream_t s = c->stream;
+  int32_t st = MYCEL_OK;
+  if (reps < 1 || (which != 0 && which != 3)) return set_error(c, MYCEL_E_ARG, "kernel_bench: which / reps");
+  if ((st = ensure_pcg_workspace(p)) || (st = ensure_mixed(p)) || (st = resolve_mv32(p))) return st;
+  MgHier* mg = nullptr;
+  if (which == 3) {
+    bool avail = false;
+    if ((st = mg_ensure(p, &avail))) return st;
+    if (!avail || p->mg->T <= 1) return set_error(c, MYCEL_E_ARG, "kernel_bench: no multigrid level 1 on the whole GPU");
+    mg = p->mg;
+    if (mg->setup_version != p->e_version) {
+      mg_setup(p);
+      mg->setup_version = p->e_version;
+    }
+  }
+  MixState* ms = nullptr;
+  MYCEL_CUDA(c, cudaMallocAsync((void**)&ms, sizeof(MixState), s));
+  struct Free {
+    MixState* m; cudaStream_t s;
+    ~Free() { cudaFreeAsync(m, s); }
+  } fr{ms, s};
+  const unsigned sb = (unsigned)stream_blocks(p);
+  if (which == 0) {  // nonzero directions on the free DOFs, a running state
+    k_mg_pow_init<<<sb, 256, 0, s>>>(p->g.n32, p->d_invdf, p->f_z);
+    k_mg_pow_init<<<sb, 256, 0, s>>>(p->g.n32, p->d_invdf, p->f_p1);
+    k_mix_init<<<1, 1, 0, s>>>(ms, 0.0, INT32_MAX, 1e-3);
+  } else {
+    const MgLevel& v = mg->lv[1];
+    k_mg_pow_init<<<std::min<unsigned>(mg_blocks(v.nd), sb), 256, 0, s>>>(v.nd, v.invd, v.xa);
+    k_mg_pow_init<<<std::min<unsigned>(mg_blocks(v.nd), sb), 256, 0, s>>>(v.nd, v.invd, v.r);
+  }
+  cudaGraph_t graph;
+  cudaGraphExec_t exec = nullptr;
+  MYCEL_CUDA(c, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  for (int k = 0; k < reps; ++k) {
+    if (which == 0) {
+      float* pcur = (k & 1) ? p->f_p1 : p->f_p0;
+      float* pold = (k & 1) ? p->f_p0 : p->f_p1;
+      launch_mv32_variant<1>(p, s, nullptr, p->f_z, pold, pcur, p->f_ap, 1, ms, p->d_part2);
+    } else {
+      const MgLevel& v = mg->lv[1];
+      launch_mg_apply(s, v, mg_one(v.xa), mg_one(v.r), v.invd, mg_one(v.t), 2, nullptr, nullptr, 1);
+    }
+  }
+  MYCEL_CUDA(c, cudaStreamEndCapture(s, &graph));
+  cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) return set_error(c, MYCEL_E_DEVICE, std::string("kernel_bench: ") + cudaGetErrorString(e));
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaGraphLaunch(exec, s);  // warm-up
+  cudaEventRecord(e0, s);
+  cudaGraphLaunch(exec, s);
+  cudaEventRecord(e1, s);
+  e = cudaEventSynchronize(e1);
+  float ms_ = 0.f;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&ms_, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaGraphExecDestroy(exec);
+  c->launches += 2 * (int64_t)reps + 3;
+  if (e != cudaSuccess) return set_error(c, MYCEL_E_DEVICE, std::string("kernel_bench: ") + cudaGetErrorString(e));
+  *avg_us = 1000.0 * ms_ / reps;
+  return MYCEL_OK;
+}
+
 bool cases_together_enabled() {
   const char* e = std::getenv("MYCEL_CASES_TOGETHER");  // "0": one case after another (for comparisons)
   return !(e && e[0] == '0');

@@ -313,7 +313,8 @@ int32_t mixed_solve_entry(mycel_problem* p, const double* d_b, const int32_t* d_
 int32_t mg_solve_cases(mycel_problem* p, int ncase, double* d_u, double tol, int max_iter,
                        const volatile int32_t* cancel, mycel_pcg_result* res);
 constexpr int kMaxBatchedCases = 8;
-bool cases_together_enabled();  // MYCEL_CASES_TOGETHER=0 turns the batched case solve off
+bool cases_together_enabled();
+int32_t kernel_bench(mycel_problem* p, int which, int reps, double* avg_us);  // MYCEL_CASES_TOGETHER=0 turns the batched case solve off
 int32_t refined_solve_entry(mycel_problem* p, const double* d_b, const int32_t* d_nz, int32_t n_nz, double* d_u,
                             double tol, int max_iter, const volatile int32_t* cancel, int precision,
                             mycel_pcg_result* res);
