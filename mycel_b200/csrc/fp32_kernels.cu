@@ -3023,15 +3023,9 @@ static unsigned mg_blocks(int64_t n) { return (unsigned)((n + 255) / 256); }
 
 // coarse-level product on the stream: a thread per DOF up to 64k nodes, a thread per node above (measured on
 // the bridge: level 2, 31k nodes, 9.6 vs 14.5 us; level 1, 233k nodes, 43 vs 51 us)
-// the small levels' kernel: an 8-CTA cluster (cluster barriers between phases), or one CTA
-// (MYCEL_MG_TAIL_CTAS=1: CTA barriers)
-static int mg_tail_ctas() {
-  static const int ctas = [] {
-    const char* e = std::getenv("MYCEL_MG_TAIL_CTAS");
-    return (e && std::atoi(e) == 1) ? 1 : kMgTailCtas;
-  }();
-  return ctas;
-}
+// the small levels' kernel: one 8-CTA cluster with cluster barriers between phases (a single CTA with CTA
+// barriers was measured slower: 51.9 against 56.6 SIMP iter/s on the bridge)
+static int mg_tail_ctas() { return kMgTailCtas; }
 
 static void launch_mg_tail(cudaStream_t s, MgHier* mg, const float* om, const MixState* st, int nc) {
   const int ctas = mg_tail_ctas();
