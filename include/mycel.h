@@ -169,6 +169,9 @@ void* mycel_ctx_stream(mycel_ctx* ctx);
 const char* mycel_last_error(mycel_ctx* ctx);
 /* Kernel launches issued by this context since creation (all of them are this library's own kernels). */
 int64_t mycel_ctx_launch_count(mycel_ctx* ctx);
+/* Right-hand sides solved through packed launches (mycel_simp_step_many) on this context since creation; no
+   counterpart in the reference (a statistic of the packed form). */
+int64_t mycel_ctx_packed_count(mycel_ctx* ctx);
 /* Live timing of the dominant kernels: when enabled, PCG chunks record CUDA events around one stiffness matvec
    launch per chunk (on the context stream). which = 0: FP32 matvec of the mixed form, 1: FP64 matvec,
    2: FP64 matvec of the fast FP64 and multigrid forms, 3: the multigrid forms' level-1 residual product
@@ -313,6 +316,21 @@ int32_t mycel_simp_step(mycel_simp_session* s, mycel_iter_record* rec, int32_t* 
 int32_t mycel_simp_read(mycel_simp_session* s, double* u_out, float* physical_density_out, float* design_density_out,
                         double* rho_phys_active_out, double* rho_design_active_out, double* lambda_out);
 int32_t mycel_simp_end(mycel_simp_session* s);
+/* 1 once the session's stop rule has fired (TopologyOptimizationResult.Converged,
+   Optimization/TopologyOptimizationResult.cs:6-17; set by the rule at TopologyOptimizer.cs:374-390), else 0. */
+int32_t mycel_simp_converged(const mycel_simp_session* s);
+
+/* One SIMP iteration of each of n sessions, with their solves packed. No counterpart in the reference, which
+   runs one optimisation at a time (Optimization/OptimizationCoordinator.cs:229 through FemWorkTeam's lock,
+   Fem/FemWorkTeam.cs:109); it replaces n calls of mycel_simp_step. The sessions share one context and each
+   has its own problem. Those in MYCEL_PRECISION_MIXED_MG advance their FP32 outer iterations (and those of
+   their load cases kept apart) together: every kernel of an outer iteration is one launch for all of them,
+   whose CTAs are split between the problems by a per-problem table (grid, vectors, CTA range); the other
+   sessions are solved one after another. Every session takes the iteration mycel_simp_step would take, to the
+   bit. recs, done and status (each n entries, may be NULL) get each session's record, done flag and status;
+   the call returns the first failure. cancel is polled between chunks of outer iterations. */
+int32_t mycel_simp_step_many(mycel_simp_session* const* sessions, int32_t n, mycel_iter_record* recs, int32_t* done,
+                             int32_t* status, const volatile int32_t* cancel);
 
 /* RunWriter snapshot frames (Persistence/RunWriter.cs:132-160 WriteSnapshotAsync, :199-245 the it_NNNNNN
    frame, :344-356 ComputeQuantizedChecksum) of the last completed iteration, without stalling the loop:

@@ -96,6 +96,7 @@ SIGNATURES = {
     "mycel_ctx_stream": (P, [P]),
     "mycel_last_error": (C.c_char_p, [P]),
     "mycel_ctx_launch_count": (i64, [P]),
+    "mycel_ctx_packed_count": (i64, [P]),
     "mycel_ctx_set_profiling": (i32, [P, i32]),
     "mycel_ctx_set_oc_wait": (i32, [P, i64, i32]),
     "mycel_problem_kernel_bench": (i32, [P, i32, i32, C.POINTER(dbl)]),
@@ -131,6 +132,8 @@ SIGNATURES = {
                              C.POINTER(i32), C.POINTER(i32), P, P, P]),
     "mycel_simp_begin": (i32, [P, C.POINTER(SimpOptions), C.POINTER(P)]),
     "mycel_simp_step": (i32, [P, C.POINTER(IterRecord), C.POINTER(i32)]),
+    "mycel_simp_step_many": (i32, [C.POINTER(P), i32, C.POINTER(IterRecord), C.POINTER(i32), C.POINTER(i32), P]),
+    "mycel_simp_converged": (i32, [P]),
     "mycel_simp_read": (i32, [P, P, P, P, P, P, C.POINTER(dbl)]),
     "mycel_simp_end": (i32, [P]),
     "mycel_simp_frame_begin": (i32, [P, C.POINTER(i32)]),

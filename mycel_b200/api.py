@@ -12,7 +12,7 @@ import ctypes as C
 import threading
 import weakref
 from dataclasses import dataclass
-from typing import Callable, List, Optional
+from typing import Callable, List, Optional, Sequence
 
 import numpy as np
 
@@ -70,6 +70,11 @@ class Context:
     @property
     def launch_count(self) -> int:
         return int(L.load().mycel_ctx_launch_count(self.handle))
+
+    @property
+    def packed_count(self) -> int:
+        """Right-hand sides solved through packed launches on this context (mycel_simp_step_many)."""
+        return int(L.load().mycel_ctx_packed_count(self.handle))
 
     def set_profiling(self, on: bool = True):
         _check(L.load().mycel_ctx_set_profiling(self.handle, int(on)), self)
@@ -445,6 +450,17 @@ def _snapshot(r: L.IterRecord, phys=None, design=None) -> IterationSnapshot:
 
 class TopologyOptimizer:
     @staticmethod
+    def run_many(models: Sequence[FeModel], options=None, ctx: Optional[Context] = None,
+                 controller: Optional[IterationController] = None) -> List[TopologyOptimizationResult]:
+        """Several optimisations side by side on one GPU, one SIMP iteration of each per step
+        (mycel_simp_step_many): the mixed multigrid form's solves are packed into shared launches. options is
+        one OptimizerOptions for all or one per model. Each result equals TopologyOptimizer.run's for that
+        model alone with the same options; the snapshots carry densities only for the last iteration."""
+        if isinstance(options, OptimizerOptions) or options is None:
+            options = [options or OptimizerOptions()] * len(models)
+        return _run_many(list(models), list(options), ctx, controller)
+
+    @staticmethod
     def run(model: FeModel, options: Optional[OptimizerOptions] = None,
             progress: Optional[Callable[[IterationSnapshot], None]] = None,
             controller: Optional[IterationController] = None, ctx: Optional[Context] = None,
@@ -495,6 +511,40 @@ class TopologyOptimizer:
             prob.close()
 
 
+def _run_many(models: Sequence[FeModel], options: Sequence[OptimizerOptions], ctx: Optional["Context"] = None,
+              controller: Optional[IterationController] = None) -> List[TopologyOptimizationResult]:
+    ctx = ctx or default_context()
+    probs = []
+    sess = []
+    try:
+        probs = [Problem(m, ctx) for m in models]
+        sess = [SimpSession(p, o) for p, o in zip(probs, options)]
+        snaps = [[] for _ in sess]
+        while not all(s.done for s in sess):
+            if controller is not None and controller.is_stopped():
+                break
+            live = [k for k, s in enumerate(sess) if not s.done]
+            out = SimpSession.step_many([sess[k] for k in live], controller)
+            for k, r in zip(live, out):
+                if r is not None:
+                    snaps[k].append(r)
+        res = []
+        for s, sn in zip(sess, snaps):
+            d = s.read(u=True, densities=True)
+            if sn:
+                sn[-1].physical_density = d["physical"]
+                sn[-1].design_density = d["design"]
+            res.append(TopologyOptimizationResult(s.converged, len(sn), sn, sn[-1].compliance if sn else 0.0,
+                                                  sn[-1].volume_fraction if sn else 0.0, d["physical"], d["design"],
+                                                  d["u"]))
+        return res
+    finally:
+        for s in sess:
+            s.close()
+        for p in probs:
+            p.close()
+
+
 class SimpSession:
     """Device-resident SIMP state stepped by the caller (mycel_simp_begin / step / read / end)."""
 
@@ -516,6 +566,34 @@ class SimpSession:
         _check(L.load().mycel_simp_step(self.handle, C.byref(r), C.byref(d)), self.problem.ctx)
         self.done = bool(d.value)
         return _snapshot(r)
+
+    @staticmethod
+    def step_many(sessions: Sequence["SimpSession"], controller: Optional[IterationController] = None):
+        """One SIMP iteration of each session (mycel_simp_step_many): one context, one session per problem.
+        Sessions in the mixed multigrid form have their solves packed (one launch per kernel of an outer
+        iteration for all of them); each takes the iteration its own step() would take. Returns the
+        snapshots (None for a session that was done already)."""
+        n = len(sessions)
+        if n == 0:
+            return []
+        hs = (C.c_void_p * n)(*[s.handle for s in sessions])
+        recs = (L.IterRecord * n)()
+        done = (C.c_int32 * n)()
+        stat = (C.c_int32 * n)()
+        was_done = [s.done for s in sessions]
+        cancel = controller._cancel if controller else None
+        st = L.load().mycel_simp_step_many(hs, n, recs, done, stat,
+                                           C.addressof(cancel) if cancel is not None else None)
+        for k, s in enumerate(sessions):
+            if stat[k] == 0:
+                s.done = bool(done[k])
+        _check(st, sessions[0].problem.ctx)
+        return [None if was_done[k] else _snapshot(recs[k]) for k in range(n)]
+
+    @property
+    def converged(self) -> bool:
+        """The stop rule has fired (TopologyOptimizationResult.Converged)."""
+        return bool(L.load().mycel_simp_converged(self.handle))
 
     def read(self, u=True, densities=True, active=False):
         m = self.problem.model

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -400,6 +401,7 @@ extern "C" int32_t mycel_ctx_create(int32_t device, mycel_ctx** out) {
 extern "C" int32_t mycel_ctx_destroy(mycel_ctx* c) {
   if (!c) return MYCEL_OK;
   cudaSetDevice(c->device);
+  pack_release(c);  // frees on the stream: before it goes
   if (c->stream) {
     cudaStreamSynchronize(c->stream);
     cudaStreamDestroy(c->stream);
@@ -416,6 +418,7 @@ extern "C" int32_t mycel_ctx_destroy(mycel_ctx* c) {
 extern "C" void* mycel_ctx_stream(mycel_ctx* c) { return c ? (void*)c->stream : nullptr; }
 extern "C" const char* mycel_last_error(mycel_ctx* c) { return c ? c->last_error.c_str() : tls_error.c_str(); }
 extern "C" int64_t mycel_ctx_launch_count(mycel_ctx* c) { return c ? c->launches : 0; }
+extern "C" int64_t mycel_ctx_packed_count(mycel_ctx* c) { return c ? c->packed_rhs : 0; }
 
 extern "C" int32_t mycel_ctx_set_profiling(mycel_ctx* c, int32_t enable) {
   if (!c) return set_error(nullptr, MYCEL_E_ARG, "NULL context");
@@ -470,6 +473,8 @@ extern "C" int32_t mycel_problem_create(mycel_ctx* c, const mycel_grid* grid, co
   cudaSetDevice(c->device);
   (void)cudaGetLastError();  // do not report a stale error of an earlier, unrelated call
   mycel_problem* p = new mycel_problem();
+  static std::atomic<uint64_t> next_serial{1};
+  p->serial = next_serial.fetch_add(1);
   p->ctx = c;
   p->g = g;
   p->h = grid->h;

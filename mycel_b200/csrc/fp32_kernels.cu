@@ -53,17 +53,21 @@ struct MixState {
 constexpr int kT = 256;
 constexpr double kFlushFactor = 1e-1;
 
-__device__ __forceinline__ bool elect_last32(unsigned int* counter) {
+// the last of nblk CTAs to arrive (a launch's CTAs, or those of one problem of a packed launch)
+__device__ __forceinline__ bool elect_last_n(unsigned int* counter, unsigned nblk) {
   __shared__ bool last;
   __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) {
     unsigned int prev = atomicAdd(counter, 1u);
-    last = (prev == gridDim.x * gridDim.y - 1);
+    last = (prev == nblk - 1);
   }
   __syncthreads();
   if (last) __threadfence();
   return last;
+}
+__device__ __forceinline__ bool elect_last32(unsigned int* counter) {
+  return elect_last_n(counter, gridDim.x * gridDim.y);
 }
 
 // deterministic block sum of a double (result valid in linear thread 0); works for 1-D and 2-D blocks
@@ -477,10 +481,8 @@ __device__ __forceinline__ void hex_apply2(const HexOpF& op, float2 E, float2 (&
 // p.Ap partials of a matvec launch: CTA sum, fixed-order sum of the CTA partials by the last CTA, alpha.
 // A launch whose bounded waits gave up has set *err; its last CTA then ends the inner solve as a breakdown.
 __device__ __forceinline__ void mv32_finish(double pap, double* sh, MixState* st, double* part, int tid,
-                                            const int* err) {
+                                            const int* err, unsigned nblk, unsigned bid) {
   const double b = bsum(pap, sh);
-  const unsigned nblk = gridDim.x * gridDim.y * gridDim.z;
-  const unsigned bid = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
   if (tid == 0) part[bid] = b;
   __shared__ bool last;
   __threadfence();
@@ -519,13 +521,16 @@ __device__ __forceinline__ void tma_load_plane(void* dst, const CUtensorMap* map
       : "memory");
 }
 
+// The kernel body, for CTA (bx, by, bz) of a grid of nblk CTAs (linear number bid, x fastest): a launch of
+// one matvec (k_mv32f) or one problem's share of a packed launch (k_mv32f_pk). tm_a / tm_b point at the
+// tensor maps (kernel parameters, or a packed launch's table in global memory).
 template <int MODE>
-__global__ void __launch_bounds__(FX * FY, 2) k_mv32f(GridDims g, const __grid_constant__ HexOpF op,
-                                                      const __grid_constant__ CUtensorMap tm_a,
-                                                      const __grid_constant__ CUtensorMap tm_b,
-                                                      float* __restrict__ pnew, float* __restrict__ y,
-                                                      const float* __restrict__ E, const uint8_t* __restrict__ nf,
-                                                      int projected, MixState* st, double* part, int zseg, int* err) {
+__device__ __forceinline__ void mv32f_body(const GridDims& g, const HexOpF& op, const CUtensorMap* tm_a,
+                                           const CUtensorMap* tm_b, float* __restrict__ pnew,
+                                           float* __restrict__ y, const float* __restrict__ E,
+                                           const uint8_t* __restrict__ nf, int projected, MixState* st,
+                                           double* part, int zseg, int* err, int bx, int by, int bz, unsigned nblk,
+                                           unsigned bid) {
   extern __shared__ __align__(128) unsigned char fac_smem[];
   // [FNST] stages of x (MODE 0) or z (MODE 1), then MODE 1: [FNST] stages of p_{t-1}; then y-exchange
   float* yb = reinterpret_cast<float*>(fac_smem + (size_t)FNST * kFacStagePitch * (MODE == 1 ? 2 : 1));
@@ -535,7 +540,7 @@ __global__ void __launch_bounds__(FX * FY, 2) k_mv32f(GridDims g, const __grid_c
   const float beta = MODE == 1 ? (float)st->beta : 0.0f;
   const bool two = MODE == 1 && st->first == 0;  // p_t = z + beta p_{t-1} (else p_t = z)
   const int l = threadIdx.x, w = threadIdx.y, tid = w * FX + l;
-  const int i0 = blockIdx.x * FOX, j0 = blockIdx.y * FOY, k0 = blockIdx.z * zseg;
+  const int i0 = bx * FOX, j0 = by * FOY, k0 = bz * zseg;
   const int k1 = min(k0 + zseg, g.nz1);
   const int xs = (3 * (i0 - 1)) & ~3;   // staged row start (floats), 16-byte aligned, may be -4
   const int rem = 3 * (i0 - 1) - xs;    // offset of node i0 - 1 in a staged row
@@ -552,8 +557,8 @@ __global__ void __launch_bounds__(FX * FY, 2) k_mv32f(GridDims g, const __grid_c
     const int sl = r % FNST;
     const uint32_t bar = smem_u32(&full[sl]);
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(tx_bytes) : "memory");
-    tma_load_plane(plane_a(sl), &tm_a, xs, j0 - 1, k0 - 1 + r, bar);
-    if (two) tma_load_plane(plane_b(sl), &tm_b, xs, j0 - 1, k0 - 1 + r, bar);
+    tma_load_plane(plane_a(sl), tm_a, xs, j0 - 1, k0 - 1 + r, bar);
+    if (two) tma_load_plane(plane_b(sl), tm_b, xs, j0 - 1, k0 - 1 + r, bar);
   };
   if (tid == 0) {
     for (int q = 0; q < FNST; ++q)
@@ -688,7 +693,19 @@ __global__ void __launch_bounds__(FX * FY, 2) k_mv32f(GridDims g, const __grid_c
       for (int c = 0; c < 3; ++c) ub[b][c] = ut[b][c];
   }
   if (!ok && err) atomicExch(err, 1);
-  if (MODE == 1) mv32_finish(pap, sh, st, part, tid, err);
+  if (MODE == 1) mv32_finish(pap, sh, st, part, tid, err, nblk, bid);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(FX * FY, 2) k_mv32f(GridDims g, const __grid_constant__ HexOpF op,
+                                                      const __grid_constant__ CUtensorMap tm_a,
+                                                      const __grid_constant__ CUtensorMap tm_b,
+                                                      float* __restrict__ pnew, float* __restrict__ y,
+                                                      const float* __restrict__ E, const uint8_t* __restrict__ nf,
+                                                      int projected, MixState* st, double* part, int zseg, int* err) {
+  mv32f_body<MODE>(g, op, &tm_a, &tm_b, pnew, y, E, nf, projected, st, part, zseg, err, blockIdx.x, blockIdx.y,
+                   blockIdx.z, gridDim.x * gridDim.y * gridDim.z,
+                   (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x);
 }
 
 // z-segment length of the factorised kernel: the CTAs of a launch run in ceil(CTAs / resident) waves of
@@ -934,7 +951,9 @@ __global__ void __launch_bounds__(FX * FY, 2) k_mv64f(GridDims g, const __grid_c
       for (int c = 0; c < 3; ++c) ub[b][c] = ut[b][c];
   }
   if (!ok && err) atomicExch(err, 1);
-  if (MODE == 1) mv32_finish(pap, sh, st, part, tid, err);
+  if (MODE == 1)
+    mv32_finish(pap, sh, st, part, tid, err, gridDim.x * gridDim.y * gridDim.z,
+                (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x);
 }
 
 // z-segment length of the FP64 factorised kernel: one element plane per step
@@ -1333,6 +1352,22 @@ static void launch_mv64f(mycel_problem* p, cudaStream_t s, const double* xin, co
                                                                      p->d_nflags, projected, st, part, zs, p->d_err);
 }
 
+// resident CTAs per SM of the factorised FP32 matvec (same for both modes: same block, registers within bounds);
+// it sets the z-segments of a launch, so every launch of a grid (alone or packed) has the same CTA decomposition
+static int mv32f_resident_per_sm() {
+  static std::once_flag once;
+  static int occ = 1;
+  std::call_once(once, [] {
+    int o = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_mv32f<1>, FX * FY, fac_smem_bytes(1)) != cudaSuccess) {
+      cudaGetLastError();
+      o = 1;
+    }
+    occ = std::max(1, o);
+  });
+  return occ;
+}
+
 // FP32 matvec launch, variant chosen per problem (MYCEL_MV32_*)
 template <int MODE>
 static void launch_mv32_variant(mycel_problem* p, cudaStream_t s, const float* xin, const float* z, const float* pold,
@@ -1347,13 +1382,7 @@ static void launch_mv32_variant(mycel_problem* p, cudaStream_t s, const float* x
     k_mv32<MODE><<<tile_grid(g, zs), dim3(TX, TY), 0, s>>>(g, p->kef, xin, z, pold, pnew, y, p->d_Ef, p->d_nflags,
                                                            projected, st, part, zs);
   } else {
-    static int occ = 0;  // resident CTAs per SM (same for both modes: same block, registers within bounds)
-    if (!occ) {
-      int o = 0;
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_mv32f<1>, FX * FY, fac_smem_bytes(1));
-      occ = std::max(1, o);
-    }
-    int zs = fac_zseg(g, occ * p->ctx->num_sms);
+    int zs = fac_zseg(g, mv32f_resident_per_sm() * p->ctx->num_sms);
     const CUtensorMap* ta = tmap_of(p, MODE == 1 ? z : xin);
     const CUtensorMap* tb = MODE == 1 ? tmap_of(p, pold) : ta;
     if (!ta || !tb) {  // internal invariant: inputs are always one of the four mapped work vectors
@@ -2301,8 +2330,8 @@ struct MgTail {
 };
 
 // phase barrier of the tail kernel: the cluster's barrier, or the CTA's when it runs as one CTA
-__device__ __forceinline__ void mg_cluster_sync() {
-  if (gridDim.x == 1) {
+__device__ __forceinline__ void mg_cluster_sync(bool one_cta) {
+  if (one_cta) {
     __syncthreads();
     return;
   }
@@ -2313,14 +2342,14 @@ __device__ __forceinline__ void mg_cluster_sync() {
 // Levels T .. L-1 of the V-cycle for ncase load cases: from r of level T (restricted by the caller) to the
 // smoothed correction of level T, left in its xa. Work items are numbered with the case fastest; a case whose
 // state is not running is skipped, and the kernel returns at once (every thread alike) when none is.
+// Body for the threads gt (of gs) of the cluster (or the single CTA when one_cta) that runs this V-cycle's tail.
 template <bool MULTI>
-__global__ void __launch_bounds__(kMgTailThreads)
-    k_mg_tail(const __grid_constant__ MgTail tl, const float* __restrict__ om, const MixState* st, int ncase) {
+__device__ __forceinline__ void mg_tail_body(const MgTail& tl, const float* __restrict__ om, const MixState* st,
+                                             int ncase, int64_t gt, int64_t gs, bool one_cta) {
   bool any = false;
   for (int k = 0; k < ncase; ++k) any = any || mg_running(st ? st + k : nullptr);
   if (!any) return;
   auto live = [&](int k) { return mg_running(st ? st + k : nullptr); };
-  const int64_t gt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x, gs = (int64_t)gridDim.x * blockDim.x;
   float* xc[kMgMaxLevels];
   // a thread per (row, case) where the level's rows fit the cluster's threads, else a thread per (node, case)
   auto apply = [&](const MgTailLevel& v, const float* x, float* y, int mode, float w) {
@@ -2350,13 +2379,13 @@ __global__ void __launch_bounds__(kMgTailThreads)
     float *x = v.xa, *o = v.xb;  // x = omega invd r, written with r by the restriction into this level
     for (int k = 1; k < tl.sweeps; ++k) {
       apply(v, x, o, 1, w);
-      mg_cluster_sync();
+      mg_cluster_sync(one_cta);
       float* tmp = x;
       x = o;
       o = tmp;
     }
     apply(v, x, v.t, 2, 0.0f);
-    mg_cluster_sync();
+    mg_cluster_sync(one_cta);
     const bool smoothed = l + 1 < tl.L - 1;  // the coarsest level is solved, not smoothed
     const float wc = smoothed ? om[l + 1] : 0.0f;
     for (int64_t q = gt; q < cnd * ncase; q += gs) {
@@ -2367,7 +2396,7 @@ __global__ void __launch_bounds__(kMgTailThreads)
         mg_restrict_comp<false>(v.d, 0, nullptr, v.t + k * nd, cv.d, cv.invd, cv.r + k * cnd, it / 3, (int)(it % 3),
                                 smoothed ? cv.xa + k * cnd : nullptr, wc);
     }
-    mg_cluster_sync();
+    mg_cluster_sync(one_cta);
     xc[l] = x;
   }
   {  // coarsest level: x = A^-1 r, one warp per (row, case)
@@ -2386,7 +2415,7 @@ __global__ void __launch_bounds__(kMgTailThreads)
       for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
       if (lane == 0) v.xa[k * nd + row] = (float)acc;
     }
-    mg_cluster_sync();
+    mg_cluster_sync(one_cta);
     xc[tl.L - 1] = v.xa;
   }
   for (int l = tl.L - 2; l >= tl.T; --l) {
@@ -2403,10 +2432,10 @@ __global__ void __launch_bounds__(kMgTailThreads)
         mg_prolong_comp<false>(v.d, 0, nullptr, v.invd, x + k * nd, tl.lv[l + 1].d, xc[l + 1] + k * cnd, it / 3,
                                (int)(it % 3));
     }
-    mg_cluster_sync();
+    mg_cluster_sync(one_cta);
     for (int k = 0; k < tl.sweeps; ++k) {
       apply(v, x, o, 1, w);
-      mg_cluster_sync();
+      mg_cluster_sync(one_cta);
       float* tmp = x;
       x = o;
       o = tmp;
@@ -2423,6 +2452,13 @@ __global__ void __launch_bounds__(kMgTailThreads)
       if (live(k)) vt.xa[k * nd + it] = xc[tl.T][k * nd + it];
     }
   }
+}
+
+template <bool MULTI>
+__global__ void __launch_bounds__(kMgTailThreads)
+    k_mg_tail(const __grid_constant__ MgTail tl, const float* __restrict__ om, const MixState* st, int ncase) {
+  mg_tail_body<MULTI>(tl, om, st, ncase, blockIdx.x * (int64_t)blockDim.x + threadIdx.x,
+                      (int64_t)gridDim.x * blockDim.x, gridDim.x == 1);
 }
 
 // Outer step, part 1. mode 0: x += alpha p, r -= alpha q (FP64, padded layout), ||r|| against the stop and
@@ -2474,17 +2510,18 @@ __global__ void __launch_bounds__(kT) k_mg_enter(GridDims g, double* __restrict_
 // sums by the last CTA. mode 0: beta = -alpha (z, A p) / rho, rho = (z, r). mode 1 (after a true-residual
 // replacement, direction kept): the same beta, new replacement threshold. mode 2 (start): rho, next direction
 // p = z.
-__device__ __forceinline__ void mg_exit_tail(double b1, double b2, double b3, MixState* st, double* part, int mode) {
+__device__ __forceinline__ void mg_exit_tail(double b1, double b2, double b3, MixState* st, double* part, int mode,
+                                             unsigned bx, unsigned nb) {
   if (threadIdx.x == 0) {
-    part[blockIdx.x] = b1;
-    part[gridDim.x + blockIdx.x] = b2;
-    part[2 * gridDim.x + blockIdx.x] = b3;
+    part[bx] = b1;
+    part[nb + bx] = b2;
+    part[2 * nb + bx] = b3;
   }
-  if (!elect_last32(&st->counter)) return;
+  if (!elect_last_n(&st->counter, nb)) return;
   if (threadIdx.x >= 32) return;
-  const double szr = warp_sum_parts(part, gridDim.x);
-  const double szq = warp_sum_parts(part + gridDim.x, gridDim.x);
-  const double srr = warp_sum_parts(part + 2 * gridDim.x, gridDim.x);
+  const double szr = warp_sum_parts(part, nb);
+  const double szq = warp_sum_parts(part + nb, nb);
+  const double srr = warp_sum_parts(part + 2 * nb, nb);
   if (threadIdx.x != 0) return;
   st->counter = 0;
   if (!(szr > 0.0) || !isfinite(szr)) {  // (z, r) > 0 for an SPD preconditioner and r != 0
@@ -2540,23 +2577,25 @@ __global__ void __launch_bounds__(kT) k_mg_exit(GridDims g, const float* __restr
   const double b1 = bsum(zr, sh);
   const double b2 = bsum(zq, sh);
   const double b3 = bsum(rr, sh);
-  mg_exit_tail(b1, b2, b3, st, part, mode);
+  mg_exit_tail(b1, b2, b3, st, part, mode, blockIdx.x, gridDim.x);
 }
 
 // The same two parts for the FP32 outer iteration (mixed multigrid form): all vectors in the padded FP32 layout,
 // the voxel level's residual is the outer residual r itself and its smoothed correction is built in place in z
 // (a mapped matvec input). Dots accumulate in FP64.
-__global__ void __launch_bounds__(kT) k_mg_enter32(int64_t n, float* __restrict__ x, float* __restrict__ r,
-                                                   const float* __restrict__ p, const float* __restrict__ q,
-                                                   const float* __restrict__ invd, float* __restrict__ xf,
-                                                   const float* __restrict__ om, MixState* st, double* part, int mode) {
+// body for CTA bx of nb (a launch, or one unit's share of a packed launch)
+__device__ __forceinline__ void mg_enter32_body(int64_t n, float* __restrict__ x, float* __restrict__ r,
+                                                const float* __restrict__ p, const float* __restrict__ q,
+                                                const float* __restrict__ invd, float* __restrict__ xf,
+                                                const float* __restrict__ om, MixState* st, double* part, int mode,
+                                                unsigned bx, unsigned nb) {
   __shared__ double sh[32];
   if (!mg_running(st)) return;
   const float alpha = (float)st->alpha;
   const float omega = *om;
   double rr = 0.0;
   const int64_t n4 = n >> 2;  // n is a multiple of 4 (row pitch)
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n4; i += (int64_t)gridDim.x * blockDim.x) {
+  for (int64_t i = bx * (int64_t)blockDim.x + threadIdx.x; i < n4; i += (int64_t)nb * blockDim.x) {
     float4 rv = reinterpret_cast<const float4*>(r)[i];
     const float4 iv = reinterpret_cast<const float4*>(invd)[i];
     if (mode == 0) {
@@ -2576,10 +2615,10 @@ __global__ void __launch_bounds__(kT) k_mg_enter32(int64_t n, float* __restrict_
   }
   if (mode != 0) return;
   const double br = bsum(rr, sh);
-  if (threadIdx.x == 0) part[blockIdx.x] = br;
-  if (!elect_last32(&st->counter)) return;
+  if (threadIdx.x == 0) part[bx] = br;
+  if (!elect_last_n(&st->counter, nb)) return;
   if (threadIdx.x >= 32) return;
-  const double s = warp_sum_parts(part, gridDim.x);
+  const double s = warp_sum_parts(part, nb);
   if (threadIdx.x != 0) return;
   st->counter = 0;
   const double rn = sqrt(s);
@@ -2589,16 +2628,23 @@ __global__ void __launch_bounds__(kT) k_mg_enter32(int64_t n, float* __restrict_
   else if (st->iter >= st->max_iter) st->status = MIX_MAXITER;
 }
 
-__global__ void __launch_bounds__(kT) k_mg_exit32(int64_t n, const float* __restrict__ r, const float* __restrict__ tf,
-                                                  float* __restrict__ z, const float* __restrict__ invd,
-                                                  const float* __restrict__ q, const float* __restrict__ om,
-                                                  MixState* st, double* part, int mode) {
+__global__ void __launch_bounds__(kT) k_mg_enter32(int64_t n, float* __restrict__ x, float* __restrict__ r,
+                                                   const float* __restrict__ p, const float* __restrict__ q,
+                                                   const float* __restrict__ invd, float* __restrict__ xf,
+                                                   const float* __restrict__ om, MixState* st, double* part, int mode) {
+  mg_enter32_body(n, x, r, p, q, invd, xf, om, st, part, mode, blockIdx.x, gridDim.x);
+}
+
+__device__ __forceinline__ void mg_exit32_body(int64_t n, const float* __restrict__ r, const float* __restrict__ tf,
+                                               float* __restrict__ z, const float* __restrict__ invd,
+                                               const float* __restrict__ q, const float* __restrict__ om,
+                                               MixState* st, double* part, int mode, unsigned bx, unsigned nb) {
   __shared__ double sh[32];
   if (!mg_running(st)) return;
   const float omega = *om;
   double zr = 0.0, zq = 0.0, rr = 0.0;
   const int64_t n4 = n >> 2;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n4; i += (int64_t)gridDim.x * blockDim.x) {
+  for (int64_t i = bx * (int64_t)blockDim.x + threadIdx.x; i < n4; i += (int64_t)nb * blockDim.x) {
     const float4 rv = reinterpret_cast<const float4*>(r)[i];
     const float4 tv = reinterpret_cast<const float4*>(tf)[i];
     const float4 iv = reinterpret_cast<const float4*>(invd)[i];
@@ -2616,7 +2662,14 @@ __global__ void __launch_bounds__(kT) k_mg_exit32(int64_t n, const float* __rest
   const double b1 = bsum(zr, sh);
   const double b2 = bsum(zq, sh);
   const double b3 = bsum(rr, sh);
-  mg_exit_tail(b1, b2, b3, st, part, mode);
+  mg_exit_tail(b1, b2, b3, st, part, mode, bx, nb);
+}
+
+__global__ void __launch_bounds__(kT) k_mg_exit32(int64_t n, const float* __restrict__ r, const float* __restrict__ tf,
+                                                  float* __restrict__ z, const float* __restrict__ invd,
+                                                  const float* __restrict__ q, const float* __restrict__ om,
+                                                  MixState* st, double* part, int mode) {
+  mg_exit32_body(n, r, tf, z, invd, q, om, st, part, mode, blockIdx.x, gridDim.x);
 }
 
 // Power iteration for lambda_max(D^-1 A) of a level: a fixed pseudo-random start on DOFs with a nonzero
@@ -3375,7 +3428,9 @@ static void launch_inner_chunk(mycel_problem* p, const InnerForm& F, int gi) {
 // input; the fast FP64 forms' own residual, overwritten here anyway), A u to a vector free at this point (g_x,
 // the fast FP64 forms' correction, already added to u and cleared again here; g_ap in the mixed form, whose
 // vectors are FP32).
-static int32_t true_residual(mycel_problem* p, const InnerForm& F, const double* d_b, const double* d_u, double* rn) {
+// Issues it and the copy of ||r||^2 to *h (pinned host memory) on the context stream, without waiting.
+static int32_t true_residual_issue(mycel_problem* p, const InnerForm& F, const double* d_b, const double* d_u,
+                                   double* h) {
   mycel_ctx* c = p->ctx;
   cudaStream_t s = c->stream;
   int sb = stream_blocks(p);
@@ -3388,9 +3443,16 @@ static int32_t true_residual(mycel_problem* p, const InnerForm& F, const double*
   else k_resid64p<float><<<sb, kT, 0, s>>>(p->g, p->d_nflags, d_b, au, (float*)F.r, part, 0);
   k_sum_part<<<1, 32, 0, s>>>(part, sb, scal);
   c->launches += 4;
-  double* h = (double*)((char*)c->pinned + 1024);
   MYCEL_CUDA(c, cudaMemcpyAsync(h, scal, sizeof(double), cudaMemcpyDeviceToHost, s));
-  MYCEL_CUDA(c, cudaStreamSynchronize(s));
+  return MYCEL_OK;
+}
+
+static int32_t true_residual(mycel_problem* p, const InnerForm& F, const double* d_b, const double* d_u, double* rn) {
+  mycel_ctx* c = p->ctx;
+  double* h = (double*)((char*)c->pinned + 1024);
+  int32_t st = true_residual_issue(p, F, d_b, d_u, h);
+  if (st) return st;
+  MYCEL_CUDA(c, cudaStreamSynchronize(c->stream));
   *rn = std::sqrt(h[0]);
   return MYCEL_OK;
 }
@@ -4105,6 +4167,1006 @@ int32_t mg_solve_cases(mycel_problem* p, int ncase, double* d_u, double tol, int
     res[k].final_residual = rel[k];
     res[k].converged = 1;
     res[k].elapsed_ms = ms;
+  }
+  return MYCEL_OK;
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// Packed solves: the FP32 outer iterations of the mixed multigrid form for many problems (and for the load
+// cases of each) advance together, every kernel of an outer iteration one launch for all of them. A packed
+// launch splits its CTAs between entries (one per right-hand side at the voxel level, one per problem on the
+// coarse levels) through a table in device memory: entry e owns the CTAs [starts[e], starts[e + 1]) and holds
+// the arguments its launch alone would take, and runs the same kernel body with its CTA number within its
+// share. Each share has the CTA decomposition of the launch alone, so every reduction sums the same partials
+// in the same order and each right-hand side gets the bits of its solve alone. Problems with different level
+// counts are aligned by level index: the step of level l covers the problems whose V-cycle launches level l
+// separately (above its cluster kernel). Rounds as for the load cases of one problem (mg_solve_cases): chunks
+// of two outer iterations run until no right-hand side is running; then each is refined in FP64 and those not
+// converged restart together. A right-hand side that stalls, breaks down or runs out of iterations is
+// finished alone from its refined u, as a single solve goes on after its FP32 outer iteration.
+// ---------------------------------------------------------------------------------------------------------
+constexpr int kPkMaxUnits = 1024;
+constexpr int kPkStall = 100;  // state op: a running right-hand side's cycle stalled (replacement point)
+
+// entry of CTA b of a packed launch: the last e with starts[e] <= b (starts ascending from 0; uniform per CTA)
+__device__ __forceinline__ int pk_entry(const unsigned* __restrict__ starts, int n, unsigned b) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(starts + mid) <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+struct alignas(64) PkMv {  // one FP32 matvec (k_mv32f) of a right-hand side
+  CUtensorMap ta, tb;
+  GridDims g;
+  HexOpF op;
+  float* pnew;
+  float* y;
+  const float* E;
+  const uint8_t* nf;
+  MixState* st;
+  double* part;
+  int* err;
+  int projected, zseg;
+  unsigned gx, gy, gz;
+};
+
+template <int MODE>
+__global__ void __launch_bounds__(FX * FY, 2) k_mv32f_pk(const PkMv* __restrict__ tab,
+                                                         const unsigned* __restrict__ starts, int n) {
+  const int e = pk_entry(starts, n, blockIdx.x);
+  const PkMv* m = tab + e;
+  const unsigned lb = blockIdx.x - __ldg(starts + e);
+  const unsigned gx = m->gx, gy = m->gy;
+  if (threadIdx.x == 0 && threadIdx.y == 0) {  // the thread that issues the copies; maps written before launch
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(&m->ta) : "memory");
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(&m->tb) : "memory");
+  }
+  const GridDims g = m->g;
+  mv32f_body<MODE>(g, m->op, &m->ta, &m->tb, m->pnew, m->y, m->E, m->nf, m->projected, m->st, m->part, m->zseg,
+                   m->err, (int)(lb % gx), (int)((lb / gx) % gy), (int)(lb / (gx * gy)), gx * gy * m->gz, lb);
+}
+
+struct PkVec {  // k_mg_enter32 / k_mg_exit32 of a right-hand side
+  int64_t n;
+  float *x, *r, *p, *q, *z, *t;
+  const float* invd;
+  const float* om;
+  MixState* st;
+  double* part;
+  unsigned nb;
+};
+
+__global__ void __launch_bounds__(kT) k_mg_enter32_pk(const PkVec* __restrict__ tab, const unsigned* __restrict__ starts,
+                                                      int n, int mode) {
+  const int e = pk_entry(starts, n, blockIdx.x);
+  const PkVec& a = tab[e];
+  mg_enter32_body(a.n, a.x, a.r, a.p, a.q, a.invd, a.z, a.om, a.st, a.part, mode, blockIdx.x - __ldg(starts + e),
+                  a.nb);
+}
+
+__global__ void __launch_bounds__(kT) k_mg_exit32_pk(const PkVec* __restrict__ tab, const unsigned* __restrict__ starts,
+                                                     int n, int mode) {
+  const int e = pk_entry(starts, n, blockIdx.x);
+  const PkVec& a = tab[e];
+  mg_exit32_body(a.n, a.r, a.t, a.z, a.invd, a.q, a.om, a.st, a.part, mode, blockIdx.x - __ldg(starts + e), a.nb);
+}
+
+struct PkApply {  // a coarse-level product of a problem (all its cases)
+  MgDims d;
+  const float* S;
+  MgPtrs x, r, y;
+  const float* invd;
+  const float* om;
+  const MixState* st;
+  int ncase;
+};
+
+template <bool MULTI>
+__global__ void __launch_bounds__(256) k_mg_apply_nodes_pk(const PkApply* __restrict__ tab,
+                                                           const unsigned* __restrict__ starts, int n, int mode) {
+  const int e = pk_entry(starts, n, blockIdx.x);
+  const PkApply& a = tab[e];
+  const int64_t nn = mg_nn(a.d);
+  int64_t q;
+  int c;
+  mg_item_case<MULTI>((int64_t)(blockIdx.x - __ldg(starts + e)) * blockDim.x + threadIdx.x, a.ncase, &q, &c);
+  if (q >= nn || !mg_running(a.st ? a.st + c : nullptr)) return;
+  mg_apply_node(a.d, nn, q, a.S, a.x.p[c], a.r.p[c], a.invd, a.y.p[c], mode, mode == 1 ? *a.om : 0.0f);
+}
+
+template <bool MULTI>
+__global__ void __launch_bounds__(kMgDofThreads) k_mg_apply_pk(const PkApply* __restrict__ tab,
+                                                               const unsigned* __restrict__ starts, int n, int mode) {
+  const int e = pk_entry(starts, n, blockIdx.x);
+  const PkApply& a = tab[e];
+  const int64_t nn = mg_nn(a.d);
+  int64_t q;
+  int c;
+  mg_item_case<MULTI>((int64_t)(blockIdx.x - __ldg(starts + e)) * 64 + (threadIdx.x & 63), a.ncase, &q, &c);
+  if (q >= nn || !mg_running(a.st ? a.st + c : nullptr)) return;
+  mg_apply_row(a.d, nn, q, (int)(threadIdx.x >> 6), a.S, a.x.p[c], a.r.p[c], a.invd, a.y.p[c], mode,
+               mode == 1 ? *a.om : 0.0f);
+}
+
+struct PkRestrict {  // restriction of a problem's level to the next coarser one (all its cases)
+  MgDims f, c;
+  int pitch, first_sweep, ncase;
+  MgPtrs rf, tf, rc, xc;
+  const float* invdc;
+  const MixState* st;
+  const float* om;
+};
+
+template <bool PAD, bool MULTI>
+__global__ void k_mg_restrict_pk(const PkRestrict* __restrict__ tab, const unsigned* __restrict__ starts, int n) {
+  const int e = pk_entry(starts, n, blockIdx.x);
+  const PkRestrict& a = tab[e];
+  int64_t q;
+  int k;
+  mg_item_case<MULTI>((int64_t)(blockIdx.x - __ldg(starts + e)) * blockDim.x + threadIdx.x, a.ncase, &q, &k);
+  if (q >= mg_nn(a.c) || !mg_running(a.st ? a.st + k : nullptr)) return;
+  const float omega = a.first_sweep ? *a.om : 0.f;
+  mg_restrict_node<PAD>(a.f, a.pitch, a.rf.p[k], a.tf.p[k], a.c, a.invdc, a.rc.p[k], q,
+                        a.first_sweep ? a.xc.p[k] : nullptr, omega);
+}
+
+struct PkProlong {  // prolongation of a problem's level to the next finer one (all its cases)
+  MgDims f, c;
+  int pitch, ncase;
+  const uint8_t* nf;
+  const float* invdf;
+  MgPtrs xf, xc;
+  const MixState* st;
+};
+
+template <bool PAD, bool MULTI>
+__global__ void k_mg_prolong_pk(const PkProlong* __restrict__ tab, const unsigned* __restrict__ starts, int n) {
+  const int e = pk_entry(starts, n, blockIdx.x);
+  const PkProlong& a = tab[e];
+  int64_t q;
+  int k;
+  mg_item_case<MULTI>((int64_t)(blockIdx.x - __ldg(starts + e)) * blockDim.x + threadIdx.x, a.ncase, &q, &k);
+  if (q >= mg_nn(a.f) || !mg_running(a.st ? a.st + k : nullptr)) return;
+  mg_prolong_node<PAD>(a.f, a.pitch, a.nf, a.invdf, a.xf.p[k], a.c, a.xc.p[k], q);
+}
+
+struct PkTail {  // the cluster kernel of a problem's V-cycle (all its cases); one cluster per entry
+  MgTail tl;
+  const float* om;
+  const MixState* st;
+  int ncase;
+};
+
+template <bool MULTI>
+__global__ void __launch_bounds__(kMgTailThreads) k_mg_tail_pk(const PkTail* __restrict__ tab) {
+  const PkTail& t = tab[blockIdx.x / kMgTailCtas];
+  mg_tail_body<MULTI>(t.tl, t.om, t.st, t.ncase, (int64_t)(blockIdx.x % kMgTailCtas) * blockDim.x + threadIdx.x,
+                      (int64_t)kMgTailCtas * blockDim.x, false);
+}
+
+// state ops of the right-hand sides (a kernel parameter, so the host may rewrite its copy at once): -1 none,
+// kPkStall FLUSH if running, else the new status
+struct PkOps {
+  int n;
+  signed char op[kPkMaxUnits];
+};
+__global__ void k_pk_set(MixState* const* __restrict__ sts, const __grid_constant__ PkOps o) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= o.n || o.op[i] < 0) return;
+  MixState* st = sts[i];
+  if (o.op[i] == kPkStall) {
+    if (st->status == MIX_RUNNING) st->status = MIX_FLUSH;
+  } else {
+    st->status = o.op[i];
+  }
+}
+__global__ void k_pk_gather(MixState* const* __restrict__ sts, int n, MixState* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = *sts[i];
+}
+struct PkInit {
+  double target;
+  int max_iter;
+  int active;  // 0: the right-hand side takes no part (its state is set done)
+};
+// k_mix_init of every active right-hand side (flush factor of the FP32 multigrid form), DONE for the others
+__global__ void k_pk_init(MixState* const* __restrict__ sts, const PkInit* __restrict__ in, int n, double flush) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (!in[i].active) {
+    sts[i]->status = MIX_DONE;
+    return;
+  }
+  MixState s = {};
+  s.status = MIX_RUNNING;
+  s.target = in[i].target;
+  s.max_iter = in[i].max_iter;
+  s.first = 1;
+  s.flush_factor = flush;
+  *sts[i] = s;
+}
+
+enum PkKind : int { PK_MV0, PK_MV1, PK_ENTER, PK_EXIT, PK_APPLY_DOF, PK_APPLY_NODE, PK_RESTRICT, PK_PROLONG, PK_TAIL };
+
+struct PkLaunch {
+  int kind;
+  bool pad, multi;
+  int mode;            // apply: 1 sweep, 2 residual (enter / exit take the step's mode)
+  size_t tab, starts;  // byte offsets in the plan's device arena
+  int n;
+  unsigned blocks;
+};
+
+// A right-hand side of a packed solve: its voxel-level FP32 vectors, state, RHS and solution.
+struct PkUnit {
+  mycel_problem* p;
+  int job, k;  // k: load case, -1 the problem's single right-hand side
+  float *x, *r, *z, *p0, *p1, *ap, *t;
+  const CUtensorMap *tz, *tp0, *tp1;
+  MixState* st;
+  double* part;
+  const double* b;
+  const int32_t* bnz;
+  int32_t nbnz;
+  double* u;
+};
+
+struct PackPlan {
+  std::vector<uint64_t> key;
+  void* arena_alloc = nullptr;
+  void* arena = nullptr;        // device tables (128-byte aligned inside arena_alloc)
+  size_t arena_bytes = 0;
+  int nu = 0;
+  MixState** d_sts = nullptr;   // [nu] state pointers (in the arena)
+  MixState* d_states = nullptr; // [nu] gathered states
+  PkInit* d_init = nullptr;     // [nu]
+  std::vector<PkLaunch> mv1[2], enter[2], exitl, vcycle;
+  cudaGraphExec_t chunk = nullptr;
+  int per_chunk = 0;
+};
+
+// packed-solve workspace of a context: the plan of the latest set of right-hand sides and pinned host slots
+struct PackWork {
+  PackPlan plan;
+  void* pinned = nullptr;
+  size_t pinned_bytes = 0;
+  std::vector<void*> part_bufs;  // per-unit partial-sum buffers of the plan (device)
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+};
+
+static void pk_release_plan(mycel_ctx* c, PackWork* w) {
+  PackPlan& P = w->plan;
+  if (P.chunk) cudaGraphExecDestroy(P.chunk);
+  if (P.arena_alloc) cudaFreeAsync(P.arena_alloc, c->stream);
+  for (void* b : w->part_bufs) cudaFreeAsync(b, c->stream);
+  w->part_bufs.clear();
+  P = PackPlan();
+}
+
+void pack_release(mycel_ctx* c) {
+  PackWork* w = (PackWork*)c->pack;
+  if (!w) return;
+  pk_release_plan(c, w);
+  if (w->pinned) cudaFreeHost(w->pinned);
+  for (cudaEvent_t e : w->ev)
+    if (e) cudaEventDestroy(e);
+  delete w;
+  c->pack = nullptr;
+}
+
+// host-side table builder: entries of one packed launch, 64-byte aligned, then their CTA starts
+struct PkBuilder {
+  std::vector<unsigned char> host;
+  size_t put(const void* src, size_t bytes, size_t align) {
+    size_t off = (host.size() + align - 1) & ~(align - 1);
+    host.resize(off + bytes);
+    std::memcpy(host.data() + off, src, bytes);
+    return off;
+  }
+  template <class T>
+  void add(std::vector<PkLaunch>& out, int kind, bool pad, bool multi, int mode, const std::vector<T>& ents,
+           const std::vector<unsigned>& nblk) {
+    if (ents.empty()) return;
+    PkLaunch L{};
+    L.kind = kind;
+    L.pad = pad;
+    L.multi = multi;
+    L.mode = mode;
+    L.n = (int)ents.size();
+    L.tab = put(ents.data(), sizeof(T) * ents.size(), 64);
+    std::vector<unsigned> st(ents.size());
+    unsigned acc = 0;
+    for (size_t e = 0; e < ents.size(); ++e) {
+      st[e] = acc;
+      acc += nblk[e];
+    }
+    L.blocks = acc;
+    L.starts = put(st.data(), sizeof(unsigned) * st.size(), 16);
+    out.push_back(L);
+  }
+};
+
+static void pk_issue(const PackPlan& P, const PkLaunch& L, cudaStream_t s, int step_mode) {
+  const char* base = (const char*)P.arena;
+  const void* tab = base + L.tab;
+  const unsigned* st = (const unsigned*)(base + L.starts);
+  switch (L.kind) {
+    case PK_MV0:
+      k_mv32f_pk<0><<<L.blocks, dim3(FX, FY), fac_smem_bytes(0), s>>>((const PkMv*)tab, st, L.n);
+      break;
+    case PK_MV1:
+      k_mv32f_pk<1><<<L.blocks, dim3(FX, FY), fac_smem_bytes(1), s>>>((const PkMv*)tab, st, L.n);
+      break;
+    case PK_ENTER:
+      k_mg_enter32_pk<<<L.blocks, kT, 0, s>>>((const PkVec*)tab, st, L.n, step_mode);
+      break;
+    case PK_EXIT:
+      k_mg_exit32_pk<<<L.blocks, kT, 0, s>>>((const PkVec*)tab, st, L.n, step_mode);
+      break;
+    case PK_APPLY_DOF:
+      (L.multi ? k_mg_apply_pk<true> : k_mg_apply_pk<false>)<<<L.blocks, kMgDofThreads, 0, s>>>(
+          (const PkApply*)tab, st, L.n, L.mode);
+      break;
+    case PK_APPLY_NODE:
+      (L.multi ? k_mg_apply_nodes_pk<true> : k_mg_apply_nodes_pk<false>)<<<L.blocks, 256, 0, s>>>(
+          (const PkApply*)tab, st, L.n, L.mode);
+      break;
+    case PK_RESTRICT: {
+      auto k = L.pad ? (L.multi ? k_mg_restrict_pk<true, true> : k_mg_restrict_pk<true, false>)
+                     : (L.multi ? k_mg_restrict_pk<false, true> : k_mg_restrict_pk<false, false>);
+      k<<<L.blocks, 256, 0, s>>>((const PkRestrict*)tab, st, L.n);
+      break;
+    }
+    case PK_PROLONG: {
+      auto k = L.pad ? (L.multi ? k_mg_prolong_pk<true, true> : k_mg_prolong_pk<true, false>)
+                     : (L.multi ? k_mg_prolong_pk<false, true> : k_mg_prolong_pk<false, false>);
+      k<<<L.blocks, 256, 0, s>>>((const PkProlong*)tab, st, L.n);
+      break;
+    }
+    case PK_TAIL: {
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3((unsigned)(kMgTailCtas * L.n));
+      cfg.blockDim = dim3(kMgTailThreads);
+      cfg.stream = s;
+      cudaLaunchAttribute at{};
+      at.id = cudaLaunchAttributeClusterDimension;
+      at.val.clusterDim.x = kMgTailCtas;
+      at.val.clusterDim.y = 1;
+      at.val.clusterDim.z = 1;
+      cfg.attrs = &at;
+      cfg.numAttrs = 1;
+      if (L.multi) cudaLaunchKernelEx(&cfg, k_mg_tail_pk<true>, (const PkTail*)tab);
+      else cudaLaunchKernelEx(&cfg, k_mg_tail_pk<false>, (const PkTail*)tab);
+      break;
+    }
+  }
+}
+
+// one outer step of every unit (mode 0: after the matvec, pcur p0 (sel 0) or p1; 1: after a replacement;
+// 2: start): k_mg_enter32, the V-cycle, k_mg_exit32, all packed. Returns the launches.
+static int pk_step(const PackPlan& P, cudaStream_t s, int mode, int sel) {
+  for (const PkLaunch& L : P.enter[sel]) pk_issue(P, L, s, mode);
+  for (const PkLaunch& L : P.vcycle) pk_issue(P, L, s, mode);
+  for (const PkLaunch& L : P.exitl) pk_issue(P, L, s, mode);
+  return (int)(P.enter[sel].size() + P.vcycle.size() + P.exitl.size());
+}
+
+// Builds the packed launches of the units (grouped by problem: the units of a problem with load cases are its
+// cases 0 .. n-1, in order) and the chunk graph, with the arguments, grids and level order that mg_vcycle,
+// launch_mg_step and launch_mv32_variant issue for each problem alone.
+static int32_t pk_build(mycel_ctx* c, PackWork* w, std::vector<PkUnit>& units, const std::vector<uint64_t>& key) {
+  cudaStream_t s = c->stream;
+  pk_release_plan(c, w);
+  PackPlan& P = w->plan;
+  const int nu = (int)units.size();
+  // per-unit partial sums: the matvec's CTA partials and 3 per stream block of k_mg_exit32
+  for (PkUnit& u : units) {
+    const GridDims& g = u.p->g;
+    const int zs = fac_zseg(g, mv32f_resident_per_sm() * c->num_sms);
+    const dim3 gr = fac_grid(g, zs);
+    const size_t need = std::max<size_t>((size_t)gr.x * gr.y * gr.z, 3 * (size_t)stream_blocks(u.p)) + 64;
+    void* b = nullptr;
+    if (cudaMallocAsync(&b, sizeof(double) * need, s) != cudaSuccess)
+      return set_error(c, MYCEL_E_OOM, "out of device memory for the packed solve's partial sums");
+    w->part_bufs.push_back(b);
+    u.part = (double*)b;
+  }
+  PkBuilder B;
+  std::vector<MixState*> sts(nu);
+  for (int i = 0; i < nu; ++i) sts[i] = units[i].st;
+  const size_t o_sts = B.put(sts.data(), sizeof(MixState*) * nu, 64);
+  std::vector<MixState> zs_(nu);
+  std::memset(zs_.data(), 0, sizeof(MixState) * nu);
+  const size_t o_states = B.put(zs_.data(), sizeof(MixState) * nu, 64);
+  std::vector<PkInit> ini(nu);
+  const size_t o_init = B.put(ini.data(), sizeof(PkInit) * nu, 64);
+  auto mv_entry = [&](const PkUnit& u, const CUtensorMap* ta, const CUtensorMap* tb, float* pnew, float* y,
+                      MixState* st, double* part, unsigned* nb) {
+    mycel_problem* p = u.p;
+    PkMv m;
+    std::memset(&m, 0, sizeof m);
+    m.ta = *ta;
+    m.tb = *tb;
+    m.g = p->g;
+    m.op = p->hexop;
+    m.pnew = pnew;
+    m.y = y;
+    m.E = p->d_Ef;
+    m.nf = p->d_nflags;
+    m.st = st;
+    m.part = part;
+    m.err = p->d_err;
+    m.projected = 1;
+    m.zseg = fac_zseg(p->g, mv32f_resident_per_sm() * c->num_sms);
+    const dim3 gr = fac_grid(p->g, m.zseg);
+    m.gx = gr.x;
+    m.gy = gr.y;
+    m.gz = gr.z;
+    *nb = gr.x * gr.y * gr.z;
+    return m;
+  };
+  for (int t = 0; t < 2; ++t) {  // outer K p: t = 0 p0 = z + beta p1, t = 1 p1 = z + beta p0
+    std::vector<PkMv> e;
+    std::vector<unsigned> nb;
+    for (const PkUnit& u : units) {
+      unsigned n_ = 0;
+      e.push_back(mv_entry(u, u.tz, t ? u.tp0 : u.tp1, t ? u.p1 : u.p0, u.ap, u.st, u.part, &n_));
+      nb.push_back(n_);
+    }
+    B.add(P.mv1[t], PK_MV1, false, false, 1, e, nb);
+  }
+  for (int sel = 0; sel < 2; ++sel) {
+    std::vector<PkVec> e;
+    std::vector<unsigned> nb;
+    for (const PkUnit& u : units) {
+      PkVec v{};
+      v.n = u.p->g.n32;
+      v.x = u.x;
+      v.r = u.r;
+      v.p = sel ? u.p1 : u.p0;
+      v.q = u.ap;
+      v.z = u.z;
+      v.t = u.t;
+      v.invd = u.p->d_invdf;
+      v.om = u.p->mg->sc->omega;
+      v.st = u.st;
+      v.part = u.part;
+      v.nb = (unsigned)stream_blocks(u.p);
+      e.push_back(v);
+      nb.push_back(v.nb);
+    }
+    B.add(P.enter[sel], PK_ENTER, false, false, 0, e, nb);
+    if (sel == 0) B.add(P.exitl, PK_EXIT, false, false, 0, e, nb);
+  }
+  struct Prob {  // a problem: its first unit and case count
+    mycel_problem* p;
+    int u0, nc;
+    const MixState* st;
+  };
+  std::vector<Prob> probs;
+  for (int i = 0; i < nu;) {
+    int j = i;
+    while (j < nu && units[j].p == units[i].p) ++j;
+    probs.push_back({units[i].p, i, j - i, units[i].st});
+    i = j;
+  }
+  auto fine_mv = [&]() {  // t = A z at the voxel level, every unit (MODE 0)
+    std::vector<PkMv> e;
+    std::vector<unsigned> nb;
+    for (const PkUnit& u : units) {
+      unsigned n_ = 0;
+      e.push_back(mv_entry(u, u.tz, u.tz, nullptr, u.t, u.st, nullptr, &n_));
+      nb.push_back(n_);
+    }
+    B.add(P.vcycle, PK_MV0, false, false, 0, e, nb);
+  };
+  auto unit_ptrs = [&](const Prob& q, int which) {  // voxel-level vectors of a problem's units: r, t or z
+    MgPtrs r{};
+    for (int k = 0; k < q.nc; ++k) {
+      const PkUnit& u = units[q.u0 + k];
+      r.p[k] = which == 0 ? u.r : (which == 1 ? u.t : u.z);
+    }
+    return r;
+  };
+  int maxT = 1;
+  for (const Prob& q : probs) maxT = std::max(maxT, q.p->mg->T);
+  std::vector<std::vector<float*>> xc(probs.size(), std::vector<float*>(kMgMaxLevels, nullptr));
+  fine_mv();
+  for (int multi = 0; multi < 2; ++multi) {  // voxel grid -> level 1, with level 1's first sweep
+    std::vector<PkRestrict> e;
+    std::vector<unsigned> nb;
+    for (const Prob& q : probs) {
+      if ((q.nc > 1) != (multi == 1)) continue;
+      MgHier* mg = q.p->mg;
+      const MgLevel& v1 = mg->lv[1];
+      PkRestrict a{};
+      a.f = mg->lv[0].d;
+      a.pitch = q.p->g.rp;
+      a.rf = unit_ptrs(q, 0);
+      a.tf = unit_ptrs(q, 1);
+      a.c = v1.d;
+      a.invdc = v1.invd;
+      a.rc = lv_ptrs(v1.r, v1.nd, q.nc);
+      a.st = q.st;
+      a.xc = lv_ptrs(v1.xa, v1.nd, q.nc);
+      a.first_sweep = 1 < mg->L - 1 ? 1 : 0;
+      a.om = mg->sc->omega + 1;
+      a.ncase = q.nc;
+      e.push_back(a);
+      nb.push_back(mg_blocks(v1.nn * q.nc));
+    }
+    B.add(P.vcycle, PK_RESTRICT, true, multi == 1, 0, e, nb);
+  }
+  auto applies = [&](int l, bool down) {  // level l's product of every problem that smooths it separately
+    for (int node = 0; node < 2; ++node)
+      for (int multi = 0; multi < 2; ++multi) {
+        std::vector<PkApply> e;
+        std::vector<unsigned> nb;
+        for (size_t qi = 0; qi < probs.size(); ++qi) {
+          const Prob& q = probs[qi];
+          MgHier* mg = q.p->mg;
+          if (l >= mg->T || (q.nc > 1) != (multi == 1)) continue;
+          const MgLevel& v = mg->lv[l];
+          const bool is_node = !(v.nn * q.nc <= 65536);
+          if (is_node != (node == 1)) continue;
+          PkApply a{};
+          a.d = v.d;
+          a.S = v.S;
+          a.invd = v.invd;
+          a.r = lv_ptrs(v.r, v.nd, q.nc);
+          a.x = lv_ptrs(v.xa, v.nd, q.nc);                  // down: the restriction's first sweep; up: prolonged
+          a.y = lv_ptrs(down ? v.t : v.xb, v.nd, q.nc);      // down: r - A x; up: one sweep into xb
+          a.om = mg->sc->omega + l;
+          a.st = q.st;
+          a.ncase = q.nc;
+          e.push_back(a);
+          nb.push_back(node ? mg_blocks(v.nn * q.nc) : mg_dof_blocks(v.nn * q.nc));
+        }
+        B.add(P.vcycle, node ? PK_APPLY_NODE : PK_APPLY_DOF, false, multi == 1, down ? 2 : 1, e, nb);
+      }
+  };
+  for (int l = 1; l < maxT; ++l) {
+    applies(l, true);
+    for (int multi = 0; multi < 2; ++multi) {  // level l -> l + 1
+      std::vector<PkRestrict> e;
+      std::vector<unsigned> nb;
+      for (size_t qi = 0; qi < probs.size(); ++qi) {
+        const Prob& q = probs[qi];
+        MgHier* mg = q.p->mg;
+        if (l >= mg->T || (q.nc > 1) != (multi == 1)) continue;
+        const MgLevel& v = mg->lv[l];
+        const MgLevel& cv = mg->lv[l + 1];
+        PkRestrict a{};
+        a.f = v.d;
+        a.pitch = 0;
+        a.rf = lv_ptrs(nullptr, 0, q.nc);
+        a.tf = lv_ptrs(v.t, v.nd, q.nc);
+        a.c = cv.d;
+        a.invdc = cv.invd;
+        a.rc = lv_ptrs(cv.r, cv.nd, q.nc);
+        a.st = q.st;
+        a.xc = lv_ptrs(cv.xa, cv.nd, q.nc);
+        a.first_sweep = l + 1 < mg->L - 1 ? 1 : 0;
+        a.om = mg->sc->omega + l + 1;
+        a.ncase = q.nc;
+        e.push_back(a);
+        nb.push_back(mg_blocks(cv.nn * q.nc));
+        xc[qi][l] = v.xa;
+      }
+      B.add(P.vcycle, PK_RESTRICT, false, multi == 1, 0, e, nb);
+    }
+  }
+  for (int multi = 0; multi < 2; ++multi) {  // the cluster kernels
+    std::vector<PkTail> e;
+    std::vector<unsigned> nb;
+    for (size_t qi = 0; qi < probs.size(); ++qi) {
+      const Prob& q = probs[qi];
+      if ((q.nc > 1) != (multi == 1)) continue;
+      MgHier* mg = q.p->mg;
+      PkTail t{};
+      t.tl = mg->tail;
+      t.om = mg->sc->omega;
+      t.st = q.st;
+      t.ncase = q.nc;
+      e.push_back(t);
+      nb.push_back(kMgTailCtas);
+      xc[qi][mg->T] = mg->lv[mg->T].xa;
+    }
+    B.add(P.vcycle, PK_TAIL, false, multi == 1, 0, e, nb);
+  }
+  for (int l = maxT - 1; l >= 1; --l) {
+    for (int multi = 0; multi < 2; ++multi) {  // level l + 1 -> l, into xa (the downward sweep's vector)
+      std::vector<PkProlong> e;
+      std::vector<unsigned> nb;
+      for (size_t qi = 0; qi < probs.size(); ++qi) {
+        const Prob& q = probs[qi];
+        MgHier* mg = q.p->mg;
+        if (l >= mg->T || (q.nc > 1) != (multi == 1)) continue;
+        const MgLevel& v = mg->lv[l];
+        PkProlong a{};
+        a.f = v.d;
+        a.pitch = 0;
+        a.nf = nullptr;
+        a.invdf = v.invd;
+        a.xf = lv_ptrs(xc[qi][l], v.nd, q.nc);
+        a.c = mg->lv[l + 1].d;
+        a.xc = lv_ptrs(xc[qi][l + 1], mg->lv[l + 1].nd, q.nc);
+        a.st = q.st;
+        a.ncase = q.nc;
+        e.push_back(a);
+        nb.push_back(mg_blocks(v.nn * q.nc));
+      }
+      B.add(P.vcycle, PK_PROLONG, false, multi == 1, 0, e, nb);
+    }
+    applies(l, false);
+    for (size_t qi = 0; qi < probs.size(); ++qi)
+      if (l < probs[qi].p->mg->T) xc[qi][l] = probs[qi].p->mg->lv[l].xb;  // one sweep: xa -> xb
+  }
+  for (int multi = 0; multi < 2; ++multi) {  // level 1 -> voxel grid, into each unit's z
+    std::vector<PkProlong> e;
+    std::vector<unsigned> nb;
+    for (size_t qi = 0; qi < probs.size(); ++qi) {
+      const Prob& q = probs[qi];
+      if ((q.nc > 1) != (multi == 1)) continue;
+      MgHier* mg = q.p->mg;
+      PkProlong a{};
+      a.f = mg->lv[0].d;
+      a.pitch = q.p->g.rp;
+      a.nf = q.p->d_nflags;
+      a.invdf = nullptr;
+      a.xf = unit_ptrs(q, 2);
+      a.c = mg->lv[1].d;
+      a.xc = lv_ptrs(xc[qi][1], mg->lv[1].nd, q.nc);
+      a.st = q.st;
+      a.ncase = q.nc;
+      e.push_back(a);
+      nb.push_back(mg_blocks(mg->lv[0].nn * q.nc));
+    }
+    B.add(P.vcycle, PK_PROLONG, true, multi == 1, 0, e, nb);
+  }
+  fine_mv();
+  P.arena_bytes = B.host.size();
+  MYCEL_CUDA(c, cudaMallocAsync(&P.arena_alloc, P.arena_bytes + 128, s));
+  P.arena = (void*)(((uintptr_t)P.arena_alloc + 127) & ~(uintptr_t)127);  // tensor maps: 64-byte aligned
+  MYCEL_CUDA(c, cudaMemcpyAsync(P.arena, B.host.data(), P.arena_bytes, cudaMemcpyHostToDevice, s));
+  MYCEL_CUDA(c, cudaStreamSynchronize(s));
+  P.nu = nu;
+  P.d_sts = (MixState**)((char*)P.arena + o_sts);
+  P.d_states = (MixState*)((char*)P.arena + o_states);
+  P.d_init = (PkInit*)((char*)P.arena + o_init);
+  P.key = key;
+  // chunk graph: two outer iterations of every unit, then the states gathered for one copy
+  cudaGraph_t graph;
+  MYCEL_CUDA(c, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  int nl = 0;
+  for (int t = 0; t < 2; ++t) {
+    for (const PkLaunch& L : P.mv1[t]) pk_issue(P, L, s, 0);
+    nl += (int)P.mv1[t].size() + pk_step(P, s, 0, t);
+  }
+  k_pk_gather<<<(nu + 127) / 128, 128, 0, s>>>(P.d_sts, nu, P.d_states);
+  nl++;
+  MYCEL_CUDA(c, cudaStreamEndCapture(s, &graph));
+  cudaError_t ge = cudaGraphInstantiate(&P.chunk, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ge != cudaSuccess) return set_error(c, MYCEL_E_DEVICE, std::string("packed chunk graph: ") + cudaGetErrorString(ge));
+  P.per_chunk = nl;
+  return MYCEL_OK;
+}
+
+static int32_t pk_set(mycel_ctx* c, const PackPlan& P, const std::vector<signed char>& op) {
+  PkOps o;
+  o.n = P.nu;
+  std::memset(o.op, -1, sizeof o.op);
+  for (int i = 0; i < P.nu; ++i) o.op[i] = op[i];
+  k_pk_set<<<(P.nu + 127) / 128, 128, 0, c->stream>>>(P.d_sts, o);
+  c->launches++;
+  MYCEL_CUDA(c, cudaGetLastError());
+  return MYCEL_OK;
+}
+
+int32_t mg_solve_packed(mycel_ctx* c, int njobs, PackJob* jobs, const volatile int32_t* cancel) {
+  cudaStream_t s = c->stream;
+  auto t0 = std::chrono::steady_clock::now();
+  int32_t st = MYCEL_OK;
+  static std::once_flag smem_once;  // the packed matvec's shared memory above the 48 KB default
+  static cudaError_t smem_err = cudaSuccess;
+  std::call_once(smem_once, [] {
+    cudaError_t a = cudaFuncSetAttribute(k_mv32f_pk<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fac_smem_bytes(0));
+    cudaError_t b = cudaFuncSetAttribute(k_mv32f_pk<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fac_smem_bytes(1));
+    smem_err = a != cudaSuccess ? a : b;
+  });
+  if (smem_err != cudaSuccess)
+    return set_error(c, MYCEL_E_DEVICE, std::string("packed matvec shared memory: ") + cudaGetErrorString(smem_err));
+  std::vector<PkUnit> units;
+  std::vector<char> packed(njobs, 0);
+  // eligibility; the others are solved alone here, in job order
+  for (int j = 0; j < njobs; ++j) {
+    PackJob& J = jobs[j];
+    mycel_problem* p = J.p;
+    for (int k = 0; k < J.ncase; ++k) std::memset(J.res + k, 0, sizeof(mycel_pcg_result));
+    if (p->ctx != c) return set_error(c, MYCEL_E_ARG, "packed solve: every problem must belong to the context");
+    if (p->n_active_fixed < 6)
+      return set_error(c, MYCEL_E_UNDERCONSTRAINED,
+                       "Model has fewer than 6 unique fixed DOFs on active nodes (found " +
+                           std::to_string(p->n_active_fixed) +
+                           "). At least 6 fixed DOFs are required to prevent rigid body modes in 3D.");
+    if (J.ncase < 1 || J.ncase > kMgMaxCases) return set_error(c, MYCEL_E_ARG, "packed solve: case count");
+    if ((st = ensure_pcg_workspace(p)) || (st = ensure_mixed(p)) || (st = ensure_f64f(p))) return st;
+    if (J.ncase > 1 && (st = ensure_cases(p))) return st;
+    bool avail = false;
+    if ((st = resolve_mv32(p)) || (st = mg_ensure(p, &avail))) return st;
+    bool ok = avail && !p->mg->prefers_f64 && p->mg->sweeps == 1 && p->mv32 == MYCEL_MV32_FACTORED &&
+              (J.ncase == 1 || J.ncase <= p->mg->ncap) && (int)units.size() + J.ncase <= kPkMaxUnits;
+    for (int i = 0; i < j && ok; ++i) ok = !(packed[i] && jobs[i].p == p);  // one job per problem
+    if (ok && J.ncase > 1 && (st = mg_ensure_cases(p, J.ncase))) return st;
+    if (!ok) {
+      if (J.ncase == 1)
+        st = refined_solve_entry(p, p->d_b, p->d_bnz, p->n_bnz, J.d_u, J.tol, J.max_iter, cancel,
+                                 MYCEL_PRECISION_MIXED_MG, J.res);
+      else
+        st = mg_solve_cases(p, J.ncase, J.d_u, J.tol, J.max_iter, cancel, J.res);
+      if (st) return st;
+      continue;
+    }
+    packed[j] = 1;
+    MgHier* mg = p->mg;
+    MYCEL_CUDA(c, cudaMemsetAsync(p->d_err, 0, sizeof(int), s));
+    if (mg->setup_version != p->e_version) {
+      mg_setup(p);
+      mg->setup_version = p->e_version;
+    }
+    const int64_t nd = p->g.nd;
+    for (int k = 0; k < J.ncase; ++k) {
+      PkUnit u{};
+      u.p = p;
+      u.job = j;
+      if (J.ncase == 1) {
+        u.k = -1;
+        u.x = p->f_x; u.r = p->f_r; u.z = p->f_z; u.p0 = p->f_p0; u.p1 = p->f_p1; u.ap = p->f_ap; u.t = mg->f_t;
+        u.tz = &p->f_tmap[1];
+        u.tp0 = &p->f_tmap[2];
+        u.tp1 = &p->f_tmap[3];
+        u.st = mix_state(p);
+        u.b = p->d_b;
+        u.bnz = p->d_bnz;
+        u.nbnz = p->n_bnz;
+        u.u = J.d_u;
+      } else {
+        u.k = k;
+        u.x = cwv(mg, k, 0); u.r = cwv(mg, k, 1); u.z = cwv(mg, k, 2); u.p0 = cwv(mg, k, 3); u.p1 = cwv(mg, k, 4);
+        u.ap = cwv(mg, k, 5); u.t = cwv(mg, k, 6);
+        u.tz = &mg->cw.tmap[k][1];
+        u.tp0 = &mg->cw.tmap[k][2];
+        u.tp1 = &mg->cw.tmap[k][3];
+        u.st = mg->cw.st + k;
+        u.b = p->d_case_b + (int64_t)k * nd;
+        u.bnz = p->d_case_nz + p->case_nz_off[2 * k + 1];
+        u.nbnz = p->case_nz_cnt[2 * k + 1];
+        u.u = J.d_u + (int64_t)k * nd;
+      }
+      units.push_back(u);
+    }
+  }
+  const int nu = (int)units.size();
+  if (nu == 0) return MYCEL_OK;
+  if (!c->pack) c->pack = new PackWork();
+  PackWork* w = (PackWork*)c->pack;
+  const size_t pin_need = (size_t)nu * (2 * sizeof(MixState) + 2 * sizeof(double) + sizeof(PkInit)) + 4096;
+  if (w->pinned_bytes < pin_need) {
+    if (w->pinned) cudaFreeHost(w->pinned);
+    w->pinned = nullptr;
+    w->pinned_bytes = 0;
+    MYCEL_CUDA(c, cudaMallocHost(&w->pinned, pin_need));
+    w->pinned_bytes = pin_need;
+  }
+  for (int q = 0; q < 2; ++q)
+    if (!w->ev[q]) MYCEL_CUDA(c, cudaEventCreateWithFlags(&w->ev[q], cudaEventDisableTiming));
+  MixState* slot[2] = {(MixState*)w->pinned, (MixState*)w->pinned + nu};
+  double* h_bn = (double*)(slot[1] + nu);
+  double* h_rn2 = h_bn + nu;
+  PkInit* h_init = (PkInit*)(h_rn2 + nu);
+  // the plan of this set of right-hand sides (rebuilt when the set changes)
+  std::vector<uint64_t> key;
+  for (const PkUnit& u : units) {
+    key.push_back(u.p->serial);
+    key.push_back((uint64_t)(int64_t)u.k);
+  }
+  if (w->plan.key != key || !w->plan.chunk) {
+    if ((st = pk_build(c, w, units, key))) return st;
+  } else {
+    for (int i = 0; i < nu; ++i) units[i].part = (double*)w->part_bufs[i];
+  }
+  PackPlan& P = w->plan;
+  c->packed_rhs += nu;
+  struct Saved {
+    mycel_problem* p;
+    double* b;
+    int32_t* nz;
+    int32_t n;
+  };
+  std::vector<Saved> saved;
+  for (const PkUnit& u : units)
+    if (saved.empty() || saved.back().p != u.p) saved.push_back({u.p, u.p->d_b, u.p->d_bnz, u.p->n_bnz});
+  struct RestoreAll {
+    std::vector<Saved>* v;
+    ~RestoreAll() {
+      for (Saved& r : *v) r.p->d_b = r.b, r.p->d_bnz = r.nz, r.p->n_bnz = r.n;
+    }
+  } restore_all{&saved};
+  auto bind = [&](const PkUnit& u) {
+    u.p->d_b = const_cast<double*>(u.b);
+    u.p->d_bnz = const_cast<int32_t*>(u.bnz);
+    u.p->n_bnz = u.nbnz;
+  };
+  auto form = [&](const PkUnit& u) {
+    InnerForm F = inner_form_mg(u.p, false);
+    F.x = u.x; F.r = u.r; F.z = u.z; F.p0 = u.p0; F.p1 = u.p1; F.ap = u.ap;
+    return F;
+  };
+  // per unit: project u, ||P b||, the true residual (one wait for all)
+  for (int i = 0; i < nu; ++i) {
+    const PkUnit& u = units[i];
+    mycel_problem* p = u.p;
+    bind(u);
+    cudaMemsetAsync(p->d_state, 0, sizeof(PcgState), s);
+    launch_project_x(p, u.u, &p->d_state->nonzero_x);
+    launch_pcg_bnorm(p);
+    MYCEL_CUDA(c, cudaMemcpyAsync(h_bn + i, &p->d_state->bnorm, sizeof(double), cudaMemcpyDeviceToHost, s));
+    if ((st = true_residual_issue(p, form(u), u.b, u.u, h_rn2 + i))) return st;
+  }
+  MYCEL_CUDA(c, cudaStreamSynchronize(s));
+  std::vector<double> bnorm(nu), rel(nu);
+  std::vector<char> active(nu, 0), ok(nu, 0), stalled(nu, 0), msg(nu, 0);
+  std::vector<int> iters(nu, 0), flushes(nu, 0), resume(nu, 0);
+  std::vector<int64_t> cycle_limit(nu, 300);
+  const int64_t stall_floor = 300;
+  int nact = 0;
+  int64_t cap = 0;
+  for (int i = 0; i < nu; ++i) {
+    const PkUnit& u = units[i];
+    PackJob& J = jobs[u.job];
+    mycel_pcg_result& r = J.res[u.k < 0 ? 0 : u.k];
+    bnorm[i] = h_bn[i];
+    h_init[i] = PkInit{0.0, 0, 0};
+    if (bnorm[i] <= 1e-30) {
+      MYCEL_CUDA(c, cudaMemsetAsync(u.u, 0, sizeof(double) * u.p->g.nd, s));
+      r.converged = 1;
+      std::snprintf(r.message, sizeof r.message, "RHS is zero. Solution is zero.");
+      ok[i] = msg[i] = 1;
+      continue;
+    }
+    rel[i] = std::sqrt(h_rn2[i]) / bnorm[i];
+    if (rel[i] <= J.tol) {
+      ok[i] = msg[i] = 1;
+      r.converged = 1;
+      r.final_residual = rel[i];
+      std::snprintf(r.message, sizeof r.message, "Initial guess already converged.");
+      continue;
+    }
+    MYCEL_CUDA(c, cudaMemsetAsync(u.x, 0, sizeof(float) * (size_t)u.p->g.n32, s));
+    h_init[i] = PkInit{0.5 * J.tol * bnorm[i], J.max_iter, 1};
+    active[i] = 1;
+    ++nact;
+    cap = std::max<int64_t>(cap, (int64_t)J.max_iter + 64 * 2 + 4096);
+  }
+  MYCEL_CUDA(c, cudaMemcpyAsync(P.d_init, h_init, sizeof(PkInit) * nu, cudaMemcpyHostToDevice, s));
+  k_pk_init<<<(nu + 127) / 128, 128, 0, s>>>(P.d_sts, P.d_init, nu, 1e-3);
+  c->launches++;
+  if (nact > 0) c->launches += pk_step(P, s, 2, 0);
+  int64_t launched = 0;
+  std::vector<signed char> op(nu, -1);
+  while (nact > 0) {
+    for (int64_t k = 0;; ++k) {  // chunk k is queued while the states after chunk k-1 are read
+      if (cancel && *cancel) {
+        cudaStreamSynchronize(s);
+        return set_error(c, MYCEL_E_CANCELLED, "The operation was canceled.");
+      }
+      if (launched > cap) {
+        cudaStreamSynchronize(s);
+        return set_error(c, MYCEL_E_TIMEOUT, "packed inner PCG device state did not reach a final status");
+      }
+      const int gi = (int)(k & 1);
+      MYCEL_CUDA(c, cudaGraphLaunch(P.chunk, s));
+      launched += 2;
+      c->launches += P.per_chunk;
+      MYCEL_CUDA(c, cudaMemcpyAsync(slot[gi], P.d_states, sizeof(MixState) * nu, cudaMemcpyDeviceToHost, s));
+      MYCEL_CUDA(c, cudaEventRecord(w->ev[gi], s));
+      if (k == 0) continue;
+      const int pi = (int)((k - 1) & 1);
+      MYCEL_CUDA(c, cudaEventSynchronize(w->ev[pi]));
+      bool running = false, any_stall = false;
+      std::fill(op.begin(), op.end(), (signed char)-1);
+      for (int q = 0; q < nu; ++q) {
+        if (!active[q] || slot[pi][q].status != MIX_RUNNING) continue;
+        if (slot[pi][q].iter - resume[q] > cycle_limit[q]) {  // stalled: stop it (the queued chunk skips it)
+          stalled[q] = 1;
+          op[q] = kPkStall;
+          any_stall = true;
+          continue;
+        }
+        running = true;
+      }
+      if (any_stall && (st = pk_set(c, P, op))) return st;
+      if (!running) break;
+    }
+    MYCEL_CUDA(c, cudaStreamSynchronize(s));
+    MixState* h = slot[0];
+    k_pk_gather<<<(nu + 127) / 128, 128, 0, s>>>(P.d_sts, nu, P.d_states);  // the live states
+    c->launches++;
+    MYCEL_CUDA(c, cudaMemcpyAsync(h, P.d_states, sizeof(MixState) * nu, cudaMemcpyDeviceToHost, s));
+    MYCEL_CUDA(c, cudaStreamSynchronize(s));
+    std::vector<int> status(nu, MIX_DONE);
+    for (int i = 0; i < nu; ++i) {
+      if (!active[i]) continue;
+      const PkUnit& u = units[i];
+      status[i] = h[i].status;
+      iters[i] = h[i].iter;
+      const int m = iters[i] - resume[i];
+      if (m > 0 && (m & 1))
+        MYCEL_CUDA(c, cudaMemcpyAsync(u.p1, u.p0, sizeof(float) * (size_t)u.p->g.n32, cudaMemcpyDeviceToDevice, s));
+      k_flush_u<float><<<stream_blocks(u.p), kT, 0, s>>>(u.p->g, u.u, u.x);
+      c->launches++;
+      ++flushes[i];
+      if ((st = true_residual_issue(u.p, form(u), u.b, u.u, h_rn2 + i))) return st;
+    }
+    MYCEL_CUDA(c, cudaStreamSynchronize(s));
+    bool restart = false;
+    std::fill(op.begin(), op.end(), (signed char)-1);
+    for (int i = 0; i < nu; ++i) {
+      if (!active[i]) continue;
+      const PackJob& J = jobs[units[i].job];
+      rel[i] = std::sqrt(h_rn2[i]) / bnorm[i];
+      cycle_limit[i] = std::max<int64_t>(stall_floor, 3 * (int64_t)iters[i]);
+      if (rel[i] <= J.tol) {
+        ok[i] = 1;
+        active[i] = 0;
+        --nact;
+        op[i] = MIX_DONE;
+      } else if (stalled[i] || status[i] != MIX_FLUSH || iters[i] >= J.max_iter) {
+        active[i] = 0;  // finished alone below
+        --nact;
+        op[i] = MIX_DONE;
+      } else {
+        op[i] = MIX_RUNNING;
+        resume[i] = iters[i];
+        restart = true;
+      }
+    }
+    if ((st = pk_set(c, P, op))) return st;
+    if (!restart) break;
+    c->launches += pk_step(P, s, 1, 0);  // the restarting units' preconditioned residual (the others skip)
+  }
+  MYCEL_CUDA(c, cudaStreamSynchronize(s));
+  const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  for (int i = 0; i < nu; ++i) {
+    const PkUnit& u = units[i];
+    PackJob& J = jobs[u.job];
+    mycel_pcg_result& r = J.res[u.k < 0 ? 0 : u.k];
+    if (msg[i]) {  // zero right-hand side or converged at the start
+      r.elapsed_ms = ms;
+      continue;
+    }
+    if (!ok[i]) {  // finished alone from the refined u, as the solve alone goes on after its FP32 iteration
+      if (stalled[i]) u.p->mg->prefers_f64 = true;
+      const int budget = (u.k < 0 && iters[i] == 0) ? J.max_iter : std::max(J.max_iter - iters[i], J.max_iter / 2);
+      if ((st = refined_solve_entry(u.p, u.b, u.bnz, u.nbnz, u.u, J.tol, budget, cancel, MYCEL_PRECISION_FP64_MG, &r)))
+        return st;
+      r.fallback_iterations = r.iterations;
+      r.inner_iterations = iters[i];
+      r.iterations += iters[i];
+      r.refinement_steps += flushes[i];
+      continue;
+    }
+    r.inner_iterations = iters[i];
+    r.iterations = iters[i];
+    r.refinement_steps = flushes[i];
+    r.final_residual = rel[i];
+    r.converged = 1;
+    r.elapsed_ms = ms;
   }
   return MYCEL_OK;
 }

@@ -114,10 +114,13 @@ struct mycel_ctx {
   int64_t prof_n[4] = {0, 0, 0, 0};
   int64_t prof_nodes[4] = {0, 0, 0, 0};     // nodes processed by the timed launches
   int64_t prof_elems[4] = {0, 0, 0, 0};     // active elements processed by the timed launches
+  void* pack = nullptr;    // packed-solve workspace (fp32_kernels.cu), built on first use
+  int64_t packed_rhs = 0;  // right-hand sides whose solves ran through packed launches (a statistic)
 };
 
 struct mycel_problem {
   mycel_ctx* ctx = nullptr;
+  uint64_t serial = 0;  // distinct for every problem the process creates (cached plans compare it)
   mycel::GridDims g{};
   float h = 1.0f;
   double e0 = 1, nu = 0.3, emin_ratio = 1e-6, emin = 1e-6, penal = 3.0;
@@ -313,6 +316,22 @@ int32_t mixed_solve_entry(mycel_problem* p, const double* d_b, const int32_t* d_
 int32_t mg_solve_cases(mycel_problem* p, int ncase, double* d_u, double tol, int max_iter,
                        const volatile int32_t* cancel, mycel_pcg_result* res);
 constexpr int kMaxBatchedCases = 8;
+// One problem's part of a packed solve (mixed multigrid form): its single right-hand side (ncase 1: p->d_b, the
+// solution in d_u) or its load cases 0 .. ncase-1 solved together (p->d_case_b; d_u: ncase x total_dofs,
+// case-major); warm starts in, solutions out, res: ncase results.
+struct PackJob {
+  mycel_problem* p;
+  int ncase;
+  double* d_u;
+  double tol;
+  int max_iter;
+  mycel_pcg_result* res;
+};
+// Solves the jobs (all problems of context c, one job per problem) with their FP32 outer iterations advanced
+// together by packed launches; jobs the packed form cannot take are solved alone. Each result equals the
+// problem's solve alone in the mixed multigrid form.
+int32_t mg_solve_packed(mycel_ctx* c, int njobs, PackJob* jobs, const volatile int32_t* cancel);
+void pack_release(mycel_ctx* c);
 bool cases_together_enabled();
 int32_t kernel_bench(mycel_problem* p, int which, int reps, double* avg_us);  // MYCEL_CASES_TOGETHER=0 turns the batched case solve off
 int32_t refined_solve_entry(mycel_problem* p, const double* d_b, const int32_t* d_nz, int32_t n_nz, double* d_u,

@@ -47,6 +47,7 @@ struct mycel_simp_session {
   mycel_iter_record frame_rec[2] = {};
   bool frame_busy[2] = {false, false};
   int frame_next = 0;
+  void* h_pin = nullptr;           // pinned host slot of the per-iteration scalar read-backs
 };
 
 namespace {
@@ -211,7 +212,9 @@ extern "C" int32_t mycel_simp_begin(mycel_problem* p, const mycel_simp_options* 
     cudaMemsetAsync(s->d_u, 0, sizeof(double) * g.nd, st);
   if (s->d_uc) cudaMemsetAsync(s->d_uc, 0, sizeof(double) * s->ncase * g.nd, st);
   for (auto& e : s->ev) cudaEventCreate(&e);
+  if (cudaMallocHost(&s->h_pin, 256) != cudaSuccess) s->h_pin = nullptr;
   cudaError_t pe = cudaGetLastError();
+  if (pe == cudaSuccess && !s->h_pin) pe = cudaErrorMemoryAllocation;
   if (pe != cudaSuccess) {
     mycel_simp_end(s);
     return set_error(c, MYCEL_E_DEVICE, std::string("SIMP set-up: ") + cudaGetErrorString(pe));
@@ -238,17 +241,22 @@ extern "C" int32_t mycel_simp_begin(mycel_problem* p, const mycel_simp_options* 
   return MYCEL_OK;
 }
 
-static int32_t simp_step_impl(mycel_simp_session* s, mycel_iter_record* rec, int32_t* done,
-                              const volatile int32_t* cancel) {
+// One SIMP iteration in four phases, so that a batch of sessions can run each phase for all of them (their
+// solves packed): simp_pre (continuation, filter, E/DiagA, tolerance), the solve, simp_post_issue
+// (compliance, sensitivities, adjoint filter, OC, read-backs queued) and, after the stream is synchronised,
+// simp_post_finish (host state, record, stop rule).
+struct SimpPre {
+  double penal = 3.0, tol = 1e-8;
+  std::chrono::steady_clock::time_point t0;
+};
+
+static void simp_pre(mycel_simp_session* s, SimpPre* pre) {
   mycel_problem* p = s->p;
   mycel_ctx* c = p->ctx;
-  cudaSetDevice(c->device);
   cudaStream_t st = c->stream;
   const mycel_simp_options& o = s->o;
-  if (done) *done = s->done ? 1 : 0;
-  if (s->done) return MYCEL_OK;
   const int iter = s->iter;
-  auto t0 = std::chrono::steady_clock::now();
+  pre->t0 = std::chrono::steady_clock::now();
   // 1. penalisation continuation (:176-183)
   double penal = o.penal;
   if (o.continuation) penal = iter < 20 ? 1.0 : (iter < 40 ? 2.0 : o.penal);
@@ -273,37 +281,72 @@ static int32_t simp_step_impl(mycel_simp_session* s, mycel_iter_record* rec, int
     double lt = lf + ta * (li - lf);
     tol = std::pow(10.0, lt);
   }
-  // 4. warm-started PCG (:226-253); with the load cases apart one solve per case from its own warm start, all
-  // on this iteration's stiffness (the solver set-up is shared)
-  mycel_pcg_result pr;
+  pre->penal = penal;
+  pre->tol = tol;
+}
+
+// the load cases' results folded into one (iterations and times summed, the largest residual, the first failure)
+static void fold_cases(const mycel_pcg_result* rs, int n, mycel_pcg_result* pr) {
+  std::memset(pr, 0, sizeof *pr);
+  pr->converged = 1;
+  for (int k = 0; k < n && pr->converged; ++k) {
+    const mycel_pcg_result& rk = rs[k];
+    pr->iterations += rk.iterations;
+    pr->inner_iterations += rk.inner_iterations;
+    pr->fallback_iterations += rk.fallback_iterations;
+    pr->refinement_steps += rk.refinement_steps;
+    pr->elapsed_ms += rk.elapsed_ms;
+    pr->final_residual = std::max(pr->final_residual, rk.final_residual);
+    pr->converged = rk.converged;
+    std::memcpy(pr->message, rk.message, sizeof pr->message);
+  }
+}
+
+// the load cases of a session are solved together (packed or alone) in the mixed multigrid form
+static bool cases_solved_together(const mycel_simp_session* s) {
+  return s->o.precision == MYCEL_PRECISION_MIXED_MG && s->ncase <= kMaxBatchedCases && cases_together_enabled();
+}
+
+// 4. warm-started PCG (:226-253); with the load cases apart one solve per case from its own warm start, all
+// on this iteration's stiffness (the solver set-up is shared)
+static int32_t simp_solve(mycel_simp_session* s, const SimpPre& pre, const volatile int32_t* cancel,
+                          mycel_pcg_result* pr) {
+  mycel_problem* p = s->p;
+  const mycel_simp_options& o = s->o;
   int32_t rc;
   const int64_t nd = p->g.nd;
-  if (s->ncase == 1) {
-    rc = solve_dispatch(p, s->d_u, tol, o.solver_max_iterations, o.precision, cancel, &pr);
-    if (rc) return rc;
-  } else {
-    std::memset(&pr, 0, sizeof pr);
-    pr.converged = 1;
-    // the mixed multigrid form solves the cases together (one V-cycle's coarse levels for all of them)
-    const bool together =
-        o.precision == MYCEL_PRECISION_MIXED_MG && s->ncase <= kMaxBatchedCases && cases_together_enabled();
+  if (s->ncase == 1) return solve_dispatch(p, s->d_u, pre.tol, o.solver_max_iterations, o.precision, cancel, pr);
+  if (cases_solved_together(s)) {  // one V-cycle's coarse levels for all cases
     mycel_pcg_result rs[kMaxBatchedCases];
-    if (together && (rc = mg_solve_cases(p, s->ncase, s->d_uc, tol, o.solver_max_iterations, cancel, rs))) return rc;
-    for (int k = 0; k < s->ncase && pr.converged; ++k) {
-      mycel_pcg_result rk;
-      if (together) rk = rs[k];
-      else if ((rc = solve_case(p, k, s->d_uc + k * nd, tol, o.solver_max_iterations, o.precision, cancel, &rk)))
-        return rc;
-      pr.iterations += rk.iterations;
-      pr.inner_iterations += rk.inner_iterations;
-      pr.fallback_iterations += rk.fallback_iterations;
-      pr.refinement_steps += rk.refinement_steps;
-      pr.elapsed_ms += rk.elapsed_ms;
-      pr.final_residual = std::max(pr.final_residual, rk.final_residual);
-      pr.converged = rk.converged;
-      std::memcpy(pr.message, rk.message, sizeof pr.message);
-    }
+    if ((rc = mg_solve_cases(p, s->ncase, s->d_uc, pre.tol, o.solver_max_iterations, cancel, rs))) return rc;
+    fold_cases(rs, s->ncase, pr);
+    return MYCEL_OK;
   }
+  std::memset(pr, 0, sizeof *pr);
+  pr->converged = 1;
+  for (int k = 0; k < s->ncase && pr->converged; ++k) {
+    mycel_pcg_result rk;
+    if ((rc = solve_case(p, k, s->d_uc + k * nd, pre.tol, o.solver_max_iterations, o.precision, cancel, &rk)))
+      return rc;
+    pr->iterations += rk.iterations;
+    pr->inner_iterations += rk.inner_iterations;
+    pr->fallback_iterations += rk.fallback_iterations;
+    pr->refinement_steps += rk.refinement_steps;
+    pr->elapsed_ms += rk.elapsed_ms;
+    pr->final_residual = std::max(pr->final_residual, rk.final_residual);
+    pr->converged = rk.converged;
+    std::memcpy(pr->message, rk.message, sizeof pr->message);
+  }
+  return MYCEL_OK;
+}
+
+static int32_t simp_post_issue(mycel_simp_session* s, const SimpPre& pre, const mycel_pcg_result& pr) {
+  mycel_problem* p = s->p;
+  mycel_ctx* c = p->ctx;
+  cudaStream_t st = c->stream;
+  const mycel_simp_options& o = s->o;
+  const double penal = pre.penal;
+  const int64_t nd = p->g.nd;
   cudaEventRecord(s->ev[2], st);
   if (!pr.converged)
     return set_error(c, MYCEL_E_NOT_CONVERGED,
@@ -344,15 +387,26 @@ static int32_t simp_step_impl(mycel_simp_session* s, mycel_iter_record* rec, int
   OcParams prm{o.volume_fraction, o.move_limit, o.rho_min, s->lambda, 1e-8, 60, o.enable_heaviside};
   prm.exact = o.precision == MYCEL_PRECISION_FP64 ? 1 : 0;
   prm.total_s = s->total_s;
-  rc = launch_oc(c, p->n_active, p->d_active, s->d_rho, s->d_dc, s->filt->d_s, s->d_pas, s->d_rho_new, s->d_rb,
-                 o.enable_heaviside ? s->d_rt : s->d_rb, prm, s->d_oc_scr, oc_scratch_doubles(c->oc_grid), s->d_oc);
+  int32_t rc = launch_oc(c, p->n_active, p->d_active, s->d_rho, s->d_dc, s->filt->d_s, s->d_pas, s->d_rho_new,
+                         s->d_rb, o.enable_heaviside ? s->d_rt : s->d_rb, prm, s->d_oc_scr,
+                         oc_scratch_doubles(c->oc_grid), s->d_oc);
   if (rc) return set_error(c, rc, "OC kernel launch failed");
   cudaEventRecord(s->ev[4], st);
-  double* hsc = (double*)c->pinned;
-  OcOut* ho = (OcOut*)((char*)c->pinned + 64);
+  double* hsc = (double*)s->h_pin;
+  OcOut* ho = (OcOut*)((char*)s->h_pin + 64);
   MYCEL_CUDA(c, cudaMemcpyAsync(hsc, s->d_scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
   MYCEL_CUDA(c, cudaMemcpyAsync(ho, s->d_oc, sizeof(OcOut), cudaMemcpyDeviceToHost, st));
-  MYCEL_CUDA(c, cudaStreamSynchronize(st));
+  return MYCEL_OK;
+}
+
+static int32_t simp_post_finish(mycel_simp_session* s, const SimpPre& pre, const mycel_pcg_result& pr,
+                                mycel_iter_record* rec, int32_t* done) {
+  mycel_problem* p = s->p;
+  mycel_ctx* c = p->ctx;
+  const mycel_simp_options& o = s->o;
+  const int iter = s->iter;
+  const double* hsc = (const double*)s->h_pin;
+  const OcOut* ho = (const OcOut*)((const char*)s->h_pin + 64);
   if (ho->trials == 0) return set_error(c, MYCEL_E_TIMEOUT, "OC grid barrier timed out");
   std::swap(s->d_rho, s->d_rho_new);
   s->lambda = ho->lambda;
@@ -378,7 +432,7 @@ static int32_t simp_step_impl(mycel_simp_session* s, mycel_iter_record* rec, int
   r.sensitivity_ms = ms;
   cudaEventElapsedTime(&ms, s->ev[3], s->ev[4]);
   r.update_ms = ms;
-  r.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  r.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - pre.t0).count();
   if (rec) *rec = r;
   s->last = r;
   s->count++;
@@ -398,9 +452,91 @@ static int32_t simp_step_impl(mycel_simp_session* s, mycel_iter_record* rec, int
   return MYCEL_OK;
 }
 
+static int32_t simp_step_impl(mycel_simp_session* s, mycel_iter_record* rec, int32_t* done,
+                              const volatile int32_t* cancel) {
+  mycel_problem* p = s->p;
+  mycel_ctx* c = p->ctx;
+  cudaSetDevice(c->device);
+  if (done) *done = s->done ? 1 : 0;
+  if (s->done) return MYCEL_OK;
+  SimpPre pre;
+  simp_pre(s, &pre);
+  mycel_pcg_result pr;
+  int32_t rc = simp_solve(s, pre, cancel, &pr);
+  if (rc) return rc;
+  if ((rc = simp_post_issue(s, pre, pr))) return rc;
+  MYCEL_CUDA(c, cudaStreamSynchronize(c->stream));
+  return simp_post_finish(s, pre, pr, rec, done);
+}
+
 extern "C" int32_t mycel_simp_step(mycel_simp_session* s, mycel_iter_record* rec, int32_t* done) {
   if (!s) return set_error(nullptr, MYCEL_E_ARG, "NULL session");
   return simp_step_impl(s, rec, done, nullptr);
+}
+
+// One SIMP iteration of each of n sessions (one context, one session per problem). The sessions in the mixed
+// multigrid form have their solves packed (mg_solve_packed: every kernel of an FP32 outer iteration one launch
+// for all of them); the others are solved one after another. Each session's iteration is the one
+// mycel_simp_step would take. status[i] (optional) gets each session's own status; the call returns the
+// first failure (MYCEL_OK when none). A session that is done is left as it is.
+extern "C" int32_t mycel_simp_step_many(mycel_simp_session* const* ss, int32_t n, mycel_iter_record* recs,
+                                        int32_t* done, int32_t* status, const volatile int32_t* cancel) {
+  if (!ss || n < 1) return set_error(nullptr, MYCEL_E_ARG, "NULL sessions or count below 1");
+  for (int i = 0; i < n; ++i)
+    if (!ss[i]) return set_error(nullptr, MYCEL_E_ARG, "NULL session");
+  mycel_ctx* c = ss[0]->p->ctx;
+  for (int i = 0; i < n; ++i) {
+    if (ss[i]->p->ctx != c) return set_error(c, MYCEL_E_ARG, "the sessions of a batch step share one context");
+    for (int j = 0; j < i; ++j)
+      if (ss[j]->p == ss[i]->p) return set_error(c, MYCEL_E_ARG, "each session of a batch step has its own problem");
+  }
+  cudaSetDevice(c->device);
+  std::vector<SimpPre> pre(n);
+  std::vector<mycel_pcg_result> pr(n);
+  std::vector<int32_t> st(n, MYCEL_OK);
+  std::vector<char> live(n, 0);
+  std::vector<std::vector<mycel_pcg_result>> cres(n);
+  std::vector<PackJob> jobs;
+  std::vector<int> job_of;
+  for (int i = 0; i < n; ++i) {
+    mycel_simp_session* s = ss[i];
+    if (done) done[i] = s->done ? 1 : 0;
+    if (s->done) continue;
+    live[i] = 1;
+    simp_pre(s, &pre[i]);
+    const bool packable = s->o.precision == MYCEL_PRECISION_MIXED_MG && (s->ncase == 1 || cases_solved_together(s));
+    if (!packable) continue;
+    cres[i].resize(s->ncase);
+    jobs.push_back(PackJob{s->p, s->ncase, s->ncase == 1 ? s->d_u : s->d_uc, pre[i].tol, s->o.solver_max_iterations,
+                           cres[i].data()});
+    job_of.push_back(i);
+  }
+  if (!jobs.empty()) {
+    int32_t rc = mg_solve_packed(c, (int)jobs.size(), jobs.data(), cancel);
+    for (size_t q = 0; q < jobs.size(); ++q) {
+      const int i = job_of[q];
+      if (rc) st[i] = rc;
+      else fold_cases(cres[i].data(), ss[i]->ncase, &pr[i]);
+    }
+  }
+  for (int i = 0; i < n; ++i) {
+    mycel_simp_session* s = ss[i];
+    if (!live[i] || !cres[i].empty() || st[i]) continue;
+    st[i] = simp_solve(s, pre[i], cancel, &pr[i]);
+  }
+  for (int i = 0; i < n; ++i)
+    if (live[i] && !st[i]) st[i] = simp_post_issue(ss[i], pre[i], pr[i]);
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  int32_t first = MYCEL_OK;
+  for (int i = 0; i < n; ++i) {
+    if (live[i] && !st[i]) {
+      if (e != cudaSuccess) st[i] = set_error(c, MYCEL_E_DEVICE, std::string("SIMP step: ") + cudaGetErrorString(e));
+      else st[i] = simp_post_finish(ss[i], pre[i], pr[i], recs ? recs + i : nullptr, done ? done + i : nullptr);
+    }
+    if (status) status[i] = st[i];
+    if (!first && st[i]) first = st[i];
+  }
+  return first;
 }
 
 static int32_t snapshot(mycel_simp_session* s) {
@@ -533,6 +669,7 @@ extern "C" int32_t mycel_simp_end(mycel_simp_session* s) {
   if (s->d_des_f) cudaFreeAsync(s->d_des_f, st);
   for (auto& e : s->ev)
     if (e) cudaEventDestroy(e);
+  if (s->h_pin) cudaFreeHost(s->h_pin);
   for (int k = 0; k < 2; ++k) {
     if (s->d_frame[k]) cudaFreeAsync(s->d_frame[k], st);
     if (s->h_frame[k]) cudaFreeHost(s->h_frame[k]);
@@ -594,6 +731,8 @@ extern "C" int32_t mycel_simp_run(mycel_problem* p, const mycel_simp_options* op
 namespace mycel {
 bool simp_session_converged(const mycel_simp_session* s) { return s && s->converged; }
 }  // namespace mycel
+
+extern "C" int32_t mycel_simp_converged(const mycel_simp_session* s) { return s && s->converged ? 1 : 0; }
 
 extern "C" int32_t mycel_simp_surface_nets(mycel_simp_session* s, const float* origin, float threshold,
                                            mycel_mesh** out) {
