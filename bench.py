@@ -106,6 +106,9 @@ def parse():
     ap.add_argument("--batched-count", type=int, default=48)
     ap.add_argument("--batched-skip-fp64", action="store_true", help="time only the timed form of --batched")
     ap.add_argument("--batched-iters", type=int, default=4)
+    ap.add_argument("--batched-mode", choices=("packed", "served", "both"), default="both",
+                    help="batched timed form: packed launches of all problems (one context), the serving loop's "
+                         "slots, or both (FP64 always through the serving loop)")
     ap.add_argument("--batched-cases", choices=("separate", "summed"), default="separate",
                     help="load cases of a batched problem: one solve per case on the shared stiffness (objective "
                          "the sum of the cases' compliances), or summed into one right-hand side as the reference")
@@ -450,7 +453,39 @@ def run_batched(args):
     hists = {}
     head = args.precision
     out["cases_together"] = os.environ.get("MYCEL_CASES_TOGETHER", "1") != "0"
+    if args.batched_mode in ("packed", "both"):
+        # one context, every problem's session stepped together (mycel_simp_step_many): the mixed multigrid
+        # solves of all problems share their launches; wall time from the first problem's creation to the end
+        ctx = api.Context(0)
+        t0 = time.perf_counter()
+        made = []
+        for bp in probs:
+            p = api.Problem(bp.model, ctx)
+            made.append((p, api.SimpSession(p, bp.options.replace(
+                max_iterations=args.batched_iters, precision=head, solver_tolerance_initial=args.job_tol,
+                solver_tolerance_final=args.job_tol, separate_load_cases=sep))))
+        sess = [s for _, s in made]
+        ph = [[] for _ in sess]
+        n_it = 0
+        packed0 = ctx.packed_count
+        while not all(s.done for s in sess):
+            live = [k for k, s in enumerate(sess) if not s.done]
+            for k, r in zip(live, api.SimpSession.step_many([sess[k] for k in live])):
+                if r is not None:
+                    ph[k].append(r.compliance)
+                    n_it += 1
+        wall = time.perf_counter() - t0
+        out["packed"] = {"simp_iter_s": n_it / wall, "wall_s": wall, "simp_iterations": n_it,
+                         "rhs_solved_packed": ctx.packed_count - packed0,
+                         "form": head, "note": "all problems' solves in shared launches (mycel_simp_step_many)"}
+        for p, s in made:
+            s.close()
+            p.close()
+        ctx.close()
+        hists["packed"] = ph
     for prec in ((head,) if args.batched_skip_fp64 else (head, "fp64")):
+        if prec == head and args.batched_mode == "packed":
+            continue
         with api.Server(slots=args.serve_slots, hbm_budget_bytes=int(args.serve_budget_gb * 1e9)) as srv:
             ids = [srv.submit(bp.model, bp.options.replace(max_iterations=args.batched_iters, precision=prec,
                                                           solver_tolerance_initial=args.job_tol,
@@ -463,9 +498,14 @@ def run_batched(args):
         span = st["last_finish_s"] - st["first_submit_s"]
         out[prec] = {"simp_iter_s": st["simp_iterations"] / span, "wall_s": span, "completed": st["completed"],
                      "p50_latency_s": st["p50_latency_s"], "p99_latency_s": st["p99_latency_s"]}
+    if "packed" in out and head in hists:
+        out["packed"]["same_histories_as_served"] = hists["packed"] == hists[head]
+        out["packed"]["speedup_vs_served"] = out["packed"]["simp_iter_s"] / out[head]["simp_iter_s"]
     if "fp64" in out:
-        out[f"speedup_{head}_vs_fp64"] = out[head]["simp_iter_s"] / out["fp64"]["simp_iter_s"]
-        out[f"rel_compliance_err_{head}_vs_fp64"] = compare_histories(hists[head], hists["fp64"])
+        fast = out["packed"] if "packed" in out else out[head]
+        out[f"speedup_{head}_vs_fp64"] = fast["simp_iter_s"] / out["fp64"]["simp_iter_s"]
+        out[f"rel_compliance_err_{head}_vs_fp64"] = compare_histories(hists["packed" if "packed" in out else head],
+                                                                      hists["fp64"])
     print(json.dumps(out), flush=True)
 
 
