@@ -465,17 +465,24 @@ def run_batched(args):
                 max_iterations=args.batched_iters, precision=head, solver_tolerance_initial=args.job_tol,
                 solver_tolerance_final=args.job_tol, separate_load_cases=sep))))
         sess = [s for _, s in made]
+        t_setup = time.perf_counter() - t0
         ph = [[] for _ in sess]
         n_it = 0
         packed0 = ctx.packed_count
+        step_s = []
         while not all(s.done for s in sess):
             live = [k for k, s in enumerate(sess) if not s.done]
+            ts = time.perf_counter()
             for k, r in zip(live, api.SimpSession.step_many([sess[k] for k in live])):
                 if r is not None:
                     ph[k].append(r.compliance)
                     n_it += 1
+            step_s.append(time.perf_counter() - ts)
         wall = time.perf_counter() - t0
+        later = step_s[1:]
         out["packed"] = {"simp_iter_s": n_it / wall, "wall_s": wall, "simp_iterations": n_it,
+                         "setup_s": t_setup, "step_s": step_s,
+                         "steady_simp_iter_s": len(probs) * len(later) / sum(later) if later else None,
                          "rhs_solved_packed": ctx.packed_count - packed0,
                          "form": head, "note": "all problems' solves in shared launches (mycel_simp_step_many)"}
         for p, s in made:

@@ -4881,6 +4881,16 @@ int32_t mg_solve_packed(mycel_ctx* c, int njobs, PackJob* jobs, const volatile i
   });
   if (smem_err != cudaSuccess)
     return set_error(c, MYCEL_E_DEVICE, std::string("packed matvec shared memory: ") + cudaGetErrorString(smem_err));
+  const bool verbose = std::getenv("MYCEL_VERBOSE") != nullptr;
+  auto tp = std::chrono::steady_clock::now();
+  auto lap = [&](const char* what, int extra) {
+    if (!verbose) return;
+    cudaStreamSynchronize(s);
+    const auto now = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "mycel: packed %s %.3f ms (%d)\n", what,
+                 std::chrono::duration<double, std::milli>(now - tp).count(), extra);
+    tp = now;
+  };
   std::vector<PkUnit> units;
   std::vector<char> packed(njobs, 0);
   // eligibility; the others are solved alone here, in job order
@@ -4952,6 +4962,7 @@ int32_t mg_solve_packed(mycel_ctx* c, int njobs, PackJob* jobs, const volatile i
     }
   }
   const int nu = (int)units.size();
+  lap("set-up and unpacked jobs", nu);
   if (nu == 0) return MYCEL_OK;
   if (!c->pack) c->pack = new PackWork();
   PackWork* w = (PackWork*)c->pack;
@@ -4981,6 +4992,7 @@ int32_t mg_solve_packed(mycel_ctx* c, int njobs, PackJob* jobs, const volatile i
     for (int i = 0; i < nu; ++i) units[i].part = (double*)w->part_bufs[i];
   }
   PackPlan& P = w->plan;
+  lap("plan", P.per_chunk);
   c->packed_rhs += nu;
   struct Saved {
     mycel_problem* p;
@@ -5057,7 +5069,9 @@ int32_t mg_solve_packed(mycel_ctx* c, int njobs, PackJob* jobs, const volatile i
   k_pk_init<<<(nu + 127) / 128, 128, 0, s>>>(P.d_sts, P.d_init, nu, 1e-3);
   c->launches++;
   if (nact > 0) c->launches += pk_step(P, s, 2, 0);
+  lap("initial residuals and start", nact);
   int64_t launched = 0;
+  int rounds = 0;
   std::vector<signed char> op(nu, -1);
   while (nact > 0) {
     for (int64_t k = 0;; ++k) {  // chunk k is queued while the states after chunk k-1 are read
@@ -5137,6 +5151,8 @@ int32_t mg_solve_packed(mycel_ctx* c, int njobs, PackJob* jobs, const volatile i
       }
     }
     if ((st = pk_set(c, P, op))) return st;
+    lap("round", (int)launched);
+    ++rounds;
     if (!restart) break;
     c->launches += pk_step(P, s, 1, 0);  // the restarting units' preconditioned residual (the others skip)
   }
@@ -5168,6 +5184,7 @@ int32_t mg_solve_packed(mycel_ctx* c, int njobs, PackJob* jobs, const volatile i
     r.converged = 1;
     r.elapsed_ms = ms;
   }
+  lap("finished alone", rounds);
   return MYCEL_OK;
 }
 

@@ -7,6 +7,8 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <string>
@@ -491,6 +493,16 @@ extern "C" int32_t mycel_simp_step_many(mycel_simp_session* const* ss, int32_t n
       if (ss[j]->p == ss[i]->p) return set_error(c, MYCEL_E_ARG, "each session of a batch step has its own problem");
   }
   cudaSetDevice(c->device);
+  // MYCEL_VERBOSE: host time of each phase, each ended by a synchronisation (for breakdowns only)
+  const bool verbose = std::getenv("MYCEL_VERBOSE") != nullptr;
+  auto tp = std::chrono::steady_clock::now();
+  auto lap = [&](const char* what) {
+    if (!verbose) return;
+    cudaStreamSynchronize(c->stream);
+    const auto now = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "mycel: step_many %s %.3f ms\n", what, std::chrono::duration<double, std::milli>(now - tp).count());
+    tp = now;
+  };
   std::vector<SimpPre> pre(n);
   std::vector<mycel_pcg_result> pr(n);
   std::vector<int32_t> st(n, MYCEL_OK);
@@ -511,6 +523,7 @@ extern "C" int32_t mycel_simp_step_many(mycel_simp_session* const* ss, int32_t n
                            cres[i].data()});
     job_of.push_back(i);
   }
+  lap("filter, E, diagonal");
   if (!jobs.empty()) {
     int32_t rc = mg_solve_packed(c, (int)jobs.size(), jobs.data(), cancel);
     for (size_t q = 0; q < jobs.size(); ++q) {
@@ -524,8 +537,10 @@ extern "C" int32_t mycel_simp_step_many(mycel_simp_session* const* ss, int32_t n
     if (!live[i] || !cres[i].empty() || st[i]) continue;
     st[i] = simp_solve(s, pre[i], cancel, &pr[i]);
   }
+  lap("solves");
   for (int i = 0; i < n; ++i)
     if (live[i] && !st[i]) st[i] = simp_post_issue(ss[i], pre[i], pr[i]);
+  lap("sensitivities, adjoint, OC");
   cudaError_t e = cudaStreamSynchronize(c->stream);
   int32_t first = MYCEL_OK;
   for (int i = 0; i < n; ++i) {
