@@ -522,10 +522,11 @@ __device__ __forceinline__ void tma_load_plane(void* dst, const CUtensorMap* map
 }
 
 // The kernel body, for CTA (bx, by, bz) of a grid of nblk CTAs (linear number bid, x fastest): a launch of
-// one matvec (k_mv32f) or one problem's share of a packed launch (k_mv32f_pk). tm_a / tm_b point at the
-// tensor maps (kernel parameters, or a packed launch's table in global memory).
+// one matvec (k_mv32f) or one tile of a packed launch (k_mv32f_pk). tm_a / tm_b point at the tensor maps
+// (kernel parameters, or a packed launch's table in global memory). Returns 0 when the state is not running
+// (nothing done, the mbarriers untouched), 1 after the tile, -1 when a bounded wait gave up (*err set).
 template <int MODE>
-__device__ __forceinline__ void mv32f_body(const GridDims& g, const HexOpF& op, const CUtensorMap* tm_a,
+__device__ __forceinline__ int mv32f_body(const GridDims& g, const HexOpF& op, const CUtensorMap* tm_a,
                                            const CUtensorMap* tm_b, float* __restrict__ pnew,
                                            float* __restrict__ y, const float* __restrict__ E,
                                            const uint8_t* __restrict__ nf, int projected, MixState* st,
@@ -536,7 +537,7 @@ __device__ __forceinline__ void mv32f_body(const GridDims& g, const HexOpF& op, 
   float* yb = reinterpret_cast<float*>(fac_smem + (size_t)FNST * kFacStagePitch * (MODE == 1 ? 2 : 1));
   __shared__ __align__(8) unsigned long long full[FNST];
   __shared__ double sh[32];
-  if (st && st->status != MIX_RUNNING) return;  // MODE 0 gets a state only inside the multigrid cycle
+  if (st && st->status != MIX_RUNNING) return 0;  // MODE 0 gets a state only inside the multigrid cycle
   const float beta = MODE == 1 ? (float)st->beta : 0.0f;
   const bool two = MODE == 1 && st->first == 0;  // p_t = z + beta p_{t-1} (else p_t = z)
   const int l = threadIdx.x, w = threadIdx.y, tid = w * FX + l;
@@ -692,8 +693,14 @@ __device__ __forceinline__ void mv32f_body(const GridDims& g, const HexOpF& op, 
 #pragma unroll
       for (int c = 0; c < 3; ++c) ub[b][c] = ut[b][c];
   }
+  // every copy has landed when all waits succeeded: the mbarriers are retired, so a persistent CTA can set
+  // them up again for its next tile (after a failed wait a copy may still be in flight: they stay as they are)
+  const bool all_ok = __syncthreads_and(ok) != 0;
+  if (all_ok && tid == 0)
+    for (int q = 0; q < FNST; ++q) asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(smem_u32(&full[q])) : "memory");
   if (!ok && err) atomicExch(err, 1);
   if (MODE == 1) mv32_finish(pap, sh, st, part, tid, err, nblk, bid);
+  return all_ok ? 1 : -1;
 }
 
 template <int MODE>
@@ -4188,15 +4195,48 @@ int32_t mg_solve_cases(mycel_problem* p, int ncase, double* d_u, double tol, int
 constexpr int kPkMaxUnits = 1024;
 constexpr int kPkStall = 100;  // state op: a running right-hand side's cycle stalled (replacement point)
 
-// entry of CTA b of a packed launch: the last e with starts[e] <= b (starts ascending from 0; uniform per CTA)
-__device__ __forceinline__ int pk_entry(const unsigned* __restrict__ starts, int n, unsigned b) {
-  int lo = 0, hi = n - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (__ldg(starts + mid) <= b) lo = mid;
-    else hi = mid - 1;
+// Work lists: a packed launch's CTAs of one entry alone become work items (entry << kPkLbBits | CTA number);
+// at the start of each outer iteration k_pk_compact lists the items of the entries whose right-hand sides are
+// still running, and the launch's persistent CTAs take the listed items in turn, so the entries that are done
+// cost nothing.
+constexpr int kPkLbBits = 22;
+constexpr unsigned kPkLbMask = (1u << kPkLbBits) - 1;
+static_assert(kPkMaxUnits <= (1 << (32 - kPkLbBits)), "entry index field of a work item");
+
+struct PkList {             // the work list of one packed launch
+  int n;                    // entries
+  const unsigned* starts;   // [n + 1] first CTA of each entry (its launch alone's CTAs), then the total
+  MixState* const* est;     // [n] the entry's first state (its cases' states follow)
+  const int* enc;           // [n] states of the entry
+  unsigned* items;          // [total] listed work items
+  unsigned* count;          // items listed
+};
+
+// one CTA per list: the running entries' items, in entry order
+__global__ void __launch_bounds__(1024) k_pk_compact(const PkList* __restrict__ lists) {
+  const PkList& L = lists[blockIdx.x];
+  __shared__ unsigned off[kPkMaxUnits + 1];
+  __shared__ unsigned char run[kPkMaxUnits];
+  for (int e = threadIdx.x; e < L.n; e += blockDim.x) {
+    bool r = false;
+    for (int k = 0; k < L.enc[e]; ++k) r = r || L.est[e][k].status == MIX_RUNNING;
+    run[e] = r ? 1 : 0;
   }
-  return lo;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned acc = 0;
+    for (int e = 0; e < L.n; ++e) {
+      off[e] = acc;
+      if (run[e]) acc += L.starts[e + 1] - L.starts[e];
+    }
+    *L.count = acc;
+  }
+  __syncthreads();
+  for (int e = 0; e < L.n; ++e) {
+    if (!run[e]) continue;
+    const unsigned nb = L.starts[e + 1] - L.starts[e], o = off[e];
+    for (unsigned j = threadIdx.x; j < nb; j += blockDim.x) L.items[o + j] = ((unsigned)e << kPkLbBits) | j;
+  }
 }
 
 struct alignas(64) PkMv {  // one FP32 matvec (k_mv32f) of a right-hand side
@@ -4215,19 +4255,24 @@ struct alignas(64) PkMv {  // one FP32 matvec (k_mv32f) of a right-hand side
 };
 
 template <int MODE>
-__global__ void __launch_bounds__(FX * FY, 2) k_mv32f_pk(const PkMv* __restrict__ tab,
-                                                         const unsigned* __restrict__ starts, int n) {
-  const int e = pk_entry(starts, n, blockIdx.x);
-  const PkMv* m = tab + e;
-  const unsigned lb = blockIdx.x - __ldg(starts + e);
-  const unsigned gx = m->gx, gy = m->gy;
-  if (threadIdx.x == 0 && threadIdx.y == 0) {  // the thread that issues the copies; maps written before launch
-    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(&m->ta) : "memory");
-    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(&m->tb) : "memory");
+__global__ void __launch_bounds__(FX * FY, 2) k_mv32f_pk(const PkMv* __restrict__ tab, const unsigned* __restrict__ items,
+                                                         const unsigned* __restrict__ count) {
+  const unsigned cnt = *count;
+  for (unsigned w = blockIdx.x; w < cnt; w += gridDim.x) {
+    __syncthreads();  // the previous tile is done with the shared memory
+    const unsigned code = items[w];
+    const PkMv* m = tab + (code >> kPkLbBits);
+    const unsigned lb = code & kPkLbMask;
+    const unsigned gx = m->gx, gy = m->gy;
+    if (threadIdx.x == 0 && threadIdx.y == 0) {  // the thread that issues the copies; maps written before launch
+      asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(&m->ta) : "memory");
+      asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(&m->tb) : "memory");
+    }
+    const int r = mv32f_body<MODE>(m->g, m->op, &m->ta, &m->tb, m->pnew, m->y, m->E, m->nf, m->projected, m->st,
+                                   m->part, m->zseg, m->err, (int)(lb % gx), (int)((lb / gx) % gy),
+                                   (int)(lb / (gx * gy)), gx * gy * m->gz, lb);
+    if (r < 0) break;  // a copy may still be in flight into this CTA's shared memory (uniform: the CTA's result)
   }
-  const GridDims g = m->g;
-  mv32f_body<MODE>(g, m->op, &m->ta, &m->tb, m->pnew, m->y, m->E, m->nf, m->projected, m->st, m->part, m->zseg,
-                   m->err, (int)(lb % gx), (int)((lb / gx) % gy), (int)(lb / (gx * gy)), gx * gy * m->gz, lb);
 }
 
 struct PkVec {  // k_mg_enter32 / k_mg_exit32 of a right-hand side
@@ -4240,19 +4285,26 @@ struct PkVec {  // k_mg_enter32 / k_mg_exit32 of a right-hand side
   unsigned nb;
 };
 
-__global__ void __launch_bounds__(kT) k_mg_enter32_pk(const PkVec* __restrict__ tab, const unsigned* __restrict__ starts,
-                                                      int n, int mode) {
-  const int e = pk_entry(starts, n, blockIdx.x);
-  const PkVec& a = tab[e];
-  mg_enter32_body(a.n, a.x, a.r, a.p, a.q, a.invd, a.z, a.om, a.st, a.part, mode, blockIdx.x - __ldg(starts + e),
-                  a.nb);
+__global__ void __launch_bounds__(kT) k_mg_enter32_pk(const PkVec* __restrict__ tab, const unsigned* __restrict__ items,
+                                                      const unsigned* __restrict__ count, int mode) {
+  const unsigned cnt = *count;
+  for (unsigned w = blockIdx.x; w < cnt; w += gridDim.x) {
+    __syncthreads();
+    const unsigned code = items[w];
+    const PkVec& a = tab[code >> kPkLbBits];
+    mg_enter32_body(a.n, a.x, a.r, a.p, a.q, a.invd, a.z, a.om, a.st, a.part, mode, code & kPkLbMask, a.nb);
+  }
 }
 
-__global__ void __launch_bounds__(kT) k_mg_exit32_pk(const PkVec* __restrict__ tab, const unsigned* __restrict__ starts,
-                                                     int n, int mode) {
-  const int e = pk_entry(starts, n, blockIdx.x);
-  const PkVec& a = tab[e];
-  mg_exit32_body(a.n, a.r, a.t, a.z, a.invd, a.q, a.om, a.st, a.part, mode, blockIdx.x - __ldg(starts + e), a.nb);
+__global__ void __launch_bounds__(kT) k_mg_exit32_pk(const PkVec* __restrict__ tab, const unsigned* __restrict__ items,
+                                                     const unsigned* __restrict__ count, int mode) {
+  const unsigned cnt = *count;
+  for (unsigned w = blockIdx.x; w < cnt; w += gridDim.x) {
+    __syncthreads();
+    const unsigned code = items[w];
+    const PkVec& a = tab[code >> kPkLbBits];
+    mg_exit32_body(a.n, a.r, a.t, a.z, a.invd, a.q, a.om, a.st, a.part, mode, code & kPkLbMask, a.nb);
+  }
 }
 
 struct PkApply {  // a coarse-level product of a problem (all its cases)
@@ -4267,29 +4319,37 @@ struct PkApply {  // a coarse-level product of a problem (all its cases)
 
 template <bool MULTI>
 __global__ void __launch_bounds__(256) k_mg_apply_nodes_pk(const PkApply* __restrict__ tab,
-                                                           const unsigned* __restrict__ starts, int n, int mode) {
-  const int e = pk_entry(starts, n, blockIdx.x);
-  const PkApply& a = tab[e];
-  const int64_t nn = mg_nn(a.d);
-  int64_t q;
-  int c;
-  mg_item_case<MULTI>((int64_t)(blockIdx.x - __ldg(starts + e)) * blockDim.x + threadIdx.x, a.ncase, &q, &c);
-  if (q >= nn || !mg_running(a.st ? a.st + c : nullptr)) return;
-  mg_apply_node(a.d, nn, q, a.S, a.x.p[c], a.r.p[c], a.invd, a.y.p[c], mode, mode == 1 ? *a.om : 0.0f);
+                                                           const unsigned* __restrict__ items,
+                                                           const unsigned* __restrict__ count, int mode) {
+  const unsigned cnt = *count;
+  for (unsigned w = blockIdx.x; w < cnt; w += gridDim.x) {
+    const unsigned code = items[w];
+    const PkApply& a = tab[code >> kPkLbBits];
+    const int64_t nn = mg_nn(a.d);
+    int64_t q;
+    int c;
+    mg_item_case<MULTI>((int64_t)(code & kPkLbMask) * blockDim.x + threadIdx.x, a.ncase, &q, &c);
+    if (q >= nn || !mg_running(a.st ? a.st + c : nullptr)) continue;
+    mg_apply_node(a.d, nn, q, a.S, a.x.p[c], a.r.p[c], a.invd, a.y.p[c], mode, mode == 1 ? *a.om : 0.0f);
+  }
 }
 
 template <bool MULTI>
 __global__ void __launch_bounds__(kMgDofThreads) k_mg_apply_pk(const PkApply* __restrict__ tab,
-                                                               const unsigned* __restrict__ starts, int n, int mode) {
-  const int e = pk_entry(starts, n, blockIdx.x);
-  const PkApply& a = tab[e];
-  const int64_t nn = mg_nn(a.d);
-  int64_t q;
-  int c;
-  mg_item_case<MULTI>((int64_t)(blockIdx.x - __ldg(starts + e)) * 64 + (threadIdx.x & 63), a.ncase, &q, &c);
-  if (q >= nn || !mg_running(a.st ? a.st + c : nullptr)) return;
-  mg_apply_row(a.d, nn, q, (int)(threadIdx.x >> 6), a.S, a.x.p[c], a.r.p[c], a.invd, a.y.p[c], mode,
-               mode == 1 ? *a.om : 0.0f);
+                                                               const unsigned* __restrict__ items,
+                                                               const unsigned* __restrict__ count, int mode) {
+  const unsigned cnt = *count;
+  for (unsigned w = blockIdx.x; w < cnt; w += gridDim.x) {
+    const unsigned code = items[w];
+    const PkApply& a = tab[code >> kPkLbBits];
+    const int64_t nn = mg_nn(a.d);
+    int64_t q;
+    int c;
+    mg_item_case<MULTI>((int64_t)(code & kPkLbMask) * 64 + (threadIdx.x & 63), a.ncase, &q, &c);
+    if (q >= nn || !mg_running(a.st ? a.st + c : nullptr)) continue;
+    mg_apply_row(a.d, nn, q, (int)(threadIdx.x >> 6), a.S, a.x.p[c], a.r.p[c], a.invd, a.y.p[c], mode,
+                 mode == 1 ? *a.om : 0.0f);
+  }
 }
 
 struct PkRestrict {  // restriction of a problem's level to the next coarser one (all its cases)
@@ -4302,16 +4362,21 @@ struct PkRestrict {  // restriction of a problem's level to the next coarser one
 };
 
 template <bool PAD, bool MULTI>
-__global__ void k_mg_restrict_pk(const PkRestrict* __restrict__ tab, const unsigned* __restrict__ starts, int n) {
-  const int e = pk_entry(starts, n, blockIdx.x);
-  const PkRestrict& a = tab[e];
-  int64_t q;
-  int k;
-  mg_item_case<MULTI>((int64_t)(blockIdx.x - __ldg(starts + e)) * blockDim.x + threadIdx.x, a.ncase, &q, &k);
-  if (q >= mg_nn(a.c) || !mg_running(a.st ? a.st + k : nullptr)) return;
-  const float omega = a.first_sweep ? *a.om : 0.f;
-  mg_restrict_node<PAD>(a.f, a.pitch, a.rf.p[k], a.tf.p[k], a.c, a.invdc, a.rc.p[k], q,
-                        a.first_sweep ? a.xc.p[k] : nullptr, omega);
+__global__ void k_mg_restrict_pk(const PkRestrict* __restrict__ tab,
+                                                        const unsigned* __restrict__ items,
+                                                        const unsigned* __restrict__ count) {
+  const unsigned cnt = *count;
+  for (unsigned w = blockIdx.x; w < cnt; w += gridDim.x) {
+    const unsigned code = items[w];
+    const PkRestrict& a = tab[code >> kPkLbBits];
+    int64_t q;
+    int k;
+    mg_item_case<MULTI>((int64_t)(code & kPkLbMask) * blockDim.x + threadIdx.x, a.ncase, &q, &k);
+    if (q >= mg_nn(a.c) || !mg_running(a.st ? a.st + k : nullptr)) continue;
+    const float omega = a.first_sweep ? *a.om : 0.f;
+    mg_restrict_node<PAD>(a.f, a.pitch, a.rf.p[k], a.tf.p[k], a.c, a.invdc, a.rc.p[k], q,
+                          a.first_sweep ? a.xc.p[k] : nullptr, omega);
+  }
 }
 
 struct PkProlong {  // prolongation of a problem's level to the next finer one (all its cases)
@@ -4324,14 +4389,19 @@ struct PkProlong {  // prolongation of a problem's level to the next finer one (
 };
 
 template <bool PAD, bool MULTI>
-__global__ void k_mg_prolong_pk(const PkProlong* __restrict__ tab, const unsigned* __restrict__ starts, int n) {
-  const int e = pk_entry(starts, n, blockIdx.x);
-  const PkProlong& a = tab[e];
-  int64_t q;
-  int k;
-  mg_item_case<MULTI>((int64_t)(blockIdx.x - __ldg(starts + e)) * blockDim.x + threadIdx.x, a.ncase, &q, &k);
-  if (q >= mg_nn(a.f) || !mg_running(a.st ? a.st + k : nullptr)) return;
-  mg_prolong_node<PAD>(a.f, a.pitch, a.nf, a.invdf, a.xf.p[k], a.c, a.xc.p[k], q);
+__global__ void k_mg_prolong_pk(const PkProlong* __restrict__ tab,
+                                                       const unsigned* __restrict__ items,
+                                                       const unsigned* __restrict__ count) {
+  const unsigned cnt = *count;
+  for (unsigned w = blockIdx.x; w < cnt; w += gridDim.x) {
+    const unsigned code = items[w];
+    const PkProlong& a = tab[code >> kPkLbBits];
+    int64_t q;
+    int k;
+    mg_item_case<MULTI>((int64_t)(code & kPkLbMask) * blockDim.x + threadIdx.x, a.ncase, &q, &k);
+    if (q >= mg_nn(a.f) || !mg_running(a.st ? a.st + k : nullptr)) continue;
+    mg_prolong_node<PAD>(a.f, a.pitch, a.nf, a.invdf, a.xf.p[k], a.c, a.xc.p[k], q);
+  }
 }
 
 struct PkTail {  // the cluster kernel of a problem's V-cycle (all its cases); one cluster per entry
@@ -4395,10 +4465,11 @@ enum PkKind : int { PK_MV0, PK_MV1, PK_ENTER, PK_EXIT, PK_APPLY_DOF, PK_APPLY_NO
 struct PkLaunch {
   int kind;
   bool pad, multi;
-  int mode;            // apply: 1 sweep, 2 residual (enter / exit take the step's mode)
-  size_t tab, starts;  // byte offsets in the plan's device arena
+  int mode;  // apply: 1 sweep, 2 residual (enter / exit take the step's mode)
+  size_t tab, starts, est, enc, items, count;  // byte offsets in the plan's device arena
   int n;
-  unsigned blocks;
+  unsigned blocks;  // work items when every entry runs (its launches alone's CTAs)
+  unsigned grid;    // persistent CTAs of the launch
 };
 
 // A right-hand side of a packed solve: its voxel-level FP32 vectors, state, RHS and solution.
@@ -4425,6 +4496,9 @@ struct PackPlan {
   MixState* d_states = nullptr; // [nu] gathered states
   PkInit* d_init = nullptr;     // [nu]
   std::vector<PkLaunch> mv1[2], enter[2], exitl, vcycle;
+  // work lists compacted together at the start of an outer iteration (t = 0, 1) and of a start / restart
+  size_t grp_iter[2] = {0, 0}, grp_step = 0;
+  int n_iter[2] = {0, 0}, n_step = 0;
   cudaGraphExec_t chunk = nullptr;
   int per_chunk = 0;
 };
@@ -4469,7 +4543,7 @@ struct PkBuilder {
   }
   template <class T>
   void add(std::vector<PkLaunch>& out, int kind, bool pad, bool multi, int mode, const std::vector<T>& ents,
-           const std::vector<unsigned>& nblk) {
+           const std::vector<unsigned>& nblk, const std::vector<std::pair<MixState*, int>>& es) {
     if (ents.empty()) return;
     PkLaunch L{};
     L.kind = kind;
@@ -4478,56 +4552,112 @@ struct PkBuilder {
     L.mode = mode;
     L.n = (int)ents.size();
     L.tab = put(ents.data(), sizeof(T) * ents.size(), 64);
-    std::vector<unsigned> st(ents.size());
+    std::vector<unsigned> st(ents.size() + 1);
+    std::vector<MixState*> ep(ents.size());
+    std::vector<int> ec(ents.size());
     unsigned acc = 0;
     for (size_t e = 0; e < ents.size(); ++e) {
       st[e] = acc;
       acc += nblk[e];
+      ep[e] = es[e].first;
+      ec[e] = es[e].second;
     }
+    st[ents.size()] = acc;
     L.blocks = acc;
     L.starts = put(st.data(), sizeof(unsigned) * st.size(), 16);
+    L.est = put(ep.data(), sizeof(MixState*) * ep.size(), 16);
+    L.enc = put(ec.data(), sizeof(int) * ec.size(), 16);
+    std::vector<unsigned> zero(acc + 1, 0u);
+    L.items = put(zero.data(), sizeof(unsigned) * acc, 16);
+    L.count = put(zero.data(), sizeof(unsigned), 16);
     out.push_back(L);
   }
 };
 
+// resident CTAs per SM of a packed kernel (its persistent grid: this times the SMs, at most its work items)
+static int pk_resident(int kind, bool pad, bool multi) {
+  static std::mutex mu;
+  static std::map<int, int> memo;
+  const int key = kind * 4 + (pad ? 2 : 0) + (multi ? 1 : 0);
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = memo.find(key);
+  if (it != memo.end()) return it->second;
+  int o = 0;
+  cudaError_t e = cudaSuccess;
+  switch (kind) {
+    case PK_MV0: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_mv32f_pk<0>, FX * FY, fac_smem_bytes(0)); break;
+    case PK_MV1: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_mv32f_pk<1>, FX * FY, fac_smem_bytes(1)); break;
+    case PK_ENTER: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_mg_enter32_pk, kT, 0); break;
+    case PK_EXIT: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_mg_exit32_pk, kT, 0); break;
+    case PK_APPLY_DOF:
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, multi ? k_mg_apply_pk<true> : k_mg_apply_pk<false>,
+                                                        kMgDofThreads, 0);
+      break;
+    case PK_APPLY_NODE:
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &o, multi ? k_mg_apply_nodes_pk<true> : k_mg_apply_nodes_pk<false>, 256, 0);
+      break;
+    case PK_RESTRICT:
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &o, pad ? (multi ? k_mg_restrict_pk<true, true> : k_mg_restrict_pk<true, false>)
+                  : (multi ? k_mg_restrict_pk<false, true> : k_mg_restrict_pk<false, false>), 256, 0);
+      break;
+    case PK_PROLONG:
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &o, pad ? (multi ? k_mg_prolong_pk<true, true> : k_mg_prolong_pk<true, false>)
+                  : (multi ? k_mg_prolong_pk<false, true> : k_mg_prolong_pk<false, false>), 256, 0);
+      break;
+    default: o = 1;
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    o = 1;
+  }
+  o = std::max(1, o);
+  memo[key] = o;
+  return o;
+}
+
 static void pk_issue(const PackPlan& P, const PkLaunch& L, cudaStream_t s, int step_mode) {
   const char* base = (const char*)P.arena;
   const void* tab = base + L.tab;
-  const unsigned* st = (const unsigned*)(base + L.starts);
+  const unsigned* it = (const unsigned*)(base + L.items);
+  const unsigned* cn = (const unsigned*)(base + L.count);
+  const unsigned g = L.grid;
   switch (L.kind) {
     case PK_MV0:
-      k_mv32f_pk<0><<<L.blocks, dim3(FX, FY), fac_smem_bytes(0), s>>>((const PkMv*)tab, st, L.n);
+      k_mv32f_pk<0><<<g, dim3(FX, FY), fac_smem_bytes(0), s>>>((const PkMv*)tab, it, cn);
       break;
     case PK_MV1:
-      k_mv32f_pk<1><<<L.blocks, dim3(FX, FY), fac_smem_bytes(1), s>>>((const PkMv*)tab, st, L.n);
+      k_mv32f_pk<1><<<g, dim3(FX, FY), fac_smem_bytes(1), s>>>((const PkMv*)tab, it, cn);
       break;
     case PK_ENTER:
-      k_mg_enter32_pk<<<L.blocks, kT, 0, s>>>((const PkVec*)tab, st, L.n, step_mode);
+      k_mg_enter32_pk<<<g, kT, 0, s>>>((const PkVec*)tab, it, cn, step_mode);
       break;
     case PK_EXIT:
-      k_mg_exit32_pk<<<L.blocks, kT, 0, s>>>((const PkVec*)tab, st, L.n, step_mode);
+      k_mg_exit32_pk<<<g, kT, 0, s>>>((const PkVec*)tab, it, cn, step_mode);
       break;
     case PK_APPLY_DOF:
-      (L.multi ? k_mg_apply_pk<true> : k_mg_apply_pk<false>)<<<L.blocks, kMgDofThreads, 0, s>>>(
-          (const PkApply*)tab, st, L.n, L.mode);
+      (L.multi ? k_mg_apply_pk<true> : k_mg_apply_pk<false>)<<<g, kMgDofThreads, 0, s>>>((const PkApply*)tab, it, cn,
+                                                                                         L.mode);
       break;
     case PK_APPLY_NODE:
-      (L.multi ? k_mg_apply_nodes_pk<true> : k_mg_apply_nodes_pk<false>)<<<L.blocks, 256, 0, s>>>(
-          (const PkApply*)tab, st, L.n, L.mode);
+      (L.multi ? k_mg_apply_nodes_pk<true> : k_mg_apply_nodes_pk<false>)<<<g, 256, 0, s>>>((const PkApply*)tab, it,
+                                                                                           cn, L.mode);
       break;
     case PK_RESTRICT: {
       auto k = L.pad ? (L.multi ? k_mg_restrict_pk<true, true> : k_mg_restrict_pk<true, false>)
                      : (L.multi ? k_mg_restrict_pk<false, true> : k_mg_restrict_pk<false, false>);
-      k<<<L.blocks, 256, 0, s>>>((const PkRestrict*)tab, st, L.n);
+      k<<<g, 256, 0, s>>>((const PkRestrict*)tab, it, cn);
       break;
     }
     case PK_PROLONG: {
       auto k = L.pad ? (L.multi ? k_mg_prolong_pk<true, true> : k_mg_prolong_pk<true, false>)
                      : (L.multi ? k_mg_prolong_pk<false, true> : k_mg_prolong_pk<false, false>);
-      k<<<L.blocks, 256, 0, s>>>((const PkProlong*)tab, st, L.n);
+      k<<<g, 256, 0, s>>>((const PkProlong*)tab, it, cn);
       break;
     }
-    case PK_TAIL: {
+    case PK_TAIL: {  // one cluster per problem (not listed: a done problem's cluster returns at once)
       cudaLaunchConfig_t cfg = {};
       cfg.gridDim = dim3((unsigned)(kMgTailCtas * L.n));
       cfg.blockDim = dim3(kMgTailThreads);
@@ -4546,6 +4676,11 @@ static void pk_issue(const PackPlan& P, const PkLaunch& L, cudaStream_t s, int s
   }
 }
 
+// the work lists of a group, compacted on the device (one CTA per list)
+static void pk_compact(const PackPlan& P, cudaStream_t s, size_t grp, int n) {
+  if (n > 0) k_pk_compact<<<n, 1024, 0, s>>>((const PkList*)((const char*)P.arena + grp));
+}
+
 // one outer step of every unit (mode 0: after the matvec, pcur p0 (sel 0) or p1; 1: after a replacement;
 // 2: start): k_mg_enter32, the V-cycle, k_mg_exit32, all packed. Returns the launches.
 static int pk_step(const PackPlan& P, cudaStream_t s, int mode, int sel) {
@@ -4553,6 +4688,12 @@ static int pk_step(const PackPlan& P, cudaStream_t s, int mode, int sel) {
   for (const PkLaunch& L : P.vcycle) pk_issue(P, L, s, mode);
   for (const PkLaunch& L : P.exitl) pk_issue(P, L, s, mode);
   return (int)(P.enter[sel].size() + P.vcycle.size() + P.exitl.size());
+}
+
+// a start (mode 2) or restart (mode 1) step of the units that run, their lists compacted first
+static int pk_restart(const PackPlan& P, cudaStream_t s, int mode) {
+  pk_compact(P, s, P.grp_step, P.n_step);
+  return 1 + pk_step(P, s, mode, 0);
 }
 
 // Builds the packed launches of the units (grouped by problem: the units of a problem with load cases are its
@@ -4612,16 +4753,19 @@ static int32_t pk_build(mycel_ctx* c, PackWork* w, std::vector<PkUnit>& units, c
   for (int t = 0; t < 2; ++t) {  // outer K p: t = 0 p0 = z + beta p1, t = 1 p1 = z + beta p0
     std::vector<PkMv> e;
     std::vector<unsigned> nb;
+    std::vector<std::pair<MixState*, int>> es;
     for (const PkUnit& u : units) {
       unsigned n_ = 0;
       e.push_back(mv_entry(u, u.tz, t ? u.tp0 : u.tp1, t ? u.p1 : u.p0, u.ap, u.st, u.part, &n_));
       nb.push_back(n_);
+      es.push_back({u.st, 1});
     }
-    B.add(P.mv1[t], PK_MV1, false, false, 1, e, nb);
+    B.add(P.mv1[t], PK_MV1, false, false, 1, e, nb, es);
   }
   for (int sel = 0; sel < 2; ++sel) {
     std::vector<PkVec> e;
     std::vector<unsigned> nb;
+    std::vector<std::pair<MixState*, int>> es;
     for (const PkUnit& u : units) {
       PkVec v{};
       v.n = u.p->g.n32;
@@ -4638,9 +4782,10 @@ static int32_t pk_build(mycel_ctx* c, PackWork* w, std::vector<PkUnit>& units, c
       v.nb = (unsigned)stream_blocks(u.p);
       e.push_back(v);
       nb.push_back(v.nb);
+      es.push_back({u.st, 1});
     }
-    B.add(P.enter[sel], PK_ENTER, false, false, 0, e, nb);
-    if (sel == 0) B.add(P.exitl, PK_EXIT, false, false, 0, e, nb);
+    B.add(P.enter[sel], PK_ENTER, false, false, 0, e, nb, es);
+    if (sel == 0) B.add(P.exitl, PK_EXIT, false, false, 0, e, nb, es);
   }
   struct Prob {  // a problem: its first unit and case count
     mycel_problem* p;
@@ -4657,12 +4802,14 @@ static int32_t pk_build(mycel_ctx* c, PackWork* w, std::vector<PkUnit>& units, c
   auto fine_mv = [&]() {  // t = A z at the voxel level, every unit (MODE 0)
     std::vector<PkMv> e;
     std::vector<unsigned> nb;
+    std::vector<std::pair<MixState*, int>> es;
     for (const PkUnit& u : units) {
       unsigned n_ = 0;
       e.push_back(mv_entry(u, u.tz, u.tz, nullptr, u.t, u.st, nullptr, &n_));
       nb.push_back(n_);
+      es.push_back({u.st, 1});
     }
-    B.add(P.vcycle, PK_MV0, false, false, 0, e, nb);
+    B.add(P.vcycle, PK_MV0, false, false, 0, e, nb, es);
   };
   auto unit_ptrs = [&](const Prob& q, int which) {  // voxel-level vectors of a problem's units: r, t or z
     MgPtrs r{};
@@ -4679,6 +4826,7 @@ static int32_t pk_build(mycel_ctx* c, PackWork* w, std::vector<PkUnit>& units, c
   for (int multi = 0; multi < 2; ++multi) {  // voxel grid -> level 1, with level 1's first sweep
     std::vector<PkRestrict> e;
     std::vector<unsigned> nb;
+    std::vector<std::pair<MixState*, int>> es;
     for (const Prob& q : probs) {
       if ((q.nc > 1) != (multi == 1)) continue;
       MgHier* mg = q.p->mg;
@@ -4698,14 +4846,16 @@ static int32_t pk_build(mycel_ctx* c, PackWork* w, std::vector<PkUnit>& units, c
       a.ncase = q.nc;
       e.push_back(a);
       nb.push_back(mg_blocks(v1.nn * q.nc));
+      es.push_back({const_cast<MixState*>(q.st), q.nc});
     }
-    B.add(P.vcycle, PK_RESTRICT, true, multi == 1, 0, e, nb);
+    B.add(P.vcycle, PK_RESTRICT, true, multi == 1, 0, e, nb, es);
   }
   auto applies = [&](int l, bool down) {  // level l's product of every problem that smooths it separately
     for (int node = 0; node < 2; ++node)
       for (int multi = 0; multi < 2; ++multi) {
         std::vector<PkApply> e;
         std::vector<unsigned> nb;
+    std::vector<std::pair<MixState*, int>> es;
         for (size_t qi = 0; qi < probs.size(); ++qi) {
           const Prob& q = probs[qi];
           MgHier* mg = q.p->mg;
@@ -4725,8 +4875,9 @@ static int32_t pk_build(mycel_ctx* c, PackWork* w, std::vector<PkUnit>& units, c
           a.ncase = q.nc;
           e.push_back(a);
           nb.push_back(node ? mg_blocks(v.nn * q.nc) : mg_dof_blocks(v.nn * q.nc));
+          es.push_back({const_cast<MixState*>(q.st), q.nc});
         }
-        B.add(P.vcycle, node ? PK_APPLY_NODE : PK_APPLY_DOF, false, multi == 1, down ? 2 : 1, e, nb);
+        B.add(P.vcycle, node ? PK_APPLY_NODE : PK_APPLY_DOF, false, multi == 1, down ? 2 : 1, e, nb, es);
       }
   };
   for (int l = 1; l < maxT; ++l) {
@@ -4734,6 +4885,7 @@ static int32_t pk_build(mycel_ctx* c, PackWork* w, std::vector<PkUnit>& units, c
     for (int multi = 0; multi < 2; ++multi) {  // level l -> l + 1
       std::vector<PkRestrict> e;
       std::vector<unsigned> nb;
+    std::vector<std::pair<MixState*, int>> es;
       for (size_t qi = 0; qi < probs.size(); ++qi) {
         const Prob& q = probs[qi];
         MgHier* mg = q.p->mg;
@@ -4755,14 +4907,16 @@ static int32_t pk_build(mycel_ctx* c, PackWork* w, std::vector<PkUnit>& units, c
         a.ncase = q.nc;
         e.push_back(a);
         nb.push_back(mg_blocks(cv.nn * q.nc));
+        es.push_back({const_cast<MixState*>(q.st), q.nc});
         xc[qi][l] = v.xa;
       }
-      B.add(P.vcycle, PK_RESTRICT, false, multi == 1, 0, e, nb);
+      B.add(P.vcycle, PK_RESTRICT, false, multi == 1, 0, e, nb, es);
     }
   }
   for (int multi = 0; multi < 2; ++multi) {  // the cluster kernels
     std::vector<PkTail> e;
     std::vector<unsigned> nb;
+    std::vector<std::pair<MixState*, int>> es;
     for (size_t qi = 0; qi < probs.size(); ++qi) {
       const Prob& q = probs[qi];
       if ((q.nc > 1) != (multi == 1)) continue;
@@ -4774,14 +4928,16 @@ static int32_t pk_build(mycel_ctx* c, PackWork* w, std::vector<PkUnit>& units, c
       t.ncase = q.nc;
       e.push_back(t);
       nb.push_back(kMgTailCtas);
+      es.push_back({const_cast<MixState*>(q.st), q.nc});
       xc[qi][mg->T] = mg->lv[mg->T].xa;
     }
-    B.add(P.vcycle, PK_TAIL, false, multi == 1, 0, e, nb);
+    B.add(P.vcycle, PK_TAIL, false, multi == 1, 0, e, nb, es);
   }
   for (int l = maxT - 1; l >= 1; --l) {
     for (int multi = 0; multi < 2; ++multi) {  // level l + 1 -> l, into xa (the downward sweep's vector)
       std::vector<PkProlong> e;
       std::vector<unsigned> nb;
+    std::vector<std::pair<MixState*, int>> es;
       for (size_t qi = 0; qi < probs.size(); ++qi) {
         const Prob& q = probs[qi];
         MgHier* mg = q.p->mg;
@@ -4799,8 +4955,9 @@ static int32_t pk_build(mycel_ctx* c, PackWork* w, std::vector<PkUnit>& units, c
         a.ncase = q.nc;
         e.push_back(a);
         nb.push_back(mg_blocks(v.nn * q.nc));
+        es.push_back({const_cast<MixState*>(q.st), q.nc});
       }
-      B.add(P.vcycle, PK_PROLONG, false, multi == 1, 0, e, nb);
+      B.add(P.vcycle, PK_PROLONG, false, multi == 1, 0, e, nb, es);
     }
     applies(l, false);
     for (size_t qi = 0; qi < probs.size(); ++qi)
@@ -4809,6 +4966,7 @@ static int32_t pk_build(mycel_ctx* c, PackWork* w, std::vector<PkUnit>& units, c
   for (int multi = 0; multi < 2; ++multi) {  // level 1 -> voxel grid, into each unit's z
     std::vector<PkProlong> e;
     std::vector<unsigned> nb;
+    std::vector<std::pair<MixState*, int>> es;
     for (size_t qi = 0; qi < probs.size(); ++qi) {
       const Prob& q = probs[qi];
       if ((q.nc > 1) != (multi == 1)) continue;
@@ -4825,27 +4983,72 @@ static int32_t pk_build(mycel_ctx* c, PackWork* w, std::vector<PkUnit>& units, c
       a.ncase = q.nc;
       e.push_back(a);
       nb.push_back(mg_blocks(mg->lv[0].nn * q.nc));
+      es.push_back({const_cast<MixState*>(q.st), q.nc});
     }
-    B.add(P.vcycle, PK_PROLONG, true, multi == 1, 0, e, nb);
+    B.add(P.vcycle, PK_PROLONG, true, multi == 1, 0, e, nb, es);
   }
   fine_mv();
+  // persistent grids: the resident CTAs, at most the work items (the cluster kernels are not persistent)
+  for (std::vector<PkLaunch>* v : {&P.mv1[0], &P.mv1[1], &P.enter[0], &P.enter[1], &P.exitl, &P.vcycle})
+    for (PkLaunch& L : *v)
+      if (L.kind != PK_TAIL)
+        L.grid = std::max(1u, std::min<unsigned>(L.blocks, (unsigned)(pk_resident(L.kind, L.pad, L.multi) * c->num_sms)));
+  // work-list groups, written once the arena's address is known
+  std::vector<const PkLaunch*> gi[2], gs;
+  auto listed = [](std::vector<const PkLaunch*>& g, const std::vector<PkLaunch>& v) {
+    for (const PkLaunch& L : v)
+      if (L.kind != PK_TAIL) g.push_back(&L);
+  };
+  for (int t = 0; t < 2; ++t) {
+    listed(gi[t], P.mv1[t]);
+    listed(gi[t], P.enter[t]);
+    listed(gi[t], P.vcycle);
+    listed(gi[t], P.exitl);
+  }
+  listed(gs, P.enter[0]);
+  listed(gs, P.vcycle);
+  listed(gs, P.exitl);
+  auto reserve = [&](const std::vector<const PkLaunch*>& g) {
+    std::vector<PkList> z(g.size());
+    std::memset(z.data(), 0, sizeof(PkList) * z.size());
+    return B.put(z.data(), sizeof(PkList) * z.size(), 64);
+  };
+  for (int t = 0; t < 2; ++t) {
+    P.grp_iter[t] = reserve(gi[t]);
+    P.n_iter[t] = (int)gi[t].size();
+  }
+  P.grp_step = reserve(gs);
+  P.n_step = (int)gs.size();
   P.arena_bytes = B.host.size();
   MYCEL_CUDA(c, cudaMallocAsync(&P.arena_alloc, P.arena_bytes + 128, s));
   P.arena = (void*)(((uintptr_t)P.arena_alloc + 127) & ~(uintptr_t)127);  // tensor maps: 64-byte aligned
+  char* base = (char*)P.arena;
+  auto fill = [&](size_t off, const std::vector<const PkLaunch*>& g) {
+    for (size_t k = 0; k < g.size(); ++k) {
+      const PkLaunch& L = *g[k];
+      PkList h{L.n, (const unsigned*)(base + L.starts), (MixState* const*)(base + L.est), (const int*)(base + L.enc),
+               (unsigned*)(base + L.items), (unsigned*)(base + L.count)};
+      std::memcpy(B.host.data() + off + k * sizeof(PkList), &h, sizeof h);
+    }
+  };
+  for (int t = 0; t < 2; ++t) fill(P.grp_iter[t], gi[t]);
+  fill(P.grp_step, gs);
   MYCEL_CUDA(c, cudaMemcpyAsync(P.arena, B.host.data(), P.arena_bytes, cudaMemcpyHostToDevice, s));
   MYCEL_CUDA(c, cudaStreamSynchronize(s));
   P.nu = nu;
-  P.d_sts = (MixState**)((char*)P.arena + o_sts);
-  P.d_states = (MixState*)((char*)P.arena + o_states);
-  P.d_init = (PkInit*)((char*)P.arena + o_init);
+  P.d_sts = (MixState**)(base + o_sts);
+  P.d_states = (MixState*)(base + o_states);
+  P.d_init = (PkInit*)(base + o_init);
   P.key = key;
-  // chunk graph: two outer iterations of every unit, then the states gathered for one copy
+  // chunk graph: two outer iterations of every unit (each starting with its work lists), then the states
+  // gathered for one copy
   cudaGraph_t graph;
   MYCEL_CUDA(c, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
   int nl = 0;
   for (int t = 0; t < 2; ++t) {
+    pk_compact(P, s, P.grp_iter[t], P.n_iter[t]);
     for (const PkLaunch& L : P.mv1[t]) pk_issue(P, L, s, 0);
-    nl += (int)P.mv1[t].size() + pk_step(P, s, 0, t);
+    nl += 1 + (int)P.mv1[t].size() + pk_step(P, s, 0, t);
   }
   k_pk_gather<<<(nu + 127) / 128, 128, 0, s>>>(P.d_sts, nu, P.d_states);
   nl++;
@@ -5068,7 +5271,7 @@ int32_t mg_solve_packed(mycel_ctx* c, int njobs, PackJob* jobs, const volatile i
   MYCEL_CUDA(c, cudaMemcpyAsync(P.d_init, h_init, sizeof(PkInit) * nu, cudaMemcpyHostToDevice, s));
   k_pk_init<<<(nu + 127) / 128, 128, 0, s>>>(P.d_sts, P.d_init, nu, 1e-3);
   c->launches++;
-  if (nact > 0) c->launches += pk_step(P, s, 2, 0);
+  if (nact > 0) c->launches += pk_restart(P, s, 2);
   lap("initial residuals and start", nact);
   int64_t launched = 0;
   int rounds = 0;
@@ -5154,7 +5357,7 @@ int32_t mg_solve_packed(mycel_ctx* c, int njobs, PackJob* jobs, const volatile i
     lap("round", (int)launched);
     ++rounds;
     if (!restart) break;
-    c->launches += pk_step(P, s, 1, 0);  // the restarting units' preconditioned residual (the others skip)
+    c->launches += pk_restart(P, s, 1);  // the restarting units' preconditioned residual (the others skip)
   }
   MYCEL_CUDA(c, cudaStreamSynchronize(s));
   const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
