@@ -4535,6 +4535,7 @@ void pack_release(mycel_ctx* c) {
 // host-side table builder: entries of one packed launch, 64-byte aligned, then their CTA starts
 struct PkBuilder {
   std::vector<unsigned char> host;
+  bool overflow = false;
   size_t put(const void* src, size_t bytes, size_t align) {
     size_t off = (host.size() + align - 1) & ~(align - 1);
     host.resize(off + bytes);
@@ -4559,6 +4560,7 @@ struct PkBuilder {
     for (size_t e = 0; e < ents.size(); ++e) {
       st[e] = acc;
       acc += nblk[e];
+      if (nblk[e] > kPkLbMask) overflow = true;  // a work item holds the CTA number in kPkLbBits bits
       ep[e] = es[e].first;
       ec[e] = es[e].second;
     }
@@ -4988,6 +4990,7 @@ static int32_t pk_build(mycel_ctx* c, PackWork* w, std::vector<PkUnit>& units, c
     B.add(P.vcycle, PK_PROLONG, true, multi == 1, 0, e, nb, es);
   }
   fine_mv();
+  if (B.overflow) return set_error(c, MYCEL_E_ARG, "packed solve: a problem's launch has too many CTAs for a work item");
   // persistent grids: the resident CTAs, at most the work items (the cluster kernels are not persistent)
   for (std::vector<PkLaunch>* v : {&P.mv1[0], &P.mv1[1], &P.enter[0], &P.enter[1], &P.exitl, &P.vcycle})
     for (PkLaunch& L : *v)
