@@ -402,6 +402,7 @@ extern "C" int32_t mycel_ctx_destroy(mycel_ctx* c) {
   if (!c) return MYCEL_OK;
   cudaSetDevice(c->device);
   pack_release(c);  // frees on the stream: before it goes
+  fan_release(c);
   if (c->stream) {
     cudaStreamSynchronize(c->stream);
     cudaStreamDestroy(c->stream);
@@ -874,6 +875,75 @@ extern "C" int32_t mycel_pcg_solve(mycel_problem* p, const double* b, double* x,
 }
 
 namespace mycel {
+namespace {
+struct Fan {
+  static constexpr int kN = 8;
+  cudaStream_t s[kN] = {}, side[kN] = {};
+  cudaEvent_t fork_ev = nullptr, join_ev[kN] = {};
+  bool used[kN] = {};
+  bool active = false;
+};
+}  // namespace
+
+int32_t fan_begin(mycel_ctx* c) {
+  Fan* f = (Fan*)c->fan;
+  if (!f) {
+    f = new Fan();
+    c->fan = f;
+    for (int k = 0; k < Fan::kN; ++k) {
+      MYCEL_CUDA(c, cudaStreamCreateWithFlags(&f->s[k], cudaStreamNonBlocking));
+      MYCEL_CUDA(c, cudaStreamCreateWithFlags(&f->side[k], cudaStreamNonBlocking));
+      MYCEL_CUDA(c, cudaEventCreateWithFlags(&f->join_ev[k], cudaEventDisableTiming));
+    }
+    MYCEL_CUDA(c, cudaEventCreateWithFlags(&f->fork_ev, cudaEventDisableTiming));
+  }
+  c->main_stream = c->stream;
+  c->main_side = c->side;
+  MYCEL_CUDA(c, cudaEventRecord(f->fork_ev, c->stream));
+  for (int k = 0; k < Fan::kN; ++k) f->used[k] = false;
+  f->active = true;
+  return MYCEL_OK;
+}
+
+void fan_use(mycel_ctx* c, int slot) {
+  Fan* f = (Fan*)c->fan;
+  if (!f || !f->active) return;
+  const int k = slot % Fan::kN;
+  if (!f->used[k]) {  // the side stream starts after the context stream's work so far
+    cudaStreamWaitEvent(f->s[k], f->fork_ev, 0);
+    cudaStreamWaitEvent(f->side[k], f->fork_ev, 0);
+    f->used[k] = true;
+  }
+  c->stream = f->s[k];
+  c->side = f->side[k];
+}
+
+void fan_end(mycel_ctx* c) {
+  Fan* f = (Fan*)c->fan;
+  if (!f || !f->active) return;
+  c->stream = c->main_stream;
+  c->side = c->main_side;
+  for (int k = 0; k < Fan::kN; ++k)
+    if (f->used[k]) {  // a side stream's side work is joined into it by the work itself (mg_setup)
+      cudaEventRecord(f->join_ev[k], f->s[k]);
+      cudaStreamWaitEvent(c->stream, f->join_ev[k], 0);
+    }
+  f->active = false;
+}
+
+void fan_release(mycel_ctx* c) {
+  Fan* f = (Fan*)c->fan;
+  if (!f) return;
+  for (int k = 0; k < Fan::kN; ++k) {
+    if (f->s[k]) cudaStreamSynchronize(f->s[k]), cudaStreamDestroy(f->s[k]);
+    if (f->side[k]) cudaStreamSynchronize(f->side[k]), cudaStreamDestroy(f->side[k]);
+    if (f->join_ev[k]) cudaEventDestroy(f->join_ev[k]);
+  }
+  if (f->fork_ev) cudaEventDestroy(f->fork_ev);
+  delete f;
+  c->fan = nullptr;
+}
+
 int32_t solve_dispatch(mycel_problem* p, double* d_u, double tol, int max_iter, int precision,
                        const volatile int32_t* cancel, mycel_pcg_result* res) {
   if (precision == MYCEL_PRECISION_MIXED || precision == MYCEL_PRECISION_FP64_FACTORED ||

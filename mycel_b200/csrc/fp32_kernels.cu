@@ -5099,6 +5099,7 @@ int32_t mg_solve_packed(mycel_ctx* c, int njobs, PackJob* jobs, const volatile i
   };
   std::vector<PkUnit> units;
   std::vector<char> packed(njobs, 0);
+  std::vector<mycel_problem*> need_setup;
   // eligibility; the others are solved alone here, in job order
   for (int j = 0; j < njobs; ++j) {
     PackJob& J = jobs[j];
@@ -5131,10 +5132,7 @@ int32_t mg_solve_packed(mycel_ctx* c, int njobs, PackJob* jobs, const volatile i
     packed[j] = 1;
     MgHier* mg = p->mg;
     MYCEL_CUDA(c, cudaMemsetAsync(p->d_err, 0, sizeof(int), s));
-    if (mg->setup_version != p->e_version) {
-      mg_setup(p);
-      mg->setup_version = p->e_version;
-    }
+    if (mg->setup_version != p->e_version) need_setup.push_back(p);
     const int64_t nd = p->g.nd;
     for (int k = 0; k < J.ncase; ++k) {
       PkUnit u{};
@@ -5166,6 +5164,16 @@ int32_t mg_solve_packed(mycel_ctx* c, int njobs, PackJob* jobs, const volatile i
       }
       units.push_back(u);
     }
+  }
+  // the coarse operators of the packed problems, rebuilt from their new E side by side on the fan's streams
+  if (!need_setup.empty()) {
+    if ((st = fan_begin(c))) return st;
+    for (size_t q = 0; q < need_setup.size(); ++q) {
+      fan_use(c, (int)q);
+      mg_setup(need_setup[q]);
+      need_setup[q]->mg->setup_version = need_setup[q]->e_version;
+    }
+    fan_end(c);
   }
   const int nu = (int)units.size();
   lap("set-up and unpacked jobs", nu);
@@ -5391,6 +5399,15 @@ int32_t mg_solve_packed(mycel_ctx* c, int njobs, PackJob* jobs, const volatile i
     r.elapsed_ms = ms;
   }
   lap("finished alone", rounds);
+  if (verbose) {
+    std::vector<int> it(iters);
+    std::sort(it.begin(), it.end());
+    int64_t sum = 0;
+    for (int v : it) sum += v;
+    std::fprintf(stderr, "mycel: packed outer iterations per right-hand side min %d median %d max %d sum %lld, "
+                 "lockstep %lld, rounds %d\n", it.front(), it[it.size() / 2], it.back(), (long long)sum,
+                 (long long)launched, rounds);
+  }
   return MYCEL_OK;
 }
 

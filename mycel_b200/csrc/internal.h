@@ -115,6 +115,8 @@ struct mycel_ctx {
   int64_t prof_nodes[4] = {0, 0, 0, 0};     // nodes processed by the timed launches
   int64_t prof_elems[4] = {0, 0, 0, 0};     // active elements processed by the timed launches
   void* pack = nullptr;    // packed-solve workspace (fp32_kernels.cu), built on first use
+  void* fan = nullptr;     // side streams for independent per-problem work of a batch step (mycel::fan_*)
+  cudaStream_t main_stream = nullptr, main_side = nullptr;  // the context's own streams while a fan slot is in use
   int64_t packed_rhs = 0;  // right-hand sides whose solves ran through packed launches (a statistic)
 };
 
@@ -332,6 +334,14 @@ struct PackJob {
 // problem's solve alone in the mixed multigrid form.
 int32_t mg_solve_packed(mycel_ctx* c, int njobs, PackJob* jobs, const volatile int32_t* cancel);
 void pack_release(mycel_ctx* c);
+// Fan-out of independent per-problem work of a batch step over side streams: fan_begin makes them wait for
+// the context stream's work so far; fan_use(c, k) issues the following work of the context on side stream k
+// (the context's stream and side stream are swapped, so every launch helper follows); fan_end returns to the
+// context's streams, which then wait for everything issued on the side streams.
+int32_t fan_begin(mycel_ctx* c);
+void fan_use(mycel_ctx* c, int slot);
+void fan_end(mycel_ctx* c);
+void fan_release(mycel_ctx* c);
 bool cases_together_enabled();
 int32_t kernel_bench(mycel_problem* p, int which, int reps, double* avg_us);  // MYCEL_CASES_TOGETHER=0 turns the batched case solve off
 int32_t refined_solve_entry(mycel_problem* p, const double* d_b, const int32_t* d_nz, int32_t n_nz, double* d_u,

@@ -510,11 +510,14 @@ extern "C" int32_t mycel_simp_step_many(mycel_simp_session* const* ss, int32_t n
   std::vector<std::vector<mycel_pcg_result>> cres(n);
   std::vector<PackJob> jobs;
   std::vector<int> job_of;
+  bool fan_on = false;
   for (int i = 0; i < n; ++i) {
     mycel_simp_session* s = ss[i];
     if (done) done[i] = s->done ? 1 : 0;
     if (s->done) continue;
     live[i] = 1;
+    if (!fan_on) fan_on = fan_begin(c) == MYCEL_OK;  // the sessions' filters and E side by side
+    if (fan_on) fan_use(c, i);
     simp_pre(s, &pre[i]);
     const bool packable = s->o.precision == MYCEL_PRECISION_MIXED_MG && (s->ncase == 1 || cases_solved_together(s));
     if (!packable) continue;
@@ -523,6 +526,7 @@ extern "C" int32_t mycel_simp_step_many(mycel_simp_session* const* ss, int32_t n
                            cres[i].data()});
     job_of.push_back(i);
   }
+  if (fan_on) fan_end(c);
   lap("filter, E, diagonal");
   if (!jobs.empty()) {
     int32_t rc = mg_solve_packed(c, (int)jobs.size(), jobs.data(), cancel);
@@ -538,8 +542,13 @@ extern "C" int32_t mycel_simp_step_many(mycel_simp_session* const* ss, int32_t n
     st[i] = simp_solve(s, pre[i], cancel, &pr[i]);
   }
   lap("solves");
+  fan_on = fan_begin(c) == MYCEL_OK;  // sensitivities, adjoint filters and OC updates side by side
   for (int i = 0; i < n; ++i)
-    if (live[i] && !st[i]) st[i] = simp_post_issue(ss[i], pre[i], pr[i]);
+    if (live[i] && !st[i]) {
+      if (fan_on) fan_use(c, i);
+      st[i] = simp_post_issue(ss[i], pre[i], pr[i]);
+    }
+  if (fan_on) fan_end(c);
   lap("sensitivities, adjoint, OC");
   cudaError_t e = cudaStreamSynchronize(c->stream);
   int32_t first = MYCEL_OK;
