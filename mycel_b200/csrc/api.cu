@@ -875,7 +875,6 @@ extern "C" int32_t mycel_pcg_solve(mycel_problem* p, const double* b, double* x,
 }
 
 namespace mycel {
-namespace {
 struct Fan {
   static constexpr int kN = 8;
   cudaStream_t s[kN] = {}, side[kN] = {};
@@ -883,7 +882,6 @@ struct Fan {
   bool used[kN] = {};
   bool active = false;
 };
-}  // namespace
 
 int32_t fan_begin(mycel_ctx* c) {
   Fan* f = (Fan*)c->fan;
