@@ -106,6 +106,8 @@ def parse():
     ap.add_argument("--batched-count", type=int, default=48)
     ap.add_argument("--batched-skip-fp64", action="store_true", help="time only the timed form of --batched")
     ap.add_argument("--batched-iters", type=int, default=4)
+    ap.add_argument("--batched-packs", type=int, default=4,
+                    help="packs of the packed batched form (each on its own context and host thread)")
     ap.add_argument("--batched-mode", choices=("packed", "served", "both"), default="both",
                     help="batched timed form: packed launches of all problems (one context), the serving loop's "
                          "slots, or both (FP64 always through the serving loop)")
@@ -454,41 +456,67 @@ def run_batched(args):
     head = args.precision
     out["cases_together"] = os.environ.get("MYCEL_CASES_TOGETHER", "1") != "0"
     if args.batched_mode in ("packed", "both"):
-        # one context, every problem's session stepped together (mycel_simp_step_many): the mixed multigrid
-        # solves of all problems share their launches; wall time from the first problem's creation to the end
-        ctx = api.Context(0)
+        # packs of problems, each on its own context and host thread: within a pack every problem's session is
+        # stepped together (mycel_simp_step_many, the mixed multigrid solves in shared launches); the packs
+        # run side by side, so one pack's slowest solve overlaps the others' work. Problems are dealt to the
+        # packs largest first (elements x load cases) onto the lightest pack. Wall time from the first problem's
+        # creation to the end.
+        import threading
+        G = max(1, min(args.batched_packs, len(probs)))
+        load = [0] * G
+        member = [[] for _ in range(G)]
+        for k in sorted(range(len(probs)), key=lambda k: -probs[k].model.total_elements * len(probs[k].load_cases)):
+            g = min(range(G), key=lambda q: load[q])
+            member[g].append(k)
+            load[g] += probs[k].model.total_elements * len(probs[k].load_cases)
+        ph = [[] for _ in probs]
+        info = [None] * G
+        errs = []
+
+        def run_pack(g):
+            try:
+                ctx = api.Context(0)
+                ts0 = time.perf_counter()
+                made = []
+                for k in member[g]:
+                    bp = probs[k]
+                    pr = api.Problem(bp.model, ctx)
+                    made.append((k, pr, api.SimpSession(pr, bp.options.replace(
+                        max_iterations=args.batched_iters, precision=head, solver_tolerance_initial=args.job_tol,
+                        solver_tolerance_final=args.job_tol, separate_load_cases=sep))))
+                t_setup = time.perf_counter() - ts0
+                packed0 = ctx.packed_count
+                steps = []
+                while not all(x[2].done for x in made):
+                    live = [x for x in made if not x[2].done]
+                    ts = time.perf_counter()
+                    for x, r in zip(live, api.SimpSession.step_many([x[2] for x in live])):
+                        if r is not None:
+                            ph[x[0]].append(r.compliance)
+                    steps.append(time.perf_counter() - ts)
+                info[g] = {"problems": len(made), "setup_s": t_setup, "step_s": steps,
+                           "rhs_solved_packed": ctx.packed_count - packed0}
+                for _, pr, se in made:
+                    se.close()
+                    pr.close()
+                ctx.close()
+            except Exception as e:  # reported below
+                errs.append(repr(e))
+
         t0 = time.perf_counter()
-        made = []
-        for bp in probs:
-            p = api.Problem(bp.model, ctx)
-            made.append((p, api.SimpSession(p, bp.options.replace(
-                max_iterations=args.batched_iters, precision=head, solver_tolerance_initial=args.job_tol,
-                solver_tolerance_final=args.job_tol, separate_load_cases=sep))))
-        sess = [s for _, s in made]
-        t_setup = time.perf_counter() - t0
-        ph = [[] for _ in sess]
-        n_it = 0
-        packed0 = ctx.packed_count
-        step_s = []
-        while not all(s.done for s in sess):
-            live = [k for k, s in enumerate(sess) if not s.done]
-            ts = time.perf_counter()
-            for k, r in zip(live, api.SimpSession.step_many([sess[k] for k in live])):
-                if r is not None:
-                    ph[k].append(r.compliance)
-                    n_it += 1
-            step_s.append(time.perf_counter() - ts)
+        ths = [threading.Thread(target=run_pack, args=(g,)) for g in range(G)]
+        for t in ths:
+            t.start()
+        for t in ths:
+            t.join()
         wall = time.perf_counter() - t0
-        later = step_s[1:]
-        out["packed"] = {"simp_iter_s": n_it / wall, "wall_s": wall, "simp_iterations": n_it,
-                         "setup_s": t_setup, "step_s": step_s,
-                         "steady_simp_iter_s": len(probs) * len(later) / sum(later) if later else None,
-                         "rhs_solved_packed": ctx.packed_count - packed0,
-                         "form": head, "note": "all problems' solves in shared launches (mycel_simp_step_many)"}
-        for p, s in made:
-            s.close()
-            p.close()
-        ctx.close()
+        if errs:
+            raise RuntimeError("packed batch failed: " + "; ".join(errs))
+        n_it = sum(len(h) for h in ph)
+        out["packed"] = {"simp_iter_s": n_it / wall, "wall_s": wall, "simp_iterations": n_it, "packs": G,
+                         "rhs_solved_packed": sum(x["rhs_solved_packed"] for x in info), "per_pack": info,
+                         "form": head, "note": "packs of problems whose solves share launches "
+                                               "(mycel_simp_step_many), the packs on concurrent contexts"}
         hists["packed"] = ph
     for prec in ((head,) if args.batched_skip_fp64 else (head, "fp64")):
         if prec == head and args.batched_mode == "packed":
