@@ -106,6 +106,9 @@ def parse():
     ap.add_argument("--batched-count", type=int, default=48)
     ap.add_argument("--batched-skip-fp64", action="store_true", help="time only the timed form of --batched")
     ap.add_argument("--batched-iters", type=int, default=4)
+    ap.add_argument("--batched-steady-extra", type=int, default=4,
+                    help="--batched: also run each form with this many more iterations per problem (steady "
+                         "SIMP iter/s from the difference; 0: off)")
     ap.add_argument("--batched-packs", type=int, default=4,
                     help="packs of the packed batched form (each on its own context and host thread)")
     ap.add_argument("--batched-mode", choices=("packed", "served", "both"), default="both",
@@ -443,25 +446,30 @@ def run_surface(args):
 
 
 def run_batched(args):
-    """Batched instances: all problems submitted at once; aggregate SIMP iter/s, the timed form vs FP64."""
+    """Batched instances: all problems at once; aggregate SIMP iter/s of the timed form in packs (solves in
+    shared launches) and through the serving loop's slots, vs FP64. Each form is also run with
+    --batched-steady-extra more iterations per problem: the extra iterations over the extra wall time give the
+    steady SIMP iter/s, without the one-time problem set-up and tear-down."""
+    import threading
     from mycel_b200 import api
     from mycel_b200 import workloads as W
     probs = W.batched_instances(count=args.batched_count)
     sep = args.batched_cases == "separate"
+    head = args.precision
     out = {"metric": "batched instances: aggregate SIMP iter/s", "problems": len(probs),
            "iterations_each": args.batched_iters, "pcg_tol": args.job_tol, "load_cases": args.batched_cases,
            "load_cases_total": int(sum(len(bp.load_cases) for bp in probs)),
-           "elements_total": int(sum(bp.model.total_elements for bp in probs))}
-    hists = {}
-    head = args.precision
-    out["cases_together"] = os.environ.get("MYCEL_CASES_TOGETHER", "1") != "0"
-    if args.batched_mode in ("packed", "both"):
-        # packs of problems, each on its own context and host thread: within a pack every problem's session is
-        # stepped together (mycel_simp_step_many, the mixed multigrid solves in shared launches); the packs
-        # run side by side, so one pack's slowest solve overlaps the others' work. Problems are dealt to the
-        # packs largest first (elements x load cases) onto the lightest pack. Wall time from the first problem's
-        # creation to the end.
-        import threading
+           "elements_total": int(sum(bp.model.total_elements for bp in probs)),
+           "cases_together": os.environ.get("MYCEL_CASES_TOGETHER", "1") != "0"}
+
+    def opts(bp, iters, prec):
+        return bp.options.replace(max_iterations=iters, precision=prec, solver_tolerance_initial=args.job_tol,
+                                  solver_tolerance_final=args.job_tol, separate_load_cases=sep)
+
+    def packed_run(iters):
+        """Packs of problems, each on its own context and host thread; within a pack every problem's session is
+        stepped together (mycel_simp_step_many). Problems go largest first (elements x load cases) to the
+        lightest pack. Returns (wall s, SIMP iterations, compliance histories, per-pack info)."""
         G = max(1, min(args.batched_packs, len(probs)))
         load = [0] * G
         member = [[] for _ in range(G)]
@@ -476,31 +484,22 @@ def run_batched(args):
         def run_pack(g):
             try:
                 ctx = api.Context(0)
-                ts0 = time.perf_counter()
                 made = []
                 for k in member[g]:
-                    bp = probs[k]
-                    pr = api.Problem(bp.model, ctx)
-                    made.append((k, pr, api.SimpSession(pr, bp.options.replace(
-                        max_iterations=args.batched_iters, precision=head, solver_tolerance_initial=args.job_tol,
-                        solver_tolerance_final=args.job_tol, separate_load_cases=sep))))
-                t_setup = time.perf_counter() - ts0
+                    pr = api.Problem(probs[k].model, ctx)
+                    made.append((k, pr, api.SimpSession(pr, opts(probs[k], iters, head))))
                 packed0 = ctx.packed_count
-                steps = []
                 while not all(x[2].done for x in made):
                     live = [x for x in made if not x[2].done]
-                    ts = time.perf_counter()
                     for x, r in zip(live, api.SimpSession.step_many([x[2] for x in live])):
                         if r is not None:
                             ph[x[0]].append(r.compliance)
-                    steps.append(time.perf_counter() - ts)
-                info[g] = {"problems": len(made), "setup_s": t_setup, "step_s": steps,
-                           "rhs_solved_packed": ctx.packed_count - packed0}
+                info[g] = {"problems": len(made), "rhs_solved_packed": ctx.packed_count - packed0}
                 for _, pr, se in made:
                     se.close()
                     pr.close()
                 ctx.close()
-            except Exception as e:  # reported below
+            except Exception as e:  # reported by the caller
                 errs.append(repr(e))
 
         t0 = time.perf_counter()
@@ -512,35 +511,57 @@ def run_batched(args):
         wall = time.perf_counter() - t0
         if errs:
             raise RuntimeError("packed batch failed: " + "; ".join(errs))
-        n_it = sum(len(h) for h in ph)
-        out["packed"] = {"simp_iter_s": n_it / wall, "wall_s": wall, "simp_iterations": n_it, "packs": G,
-                         "rhs_solved_packed": sum(x["rhs_solved_packed"] for x in info), "per_pack": info,
-                         "form": head, "note": "packs of problems whose solves share launches "
-                                               "(mycel_simp_step_many), the packs on concurrent contexts"}
-        hists["packed"] = ph
-    for prec in ((head,) if args.batched_skip_fp64 else (head, "fp64")):
-        if prec == head and args.batched_mode == "packed":
-            continue
+        return wall, sum(len(h) for h in ph), ph, info
+
+    def served_run(iters, prec):
+        """All problems submitted at once to the serving loop (one slot per context and host thread)."""
         with api.Server(slots=args.serve_slots, hbm_budget_bytes=int(args.serve_budget_gb * 1e9)) as srv:
-            ids = [srv.submit(bp.model, bp.options.replace(max_iterations=args.batched_iters, precision=prec,
-                                                          solver_tolerance_initial=args.job_tol,
-                                                          solver_tolerance_final=args.job_tol,
-                                                          separate_load_cases=sep))
-                   for bp in probs]
+            ids = [srv.submit(bp.model, opts(bp, iters, prec)) for bp in probs]
             srv.wait()
             st = srv.stats()
-            hists[prec] = [[h.compliance for h in srv.result(j)["history"]] for j in ids]
-        span = st["last_finish_s"] - st["first_submit_s"]
-        out[prec] = {"simp_iter_s": st["simp_iterations"] / span, "wall_s": span, "completed": st["completed"],
-                     "p50_latency_s": st["p50_latency_s"], "p99_latency_s": st["p99_latency_s"]}
-    if "packed" in out and head in hists:
+            hist = [[h.compliance for h in srv.result(j)["history"]] for j in ids]
+        return st["last_finish_s"] - st["first_submit_s"], st["simp_iterations"], hist, st
+
+    extra = args.batched_steady_extra
+    hists = {}
+
+    def measured(name, run):
+        wall, n_it, hist, more = run(args.batched_iters)
+        rec = {"simp_iter_s": n_it / wall, "wall_s": wall, "simp_iterations": n_it}
+        if extra > 0:
+            wall2, n_it2, hist2, _ = run(args.batched_iters + extra)
+            rec["steady_simp_iter_s"] = (n_it2 - n_it) / (wall2 - wall) if wall2 > wall else None
+            rec["wall_s_longer_run"] = wall2
+            rec["histories_prefix_consistent"] = all(h2[:len(h)] == h for h, h2 in zip(hist, hist2))
+        hists[name] = hist
+        return rec, more
+
+    if args.batched_mode in ("packed", "both"):
+        rec, info = measured("packed", packed_run)
+        rec.update({"packs": len(info), "rhs_solved_packed": sum(x["rhs_solved_packed"] for x in info),
+                    "form": head, "note": "packs of problems whose solves share launches (mycel_simp_step_many), "
+                                          "the packs on concurrent contexts"})
+        out["packed"] = rec
+    if args.batched_mode in ("served", "both"):
+        rec, st = measured(head, lambda it: served_run(it, head))
+        rec.update({"completed": st["completed"], "p50_latency_s": st["p50_latency_s"],
+                    "p99_latency_s": st["p99_latency_s"], "slots": args.serve_slots})
+        out[head] = rec
+    if not args.batched_skip_fp64:
+        wall, n_it, hist, st = served_run(args.batched_iters, "fp64")
+        out["fp64"] = {"simp_iter_s": n_it / wall, "wall_s": wall, "completed": st["completed"],
+                       "p50_latency_s": st["p50_latency_s"], "p99_latency_s": st["p99_latency_s"]}
+        hists["fp64"] = hist
+    if "packed" in out and head in out:
         out["packed"]["same_histories_as_served"] = hists["packed"] == hists[head]
         out["packed"]["speedup_vs_served"] = out["packed"]["simp_iter_s"] / out[head]["simp_iter_s"]
+        if out["packed"].get("steady_simp_iter_s") and out[head].get("steady_simp_iter_s"):
+            out["packed"]["steady_speedup_vs_served"] = (out["packed"]["steady_simp_iter_s"] /
+                                                         out[head]["steady_simp_iter_s"])
     if "fp64" in out:
-        fast = out["packed"] if "packed" in out else out[head]
-        out[f"speedup_{head}_vs_fp64"] = fast["simp_iter_s"] / out["fp64"]["simp_iter_s"]
-        out[f"rel_compliance_err_{head}_vs_fp64"] = compare_histories(hists["packed" if "packed" in out else head],
-                                                                      hists["fp64"])
+        fast = "packed" if "packed" in out else head
+        out[f"speedup_{head}_vs_fp64"] = out[fast]["simp_iter_s"] / out["fp64"]["simp_iter_s"]
+        out[f"rel_compliance_err_{head}_vs_fp64"] = compare_histories(hists[fast], hists["fp64"])
     print(json.dumps(out), flush=True)
 
 
