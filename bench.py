@@ -109,7 +109,9 @@ def parse():
     ap.add_argument("--batched-steady-extra", type=int, default=4,
                     help="--batched: also run each form with this many more iterations per problem (steady "
                          "SIMP iter/s from the difference; 0: off)")
-    ap.add_argument("--batched-packs", type=int, default=4,
+    ap.add_argument("--batched-warmup", type=int, default=1,
+                    help="--batched: SIMP iterations per problem of an untimed warm-up batch (0: none)")
+    ap.add_argument("--batched-packs", type=int, default=1,
                     help="packs of the packed batched form (each on its own context and host thread)")
     ap.add_argument("--batched-mode", choices=("packed", "served", "both"), default="both",
                     help="batched timed form: packed launches of all problems (one context), the serving loop's "
@@ -524,6 +526,10 @@ def run_batched(args):
 
     extra = args.batched_steady_extra
     hists = {}
+    if args.batched_warmup > 0:  # one-time costs of the process (matvec autotune per grid, module loads) first
+        t0 = time.perf_counter()
+        served_run(args.batched_warmup, head)
+        out["warmup_s"] = time.perf_counter() - t0
 
     def measured(name, run):
         wall, n_it, hist, more = run(args.batched_iters)
