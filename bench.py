@@ -111,7 +111,7 @@ def parse():
                          "SIMP iter/s from the difference; 0: off)")
     ap.add_argument("--batched-warmup", type=int, default=1,
                     help="--batched: SIMP iterations per problem of an untimed warm-up batch (0: none)")
-    ap.add_argument("--batched-packs", type=int, default=1,
+    ap.add_argument("--batched-packs", type=int, default=4,
                     help="packs of the packed batched form (each on its own context and host thread)")
     ap.add_argument("--batched-mode", choices=("packed", "served", "both"), default="both",
                     help="batched timed form: packed launches of all problems (one context), the serving loop's "
