@@ -331,6 +331,16 @@ int32_t mycel_simp_converged(const mycel_simp_session* s);
    the call returns the first failure. cancel is polled between chunks of outer iterations. */
 int32_t mycel_simp_step_many(mycel_simp_session* const* sessions, int32_t n, mycel_iter_record* recs, int32_t* done,
                              int32_t* status, const volatile int32_t* cancel);
+/* Whole optimisations of n sessions (one context, one session per problem), each to its stop rule or
+   max_iterations, as mycel_simp_step in a loop would take them, to the bit; no counterpart in the reference
+   (same seams as mycel_simp_step_many). When every session is in MYCEL_PRECISION_MIXED_MG, the solves share
+   one packed plan for the whole run and each problem goes on to its next SIMP iteration as soon as its own
+   solve has ended, while the others still solve (no SIMP iteration waits for the slowest problem); otherwise
+   the sessions are stepped together by mycel_simp_step_many. Records go to history[i * cap ...], n_iters[i] of
+   them (only the first cap are kept); status[i] is each session's status (all three may be NULL); the call
+   returns the first failure. cancel is polled between chunks of outer iterations. */
+int32_t mycel_simp_run_many(mycel_simp_session* const* sessions, int32_t n, mycel_iter_record* history, int32_t cap,
+                            int32_t* n_iters, int32_t* status, const volatile int32_t* cancel);
 
 /* RunWriter snapshot frames (Persistence/RunWriter.cs:132-160 WriteSnapshotAsync, :199-245 the it_NNNNNN
    frame, :344-356 ComputeQuantizedChecksum) of the last completed iteration, without stalling the loop:

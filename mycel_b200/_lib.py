@@ -134,6 +134,7 @@ SIGNATURES = {
     "mycel_simp_step": (i32, [P, C.POINTER(IterRecord), C.POINTER(i32)]),
     "mycel_simp_step_many": (i32, [C.POINTER(P), i32, C.POINTER(IterRecord), C.POINTER(i32), C.POINTER(i32), P]),
     "mycel_simp_converged": (i32, [P]),
+    "mycel_simp_run_many": (i32, [C.POINTER(P), i32, C.POINTER(IterRecord), i32, C.POINTER(i32), C.POINTER(i32), P]),
     "mycel_simp_read": (i32, [P, P, P, P, P, P, C.POINTER(dbl)]),
     "mycel_simp_end": (i32, [P]),
     "mycel_simp_frame_begin": (i32, [P, C.POINTER(i32)]),

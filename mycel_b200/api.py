@@ -519,15 +519,7 @@ def _run_many(models: Sequence[FeModel], options: Sequence[OptimizerOptions], ct
     try:
         probs = [Problem(m, ctx) for m in models]
         sess = [SimpSession(p, o) for p, o in zip(probs, options)]
-        snaps = [[] for _ in sess]
-        while not all(s.done for s in sess):
-            if controller is not None and controller.is_stopped():
-                break
-            live = [k for k, s in enumerate(sess) if not s.done]
-            out = SimpSession.step_many([sess[k] for k in live], controller)
-            for k, r in zip(live, out):
-                if r is not None:
-                    snaps[k].append(r)
+        snaps = SimpSession.run_many(sess, controller)
         res = []
         for s, sn in zip(sess, snaps):
             d = s.read(u=True, densities=True)
@@ -556,6 +548,7 @@ class SimpSession:
         _check(L.load().mycel_simp_begin(problem.handle, C.byref(so), C.byref(h)), problem.ctx)
         self.handle = h.value
         self.done = False
+        self._max_iterations = max(1, int(options.max_iterations) - int(options.start_iteration) + 1)
         if not hasattr(problem, "_sessions"):
             problem._sessions = weakref.WeakSet()
         problem._sessions.add(self)
@@ -589,6 +582,28 @@ class SimpSession:
                 s.done = bool(done[k])
         _check(st, sessions[0].problem.ctx)
         return [None if was_done[k] else _snapshot(recs[k]) for k in range(n)]
+
+    @staticmethod
+    def run_many(sessions: Sequence["SimpSession"], controller: Optional[IterationController] = None, cap: int = 0):
+        """Every session to its end (mycel_simp_run_many): one context, one session per problem. In the mixed
+        multigrid form the solves share one packed plan and each problem goes on to its next SIMP iteration as
+        soon as its own solve ends. Returns each session's snapshots (records only)."""
+        n = len(sessions)
+        if n == 0:
+            return []
+        cap = cap or max(1, max(s._max_iterations for s in sessions))
+        hs = (C.c_void_p * n)(*[s.handle for s in sessions])
+        hist = (L.IterRecord * (n * cap))()
+        nit = (C.c_int32 * n)()
+        stat = (C.c_int32 * n)()
+        cancel = controller._cancel if controller else None
+        st = L.load().mycel_simp_run_many(hs, n, hist, cap, nit, stat,
+                                          C.addressof(cancel) if cancel is not None else None)
+        out = [[_snapshot(hist[k * cap + q]) for q in range(min(nit[k], cap))] for k in range(n)]
+        for s in sessions:
+            s.done = True
+        _check(st, sessions[0].problem.ctx)
+        return out
 
     @property
     def converged(self) -> bool:

@@ -47,7 +47,7 @@ struct MixState {
   double rho0, alpha, beta, rn, pap;
   double flush_factor;  // a replacement when the recursive residual has dropped by this factor
   unsigned int counter;
-  unsigned int pad2;
+  int pmode;  // packed runs: the outer step a right-hand side takes next (0 after a matvec, 1 restart, 2 start)
 };
 
 constexpr int kT = 256;
@@ -2531,6 +2531,7 @@ __device__ __forceinline__ void mg_exit_tail(double b1, double b2, double b3, Mi
   const double srr = warp_sum_parts(part + 2 * nb, nb);
   if (threadIdx.x != 0) return;
   st->counter = 0;
+  st->pmode = 0;  // the next step follows a matvec
   if (!(szr > 0.0) || !isfinite(szr)) {  // (z, r) > 0 for an SPD preconditioner and r != 0
     st->status = MIX_BREAKDOWN;
     return;
@@ -4210,6 +4211,7 @@ struct PkList {             // the work list of one packed launch
   const int* enc;           // [n] states of the entry
   unsigned* items;          // [total] listed work items
   unsigned* count;          // items listed
+  int after_matvec;         // list only right-hand sides whose next step follows a matvec (pmode 0)
 };
 
 // one CTA per list: the running entries' items, in entry order
@@ -4219,7 +4221,8 @@ __global__ void __launch_bounds__(1024) k_pk_compact(const PkList* __restrict__ 
   __shared__ unsigned char run[kPkMaxUnits];
   for (int e = threadIdx.x; e < L.n; e += blockDim.x) {
     bool r = false;
-    for (int k = 0; k < L.enc[e]; ++k) r = r || L.est[e][k].status == MIX_RUNNING;
+    for (int k = 0; k < L.enc[e]; ++k)
+      r = r || (L.est[e][k].status == MIX_RUNNING && (!L.after_matvec || L.est[e][k].pmode == 0));
     run[e] = r ? 1 : 0;
   }
   __syncthreads();
@@ -4292,7 +4295,8 @@ __global__ void __launch_bounds__(kT) k_mg_enter32_pk(const PkVec* __restrict__ 
     __syncthreads();
     const unsigned code = items[w];
     const PkVec& a = tab[code >> kPkLbBits];
-    mg_enter32_body(a.n, a.x, a.r, a.p, a.q, a.invd, a.z, a.om, a.st, a.part, mode, code & kPkLbMask, a.nb);
+    const int md = mode >= 0 ? mode : *(const volatile int*)&a.st->pmode;
+    mg_enter32_body(a.n, a.x, a.r, a.p, a.q, a.invd, a.z, a.om, a.st, a.part, md, code & kPkLbMask, a.nb);
   }
 }
 
@@ -4303,7 +4307,8 @@ __global__ void __launch_bounds__(kT) k_mg_exit32_pk(const PkVec* __restrict__ t
     __syncthreads();
     const unsigned code = items[w];
     const PkVec& a = tab[code >> kPkLbBits];
-    mg_exit32_body(a.n, a.r, a.t, a.z, a.invd, a.q, a.om, a.st, a.part, mode, code & kPkLbMask, a.nb);
+    const int md = mode >= 0 ? mode : *(const volatile int*)&a.st->pmode;
+    mg_exit32_body(a.n, a.r, a.t, a.z, a.invd, a.q, a.om, a.st, a.part, md, code & kPkLbMask, a.nb);
   }
 }
 
@@ -4424,12 +4429,16 @@ struct PkOps {
   int n;
   signed char op[kPkMaxUnits];
 };
+constexpr int kPkRestart = 101;  // state op: running again, next step a restart (after a replacement)
 __global__ void k_pk_set(MixState* const* __restrict__ sts, const __grid_constant__ PkOps o) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= o.n || o.op[i] < 0) return;
   MixState* st = sts[i];
   if (o.op[i] == kPkStall) {
     if (st->status == MIX_RUNNING) st->status = MIX_FLUSH;
+  } else if (o.op[i] == kPkRestart) {
+    st->status = MIX_RUNNING;
+    st->pmode = 1;
   } else {
     st->status = o.op[i];
   }
@@ -4441,13 +4450,13 @@ __global__ void k_pk_gather(MixState* const* __restrict__ sts, int n, MixState* 
 struct PkInit {
   double target;
   int max_iter;
-  int active;  // 0: the right-hand side takes no part (its state is set done)
+  int op;  // 0: left as it is, 1: a new solve (k_mix_init, next step the start), 2: set done
 };
-// k_mix_init of every active right-hand side (flush factor of the FP32 multigrid form), DONE for the others
+// k_mix_init of the right-hand sides that start a solve (flush factor of the FP32 multigrid form)
 __global__ void k_pk_init(MixState* const* __restrict__ sts, const PkInit* __restrict__ in, int n, double flush) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  if (!in[i].active) {
+  if (i >= n || in[i].op == 0) return;
+  if (in[i].op == 2) {
     sts[i]->status = MIX_DONE;
     return;
   }
@@ -4457,6 +4466,7 @@ __global__ void k_pk_init(MixState* const* __restrict__ sts, const PkInit* __res
   s.max_iter = in[i].max_iter;
   s.first = 1;
   s.flush_factor = flush;
+  s.pmode = 2;
   *sts[i] = s;
 }
 
@@ -5030,7 +5040,7 @@ static int32_t pk_build(mycel_ctx* c, PackWork* w, std::vector<PkUnit>& units, c
     for (size_t k = 0; k < g.size(); ++k) {
       const PkLaunch& L = *g[k];
       PkList h{L.n, (const unsigned*)(base + L.starts), (MixState* const*)(base + L.est), (const int*)(base + L.enc),
-               (unsigned*)(base + L.items), (unsigned*)(base + L.count)};
+               (unsigned*)(base + L.items), (unsigned*)(base + L.count), L.kind == PK_MV1 ? 1 : 0};
       std::memcpy(B.host.data() + off + k * sizeof(PkList), &h, sizeof h);
     }
   };
@@ -5257,7 +5267,7 @@ int32_t mg_solve_packed(mycel_ctx* c, int njobs, PackJob* jobs, const volatile i
     PackJob& J = jobs[u.job];
     mycel_pcg_result& r = J.res[u.k < 0 ? 0 : u.k];
     bnorm[i] = h_bn[i];
-    h_init[i] = PkInit{0.0, 0, 0};
+    h_init[i] = PkInit{0.0, 0, 2};
     if (bnorm[i] <= 1e-30) {
       MYCEL_CUDA(c, cudaMemsetAsync(u.u, 0, sizeof(double) * u.p->g.nd, s));
       r.converged = 1;
@@ -5410,6 +5420,367 @@ int32_t mg_solve_packed(mycel_ctx* c, int njobs, PackJob* jobs, const volatile i
   }
   return MYCEL_OK;
 }
+
+// ---------------------------------------------------------------------------------------------------------
+// Asynchronous packed runs (mycel_simp_run_many): the right-hand sides of several problems stay in one packed
+// plan for a whole optimisation, and each problem's solves start and end on their own. Every chunk of outer
+// iterations advances the right-hand sides that are running; one that stops (replacement point, breakdown,
+// iteration limit) is refined in FP64 right after that chunk and restarts with the next one (its restart step
+// then runs inside the chunk: the step mode is per right-hand side), so no right-hand side waits for another
+// and a problem whose solve has ended goes on to its next SIMP iteration while the others still solve.
+// A (re)started right-hand side takes its first matvec in the chunk's second slot (its restart step fills the
+// first), so after m outer iterations its latest direction is in p1 when m is odd: it is copied to p0, where
+// the next restart's first matvec reads it. Per right-hand side the arithmetic is that of its solve alone.
+// ---------------------------------------------------------------------------------------------------------
+struct PackRun {
+  mycel_ctx* c = nullptr;
+  std::vector<PkUnit> units;
+  std::vector<mycel_problem*> jp;
+  std::vector<int> ju0, jnc;
+  std::vector<std::chrono::steady_clock::time_point> jt0;
+  // per right-hand side: 0 idle, 1 start issued, 2 running, 3 stopped (refinement issued), 4 converged,
+  // 5 finished alone, 6 done at the start (zero right-hand side or converged already)
+  std::vector<char> state, stalled, stall_pending;
+  std::vector<int> iters, flushes, resume, stop_status, max_iter;
+  std::vector<int64_t> cycle_limit;
+  std::vector<double> bnorm, rel, tol;
+  std::vector<mycel_pcg_result> res;
+  double *h_bn = nullptr, *h_rn2 = nullptr;
+  MixState* h_st = nullptr;
+  PkInit* h_init = nullptr;
+};
+
+void pkr_close(PackRun* r) { delete r; }
+
+int32_t pkr_open(mycel_ctx* c, const std::vector<PackRunJob>& jobs, PackRun** out) {
+  *out = nullptr;
+  cudaStream_t s = c->stream;
+  int32_t st = MYCEL_OK;
+  static std::once_flag smem_once;
+  static cudaError_t smem_err = cudaSuccess;
+  std::call_once(smem_once, [] {
+    cudaError_t a = cudaFuncSetAttribute(k_mv32f_pk<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fac_smem_bytes(0));
+    cudaError_t b = cudaFuncSetAttribute(k_mv32f_pk<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fac_smem_bytes(1));
+    smem_err = a != cudaSuccess ? a : b;
+  });
+  if (smem_err != cudaSuccess)
+    return set_error(c, MYCEL_E_DEVICE, std::string("packed matvec shared memory: ") + cudaGetErrorString(smem_err));
+  PackRun* r = new PackRun();
+  r->c = c;
+  struct Del { PackRun** r; ~Del() { if (*r) delete *r; } } del{&r};
+  for (size_t j = 0; j < jobs.size(); ++j) {
+    mycel_problem* p = jobs[j].p;
+    const int nc = jobs[j].ncase;
+    if (p->ctx != c) return set_error(c, MYCEL_E_ARG, "packed run: every problem must belong to the context");
+    for (size_t i = 0; i < j; ++i)
+      if (jobs[i].p == p) return set_error(c, MYCEL_E_ARG, "packed run: one job per problem");
+    if (p->n_active_fixed < 6 || nc < 1 || nc > kMgMaxCases)
+      return set_error(c, MYCEL_E_ARG, "packed run: a problem the packed form cannot take");
+    if ((st = ensure_pcg_workspace(p)) || (st = ensure_mixed(p)) || (st = ensure_f64f(p))) return st;
+    if (nc > 1 && (st = ensure_cases(p))) return st;
+    bool avail = false;
+    if ((st = resolve_mv32(p)) || (st = mg_ensure(p, &avail))) return st;
+    if (!avail || p->mg->prefers_f64 || p->mg->sweeps != 1 || p->mv32 != MYCEL_MV32_FACTORED ||
+        (nc > 1 && nc > p->mg->ncap) || (int)r->units.size() + nc > kPkMaxUnits)
+      return set_error(c, MYCEL_E_ARG, "packed run: a problem the packed form cannot take");
+    if (nc > 1 && (st = mg_ensure_cases(p, nc))) return st;
+    MgHier* mg = p->mg;
+    const int64_t nd = p->g.nd;
+    r->jp.push_back(p);
+    r->ju0.push_back((int)r->units.size());
+    r->jnc.push_back(nc);
+    for (int k = 0; k < nc; ++k) {
+      PkUnit u{};
+      u.p = p;
+      u.job = (int)j;
+      if (nc == 1) {
+        u.k = -1;
+        u.x = p->f_x; u.r = p->f_r; u.z = p->f_z; u.p0 = p->f_p0; u.p1 = p->f_p1; u.ap = p->f_ap; u.t = mg->f_t;
+        u.tz = &p->f_tmap[1];
+        u.tp0 = &p->f_tmap[2];
+        u.tp1 = &p->f_tmap[3];
+        u.st = mix_state(p);
+        u.b = p->d_b;
+        u.bnz = p->d_bnz;
+        u.nbnz = p->n_bnz;
+        u.u = jobs[j].d_u;
+      } else {
+        u.k = k;
+        u.x = cwv(mg, k, 0); u.r = cwv(mg, k, 1); u.z = cwv(mg, k, 2); u.p0 = cwv(mg, k, 3); u.p1 = cwv(mg, k, 4);
+        u.ap = cwv(mg, k, 5); u.t = cwv(mg, k, 6);
+        u.tz = &mg->cw.tmap[k][1];
+        u.tp0 = &mg->cw.tmap[k][2];
+        u.tp1 = &mg->cw.tmap[k][3];
+        u.st = mg->cw.st + k;
+        u.b = p->d_case_b + (int64_t)k * nd;
+        u.bnz = p->d_case_nz + p->case_nz_off[2 * k + 1];
+        u.nbnz = p->case_nz_cnt[2 * k + 1];
+        u.u = jobs[j].d_u + (int64_t)k * nd;
+      }
+      r->units.push_back(u);
+    }
+  }
+  const int nu = (int)r->units.size();
+  if (nu == 0) return set_error(c, MYCEL_E_ARG, "packed run: no right-hand side");
+  r->jt0.resize(jobs.size());
+  r->state.assign(nu, 0);
+  r->stalled.assign(nu, 0);
+  r->stall_pending.assign(nu, 0);
+  r->iters.assign(nu, 0);
+  r->flushes.assign(nu, 0);
+  r->resume.assign(nu, 0);
+  r->stop_status.assign(nu, MIX_DONE);
+  r->max_iter.assign(nu, 0);
+  r->cycle_limit.assign(nu, 300);
+  r->bnorm.assign(nu, 0.0);
+  r->rel.assign(nu, 0.0);
+  r->tol.assign(nu, 0.0);
+  r->res.assign(nu, mycel_pcg_result{});
+  if (!c->pack) c->pack = new PackWork();
+  PackWork* w = (PackWork*)c->pack;
+  const size_t pin_need = (size_t)nu * (2 * sizeof(MixState) + 2 * sizeof(double) + sizeof(PkInit)) + 4096;
+  if (w->pinned_bytes < pin_need) {
+    if (w->pinned) cudaFreeHost(w->pinned);
+    w->pinned = nullptr;
+    w->pinned_bytes = 0;
+    MYCEL_CUDA(c, cudaMallocHost(&w->pinned, pin_need));
+    w->pinned_bytes = pin_need;
+  }
+  r->h_st = (MixState*)w->pinned;
+  r->h_bn = (double*)(r->h_st + 2 * nu);
+  r->h_rn2 = r->h_bn + nu;
+  r->h_init = (PkInit*)(r->h_rn2 + nu);
+  std::vector<uint64_t> key;
+  for (const PkUnit& u : r->units) {
+    key.push_back(u.p->serial);
+    key.push_back((uint64_t)(int64_t)u.k);
+  }
+  if (w->plan.key != key || !w->plan.chunk) {
+    if ((st = pk_build(c, w, r->units, key))) return st;
+  } else {
+    for (int i = 0; i < nu; ++i) r->units[i].part = (double*)w->part_bufs[i];
+  }
+  for (int i = 0; i < nu; ++i) r->h_init[i] = PkInit{0.0, 0, 2};  // nothing runs until its start
+  MYCEL_CUDA(c, cudaMemcpyAsync(w->plan.d_init, r->h_init, sizeof(PkInit) * nu, cudaMemcpyHostToDevice, s));
+  k_pk_init<<<(nu + 127) / 128, 128, 0, s>>>(w->plan.d_sts, w->plan.d_init, nu, 1e-3);
+  c->launches++;
+  MYCEL_CUDA(c, cudaStreamSynchronize(s));
+  *out = r;
+  r = nullptr;
+  return MYCEL_OK;
+}
+
+static InnerForm pkr_form(const PkUnit& u) {
+  InnerForm F = inner_form_mg(u.p, false);
+  F.x = u.x; F.r = u.r; F.z = u.z; F.p0 = u.p0; F.p1 = u.p1; F.ap = u.ap;
+  return F;
+}
+
+// the start of job j's next solve on the context stream: its coarse operators (when E has changed), then per
+// right-hand side the projection of u, ||P b|| and the true residual, copied to pinned memory
+int32_t pkr_begin(PackRun* r, int j, double tol, int max_iter) {
+  mycel_ctx* c = r->c;
+  cudaStream_t s = c->stream;
+  mycel_problem* p = r->jp[j];
+  int32_t st = MYCEL_OK;
+  r->jt0[j] = std::chrono::steady_clock::now();
+  MYCEL_CUDA(c, cudaMemsetAsync(p->d_err, 0, sizeof(int), s));
+  if (p->mg->setup_version != p->e_version) {
+    mg_setup(p);
+    p->mg->setup_version = p->e_version;
+  }
+  double* sb = p->d_b;
+  int32_t* snz = p->d_bnz;
+  const int32_t sn = p->n_bnz;
+  for (int i = r->ju0[j]; i < r->ju0[j] + r->jnc[j]; ++i) {
+    const PkUnit& u = r->units[i];
+    p->d_b = const_cast<double*>(u.b);
+    p->d_bnz = const_cast<int32_t*>(u.bnz);
+    p->n_bnz = u.nbnz;
+    cudaMemsetAsync(p->d_state, 0, sizeof(PcgState), s);
+    launch_project_x(p, u.u, &p->d_state->nonzero_x);
+    launch_pcg_bnorm(p);
+    st = cudaMemcpyAsync(r->h_bn + i, &p->d_state->bnorm, sizeof(double), cudaMemcpyDeviceToHost, s) == cudaSuccess
+             ? true_residual_issue(p, pkr_form(u), u.b, u.u, r->h_rn2 + i)
+             : set_error(c, MYCEL_E_DEVICE, "packed run: read-back of ||P b||");
+    r->tol[i] = tol;
+    r->max_iter[i] = max_iter;
+    r->state[i] = 1;
+    c->packed_rhs++;
+    r->res[i] = mycel_pcg_result{};
+    if (st) break;
+  }
+  p->d_b = sb;
+  p->d_bnz = snz;
+  p->n_bnz = sn;
+  return st;
+}
+
+// after a synchronisation: the started right-hand sides run, or are done at once
+int32_t pkr_after_begin(PackRun* r) {
+  mycel_ctx* c = r->c;
+  cudaStream_t s = c->stream;
+  const int nu = (int)r->units.size();
+  bool any = false;
+  for (int i = 0; i < nu; ++i) {
+    r->h_init[i] = PkInit{0.0, 0, 0};
+    if (r->state[i] != 1) continue;
+    const PkUnit& u = r->units[i];
+    mycel_pcg_result& res = r->res[i];
+    r->bnorm[i] = r->h_bn[i];
+    r->iters[i] = r->flushes[i] = r->resume[i] = 0;
+    r->cycle_limit[i] = 300;
+    r->stalled[i] = r->stall_pending[i] = 0;
+    if (r->bnorm[i] <= 1e-30) {
+      MYCEL_CUDA(c, cudaMemsetAsync(u.u, 0, sizeof(double) * u.p->g.nd, s));
+      res.converged = 1;
+      std::snprintf(res.message, sizeof res.message, "RHS is zero. Solution is zero.");
+      r->state[i] = 6;
+      continue;
+    }
+    r->rel[i] = std::sqrt(r->h_rn2[i]) / r->bnorm[i];
+    if (r->rel[i] <= r->tol[i]) {
+      res.converged = 1;
+      res.final_residual = r->rel[i];
+      std::snprintf(res.message, sizeof res.message, "Initial guess already converged.");
+      r->state[i] = 6;
+      continue;
+    }
+    MYCEL_CUDA(c, cudaMemsetAsync(u.x, 0, sizeof(float) * (size_t)u.p->g.n32, s));
+    r->h_init[i] = PkInit{0.5 * r->tol[i] * r->bnorm[i], r->max_iter[i], 1};
+    r->state[i] = 2;
+    any = true;
+  }
+  if (!any) return MYCEL_OK;
+  PackPlan& P = ((PackWork*)c->pack)->plan;
+  MYCEL_CUDA(c, cudaMemcpyAsync(P.d_init, r->h_init, sizeof(PkInit) * nu, cudaMemcpyHostToDevice, s));
+  k_pk_init<<<(nu + 127) / 128, 128, 0, s>>>(P.d_sts, P.d_init, nu, 1e-3);
+  c->launches++;
+  MYCEL_CUDA(c, cudaGetLastError());
+  return MYCEL_OK;
+}
+
+bool pkr_running(const PackRun* r) {
+  for (char v : r->state)
+    if (v == 2) return true;
+  return false;
+}
+
+// One chunk of every running right-hand side (synchronised); the stopped ones are refined and restarted (or
+// end); the jobs whose solves have ended are appended to ended (their results: pkr_result).
+int32_t pkr_advance(PackRun* r, const volatile int32_t* cancel, std::vector<int>* ended) {
+  mycel_ctx* c = r->c;
+  cudaStream_t s = c->stream;
+  const int nu = (int)r->units.size();
+  PackWork* w = (PackWork*)c->pack;
+  PackPlan& P = w->plan;
+  int32_t st = MYCEL_OK;
+  if (cancel && *cancel) return set_error(c, MYCEL_E_CANCELLED, "The operation was canceled.");
+  std::vector<signed char> op(nu, -1);
+  bool any_op = false, any_stop = false;
+  if (pkr_running(r)) {
+    MYCEL_CUDA(c, cudaGraphLaunch(P.chunk, s));
+    c->launches += P.per_chunk;
+    MYCEL_CUDA(c, cudaMemcpyAsync(r->h_st, P.d_states, sizeof(MixState) * nu, cudaMemcpyDeviceToHost, s));
+    MYCEL_CUDA(c, cudaStreamSynchronize(s));
+    for (int i = 0; i < nu; ++i) {
+      if (r->state[i] != 2) continue;
+      const MixState& m = r->h_st[i];
+      bool stop = m.status != MIX_RUNNING && m.pmode == 0;  // a restart set after this chunk's copy reads pmode 1
+      if (!stop) {
+        if (r->stall_pending[i]) {  // the chunk after the one that showed the stall ran: stop it
+          r->stalled[i] = 1;
+          op[i] = kPkStall;
+          any_op = stop = true;
+        } else if (m.iter - r->resume[i] > r->cycle_limit[i] || (int64_t)m.iter > (int64_t)r->max_iter[i] + 4096) {
+          r->stall_pending[i] = 1;
+        }
+      }
+      if (!stop) continue;
+      r->iters[i] = m.iter;
+      r->stop_status[i] = r->stalled[i] ? MIX_FLUSH : m.status;
+      r->state[i] = 3;
+      any_stop = true;
+    }
+    if (any_op && (st = pk_set(c, P, op))) return st;
+    for (int i = 0; i < nu; ++i) {
+      if (r->state[i] != 3) continue;
+      const PkUnit& u = r->units[i];
+      const int mm = r->iters[i] - r->resume[i];
+      if (mm > 0 && (mm & 1))
+        MYCEL_CUDA(c, cudaMemcpyAsync(u.p0, u.p1, sizeof(float) * (size_t)u.p->g.n32, cudaMemcpyDeviceToDevice, s));
+      k_flush_u<float><<<stream_blocks(u.p), kT, 0, s>>>(u.p->g, u.u, u.x);
+      c->launches++;
+      ++r->flushes[i];
+      if ((st = true_residual_issue(u.p, pkr_form(u), u.b, u.u, r->h_rn2 + i))) return st;
+    }
+  }
+  if (any_stop) {
+    MYCEL_CUDA(c, cudaStreamSynchronize(s));
+    std::fill(op.begin(), op.end(), (signed char)-1);
+    for (int i = 0; i < nu; ++i) {
+      if (r->state[i] != 3) continue;
+      r->rel[i] = std::sqrt(r->h_rn2[i]) / r->bnorm[i];
+      r->cycle_limit[i] = std::max<int64_t>(300, 3 * (int64_t)r->iters[i]);
+      if (r->rel[i] <= r->tol[i]) {
+        op[i] = MIX_DONE;
+        r->state[i] = 4;
+      } else if (r->stalled[i] || r->stop_status[i] != MIX_FLUSH || r->iters[i] >= r->max_iter[i]) {
+        op[i] = MIX_DONE;
+        r->state[i] = 5;  // finished alone below
+      } else {
+        op[i] = kPkRestart;
+        r->resume[i] = r->iters[i];
+        r->stall_pending[i] = 0;
+        r->state[i] = 2;
+      }
+    }
+    if ((st = pk_set(c, P, op))) return st;
+  }
+  for (size_t j = 0; j < r->jp.size(); ++j) {
+    bool live = false, over = true;
+    for (int i = r->ju0[j]; i < r->ju0[j] + r->jnc[j]; ++i) {
+      live = live || r->state[i] != 0;
+      over = over && (r->state[i] >= 4);
+    }
+    if (!live || !over) continue;
+    const double ms =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - r->jt0[j]).count();
+    for (int i = r->ju0[j]; i < r->ju0[j] + r->jnc[j]; ++i) {
+      const PkUnit& u = r->units[i];
+      mycel_pcg_result& res = r->res[i];
+      if (r->state[i] == 6) {
+        res.elapsed_ms = ms;
+      } else if (r->state[i] == 5) {  // from the refined u, as the solve alone goes on after its FP32 iteration
+        if (r->stalled[i]) u.p->mg->prefers_f64 = true;
+        const int mx = r->max_iter[i];
+        const int budget = (u.k < 0 && r->iters[i] == 0) ? mx : std::max(mx - r->iters[i], mx / 2);
+        if ((st = refined_solve_entry(u.p, u.b, u.bnz, u.nbnz, u.u, r->tol[i], budget, cancel, MYCEL_PRECISION_FP64_MG,
+                                      &res)))
+          return st;
+        res.fallback_iterations = res.iterations;
+        res.inner_iterations = r->iters[i];
+        res.iterations += r->iters[i];
+        res.refinement_steps += r->flushes[i];
+        std::vector<signed char> done_op(nu, -1);  // the solve alone used the same state: no chunk may take it
+        done_op[i] = MIX_DONE;
+        if ((st = pk_set(c, P, done_op))) return st;
+      } else {
+        res.inner_iterations = r->iters[i];
+        res.iterations = r->iters[i];
+        res.refinement_steps = r->flushes[i];
+        res.final_residual = r->rel[i];
+        res.converged = 1;
+        res.elapsed_ms = ms;
+      }
+      r->state[i] = 0;
+    }
+    ended->push_back((int)j);
+  }
+  return MYCEL_OK;
+}
+
+const mycel_pcg_result* pkr_results(const PackRun* r, int j) { return r->res.data() + r->ju0[j]; }
 
 int32_t mixed_solve_entry(mycel_problem* p, const double* d_b, const int32_t* d_nz, int32_t n_nz, double* d_u,
                           double tol, int max_iter, const volatile int32_t* cancel, mycel_pcg_result* res) {

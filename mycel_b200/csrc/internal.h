@@ -334,6 +334,25 @@ struct PackJob {
 // problem's solve alone in the mixed multigrid form.
 int32_t mg_solve_packed(mycel_ctx* c, int njobs, PackJob* jobs, const volatile int32_t* cancel);
 void pack_release(mycel_ctx* c);
+// Asynchronous packed run (mycel_simp_run_many): the right-hand sides of the jobs share one packed plan for a
+// whole optimisation and each job's solves start and end on their own. pkr_open fails with MYCEL_E_ARG when a
+// job cannot be packed. pkr_begin issues the start of job j's next solve; after the caller synchronises the
+// context stream, pkr_after_begin lets the started right-hand sides run; pkr_advance runs one chunk of outer
+// iterations (synchronised), refines and restarts what stopped, and appends the jobs whose solves ended;
+// pkr_results gives an ended job's results (ncase of them).
+struct PackRunJob {
+  mycel_problem* p;
+  int ncase;
+  double* d_u;
+};
+struct PackRun;
+int32_t pkr_open(mycel_ctx* c, const std::vector<PackRunJob>& jobs, PackRun** out);
+void pkr_close(PackRun* r);
+int32_t pkr_begin(PackRun* r, int j, double tol, int max_iter);
+int32_t pkr_after_begin(PackRun* r);
+bool pkr_running(const PackRun* r);
+int32_t pkr_advance(PackRun* r, const volatile int32_t* cancel, std::vector<int>* ended);
+const mycel_pcg_result* pkr_results(const PackRun* r, int j);
 // Fan-out of independent per-problem work of a batch step over side streams: fan_begin makes them wait for
 // the context stream's work so far; fan_use(c, k) issues the following work of the context on side stream k
 // (the context's stream and side stream are swapped, so every launch helper follows); fan_end returns to the

@@ -752,6 +752,132 @@ extern "C" int32_t mycel_simp_run(mycel_problem* p, const mycel_simp_options* op
   return err;
 }
 
+// Whole optimisations of n sessions (one context, one session per problem) to their ends: every session runs
+// until its stop rule fires or max_iterations is reached, as with mycel_simp_step in a loop, and its records
+// go to history[i * cap ...] (n_iters[i] of them, at most cap). When every session is in the mixed multigrid
+// form (load cases summed, or kept apart and solved together) their solves share one packed plan for the
+// whole run and each problem goes on to its next SIMP iteration as soon as its own solve ends (the others may
+// still be solving); otherwise the sessions are stepped together by mycel_simp_step_many. Each session's
+// iterates are those of its run alone.
+extern "C" int32_t mycel_simp_run_many(mycel_simp_session* const* ss, int32_t n, mycel_iter_record* history,
+                                       int32_t cap, int32_t* n_iters, int32_t* status,
+                                       const volatile int32_t* cancel) {
+  if (!ss || n < 1) return set_error(nullptr, MYCEL_E_ARG, "NULL sessions or count below 1");
+  for (int i = 0; i < n; ++i)
+    if (!ss[i]) return set_error(nullptr, MYCEL_E_ARG, "NULL session");
+  mycel_ctx* c = ss[0]->p->ctx;
+  for (int i = 0; i < n; ++i) {
+    if (ss[i]->p->ctx != c) return set_error(c, MYCEL_E_ARG, "the sessions of a batch run share one context");
+    for (int j = 0; j < i; ++j)
+      if (ss[j]->p == ss[i]->p) return set_error(c, MYCEL_E_ARG, "each session of a batch run has its own problem");
+  }
+  cudaSetDevice(c->device);
+  std::vector<int32_t> st(n, MYCEL_OK);
+  auto record = [&](int i, const mycel_iter_record& r) {
+    if (n_iters) {
+      if (history && n_iters[i] < cap) history[(int64_t)i * cap + n_iters[i]] = r;
+      n_iters[i]++;
+    }
+  };
+  if (n_iters)
+    for (int i = 0; i < n; ++i) n_iters[i] = 0;
+  bool packable = true;
+  std::vector<PackRunJob> jobs;
+  for (int i = 0; i < n; ++i) {
+    mycel_simp_session* s = ss[i];
+    packable = packable && s->o.precision == MYCEL_PRECISION_MIXED_MG && (s->ncase == 1 || cases_solved_together(s));
+    jobs.push_back(PackRunJob{s->p, s->ncase, s->ncase == 1 ? s->d_u : s->d_uc});
+  }
+  PackRun* run = nullptr;
+  if (packable && pkr_open(c, jobs, &run) != MYCEL_OK) run = nullptr;
+  if (!run) {  // sessions stepped together, each SIMP iteration a barrier
+    std::vector<mycel_iter_record> recs(n);
+    std::vector<int32_t> dn(n), sst(n);
+    for (;;) {
+      std::vector<mycel_simp_session*> live;
+      std::vector<int> idx;
+      for (int i = 0; i < n; ++i)
+        if (!ss[i]->done && !st[i]) live.push_back(ss[i]), idx.push_back(i);
+      if (live.empty()) break;
+      if (cancel && *cancel) break;
+      mycel_simp_step_many(live.data(), (int)live.size(), recs.data(), dn.data(), sst.data(), cancel);
+      for (size_t q = 0; q < live.size(); ++q) {
+        if (sst[q]) st[idx[q]] = sst[q];
+        else record(idx[q], recs[q]);
+      }
+    }
+  } else {
+    std::vector<SimpPre> pre(n);
+    std::vector<char> live(n, 0);
+    auto begin = [&](int i) -> int32_t {
+      simp_pre(ss[i], &pre[i]);
+      return pkr_begin(run, i, pre[i].tol, ss[i]->o.solver_max_iterations);
+    };
+    for (int i = 0; i < n; ++i)
+      if (!ss[i]->done) {
+        live[i] = 1;
+        if ((st[i] = begin(i))) live[i] = 0;
+      }
+    int32_t rc = cudaStreamSynchronize(c->stream) == cudaSuccess ? pkr_after_begin(run)
+                                                                  : set_error(c, MYCEL_E_DEVICE, "packed run start");
+    std::vector<int> ended;
+    while (!rc) {
+      bool any = false;
+      for (int i = 0; i < n; ++i) any = any || live[i];
+      if (!any) break;
+      ended.clear();
+      if ((rc = pkr_advance(run, cancel, &ended))) break;
+      if (ended.empty()) {
+        if (!pkr_running(run)) rc = set_error(c, MYCEL_E_TIMEOUT, "packed run: no solve running");
+        continue;
+      }
+      std::vector<mycel_pcg_result> pr(ended.size());
+      for (size_t q = 0; q < ended.size(); ++q) {
+        const int i = ended[q];
+        fold_cases(pkr_results(run, i), ss[i]->ncase, &pr[q]);
+        if ((st[i] = simp_post_issue(ss[i], pre[i], pr[q]))) live[i] = 0;
+      }
+      if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
+        rc = set_error(c, MYCEL_E_DEVICE, "packed run: SIMP update");
+        break;
+      }
+      bool began = false;
+      for (size_t q = 0; q < ended.size(); ++q) {
+        const int i = ended[q];
+        if (!live[i]) continue;
+        mycel_iter_record r{};
+        int32_t d = 0;
+        if ((st[i] = simp_post_finish(ss[i], pre[i], pr[q], &r, &d))) {
+          live[i] = 0;
+          continue;
+        }
+        record(i, r);
+        if (d || (cancel && *cancel)) {
+          live[i] = 0;
+          continue;
+        }
+        if ((st[i] = begin(i))) live[i] = 0;
+        else began = true;
+      }
+      if (began) {
+        rc = cudaStreamSynchronize(c->stream) == cudaSuccess ? pkr_after_begin(run)
+                                                             : set_error(c, MYCEL_E_DEVICE, "packed run start");
+      }
+    }
+    cudaStreamSynchronize(c->stream);
+    pkr_close(run);
+    if (rc && rc != MYCEL_E_CANCELLED)
+      for (int i = 0; i < n; ++i)
+        if (live[i] && !st[i]) st[i] = rc;
+  }
+  int32_t first = MYCEL_OK;
+  for (int i = 0; i < n; ++i) {
+    if (status) status[i] = st[i];
+    if (!first && st[i]) first = st[i];
+  }
+  return first;
+}
+
 namespace mycel {
 bool simp_session_converged(const mycel_simp_session* s) { return s && s->converged; }
 }  // namespace mycel

@@ -148,3 +148,24 @@ def test_batch_arguments(ctx):
         s.close()
         p.close()
         other.close()
+
+
+def test_run_many_each_problem_as_alone(ctx):
+    """Whole runs side by side (mycel_simp_run_many): each problem goes on to its next SIMP iteration as soon as
+    its own solve ends; runs of different lengths end at different times. Each equals its run alone."""
+    jobs = [(m, o.replace(max_iterations=2 + k % 3)) for k, (m, o) in enumerate(_jobs())]
+    alone = [_alone(ctx, m, o, o.max_iterations) for m, o in jobs]
+    made = [_session(ctx, m, o) for m, o in jobs]
+    try:
+        before = ctx.packed_count
+        out = api.SimpSession.run_many([s for _, s in made])
+        reads = [s.read() for _, s in made]
+        rhs = sum((len(m.loads) if o.separate_load_cases and len(m.loads) > 1 else 1) * o.max_iterations
+                  for m, o in jobs)
+        assert ctx.packed_count - before == rhs, "every solve ran in the packed plan"
+    finally:
+        for p, s in made:
+            s.close()
+            p.close()
+    for k, (ra, da) in enumerate(alone):
+        _same(ra, da, out[k], reads[k])
