@@ -111,6 +111,9 @@ def parse():
                          "SIMP iter/s from the difference; 0: off)")
     ap.add_argument("--batched-warmup", type=int, default=1,
                     help="--batched: SIMP iterations per problem of an untimed warm-up batch (0: none)")
+    ap.add_argument("--batched-lockstep", action="store_true",
+                    help="packed batched form: one SIMP iteration of every problem per call (mycel_simp_step_many) "
+                         "instead of whole runs in which each problem goes on by itself (mycel_simp_run_many)")
     ap.add_argument("--batched-packs", type=int, default=4,
                     help="packs of the packed batched form (each on its own context and host thread)")
     ap.add_argument("--batched-mode", choices=("packed", "served", "both"), default="both",
@@ -491,11 +494,15 @@ def run_batched(args):
                     pr = api.Problem(probs[k].model, ctx)
                     made.append((k, pr, api.SimpSession(pr, opts(probs[k], iters, head))))
                 packed0 = ctx.packed_count
-                while not all(x[2].done for x in made):
-                    live = [x for x in made if not x[2].done]
-                    for x, r in zip(live, api.SimpSession.step_many([x[2] for x in live])):
-                        if r is not None:
-                            ph[x[0]].append(r.compliance)
+                if args.batched_lockstep:  # every SIMP iteration of the pack a barrier (mycel_simp_step_many)
+                    while not all(x[2].done for x in made):
+                        live = [x for x in made if not x[2].done]
+                        for x, r in zip(live, api.SimpSession.step_many([x[2] for x in live])):
+                            if r is not None:
+                                ph[x[0]].append(r.compliance)
+                else:  # whole runs (mycel_simp_run_many): each problem goes on as soon as its own solve ends
+                    for x, recs in zip(made, api.SimpSession.run_many([x[2] for x in made])):
+                        ph[x[0]].extend(r.compliance for r in recs)
                 info[g] = {"problems": len(made), "rhs_solved_packed": ctx.packed_count - packed0}
                 for _, pr, se in made:
                     se.close()
