@@ -5061,7 +5061,9 @@ static int32_t pk_build(mycel_ctx* c, PackWork* w, std::vector<PkUnit>& units, c
   for (int t = 0; t < 2; ++t) {
     pk_compact(P, s, P.grp_iter[t], P.n_iter[t]);
     for (const PkLaunch& L : P.mv1[t]) pk_issue(P, L, s, 0);
-    nl += 1 + (int)P.mv1[t].size() + pk_step(P, s, 0, t);
+    // the step each right-hand side takes next: 0 after its matvec; a (re)start of a packed run (1, 2) in the
+    // first slot, whose matvec list left it out
+    nl += 1 + (int)P.mv1[t].size() + pk_step(P, s, -1, t);
   }
   k_pk_gather<<<(nu + 127) / 128, 128, 0, s>>>(P.d_sts, nu, P.d_states);
   nl++;
