@@ -1402,7 +1402,8 @@ static void launch_mv32_variant(mycel_problem* p, cudaStream_t s, const float* x
 }
 
 // Autotuner: on first use, time every variant (K x on the problem's FP32 buffers, after one warm-up launch)
-// and keep the fastest; a tensor-core run that reports a failed wait is never chosen.
+// and keep the factorised one unless another takes under 3/4 of its time; a tensor-core run that reports a
+// failed wait is never chosen.
 // Variant choices are shared by every problem of the process with the same grid, so a problem's arithmetic
 // does not depend on what else was running when it was first timed (first measurement wins).
 static std::mutex g_mv32_mu;
@@ -1462,9 +1463,12 @@ static int32_t resolve_mv32(mycel_problem* p) {
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  // the factorised operator (variants[0]) unless another is clearly faster: timings taken while other work
+  // shares the GPU (several jobs at once) scatter by more than the variants differ on small grids
+  constexpr float kTuneMargin = 0.75f;
   int best = 0;
   for (int v = 1; v < 3; ++v)
-    if (t[v] < t[best]) best = v;
+    if (t[v] < kTuneMargin * t[0] && t[v] < t[best]) best = v;
   p->mv32 = variants[best];
   {
     std::lock_guard<std::mutex> lk(g_mv32_mu);
@@ -5454,8 +5458,9 @@ struct PackRun {
 
 void pkr_close(PackRun* r) { delete r; }
 
-int32_t pkr_open(mycel_ctx* c, const std::vector<PackRunJob>& jobs, PackRun** out) {
+int32_t pkr_open(mycel_ctx* c, const std::vector<PackRunJob>& jobs, PackRun** out, std::vector<char>* packed) {
   *out = nullptr;
+  packed->assign(jobs.size(), 0);
   cudaStream_t s = c->stream;
   int32_t st = MYCEL_OK;
   static std::once_flag smem_once;
@@ -5473,6 +5478,12 @@ int32_t pkr_open(mycel_ctx* c, const std::vector<PackRunJob>& jobs, PackRun** ou
   for (size_t j = 0; j < jobs.size(); ++j) {
     mycel_problem* p = jobs[j].p;
     const int nc = jobs[j].ncase;
+    if (nc == 0) {  // not in the mixed multigrid form: stepped alone by the caller
+      r->jp.push_back(nullptr);
+      r->ju0.push_back((int)r->units.size());
+      r->jnc.push_back(0);
+      continue;
+    }
     if (p->ctx != c) return set_error(c, MYCEL_E_ARG, "packed run: every problem must belong to the context");
     for (size_t i = 0; i < j; ++i)
       if (jobs[i].p == p) return set_error(c, MYCEL_E_ARG, "packed run: one job per problem");
@@ -5483,9 +5494,14 @@ int32_t pkr_open(mycel_ctx* c, const std::vector<PackRunJob>& jobs, PackRun** ou
     bool avail = false;
     if ((st = resolve_mv32(p)) || (st = mg_ensure(p, &avail))) return st;
     if (!avail || p->mg->prefers_f64 || p->mg->sweeps != 1 || p->mv32 != MYCEL_MV32_FACTORED ||
-        (nc > 1 && nc > p->mg->ncap) || (int)r->units.size() + nc > kPkMaxUnits)
-      return set_error(c, MYCEL_E_ARG, "packed run: a problem the packed form cannot take");
+        (nc > 1 && nc > p->mg->ncap) || (int)r->units.size() + nc > kPkMaxUnits) {
+      r->jp.push_back(nullptr);  // stepped alone by the caller
+      r->ju0.push_back((int)r->units.size());
+      r->jnc.push_back(0);
+      continue;
+    }
     if (nc > 1 && (st = mg_ensure_cases(p, nc))) return st;
+    (*packed)[j] = 1;
     MgHier* mg = p->mg;
     const int64_t nd = p->g.nd;
     r->jp.push_back(p);
@@ -5523,7 +5539,7 @@ int32_t pkr_open(mycel_ctx* c, const std::vector<PackRunJob>& jobs, PackRun** ou
     }
   }
   const int nu = (int)r->units.size();
-  if (nu == 0) return set_error(c, MYCEL_E_ARG, "packed run: no right-hand side");
+  if (nu == 0) return set_error(c, MYCEL_E_ARG, "packed run: no problem the packed form can take");
   r->jt0.resize(jobs.size());
   r->state.assign(nu, 0);
   r->stalled.assign(nu, 0);
@@ -5740,6 +5756,7 @@ int32_t pkr_advance(PackRun* r, const volatile int32_t* cancel, std::vector<int>
     if ((st = pk_set(c, P, op))) return st;
   }
   for (size_t j = 0; j < r->jp.size(); ++j) {
+    if (!r->jp[j]) continue;
     bool live = false, over = true;
     for (int i = r->ju0[j]; i < r->ju0[j] + r->jnc[j]; ++i) {
       live = live || r->state[i] != 0;

@@ -335,8 +335,8 @@ struct PackJob {
 int32_t mg_solve_packed(mycel_ctx* c, int njobs, PackJob* jobs, const volatile int32_t* cancel);
 void pack_release(mycel_ctx* c);
 // Asynchronous packed run (mycel_simp_run_many): the right-hand sides of the jobs share one packed plan for a
-// whole optimisation and each job's solves start and end on their own. pkr_open fails with MYCEL_E_ARG when a
-// job cannot be packed. pkr_begin issues the start of job j's next solve; after the caller synchronises the
+// whole optimisation and each job's solves start and end on their own. pkr_open leaves out the jobs the
+// packed form cannot take (packed[j] 0: the caller steps them alone). pkr_begin issues the start of job j's next solve; after the caller synchronises the
 // context stream, pkr_after_begin lets the started right-hand sides run; pkr_advance runs one chunk of outer
 // iterations (synchronised), refines and restarts what stopped, and appends the jobs whose solves ended;
 // pkr_results gives an ended job's results (ncase of them).
@@ -346,7 +346,7 @@ struct PackRunJob {
   double* d_u;
 };
 struct PackRun;
-int32_t pkr_open(mycel_ctx* c, const std::vector<PackRunJob>& jobs, PackRun** out);
+int32_t pkr_open(mycel_ctx* c, const std::vector<PackRunJob>& jobs, PackRun** out, std::vector<char>* packed);
 void pkr_close(PackRun* r);
 int32_t pkr_begin(PackRun* r, int j, double tol, int max_iter);
 int32_t pkr_after_begin(PackRun* r);

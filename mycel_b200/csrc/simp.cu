@@ -781,15 +781,15 @@ extern "C" int32_t mycel_simp_run_many(mycel_simp_session* const* ss, int32_t n,
   };
   if (n_iters)
     for (int i = 0; i < n; ++i) n_iters[i] = 0;
-  bool packable = true;
   std::vector<PackRunJob> jobs;
   for (int i = 0; i < n; ++i) {
     mycel_simp_session* s = ss[i];
-    packable = packable && s->o.precision == MYCEL_PRECISION_MIXED_MG && (s->ncase == 1 || cases_solved_together(s));
-    jobs.push_back(PackRunJob{s->p, s->ncase, s->ncase == 1 ? s->d_u : s->d_uc});
+    const bool form = s->o.precision == MYCEL_PRECISION_MIXED_MG && (s->ncase == 1 || cases_solved_together(s));
+    jobs.push_back(PackRunJob{s->p, form ? s->ncase : 0, s->ncase == 1 ? s->d_u : s->d_uc});
   }
   PackRun* run = nullptr;
-  if (packable && pkr_open(c, jobs, &run) != MYCEL_OK) run = nullptr;
+  std::vector<char> pmask(n, 0);
+  if (pkr_open(c, jobs, &run, &pmask) != MYCEL_OK) run = nullptr;
   if (!run) {  // sessions stepped together, each SIMP iteration a barrier
     std::vector<mycel_iter_record> recs(n);
     std::vector<int32_t> dn(n), sst(n);
@@ -816,15 +816,27 @@ extern "C" int32_t mycel_simp_run_many(mycel_simp_session* const* ss, int32_t n,
     for (int i = 0; i < n; ++i)
       if (!ss[i]->done) {
         live[i] = 1;
-        if ((st[i] = begin(i))) live[i] = 0;
+        if (pmask[i] && (st[i] = begin(i))) live[i] = 0;
       }
     int32_t rc = cudaStreamSynchronize(c->stream) == cudaSuccess ? pkr_after_begin(run)
                                                                   : set_error(c, MYCEL_E_DEVICE, "packed run start");
     std::vector<int> ended;
     while (!rc) {
-      bool any = false;
-      for (int i = 0; i < n; ++i) any = any || live[i];
+      bool any = false, any_packed = false;
+      for (int i = 0; i < n; ++i) any = any || live[i], any_packed = any_packed || (live[i] && pmask[i]);
       if (!any) break;
+      for (int i = 0; i < n; ++i) {  // the sessions the packed form cannot take: one SIMP iteration each
+        if (!live[i] || pmask[i]) continue;
+        mycel_iter_record r{};
+        int32_t d = 0;
+        if ((st[i] = simp_step_impl(ss[i], &r, &d, cancel))) {
+          live[i] = 0;
+          continue;
+        }
+        record(i, r);
+        if (d || (cancel && *cancel)) live[i] = 0;
+      }
+      if (!any_packed) continue;
       ended.clear();
       if ((rc = pkr_advance(run, cancel, &ended))) break;
       if (ended.empty()) {

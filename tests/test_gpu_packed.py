@@ -169,3 +169,22 @@ def test_run_many_each_problem_as_alone(ctx):
             p.close()
     for k, (ra, da) in enumerate(alone):
         _same(ra, da, out[k], reads[k])
+
+
+def test_run_many_with_a_session_of_another_form(ctx):
+    """A session the packed form cannot take (FP64 here) is stepped alone inside the run; all equal their runs
+    alone."""
+    jobs = _jobs()[:3]
+    jobs[1] = (jobs[1][0], jobs[1][1].replace(precision="fp64", solver_tolerance_initial=1e-8,
+                                              solver_tolerance_final=1e-8, max_iterations=2))
+    alone = [_alone(ctx, m, o, o.max_iterations) for m, o in jobs]
+    made = [_session(ctx, m, o) for m, o in jobs]
+    try:
+        out = api.SimpSession.run_many([s for _, s in made])
+        reads = [s.read() for _, s in made]
+    finally:
+        for p, s in made:
+            s.close()
+            p.close()
+    for k, (ra, da) in enumerate(alone):
+        _same(ra, da, out[k], reads[k])
