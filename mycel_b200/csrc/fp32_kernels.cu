@@ -4197,6 +4197,24 @@ int32_t mg_solve_cases(mycel_problem* p, int ncase, double* d_u, double tol, int
 // converged restart together. A right-hand side that stalls, breaks down or runs out of iterations is
 // finished alone from its refined u, as a single solve goes on after its FP32 outer iteration.
 // ---------------------------------------------------------------------------------------------------------
+// A packed solve runs the factorised FP32 matvec: a problem whose variant the autotuner chose (not the
+// caller) goes over to it, with its captured solver graphs dropped (they hold the other variant's launches).
+// Its later solves alone then use it too, so alone and packed it computes the same.
+static void pack_matvec(mycel_problem* p) {
+  if (p->tune_mv32 != 0 || p->mv32 == MYCEL_MV32_FACTORED) return;
+  p->mv32 = MYCEL_MV32_FACTORED;
+  for (int k = 0; k < 2; ++k) {
+    if (p->pcg32_graph[k]) cudaGraphExecDestroy(p->pcg32_graph[k]);
+    p->pcg32_graph[k] = nullptr;
+    if (MgHier* mg = p->mg) {
+      if (mg->graph[k]) cudaGraphExecDestroy(mg->graph[k]);
+      if (mg->graph32[k]) cudaGraphExecDestroy(mg->graph32[k]);
+      if (mg->cw.graph[k]) cudaGraphExecDestroy(mg->cw.graph[k]);
+      mg->graph[k] = mg->graph32[k] = mg->cw.graph[k] = nullptr;
+    }
+  }
+}
+
 constexpr int kPkMaxUnits = 1024;
 constexpr int kPkStall = 100;  // state op: a running right-hand side's cycle stalled (replacement point)
 
@@ -5132,6 +5150,7 @@ int32_t mg_solve_packed(mycel_ctx* c, int njobs, PackJob* jobs, const volatile i
     if (J.ncase > 1 && (st = ensure_cases(p))) return st;
     bool avail = false;
     if ((st = resolve_mv32(p)) || (st = mg_ensure(p, &avail))) return st;
+    if (avail) pack_matvec(p);
     bool ok = avail && !p->mg->prefers_f64 && p->mg->sweeps == 1 && p->mv32 == MYCEL_MV32_FACTORED &&
               (J.ncase == 1 || J.ncase <= p->mg->ncap) && (int)units.size() + J.ncase <= kPkMaxUnits;
     for (int i = 0; i < j && ok; ++i) ok = !(packed[i] && jobs[i].p == p);  // one job per problem
@@ -5493,6 +5512,7 @@ int32_t pkr_open(mycel_ctx* c, const std::vector<PackRunJob>& jobs, PackRun** ou
     if (nc > 1 && (st = ensure_cases(p))) return st;
     bool avail = false;
     if ((st = resolve_mv32(p)) || (st = mg_ensure(p, &avail))) return st;
+    if (avail) pack_matvec(p);
     if (!avail || p->mg->prefers_f64 || p->mg->sweeps != 1 || p->mv32 != MYCEL_MV32_FACTORED ||
         (nc > 1 && nc > p->mg->ncap) || (int)r->units.size() + nc > kPkMaxUnits) {
       r->jp.push_back(nullptr);  // stepped alone by the caller

@@ -821,6 +821,21 @@ extern "C" int32_t mycel_simp_run_many(mycel_simp_session* const* ss, int32_t n,
     int32_t rc = cudaStreamSynchronize(c->stream) == cudaSuccess ? pkr_after_begin(run)
                                                                   : set_error(c, MYCEL_E_DEVICE, "packed run start");
     std::vector<int> ended;
+    // MYCEL_VERBOSE: host time in the chunks (with the refinement of what stopped) and in the SIMP phases
+    const bool verbose = std::getenv("MYCEL_VERBOSE") != nullptr;
+    double t_adv = 0.0, t_phase = 0.0;
+    int64_t n_adv = 0, n_end = 0;
+    auto now = [] { return std::chrono::steady_clock::now(); };
+    auto since = [](std::chrono::steady_clock::time_point a) {
+      return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - a).count();
+    };
+    struct Report {
+      bool on; double* a; double* p; int64_t* na; int64_t* ne;
+      ~Report() {
+        if (on) std::fprintf(stderr, "mycel: run_many chunks %lld (%.1f ms), solves ended %lld, SIMP phases %.1f ms\n",
+                             (long long)*na, *a, (long long)*ne, *p);
+      }
+    } report{verbose, &t_adv, &t_phase, &n_adv, &n_end};
     while (!rc) {
       bool any = false, any_packed = false;
       for (int i = 0; i < n; ++i) any = any || live[i], any_packed = any_packed || (live[i] && pmask[i]);
@@ -838,7 +853,16 @@ extern "C" int32_t mycel_simp_run_many(mycel_simp_session* const* ss, int32_t n,
       }
       if (!any_packed) continue;
       ended.clear();
-      if ((rc = pkr_advance(run, cancel, &ended))) break;
+      const auto ta = now();
+      rc = pkr_advance(run, cancel, &ended);
+      t_adv += since(ta);
+      ++n_adv;
+      n_end += (int64_t)ended.size();
+      if (rc) break;
+      const auto tp = now();
+      struct Lap { double* t; std::chrono::steady_clock::time_point t0;
+        ~Lap() { *t += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count(); } };
+      Lap lap{&t_phase, tp};
       if (ended.empty()) {
         if (!pkr_running(run)) rc = set_error(c, MYCEL_E_TIMEOUT, "packed run: no solve running");
         continue;
