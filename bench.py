@@ -552,8 +552,9 @@ def run_batched(args):
     if args.batched_mode in ("packed", "both"):
         rec, info = measured("packed", packed_run)
         rec.update({"packs": len(info), "rhs_solved_packed": sum(x["rhs_solved_packed"] for x in info),
-                    "form": head, "note": "packs of problems whose solves share launches (mycel_simp_step_many), "
-                                          "the packs on concurrent contexts"})
+                    "form": head, "note": "packs of problems whose solves share launches (mycel_simp_run_many, or "
+                                          "mycel_simp_step_many with --batched-lockstep), the packs on concurrent "
+                                          "contexts"})
         out["packed"] = rec
     if args.batched_mode in ("served", "both"):
         rec, st = measured(head, lambda it: served_run(it, head))
@@ -567,6 +568,7 @@ def run_batched(args):
         hists["fp64"] = hist
     if "packed" in out and head in out:
         out["packed"]["same_histories_as_served"] = hists["packed"] == hists[head]
+        out["packed"]["rel_compliance_err_vs_served"] = compare_histories(hists["packed"], hists[head])
         out["packed"]["speedup_vs_served"] = out["packed"]["simp_iter_s"] / out[head]["simp_iter_s"]
         if out["packed"].get("steady_simp_iter_s") and out[head].get("steady_simp_iter_s"):
             out["packed"]["steady_speedup_vs_served"] = (out["packed"]["steady_simp_iter_s"] /
