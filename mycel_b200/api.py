@@ -73,7 +73,7 @@ class Context:
 
     @property
     def packed_count(self) -> int:
-        """Right-hand sides solved through packed launches on this context (mycel_simp_step_many)."""
+        """Right-hand sides solved through packed launches on this context (mycel_simp_step_many / run_many)."""
         return int(L.load().mycel_ctx_packed_count(self.handle))
 
     def set_profiling(self, on: bool = True):
@@ -610,11 +610,25 @@ class SimpSession:
         """The stop rule has fired (TopologyOptimizationResult.Converged)."""
         return bool(L.load().mycel_simp_converged(self.handle))
 
-    def read(self, u=True, densities=True, active=False):
+    def read(self, u=True, densities=True, active=False, out: Optional[dict] = None):
+        """u, the physical and design densities (box, float) and, with active, the active-indexed FP64
+        densities. out may hold preallocated arrays ("u", "physical", "design"; pinned host memory makes the
+        copies faster), which are filled and returned instead of new ones."""
         m = self.problem.model
-        uu = np.zeros(m.total_dofs) if u else None
-        ph = np.zeros(m.total_elements, dtype=np.float32) if densities else None
-        de = np.zeros(m.total_elements, dtype=np.float32) if densities else None
+        out = out or {}
+
+        def buf(key, want, n, dt):
+            if not want:
+                return None
+            a = out.get(key)
+            if a is None:
+                return np.zeros(n, dtype=dt)
+            if a.dtype != np.dtype(dt) or a.size != n or not a.flags.c_contiguous:
+                raise ArgumentError(f"out[{key!r}]: {n} contiguous {np.dtype(dt).name} values expected")
+            return a
+        uu = buf("u", u, m.total_dofs, np.float64)
+        ph = buf("physical", densities, m.total_elements, np.float32)
+        de = buf("design", densities, m.total_elements, np.float32)
         rpa = np.zeros(m.active_element_count) if active else None
         rda = np.zeros(m.active_element_count) if active else None
         lam = C.c_double(0)
