@@ -929,6 +929,27 @@ void fan_end(mycel_ctx* c) {
   f->active = false;
 }
 
+int32_t fan_use_free(mycel_ctx* c, int slot, cudaStream_t* fan_stream) {
+  Fan* f = (Fan*)c->fan;
+  if (!f) {  // the streams, made as fan_begin makes them
+    if (int32_t st = fan_begin(c)) return st;
+    fan_end(c);
+    f = (Fan*)c->fan;
+  }
+  const int k = slot % Fan::kN;
+  c->main_stream = c->stream;
+  c->main_side = c->side;
+  c->stream = f->s[k];
+  c->side = f->side[k];
+  if (fan_stream) *fan_stream = f->s[k];
+  return MYCEL_OK;
+}
+
+void fan_restore(mycel_ctx* c) {
+  c->stream = c->main_stream;
+  c->side = c->main_side;
+}
+
 void fan_release(mycel_ctx* c) {
   Fan* f = (Fan*)c->fan;
   if (!f) return;

@@ -5698,6 +5698,71 @@ int32_t pkr_after_begin(PackRun* r) {
   return MYCEL_OK;
 }
 
+// k_mix_init of one job's right-hand sides (kernel parameters: the host may start other jobs at once)
+struct PkInitJob {
+  int n;
+  MixState* st[kMgMaxCases];
+  double target[kMgMaxCases];
+  int max_iter[kMgMaxCases];
+};
+__global__ void k_pk_init_job(const __grid_constant__ PkInitJob J, double flush) {
+  const int i = threadIdx.x;
+  if (i >= J.n || !J.st[i]) return;
+  MixState s = {};
+  s.status = MIX_RUNNING;
+  s.target = J.target[i];
+  s.max_iter = J.max_iter[i];
+  s.first = 1;
+  s.flush_factor = flush;
+  s.pmode = 2;
+  *J.st[i] = s;
+}
+
+int32_t pkr_after_begin_job(PackRun* r, int j) {
+  mycel_ctx* c = r->c;
+  cudaStream_t s = c->stream;
+  PkInitJob J{};
+  J.n = r->jnc[j];
+  bool any = false;
+  for (int q = 0; q < r->jnc[j]; ++q) {
+    const int i = r->ju0[j] + q;
+    J.st[q] = nullptr;
+    if (r->state[i] != 1) continue;
+    const PkUnit& u = r->units[i];
+    mycel_pcg_result& res = r->res[i];
+    r->bnorm[i] = r->h_bn[i];
+    r->iters[i] = r->flushes[i] = r->resume[i] = 0;
+    r->cycle_limit[i] = 300;
+    r->stalled[i] = r->stall_pending[i] = 0;
+    if (r->bnorm[i] <= 1e-30) {
+      MYCEL_CUDA(c, cudaMemsetAsync(u.u, 0, sizeof(double) * u.p->g.nd, s));
+      res.converged = 1;
+      std::snprintf(res.message, sizeof res.message, "RHS is zero. Solution is zero.");
+      r->state[i] = 6;
+      continue;
+    }
+    r->rel[i] = std::sqrt(r->h_rn2[i]) / r->bnorm[i];
+    if (r->rel[i] <= r->tol[i]) {
+      res.converged = 1;
+      res.final_residual = r->rel[i];
+      std::snprintf(res.message, sizeof res.message, "Initial guess already converged.");
+      r->state[i] = 6;
+      continue;
+    }
+    MYCEL_CUDA(c, cudaMemsetAsync(u.x, 0, sizeof(float) * (size_t)u.p->g.n32, s));
+    J.st[q] = u.st;
+    J.target[q] = 0.5 * r->tol[i] * r->bnorm[i];
+    J.max_iter[q] = r->max_iter[i];
+    r->state[i] = 2;
+    any = true;
+  }
+  if (!any) return MYCEL_OK;
+  k_pk_init_job<<<1, 32, 0, s>>>(J, 1e-3);
+  c->launches++;
+  MYCEL_CUDA(c, cudaGetLastError());
+  return MYCEL_OK;
+}
+
 bool pkr_running(const PackRun* r) {
   for (char v : r->state)
     if (v == 2) return true;

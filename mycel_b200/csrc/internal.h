@@ -350,6 +350,7 @@ int32_t pkr_open(mycel_ctx* c, const std::vector<PackRunJob>& jobs, PackRun** ou
 void pkr_close(PackRun* r);
 int32_t pkr_begin(PackRun* r, int j, double tol, int max_iter);
 int32_t pkr_after_begin(PackRun* r);
+int32_t pkr_after_begin_job(PackRun* r, int j);  // the same for job j only (its start read back already)
 bool pkr_running(const PackRun* r);
 int32_t pkr_advance(PackRun* r, const volatile int32_t* cancel, std::vector<int>* ended);
 const mycel_pcg_result* pkr_results(const PackRun* r, int j);
@@ -361,6 +362,10 @@ int32_t fan_begin(mycel_ctx* c);
 void fan_use(mycel_ctx* c, int slot);
 void fan_end(mycel_ctx* c);
 void fan_release(mycel_ctx* c);
+// The same side stream k for work that depends on nothing queued on the context stream (the caller orders it
+// by events): fan_use_free issues the following work of the context there, fan_restore returns.
+int32_t fan_use_free(mycel_ctx* c, int slot, cudaStream_t* fan_stream);
+void fan_restore(mycel_ctx* c);
 bool cases_together_enabled();
 int32_t kernel_bench(mycel_problem* p, int which, int reps, double* avg_us);  // MYCEL_CASES_TOGETHER=0 turns the batched case solve off
 int32_t refined_solve_entry(mycel_problem* p, const double* d_b, const int32_t* d_nz, int32_t n_nz, double* d_u,

@@ -807,38 +807,38 @@ extern "C" int32_t mycel_simp_run_many(mycel_simp_session* const* ss, int32_t n,
       }
     }
   } else {
+    // Each packed session cycles through: solving (its right-hand sides in the packed chunks), SIMP update
+    // (sensitivities, adjoint filter, OC) and start of the next solve (filter, E, set-up, start of the solve)
+    // on a side stream of the context while the chunks of the others go on; the host polls the side stream's
+    // event and takes the next step when it has passed.
+    enum : int { J_SOLVE = 0, J_POST = 1, J_BEGIN = 2, J_OFF = 3 };
     std::vector<SimpPre> pre(n);
     std::vector<char> live(n, 0);
-    auto begin = [&](int i) -> int32_t {
+    std::vector<int> phase(n, J_OFF);
+    std::vector<cudaEvent_t> ev(n, nullptr);
+    std::vector<mycel_pcg_result> pr(n);
+    int32_t rc = MYCEL_OK;
+    for (int i = 0; i < n && !rc; ++i)
+      if (pmask[i] && cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming) != cudaSuccess)
+        rc = set_error(c, MYCEL_E_DEVICE, "packed run: events");
+    for (int i = 0; i < n && !rc; ++i) {  // first starts on the context stream, then one wait
+      if (ss[i]->done) continue;
+      live[i] = 1;
+      if (!pmask[i]) continue;
       simp_pre(ss[i], &pre[i]);
-      return pkr_begin(run, i, pre[i].tol, ss[i]->o.solver_max_iterations);
-    };
-    for (int i = 0; i < n; ++i)
-      if (!ss[i]->done) {
-        live[i] = 1;
-        if (pmask[i] && (st[i] = begin(i))) live[i] = 0;
-      }
-    int32_t rc = cudaStreamSynchronize(c->stream) == cudaSuccess ? pkr_after_begin(run)
+      if ((st[i] = pkr_begin(run, i, pre[i].tol, ss[i]->o.solver_max_iterations))) live[i] = 0;
+      else phase[i] = J_SOLVE;
+    }
+    if (!rc) rc = cudaStreamSynchronize(c->stream) == cudaSuccess ? pkr_after_begin(run)
                                                                   : set_error(c, MYCEL_E_DEVICE, "packed run start");
-    std::vector<int> ended;
-    // MYCEL_VERBOSE: host time in the chunks (with the refinement of what stopped) and in the SIMP phases
+    // MYCEL_VERBOSE: host time in the chunks (with the refinement of what stopped) and waiting for side work
     const bool verbose = std::getenv("MYCEL_VERBOSE") != nullptr;
-    double t_adv = 0.0, t_phase = 0.0;
+    double t_adv = 0.0, t_wait = 0.0;
     int64_t n_adv = 0, n_end = 0;
-    auto now = [] { return std::chrono::steady_clock::now(); };
-    auto since = [](std::chrono::steady_clock::time_point a) {
-      return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - a).count();
-    };
-    struct Report {
-      bool on; double* a; double* p; int64_t* na; int64_t* ne;
-      ~Report() {
-        if (on) std::fprintf(stderr, "mycel: run_many chunks %lld (%.1f ms), solves ended %lld, SIMP phases %.1f ms\n",
-                             (long long)*na, *a, (long long)*ne, *p);
-      }
-    } report{verbose, &t_adv, &t_phase, &n_adv, &n_end};
+    std::vector<int> ended;
     while (!rc) {
-      bool any = false, any_packed = false;
-      for (int i = 0; i < n; ++i) any = any || live[i], any_packed = any_packed || (live[i] && pmask[i]);
+      bool any = false;
+      for (int i = 0; i < n; ++i) any = any || live[i];
       if (!any) break;
       for (int i = 0; i < n; ++i) {  // the sessions the packed form cannot take: one SIMP iteration each
         if (!live[i] || pmask[i]) continue;
@@ -851,56 +851,81 @@ extern "C" int32_t mycel_simp_run_many(mycel_simp_session* const* ss, int32_t n,
         record(i, r);
         if (d || (cancel && *cancel)) live[i] = 0;
       }
-      if (!any_packed) continue;
       ended.clear();
-      const auto ta = now();
-      rc = pkr_advance(run, cancel, &ended);
-      t_adv += since(ta);
+      const auto ta = std::chrono::steady_clock::now();
+      if ((rc = pkr_advance(run, cancel, &ended))) break;
+      t_adv += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - ta).count();
       ++n_adv;
       n_end += (int64_t)ended.size();
+      for (int i : ended) {  // the solve has ended: the SIMP update on the session's side stream
+        fold_cases(pkr_results(run, i), ss[i]->ncase, &pr[i]);
+        cudaStream_t fs = nullptr;
+        if ((rc = fan_use_free(c, i, &fs))) break;
+        st[i] = simp_post_issue(ss[i], pre[i], pr[i]);
+        if (!st[i] && cudaEventRecord(ev[i], fs) != cudaSuccess) st[i] = set_error(c, MYCEL_E_DEVICE, "packed run: event");
+        fan_restore(c);
+        if (st[i]) live[i] = 0, phase[i] = J_OFF;
+        else phase[i] = J_POST;
+      }
       if (rc) break;
-      const auto tp = now();
-      struct Lap { double* t; std::chrono::steady_clock::time_point t0;
-        ~Lap() { *t += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count(); } };
-      Lap lap{&t_phase, tp};
-      if (ended.empty()) {
-        if (!pkr_running(run)) rc = set_error(c, MYCEL_E_TIMEOUT, "packed run: no solve running");
-        continue;
-      }
-      std::vector<mycel_pcg_result> pr(ended.size());
-      for (size_t q = 0; q < ended.size(); ++q) {
-        const int i = ended[q];
-        fold_cases(pkr_results(run, i), ss[i]->ncase, &pr[q]);
-        if ((st[i] = simp_post_issue(ss[i], pre[i], pr[q]))) live[i] = 0;
-      }
-      if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
-        rc = set_error(c, MYCEL_E_DEVICE, "packed run: SIMP update");
-        break;
-      }
-      bool began = false;
-      for (size_t q = 0; q < ended.size(); ++q) {
-        const int i = ended[q];
-        if (!live[i]) continue;
+      bool waiting = false;
+      for (int i = 0; i < n && !rc; ++i) {
+        if (!live[i] || (phase[i] != J_POST && phase[i] != J_BEGIN)) continue;
+        const cudaError_t q = cudaEventQuery(ev[i]);
+        if (q == cudaErrorNotReady) {
+          waiting = true;
+          continue;
+        }
+        if (q != cudaSuccess) {
+          rc = set_error(c, MYCEL_E_DEVICE, std::string("packed run: ") + cudaGetErrorString(q));
+          break;
+        }
+        if (phase[i] == J_BEGIN) {  // its start has been read back: it joins the chunks
+          if ((st[i] = pkr_after_begin_job(run, i))) live[i] = 0, phase[i] = J_OFF;
+          else phase[i] = J_SOLVE;
+          continue;
+        }
         mycel_iter_record r{};
         int32_t d = 0;
-        if ((st[i] = simp_post_finish(ss[i], pre[i], pr[q], &r, &d))) {
+        if ((st[i] = simp_post_finish(ss[i], pre[i], pr[i], &r, &d))) {
           live[i] = 0;
+          phase[i] = J_OFF;
           continue;
         }
         record(i, r);
         if (d || (cancel && *cancel)) {
           live[i] = 0;
+          phase[i] = J_OFF;
           continue;
         }
-        if ((st[i] = begin(i))) live[i] = 0;
-        else began = true;
+        cudaStream_t fs = nullptr;  // the next iteration's filter, E, set-up and solve start, on the side stream
+        if ((rc = fan_use_free(c, i, &fs))) break;
+        simp_pre(ss[i], &pre[i]);
+        st[i] = pkr_begin(run, i, pre[i].tol, ss[i]->o.solver_max_iterations);
+        if (!st[i] && cudaEventRecord(ev[i], fs) != cudaSuccess) st[i] = set_error(c, MYCEL_E_DEVICE, "packed run: event");
+        fan_restore(c);
+        if (st[i]) live[i] = 0, phase[i] = J_OFF;
+        else phase[i] = J_BEGIN, waiting = true;
       }
-      if (began) {
-        rc = cudaStreamSynchronize(c->stream) == cudaSuccess ? pkr_after_begin(run)
-                                                             : set_error(c, MYCEL_E_DEVICE, "packed run start");
+      if (rc) break;
+      if (waiting && !pkr_running(run)) {  // nothing to iterate: wait for the first pending side work
+        const auto tw = std::chrono::steady_clock::now();
+        for (int i = 0; i < n; ++i)
+          if (live[i] && (phase[i] == J_POST || phase[i] == J_BEGIN)) {
+            cudaEventSynchronize(ev[i]);
+            break;
+          }
+        t_wait += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tw).count();
       }
     }
     cudaStreamSynchronize(c->stream);
+    for (int i = 0; i < n; ++i)  // side work still in flight after an error or a cancellation
+      if (ev[i]) cudaEventSynchronize(ev[i]);
+    if (verbose)
+      std::fprintf(stderr, "mycel: run_many chunks %lld (%.1f ms), solves ended %lld, waiting for side work %.1f ms\n",
+                   (long long)n_adv, t_adv, (long long)n_end, t_wait);
+    for (cudaEvent_t e : ev)
+      if (e) cudaEventDestroy(e);
     pkr_close(run);
     if (rc && rc != MYCEL_E_CANCELLED)
       for (int i = 0; i < n; ++i)
