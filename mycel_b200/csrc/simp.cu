@@ -908,6 +908,14 @@ extern "C" int32_t mycel_simp_run_many(mycel_simp_session* const* ss, int32_t n,
         else phase[i] = J_BEGIN, waiting = true;
       }
       if (rc) break;
+      bool stepped_alone = false;
+      for (int i = 0; i < n; ++i) stepped_alone = stepped_alone || (live[i] && !pmask[i]);
+      if (!waiting && ended.empty() && !stepped_alone && !pkr_running(run)) {
+        bool solving = false;  // a session that solves but has nothing running would never go on
+        for (int i = 0; i < n; ++i) solving = solving || (live[i] && phase[i] == J_SOLVE);
+        if (solving) rc = set_error(c, MYCEL_E_TIMEOUT, "packed run: a solve has nothing left to run");
+        break;
+      }
       if (waiting && !pkr_running(run)) {  // nothing to iterate: wait for the first pending side work
         const auto tw = std::chrono::steady_clock::now();
         for (int i = 0; i < n; ++i)
