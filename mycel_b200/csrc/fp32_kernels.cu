@@ -525,13 +525,25 @@ __device__ __forceinline__ void tma_load_plane(void* dst, const CUtensorMap* map
 // one matvec (k_mv32f) or one tile of a packed launch (k_mv32f_pk). tm_a / tm_b point at the tensor maps
 // (kernel parameters, or a packed launch's table in global memory). Returns 0 when the state is not running
 // (nothing done, the mbarriers untouched), 1 after the tile, -1 when a bounded wait gave up (*err set).
-template <int MODE>
-__device__ __forceinline__ int mv32f_body(const GridDims& g, const HexOpF& op, const CUtensorMap* tm_a,
-                                           const CUtensorMap* tm_b, float* __restrict__ pnew,
-                                           float* __restrict__ y, const float* __restrict__ E,
-                                           const uint8_t* __restrict__ nf, int projected, MixState* st,
-                                           double* part, int zseg, int* err, int bx, int by, int bz, unsigned nblk,
-                                           unsigned bid) {
+// The matvec's pointers and constants: kernel parameters (a launch alone: read from the constant bank) or a
+// packed tile's copy in shared memory (read again after each barrier, so they hold no registers across steps).
+struct MvArgs {
+  const HexOpF* op;
+  const CUtensorMap *tm_a, *tm_b;
+  float* pnew;
+  float* y;
+  const float* E;
+  const uint8_t* nf;
+  MixState* st;
+  double* part;
+  int* err;
+  int projected;
+};
+
+template <int MODE, class A>
+__device__ __forceinline__ int mv32f_body(const GridDims& g, const A& a, int zseg, int bx, int by, int bz, unsigned nblk,
+                                          unsigned bid) {
+  MixState* const st = a.st;
   extern __shared__ __align__(128) unsigned char fac_smem[];
   // [FNST] stages of x (MODE 0) or z (MODE 1), then MODE 1: [FNST] stages of p_{t-1}; then y-exchange
   float* yb = reinterpret_cast<float*>(fac_smem + (size_t)FNST * kFacStagePitch * (MODE == 1 ? 2 : 1));
@@ -558,8 +570,8 @@ __device__ __forceinline__ int mv32f_body(const GridDims& g, const HexOpF& op, c
     const int sl = r % FNST;
     const uint32_t bar = smem_u32(&full[sl]);
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(tx_bytes) : "memory");
-    tma_load_plane(plane_a(sl), tm_a, xs, j0 - 1, k0 - 1 + r, bar);
-    if (two) tma_load_plane(plane_b(sl), tm_b, xs, j0 - 1, k0 - 1 + r, bar);
+    tma_load_plane(plane_a(sl), a.tm_a, xs, j0 - 1, k0 - 1 + r, bar);
+    if (two) tma_load_plane(plane_b(sl), a.tm_b, xs, j0 - 1, k0 - 1 + r, bar);
   };
   if (tid == 0) {
     for (int q = 0; q < FNST; ++q)
@@ -591,7 +603,7 @@ __device__ __forceinline__ int mv32f_body(const GridDims& g, const HexOpF& op, c
   const int ex = i0 - 1 + l, ey = j0 - 1 + w;
   const bool exy = ex >= 0 && ex < g.nx && ey >= 0 && ey < g.ny;
   const int64_t ebase = (int64_t)ex + (int64_t)g.nx * ey, eplane = (int64_t)g.nx * g.ny;
-  auto eload = [&](int kk) -> float { return (exy && kk >= 0 && kk < g.nz) ? __ldg(E + ebase + eplane * kk) : 0.f; };
+  auto eload = [&](int kk) -> float { return (exy && kk >= 0 && kk < g.nz) ? __ldg(a.E + ebase + eplane * kk) : 0.f; };
   const int nxo = i0 + l, nyo = j0 + w;  // owned node (local node (1, 1) of this thread's elements)
   const bool mine = l < FOX && w < FOY && nxo < g.nx1 && nyo < g.ny1;
   const int64_t nbase = nxo + (int64_t)g.nx1 * nyo;     // node index at plane 0
@@ -599,7 +611,7 @@ __device__ __forceinline__ int mv32f_body(const GridDims& g, const HexOpF& op, c
   const int64_t fplane = (int64_t)g.rp * g.ny1;
   const int64_t nplane = (int64_t)g.nx1 * g.ny1;
   auto fload = [&](int kk) -> uint8_t {
-    return (mine && projected && kk >= k0 && kk < k1) ? nf[nbase + nplane * kk] : (uint8_t)0;
+    return (mine && a.projected && kk >= k0 && kk < k1) ? a.nf[nbase + nplane * kk] : (uint8_t)0;
   };
 
   wait_rel(0);
@@ -632,11 +644,11 @@ __device__ __forceinline__ int mv32f_body(const GridDims& g, const HexOpF& op, c
     if (MODE == 1 && mine) {
       if (kk + 1 >= k0 && kk + 1 < k1) {
 #pragma unroll
-        for (int c = 0; c < 3; ++c) pnew[fbase + fplane * (kk + 1) + c] = um[3][c];
+        for (int c = 0; c < 3; ++c) a.pnew[fbase + fplane * (kk + 1) + c] = um[3][c];
       }
       if (kk + 2 < k1) {
 #pragma unroll
-        for (int c = 0; c < 3; ++c) pnew[fbase + fplane * (kk + 2) + c] = ut[3][c];
+        for (int c = 0; c < 3; ++c) a.pnew[fbase + fplane * (kk + 2) + c] = ut[3][c];
       }
     }
     float2 u[3][8];
@@ -649,7 +661,7 @@ __device__ __forceinline__ int mv32f_body(const GridDims& g, const HexOpF& op, c
       }
     // comb[by][pl][c]: node column ex + 1, node row ey + by, node plane kk + pl, after the x-neighbour's part
     float comb[2][3][3];
-    hex_apply2(op, e2, u, [&](int c, float2 (&yc)[8]) {
+    hex_apply2(*a.op, e2, u, [&](int c, float2 (&yc)[8]) {
 #pragma unroll
       for (int by = 0; by < 2; ++by) {
         const int a = 2 * by;
@@ -676,13 +688,13 @@ __device__ __forceinline__ int mv32f_body(const GridDims& g, const HexOpF& op, c
         if (kk >= k0) {  // node plane kk: the element plane below (carried) + plane kk's bottom faces
           const float pv = ub[3][c];
           const float yo = (f0 >> c & 1) ? pv : carry[c] + s0;
-          y[fbase + fplane * kk + c] = yo;
+          a.y[fbase + fplane * kk + c] = yo;
           if (MODE == 1) pap += (double)pv * (double)yo;
         }
         if (kk + 1 < k1) {  // node plane kk + 1: complete within this step
           const float pv = um[3][c];
           const float yo = (f1 >> c & 1) ? pv : s1;
-          y[fbase + fplane * (kk + 1) + c] = yo;
+          a.y[fbase + fplane * (kk + 1) + c] = yo;
           if (MODE == 1) pap += (double)pv * (double)yo;
         }
         carry[c] = s2;
@@ -698,8 +710,8 @@ __device__ __forceinline__ int mv32f_body(const GridDims& g, const HexOpF& op, c
   const bool all_ok = __syncthreads_and(ok) != 0;
   if (all_ok && tid == 0)
     for (int q = 0; q < FNST; ++q) asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(smem_u32(&full[q])) : "memory");
-  if (!ok && err) atomicExch(err, 1);
-  if (MODE == 1) mv32_finish(pap, sh, st, part, tid, err, nblk, bid);
+  if (!ok && a.err) atomicExch(a.err, 1);
+  if (MODE == 1) mv32_finish(pap, sh, a.st, a.part, tid, a.err, nblk, bid);
   return all_ok ? 1 : -1;
 }
 
@@ -710,7 +722,8 @@ __global__ void __launch_bounds__(FX * FY, 2) k_mv32f(GridDims g, const __grid_c
                                                       float* __restrict__ pnew, float* __restrict__ y,
                                                       const float* __restrict__ E, const uint8_t* __restrict__ nf,
                                                       int projected, MixState* st, double* part, int zseg, int* err) {
-  mv32f_body<MODE>(g, op, &tm_a, &tm_b, pnew, y, E, nf, projected, st, part, zseg, err, blockIdx.x, blockIdx.y,
+  const MvArgs a{&op, &tm_a, &tm_b, pnew, y, E, nf, st, part, err, projected};
+  mv32f_body<MODE>(g, a, zseg, blockIdx.x, blockIdx.y,
                    blockIdx.z, gridDim.x * gridDim.y * gridDim.z,
                    (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x);
 }
@@ -4289,13 +4302,19 @@ __global__ void __launch_bounds__(FX * FY, 2) k_mv32f_pk(const PkMv* __restrict_
     const PkMv* m = tab + (code >> kPkLbBits);
     const unsigned lb = code & kPkLbMask;
     const unsigned gx = m->gx, gy = m->gy;
+    __shared__ MvArgs sa;
+    __shared__ HexOpF sop;
+    __shared__ GridDims sg;
     if (threadIdx.x == 0 && threadIdx.y == 0) {  // the thread that issues the copies; maps written before launch
       asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(&m->ta) : "memory");
       asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(&m->tb) : "memory");
+      sop = m->op;
+      sg = m->g;
+      sa = MvArgs{&sop, &m->ta, &m->tb, m->pnew, m->y, m->E, m->nf, m->st, m->part, m->err, m->projected};
     }
-    const int r = mv32f_body<MODE>(m->g, m->op, &m->ta, &m->tb, m->pnew, m->y, m->E, m->nf, m->projected, m->st,
-                                   m->part, m->zseg, m->err, (int)(lb % gx), (int)((lb / gx) % gy),
-                                   (int)(lb / (gx * gy)), gx * gy * m->gz, lb);
+    __syncthreads();
+    const int r = mv32f_body<MODE>(sg, sa, m->zseg, (int)(lb % gx), (int)((lb / gx) % gy), (int)(lb / (gx * gy)),
+                                   gx * gy * m->gz, lb);
     if (r < 0) break;  // a copy may still be in flight into this CTA's shared memory (uniform: the CTA's result)
   }
 }
