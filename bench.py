@@ -15,6 +15,8 @@ adjoint filter, OC bisection) on the device-resident state. Prints one JSON line
   roofline   the FP32 stiffness matvec (the dominant kernel), timed live by events captured in the PCG graph
   fp64       the plain FP64 path (bit-exact drop-in) on the same workload, and the timed path's compliance error
   cpu_baseline  the CPU oracle (C++ restatement, all host threads) on a bounded sample of the same iteration
+  serving    a bounded sample of the served job stream (p50/p99 latency, aggregate SIMP iter/s)
+  batched    the 48 batched instances: packed whole runs (solves in shared launches) against the serving loop
 
 --impl reference runs only the CPU restatement of the reference path (rank 0) on the same workload.
 Multi-GPU (torchrun): each rank runs its own replica of the workload (no collective on the data path).
@@ -82,6 +84,7 @@ def parse():
     ap.add_argument("--probe-variant", type=int, default=0,
                     help="FP32 matvec variant for --probe mixed (0 autotune, 1 dense, 2 tensor, 3 factored)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving sample of the default run")
+    ap.add_argument("--no-batched-sample", action="store_true", help="skip the batched sample of the default run")
     ap.add_argument("--mv32-variant", type=int, default=0,
                     help="FP32 matvec variant of the timed mixed run (0 autotune; for profiler runs)")
     ap.add_argument("--serve-sample-jobs", type=int, default=12)
@@ -450,7 +453,7 @@ def run_surface(args):
     print(json.dumps(out), flush=True)
 
 
-def run_batched(args):
+def batched_measure(args):
     """Batched instances: all problems at once; aggregate SIMP iter/s of the timed form in packs (solves in
     shared launches) and through the serving loop's slots, vs FP64. Each form is also run with
     --batched-steady-extra more iterations per problem: the extra iterations over the extra wall time give the
@@ -577,7 +580,11 @@ def run_batched(args):
         fast = "packed" if "packed" in out else head
         out[f"speedup_{head}_vs_fp64"] = out[fast]["simp_iter_s"] / out["fp64"]["simp_iter_s"]
         out[f"rel_compliance_err_{head}_vs_fp64"] = compare_histories(hists[fast], hists["fp64"])
-    print(json.dumps(out), flush=True)
+    return out
+
+
+def run_batched(args):
+    print(json.dumps(batched_measure(args)), flush=True)
 
 
 def run_mycel(args):
@@ -805,6 +812,15 @@ def run_mycel(args):
                                         args.serve_slots, 150.0, [args.precision, "fp64"])
         out["serving"]["note"] = ("bounded sample of the served stream: first jobs of the Poisson(20/s) stream, "
                                   "sizes log-uniform up to serve_sample_max_elems; full stream: bench.py --serve")
+
+    # ---------------- batched sample (rank 0): the 48 batched instances, packed and through the serving loop ---
+    if rank == 0 and not args.no_batched_sample:
+        ns = argparse.Namespace(**vars(args))
+        ns.batched_skip_fp64, ns.batched_steady_extra, ns.batched_mode = True, 0, "both"
+        out["batched"] = batched_measure(ns)
+        out["batched"]["note"] = ("48 batched instances x 4 SIMP iterations, load cases kept apart, after a "
+                                  "one-iteration warm-up batch: packed whole runs (mycel_simp_run_many, 4 packs) "
+                                  "against the serving loop; FP64 and steady figures: bench.py --batched")
 
     if rank == 0:
         print(json.dumps(out), flush=True)
