@@ -188,3 +188,22 @@ def test_run_many_with_a_session_of_another_form(ctx):
             p.close()
     for k, (ra, da) in enumerate(alone):
         _same(ra, da, out[k], reads[k])
+
+
+def test_read_into_caller_buffers(ctx):
+    """SimpSession.read(out=...) fills the caller's (pinned or plain) arrays with what read() returns."""
+    m, o = _jobs()[3]
+    p, s = _session(ctx, m, o)
+    try:
+        s.step()
+        ref = s.read(u=True, densities=True)
+        out = {"u": np.empty(m.total_dofs), "physical": np.empty(m.total_elements, dtype=np.float32),
+               "design": np.empty(m.total_elements, dtype=np.float32)}
+        got = s.read(u=True, densities=True, out=out)
+        for k in ("u", "physical", "design"):
+            assert got[k] is out[k] and np.array_equal(got[k], ref[k])
+        with pytest.raises(Exception, match="contiguous"):
+            s.read(u=True, densities=False, out={"u": np.empty(3)})
+    finally:
+        s.close()
+        p.close()
