@@ -600,8 +600,9 @@ class SimpSession:
         st = L.load().mycel_simp_run_many(hs, n, hist, cap, nit, stat,
                                           C.addressof(cancel) if cancel is not None else None)
         out = [[_snapshot(hist[k * cap + q]) for q in range(min(nit[k], cap))] for k in range(n)]
+        stopped = cancel is not None and bool(cancel.value)
         for s in sessions:
-            s.done = True
+            s.done = s.done or not stopped
         _check(st, sessions[0].problem.ctx)
         return out
 

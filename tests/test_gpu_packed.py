@@ -207,3 +207,27 @@ def test_read_into_caller_buffers(ctx):
     finally:
         s.close()
         p.close()
+
+
+def test_run_many_cancelled_then_stepped_alone(ctx):
+    """A cancelled packed run (CancellationToken, TopologyOptimizer.cs:169-172) returns without error and without
+    records, and leaves the sessions to step on by themselves. Their next iteration is the first one again (the
+    multigrid damping estimate may start warm, so its compliance is compared within 1e-5 relative: both solves
+    meet the 1e-6 residual tolerance)."""
+    jobs = _jobs()[:2]
+    fresh = [_alone(ctx, m, o, 1) for m, o in jobs]
+    made = [_session(ctx, m, o) for m, o in jobs]
+    try:
+        ctl = api.IterationController()
+        ctl.stop()
+        out = api.SimpSession.run_many([s for _, s in made], controller=ctl)
+        assert all(len(r) == 0 for r in out)
+        for k, (_, s) in enumerate(made):
+            assert not s.done
+            r = s.step()
+            assert r.iteration == fresh[k][0][0].iteration
+            assert abs(r.compliance - fresh[k][0][0].compliance) <= 1e-5 * abs(fresh[k][0][0].compliance)
+    finally:
+        for p, s in made:
+            s.close()
+            p.close()
