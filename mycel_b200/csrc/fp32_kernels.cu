@@ -5127,6 +5127,42 @@ static int32_t pk_set(mycel_ctx* c, const PackPlan& P, const std::vector<signed 
   return MYCEL_OK;
 }
 
+// The right-hand sides of one problem: its single solve's vectors (ncase 1) or its load cases' (0 .. ncase-1)
+static void pk_add_units(mycel_problem* p, int job, int ncase, double* d_u, std::vector<PkUnit>* out) {
+  MgHier* mg = p->mg;
+  const int64_t nd = p->g.nd;
+  for (int k = 0; k < ncase; ++k) {
+    PkUnit u{};
+    u.p = p;
+    u.job = job;
+    if (ncase == 1) {
+      u.k = -1;
+      u.x = p->f_x; u.r = p->f_r; u.z = p->f_z; u.p0 = p->f_p0; u.p1 = p->f_p1; u.ap = p->f_ap; u.t = mg->f_t;
+      u.tz = &p->f_tmap[1];
+      u.tp0 = &p->f_tmap[2];
+      u.tp1 = &p->f_tmap[3];
+      u.st = mix_state(p);
+      u.b = p->d_b;
+      u.bnz = p->d_bnz;
+      u.nbnz = p->n_bnz;
+      u.u = d_u;
+    } else {
+      u.k = k;
+      u.x = cwv(mg, k, 0); u.r = cwv(mg, k, 1); u.z = cwv(mg, k, 2); u.p0 = cwv(mg, k, 3); u.p1 = cwv(mg, k, 4);
+      u.ap = cwv(mg, k, 5); u.t = cwv(mg, k, 6);
+      u.tz = &mg->cw.tmap[k][1];
+      u.tp0 = &mg->cw.tmap[k][2];
+      u.tp1 = &mg->cw.tmap[k][3];
+      u.st = mg->cw.st + k;
+      u.b = p->d_case_b + (int64_t)k * nd;
+      u.bnz = p->d_case_nz + p->case_nz_off[2 * k + 1];
+      u.nbnz = p->case_nz_cnt[2 * k + 1];
+      u.u = d_u + (int64_t)k * nd;
+    }
+    out->push_back(u);
+  }
+}
+
 int32_t mg_solve_packed(mycel_ctx* c, int njobs, PackJob* jobs, const volatile int32_t* cancel) {
   cudaStream_t s = c->stream;
   auto t0 = std::chrono::steady_clock::now();
@@ -5187,37 +5223,7 @@ int32_t mg_solve_packed(mycel_ctx* c, int njobs, PackJob* jobs, const volatile i
     MgHier* mg = p->mg;
     MYCEL_CUDA(c, cudaMemsetAsync(p->d_err, 0, sizeof(int), s));
     if (mg->setup_version != p->e_version) need_setup.push_back(p);
-    const int64_t nd = p->g.nd;
-    for (int k = 0; k < J.ncase; ++k) {
-      PkUnit u{};
-      u.p = p;
-      u.job = j;
-      if (J.ncase == 1) {
-        u.k = -1;
-        u.x = p->f_x; u.r = p->f_r; u.z = p->f_z; u.p0 = p->f_p0; u.p1 = p->f_p1; u.ap = p->f_ap; u.t = mg->f_t;
-        u.tz = &p->f_tmap[1];
-        u.tp0 = &p->f_tmap[2];
-        u.tp1 = &p->f_tmap[3];
-        u.st = mix_state(p);
-        u.b = p->d_b;
-        u.bnz = p->d_bnz;
-        u.nbnz = p->n_bnz;
-        u.u = J.d_u;
-      } else {
-        u.k = k;
-        u.x = cwv(mg, k, 0); u.r = cwv(mg, k, 1); u.z = cwv(mg, k, 2); u.p0 = cwv(mg, k, 3); u.p1 = cwv(mg, k, 4);
-        u.ap = cwv(mg, k, 5); u.t = cwv(mg, k, 6);
-        u.tz = &mg->cw.tmap[k][1];
-        u.tp0 = &mg->cw.tmap[k][2];
-        u.tp1 = &mg->cw.tmap[k][3];
-        u.st = mg->cw.st + k;
-        u.b = p->d_case_b + (int64_t)k * nd;
-        u.bnz = p->d_case_nz + p->case_nz_off[2 * k + 1];
-        u.nbnz = p->case_nz_cnt[2 * k + 1];
-        u.u = J.d_u + (int64_t)k * nd;
-      }
-      units.push_back(u);
-    }
+    pk_add_units(p, j, J.ncase, J.d_u, &units);
   }
   // the coarse operators of the packed problems, rebuilt from their new E side by side on the fan's streams
   if (!need_setup.empty()) {
@@ -5541,41 +5547,10 @@ int32_t pkr_open(mycel_ctx* c, const std::vector<PackRunJob>& jobs, PackRun** ou
     }
     if (nc > 1 && (st = mg_ensure_cases(p, nc))) return st;
     (*packed)[j] = 1;
-    MgHier* mg = p->mg;
-    const int64_t nd = p->g.nd;
     r->jp.push_back(p);
     r->ju0.push_back((int)r->units.size());
     r->jnc.push_back(nc);
-    for (int k = 0; k < nc; ++k) {
-      PkUnit u{};
-      u.p = p;
-      u.job = (int)j;
-      if (nc == 1) {
-        u.k = -1;
-        u.x = p->f_x; u.r = p->f_r; u.z = p->f_z; u.p0 = p->f_p0; u.p1 = p->f_p1; u.ap = p->f_ap; u.t = mg->f_t;
-        u.tz = &p->f_tmap[1];
-        u.tp0 = &p->f_tmap[2];
-        u.tp1 = &p->f_tmap[3];
-        u.st = mix_state(p);
-        u.b = p->d_b;
-        u.bnz = p->d_bnz;
-        u.nbnz = p->n_bnz;
-        u.u = jobs[j].d_u;
-      } else {
-        u.k = k;
-        u.x = cwv(mg, k, 0); u.r = cwv(mg, k, 1); u.z = cwv(mg, k, 2); u.p0 = cwv(mg, k, 3); u.p1 = cwv(mg, k, 4);
-        u.ap = cwv(mg, k, 5); u.t = cwv(mg, k, 6);
-        u.tz = &mg->cw.tmap[k][1];
-        u.tp0 = &mg->cw.tmap[k][2];
-        u.tp1 = &mg->cw.tmap[k][3];
-        u.st = mg->cw.st + k;
-        u.b = p->d_case_b + (int64_t)k * nd;
-        u.bnz = p->d_case_nz + p->case_nz_off[2 * k + 1];
-        u.nbnz = p->case_nz_cnt[2 * k + 1];
-        u.u = jobs[j].d_u + (int64_t)k * nd;
-      }
-      r->units.push_back(u);
-    }
+    pk_add_units(p, (int)j, nc, jobs[j].d_u, &r->units);
   }
   const int nu = (int)r->units.size();
   if (nu == 0) return set_error(c, MYCEL_E_ARG, "packed run: no problem the packed form can take");
