@@ -102,7 +102,10 @@ typedef struct {
   int32_t fallback_iterations;
 } mycel_pcg_result;
 
-/* StaticAnalysisOptions (Fem/StaticAnalysis.cs:8-17); the preconditioner is Jacobi. */
+/* StaticAnalysisOptions (Fem/StaticAnalysis.cs:8-17). The reference's IPreconditioner option
+   (Fem/IPreconditioner.cs:9-20, default JacobiPreconditioner at Fem/StaticAnalysis.cs:74) is carried by
+   precision: the FP64 forms and the mixed forms precondition with Jacobi, the MG forms with the geometric
+   multigrid; a managed preconditioner has no device counterpart. */
 typedef struct {
   double tolerance;        /* default 1e-6 */
   int32_t max_iterations;  /* default 5000 */
