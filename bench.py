@@ -679,7 +679,8 @@ def run_mycel(args):
             (model.grid.nz // 2 + 1 + model.grid.nz % 2)  # nodes of the level-1 grid (element counts halved, rounded up)
         l1_bytes = 552.0 * l1_nodes
         l1_ach = l1_bytes / (kb_l1 * 1e-6) / 1e9
-        roof_l1 = {"kernel": "k_mg_apply_nodes (multigrid level-1 residual product, thread per node)", "bound": "hbm",
+        roof_l1 = {"kernel": "k_mg_apply_nodes_tma (multigrid level-1 residual product, stencil staged by TMA)",
+                   "bound": "hbm",
                    "achieved": l1_ach, "peak": hbm, "unit": "GB/s", "frac": l1_ach / hbm,
                    "traffic": NCU_DRAM_BYTES.get(("mg-level1", args.precision, args.workload)),
                    "peak_source": "measured" if pk else "fallback", "avg_launch_us": kb_l1,

@@ -1307,7 +1307,7 @@ constexpr int kTcPadSmem = 20 * 1024;
 
 // TMA descriptor of a work vector: 3-D [nz1][ny1][pitch] elements (floats: pitch rp, box [1][FPY][FBW];
 // doubles: pitch rp64, box [1][FPY][FBW64]), zero fill outside.
-static int32_t encode_plane_map(mycel_problem* p, void* base, bool f64, CUtensorMap* out) {
+static PFN_cuTensorMapEncodeTiled tensor_map_encoder() {
   static PFN_cuTensorMapEncodeTiled encode = nullptr;
   static std::once_flag once;
   std::call_once(once, [] {
@@ -1317,6 +1317,11 @@ static int32_t encode_plane_map(mycel_problem* p, void* base, bool f64, CUtensor
         q == cudaDriverEntryPointSuccess)
       encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled>(fn);
   });
+  return encode;
+}
+
+static int32_t encode_plane_map(mycel_problem* p, void* base, bool f64, CUtensorMap* out) {
+  const PFN_cuTensorMapEncodeTiled encode = tensor_map_encoder();
   if (!encode) return set_error(p->ctx, MYCEL_E_DEVICE, "cuTensorMapEncodeTiled is not available from the driver");
   const GridDims& g = p->g;
   const cuuint64_t pitch = f64 ? (cuuint64_t)g.rp64 : (cuuint64_t)g.rp, es = f64 ? 8 : 4;
@@ -1754,6 +1759,9 @@ __host__ __device__ __forceinline__ MgPtrs mg_one(float* v) {
 __host__ __device__ __forceinline__ int64_t mg_nn(const MgDims& d) {
   return (int64_t)(d.nx + 1) * (d.ny + 1) * (d.nz + 1);
 }
+// row stride of a level's stencil array: the node count rounded up to 4 floats, so every row starts on a
+// 16-byte boundary (TMA rows); the padding entries stay 0
+__host__ __device__ __forceinline__ int64_t mg_ns(const MgDims& d) { return (mg_nn(d) + 3) & ~int64_t(3); }
 
 // per-axis interpolation weight of coarse node c at fine node f, for a fine axis of n elements
 __device__ __forceinline__ float mg_pw(int f, int c, int n) {
@@ -1896,7 +1904,7 @@ __global__ void __launch_bounds__(256) k_mg_build1(MgDims c, MgDims f, const flo
 
 // Assembled 27-point stencil of a level from its element matrices, in symmetric half storage: node n keeps the
 // blocks of its neighbours nb = 13 .. 26 (itself and the 13 neighbours later in node order), nb = (dx+1) +
-// 3 (dy+1) + 9 (dz+1); S[((nb - 13) * 9 + 3 ci + cj) * nn + n] is the entry (DOF ci of node n, DOF cj of
+// 3 (dy+1) + 9 (dz+1); S[((nb - 13) * 9 + 3 ci + cj) * ns + n] is the entry (DOF ci of node n, DOF cj of
 // neighbour nb). The block of an earlier neighbour m is the transpose of m's block for offset 26 - nb. Also
 // 1/diag (0 where the diagonal is 0: DOFs no free fine DOF reaches).
 constexpr int kMgHalf = 14;  // stored blocks per node
@@ -1936,7 +1944,7 @@ __global__ void __launch_bounds__(256) k_mg_stencil(MgDims d, const float* __res
 #pragma unroll
   for (int h = 0; h < kMgHalf; ++h)
 #pragma unroll
-    for (int cj = 0; cj < 3; ++cj) S[((int64_t)h * 9 + 3 * ci + cj) * nn + n] = acc[h][cj];
+    for (int cj = 0; cj < 3; ++cj) S[((int64_t)h * 9 + 3 * ci + cj) * mg_ns(d) + n] = acc[h][cj];
   const float dg = ci == 0 ? acc[0][0] : (ci == 1 ? acc[0][1] : acc[0][2]);  // keeps acc in registers
   invd[3 * n + ci] = dg > 0.f ? 1.0f / dg : 0.0f;
 }
@@ -1945,13 +1953,14 @@ __global__ void __launch_bounds__(256) k_mg_stencil(MgDims d, const float* __res
 // 0-1 take component 0 of 64 consecutive nodes, warps 2-3 component 1, warps 4-5 component 2 (coalesced loads,
 // three times the threads in flight of a thread per node).
 constexpr int kMgDofThreads = 192;
+constexpr int64_t kMgDofMaxNodes = 65536;  // levels (x cases) up to this many nodes: a thread per DOF
 __device__ __forceinline__ int64_t mg_dof_node() { return blockIdx.x * (int64_t)64 + (threadIdx.x & 63); }
 __device__ __forceinline__ int mg_dof_comp() { return threadIdx.x >> 6; }
 static inline unsigned mg_dof_blocks(int64_t nn) { return (unsigned)((nn + 63) / 64); }
 
-// coarse-level product at node n by gather. mode 0: y = A x; 1: y = x + omega invd (r - A x) (one Jacobi
-// sweep); 2: y = r - A x on DOFs with a nonzero diagonal, 0 elsewhere
-__device__ __forceinline__ void mg_apply_node(const MgDims& d, int64_t nn, int64_t n, const float* __restrict__ S,
+// coarse-level product at node n by gather (ns: the stencil's row stride). mode 0: y = A x; 1: y = x + omega
+// invd (r - A x) (one Jacobi sweep); 2: y = r - A x on DOFs with a nonzero diagonal, 0 elsewhere
+__device__ __forceinline__ void mg_apply_node(const MgDims& d, int64_t ns, int64_t n, const float* __restrict__ S,
                                               const float* __restrict__ x, const float* __restrict__ r,
                                               const float* __restrict__ invd, float* __restrict__ y, int mode,
                                               float omega) {
@@ -1969,15 +1978,15 @@ __device__ __forceinline__ void mg_apply_node(const MgDims& d, int64_t nn, int64
     const int64_t m = mi + (int64_t)nx1 * (mj + (int64_t)ny1 * mk);
     const float x0 = in ? x[3 * m] : 0.f, x1 = in ? x[3 * m + 1] : 0.f, x2 = in ? x[3 * m + 2] : 0.f;
     if (nb >= 13) {
-      const float* s = S + (int64_t)(nb - 13) * 9 * nn + n;
-      a0 = fmaf(s[0], x0, fmaf(s[nn], x1, fmaf(s[2 * nn], x2, a0)));
-      a1 = fmaf(s[3 * nn], x0, fmaf(s[4 * nn], x1, fmaf(s[5 * nn], x2, a1)));
-      a2 = fmaf(s[6 * nn], x0, fmaf(s[7 * nn], x1, fmaf(s[8 * nn], x2, a2)));
+      const float* s = S + (int64_t)(nb - 13) * 9 * ns + n;
+      a0 = fmaf(s[0], x0, fmaf(s[ns], x1, fmaf(s[2 * ns], x2, a0)));
+      a1 = fmaf(s[3 * ns], x0, fmaf(s[4 * ns], x1, fmaf(s[5 * ns], x2, a1)));
+      a2 = fmaf(s[6 * ns], x0, fmaf(s[7 * ns], x1, fmaf(s[8 * ns], x2, a2)));
     } else {
-      const float* s = S + (int64_t)(13 - nb) * 9 * nn + m;
-      a0 = fmaf(s[0], x0, fmaf(s[3 * nn], x1, fmaf(s[6 * nn], x2, a0)));
-      a1 = fmaf(s[nn], x0, fmaf(s[4 * nn], x1, fmaf(s[7 * nn], x2, a1)));
-      a2 = fmaf(s[2 * nn], x0, fmaf(s[5 * nn], x1, fmaf(s[8 * nn], x2, a2)));
+      const float* s = S + (int64_t)(13 - nb) * 9 * ns + m;
+      a0 = fmaf(s[0], x0, fmaf(s[3 * ns], x1, fmaf(s[6 * ns], x2, a0)));
+      a1 = fmaf(s[ns], x0, fmaf(s[4 * ns], x1, fmaf(s[7 * ns], x2, a1)));
+      a2 = fmaf(s[2 * ns], x0, fmaf(s[5 * ns], x1, fmaf(s[8 * ns], x2, a2)));
     }
   }
   const float acc[3] = {a0, a1, a2};
@@ -1991,7 +2000,7 @@ __device__ __forceinline__ void mg_apply_node(const MgDims& d, int64_t nn, int64
 }
 
 // the same for one row (DOF ci of node n): a third of the loads of a node
-__device__ __forceinline__ void mg_apply_row(const MgDims& d, int64_t nn, int64_t n, int ci,
+__device__ __forceinline__ void mg_apply_row(const MgDims& d, int64_t ns, int64_t n, int ci,
                                              const float* __restrict__ S, const float* __restrict__ x,
                                              const float* __restrict__ r, const float* __restrict__ invd,
                                              float* __restrict__ y, int mode, float omega) {
@@ -2006,11 +2015,11 @@ __device__ __forceinline__ void mg_apply_row(const MgDims& d, int64_t nn, int64_
     const int64_t m = mi + (int64_t)nx1 * (mj + (int64_t)ny1 * mk);
     const float x0 = in ? x[3 * m] : 0.f, x1 = in ? x[3 * m + 1] : 0.f, x2 = in ? x[3 * m + 2] : 0.f;
     if (nb >= 13) {
-      const float* s = S + ((int64_t)(nb - 13) * 9 + 3 * ci) * nn + n;
-      a = fmaf(s[0], x0, fmaf(s[nn], x1, fmaf(s[2 * nn], x2, a)));
+      const float* s = S + ((int64_t)(nb - 13) * 9 + 3 * ci) * ns + n;
+      a = fmaf(s[0], x0, fmaf(s[ns], x1, fmaf(s[2 * ns], x2, a)));
     } else {
-      const float* s = S + ((int64_t)(13 - nb) * 9 + ci) * nn + m;
-      a = fmaf(s[0], x0, fmaf(s[3 * nn], x1, fmaf(s[6 * nn], x2, a)));
+      const float* s = S + ((int64_t)(13 - nb) * 9 + ci) * ns + m;
+      a = fmaf(s[0], x0, fmaf(s[3 * ns], x1, fmaf(s[6 * ns], x2, a)));
     }
   }
   const int64_t q = 3 * n + ci;
@@ -2034,7 +2043,7 @@ __global__ void __launch_bounds__(256) k_mg_apply_nodes(MgDims d, const float* _
   int c;
   mg_item_case<MULTI>(blockIdx.x * (int64_t)blockDim.x + threadIdx.x, ncase, &n, &c);
   if (n >= nn || !mg_running(st ? st + c : nullptr)) return;
-  mg_apply_node(d, nn, n, S, x.p[c], r.p[c], invd, y.p[c], mode, mode == 1 ? *om : 0.0f);
+  mg_apply_node(d, mg_ns(d), n, S, x.p[c], r.p[c], invd, y.p[c], mode, mode == 1 ? *om : 0.0f);
 }
 
 template <bool MULTI>
@@ -2050,7 +2059,120 @@ __global__ void __launch_bounds__(kMgDofThreads) k_mg_apply(MgDims d, const floa
   int c;
   mg_item_case<MULTI>(mg_dof_node(), ncase, &n, &c);
   if (n >= nn || !mg_running(st ? st + c : nullptr)) return;
-  mg_apply_row(d, nn, n, mg_dof_comp(), S, x.p[c], r.p[c], invd, y.p[c], mode, mode == 1 ? *om : 0.0f);
+  mg_apply_row(d, mg_ns(d), n, mg_dof_comp(), S, x.p[c], r.p[c], invd, y.p[c], mode, mode == 1 ? *om : 0.0f);
+}
+
+// Coarse-level product of a large level (one case) with the stencil streamed into shared memory by TMA: the
+// thread-per-node gather above holds at most a few of its 243 stencil loads in flight and waits on them (load
+// latency, not bandwidth, bounds it). Here a CTA takes kS1Nodes consecutive nodes and brings, neighbour by
+// neighbour in the gather's order, the 9 stencil rows every thread needs for that neighbour as one 2-D box of
+// [9 rows][kS1Box nodes]: the nodes' own rows (nb >= 13), or the transposed rows the earlier neighbour stores
+// (nb < 13: the CTA's nodes shifted by the neighbour's offset; the box starts at that node rounded down to 16
+// bytes and each thread reads at its remainder). kS1Stages boxes are in flight; a group of kS1Group neighbours
+// is released by one CTA barrier. Each product is the same fmaf chain in the same order as mg_apply_node, so
+// the results are bit-identical to it: where the neighbour lies outside the grid, x is 0 and the staged value
+// (another node's entry, the zero padding or TMA's zero fill) is finite.
+constexpr int kS1Nodes = 252;   // nodes per CTA (+ up to 3 of rounding <= kS1Box)
+constexpr int kS1Box = 256;     // staged nodes per row
+constexpr int kS1Stages = 6;
+constexpr int kS1Group = 3;
+constexpr int kS1StageBytes = 9 * kS1Box * 4;
+constexpr int kS1Smem = kS1Stages * kS1StageBytes;
+static_assert(kS1Stages % kS1Group == 0 && 27 % kS1Group == 0, "stage groups");
+static_assert(kS1Nodes % 4 == 0 && kS1Nodes + 3 < kS1Box, "TMA boxes: 16-byte aligned starts cover the CTA");
+
+__global__ void __launch_bounds__(256) k_mg_apply_nodes_tma(MgDims d, const __grid_constant__ CUtensorMap tm,
+                                                            const float* __restrict__ x, const float* __restrict__ r,
+                                                            const float* __restrict__ invd, float* __restrict__ y,
+                                                            int mode, const float* __restrict__ om,
+                                                            const MixState* st, int* err) {
+  extern __shared__ __align__(128) unsigned char s1_smem[];
+  __shared__ __align__(8) unsigned long long full[kS1Stages];
+  if (!mg_running(st)) return;  // one case: the same for every CTA
+  const int64_t nn = mg_nn(d);
+  const int tid = threadIdx.x;
+  const int64_t n0 = (int64_t)blockIdx.x * kS1Nodes, n = n0 + tid;
+  const int nx1 = d.nx + 1, ny1 = d.ny + 1;
+  const int64_t sxy = (int64_t)nx1 * ny1;
+  // node whose entries thread 0 uses in block nb
+  auto first = [&](int nb) -> int64_t {
+    return nb >= 13 ? n0 : n0 + (nb % 3 - 1) + (int64_t)nx1 * ((nb / 3) % 3 - 1) + sxy * (nb / 9 - 1);
+  };
+  auto issue = [&](int nb) {  // one thread
+    const int sl = nb % kS1Stages;
+    const uint32_t bar = smem_u32(&full[sl]);
+    const int xs = (int)(first(nb) & ~int64_t(3));  // 16-byte aligned start (may be negative: zero fill)
+    const int row = nb >= 13 ? (nb - 13) * 9 : (13 - nb) * 9;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"((uint32_t)kS1StageBytes)
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n"
+        ::"r"(smem_u32(s1_smem + (size_t)sl * kS1StageBytes)), "l"(reinterpret_cast<uint64_t>(&tm)), "r"(xs), "r"(row),
+        "r"(bar)
+        : "memory");
+  };
+  if (tid == 0) {
+    for (int q = 0; q < kS1Stages; ++q)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&full[q])) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  }
+  __syncthreads();
+  bool ok = true;
+  if (tid == 0)
+    for (int nb = 0; nb < kS1Stages; ++nb) issue(nb);
+  const bool act = tid < kS1Nodes && n < nn;
+  const int ts = tid < kS1Nodes ? tid : 0;  // staged column read (threads past kS1Nodes read column 0..3)
+  const int64_t nc = act ? n : 0;
+  const int i = (int)(nc % nx1), j = (int)((nc / nx1) % ny1), k = (int)(nc / sxy);
+  float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+#pragma unroll
+  for (int g = 0; g < 27 / kS1Group; ++g) {
+#pragma unroll
+    for (int q = 0; q < kS1Group; ++q) {
+      const int nb = kS1Group * g + q;
+      const int sl = nb % kS1Stages;
+      if (!mbar_wait(smem_u32(&full[sl]), (uint32_t)((nb / kS1Stages) & 1))) ok = false;
+      const int ui = i + nb % 3 - 1, uj = j + (nb / 3) % 3 - 1, uk = k + nb / 9 - 1;
+      const int mi = min(max(ui, 0), d.nx), mj = min(max(uj, 0), d.ny), mk = min(max(uk, 0), d.nz);
+      const bool in = act && mi == ui && mj == uj && mk == uk;
+      const int64_t m = mi + (int64_t)nx1 * (mj + (int64_t)ny1 * mk);
+      const float x0 = in ? x[3 * m] : 0.f, x1 = in ? x[3 * m + 1] : 0.f, x2 = in ? x[3 * m + 2] : 0.f;
+      const float* s = reinterpret_cast<const float*>(s1_smem + (size_t)sl * kS1StageBytes) + ts +
+                       (int)(first(nb) & 3);
+      if (nb >= 13) {
+        a0 = fmaf(s[0], x0, fmaf(s[kS1Box], x1, fmaf(s[2 * kS1Box], x2, a0)));
+        a1 = fmaf(s[3 * kS1Box], x0, fmaf(s[4 * kS1Box], x1, fmaf(s[5 * kS1Box], x2, a1)));
+        a2 = fmaf(s[6 * kS1Box], x0, fmaf(s[7 * kS1Box], x1, fmaf(s[8 * kS1Box], x2, a2)));
+      } else {
+        a0 = fmaf(s[0], x0, fmaf(s[3 * kS1Box], x1, fmaf(s[6 * kS1Box], x2, a0)));
+        a1 = fmaf(s[kS1Box], x0, fmaf(s[4 * kS1Box], x1, fmaf(s[7 * kS1Box], x2, a1)));
+        a2 = fmaf(s[2 * kS1Box], x0, fmaf(s[5 * kS1Box], x1, fmaf(s[8 * kS1Box], x2, a2)));
+      }
+    }
+    if (kS1Group * (g + 1) + kS1Stages - kS1Group < 27) {  // a later group reuses these stages
+      __syncthreads();
+      // a wait that gave up leaves its copy possibly in flight: issue nothing more into the stages
+      if (tid == 0 && ok) {
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+#pragma unroll
+        for (int q = 0; q < kS1Group; ++q) {
+          const int nb = kS1Group * g + kS1Stages + q;
+          if (nb < 27) issue(nb);
+        }
+      }
+    }
+  }
+  if (!ok && err) atomicExch(err, 1);
+  if (!act) return;
+  const float acc[3] = {a0, a1, a2};
+#pragma unroll
+  for (int cc = 0; cc < 3; ++cc) {
+    const int64_t q = 3 * n + cc;
+    if (mode == 0) y[q] = acc[cc];
+    else if (mode == 1) y[q] = fmaf(*om * invd[q], r[q] - acc[cc], x[q]);
+    else y[q] = invd[q] != 0.0f ? r[q] - acc[cc] : 0.0f;
+  }
 }
 
 // a further sweep on the voxel grid (padded FP32 layout, t = A x): x += omega invd (r - t)
@@ -2265,7 +2387,7 @@ __global__ void k_mg_prolong(MgDims f, int pitch, const uint8_t* __restrict__ nf
 __global__ void __launch_bounds__(1024) k_mg_coarse_setup(MgDims d, const float* __restrict__ S,
                                                           double* __restrict__ ainv) {
   extern __shared__ __align__(16) unsigned char mg_smem[];
-  const int64_t nn = mg_nn(d);
+  const int64_t nn = mg_nn(d), ns = mg_ns(d);
   const int n = (int)(3 * nn);
   double* A = reinterpret_cast<double*>(mg_smem);
   double* dg = A + (size_t)n * n;
@@ -2278,7 +2400,7 @@ __global__ void __launch_bounds__(1024) k_mg_coarse_setup(MgDims d, const float*
     double v = 0.0;
     if (dx >= -1 && dx <= 1 && dy >= -1 && dy <= 1 && dz >= -1 && dz <= 1) {
       const int nb = (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1);
-      v = nb >= 13 ? (double)S[((nb - 13) * 9 + 3 * ci + cj) * nn + a] : (double)S[((13 - nb) * 9 + 3 * cj + ci) * nn + b];
+      v = nb >= 13 ? (double)S[((nb - 13) * 9 + 3 * ci + cj) * ns + a] : (double)S[((13 - nb) * 9 + 3 * cj + ci) * ns + b];
     }
     A[o] = v;
   }
@@ -2384,14 +2506,15 @@ __device__ __forceinline__ void mg_tail_body(const MgTail& tl, const float* __re
         int k;
         mg_item_case<MULTI>(t, ncase, &it, &k);
         if (live(k))
-          mg_apply_row(v.d, v.nn, it / 3, (int)(it % 3), v.S, x + k * nd, v.r + k * nd, v.invd, y + k * nd, mode, w);
+          mg_apply_row(v.d, mg_ns(v.d), it / 3, (int)(it % 3), v.S, x + k * nd, v.r + k * nd, v.invd, y + k * nd,
+                       mode, w);
       }
     } else {
       for (int64_t t = gt; t < v.nn * ncase; t += gs) {
         int64_t n;
         int k;
         mg_item_case<MULTI>(t, ncase, &n, &k);
-        if (live(k)) mg_apply_node(v.d, v.nn, n, v.S, x + k * nd, v.r + k * nd, v.invd, y + k * nd, mode, w);
+        if (live(k)) mg_apply_node(v.d, mg_ns(v.d), n, v.S, x + k * nd, v.r + k * nd, v.invd, y + k * nd, mode, w);
       }
     }
   };
@@ -2862,6 +2985,9 @@ struct MgLevel {
   MgDims d{};
   int64_t nn = 0, nd = 0;
   float *S = nullptr, *invd = nullptr, *xa = nullptr, *xb = nullptr, *r = nullptr, *t = nullptr;
+  bool staged = false;  // products of one case by k_mg_apply_nodes_tma through tm_s
+  int* err = nullptr;   // the problem's bounded-wait error word
+  CUtensorMap tm_s{};   // the stencil as a 2-D tensor [126 rows][ns nodes], boxes of [9][kS1Box]
 };
 
 struct MgHier {
@@ -2933,7 +3059,7 @@ int64_t mg_device_bytes(int nx, int ny, int nz, int n_cases, bool cases_together
   if (!L) return 0;
   const int nc = std::min(kMgMaxCases, std::max(1, n_cases));  // level vectors have room for the cases
   int64_t b = 0;
-  for (int l = 1; l < L; ++l) b += 4 * (9 * kMgHalf + 3 + 12 * nc) * mg_nn(lv[l]) + 6 * 64;
+  for (int l = 1; l < L; ++l) b += 4 * (9 * kMgHalf * mg_ns(lv[l]) + (3 + 12 * nc) * mg_nn(lv[l])) + 6 * 64;
   b += sizeof(MgScratch) + 64 + 4 * 8 * 576 + 64 + (int64_t)lv[1].nx * lv[1].ny * lv[1].nz + 64;
   const int64_t rp = (3 * (int64_t)(nx + 1) + 3) & ~int64_t(3);  // FP32 row pitch of the voxel level
   b += 4 * rp * (ny + 1) * (nz + 1) + 64;                         // f_t
@@ -2973,6 +3099,10 @@ static int32_t mg_ensure(mycel_problem* p, bool* available) {
   static cudaError_t smem_err = cudaSuccess;
   std::call_once(smem_once, [] {
     smem_err = cudaFuncSetAttribute(k_mg_coarse_setup, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMgCoarseSmem);
+    if (smem_err == cudaSuccess)
+      smem_err = cudaFuncSetAttribute(k_mg_apply_nodes_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, kS1Smem);
+    if (smem_err == cudaSuccess)  // four CTAs of 54 KB per SM
+      smem_err = cudaFuncSetAttribute(k_mg_apply_nodes_tma, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
   });
   if (smem_err != cudaSuccess)
     return set_error(p->ctx, MYCEL_E_DEVICE, std::string("multigrid shared memory: ") + cudaGetErrorString(smem_err));
@@ -3007,8 +3137,20 @@ static int32_t mg_ensure(mycel_problem* p, bool* available) {
     v.nn = mg_nn(v.d);
     v.nd = 3 * v.nn;
     if (l == 0) continue;
-    v.S = (float*)alloc(sizeof(float) * 9 * kMgHalf * v.nn);
+    v.S = (float*)alloc(sizeof(float) * 9 * kMgHalf * mg_ns(v.d));  // zeroed: the row padding stays 0
     v.invd = (float*)alloc(sizeof(float) * v.nd);
+    v.err = p->d_err;
+    if (v.S && v.nn > kMgDofMaxNodes) {  // the levels whose products run a thread per node
+      const PFN_cuTensorMapEncodeTiled encode = tensor_map_encoder();
+      cuuint64_t dims[2] = {(cuuint64_t)mg_ns(v.d), (cuuint64_t)(9 * kMgHalf)};
+      cuuint64_t strides[1] = {(cuuint64_t)mg_ns(v.d) * 4};
+      cuuint32_t box[2] = {(cuuint32_t)kS1Box, 9};
+      cuuint32_t estr[2] = {1, 1};
+      v.staged = encode && mg_ns(v.d) < (int64_t)INT32_MAX - kS1Box &&
+                 encode(&v.tm_s, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, v.S, dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+    }
     float** vecs[] = {&v.xa, &v.xb, &v.r, &v.t};
     for (float** q : vecs) *q = (float*)alloc(sizeof(float) * v.nd * mg->ncap);
   }
@@ -3131,9 +3273,12 @@ static MgPtrs lv_ptrs(float* base, int64_t nd, int n) {
 
 static void launch_mg_apply(cudaStream_t s, const MgLevel& v, const MgPtrs& x, const MgPtrs& r, const float* invd,
                             const MgPtrs& y, int mode, const float* om, const MixState* st, int nc) {
-  if (v.nn * nc <= 65536)
+  if (v.nn * nc <= kMgDofMaxNodes)
     (nc == 1 ? k_mg_apply<false> : k_mg_apply<true>)<<<mg_dof_blocks(v.nn * nc), kMgDofThreads, 0, s>>>(
         v.d, v.S, x, r, invd, y, mode, om, st, nc);
+  else if (nc == 1 && v.staged)
+    k_mg_apply_nodes_tma<<<(unsigned)((v.nn + kS1Nodes - 1) / kS1Nodes), 256, kS1Smem, s>>>(
+        v.d, v.tm_s, x.p[0], r.p[0], invd, y.p[0], mode, om, st, v.err);
   else
     (nc == 1 ? k_mg_apply_nodes<false> : k_mg_apply_nodes<true>)<<<mg_blocks(v.nn * nc), 256, 0, s>>>(
         v.d, v.S, x, r, invd, y, mode, om, st, nc);
@@ -4376,7 +4521,7 @@ __global__ void __launch_bounds__(256) k_mg_apply_nodes_pk(const PkApply* __rest
     int c;
     mg_item_case<MULTI>((int64_t)(code & kPkLbMask) * blockDim.x + threadIdx.x, a.ncase, &q, &c);
     if (q >= nn || !mg_running(a.st ? a.st + c : nullptr)) continue;
-    mg_apply_node(a.d, nn, q, a.S, a.x.p[c], a.r.p[c], a.invd, a.y.p[c], mode, mode == 1 ? *a.om : 0.0f);
+    mg_apply_node(a.d, mg_ns(a.d), q, a.S, a.x.p[c], a.r.p[c], a.invd, a.y.p[c], mode, mode == 1 ? *a.om : 0.0f);
   }
 }
 
@@ -4393,7 +4538,7 @@ __global__ void __launch_bounds__(kMgDofThreads) k_mg_apply_pk(const PkApply* __
     int c;
     mg_item_case<MULTI>((int64_t)(code & kPkLbMask) * 64 + (threadIdx.x & 63), a.ncase, &q, &c);
     if (q >= nn || !mg_running(a.st ? a.st + c : nullptr)) continue;
-    mg_apply_row(a.d, nn, q, (int)(threadIdx.x >> 6), a.S, a.x.p[c], a.r.p[c], a.invd, a.y.p[c], mode,
+    mg_apply_row(a.d, mg_ns(a.d), q, (int)(threadIdx.x >> 6), a.S, a.x.p[c], a.r.p[c], a.invd, a.y.p[c], mode,
                  mode == 1 ? *a.om : 0.0f);
   }
 }
@@ -4914,7 +5059,7 @@ static int32_t pk_build(mycel_ctx* c, PackWork* w, std::vector<PkUnit>& units, c
           MgHier* mg = q.p->mg;
           if (l >= mg->T || (q.nc > 1) != (multi == 1)) continue;
           const MgLevel& v = mg->lv[l];
-          const bool is_node = !(v.nn * q.nc <= 65536);
+          const bool is_node = !(v.nn * q.nc <= kMgDofMaxNodes);
           if (is_node != (node == 1)) continue;
           PkApply a{};
           a.d = v.d;

@@ -231,3 +231,17 @@ def test_run_many_cancelled_then_stepped_alone(ctx):
         for p, s in made:
             s.close()
             p.close()
+
+
+def test_staged_level_product_equals_the_gather(ctx):
+    """Coarse levels of more than 64k nodes: alone, their products run with the stencil staged by TMA
+    (k_mg_apply_nodes_tma); packed, by the thread-per-node gather (k_mg_apply_nodes_pk). The two must give the
+    same bits: an even bridge and an odd-sized cantilever (level 1: 81x41x21 and 82x42x22 nodes)."""
+    o = OptimizerOptions(volume_fraction=0.3, filter_radius_mm=1.5, max_iterations=2, precision="mixed-mg",
+                         solver_tolerance_initial=1e-6, solver_tolerance_final=1e-6, solver_max_iterations=20000)
+    jobs = [(W.bridge(160, 80, 40, support=6, load_patch=10), o),
+            (W.cantilever(161, 81, 41, e0=1.0, emin_ratio=1e-9, force=-1.0), o.replace(volume_fraction=0.2))]
+    alone = [_alone(ctx, m, jo, 2) for m, jo in jobs]
+    rp, dp = _packed(ctx, jobs, 2)
+    for k, (ra, da) in enumerate(alone):
+        _same(ra, da, rp[k], dp[k])
