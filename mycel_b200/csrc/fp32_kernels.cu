@@ -1763,6 +1763,15 @@ __host__ __device__ __forceinline__ int64_t mg_nn(const MgDims& d) {
 // 16-byte boundary (TMA rows); the padding entries stay 0
 __host__ __device__ __forceinline__ int64_t mg_ns(const MgDims& d) { return (mg_nn(d) + 3) & ~int64_t(3); }
 
+// coordinates (i, j, k) of entry n of an a x b x . box (nodes or elements) by 32-bit division: every level's
+// node count is far below 2^32 (a grid that large would not fit in device memory)
+__device__ __forceinline__ void mg_ijk(int64_t n, int a, int b, int* i, int* j, int* k) {
+  const uint32_t u = (uint32_t)n, q = u / (uint32_t)a, r = q / (uint32_t)b;
+  *i = (int)(u - q * (uint32_t)a);
+  *j = (int)(q - r * (uint32_t)b);
+  *k = (int)r;
+}
+
 // per-axis interpolation weight of coarse node c at fine node f, for a fine axis of n elements
 __device__ __forceinline__ float mg_pw(int f, int c, int n) {
   if (!(f & 1)) return c == (f >> 1) ? 1.0f : 0.0f;
@@ -1789,7 +1798,8 @@ __global__ void __launch_bounds__(64) k_mg_build(MgDims c, MgDims f, const __gri
   __shared__ uint8_t fr[24];
   const int64_t e = blockIdx.x;
   if (only && !only[e]) return;  // done by k_mg_build1
-  const int ex = (int)(e % c.nx), ey = (int)((e / c.nx) % c.ny), ez = (int)(e / ((int64_t)c.nx * c.ny));
+  int ex, ey, ez;
+  mg_ijk(e, c.nx, c.ny, &ex, &ey, &ez);
   const int tid = threadIdx.x;
   float acc[9];
 #pragma unroll
@@ -1867,7 +1877,8 @@ __global__ void __launch_bounds__(256) k_mg_build1(MgDims c, MgDims f, const flo
     if (lt == 0) sp[grp] = 0;
     __syncthreads();
     if (valid) {
-      const int ex = (int)(e % c.nx), ey = (int)((e / c.nx) % c.ny), ez = (int)(e / ((int64_t)c.nx * c.ny));
+      int ex, ey, ez;
+      mg_ijk(e, c.nx, c.ny, &ex, &ey, &ez);
       if (lt < 8) {
         const int fx = 2 * ex + (lt & 1), fy = 2 * ey + ((lt >> 1) & 1), fz = 2 * ez + (lt >> 2);
         if (fx < f.nx && fy < f.ny && fz < f.nz) Es[grp][lt] = Ef[fx + (int64_t)f.nx * (fy + (int64_t)f.ny * fz)];
@@ -1919,7 +1930,8 @@ __global__ void __launch_bounds__(256) k_mg_stencil(MgDims d, const float* __res
   const int ci = (int)(t / nn);
   const int64_t n = t - ci * nn;
   const int nx1 = d.nx + 1, ny1 = d.ny + 1;
-  const int i = (int)(n % nx1), j = (int)((n / nx1) % ny1), k = (int)(n / ((int64_t)nx1 * ny1));
+  int i, j, k;
+  mg_ijk(n, nx1, ny1, &i, &j, &k);
   float acc[kMgHalf][3];
 #pragma unroll
   for (int h = 0; h < kMgHalf; ++h) acc[h][0] = acc[h][1] = acc[h][2] = 0.f;
@@ -1965,7 +1977,8 @@ __device__ __forceinline__ void mg_apply_node(const MgDims& d, int64_t ns, int64
                                               const float* __restrict__ invd, float* __restrict__ y, int mode,
                                               float omega) {
   const int nx1 = d.nx + 1, ny1 = d.ny + 1;
-  const int i = (int)(n % nx1), j = (int)((n / nx1) % ny1), k = (int)(n / ((int64_t)nx1 * ny1));
+  int i, j, k;
+  mg_ijk(n, nx1, ny1, &i, &j, &k);
   float a0 = 0.f, a1 = 0.f, a2 = 0.f;
   // all 27 blocks without branches: a neighbour outside the grid is read at a clamped (valid) node with x
   // taken as 0. Later neighbours' blocks are n's own (row ci at entries 3 ci + cj), earlier ones the transposed
@@ -2005,7 +2018,8 @@ __device__ __forceinline__ void mg_apply_row(const MgDims& d, int64_t ns, int64_
                                              const float* __restrict__ r, const float* __restrict__ invd,
                                              float* __restrict__ y, int mode, float omega) {
   const int nx1 = d.nx + 1, ny1 = d.ny + 1;
-  const int i = (int)(n % nx1), j = (int)((n / nx1) % ny1), k = (int)(n / ((int64_t)nx1 * ny1));
+  int i, j, k;
+  mg_ijk(n, nx1, ny1, &i, &j, &k);
   float a = 0.f;
 #pragma unroll
   for (int nb = 0; nb < 27; ++nb) {
@@ -2124,7 +2138,8 @@ __global__ void __launch_bounds__(256) k_mg_apply_nodes_tma(MgDims d, const __gr
   const bool act = tid < kS1Nodes && n < nn;
   const int ts = tid < kS1Nodes ? tid : 0;  // staged column read (threads past kS1Nodes read column 0..3)
   const int64_t nc = act ? n : 0;
-  const int i = (int)(nc % nx1), j = (int)((nc / nx1) % ny1), k = (int)(nc / sxy);
+  int i, j, k;
+  mg_ijk(nc, nx1, ny1, &i, &j, &k);
   float a0 = 0.f, a1 = 0.f, a2 = 0.f;
 #pragma unroll
   for (int g = 0; g < 27 / kS1Group; ++g) {
@@ -2194,7 +2209,8 @@ __device__ __forceinline__ void mg_restrict_comp(const MgDims& f, int pitch, con
                                                  const float* __restrict__ invdc, float* __restrict__ rc, int64_t n,
                                                  int cc, float* __restrict__ xc, float omega) {
   const int cx1 = c.nx + 1, cy1 = c.ny + 1;
-  const int I = (int)(n % cx1), J = (int)((n / cx1) % cy1), K = (int)(n / ((int64_t)cx1 * cy1));
+  int I, J, K;
+  mg_ijk(n, cx1, cy1, &I, &J, &K);
   const int pi = min(2 * I, f.nx), pj = min(2 * J, f.ny), pk = min(2 * K, f.nz);
   float a = 0.f;
   // the 27 candidate fine nodes around the coarse node's position, without branches: a candidate outside the
@@ -2230,7 +2246,8 @@ __device__ __forceinline__ void mg_prolong_comp(const MgDims& f, int pitch, cons
                                                 const float* __restrict__ invdf, float* __restrict__ xf,
                                                 const MgDims& c, const float* __restrict__ xc, int64_t n, int cc) {
   const int fx1 = f.nx + 1, fy1 = f.ny + 1;
-  const int i = (int)(n % fx1), j = (int)((n / fx1) % fy1), k = (int)(n / ((int64_t)fx1 * fy1));
+  int i, j, k;
+  mg_ijk(n, fx1, fy1, &i, &j, &k);
   // per axis: two coarse nodes with their weights (the second with weight 0 unless the fine node lies midway)
   int ci[2], cj[2], ck[2];
   float wi[2], wj[2], wk[2];
@@ -2268,7 +2285,8 @@ __device__ __forceinline__ void mg_restrict_node(const MgDims& f, int pitch, con
                                                  const float* __restrict__ invdc, float* __restrict__ rc, int64_t n,
                                                  float* __restrict__ xc, float omega) {
   const int cx1 = c.nx + 1, cy1 = c.ny + 1;
-  const int I = (int)(n % cx1), J = (int)((n / cx1) % cy1), K = (int)(n / ((int64_t)cx1 * cy1));
+  int I, J, K;
+  mg_ijk(n, cx1, cy1, &I, &J, &K);
   const int pi = min(2 * I, f.nx), pj = min(2 * J, f.ny), pk = min(2 * K, f.nz);
   float a0 = 0.f, a1 = 0.f, a2 = 0.f;
   // the 27 candidate fine nodes around the coarse node's position, without branches: a candidate outside the
@@ -2331,7 +2349,8 @@ __device__ __forceinline__ void mg_prolong_node(const MgDims& f, int pitch, cons
                                                 const float* __restrict__ invdf, float* __restrict__ xf,
                                                 const MgDims& c, const float* __restrict__ xc, int64_t n) {
   const int fx1 = f.nx + 1, fy1 = f.ny + 1;
-  const int i = (int)(n % fx1), j = (int)((n / fx1) % fy1), k = (int)(n / ((int64_t)fx1 * fy1));
+  int i, j, k;
+  mg_ijk(n, fx1, fy1, &i, &j, &k);
   // per axis: two coarse nodes with their weights (the second with weight 0 unless the fine node lies midway)
   int ci[2], cj[2], ck[2];
   float wi[2], wj[2], wk[2];
