@@ -52,10 +52,10 @@ FP64_PCG_PER_SIMP_ITER = {"bridge_192x96x96": 1810}
 # Mixed multigrid form (`--probe mixed-mg --probe-grid 192x96x96 --probe-variant 3`, third MODE-1 launch):
 # 53.52 MB read, 4.88 MB written.
 # Multigrid level-1 residual product (`--probe mixed-mg --probe-grid 192x96x96 --probe-variant 3`, fifth
-# k_mg_apply_nodes launch): 122.26 MB read, 4.54 MB written.
+# k_mg_apply_nodes_tma launch): 127.11 MB read, 5.62 MB written.
 NCU_DRAM_BYTES = {("mixed", 3, "bridge_192x96x96"): 53.47e6 + 5.53e6,
                   ("mixed-mg", 3, "bridge_192x96x96"): 53.52e6 + 4.88e6,
-                  ("mg-level1", "mixed-mg", "bridge_192x96x96"): 122.26e6 + 4.54e6}
+                  ("mg-level1", "mixed-mg", "bridge_192x96x96"): 127.11e6 + 5.62e6}
 
 
 def parse():
