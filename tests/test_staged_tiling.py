@@ -85,7 +85,7 @@ def _check_level(nx, ny, nz):
     assert np.all(cover == 1)
 
 
-GRIDS = [(192, 96, 96), (160, 80, 40), (161, 81, 41), (128, 128, 8), (200, 67, 33), (80, 80, 80)]
+GRIDS = [(192, 96, 96), (160, 80, 40), (161, 81, 41), (256, 256, 8), (203, 67, 35), (80, 80, 80)]
 
 
 @pytest.mark.parametrize("grid", GRIDS)
