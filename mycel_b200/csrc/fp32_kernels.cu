@@ -2086,7 +2086,8 @@ __global__ void __launch_bounds__(kMgDofThreads) k_mg_apply(MgDims d, const floa
 // is released by one CTA barrier. Each product is the same fmaf chain in the same order as mg_apply_node, so
 // the results are bit-identical to it: where the neighbour lies outside the grid, x is 0 and the staged value
 // (another node's entry, the zero padding or TMA's zero fill) is finite, so its products are signed zeros,
-// which leave the accumulators unchanged (they start at +0 and an fma never turns them into -0).
+// which leave an accumulator unchanged unless it is -0 (it starts at +0 and reaches -0 only when a partial sum
+// underflows to zero from below; then only the sign of that zero could differ from the gather's).
 constexpr int kS1Nodes = 252;   // nodes per CTA (+ up to 3 of rounding <= kS1Box)
 constexpr int kS1Box = 256;     // staged nodes per row
 constexpr int kS1Stages = 6;
